@@ -1,0 +1,386 @@
+/*
+ * prism_gpu.h — C ABI of the B200 (sm_100a) hash join / hash aggregate /
+ * filter-project engine.
+ *
+ * The entry points mirror the Rust operator API of prism-executor
+ * (native/prism-executor/src/lib.rs:5-15) one function per reference
+ * function, with arrow-rs `RecordBatch` carried across the boundary as the
+ * Arrow C Data Interface (prism_arrow_c.h). Every function:
+ *   - borrows its inputs; outputs are new objects owned by the caller;
+ *   - returns a status code (PRISM_OK or one of PRISM_ERR_*) and never aborts
+ *     the process; the message of the last failure on a context is available
+ *     from prism_last_error();
+ *   - is safe to call from several host threads on the same context (calls
+ *     are serialised on the context's stream; use one context per stream for
+ *     overlap).
+ *
+ * Two call styles exist:
+ *   1. "Arrow" style (suffix _arrow): host ArrowArray/ArrowSchema in, host
+ *      ArrowArray/ArrowSchema out. Each call uploads its inputs, runs on the
+ *      device and downloads the result — the drop-in replacement for the
+ *      reference function of the same name.
+ *   2. Resident style: prism_batch handles that live in device memory
+ *      (imported once with prism_batch_import / prism_batch_import_device and
+ *      exported with prism_batch_export). Operators chain on the device with
+ *      no host round trip; build-side hash tables stay resident across probes
+ *      (the analogue of the reference's PartitionStore,
+ *      native/prism-flight/src/shuffle_writer.rs:42-86).
+ *
+ * Tree-shaped configuration (Predicate, ScalarExpr) crosses as flat arrays of
+ * POD nodes in post-order (children before parent).
+ */
+#ifndef PRISM_GPU_H
+#define PRISM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "prism_arrow_c.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes. 1..7 mirror the PrismError variants                         */
+/* (native/prism-executor/src/error.rs:6-27); 8..11 are device conditions.   */
+/* ------------------------------------------------------------------------ */
+#define PRISM_OK 0
+#define PRISM_ERR_ARROW 1
+#define PRISM_ERR_SCHEMA_MISMATCH 2
+#define PRISM_ERR_INVALID_ARGUMENT 3
+#define PRISM_ERR_EXECUTION 4
+#define PRISM_ERR_JOIN 5
+#define PRISM_ERR_UNSUPPORTED_AGGREGATION 6
+#define PRISM_ERR_INTERNAL 7
+#define PRISM_ERR_TABLE_FULL 8
+#define PRISM_ERR_NO_MEMORY 9
+#define PRISM_ERR_TIMEOUT 10
+#define PRISM_ERR_CUDA 11
+
+/* ------------------------------------------------------------------------ */
+/* Configuration PODs                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* JoinType (native/prism-executor/src/hash_join.rs:48-56). */
+#define PRISM_JOIN_INNER 0
+#define PRISM_JOIN_LEFT 1
+#define PRISM_JOIN_RIGHT 2
+#define PRISM_JOIN_FULL 3
+#define PRISM_JOIN_LEFT_SEMI 4
+#define PRISM_JOIN_LEFT_ANTI 5
+
+/* HashJoinConfig (hash_join.rs:59-64). probe_keys[i] pairs with build_keys[i]. */
+typedef struct prism_join_config {
+  int32_t join_type;
+  int32_t n_keys;
+  const int32_t* probe_keys;
+  const int32_t* build_keys;
+} prism_join_config;
+
+/* AggFunc (native/prism-executor/src/hash_aggregate.rs:79-86). */
+#define PRISM_AGG_SUM 0
+#define PRISM_AGG_COUNT 1
+#define PRISM_AGG_AVG 2
+#define PRISM_AGG_MIN 3
+#define PRISM_AGG_MAX 4
+#define PRISM_AGG_COUNT_DISTINCT 5
+
+/* AggExpr (hash_aggregate.rs:90-94). */
+typedef struct prism_agg_expr {
+  int32_t column;
+  int32_t func;
+  const char* output_name; /* NUL-terminated UTF-8 */
+} prism_agg_expr;
+
+/* HashAggConfig (hash_aggregate.rs:98-101). */
+typedef struct prism_agg_config {
+  int32_t n_group_by;
+  const int32_t* group_by;
+  int32_t n_aggs;
+  const prism_agg_expr* aggs;
+} prism_agg_config;
+
+/* ScalarValue (native/prism-executor/src/filter_project.rs:55-62). */
+#define PRISM_SCALAR_INT32 0
+#define PRISM_SCALAR_INT64 1
+#define PRISM_SCALAR_FLOAT64 2
+#define PRISM_SCALAR_UTF8 3
+#define PRISM_SCALAR_BOOLEAN 4
+#define PRISM_SCALAR_DATE32 5
+
+typedef struct prism_scalar {
+  int32_t type;     /* PRISM_SCALAR_* */
+  int32_t reserved;
+  int64_t i64;      /* INT32, INT64, DATE32, BOOLEAN (0/1) */
+  double f64;       /* FLOAT64 */
+  const char* str;  /* UTF8 bytes (not necessarily NUL-terminated) */
+  int64_t str_len;
+} prism_scalar;
+
+/* Predicate (filter_project.rs:22-51). */
+#define PRISM_PRED_LITERAL 0
+#define PRISM_PRED_EQ 1
+#define PRISM_PRED_NE 2
+#define PRISM_PRED_LT 3
+#define PRISM_PRED_LE 4
+#define PRISM_PRED_GT 5
+#define PRISM_PRED_GE 6
+#define PRISM_PRED_IS_NULL 7
+#define PRISM_PRED_IS_NOT_NULL 8
+#define PRISM_PRED_AND 9
+#define PRISM_PRED_OR 10
+#define PRISM_PRED_NOT 11
+#define PRISM_PRED_LIKE 12
+#define PRISM_PRED_ILIKE 13
+
+/* One predicate node. LITERAL uses value.i64 (0/1); comparisons use column +
+ * value; IS_NULL/IS_NOT_NULL use column; LIKE/ILIKE use column + value.str as
+ * the pattern; AND/OR pop two operands, NOT pops one. */
+typedef struct prism_pred_node {
+  int32_t op;
+  int32_t column;
+  prism_scalar value;
+} prism_pred_node;
+
+typedef struct prism_predicate {
+  const prism_pred_node* nodes; /* post-order */
+  int32_t n_nodes;
+} prism_predicate;
+
+/* ScalarExpr (filter_project.rs:186-213). */
+#define PRISM_EXPR_COLUMN 0
+#define PRISM_EXPR_LITERAL 1
+#define PRISM_EXPR_ADD 2
+#define PRISM_EXPR_SUB 3
+#define PRISM_EXPR_MUL 4
+#define PRISM_EXPR_DIV 5
+#define PRISM_EXPR_NEG 6
+#define PRISM_EXPR_IF_THEN 7
+
+/* One expression node. ADD..DIV pop two operands (left pushed first), NEG
+ * pops one. IF_THEN pops n_clauses "then" expressions followed by the else
+ * expression when has_else != 0 (all pushed in that order); clause i's
+ * predicate is preds[clauses[clause_begin + i].pred_begin ...
+ * + pred_len) of the enclosing prism_expr. */
+typedef struct prism_expr_node {
+  int32_t op;
+  int32_t column;
+  prism_scalar literal;
+  int32_t n_clauses;
+  int32_t has_else;
+  int32_t clause_begin;
+  int32_t reserved;
+} prism_expr_node;
+
+typedef struct prism_expr_clause {
+  int32_t pred_begin;
+  int32_t pred_len;
+} prism_expr_clause;
+
+typedef struct prism_expr {
+  const prism_expr_node* nodes; /* post-order */
+  int32_t n_nodes;
+  const prism_pred_node* preds; /* pool for IF_THEN clause predicates */
+  int32_t n_preds;
+  const prism_expr_clause* clauses;
+  int32_t n_clauses;
+} prism_expr;
+
+/* Arithmetic mode of projected expressions.
+ * F64: the reference's semantics — both operands of every binary operation
+ *      are cast to Float64 (filter_project.rs:233-247).
+ * EXACT: integer and decimal operands are computed exactly in 128-bit
+ *      integers (decimal scales add under MUL and align under ADD/SUB); the
+ *      result column is Decimal128(38, s); sums over it are exact. Division
+ *      and any Float64 operand fall back to F64 for that node. */
+#define PRISM_ARITH_F64 0
+#define PRISM_ARITH_EXACT 1
+
+/* Special output-column codes for prism_join_project. */
+#define PRISM_COL_PROBE_ROW_INDEX (-1)
+#define PRISM_COL_BUILD_ROW_INDEX (-2)
+
+/* ------------------------------------------------------------------------ */
+/* Opaque handles                                                            */
+/* ------------------------------------------------------------------------ */
+typedef struct prism_ctx prism_ctx;
+typedef struct prism_batch prism_batch;
+typedef struct prism_hash_table prism_hash_table;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device`. memory_budget_bytes caps the
+ * device memory the context's allocator may hold (0 = 90% of free memory);
+ * allocations over budget fail with PRISM_ERR_NO_MEMORY. */
+int prism_ctx_create(int device, uint64_t memory_budget_bytes, prism_ctx** out);
+void prism_ctx_destroy(prism_ctx* ctx);
+/* Message of the last failed call on this context ("" if none). The pointer
+ * stays valid until the next call on the context. */
+const char* prism_last_error(const prism_ctx* ctx);
+/* Runs subsequent work on `cuda_stream` (a cudaStream_t; NULL restores the
+ * context's own stream). */
+int prism_ctx_set_stream(prism_ctx* ctx, void* cuda_stream);
+int prism_ctx_synchronize(prism_ctx* ctx);
+/* Device bytes currently held by the context's allocator. */
+uint64_t prism_ctx_bytes_in_use(const prism_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+uint64_t prism_ctx_kernel_launches(const prism_ctx* ctx);
+const char* prism_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident batches                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Copies a host RecordBatch (exported as a struct array) to the device.
+ * The caller keeps ownership of `array`/`schema` (they are not released). */
+int prism_batch_import(prism_ctx* ctx, const struct ArrowArray* array,
+                       const struct ArrowSchema* schema, prism_batch** out);
+/* Wraps a batch whose buffers already live in device memory (device_type
+ * ARROW_DEVICE_CUDA) without copying; the caller keeps the buffers alive for
+ * the lifetime of the batch. Host (ARROW_DEVICE_CPU / CUDA_HOST) arrays are
+ * copied as by prism_batch_import. */
+int prism_batch_import_device(prism_ctx* ctx, const struct ArrowDeviceArray* array,
+                              const struct ArrowSchema* schema, prism_batch** out);
+/* Copies a device batch back to host memory as a struct array. The caller
+ * owns the result and must call its release callbacks. */
+int prism_batch_export(prism_ctx* ctx, const prism_batch* batch,
+                       struct ArrowArray* out_array, struct ArrowSchema* out_schema);
+int64_t prism_batch_num_rows(const prism_batch* batch);
+int32_t prism_batch_num_columns(const prism_batch* batch);
+void prism_batch_free(prism_batch* batch);
+
+/* ------------------------------------------------------------------------ */
+/* Hash join (native/prism-executor/src/hash_join.rs)                        */
+/* ------------------------------------------------------------------------ */
+
+/* HashTable::build (hash_join.rs:87-141). The table keeps a reference to the
+ * build batch; the batch must outlive the table. */
+int prism_hash_table_build(prism_ctx* ctx, const prism_batch* build,
+                           const int32_t* key_cols, int32_t n_keys,
+                           prism_hash_table** out);
+/* HashTable::probe (hash_join.rs:143-200). Output: 2 columns
+ * (probe_idx UInt32, build_idx UInt32), probe rows ascending and, per probe
+ * row, build rows ascending — the reference's emission order. */
+int prism_hash_table_probe(prism_ctx* ctx, const prism_hash_table* table,
+                           const prism_batch* probe, const int32_t* key_cols,
+                           int32_t n_keys, prism_batch** out);
+int64_t prism_hash_table_num_rows(const prism_hash_table* table);
+int prism_hash_table_has_duplicates(const prism_hash_table* table);
+void prism_hash_table_free(prism_hash_table* table);
+
+/* Fused probe + gather: emits the selected columns of the inner join of
+ * `probe` with the table's build batch, in the reference's match order.
+ * out_cols index the joined schema (probe columns, then build columns, as in
+ * executor.rs:474-551 project_join_matches); PRISM_COL_PROBE_ROW_INDEX and
+ * PRISM_COL_BUILD_ROW_INDEX emit the matched row indices as UInt32. */
+int prism_join_project(prism_ctx* ctx, const prism_hash_table* table,
+                       const prism_batch* probe, const int32_t* probe_keys,
+                       int32_t n_keys, const int32_t* out_cols, int32_t n_out,
+                       prism_batch** out);
+
+/* hash_join (hash_join.rs:312-365). */
+int prism_hash_join(prism_ctx* ctx, const prism_batch* probe, const prism_batch* build,
+                    const prism_join_config* config, prism_batch** out);
+/* probe_matches_chunked (hash_join.rs:286-309): one (probe_idx, build_idx)
+ * batch per probe batch, written to out[0..n_probes). */
+int prism_probe_matches_chunked(prism_ctx* ctx, const prism_batch* const* probes,
+                                int32_t n_probes, const prism_batch* build,
+                                const int32_t* probe_keys, const int32_t* build_keys,
+                                int32_t n_keys, prism_batch** out);
+/* hash_join_probe_chunked (hash_join.rs:206-282): empty outputs are
+ * dropped; *n_out receives the number written to out (capacity n_probes). */
+int prism_hash_join_probe_chunked(prism_ctx* ctx, const prism_batch* const* probes,
+                                  int32_t n_probes, const prism_batch* build,
+                                  const prism_join_config* config, prism_batch** out,
+                                  int32_t* n_out);
+
+/* ------------------------------------------------------------------------ */
+/* Hash aggregation (native/prism-executor/src/hash_aggregate.rs)            */
+/* ------------------------------------------------------------------------ */
+
+/* hash_aggregate (hash_aggregate.rs:174-176). */
+int prism_hash_aggregate(prism_ctx* ctx, const prism_batch* batch,
+                         const prism_agg_config* config, prism_batch** out);
+/* hash_aggregate_batches (hash_aggregate.rs:182-339). Groups are emitted in
+ * first-seen order over the concatenated batches, as the reference does. */
+int prism_hash_aggregate_batches(prism_ctx* ctx, const prism_batch* const* batches,
+                                 int32_t n_batches, const prism_agg_config* config,
+                                 prism_batch** out);
+
+/* ------------------------------------------------------------------------ */
+/* Filter / project (native/prism-executor/src/filter_project.rs)            */
+/* ------------------------------------------------------------------------ */
+
+/* evaluate_predicate (filter_project.rs:65-123): one Boolean column. */
+int prism_evaluate_predicate(prism_ctx* ctx, const prism_batch* batch,
+                             const prism_predicate* predicate, prism_batch** out_mask);
+/* filter_batch (filter_project.rs:126-135); mask = a 1-column Boolean batch. */
+int prism_filter_batch(prism_ctx* ctx, const prism_batch* batch, const prism_batch* mask,
+                       prism_batch** out);
+/* project_batch (filter_project.rs:138-160). */
+int prism_project_batch(prism_ctx* ctx, const prism_batch* batch, const int32_t* cols,
+                        int32_t n_cols, prism_batch** out);
+/* filter_and_project (filter_project.rs:163-180); predicate may be NULL. */
+int prism_filter_and_project(prism_ctx* ctx, const prism_batch* batch,
+                             const prism_predicate* predicate, const int32_t* cols,
+                             int32_t n_cols, prism_batch** out);
+/* evaluate_scalar_expr (filter_project.rs:216-294): one column. */
+int prism_evaluate_scalar_expr(prism_ctx* ctx, const prism_batch* batch,
+                               const prism_expr* expr, int32_t arith_mode,
+                               prism_batch** out);
+/* project_batch_with_exprs (filter_project.rs:305-333). */
+int prism_project_batch_with_exprs(prism_ctx* ctx, const prism_batch* batch,
+                                   const int32_t* cols, int32_t n_cols,
+                                   const prism_expr* exprs, int32_t n_exprs,
+                                   int32_t arith_mode, prism_batch** out);
+
+/* ------------------------------------------------------------------------ */
+/* Fused operators                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* filter -> project_batch_with_exprs -> hash_aggregate_batches in one pass
+ * over the input (no filtered or projected intermediate is materialised).
+ * The aggregate config indexes the projected schema (cols, then expr_i). */
+int prism_filter_project_aggregate(prism_ctx* ctx, const prism_batch* const* batches,
+                                   int32_t n_batches, const prism_predicate* predicate,
+                                   const int32_t* cols, int32_t n_cols,
+                                   const prism_expr* exprs, int32_t n_exprs,
+                                   int32_t arith_mode, const prism_agg_config* agg,
+                                   prism_batch** out);
+/* Inner join -> project -> aggregate, the semantics of the reference's fused
+ * join-aggregate (native/prism-substrait/src/executor.rs:333-458): cols and
+ * exprs index the joined schema; the aggregate config indexes the projected
+ * schema. No joined rows are materialised. */
+int prism_join_aggregate(prism_ctx* ctx, const prism_batch* const* probes, int32_t n_probes,
+                         const prism_batch* build, const int32_t* probe_keys,
+                         const int32_t* build_keys, int32_t n_keys, const int32_t* cols,
+                         int32_t n_cols, const prism_expr* exprs, int32_t n_exprs,
+                         const prism_agg_config* agg, prism_batch** out);
+
+/* ------------------------------------------------------------------------ */
+/* Arrow-style wrappers: host batches in, host batch out                     */
+/* ------------------------------------------------------------------------ */
+int prism_hash_join_arrow(prism_ctx* ctx, const struct ArrowArray* probe,
+                          const struct ArrowSchema* probe_schema,
+                          const struct ArrowArray* build,
+                          const struct ArrowSchema* build_schema,
+                          const prism_join_config* config, struct ArrowArray* out,
+                          struct ArrowSchema* out_schema);
+int prism_hash_aggregate_arrow(prism_ctx* ctx, const struct ArrowArray* batch,
+                               const struct ArrowSchema* schema,
+                               const prism_agg_config* config, struct ArrowArray* out,
+                               struct ArrowSchema* out_schema);
+int prism_filter_and_project_arrow(prism_ctx* ctx, const struct ArrowArray* batch,
+                                   const struct ArrowSchema* schema,
+                                   const prism_predicate* predicate, const int32_t* cols,
+                                   int32_t n_cols, struct ArrowArray* out,
+                                   struct ArrowSchema* out_schema);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRISM_GPU_H */

@@ -1,0 +1,467 @@
+"""prism_gpu — host mirror of prism-executor's operator API over the B200 engine.
+
+Every function here has the name, argument meaning and error behaviour of the
+reference Rust function it replaces (native/prism-executor/src/lib.rs:5-15)
+and runs on the GPU through the C ABI of libprism_gpu.so (include/prism_gpu.h).
+There is no CPU fallback: if the CUDA library is missing or cannot reach a
+device, calls raise ``PrismError``.
+
+Batches are pyarrow ``RecordBatch``es (arrow-rs ``RecordBatch`` on the
+reference side); device-resident batches are ``DeviceBatch`` handles.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import pyarrow as pa
+
+from . import _abi
+from .config import (  # noqa: F401  (re-exported API)
+    ARITH_EXACT,
+    ARITH_F64,
+    AggExpr,
+    AggFunc,
+    ArithmeticOp,
+    HashAggConfig,
+    HashJoinConfig,
+    JoinType,
+    Predicate,
+    ScalarExpr,
+    ScalarValue,
+    encode_exprs,
+)
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("PRISM_GPU_LIB", os.path.join(PKG_DIR, "libprism_gpu.so"))
+
+PRISM_COL_PROBE_ROW_INDEX = -1
+PRISM_COL_BUILD_ROW_INDEX = -2
+
+
+class PrismError(RuntimeError):
+    """Mirrors PrismError (native/prism-executor/src/error.rs:6-27)."""
+
+    def __init__(self, code: int, msg: str):
+        self.code = code
+        self.kind = _abi.ERROR_NAMES.get(code, str(code))
+        super().__init__(f"{self.kind}: {msg}")
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def _declare(lib):
+    P = C.c_void_p
+    I = C.c_int
+    i32 = C.c_int32
+    lib.prism_ctx_create.argtypes = [I, C.c_uint64, C.POINTER(P)]
+    lib.prism_ctx_destroy.argtypes = [P]
+    lib.prism_ctx_destroy.restype = None
+    lib.prism_last_error.argtypes = [P]
+    lib.prism_last_error.restype = C.c_char_p
+    lib.prism_ctx_set_stream.argtypes = [P, P]
+    lib.prism_ctx_synchronize.argtypes = [P]
+    lib.prism_ctx_bytes_in_use.argtypes = [P]
+    lib.prism_ctx_bytes_in_use.restype = C.c_uint64
+    lib.prism_ctx_kernel_launches.argtypes = [P]
+    lib.prism_ctx_kernel_launches.restype = C.c_uint64
+    lib.prism_version.restype = C.c_char_p
+    lib.prism_batch_import.argtypes = [P, P, P, C.POINTER(P)]
+    lib.prism_batch_import_device.argtypes = [P, P, P, C.POINTER(P)]
+    lib.prism_batch_export.argtypes = [P, P, P, P]
+    lib.prism_batch_num_rows.argtypes = [P]
+    lib.prism_batch_num_rows.restype = C.c_int64
+    lib.prism_batch_num_columns.argtypes = [P]
+    lib.prism_batch_num_columns.restype = i32
+    lib.prism_batch_free.argtypes = [P]
+    lib.prism_batch_free.restype = None
+    lib.prism_hash_table_build.argtypes = [P, P, P, i32, C.POINTER(P)]
+    lib.prism_hash_table_probe.argtypes = [P, P, P, P, i32, C.POINTER(P)]
+    lib.prism_hash_table_num_rows.argtypes = [P]
+    lib.prism_hash_table_num_rows.restype = C.c_int64
+    lib.prism_hash_table_has_duplicates.argtypes = [P]
+    lib.prism_hash_table_free.argtypes = [P]
+    lib.prism_hash_table_free.restype = None
+    lib.prism_join_project.argtypes = [P, P, P, P, i32, P, i32, C.POINTER(P)]
+    lib.prism_hash_join.argtypes = [P, P, P, P, C.POINTER(P)]
+    lib.prism_probe_matches_chunked.argtypes = [P, P, i32, P, P, P, i32, P]
+    lib.prism_hash_join_probe_chunked.argtypes = [P, P, i32, P, P, P, C.POINTER(i32)]
+    lib.prism_hash_aggregate.argtypes = [P, P, P, C.POINTER(P)]
+    lib.prism_hash_aggregate_batches.argtypes = [P, P, i32, P, C.POINTER(P)]
+    lib.prism_evaluate_predicate.argtypes = [P, P, P, C.POINTER(P)]
+    lib.prism_filter_batch.argtypes = [P, P, P, C.POINTER(P)]
+    lib.prism_project_batch.argtypes = [P, P, P, i32, C.POINTER(P)]
+    lib.prism_filter_and_project.argtypes = [P, P, P, P, i32, C.POINTER(P)]
+    lib.prism_evaluate_scalar_expr.argtypes = [P, P, P, i32, C.POINTER(P)]
+    lib.prism_project_batch_with_exprs.argtypes = [P, P, P, i32, P, i32, i32, C.POINTER(P)]
+    lib.prism_filter_project_aggregate.argtypes = [P, P, i32, P, P, i32, P, i32, i32, P, C.POINTER(P)]
+    lib.prism_join_aggregate.argtypes = [P, P, i32, P, P, P, i32, P, i32, P, i32, P, C.POINTER(P)]
+    lib.prism_hash_join_arrow.argtypes = [P, P, P, P, P, P, P, P]
+    lib.prism_hash_aggregate_arrow.argtypes = [P, P, P, P, P, P]
+    lib.prism_filter_and_project_arrow.argtypes = [P, P, P, P, P, i32, P, P]
+
+
+def lib():
+    """Loads libprism_gpu.so (raises PrismError if it is absent)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise PrismError(11, f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+            lib_ = C.CDLL(LIB_PATH)
+            _declare(lib_)
+            _lib = lib_
+    return _lib
+
+
+class Context:
+    """A device context (prism_ctx): stream, allocator and counters."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 0):
+        self._h = C.c_void_p()
+        rc = lib().prism_ctx_create(device, memory_budget, C.byref(self._h))
+        if rc != 0:
+            raise PrismError(rc, "prism_ctx_create failed (no usable CUDA device?)")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc: int):
+        if rc != 0:
+            msg = lib().prism_last_error(self._h)
+            raise PrismError(rc, msg.decode(errors="replace") if msg else "")
+
+    def synchronize(self):
+        self.check(lib().prism_ctx_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self.check(lib().prism_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib().prism_ctx_bytes_in_use(self._h))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().prism_ctx_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            lib().prism_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(int(os.environ.get("PRISM_GPU_DEVICE", "0")))
+    return _default_ctx
+
+
+class DeviceBatch:
+    """A device-resident RecordBatch (prism_batch)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, keepalive=None):
+        self.ctx = ctx
+        self._h = handle
+        self._keep = keepalive
+
+    @staticmethod
+    def from_arrow(batch: pa.RecordBatch, ctx: Optional[Context] = None) -> "DeviceBatch":
+        ctx = ctx or default_context()
+        e = _abi.ExportedBatch(batch)
+        h = C.c_void_p()
+        ctx.check(lib().prism_batch_import(ctx.handle, e.array_ptr, e.schema_ptr, C.byref(h)))
+        e.release()
+        return DeviceBatch(ctx, h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_rows(self) -> int:
+        return int(lib().prism_batch_num_rows(self._h))
+
+    @property
+    def num_columns(self) -> int:
+        return int(lib().prism_batch_num_columns(self._h))
+
+    def to_arrow(self) -> pa.RecordBatch:
+        a, s = _abi.ArrowArray(), _abi.ArrowSchema()
+        self.ctx.check(lib().prism_batch_export(self.ctx.handle, self._h, C.byref(a), C.byref(s)))
+        return _abi.import_batch(a, s)
+
+    def free(self):
+        if self._h:
+            lib().prism_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _dev(batch, ctx) -> DeviceBatch:
+    if isinstance(batch, DeviceBatch):
+        return batch
+    return DeviceBatch.from_arrow(batch, ctx)
+
+
+def _ptrs(batches: Sequence[DeviceBatch]):
+    arr = (C.c_void_p * max(1, len(batches)))()
+    for i, b in enumerate(batches):
+        arr[i] = b.handle
+    return arr
+
+
+def _result(ctx, h, as_device: bool):
+    db = DeviceBatch(ctx, h)
+    return db if as_device else db.to_arrow()
+
+
+# ------------------------------------------------------------ hash join ----
+
+
+@dataclass
+class ProbeMatches:
+    """hash_join.rs:67-70."""
+
+    probe_indices: pa.Array
+    build_indices: pa.Array
+
+
+class HashTable:
+    """Resident build-side table (HashTable, hash_join.rs:77-201)."""
+
+    def __init__(self, ctx: Context, handle, build: DeviceBatch):
+        self.ctx = ctx
+        self._h = handle
+        self._build = build
+
+    @staticmethod
+    def build(batch, key_cols: Sequence[int], ctx: Optional[Context] = None) -> "HashTable":
+        ctx = ctx or default_context()
+        db = _dev(batch, ctx)
+        keys = _abi.int_array(key_cols)
+        h = C.c_void_p()
+        ctx.check(lib().prism_hash_table_build(ctx.handle, db.handle, keys, len(key_cols), C.byref(h)))
+        return HashTable(ctx, h, db)
+
+    def probe(self, probe_batch, probe_key_cols: Sequence[int], as_device=False):
+        db = _dev(probe_batch, self.ctx)
+        keys = _abi.int_array(probe_key_cols)
+        h = C.c_void_p()
+        self.ctx.check(lib().prism_hash_table_probe(self.ctx.handle, self._h, db.handle, keys, len(probe_key_cols), C.byref(h)))
+        out = _result(self.ctx, h, as_device)
+        if as_device:
+            return out
+        return out.column(0), out.column(1)
+
+    def join_project(self, probe_batch, probe_key_cols: Sequence[int], out_cols: Sequence[int], as_device=False):
+        db = _dev(probe_batch, self.ctx)
+        keys = _abi.int_array(probe_key_cols)
+        oc = _abi.int_array(out_cols)
+        h = C.c_void_p()
+        self.ctx.check(
+            lib().prism_join_project(self.ctx.handle, self._h, db.handle, keys, len(probe_key_cols), oc, len(out_cols), C.byref(h))
+        )
+        return _result(self.ctx, h, as_device)
+
+    @property
+    def has_duplicates(self) -> bool:
+        return bool(lib().prism_hash_table_has_duplicates(self._h))
+
+    def free(self):
+        if self._h:
+            lib().prism_hash_table_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def hash_join(probe_batch, build_batch, config: HashJoinConfig, ctx: Optional[Context] = None, as_device=False):
+    """hash_join (hash_join.rs:312-365)."""
+    ctx = ctx or default_context()
+    p, b = _dev(probe_batch, ctx), _dev(build_batch, ctx)
+    cfg = config.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_hash_join(ctx.handle, p.handle, b.handle, C.byref(cfg), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def probe_matches_chunked(probe_batches, build_batch, probe_key_cols, build_key_cols, ctx: Optional[Context] = None) -> List[ProbeMatches]:
+    """probe_matches_chunked (hash_join.rs:286-309)."""
+    ctx = ctx or default_context()
+    ps = [_dev(p, ctx) for p in probe_batches]
+    b = _dev(build_batch, ctx)
+    outs = (C.c_void_p * max(1, len(ps)))()
+    pk, bk = _abi.int_array(probe_key_cols), _abi.int_array(build_key_cols)
+    ctx.check(lib().prism_probe_matches_chunked(ctx.handle, _ptrs(ps), len(ps), b.handle, pk, bk, len(probe_key_cols), outs))
+    res = []
+    for i in range(len(ps)):
+        rb = DeviceBatch(ctx, C.c_void_p(outs[i])).to_arrow()
+        res.append(ProbeMatches(rb.column(0), rb.column(1)))
+    return res
+
+
+def hash_join_probe_chunked(probe_batches, build_batch, config: HashJoinConfig, ctx: Optional[Context] = None) -> List[pa.RecordBatch]:
+    """hash_join_probe_chunked (hash_join.rs:206-282)."""
+    ctx = ctx or default_context()
+    ps = [_dev(p, ctx) for p in probe_batches]
+    b = _dev(build_batch, ctx)
+    outs = (C.c_void_p * max(1, len(ps)))()
+    n_out = C.c_int32(0)
+    cfg = config.encode()
+    ctx.check(lib().prism_hash_join_probe_chunked(ctx.handle, _ptrs(ps), len(ps), b.handle, C.byref(cfg), outs, C.byref(n_out)))
+    return [DeviceBatch(ctx, C.c_void_p(outs[i])).to_arrow() for i in range(n_out.value)]
+
+
+# ------------------------------------------------------------ aggregate ----
+
+
+def hash_aggregate_batches(batches, config: HashAggConfig, ctx: Optional[Context] = None, as_device=False):
+    """hash_aggregate_batches (hash_aggregate.rs:182-339)."""
+    ctx = ctx or default_context()
+    ds = [_dev(b, ctx) for b in batches]
+    cfg = config.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_hash_aggregate_batches(ctx.handle, _ptrs(ds), len(ds), C.byref(cfg), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def hash_aggregate(batch, config: HashAggConfig, ctx: Optional[Context] = None, as_device=False):
+    """hash_aggregate (hash_aggregate.rs:174-176)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    cfg = config.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_hash_aggregate(ctx.handle, d.handle, C.byref(cfg), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+# ------------------------------------------------------- filter / project --
+
+
+def evaluate_predicate(batch, predicate: Predicate, ctx: Optional[Context] = None) -> pa.Array:
+    """evaluate_predicate (filter_project.rs:65-123)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    p = predicate.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_evaluate_predicate(ctx.handle, d.handle, C.byref(p), C.byref(h)))
+    return DeviceBatch(ctx, h).to_arrow().column(0)
+
+
+def filter_batch(batch, mask, ctx: Optional[Context] = None, as_device=False):
+    """filter_batch (filter_project.rs:126-135)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    if isinstance(mask, DeviceBatch):
+        m = mask
+    else:
+        m = DeviceBatch.from_arrow(pa.RecordBatch.from_arrays([mask], names=["mask"]), ctx)
+    h = C.c_void_p()
+    ctx.check(lib().prism_filter_batch(ctx.handle, d.handle, m.handle, C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def project_batch(batch, column_indices: Sequence[int], ctx: Optional[Context] = None, as_device=False):
+    """project_batch (filter_project.rs:138-160)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    c = _abi.int_array(column_indices)
+    h = C.c_void_p()
+    ctx.check(lib().prism_project_batch(ctx.handle, d.handle, c, len(column_indices), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def filter_and_project(batch, predicate: Optional[Predicate], column_indices: Sequence[int], ctx: Optional[Context] = None, as_device=False):
+    """filter_and_project (filter_project.rs:163-180)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    p = predicate.encode() if predicate is not None else None
+    c = _abi.int_array(column_indices)
+    h = C.c_void_p()
+    ctx.check(lib().prism_filter_and_project(ctx.handle, d.handle, C.byref(p) if p is not None else None, c, len(column_indices), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def evaluate_scalar_expr(batch, expr: ScalarExpr, arith_mode: int = ARITH_F64, ctx: Optional[Context] = None) -> pa.Array:
+    """evaluate_scalar_expr (filter_project.rs:216-294)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    e = expr.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_evaluate_scalar_expr(ctx.handle, d.handle, C.byref(e), arith_mode, C.byref(h)))
+    return DeviceBatch(ctx, h).to_arrow().column(0)
+
+
+def project_batch_with_exprs(batch, column_indices: Sequence[int], expressions: Sequence[ScalarExpr], arith_mode: int = ARITH_F64, ctx: Optional[Context] = None, as_device=False):
+    """project_batch_with_exprs (filter_project.rs:305-333)."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    c = _abi.int_array(column_indices)
+    ex = encode_exprs(expressions)
+    h = C.c_void_p()
+    ctx.check(lib().prism_project_batch_with_exprs(ctx.handle, d.handle, c, len(column_indices), ex, len(expressions), arith_mode, C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+# ------------------------------------------------------------------ fused --
+
+
+def filter_project_aggregate(batches, predicate: Optional[Predicate], column_indices: Sequence[int], expressions: Sequence[ScalarExpr], agg: HashAggConfig, arith_mode: int = ARITH_F64, ctx: Optional[Context] = None, as_device=False):
+    """Filter -> project -> aggregate in one pass (executor.rs:91-186 node chain)."""
+    ctx = ctx or default_context()
+    ds = [_dev(b, ctx) for b in batches]
+    p = predicate.encode() if predicate is not None else None
+    c = _abi.int_array(column_indices)
+    ex = encode_exprs(expressions)
+    cfg = agg.encode()
+    h = C.c_void_p()
+    ctx.check(
+        lib().prism_filter_project_aggregate(
+            ctx.handle, _ptrs(ds), len(ds), C.byref(p) if p is not None else None, c, len(column_indices), ex, len(expressions), arith_mode, C.byref(cfg), C.byref(h)
+        )
+    )
+    return _result(ctx, h, as_device)
+
+
+def join_aggregate(probe_batches, build_batch, probe_keys, build_keys, column_indices: Sequence[int], expressions: Sequence[ScalarExpr], agg: HashAggConfig, ctx: Optional[Context] = None, as_device=False):
+    """Fused inner join -> project -> aggregate (executor.rs:333-458)."""
+    ctx = ctx or default_context()
+    ps = [_dev(b, ctx) for b in probe_batches]
+    b = _dev(build_batch, ctx)
+    pk, bk = _abi.int_array(probe_keys), _abi.int_array(build_keys)
+    c = _abi.int_array(column_indices)
+    ex = encode_exprs(expressions)
+    cfg = agg.encode()
+    h = C.c_void_p()
+    ctx.check(
+        lib().prism_join_aggregate(
+            ctx.handle, _ptrs(ps), len(ps), b.handle, pk, bk, len(probe_keys), c, len(column_indices), ex, len(expressions), C.byref(cfg), C.byref(h)
+        )
+    )
+    return _result(ctx, h, as_device)

@@ -1,0 +1,219 @@
+"""Python face of the CPU oracle (oracle/liboracle.so) — TEST INFRASTRUCTURE.
+
+Only the test-suite, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
+baseline use this module; the product path never imports it. Signatures
+mirror ``prism_gpu``'s so parity tests read ``oracle.f(...) == prism_gpu.f(...)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+from typing import List, Optional, Sequence
+
+import pyarrow as pa
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "prism-query_b200"))
+
+from prism_gpu import _abi  # noqa: E402
+from prism_gpu.config import (  # noqa: E402
+    ARITH_F64,
+    HashAggConfig,
+    HashJoinConfig,
+    Predicate,
+    ScalarExpr,
+    encode_exprs,
+)
+
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_abi.ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+        self.kind = _abi.ERROR_NAMES.get(code, str(code))
+
+
+def build_oracle() -> str:
+    srcs = ["oracle.cpp", "oracle_arrow.hpp", "oracle.h"]
+    newest = max(os.path.getmtime(os.path.join(ORACLE_DIR, s)) for s in srcs)
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < newest:
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+    return ORACLE_SO
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build_oracle())
+        _lib.oracle_last_error.restype = C.c_char_p
+        _lib.oracle_join_count_matches.restype = C.c_int64
+        _lib.oracle_exact_sum_f64.restype = C.c_double
+        _lib.oracle_exact_sum_f64.argtypes = [C.c_void_p, C.c_int64]
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise OracleError(rc, lib().oracle_last_error().decode(errors="replace"))
+
+
+def _ptr_array(exported: Sequence[_abi.ExportedBatch]):
+    arr = (C.POINTER(_abi.ArrowArray) * max(1, len(exported)))()
+    for i, e in enumerate(exported):
+        arr[i] = e.array_ptr
+    return arr
+
+
+def _out():
+    return _abi.ArrowArray(), _abi.ArrowSchema()
+
+
+def _take(a, s) -> pa.RecordBatch:
+    return _abi.import_batch(a, s)
+
+
+def _schema_of(batches, fallback: Optional[pa.Schema] = None):
+    schema = batches[0].schema if batches else fallback
+    if schema is None:
+        return None, None
+    es = _abi.ExportedBatch(pa.RecordBatch.from_arrays([pa.array([], type=f.type) for f in schema], schema=schema))
+    return es, es.schema_ptr
+
+
+DEFAULT_THREADS = 1
+
+
+def hash_join(probe: pa.RecordBatch, build: pa.RecordBatch, config: HashJoinConfig, n_threads: int = DEFAULT_THREADS):
+    ep, eb = _abi.ExportedBatch(probe), _abi.ExportedBatch(build)
+    cfg = config.encode()
+    a, s = _out()
+    _check(lib().oracle_hash_join(ep.array_ptr, ep.schema_ptr, eb.array_ptr, eb.schema_ptr, C.byref(cfg), n_threads, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def probe_matches_chunked(probes: List[pa.RecordBatch], build: pa.RecordBatch, probe_keys, build_keys, n_threads: int = DEFAULT_THREADS):
+    eps = [_abi.ExportedBatch(p) for p in probes]
+    eb = _abi.ExportedBatch(build)
+    outs = (_abi.ArrowArray * len(probes))()
+    schs = (_abi.ArrowSchema * len(probes))()
+    pk, bk = _abi.int_array(probe_keys), _abi.int_array(build_keys)
+    _check(lib().oracle_probe_matches_chunked(_ptr_array(eps), eps[0].schema_ptr, len(probes), eb.array_ptr, eb.schema_ptr, pk, bk, len(probe_keys), n_threads, outs, schs))
+    return [_take(outs[i], schs[i]) for i in range(len(probes))]
+
+
+def hash_join_probe_chunked(probes: List[pa.RecordBatch], build: pa.RecordBatch, config: HashJoinConfig, n_threads: int = DEFAULT_THREADS):
+    eps = [_abi.ExportedBatch(p) for p in probes]
+    eb = _abi.ExportedBatch(build)
+    outs = (_abi.ArrowArray * len(probes))()
+    schs = (_abi.ArrowSchema * len(probes))()
+    n_out = C.c_int(0)
+    cfg = config.encode()
+    _check(lib().oracle_hash_join_probe_chunked(_ptr_array(eps), eps[0].schema_ptr, len(probes), eb.array_ptr, eb.schema_ptr, C.byref(cfg), n_threads, outs, schs, C.byref(n_out)))
+    return [_take(outs[i], schs[i]) for i in range(n_out.value)]
+
+
+def join_count_matches(probes: List[pa.RecordBatch], build: pa.RecordBatch, probe_keys, build_keys, n_threads: int, materialize: int = 1) -> int:
+    eps = [_abi.ExportedBatch(p) for p in probes]
+    eb = _abi.ExportedBatch(build)
+    pk, bk = _abi.int_array(probe_keys), _abi.int_array(build_keys)
+    r = lib().oracle_join_count_matches(_ptr_array(eps), eps[0].schema_ptr, len(probes), eb.array_ptr, eb.schema_ptr, pk, bk, len(probe_keys), n_threads, materialize)
+    if r < 0:
+        _check(int(-r))
+    return int(r)
+
+
+def hash_aggregate_batches(batches: List[pa.RecordBatch], config: HashAggConfig, n_threads: int = DEFAULT_THREADS, schema: Optional[pa.Schema] = None):
+    eps = [_abi.ExportedBatch(b) for b in batches]
+    es, sptr = _schema_of(batches, schema)
+    cfg = config.encode()
+    a, s = _out()
+    _check(lib().oracle_hash_aggregate_batches(_ptr_array(eps), sptr, len(batches), C.byref(cfg), n_threads, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def hash_aggregate(batch: pa.RecordBatch, config: HashAggConfig, n_threads: int = DEFAULT_THREADS):
+    return hash_aggregate_batches([batch], config, n_threads)
+
+
+def evaluate_predicate(batch: pa.RecordBatch, predicate: Predicate) -> pa.Array:
+    e = _abi.ExportedBatch(batch)
+    p = predicate.encode()
+    a, s = _out()
+    _check(lib().oracle_evaluate_predicate(e.array_ptr, e.schema_ptr, C.byref(p), C.byref(a), C.byref(s)))
+    return _take(a, s).column(0)
+
+
+def filter_batch(batch: pa.RecordBatch, mask: pa.Array) -> pa.RecordBatch:
+    e = _abi.ExportedBatch(batch)
+    m = _abi.ExportedBatch(pa.RecordBatch.from_arrays([mask], names=["mask"]))
+    a, s = _out()
+    _check(lib().oracle_filter_batch(e.array_ptr, e.schema_ptr, m.array_ptr, m.schema_ptr, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def project_batch(batch: pa.RecordBatch, cols: Sequence[int]) -> pa.RecordBatch:
+    e = _abi.ExportedBatch(batch)
+    c = _abi.int_array(cols)
+    a, s = _out()
+    _check(lib().oracle_project_batch(e.array_ptr, e.schema_ptr, c, len(cols), C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def filter_and_project(batch: pa.RecordBatch, predicate: Optional[Predicate], cols: Sequence[int]) -> pa.RecordBatch:
+    e = _abi.ExportedBatch(batch)
+    p = predicate.encode() if predicate is not None else None
+    c = _abi.int_array(cols)
+    a, s = _out()
+    _check(lib().oracle_filter_and_project(e.array_ptr, e.schema_ptr, C.byref(p) if p is not None else None, c, len(cols), C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def project_batch_with_exprs(batch: pa.RecordBatch, cols: Sequence[int], exprs: Sequence[ScalarExpr], arith_mode: int = ARITH_F64) -> pa.RecordBatch:
+    e = _abi.ExportedBatch(batch)
+    c = _abi.int_array(cols)
+    ex = encode_exprs(exprs)
+    a, s = _out()
+    _check(lib().oracle_project_batch_with_exprs(e.array_ptr, e.schema_ptr, c, len(cols), ex, len(exprs), arith_mode, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def evaluate_scalar_expr(batch: pa.RecordBatch, expr: ScalarExpr, arith_mode: int = ARITH_F64) -> pa.Array:
+    return project_batch_with_exprs(batch, [], [expr], arith_mode).column(0)
+
+
+def filter_project_aggregate(batches: List[pa.RecordBatch], predicate: Optional[Predicate], cols: Sequence[int], exprs: Sequence[ScalarExpr], agg: HashAggConfig, arith_mode: int = ARITH_F64, n_threads: int = DEFAULT_THREADS):
+    eps = [_abi.ExportedBatch(b) for b in batches]
+    p = predicate.encode() if predicate is not None else None
+    c = _abi.int_array(cols)
+    ex = encode_exprs(exprs)
+    cfg = agg.encode()
+    a, s = _out()
+    _check(lib().oracle_filter_project_aggregate(_ptr_array(eps), eps[0].schema_ptr, len(batches), C.byref(p) if p is not None else None, c, len(cols), ex, len(exprs), arith_mode, C.byref(cfg), n_threads, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def join_aggregate(probes: List[pa.RecordBatch], build: pa.RecordBatch, probe_keys, build_keys, cols: Sequence[int], exprs: Sequence[ScalarExpr], agg: HashAggConfig, n_threads: int = DEFAULT_THREADS):
+    eps = [_abi.ExportedBatch(b) for b in probes]
+    eb = _abi.ExportedBatch(build)
+    pk, bk = _abi.int_array(probe_keys), _abi.int_array(build_keys)
+    c = _abi.int_array(cols)
+    ex = encode_exprs(exprs)
+    cfg = agg.encode()
+    a, s = _out()
+    _check(lib().oracle_join_aggregate(_ptr_array(eps), eps[0].schema_ptr, len(probes), eb.array_ptr, eb.schema_ptr, pk, bk, len(probe_keys), c, len(cols), ex, len(exprs), C.byref(cfg), n_threads, C.byref(a), C.byref(s)))
+    return _take(a, s)
+
+
+def exact_sum_f64(values) -> float:
+    import numpy as np
+
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    return float(lib().oracle_exact_sum_f64(v.ctypes.data, len(v)))
