@@ -228,6 +228,13 @@ int prism_ctx_synchronize(prism_ctx* ctx);
 uint64_t prism_ctx_bytes_in_use(const prism_ctx* ctx);
 /* Number of kernels this context has launched since creation. */
 uint64_t prism_ctx_kernel_launches(const prism_ctx* ctx);
+/* Per-kernel device timing: when enabled, the hot kernels (probe, build
+ * insert, aggregation, predicate, expression) are bracketed by CUDA events on
+ * the context's stream. prism_ctx_kernel_stats synchronises and returns the
+ * launch count and summed device milliseconds of the kernel `name` since
+ * profiling was (re-)enabled. */
+int prism_ctx_set_profiling(prism_ctx* ctx, int enable);
+int prism_ctx_kernel_stats(prism_ctx* ctx, const char* name, uint64_t* launches, double* total_ms);
 const char* prism_version(void);
 
 /* ------------------------------------------------------------------------ */

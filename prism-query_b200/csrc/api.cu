@@ -1,0 +1,746 @@
+// api.cpp — the extern "C" entry points of include/prism_gpu.h.
+//
+// Every entry point catches failures and returns a status code (the library
+// never aborts); the message is kept on the context for prism_last_error().
+#include <cstring>
+#include <functional>
+
+#include "agg.hpp"
+#include "arrow_io.hpp"
+#include "filter_project.hpp"
+#include "join.hpp"
+#include "prims.hpp"
+
+using namespace prism;
+
+struct prism_hash_table {
+  prism_ctx* ctx = nullptr;
+  std::unique_ptr<JoinTable> t;
+};
+
+namespace {
+
+thread_local std::string t_err;  // errors before a context exists
+
+int run(prism_ctx* ctx, const std::function<void()>& fn) {
+  if (!ctx) return PRISM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->impl.mu);
+  try {
+    fn();
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    ctx->impl.last_error = f.msg;
+    cudaGetLastError();
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    ctx->impl.last_error = "host allocation failed";
+    return PRISM_ERR_NO_MEMORY;
+  } catch (const std::exception& e) {
+    ctx->impl.last_error = e.what();
+    return PRISM_ERR_INTERNAL;
+  }
+}
+
+prism_batch* wrap(prism_ctx* ctx, Batch b) {
+  auto* out = new prism_batch();
+  out->impl = std::move(b);
+  out->ctx = ctx;
+  return out;
+}
+
+const Batch& B(const prism_batch* b) {
+  if (!b) fail(PRISM_ERR_INVALID_ARGUMENT, "null batch");
+  return b->impl;
+}
+
+std::vector<int> ints(const int32_t* p, int n) {
+  if (n > 0 && !p) fail(PRISM_ERR_INVALID_ARGUMENT, "null column list");
+  return std::vector<int>(p, p + std::max(0, n));
+}
+
+JoinTuning join_tuning() { return JoinTuning{}; }
+AggTuning agg_tuning() { return AggTuning{}; }
+
+std::string right_name(const Batch& probe, const std::string& nm) {
+  for (auto& c : probe.cols)
+    if (c->name == nm) return nm + "_right";
+  return nm;
+}
+
+__global__ void fill_u32_kernel(uint32_t* p, int64_t n, uint32_t v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+// bits [0, n_valid) set, [n_valid, n) clear, whole words
+__global__ void prefix_bits_kernel(uint32_t* w, int64_t n, int64_t n_valid) {
+  int64_t nw = (n + 31) / 32;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nw; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = i * 32;
+    uint32_t v;
+    if (lo + 32 <= n_valid) v = 0xffffffffu;
+    else if (lo >= n_valid) v = 0u;
+    else v = (1u << (n_valid - lo)) - 1u;
+    w[i] = v;
+  }
+}
+// bits [0, n_null) clear, [n_null, n) set
+__global__ void suffix_bits_kernel(uint32_t* w, int64_t n, int64_t n_null) {
+  int64_t nw = (n + 31) / 32;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nw; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = i * 32;
+    uint32_t v;
+    if (lo + 32 <= n_null) v = 0u;
+    else if (lo >= n_null) v = 0xffffffffu;
+    else v = ~((1u << (n_null - lo)) - 1u);
+    w[i] = v;
+  }
+}
+
+struct IndexVec {
+  MemP mem;
+  uint32_t* ptr = nullptr;
+  MemP vmem;
+  uint8_t* valid = nullptr;  // null: all valid
+  int64_t n = 0;
+};
+
+// concatenates index pieces: (ptr, n) or a constant fill (ptr null)
+IndexVec concat_idx(Ctx& ctx, const std::vector<std::pair<const uint32_t*, int64_t>>& parts, uint32_t fill) {
+  IndexVec v;
+  for (auto& p : parts) v.n += p.second;
+  v.ptr = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(v.n, 1), v.mem);
+  int64_t off = 0;
+  for (auto& p : parts) {
+    if (p.second == 0) continue;
+    if (p.first) PRISM_CUDA(cudaMemcpyAsync(v.ptr + off, p.first, p.second * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+    else {
+      fill_u32_kernel<<<grid_for(ctx, p.second, 256), 256, 0, ctx.stream>>>(v.ptr + off, p.second, fill);
+      ctx.check_launch("fill_u32_kernel");
+    }
+    off += p.second;
+  }
+  return v;
+}
+
+Batch assemble(Ctx& ctx, const Batch& probe, const IndexVec& pi, const Batch& build, const IndexVec& bi, int mode) {
+  Batch out;
+  out.rows = pi.n;
+  for (auto& c : probe.cols)
+    out.cols.push_back(take(ctx, *c, pi.ptr, pi.valid, pi.n, c->name, mode == 0 ? c->nullable : true));
+  for (auto& c : build.cols) {
+    std::string nm = right_name(probe, c->name);
+    bool nullable = c->nullable;
+    if (mode == 2 && nm != c->name) nullable = true;
+    out.cols.push_back(take(ctx, *c, bi.ptr, bi.valid, bi.n, nm, nullable));
+  }
+  return out;
+}
+
+IndexVec as_vec(const MemP& m, int64_t n) {
+  IndexVec v;
+  v.mem = m;
+  v.ptr = m ? static_cast<uint32_t*>(m->ptr) : nullptr;
+  v.n = n;
+  return v;
+}
+
+MemP matched_bits(Ctx& ctx, const uint32_t* idx, int64_t n_idx, int64_t n_rows) {
+  MemP m = ctx.alloc((size_t)(n_rows + 31) / 32 * 4 + 8);
+  PRISM_CUDA(cudaMemsetAsync(m->ptr, 0, (size_t)(n_rows + 31) / 32 * 4 + 8, ctx.stream));
+  scatter_bits(ctx, idx, n_idx, static_cast<uint8_t*>(m->ptr));
+  return m;
+}
+
+// hash_join / per-batch assembly of hash_join_probe_chunked
+// (native/prism-executor/src/hash_join.rs:206-282, 312-365)
+Batch join_one(Ctx& ctx, const Batch& probe, const Batch& build, const JoinTable& t, const std::vector<int>& pk,
+               int join_type, bool chunked) {
+  std::vector<ProbeGather> none;
+  ProbeResult pr = probe_join_table(ctx, t, probe, pk, true, true, none, -1, join_tuning());
+  int64_t n = pr.matches;
+  IndexVec pi = as_vec(pr.probe_idx, n), bi = as_vec(pr.build_idx, n);
+  switch (join_type) {
+    case PRISM_JOIN_INNER:
+      return assemble(ctx, probe, pi, build, bi, 0);
+    case PRISM_JOIN_LEFT: {
+      // left_join_indices (hash_join.rs:455-483): unmatched probe rows pair
+      // with build index 0, i.e. they carry build row 0's values
+      MemP mb = matched_bits(ctx, pi.ptr, n, probe.rows);
+      int64_t nu = 0;
+      MemP un = compact_bits(ctx, static_cast<uint8_t*>(mb->ptr), probe.rows, true, &nu);
+      if (nu > 0 && build.rows == 0)
+        fail(PRISM_ERR_JOIN, "left join of unmatched probe rows against an empty build side "
+                             "(the reference indexes build row 0)");
+      IndexVec p2 = concat_idx(ctx, {{pi.ptr, n}, {static_cast<uint32_t*>(un->ptr), nu}}, 0);
+      IndexVec b2 = concat_idx(ctx, {{bi.ptr, n}, {nullptr, nu}}, 0);
+      return assemble(ctx, probe, p2, build, b2, 0);
+    }
+    case PRISM_JOIN_LEFT_SEMI: case PRISM_JOIN_LEFT_ANTI: {
+      MemP mb = matched_bits(ctx, pi.ptr, n, probe.rows);
+      int64_t nk = 0;
+      MemP rows = compact_bits(ctx, static_cast<uint8_t*>(mb->ptr), probe.rows, join_type == PRISM_JOIN_LEFT_ANTI, &nk);
+      Batch out = filter_rows(ctx, probe, static_cast<uint32_t*>(rows->ptr), nk);
+      return out;
+    }
+    case PRISM_JOIN_RIGHT: case PRISM_JOIN_FULL: {
+      if (chunked) return assemble(ctx, probe, pi, build, bi, 0);  // hash_join.rs:261-270
+      MemP bm = matched_bits(ctx, bi.ptr, n, build.rows);
+      int64_t nub = 0;
+      MemP unb = compact_bits(ctx, static_cast<uint8_t*>(bm->ptr), build.rows, true, &nub);
+      int64_t nup = 0;
+      MemP unp;
+      if (join_type == PRISM_JOIN_FULL) {
+        MemP pm = matched_bits(ctx, pi.ptr, n, probe.rows);
+        unp = compact_bits(ctx, static_cast<uint8_t*>(pm->ptr), probe.rows, true, &nup);
+        // non-nullable, non-renamed build fields would receive nulls: arrow-rs
+        // RecordBatch::try_new rejects that batch in the reference
+        if (nup > 0)
+          for (auto& c : build.cols)
+            if (!c->nullable && right_name(probe, c->name) == c->name)
+              fail(PRISM_ERR_ARROW, "Invalid argument error: Column '" + c->name +
+                                        "' is declared as non-nullable but contains null values");
+      }
+      // probe indices: matched, unmatched probe (FULL), null for unmatched build
+      IndexVec p2 = concat_idx(ctx, {{pi.ptr, n}, {unp ? static_cast<uint32_t*>(unp->ptr) : nullptr, nup}, {nullptr, nub}}, 0);
+      p2.vmem = ctx.alloc((size_t)(p2.n + 31) / 32 * 4 + 8);
+      p2.valid = static_cast<uint8_t*>(p2.vmem->ptr);
+      prefix_bits_kernel<<<grid_for(ctx, (p2.n + 31) / 32 + 1, 256), 256, 0, ctx.stream>>>(
+          reinterpret_cast<uint32_t*>(p2.valid), p2.n, n + nup);
+      ctx.check_launch("prefix_bits_kernel");
+      IndexVec b2 = concat_idx(ctx, {{bi.ptr, n}, {nullptr, nup}, {static_cast<uint32_t*>(unb->ptr), nub}}, 0);
+      if (join_type == PRISM_JOIN_FULL && nup > 0) {
+        // build indices null for the unmatched probe rows [n, n + nup)
+        b2.vmem = ctx.alloc((size_t)(b2.n + 31) / 32 * 4 + 8);
+        b2.valid = static_cast<uint8_t*>(b2.vmem->ptr);
+        // set all, then clear [n, n+nup): compose prefix [0,n) with suffix [n+nup, end)
+        MemP tmp1 = ctx.alloc((size_t)(b2.n + 31) / 32 * 4 + 8), tmp2 = ctx.alloc((size_t)(b2.n + 31) / 32 * 4 + 8);
+        int g = grid_for(ctx, (b2.n + 31) / 32 + 1, 256);
+        prefix_bits_kernel<<<g, 256, 0, ctx.stream>>>(static_cast<uint32_t*>(tmp1->ptr), b2.n, n);
+        suffix_bits_kernel<<<g, 256, 0, ctx.stream>>>(static_cast<uint32_t*>(tmp2->ptr), b2.n, n + nup);
+        ctx.check_launch("bits_kernel");
+        // or the two masks
+        std::vector<uint32_t> h1((size_t)(b2.n + 31) / 32), h2(h1.size());
+        PRISM_CUDA(cudaMemcpyAsync(h1.data(), tmp1->ptr, h1.size() * 4, cudaMemcpyDeviceToHost, ctx.stream));
+        PRISM_CUDA(cudaMemcpyAsync(h2.data(), tmp2->ptr, h2.size() * 4, cudaMemcpyDeviceToHost, ctx.stream));
+        PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (size_t i = 0; i < h1.size(); ++i) h1[i] |= h2[i];
+        PRISM_CUDA(cudaMemcpyAsync(b2.valid, h1.data(), h1.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+        PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+      }
+      return assemble(ctx, probe, p2, build, b2, join_type == PRISM_JOIN_FULL ? 2 : 1);
+    }
+  }
+  fail(PRISM_ERR_INVALID_ARGUMENT, "unknown join type");
+}
+
+std::string joined_name(const Batch& probe, const Batch& build, int col) {
+  int np = (int)probe.cols.size();
+  if (col < np) return probe.cols[col]->name;
+  return right_name(probe, build.cols[col - np]->name);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* prism_version(void) { return "prism-gpu 0.1 (sm_100a)"; }
+
+int prism_ctx_create(int device, uint64_t budget, prism_ctx** out) {
+  if (!out) return PRISM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  auto* c = new prism_ctx();
+  Ctx& x = c->impl;
+  try {
+    PRISM_CUDA(cudaSetDevice(device));
+    x.device = device;
+    PRISM_CUDA(cudaStreamCreateWithFlags(&x.own_stream, cudaStreamNonBlocking));
+    x.stream = x.own_stream;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    PRISM_CUDA(cudaMemPoolCreate(&x.pool, &props));
+    uint64_t thr = UINT64_MAX;
+    PRISM_CUDA(cudaMemPoolSetAttribute(x.pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    size_t free_b = 0, total_b = 0;
+    PRISM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    x.budget = budget ? budget : (uint64_t)(free_b * 0.9);
+    PRISM_CUDA(cudaDeviceGetAttribute(&x.sm_count, cudaDevAttrMultiProcessorCount, device));
+    PRISM_CUDA(cudaMalloc(&x.d_err, 64));
+    PRISM_CUDA(cudaMemset(x.d_err, 0, 64));
+    PRISM_CUDA(cudaMallocHost(&x.h_err, 64));
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    if (x.pool) cudaMemPoolDestroy(x.pool);
+    if (x.own_stream) cudaStreamDestroy(x.own_stream);
+    delete c;
+    cudaGetLastError();
+    return f.code;
+  }
+  *out = c;
+  return PRISM_OK;
+}
+
+void prism_ctx_destroy(prism_ctx* c) {
+  if (!c) return;
+  Ctx& x = c->impl;
+  cudaStreamSynchronize(x.stream);
+  x.clear_timings();
+  for (auto e : x.event_pool) cudaEventDestroy(e);
+  if (x.d_err) cudaFree(x.d_err);
+  if (x.h_err) cudaFreeHost(x.h_err);
+  if (x.pool) cudaMemPoolDestroy(x.pool);
+  if (x.own_stream) cudaStreamDestroy(x.own_stream);
+  delete c;
+}
+
+const char* prism_last_error(const prism_ctx* c) { return c ? c->impl.last_error.c_str() : t_err.c_str(); }
+
+int prism_ctx_set_stream(prism_ctx* c, void* s) {
+  return run(c, [&] {
+    PRISM_CUDA(cudaStreamSynchronize(c->impl.stream));
+    c->impl.stream = s ? static_cast<cudaStream_t>(s) : c->impl.own_stream;
+  });
+}
+
+int prism_ctx_synchronize(prism_ctx* c) { return run(c, [&] { c->impl.sync(); }); }
+uint64_t prism_ctx_bytes_in_use(const prism_ctx* c) { return c ? c->impl.in_use.load() : 0; }
+
+int prism_ctx_set_profiling(prism_ctx* c, int enable) {
+  return run(c, [&] {
+    c->impl.sync();
+    c->impl.clear_timings();
+    c->impl.profiling = enable != 0;
+  });
+}
+
+int prism_ctx_kernel_stats(prism_ctx* c, const char* name, uint64_t* launches, double* total_ms) {
+  return run(c, [&] {
+    if (!name || !launches || !total_ms) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    c->impl.sync();
+    *launches = 0;
+    *total_ms = 0;
+    auto it = c->impl.timings.find(name);
+    if (it == c->impl.timings.end()) return;
+    for (auto& pr : it->second) {
+      float ms = 0;
+      PRISM_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      *total_ms += ms;
+      *launches += 1;
+    }
+  });
+}
+uint64_t prism_ctx_kernel_launches(const prism_ctx* c) { return c ? c->impl.launches.load() : 0; }
+
+// ------------------------------------------------------------- batches ---
+int prism_batch_import(prism_ctx* c, const ArrowArray* a, const ArrowSchema* s, prism_batch** out) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    *out = wrap(c, import_batch(c->impl, a, s, false));
+  });
+}
+
+int prism_batch_import_device(prism_ctx* c, const ArrowDeviceArray* a, const ArrowSchema* s, prism_batch** out) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    *out = wrap(c, import_device_batch(c->impl, a, s));
+  });
+}
+
+int prism_batch_export(prism_ctx* c, const prism_batch* b, ArrowArray* a, ArrowSchema* s) {
+  return run(c, [&] { export_batch(c->impl, B(b), a, s); });
+}
+
+int64_t prism_batch_num_rows(const prism_batch* b) { return b ? b->impl.rows : -1; }
+int32_t prism_batch_num_columns(const prism_batch* b) { return b ? (int32_t)b->impl.cols.size() : -1; }
+void prism_batch_free(prism_batch* b) {
+  if (!b) return;
+  if (b->ctx) {
+    std::lock_guard<std::recursive_mutex> lk(b->ctx->impl.mu);
+    delete b;
+  } else {
+    delete b;
+  }
+}
+
+// ---------------------------------------------------------------- join ---
+int prism_hash_table_build(prism_ctx* c, const prism_batch* build, const int32_t* keys, int32_t n, prism_hash_table** out) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    auto* h = new prism_hash_table();
+    h->ctx = c;
+    try {
+      h->t = build_join_table(c->impl, B(build), ints(keys, n), join_tuning());
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int prism_hash_table_probe(prism_ctx* c, const prism_hash_table* t, const prism_batch* probe, const int32_t* keys,
+                           int32_t n, prism_batch** out) {
+  return run(c, [&] {
+    if (!t || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
+    std::vector<ProbeGather> none;
+    ProbeResult r = probe_join_table(c->impl, *t->t, B(probe), ints(keys, n), true, true, none, -1, join_tuning());
+    Batch b;
+    b.rows = r.matches;
+    b.cols.push_back(u32_column(c->impl, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
+    b.cols.push_back(u32_column(c->impl, "build_idx", r.build_idx, static_cast<uint32_t*>(r.build_idx->ptr), r.matches));
+    *out = wrap(c, std::move(b));
+  });
+}
+
+int64_t prism_hash_table_num_rows(const prism_hash_table* t) { return t ? t->t->build.rows : -1; }
+int prism_hash_table_has_duplicates(const prism_hash_table* t) { return t && t->t->has_dups ? 1 : 0; }
+void prism_hash_table_free(prism_hash_table* t) {
+  if (!t) return;
+  if (t->ctx) {
+    std::lock_guard<std::recursive_mutex> lk(t->ctx->impl.mu);
+    delete t;
+  } else {
+    delete t;
+  }
+}
+
+int prism_join_project(prism_ctx* c, const prism_hash_table* tab, const prism_batch* probe_b, const int32_t* probe_keys,
+                       int32_t n_keys, const int32_t* out_cols, int32_t n_out, prism_batch** out) {
+  return run(c, [&] {
+    if (!tab || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
+    Ctx& x = c->impl;
+    const JoinTable& t = *tab->t;
+    const Batch& probe = B(probe_b);
+    const Batch& build = t.build;
+    std::vector<int> pk = ints(probe_keys, n_keys), oc = ints(out_cols, n_out);
+    int np = (int)probe.cols.size(), nb = (int)build.cols.size();
+    for (int col : oc)
+      if (col < PRISM_COL_BUILD_ROW_INDEX || col >= np + nb) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+    // gather fixed-width null-free columns inside the probe kernel
+    bool fusable = (int)oc.size() <= 6;
+    int n_gather = 0;
+    for (int col : oc) {
+      if (col < 0) continue;
+      const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+      int w = width_of(src.type);
+      if (src.validity || (w != 4 && w != 8) || src.type == TY_DICT) fusable = false;
+      ++n_gather;
+    }
+    if (n_gather > 4) fusable = false;
+    int64_t cap = match_upper_bound(t, probe.rows);
+    if (cap < 0) cap = probe_count(x, t, probe, pk, join_tuning());
+    bool want_p = !fusable, want_b = !fusable;
+    for (int col : oc) {
+      if (col == PRISM_COL_PROBE_ROW_INDEX) want_p = true;
+      if (col == PRISM_COL_BUILD_ROW_INDEX) want_b = true;
+    }
+    std::vector<ProbeGather> gathers;
+    std::vector<ColP> gcols;
+    if (fusable) {
+      for (int col : oc) {
+        if (col < 0) continue;
+        const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+        ColP dst = make_column(x, src.type, joined_name(probe, build, col), cap, false);
+        dst->nullable = src.nullable;
+        dst->precision = src.precision;
+        dst->scale = src.scale;
+        gathers.push_back({col < np ? 0 : 1, src.values, width_of(src.type), dst->values});
+        gcols.push_back(dst);
+      }
+    }
+    ProbeResult r = probe_join_table(x, t, probe, pk, want_p, want_b, gathers, cap, join_tuning());
+    Batch res;
+    res.rows = r.matches;
+    size_t gi = 0;
+    for (int col : oc) {
+      if (col == PRISM_COL_PROBE_ROW_INDEX) {
+        res.cols.push_back(u32_column(x, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
+      } else if (col == PRISM_COL_BUILD_ROW_INDEX) {
+        res.cols.push_back(u32_column(x, "build_idx", r.build_idx, static_cast<uint32_t*>(r.build_idx->ptr), r.matches));
+      } else if (fusable) {
+        ColP g = gcols[gi++];
+        g->length = r.matches;
+        res.cols.push_back(g);
+      } else {
+        const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+        const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
+        res.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(probe, build, col), src.nullable));
+      }
+    }
+    x.sync();
+    *out = wrap(c, std::move(res));
+  });
+}
+
+int prism_hash_join(prism_ctx* c, const prism_batch* probe, const prism_batch* build, const prism_join_config* cfg,
+                    prism_batch** out) {
+  return run(c, [&] {
+    if (!cfg || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/output");
+    std::vector<int> pk = ints(cfg->probe_keys, cfg->n_keys), bk = ints(cfg->build_keys, cfg->n_keys);
+    check_join_keys(B(probe), pk, B(build), bk);
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    Batch r = join_one(c->impl, B(probe), B(build), *t, pk, cfg->join_type, false);
+    c->impl.sync();
+    *out = wrap(c, std::move(r));
+  });
+}
+
+int prism_probe_matches_chunked(prism_ctx* c, const prism_batch* const* probes, int32_t n_probes, const prism_batch* build,
+                                const int32_t* probe_keys, const int32_t* build_keys, int32_t n_keys, prism_batch** out) {
+  return run(c, [&] {
+    if (!out || (n_probes > 0 && !probes)) fail(PRISM_ERR_INVALID_ARGUMENT, "null probes/output");
+    std::vector<int> pk = ints(probe_keys, n_keys), bk = ints(build_keys, n_keys);
+    for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, B(build), bk);
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    std::vector<prism_batch*> res;
+    try {
+      for (int i = 0; i < n_probes; ++i) {
+        std::vector<ProbeGather> none;
+        ProbeResult r = probe_join_table(c->impl, *t, B(probes[i]), pk, true, true, none, -1, join_tuning());
+        Batch b;
+        b.rows = r.matches;
+        b.cols.push_back(u32_column(c->impl, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
+        b.cols.push_back(u32_column(c->impl, "build_idx", r.build_idx, static_cast<uint32_t*>(r.build_idx->ptr), r.matches));
+        res.push_back(wrap(c, std::move(b)));
+      }
+    } catch (...) {
+      for (auto* r : res) delete r;
+      throw;
+    }
+    for (int i = 0; i < n_probes; ++i) out[i] = res[i];
+  });
+}
+
+int prism_hash_join_probe_chunked(prism_ctx* c, const prism_batch* const* probes, int32_t n_probes,
+                                  const prism_batch* build, const prism_join_config* cfg, prism_batch** out,
+                                  int32_t* n_out) {
+  return run(c, [&] {
+    if (!cfg || !out || !n_out) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/output");
+    std::vector<int> pk = ints(cfg->probe_keys, cfg->n_keys), bk = ints(cfg->build_keys, cfg->n_keys);
+    for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, B(build), bk);
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    std::vector<prism_batch*> res;
+    try {
+      for (int i = 0; i < n_probes; ++i) {
+        Batch r = join_one(c->impl, B(probes[i]), B(build), *t, pk, cfg->join_type, true);
+        if (r.rows > 0) res.push_back(wrap(c, std::move(r)));
+      }
+      c->impl.sync();
+    } catch (...) {
+      for (auto* r : res) delete r;
+      throw;
+    }
+    for (size_t i = 0; i < res.size(); ++i) out[i] = res[i];
+    *n_out = (int32_t)res.size();
+  });
+}
+
+// ----------------------------------------------------------- aggregate ---
+int prism_hash_aggregate_batches(prism_ctx* c, const prism_batch* const* batches, int32_t n, const prism_agg_config* cfg,
+                                 prism_batch** out) {
+  return run(c, [&] {
+    if (!cfg || !out || (n > 0 && !batches)) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/batches/output");
+    std::vector<const Batch*> bs;
+    for (int i = 0; i < n; ++i) bs.push_back(&B(batches[i]));
+    *out = wrap(c, aggregate(c->impl, bs, *cfg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, agg_tuning()));
+  });
+}
+
+int prism_hash_aggregate(prism_ctx* c, const prism_batch* batch, const prism_agg_config* cfg, prism_batch** out) {
+  const prism_batch* one[1] = {batch};
+  return prism_hash_aggregate_batches(c, one, 1, cfg, out);
+}
+
+// -------------------------------------------------------- filter/project -
+int prism_evaluate_predicate(prism_ctx* c, const prism_batch* b, const prism_predicate* p, prism_batch** out) {
+  return run(c, [&] {
+    if (!p || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null predicate/output");
+    Batch r;
+    r.rows = B(b).rows;
+    r.cols.push_back(evaluate_predicate(c->impl, B(b), *p));
+    *out = wrap(c, std::move(r));
+  });
+}
+
+int prism_filter_batch(prism_ctx* c, const prism_batch* b, const prism_batch* mask, prism_batch** out) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    const Batch& m = B(mask);
+    if (m.cols.size() != 1) fail(PRISM_ERR_INVALID_ARGUMENT, "mask must be a one-column Boolean batch");
+    *out = wrap(c, filter_by_mask(c->impl, B(b), *m.cols[0]));
+  });
+}
+
+int prism_project_batch(prism_ctx* c, const prism_batch* b, const int32_t* cols, int32_t n, prism_batch** out) {
+  return run(c, [&] {
+    if (!out || (n > 0 && !cols)) fail(PRISM_ERR_INVALID_ARGUMENT, "null columns/output");
+    *out = wrap(c, project(B(b), cols, n));
+  });
+}
+
+int prism_filter_and_project(prism_ctx* c, const prism_batch* b, const prism_predicate* p, const int32_t* cols, int32_t n,
+                             prism_batch** out) {
+  return run(c, [&] {
+    if (!out || (n > 0 && !cols)) fail(PRISM_ERR_INVALID_ARGUMENT, "null columns/output");
+    Batch f = B(b);
+    if (p) {
+      ColP m = evaluate_predicate(c->impl, f, *p);
+      f = filter_by_mask(c->impl, f, *m);
+    }
+    *out = wrap(c, n == 0 ? f : project(f, cols, n));
+  });
+}
+
+int prism_evaluate_scalar_expr(prism_ctx* c, const prism_batch* b, const prism_expr* e, int32_t mode, prism_batch** out) {
+  return run(c, [&] {
+    if (!e || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null expression/output");
+    Batch r = project_with_exprs(c->impl, B(b), nullptr, 0, e, 1, mode);
+    *out = wrap(c, std::move(r));
+  });
+}
+
+int prism_project_batch_with_exprs(prism_ctx* c, const prism_batch* b, const int32_t* cols, int32_t n,
+                                   const prism_expr* exprs, int32_t n_exprs, int32_t mode, prism_batch** out) {
+  return run(c, [&] {
+    if (!out || (n > 0 && !cols) || (n_exprs > 0 && !exprs)) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    *out = wrap(c, project_with_exprs(c->impl, B(b), cols, n, exprs, n_exprs, mode));
+  });
+}
+
+// --------------------------------------------------------------- fused ---
+int prism_filter_project_aggregate(prism_ctx* c, const prism_batch* const* batches, int32_t n, const prism_predicate* p,
+                                   const int32_t* cols, int32_t n_cols, const prism_expr* exprs, int32_t n_exprs,
+                                   int32_t mode, const prism_agg_config* agg, prism_batch** out) {
+  return run(c, [&] {
+    if (!agg || !out || (n > 0 && !batches)) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    std::vector<const Batch*> bs;
+    for (int i = 0; i < n; ++i) bs.push_back(&B(batches[i]));
+    try {
+      *out = wrap(c, aggregate(c->impl, bs, *agg, p, cols, n_cols, exprs, n_exprs, mode, true, agg_tuning()));
+      return;
+    } catch (const Failure& f) {
+      if (f.code != PRISM_ERR_INVALID_ARGUMENT || f.msg.find("fused path") == std::string::npos) throw;
+    }
+    // shapes the one-pass kernel does not take: filter, project, then aggregate
+    std::vector<Batch> mats;
+    for (auto* b : bs) {
+      Batch f = *b;
+      if (p) {
+        ColP m = evaluate_predicate(c->impl, f, *p);
+        f = filter_by_mask(c->impl, f, *m);
+      }
+      mats.push_back(project_with_exprs(c->impl, f, cols, n_cols, exprs, n_exprs, mode));
+    }
+    std::vector<const Batch*> ms;
+    for (auto& m : mats) ms.push_back(&m);
+    *out = wrap(c, aggregate(c->impl, ms, *agg, nullptr, nullptr, 0, nullptr, 0, mode, false, agg_tuning()));
+  });
+}
+
+int prism_join_aggregate(prism_ctx* c, const prism_batch* const* probes, int32_t n_probes, const prism_batch* build,
+                         const int32_t* probe_keys, const int32_t* build_keys, int32_t n_keys, const int32_t* cols,
+                         int32_t n_cols, const prism_expr* exprs, int32_t n_exprs, const prism_agg_config* agg,
+                         prism_batch** out) {
+  return run(c, [&] {
+    if (!agg || !out || n_probes <= 0 || !probes) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    Ctx& x = c->impl;
+    std::vector<int> pk = ints(probe_keys, n_keys), bk = ints(build_keys, n_keys);
+    const Batch& bb = B(build);
+    for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, bb, bk);
+    auto t = build_join_table(x, bb, bk, join_tuning());
+    // joined columns referenced by the projection (executor.rs:474-551)
+    const Batch& p0 = B(probes[0]);
+    int np = (int)p0.cols.size(), total = np + (int)bb.cols.size();
+    std::vector<bool> need(total, false);
+    for (int i = 0; i < n_cols; ++i) {
+      if (cols[i] < 0 || cols[i] >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+      need[cols[i]] = true;
+    }
+    for (int e = 0; e < n_exprs; ++e) {
+      for (int k = 0; k < exprs[e].n_nodes; ++k)
+        if (exprs[e].nodes[k].op == PRISM_EXPR_COLUMN) {
+          int col = exprs[e].nodes[k].column;
+          if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+          need[col] = true;
+        }
+      for (int k = 0; k < exprs[e].n_preds; ++k) {
+        int op = exprs[e].preds[k].op;
+        if (op != PRISM_PRED_LITERAL && op != PRISM_PRED_AND && op != PRISM_PRED_OR && op != PRISM_PRED_NOT) {
+          int col = exprs[e].preds[k].column;
+          if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+          need[col] = true;
+        }
+      }
+    }
+    std::vector<Batch> projected;
+    for (int i = 0; i < n_probes; ++i) {
+      const Batch& pb = B(probes[i]);
+      std::vector<ProbeGather> none;
+      ProbeResult r = probe_join_table(x, *t, pb, pk, true, true, none, -1, join_tuning());
+      if (r.matches == 0 && !projected.empty()) continue;
+      Batch joined;
+      joined.rows = r.matches;
+      for (int col = 0; col < total; ++col) {
+        if (!need[col]) {
+          auto z = std::make_shared<Column>();
+          z->type = TY_NULL;
+          z->length = r.matches;
+          joined.cols.push_back(z);
+          continue;
+        }
+        const Column& src = col < np ? *pb.cols[col] : *bb.cols[col - np];
+        const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
+        joined.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(pb, bb, col), src.nullable));
+      }
+      projected.push_back(project_with_exprs(x, joined, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64));
+    }
+    std::vector<const Batch*> ps;
+    for (auto& p : projected)
+      if (p.rows > 0 || projected.size() == 1) ps.push_back(&p);
+    *out = wrap(c, aggregate(x, ps, *agg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, agg_tuning()));
+  });
+}
+
+// ------------------------------------------------------- arrow wrappers --
+int prism_hash_join_arrow(prism_ctx* c, const ArrowArray* probe, const ArrowSchema* ps, const ArrowArray* build,
+                          const ArrowSchema* bs, const prism_join_config* cfg, ArrowArray* out, ArrowSchema* os) {
+  return run(c, [&] {
+    Batch p = import_batch(c->impl, probe, ps, false), b = import_batch(c->impl, build, bs, false);
+    prism_batch pw, bw;
+    pw.impl = p;
+    bw.impl = b;
+    prism_batch* r = nullptr;
+    int rc = prism_hash_join(c, &pw, &bw, cfg, &r);
+    if (rc) fail(rc, c->impl.last_error);
+    std::unique_ptr<prism_batch> hold(r);
+    export_batch(c->impl, r->impl, out, os);
+  });
+}
+
+int prism_hash_aggregate_arrow(prism_ctx* c, const ArrowArray* batch, const ArrowSchema* s, const prism_agg_config* cfg,
+                               ArrowArray* out, ArrowSchema* os) {
+  return run(c, [&] {
+    prism_batch bw;
+    bw.impl = import_batch(c->impl, batch, s, false);
+    prism_batch* r = nullptr;
+    int rc = prism_hash_aggregate(c, &bw, cfg, &r);
+    if (rc) fail(rc, c->impl.last_error);
+    std::unique_ptr<prism_batch> hold(r);
+    export_batch(c->impl, r->impl, out, os);
+  });
+}
+
+int prism_filter_and_project_arrow(prism_ctx* c, const ArrowArray* batch, const ArrowSchema* s, const prism_predicate* p,
+                                   const int32_t* cols, int32_t n, ArrowArray* out, ArrowSchema* os) {
+  return run(c, [&] {
+    prism_batch bw;
+    bw.impl = import_batch(c->impl, batch, s, false);
+    prism_batch* r = nullptr;
+    int rc = prism_filter_and_project(c, &bw, p, cols, n, &r);
+    if (rc) fail(rc, c->impl.last_error);
+    std::unique_ptr<prism_batch> hold(r);
+    export_batch(c->impl, r->impl, out, os);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,611 @@
+// join.cu — open-addressing device hash table, build and ordered probe.
+//
+// Replaces HashTable::build / HashTable::probe
+// (native/prism-executor/src/hash_join.rs:87-200). The reference partitions
+// `(hash, row)` pairs 64 ways and builds one hashbrown map of row lists per
+// partition; here one linear-probing table in HBM holds 16-byte slots
+// {key, cnt << 32 | row} inserted with 64-bit atomicCAS, and rows of keys
+// that occur more than once live in contiguous ascending segments.
+//
+// The probe is one pass over the probe keys: each CTA takes a tile of 2048
+// rows, resolves its slots (8 independent 16-byte loads in flight per lane),
+// ranks the matches with warp scans, obtains the tile's output offset by
+// decoupled look-back over the preceding tiles, and writes matches in the
+// reference's order (probe row ascending, build rows ascending) — no second
+// read of the probe side and no post-sort.
+#include "join.hpp"
+#include "prims.hpp"
+
+namespace prism {
+
+namespace {
+
+constexpr uint64_t EMPTY = 0x8000000000000000ULL;
+constexpr uint64_t Y_INIT = 0x00000000FFFFFFFFULL;  // cnt 0, row = max
+constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
+
+constexpr int PW = 8;              // warps per probe CTA
+constexpr int PI = 8;              // rows per lane
+constexpr int PT = PW * 32 * PI;   // rows per tile (2048)
+
+__device__ __forceinline__ uint64_t slot_of(uint64_t k, int shift) { return (k * FIB) >> shift; }
+
+// General-path row hash over the key columns; equal keys hash equal across
+// the two sides (types are checked on the host). Null rows contribute a
+// marker word only, as the reference hashes 0u8 for them (hash_join.rs:394-398).
+__device__ __forceinline__ uint64_t general_hash(const DCol* cols, int n, int64_t row) {
+  uint64_t h = 0x2545F4914F6CDD1DULL;
+  for (int i = 0; i < n; ++i) {
+    const DCol& c = cols[i];
+    uint64_t w;
+    if (!dcol_valid(c, row)) w = 0x6a09e667f3bcc909ULL;
+    else if (c.type == TY_UTF8 || c.type == TY_DICT) {
+      const uint8_t* p;
+      int32_t len;
+      dcol_str(c, row, p, len);
+      w = fx_str(0, p, len);
+    } else if (c.type == TY_F64) w = (uint64_t)__double_as_longlong(static_cast<const double*>(c.values)[row]);
+    else if (c.type == TY_F32) w = (uint64_t)__float_as_uint(static_cast<const float*>(c.values)[row]);
+    else if (c.type == TY_DEC128) {
+      const uint64_t* p = static_cast<const uint64_t*>(c.values) + 2 * row;
+      w = p[0] ^ mix64(p[1]);
+    } else w = (uint64_t)dcol_ival(c, row);
+    h = mix64(h ^ w) + FIB;
+  }
+  return h;
+}
+
+__device__ __forceinline__ bool bytes_equal(const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb) {
+  if (na != nb) return false;
+  for (int32_t i = 0; i < na; ++i)
+    if (a[i] != b[i]) return false;
+  return true;
+}
+
+// keys_equal (hash_join.rs:628-670) plus the hash precondition: null flags
+// must agree and raw values must be equal; Float64 needs equal bits and `==`.
+__device__ __forceinline__ bool rows_equal(const DCol* pc, const DCol* bc, int n, int64_t pr, int64_t br) {
+  for (int i = 0; i < n; ++i) {
+    const DCol& a = pc[i];
+    const DCol& b = bc[i];
+    if (dcol_valid(a, pr) != dcol_valid(b, br)) return false;
+    switch (a.type) {
+      case TY_UTF8: case TY_DICT: {
+        const uint8_t *x, *y;
+        int32_t nx, ny;
+        dcol_str(a, pr, x, nx);
+        dcol_str(b, br, y, ny);
+        if (!bytes_equal(x, nx, y, ny)) return false;
+        break;
+      }
+      case TY_F64: {
+        double x = static_cast<const double*>(a.values)[pr], y = static_cast<const double*>(b.values)[br];
+        if (!(x == y) || __double_as_longlong(x) != __double_as_longlong(y)) return false;
+        break;
+      }
+      case TY_F32: {
+        float x = static_cast<const float*>(a.values)[pr], y = static_cast<const float*>(b.values)[br];
+        if (!(x == y) || __float_as_uint(x) != __float_as_uint(y)) return false;
+        break;
+      }
+      case TY_DEC128: {
+        const uint64_t* x = static_cast<const uint64_t*>(a.values) + 2 * pr;
+        const uint64_t* y = static_cast<const uint64_t*>(b.values) + 2 * br;
+        if (x[0] != y[0] || x[1] != y[1]) return false;
+        break;
+      }
+      case TY_NULL: break;
+      default:
+        if (dcol_ival(a, pr) != dcol_ival(b, br)) return false;
+    }
+  }
+  return true;
+}
+
+struct KeysFast {
+  static constexpr bool kFast = true;
+  const int64_t* k;
+  __device__ __forceinline__ uint64_t key(int64_t r) const { return (uint64_t)__ldg(k + r); }
+};
+struct KeysGeneral {
+  static constexpr bool kFast = false;
+  const DCol* cols;
+  int n;
+  __device__ __forceinline__ uint64_t key(int64_t r) const {
+    uint64_t h = general_hash(cols, n, r);
+    return h == EMPTY ? EMPTY + 1 : h;
+  }
+};
+
+__global__ void init_slots_kernel(ulonglong2* slots, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    slots[i] = make_ulonglong2(EMPTY, Y_INIT);
+}
+
+template <class K>
+__global__ void insert_kernel(K keys, int64_t n, ulonglong2* slots, int shift, uint64_t mask, uint64_t cap,
+                              uint32_t* dupflag, uint32_t* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = keys.key(i);
+    uint64_t s;
+    if (K::kFast && k == EMPTY) {
+      s = cap;  // side slot for the sentinel value
+    } else {
+      s = slot_of(k, shift);
+      uint64_t steps = 0;
+      bool ok = false;
+      while (steps <= mask) {
+        uint64_t cur = *(volatile unsigned long long*)&slots[s].x;
+        if (cur == k) { ok = true; break; }
+        if (cur == EMPTY) {
+          unsigned long long prev = atomicCAS((unsigned long long*)&slots[s].x, (unsigned long long)EMPTY,
+                                              (unsigned long long)k);
+          if (prev == EMPTY || prev == k) { ok = true; break; }
+        }
+        s = (s + 1) & mask;
+        ++steps;
+      }
+      if (!ok) { atomicOr(err, DERR_TABLE_FULL); continue; }
+    }
+    unsigned long long* yp = (unsigned long long*)&slots[s].y;
+    unsigned long long old = *(volatile unsigned long long*)yp, assumed;
+    do {
+      assumed = old;
+      uint32_t row = (uint32_t)assumed, cnt = (uint32_t)(assumed >> 32);
+      uint32_t nr = (uint32_t)i < row ? (uint32_t)i : row;
+      unsigned long long nw = ((unsigned long long)(cnt + 1) << 32) | nr;
+      old = atomicCAS(yp, assumed, nw);
+    } while (old != assumed);
+    if ((old >> 32) >= 1) *dupflag = 1;
+  }
+}
+
+// For each build row: its slot, and whether the slot holds several rows.
+template <class K>
+__global__ void locate_kernel(K keys, int64_t n, const ulonglong2* __restrict__ slots, int shift, uint64_t mask,
+                              uint64_t cap, uint32_t* __restrict__ row_slot, uint8_t* __restrict__ is_dup) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = keys.key(i);
+    uint64_t s;
+    if (K::kFast && k == EMPTY) s = cap;
+    else {
+      s = slot_of(k, shift);
+      uint64_t steps = 0;
+      while (slots[s].x != k && steps <= mask) { s = (s + 1) & mask; ++steps; }
+    }
+    row_slot[i] = (uint32_t)s;
+    is_dup[i] = (slots[s].y >> 32) > 1 ? 1 : 0;
+  }
+}
+
+__global__ void gather_u32_kernel(const uint32_t* src, const uint32_t* idx, int64_t n, uint32_t* dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
+}
+
+// sorted_slot[i] starts a segment -> slots[slot].row = i (cnt unchanged)
+__global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulonglong2* slots) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t s = sorted_slot[i];
+    if (i == 0 || sorted_slot[i - 1] != s) {
+      unsigned long long y = slots[s].y;
+      slots[s].y = (y & 0xFFFFFFFF00000000ULL) | (uint32_t)i;
+    }
+  }
+}
+
+// ------------------------------------------------------------- the probe --
+struct ProbeArgs {
+  int64_t n;
+  const ulonglong2* slots;
+  int shift;
+  uint64_t mask;
+  uint64_t cap;
+  const uint32_t* dup_rows;
+  const DCol* pcols;  // verify (general path)
+  const DCol* bcols;
+  int nkeys;
+  uint32_t* out_probe;
+  uint32_t* out_build;
+  int ngather;
+  int g_side[4];
+  const void* g_src[4];
+  int g_width[4];
+  void* g_dst[4];
+  uint64_t out_capacity;
+  unsigned long long* tile_status;
+  unsigned long long* tile_counter;
+  int64_t n_tiles;
+  unsigned long long* total;
+  uint32_t* err;
+};
+
+constexpr unsigned long long FLAG_A = 1ULL << 62;
+constexpr unsigned long long FLAG_P = 2ULL << 62;
+constexpr unsigned long long VAL_MASK = (1ULL << 62) - 1;
+
+// Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan
+// with Decoupled Look-back", 2016): publish this tile's aggregate, sum
+// predecessors' aggregates until one publishes an inclusive prefix. Tiles are
+// handed out in increasing order, so every predecessor is running or done;
+// the wait is still bounded and reports DERR_TIMEOUT.
+__device__ unsigned long long tile_lookback(unsigned long long* status, int64_t tile, unsigned long long agg,
+                                            uint32_t* err) {
+  if (tile == 0) {
+    atomicExch(&status[0], FLAG_P | agg);
+    return 0;
+  }
+  atomicExch(&status[tile], FLAG_A | agg);
+  unsigned long long excl = 0;
+  int64_t t = tile - 1;
+  uint32_t spins = 0;
+  while (t >= 0) {
+    unsigned long long s = *(volatile unsigned long long*)&status[t];
+    unsigned long long f = s & ~VAL_MASK;
+    if (f == 0) {
+      if (++spins > SPIN_LIMIT) {
+        atomicOr(err, DERR_TIMEOUT);
+        break;
+      }
+      __nanosleep(20);
+      continue;
+    }
+    excl += s & VAL_MASK;
+    if (f == FLAG_P) break;
+    --t;
+  }
+  atomicExch(&status[tile], FLAG_P | (excl + agg));
+  return excl;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan32(uint32_t x) {
+  int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void emit_one(const ProbeArgs& a, uint64_t pos, int64_t prow, uint32_t brow) {
+  if (a.out_probe) a.out_probe[pos] = (uint32_t)prow;
+  if (a.out_build) a.out_build[pos] = brow;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    if (g >= a.ngather) break;
+    int64_t src = a.g_side[g] ? (int64_t)brow : prow;
+    if (a.g_width[g] == 8)
+      static_cast<uint64_t*>(a.g_dst[g])[pos] = __ldg(static_cast<const unsigned long long*>(a.g_src[g]) + src);
+    else
+      static_cast<uint32_t*>(a.g_dst[g])[pos] = __ldg(static_cast<const unsigned int*>(a.g_src[g]) + src);
+  }
+}
+
+template <class K, bool DUPS, bool VERIFY, bool EMIT>
+__global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
+  __shared__ uint32_t s_wexcl[PW];
+  __shared__ unsigned long long s_excl;
+  __shared__ int64_t s_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.tile_counter, 1ULL);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    if (tile >= a.n_tiles) break;
+    const int64_t base = tile * PT + warp * (32 * PI);
+
+    uint64_t key[PI];
+    uint64_t s[PI];
+    ulonglong2 e[PI];
+#pragma unroll
+    for (int it = 0; it < PI; ++it) {
+      int64_t r = base + it * 32 + lane;
+      key[it] = r < a.n ? keys.key(r) : EMPTY;
+    }
+#pragma unroll
+    for (int it = 0; it < PI; ++it) {
+      int64_t r = base + it * 32 + lane;
+      if (r < a.n) {
+        s[it] = (K::kFast && key[it] == EMPTY) ? a.cap : slot_of(key[it], a.shift);
+        e[it] = __ldg(a.slots + s[it]);
+      } else {
+        e[it] = make_ulonglong2(EMPTY, 0);
+      }
+    }
+    uint32_t c[PI];
+#pragma unroll
+    for (int it = 0; it < PI; ++it) {
+      int64_t r = base + it * 32 + lane;
+      c[it] = 0;
+      if (r >= a.n) continue;
+      uint64_t steps = 0;
+      while (e[it].x != key[it] && e[it].x != EMPTY && steps <= a.mask) {
+        s[it] = (s[it] + 1) & a.mask;
+        e[it] = __ldg(a.slots + s[it]);
+        ++steps;
+      }
+      uint32_t cnt = (uint32_t)(e[it].y >> 32);
+      if (e[it].x != key[it] || cnt == 0) continue;
+      uint32_t v = (uint32_t)e[it].y;
+      if (!VERIFY) {
+        c[it] = DUPS ? cnt : 1u;
+      } else if (cnt == 1) {
+        c[it] = rows_equal(a.pcols, a.bcols, a.nkeys, r, v) ? 1u : 0u;
+      } else {
+        uint32_t m = 0;
+        for (uint32_t j = 0; j < cnt; ++j) m += rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v + j]) ? 1u : 0u;
+        c[it] = m;
+      }
+    }
+    // rank matches inside the warp (row order = it-major, lane-minor)
+    uint32_t lex[PI];
+    uint32_t run = 0;
+#pragma unroll
+    for (int it = 0; it < PI; ++it) {
+      uint32_t incl = warp_incl_scan32(c[it]);
+      lex[it] = run + incl - c[it];
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) s_wexcl[warp] = run;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t v = lane < PW ? s_wexcl[lane] : 0;
+      uint32_t incl = warp_incl_scan32(v);
+      uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
+      if (lane < PW) s_wexcl[lane] = incl - v;
+      if (lane == 0) {
+        if (EMIT) {
+          unsigned long long ex = tile_lookback(a.tile_status, tile, tile_total, a.err);
+          s_excl = ex;
+          if (tile == a.n_tiles - 1) *a.total = ex + tile_total;
+        } else {
+          if (tile_total) atomicAdd(a.total, (unsigned long long)tile_total);
+          s_excl = 0;
+        }
+      }
+    }
+    __syncthreads();
+    if (EMIT) {
+      const uint64_t wbase = s_excl + s_wexcl[warp];
+#pragma unroll
+      for (int it = 0; it < PI; ++it) {
+        if (!c[it]) continue;
+        int64_t r = base + it * 32 + lane;
+        uint64_t pos = wbase + lex[it];
+        if (pos + c[it] > a.out_capacity) {
+          atomicOr(a.err, DERR_CAPACITY);
+          continue;
+        }
+        uint32_t cnt = (uint32_t)(e[it].y >> 32);
+        uint32_t v = (uint32_t)e[it].y;
+        if (!DUPS && !VERIFY) {
+          emit_one(a, pos, r, v);
+        } else if (cnt == 1) {
+          emit_one(a, pos, r, v);
+        } else {
+          for (uint32_t j = 0; j < cnt; ++j) {
+            uint32_t b = a.dup_rows[v + j];
+            if (VERIFY && !rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
+            emit_one(a, pos++, r, b);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class K, bool EMIT>
+void launch_probe(Ctx& ctx, const JoinTable& t, K keys, ProbeArgs& a, int blocks_per_sm) {
+  int grid = (int)std::min<int64_t>(a.n_tiles, (int64_t)ctx.sm_count * blocks_per_sm);
+  if (grid < 1) grid = 1;
+  bool verify = !t.int64_fast;
+  KernelTimer kt(ctx, EMIT ? "probe_kernel" : "probe_count_kernel");
+  if (!t.has_dups && !verify)
+    probe_kernel<K, false, false, EMIT><<<grid, PW * 32, 0, ctx.stream>>>(keys, a);
+  else if (!verify)
+    probe_kernel<K, true, false, EMIT><<<grid, PW * 32, 0, ctx.stream>>>(keys, a);
+  else
+    probe_kernel<K, true, true, EMIT><<<grid, PW * 32, 0, ctx.stream>>>(keys, a);
+  ctx.check_launch("probe_kernel");
+}
+
+}  // namespace
+
+void check_join_keys(const Batch& probe, const std::vector<int>& pk, const Batch& build, const std::vector<int>& bk) {
+  if (pk.empty() || pk.size() != bk.size())
+    fail(PRISM_ERR_INVALID_ARGUMENT, "probe and build key lists must be non-empty and of equal length");
+  for (size_t i = 0; i < pk.size(); ++i) {
+    if (pk[i] < 0 || pk[i] >= (int)probe.cols.size()) fail(PRISM_ERR_INVALID_ARGUMENT, "probe key column out of range");
+    if (bk[i] < 0 || bk[i] >= (int)build.cols.size()) fail(PRISM_ERR_INVALID_ARGUMENT, "build key column out of range");
+    int a = probe.cols[pk[i]]->type, b = build.cols[bk[i]]->type;
+    bool sa = a == TY_UTF8 || a == TY_DICT, sb = b == TY_UTF8 || b == TY_DICT;
+    if (a != b && !(sa && sb))
+      fail(PRISM_ERR_SCHEMA_MISMATCH, "join key types differ between probe and build (column " +
+                                          std::to_string(pk[i]) + " vs " + std::to_string(bk[i]) + ")");
+  }
+}
+
+std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,
+                                            const JoinTuning& tune) {
+  auto t = std::make_unique<JoinTable>();
+  t->ctx = &ctx;
+  t->build = build;
+  t->key_cols = keys;
+  for (int k : keys)
+    if (k < 0 || k >= (int)build.cols.size()) fail(PRISM_ERR_INVALID_ARGUMENT, "build key column out of range");
+  if (keys.empty()) fail(PRISM_ERR_INVALID_ARGUMENT, "no join keys");
+  int64_t n = build.rows;
+  if (n >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "build side exceeds 2^32-1 rows");
+  t->int64_fast = keys.size() == 1 && build.cols[keys[0]]->type == TY_I64;
+  double lf = std::min(0.9, std::max(0.1, tune.load_factor));
+  uint64_t cap = next_pow2((uint64_t)std::ceil((double)std::max<int64_t>(n, 1) / lf));
+  if (cap < 16) cap = 16;
+  t->capacity = cap;
+  t->log2cap = 63 - __builtin_clzll(cap);
+  t->slots = ctx.alloc((cap + 1) * sizeof(ulonglong2));
+  ulonglong2* slots = static_cast<ulonglong2*>(t->slots->ptr);
+  init_slots_kernel<<<grid_for(ctx, (int64_t)cap + 1, 256), 256, 0, ctx.stream>>>(slots, cap + 1);
+  ctx.check_launch("init_slots_kernel");
+
+  for (int k : keys) t->key_views.push_back(build.cols[k]->view());
+  t->key_views_dev = ctx.alloc(t->key_views.size() * sizeof(DCol));
+  PRISM_CUDA(cudaMemcpyAsync(t->key_views_dev->ptr, t->key_views.data(), t->key_views.size() * sizeof(DCol),
+                             cudaMemcpyHostToDevice, ctx.stream));
+  MemP mflag;
+  uint32_t* dupflag = ctx.alloc_t<uint32_t>(1, mflag);
+  PRISM_CUDA(cudaMemsetAsync(dupflag, 0, 4, ctx.stream));
+  int shift = 64 - t->log2cap;
+  uint64_t mask = cap - 1;
+  if (n > 0) {
+    int g = grid_for(ctx, n, 256, 16);
+    KernelTimer kt(ctx, "insert_kernel");
+    if (t->int64_fast) {
+      KeysFast kf{static_cast<const int64_t*>(build.cols[keys[0]]->values)};
+      insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err);
+    } else {
+      KeysGeneral kg{static_cast<const DCol*>(t->key_views_dev->ptr), (int)keys.size()};
+      insert_kernel<<<g, 256, 0, ctx.stream>>>(kg, n, slots, shift, mask, cap, dupflag, ctx.d_err);
+    }
+    ctx.check_launch("insert_kernel");
+  }
+  uint32_t hdup = 0;
+  PRISM_CUDA(cudaMemcpyAsync(&hdup, dupflag, 4, cudaMemcpyDeviceToHost, ctx.stream));
+  uint32_t derr = ctx.take_device_errors();
+  if (derr & DERR_TABLE_FULL) fail(PRISM_ERR_TABLE_FULL, "join hash table full");
+  t->has_dups = hdup != 0;
+  if (t->has_dups) {
+    // rows of multi-row slots, in row order, stably grouped by slot
+    MemP mrs, mdup;
+    uint32_t* row_slot = ctx.alloc_t<uint32_t>((size_t)n, mrs);
+    uint8_t* is_dup = ctx.alloc_t<uint8_t>((size_t)n, mdup);
+    int g = grid_for(ctx, n, 256, 16);
+    if (t->int64_fast) {
+      KeysFast kf{static_cast<const int64_t*>(build.cols[keys[0]]->values)};
+      locate_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, row_slot, is_dup);
+    } else {
+      KeysGeneral kg{static_cast<const DCol*>(t->key_views_dev->ptr), (int)keys.size()};
+      locate_kernel<<<g, 256, 0, ctx.stream>>>(kg, n, slots, shift, mask, cap, row_slot, is_dup);
+    }
+    ctx.check_launch("locate_kernel");
+    MemP mbits;
+    uint8_t* bits = ctx.alloc_t<uint8_t>((size_t)(n + 31) / 8 + 8, mbits);
+    pack_bits(ctx, is_dup, n, bits);
+    int64_t nd = 0;
+    MemP rows = compact_bits(ctx, bits, n, false, &nd);
+    MemP mks;
+    uint32_t* seg_slot = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(nd, 1), mks);
+    if (nd) {
+      gather_u32_kernel<<<grid_for(ctx, nd, 256), 256, 0, ctx.stream>>>(row_slot, static_cast<uint32_t*>(rows->ptr),
+                                                                         nd, seg_slot);
+      ctx.check_launch("gather_u32_kernel");
+      stable_sort_pairs_u32(ctx, seg_slot, static_cast<uint32_t*>(rows->ptr), nd, t->log2cap + 1);
+      segment_heads_kernel<<<grid_for(ctx, nd, 256), 256, 0, ctx.stream>>>(seg_slot, nd, slots);
+      ctx.check_launch("segment_heads_kernel");
+    }
+    t->dup_rows = rows;
+    t->n_dup_rows = nd;
+  }
+  return t;
+}
+
+int64_t match_upper_bound(const JoinTable& t, int64_t probe_rows) {
+  return t.has_dups ? -1 : probe_rows;
+}
+
+static void fill_common(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys, ProbeArgs& a,
+                        std::vector<DCol>& pviews, MemP& pviews_dev) {
+  a = ProbeArgs{};
+  a.n = probe.rows;
+  a.slots = static_cast<const ulonglong2*>(t.slots->ptr);
+  a.shift = 64 - t.log2cap;
+  a.mask = t.capacity - 1;
+  a.cap = t.capacity;
+  a.dup_rows = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+  a.nkeys = (int)keys.size();
+  a.err = ctx.d_err;
+  a.bcols = static_cast<const DCol*>(t.key_views_dev->ptr);
+  for (int k : keys) pviews.push_back(probe.cols[k]->view());
+  pviews_dev = ctx.alloc(pviews.size() * sizeof(DCol));
+  PRISM_CUDA(cudaMemcpyAsync(pviews_dev->ptr, pviews.data(), pviews.size() * sizeof(DCol), cudaMemcpyHostToDevice,
+                             ctx.stream));
+  a.pcols = static_cast<const DCol*>(pviews_dev->ptr);
+  a.n_tiles = ceil_div(a.n, PT);
+}
+
+int64_t probe_count(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
+                    const JoinTuning& tune) {
+  check_join_keys(probe, keys, t.build, t.key_cols);
+  if (probe.rows == 0 || t.build.rows == 0) return 0;
+  ProbeArgs a;
+  std::vector<DCol> pv;
+  MemP pvd;
+  fill_common(ctx, t, probe, keys, a, pv, pvd);
+  MemP mc, mt;
+  a.tile_counter = ctx.alloc_t<unsigned long long>(1, mc);
+  a.total = ctx.alloc_t<unsigned long long>(1, mt);
+  PRISM_CUDA(cudaMemsetAsync(a.tile_counter, 0, 8, ctx.stream));
+  PRISM_CUDA(cudaMemsetAsync(a.total, 0, 8, ctx.stream));
+  if (t.int64_fast)
+    launch_probe<KeysFast, false>(ctx, t, KeysFast{static_cast<const int64_t*>(probe.cols[keys[0]]->values)}, a,
+                                  tune.probe_blocks_per_sm);
+  else
+    launch_probe<KeysGeneral, false>(ctx, t, KeysGeneral{a.pcols, a.nkeys}, a, tune.probe_blocks_per_sm);
+  unsigned long long total = 0;
+  PRISM_CUDA(cudaMemcpyAsync(&total, a.total, 8, cudaMemcpyDeviceToHost, ctx.stream));
+  uint32_t derr = ctx.take_device_errors();
+  if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+  return (int64_t)total;
+}
+
+ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
+                             bool want_probe_idx, bool want_build_idx, std::vector<ProbeGather>& gathers,
+                             int64_t gather_capacity, const JoinTuning& tune) {
+  check_join_keys(probe, keys, t.build, t.key_cols);
+  ProbeResult res;
+  if (gathers.size() > 4) fail(PRISM_ERR_INTERNAL, "at most 4 fused gathers");
+  int64_t cap = gather_capacity;
+  if (cap < 0) {
+    int64_t ub = match_upper_bound(t, probe.rows);
+    cap = ub >= 0 ? ub : probe_count(ctx, t, probe, keys, tune);
+  }
+  if (want_probe_idx) res.probe_idx = ctx.alloc((size_t)std::max<int64_t>(cap, 1) * 4);
+  if (want_build_idx) res.build_idx = ctx.alloc((size_t)std::max<int64_t>(cap, 1) * 4);
+  if (probe.rows == 0 || t.build.rows == 0) return res;
+  ProbeArgs a;
+  std::vector<DCol> pv;
+  MemP pvd;
+  fill_common(ctx, t, probe, keys, a, pv, pvd);
+  a.out_probe = want_probe_idx ? static_cast<uint32_t*>(res.probe_idx->ptr) : nullptr;
+  a.out_build = want_build_idx ? static_cast<uint32_t*>(res.build_idx->ptr) : nullptr;
+  a.ngather = (int)gathers.size();
+  for (size_t g = 0; g < gathers.size(); ++g) {
+    a.g_side[g] = gathers[g].side;
+    a.g_src[g] = gathers[g].src;
+    a.g_width[g] = gathers[g].width;
+    a.g_dst[g] = gathers[g].dst;
+  }
+  a.out_capacity = (uint64_t)cap;
+  MemP ms, mc, mt;
+  a.tile_status = ctx.alloc_t<unsigned long long>((size_t)a.n_tiles, ms);
+  a.tile_counter = ctx.alloc_t<unsigned long long>(1, mc);
+  a.total = ctx.alloc_t<unsigned long long>(1, mt);
+  PRISM_CUDA(cudaMemsetAsync(a.tile_status, 0, (size_t)a.n_tiles * 8, ctx.stream));
+  PRISM_CUDA(cudaMemsetAsync(a.tile_counter, 0, 8, ctx.stream));
+  PRISM_CUDA(cudaMemsetAsync(a.total, 0, 8, ctx.stream));
+  if (t.int64_fast)
+    launch_probe<KeysFast, true>(ctx, t, KeysFast{static_cast<const int64_t*>(probe.cols[keys[0]]->values)}, a,
+                                 tune.probe_blocks_per_sm);
+  else
+    launch_probe<KeysGeneral, true>(ctx, t, KeysGeneral{a.pcols, a.nkeys}, a, tune.probe_blocks_per_sm);
+  unsigned long long total = 0;
+  PRISM_CUDA(cudaMemcpyAsync(&total, a.total, 8, cudaMemcpyDeviceToHost, ctx.stream));
+  uint32_t derr = ctx.take_device_errors();
+  if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+  if (derr & DERR_CAPACITY) fail(PRISM_ERR_INTERNAL, "probe output capacity exceeded");
+  res.matches = (int64_t)total;
+  return res;
+}
+
+}  // namespace prism

@@ -1,0 +1,63 @@
+// join.hpp — device hash table and probe of the hash join
+// (native/prism-executor/src/hash_join.rs).
+#pragma once
+
+#include "runtime.hpp"
+
+namespace prism {
+
+struct JoinTable {
+  Ctx* ctx = nullptr;
+  Batch build;               // shares the build batch's device columns
+  std::vector<int> key_cols;
+  bool int64_fast = false;   // single Int64 key: keyed by raw value, validity ignored
+  int log2cap = 0;
+  uint64_t capacity = 0;     // power of two (+1 side slot at [capacity])
+  MemP slots;                // ulonglong2 per slot: x = key (or row hash), y = cnt << 32 | row
+  bool has_dups = false;     // some slot holds more than one build row
+  MemP dup_rows;             // build rows grouped by slot, ascending inside a slot
+  int64_t n_dup_rows = 0;
+  std::vector<DCol> key_views;
+  MemP key_views_dev;
+};
+
+struct JoinTuning {
+  double load_factor = 0.5;
+  int probe_blocks_per_sm = 8;
+};
+
+std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,
+                                            const JoinTuning& tune);
+
+// Output spec of a probe: which index arrays to emit and which fixed-width
+// null-free columns to gather inside the probe kernel.
+struct ProbeGather {
+  int side;          // 0 probe, 1 build
+  const void* src;   // column values
+  int width;         // 4 or 8
+  void* dst;         // output values (capacity rows)
+};
+
+struct ProbeResult {
+  int64_t matches = 0;
+  MemP probe_idx, build_idx;  // u32 arrays (may be empty if not requested)
+};
+
+// Probes `probe` (key columns `keys`, types checked against the table) and
+// emits matches in the reference's order: probe rows ascending, build rows
+// ascending within a probe row. Fused gathers write into caller buffers of
+// `gather_capacity` rows (must be >= the match count; use probe_count first).
+ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
+                             bool want_probe_idx, bool want_build_idx, std::vector<ProbeGather>& gathers,
+                             int64_t gather_capacity, const JoinTuning& tune);
+
+// Number of matches of `probe` against the table (no output).
+int64_t probe_count(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
+                    const JoinTuning& tune);
+
+// Upper bound on the match count usable without a counting pass (-1 if none).
+int64_t match_upper_bound(const JoinTable& t, int64_t probe_rows);
+
+void check_join_keys(const Batch& probe, const std::vector<int>& pk, const Batch& build, const std::vector<int>& bk);
+
+}  // namespace prism

@@ -71,6 +71,8 @@ def _declare(lib):
     lib.prism_ctx_kernel_launches.argtypes = [P]
     lib.prism_ctx_kernel_launches.restype = C.c_uint64
     lib.prism_version.restype = C.c_char_p
+    lib.prism_ctx_set_profiling.argtypes = [P, I]
+    lib.prism_ctx_kernel_stats.argtypes = [P, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     lib.prism_batch_import.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_import_device.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_export.argtypes = [P, P, P, P]
@@ -151,6 +153,17 @@ class Context:
     def kernel_launches(self) -> int:
         return int(lib().prism_ctx_kernel_launches(self._h))
 
+    def set_profiling(self, enable: bool):
+        """Brackets the hot kernels with CUDA events (see kernel_stats)."""
+        self.check(lib().prism_ctx_set_profiling(self._h, 1 if enable else 0))
+
+    def kernel_stats(self, name: str):
+        """(launches, total device ms) of kernel `name` since profiling was enabled."""
+        n = C.c_uint64(0)
+        ms = C.c_double(0)
+        self.check(lib().prism_ctx_kernel_stats(self._h, name.encode(), C.byref(n), C.byref(ms)))
+        return int(n.value), float(ms.value)
+
     def close(self):
         if self._h:
             lib().prism_ctx_destroy(self._h)
@@ -189,6 +202,37 @@ class DeviceBatch:
         ctx.check(lib().prism_batch_import(ctx.handle, e.array_ptr, e.schema_ptr, C.byref(h)))
         e.release()
         return DeviceBatch(ctx, h)
+
+    @staticmethod
+    def from_device_buffers(columns, num_rows: int, ctx: Optional[Context] = None, device_id: int = 0) -> "DeviceBatch":
+        """Wraps device-resident, null-free fixed-width columns without a copy.
+
+        columns: list of (name, arrow_format, device_pointer); the memory must
+        outlive the batch (e.g. torch tensors the caller keeps).
+        """
+        ctx = ctx or default_context()
+        keep = []
+        n = len(columns)
+        child_arrays = (C.POINTER(_abi.ArrowArray) * n)()
+        child_schemas = (C.POINTER(_abi.ArrowSchema) * n)()
+        for i, (name, fmt, ptr) in enumerate(columns):
+            bufs = (C.c_void_p * 2)(None, ptr)
+            a = _abi.ArrowArray(num_rows, 0, 0, 2, 0, bufs, None, None)
+            nm, fm = name.encode(), fmt.encode()
+            s_ = _abi.ArrowSchema(fm, nm, None, 0, 0, None, None)
+            keep += [bufs, a, s_, nm, fm]
+            child_arrays[i] = C.pointer(a)
+            child_schemas[i] = C.pointer(s_)
+        top_bufs = (C.c_void_p * 1)(None)
+        dev = _abi.ArrowDeviceArray()
+        dev.array = _abi.ArrowArray(num_rows, 0, 0, 1, n, top_bufs, child_arrays, None)
+        dev.device_id = device_id
+        dev.device_type = _abi.ARROW_DEVICE_CUDA
+        sch = _abi.ArrowSchema(b"+s", b"", None, 0, n, child_schemas, None)
+        keep += [top_bufs, child_arrays, child_schemas]
+        h = C.c_void_p()
+        ctx.check(lib().prism_batch_import_device(ctx.handle, C.byref(dev), C.byref(sch), C.byref(h)))
+        return DeviceBatch(ctx, h, keepalive=keep)
 
     @property
     def handle(self):
