@@ -42,12 +42,21 @@ CPU_SAMPLE_PROBE = 10_000_000
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["prism", "reference"], default="prism")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="scale all sizes (profiling captures use a smaller case; bench lines use 1.0)")
+    a = ap.parse_args()
+    global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE
+    if a.scale != 1.0:
+        N_BUILD = int(N_BUILD * a.scale)
+        N_PROBE = int(N_PROBE * a.scale)
+        ZIPF_RANKS = int(ZIPF_RANKS * a.scale)
+        CPU_SAMPLE_PROBE = min(CPU_SAMPLE_PROBE, N_PROBE)
+    return a
 
 
 def peaks():
@@ -195,6 +204,7 @@ def main():
     launches0 = ctx.kernel_launches
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_index) as clocks:
+        time.sleep(0.5)  # let the sampler start before the timed region
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -207,7 +217,11 @@ def main():
             dist.barrier()
     ms = start.elapsed_time(stop)
     launches = ctx.kernel_launches - launches0
-    n_probe_launch, probe_ms = ctx.kernel_stats("probe_kernel")
+    # the probe phase: probe_rows_kernel + emit_rows_kernel (unique int64
+    # keys) or the single-pass probe_kernel (duplicate / general keys)
+    kstats = {k: ctx.kernel_stats(k) for k in ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel")}
+    n_probe_launch = max(kstats["probe_rows_kernel"][0], kstats["probe_kernel"][0])
+    probe_ms = sum(v[1] for v in kstats.values())
     n_ins, ins_ms = ctx.kernel_stats("insert_kernel")
     ctx.set_profiling(False)
     t = torch.tensor([ms], device=device, dtype=torch.float64)
@@ -267,7 +281,8 @@ def main():
             },
             "roofline": {
                 "bound": "hbm",
-                "kernel": "probe_kernel",
+                "kernel": "probe phase (probe_rows_kernel + emit_rows_kernel)",
+                "kernel_ms_per_launch": {k: (v[1] / v[0] if v[0] else None) for k, v in kstats.items()},
                 "achieved": achieved,
                 "peak": peak,
                 "unit": "GB/s",

@@ -255,22 +255,6 @@ __device__ __forceinline__ uint64_t dist_value_id(const AggArgs& a, const Op& o,
   }
 }
 
-__device__ __forceinline__ unsigned long long cas128(unsigned long long* p, unsigned long long cmp_lo,
-                                                     unsigned long long cmp_hi, unsigned long long new_lo,
-                                                     unsigned long long new_hi, unsigned long long& old_hi) {
-  unsigned long long old_lo;
-  asm volatile(
-      "{\n\t.reg .b128 d, c, n;\n\t"
-      "mov.b128 c, {%3, %4};\n\t"
-      "mov.b128 n, {%5, %6};\n\t"
-      "atom.global.cas.b128 d, [%2], c, n;\n\t"
-      "mov.b128 {%0, %1}, d;\n\t}"
-      : "=l"(old_lo), "=l"(old_hi)
-      : "l"(p), "l"(cmp_lo), "l"(cmp_hi), "l"(new_lo), "l"(new_hi)
-      : "memory");
-  return old_lo;
-}
-
 // Inserts (group, value) into a distinct set; duplicates are ignored.
 __device__ void distinct_insert(const DistinctTable& t, uint64_t g, uint64_t v, uint32_t* err) {
   uint64_t s = mix64(g * FIB ^ mix64(v)) & t.mask;

@@ -183,6 +183,24 @@ __device__ __forceinline__ double from_total_key(int64_t k) {
   return __longlong_as_double(i);
 }
 
+// 128-bit compare-and-swap (sm_90+ atom.cas.b128) on global memory;
+// returns the old low word, old high word in old_hi.
+__device__ __forceinline__ unsigned long long cas128(unsigned long long* p, unsigned long long cmp_lo,
+                                                     unsigned long long cmp_hi, unsigned long long new_lo,
+                                                     unsigned long long new_hi, unsigned long long& old_hi) {
+  unsigned long long old_lo;
+  asm volatile(
+      "{\n\t.reg .b128 d, c, n;\n\t"
+      "mov.b128 c, {%3, %4};\n\t"
+      "mov.b128 n, {%5, %6};\n\t"
+      "atom.global.cas.b128 d, [%2], c, n;\n\t"
+      "mov.b128 {%0, %1}, d;\n\t}"
+      : "=l"(old_lo), "=l"(old_hi)
+      : "l"(p), "l"(cmp_lo), "l"(cmp_hi), "l"(new_lo), "l"(new_hi)
+      : "memory");
+  return old_lo;
+}
+
 // Bounded spin limit for every wait on another CTA.
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
 

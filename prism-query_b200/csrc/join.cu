@@ -8,7 +8,7 @@
 // that occur more than once live in contiguous ascending segments.
 //
 // The probe is one pass over the probe keys: each CTA takes a tile of 2048
-// rows, resolves its slots (8 independent 16-byte loads in flight per lane),
+// rows, resolves its slots (4 independent 16-byte loads in flight per lane),
 // ranks the matches with warp scans, obtains the tile's output offset by
 // decoupled look-back over the preceding tiles, and writes matches in the
 // reference's order (probe row ascending, build rows ascending) — no second
@@ -21,11 +21,11 @@ namespace prism {
 namespace {
 
 constexpr uint64_t EMPTY = 0x8000000000000000ULL;
-constexpr uint64_t Y_INIT = 0x00000000FFFFFFFFULL;  // cnt 0, row = max
+constexpr uint64_t Y_INIT = 0;  // cnt 0
 constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
 
-constexpr int PW = 8;              // warps per probe CTA
-constexpr int PI = 8;              // rows per lane
+constexpr int PW = 16;             // warps per probe CTA
+constexpr int PI = 4;              // rows per lane
 constexpr int PT = PW * 32 * PI;   // rows per tile (2048)
 
 __device__ __forceinline__ uint64_t slot_of(uint64_t k, int shift) { return (k * FIB) >> shift; }
@@ -128,34 +128,36 @@ __global__ void insert_kernel(K keys, int64_t n, ulonglong2* slots, int shift, u
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint64_t k = keys.key(i);
     uint64_t s;
+    bool winner = false;
     if (K::kFast && k == EMPTY) {
       s = cap;  // side slot for the sentinel value
+      winner = true;
     } else {
+      // one 128-bit CAS claims an empty slot with {key, count 1 | row};
+      // finding the key already there falls through to the count update
       s = slot_of(k, shift);
       uint64_t steps = 0;
       bool ok = false;
       while (steps <= mask) {
-        uint64_t cur = *(volatile unsigned long long*)&slots[s].x;
-        if (cur == k) { ok = true; break; }
-        if (cur == EMPTY) {
-          unsigned long long prev = atomicCAS((unsigned long long*)&slots[s].x, (unsigned long long)EMPTY,
-                                              (unsigned long long)k);
-          if (prev == EMPTY || prev == k) { ok = true; break; }
-        }
+        unsigned long long old_y;
+        unsigned long long prev = cas128((unsigned long long*)&slots[s], EMPTY, Y_INIT, k,
+                                         (1ULL << 32) | (uint32_t)i, old_y);
+        if (prev == EMPTY && old_y == Y_INIT) { ok = winner = true; break; }
+        if (prev == k) { ok = true; break; }
         s = (s + 1) & mask;
         ++steps;
       }
       if (!ok) { atomicOr(err, DERR_TABLE_FULL); continue; }
+      if (winner) continue;  // inserted with its count and row
     }
-    unsigned long long* yp = (unsigned long long*)&slots[s].y;
-    unsigned long long old = *(volatile unsigned long long*)yp, assumed;
-    do {
-      assumed = old;
-      uint32_t row = (uint32_t)assumed, cnt = (uint32_t)(assumed >> 32);
-      uint32_t nr = (uint32_t)i < row ? (uint32_t)i : row;
-      unsigned long long nw = ((unsigned long long)(cnt + 1) << 32) | nr;
-      old = atomicCAS(yp, assumed, nw);
-    } while (old != assumed);
+    // one atomic: count the row, and let the slot's first inserter record
+    // its row (slots with several rows get sorted segments afterwards)
+    unsigned long long add = (1ULL << 32) | (winner && !(K::kFast && k == EMPTY) ? (uint32_t)i : 0u);
+    unsigned long long old = atomicAdd((unsigned long long*)&slots[s].y, add);
+    if (K::kFast && k == EMPTY && (old >> 32) == 0) {
+      // side slot: the first arrival stores its row (count already added)
+      atomicOr((unsigned long long*)&slots[s].y, (unsigned long long)(uint32_t)i);
+    }
     if ((old >> 32) >= 1) *dupflag = 1;
   }
 }
@@ -225,36 +227,47 @@ constexpr unsigned long long FLAG_P = 2ULL << 62;
 constexpr unsigned long long VAL_MASK = (1ULL << 62) - 1;
 
 // Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan
-// with Decoupled Look-back", 2016): publish this tile's aggregate, sum
-// predecessors' aggregates until one publishes an inclusive prefix. Tiles are
-// handed out in increasing order, so every predecessor is running or done;
-// the wait is still bounded and reports DERR_TIMEOUT.
-__device__ unsigned long long tile_lookback(unsigned long long* status, int64_t tile, unsigned long long agg,
+// with Decoupled Look-back", 2016), run by one warp: publish this tile's
+// aggregate, then inspect 32 predecessors per round trip, summing aggregates
+// up to the nearest tile that already published its inclusive prefix. Tiles
+// are handed out in increasing order, so every predecessor is running or
+// done; the wait is still bounded and reports DERR_TIMEOUT.
+__device__ unsigned long long warp_lookback(unsigned long long* status, int64_t tile, unsigned long long agg,
                                             uint32_t* err) {
+  const int lane = threadIdx.x & 31;
   if (tile == 0) {
-    atomicExch(&status[0], FLAG_P | agg);
+    if (lane == 0) atomicExch(&status[0], FLAG_P | agg);
     return 0;
   }
-  atomicExch(&status[tile], FLAG_A | agg);
+  if (lane == 0) atomicExch(&status[tile], FLAG_A | agg);
   unsigned long long excl = 0;
   int64_t t = tile - 1;
   uint32_t spins = 0;
-  while (t >= 0) {
-    unsigned long long s = *(volatile unsigned long long*)&status[t];
-    unsigned long long f = s & ~VAL_MASK;
-    if (f == 0) {
+  for (;;) {
+    int64_t idx = t - lane;
+    unsigned long long st = FLAG_P + 0ULL;
+    if (idx >= 0) st = *(volatile unsigned long long*)&status[idx];
+    unsigned long long f = st & ~VAL_MASK;
+    uint32_t pmask = __ballot_sync(0xffffffffu, f == FLAG_P);
+    uint32_t zmask = __ballot_sync(0xffffffffu, f == 0);
+    int first_p = pmask ? __ffs(pmask) - 1 : 31;
+    uint32_t need = (first_p == 31) ? 0xffffffffu : ((2u << first_p) - 1u);
+    if (zmask & need) {
       if (++spins > SPIN_LIMIT) {
-        atomicOr(err, DERR_TIMEOUT);
+        if (lane == 0) atomicOr(err, DERR_TIMEOUT);
         break;
       }
-      __nanosleep(20);
+      __nanosleep(32);
       continue;
     }
-    excl += s & VAL_MASK;
-    if (f == FLAG_P) break;
-    --t;
+    unsigned long long v = lane <= first_p ? (st & VAL_MASK) : 0ULL;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    excl += v;
+    if (pmask) break;
+    t -= 32;
   }
-  atomicExch(&status[tile], FLAG_P | (excl + agg));
+  if (lane == 0) atomicExch(&status[tile], FLAG_P | (excl + agg));
   return excl;
 }
 
@@ -282,8 +295,11 @@ __device__ __forceinline__ void emit_one(const ProbeArgs& a, uint64_t pos, int64
   }
 }
 
+// One CTA = PW warps; a tile = PT consecutive probe rows; warp w owns rows
+// [tile*PT + w*32*PI, +32*PI) in PI lane-strided groups (coalesced loads,
+// row order = item-major, lane-minor).
 template <class K, bool DUPS, bool VERIFY, bool EMIT>
-__global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
+__global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) {
   __shared__ uint32_t s_wexcl[PW];
   __shared__ unsigned long long s_excl;
   __shared__ int64_t s_tile;
@@ -295,50 +311,55 @@ __global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
     if (tile >= a.n_tiles) break;
     const int64_t base = tile * PT + warp * (32 * PI);
 
-    uint64_t key[PI];
-    uint64_t s[PI];
-    ulonglong2 e[PI];
+    uint32_t c[PI], v[PI], cand[PI];
+    {
+      uint64_t key[PI];
+      uint64_t s[PI];
+      ulonglong2 e[PI];
 #pragma unroll
-    for (int it = 0; it < PI; ++it) {
-      int64_t r = base + it * 32 + lane;
-      key[it] = r < a.n ? keys.key(r) : EMPTY;
-    }
+      for (int it = 0; it < PI; ++it) {
+        int64_t r = base + it * 32 + lane;
+        key[it] = r < a.n ? keys.key(r) : EMPTY;
+      }
 #pragma unroll
-    for (int it = 0; it < PI; ++it) {
-      int64_t r = base + it * 32 + lane;
-      if (r < a.n) {
-        s[it] = (K::kFast && key[it] == EMPTY) ? a.cap : slot_of(key[it], a.shift);
-        e[it] = __ldg(a.slots + s[it]);
-      } else {
-        e[it] = make_ulonglong2(EMPTY, 0);
+      for (int it = 0; it < PI; ++it) {
+        int64_t r = base + it * 32 + lane;
+        if (r < a.n) {
+          s[it] = (K::kFast && key[it] == EMPTY) ? a.cap : slot_of(key[it], a.shift);
+          e[it] = __ldg(a.slots + s[it]);
+        } else {
+          e[it] = make_ulonglong2(EMPTY, 0);
+        }
+      }
+#pragma unroll
+      for (int it = 0; it < PI; ++it) {
+        int64_t r = base + it * 32 + lane;
+        c[it] = 0;
+        v[it] = 0;
+        cand[it] = 0;
+        if (r >= a.n) continue;
+        uint64_t steps = 0;
+        while (e[it].x != key[it] && e[it].x != EMPTY && steps <= a.mask) {
+          s[it] = (s[it] + 1) & a.mask;
+          e[it] = __ldg(a.slots + s[it]);
+          ++steps;
+        }
+        uint32_t cnt = (uint32_t)(e[it].y >> 32);
+        if (e[it].x != key[it] || cnt == 0) continue;
+        v[it] = (uint32_t)e[it].y;
+        cand[it] = cnt;
+        if (!VERIFY) {
+          c[it] = DUPS ? cnt : 1u;
+        } else if (cnt == 1) {
+          c[it] = rows_equal(a.pcols, a.bcols, a.nkeys, r, v[it]) ? 1u : 0u;
+        } else {
+          uint32_t m = 0;
+          for (uint32_t j = 0; j < cnt; ++j) m += rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v[it] + j]) ? 1u : 0u;
+          c[it] = m;
+        }
       }
     }
-    uint32_t c[PI];
-#pragma unroll
-    for (int it = 0; it < PI; ++it) {
-      int64_t r = base + it * 32 + lane;
-      c[it] = 0;
-      if (r >= a.n) continue;
-      uint64_t steps = 0;
-      while (e[it].x != key[it] && e[it].x != EMPTY && steps <= a.mask) {
-        s[it] = (s[it] + 1) & a.mask;
-        e[it] = __ldg(a.slots + s[it]);
-        ++steps;
-      }
-      uint32_t cnt = (uint32_t)(e[it].y >> 32);
-      if (e[it].x != key[it] || cnt == 0) continue;
-      uint32_t v = (uint32_t)e[it].y;
-      if (!VERIFY) {
-        c[it] = DUPS ? cnt : 1u;
-      } else if (cnt == 1) {
-        c[it] = rows_equal(a.pcols, a.bcols, a.nkeys, r, v) ? 1u : 0u;
-      } else {
-        uint32_t m = 0;
-        for (uint32_t j = 0; j < cnt; ++j) m += rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v + j]) ? 1u : 0u;
-        c[it] = m;
-      }
-    }
-    // rank matches inside the warp (row order = it-major, lane-minor)
+    // rank matches inside the warp (row order = item-major, lane-minor)
     uint32_t lex[PI];
     uint32_t run = 0;
 #pragma unroll
@@ -350,19 +371,19 @@ __global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
     if (lane == 0) s_wexcl[warp] = run;
     __syncthreads();
     if (warp == 0) {
-      uint32_t v = lane < PW ? s_wexcl[lane] : 0;
-      uint32_t incl = warp_incl_scan32(v);
+      uint32_t wv = lane < PW ? s_wexcl[lane] : 0;
+      uint32_t incl = warp_incl_scan32(wv);
       uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
-      if (lane < PW) s_wexcl[lane] = incl - v;
-      if (lane == 0) {
-        if (EMIT) {
-          unsigned long long ex = tile_lookback(a.tile_status, tile, tile_total, a.err);
+      if (lane < PW) s_wexcl[lane] = incl - wv;
+      if (EMIT) {
+        unsigned long long ex = warp_lookback(a.tile_status, tile, tile_total, a.err);
+        if (lane == 0) {
           s_excl = ex;
           if (tile == a.n_tiles - 1) *a.total = ex + tile_total;
-        } else {
-          if (tile_total) atomicAdd(a.total, (unsigned long long)tile_total);
-          s_excl = 0;
         }
+      } else if (lane == 0) {
+        if (tile_total) atomicAdd(a.total, (unsigned long long)tile_total);
+        s_excl = 0;
       }
     }
     __syncthreads();
@@ -377,15 +398,11 @@ __global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
           atomicOr(a.err, DERR_CAPACITY);
           continue;
         }
-        uint32_t cnt = (uint32_t)(e[it].y >> 32);
-        uint32_t v = (uint32_t)e[it].y;
-        if (!DUPS && !VERIFY) {
-          emit_one(a, pos, r, v);
-        } else if (cnt == 1) {
-          emit_one(a, pos, r, v);
+        if ((!DUPS && !VERIFY) || cand[it] == 1) {
+          emit_one(a, pos, r, v[it]);
         } else {
-          for (uint32_t j = 0; j < cnt; ++j) {
-            uint32_t b = a.dup_rows[v + j];
+          for (uint32_t j = 0; j < cand[it]; ++j) {
+            uint32_t b = a.dup_rows[v[it] + j];
             if (VERIFY && !rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
             emit_one(a, pos++, r, b);
           }
@@ -396,9 +413,108 @@ __global__ void __launch_bounds__(PW * 32) probe_kernel(K keys, ProbeArgs a) {
   }
 }
 
+// ---------------------------------------------------- unique int64 keys ----
+// Two sync-free kernels for the common case (single Int64 key, unique build
+// keys): the probe writes one u32 per probe row (matched build row, or
+// NO_MATCH) and one match count per tile; after an exclusive scan of the tile
+// counts the emit kernel streams those words back and writes the matches at
+// their final positions. Neither kernel waits on another CTA, so the random
+// slot loads of many tiles overlap freely.
+constexpr int QB = 256;            // threads per CTA
+constexpr int QI = 8;              // rows per thread
+constexpr int QT = QB * QI;        // rows per tile (2048)
+constexpr uint32_t NO_MATCH = 0xFFFFFFFFu;
+
+__global__ void __launch_bounds__(QB, 3) probe_rows_kernel(const int64_t* __restrict__ keys, int64_t n,
+                                                          const ulonglong2* __restrict__ slots, int shift,
+                                                          uint64_t mask, uint64_t cap, uint32_t* __restrict__ rowv,
+                                                          uint32_t* __restrict__ tile_cnt) {
+  const int64_t base = (int64_t)blockIdx.x * QT;
+  uint64_t key[QI], s[QI];
+  ulonglong2 e[QI];
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    key[it] = r < n ? (uint64_t)__ldg(keys + r) : EMPTY;
+  }
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    if (r < n) {
+      s[it] = key[it] == EMPTY ? cap : slot_of(key[it], shift);
+      e[it] = __ldg(slots + s[it]);
+    }
+  }
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    if (r >= n) continue;
+    uint64_t steps = 0;
+    while (e[it].x != key[it] && e[it].x != EMPTY && steps <= mask) {
+      s[it] = (s[it] + 1) & mask;
+      e[it] = __ldg(slots + s[it]);
+      ++steps;
+    }
+    bool hit = e[it].x == key[it] && (e[it].y >> 32) != 0;
+    rowv[r] = hit ? (uint32_t)e[it].y : NO_MATCH;
+    cnt += hit ? 1u : 0u;
+  }
+  // CTA total
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+  __shared__ uint32_t wsum[QB / 32];
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < QB / 32; ++w) t += wsum[w];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restrict__ rowv, int64_t n,
+                                                       const uint64_t* __restrict__ tile_off, ProbeArgs a) {
+  __shared__ uint32_t seg[QI][QB / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * QT;
+  uint32_t v[QI], lpos[QI];
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    v[it] = r < n ? __ldg(rowv + r) : NO_MATCH;
+    uint32_t m = __ballot_sync(0xffffffffu, v[it] != NO_MATCH);
+    lpos[it] = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) seg[it][warp] = __popc(m);
+  }
+  __syncthreads();
+  // exclusive offsets of the (item, warp) segments in row order
+  if (warp == 0) {
+    uint32_t x0 = seg[lane >> 3][lane & 7], x1 = seg[(lane + 32) >> 3][(lane + 32) & 7];
+    uint32_t s0 = warp_incl_scan32(x0);
+    uint32_t tot0 = __shfl_sync(0xffffffffu, s0, 31);
+    uint32_t s1 = warp_incl_scan32(x1) + tot0;
+    seg[lane >> 3][lane & 7] = s0 - x0;
+    seg[(lane + 32) >> 3][(lane + 32) & 7] = s1 - x1;
+  }
+  __syncthreads();
+  const uint64_t off = tile_off[blockIdx.x];
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    if (v[it] == NO_MATCH) continue;
+    uint64_t pos = off + seg[it][warp] + lpos[it];
+    if (pos >= a.out_capacity) {
+      atomicOr(a.err, DERR_CAPACITY);
+      continue;
+    }
+    emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
+  }
+}
+
 template <class K, bool EMIT>
 void launch_probe(Ctx& ctx, const JoinTable& t, K keys, ProbeArgs& a, int blocks_per_sm) {
-  int grid = (int)std::min<int64_t>(a.n_tiles, (int64_t)ctx.sm_count * blocks_per_sm);
+  int grid = (int)std::min<int64_t>(a.n_tiles, (int64_t)ctx.sm_count * std::min(blocks_per_sm, 2));
   if (grid < 1) grid = 1;
   bool verify = !t.int64_fast;
   KernelTimer kt(ctx, EMIT ? "probe_kernel" : "probe_count_kernel");
@@ -587,6 +703,34 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     a.g_dst[g] = gathers[g].dst;
   }
   a.out_capacity = (uint64_t)cap;
+  if (t.int64_fast && !t.has_dups) {
+    // unique Int64 keys: probe, scan of tile counts, ordered emit
+    int64_t n = probe.rows, ntiles = ceil_div(n, QT);
+    MemP mrow, mcnt, moff, mtot;
+    uint32_t* rowv = ctx.alloc_t<uint32_t>((size_t)n, mrow);
+    uint32_t* tcnt = ctx.alloc_t<uint32_t>((size_t)ntiles, mcnt);
+    uint64_t* toff = ctx.alloc_t<uint64_t>((size_t)ntiles, moff);
+    uint64_t* dtot = ctx.alloc_t<uint64_t>(1, mtot);
+    a.err = ctx.d_err;
+    {
+      KernelTimer kt(ctx, "probe_rows_kernel");
+      probe_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(static_cast<const int64_t*>(probe.cols[keys[0]]->values),
+                                                                  n, a.slots, a.shift, a.mask, a.cap, rowv, tcnt);
+    }
+    ctx.check_launch("probe_rows_kernel");
+    scan_u32_async(ctx, tcnt, toff, ntiles, dtot);
+    {
+      KernelTimer kt(ctx, "emit_rows_kernel");
+      emit_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(rowv, n, toff, a);
+    }
+    ctx.check_launch("emit_rows_kernel");
+    uint64_t total = 0;
+    PRISM_CUDA(cudaMemcpyAsync(&total, dtot, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    uint32_t derr = ctx.take_device_errors();
+    if (derr & DERR_CAPACITY) fail(PRISM_ERR_INTERNAL, "probe output capacity exceeded");
+    res.matches = (int64_t)total;
+    return res;
+  }
   MemP ms, mc, mt;
   a.tile_status = ctx.alloc_t<unsigned long long>((size_t)a.n_tiles, ms);
   a.tile_counter = ctx.alloc_t<unsigned long long>(1, mc);

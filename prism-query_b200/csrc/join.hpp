@@ -23,7 +23,7 @@ struct JoinTable {
 
 struct JoinTuning {
   double load_factor = 0.5;
-  int probe_blocks_per_sm = 8;
+  int probe_blocks_per_sm = 2;
 };
 
 std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,

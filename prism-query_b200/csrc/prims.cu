@@ -225,6 +225,26 @@ __global__ void scatter_bits_kernel(const uint32_t* idx, int64_t n, uint32_t* wo
 
 }  // namespace
 
+static __global__ void copy_total_kernel(const uint64_t* src, uint64_t* dst) { *dst = *src; }
+
+void scan_u32_async(Ctx& ctx, const uint32_t* in, uint64_t* out, int64_t n, uint64_t* total_dev) {
+  if (n <= 0) {
+    PRISM_CUDA(cudaMemsetAsync(total_dev, 0, 8, ctx.stream));
+    return;
+  }
+  int64_t ntiles = ceil_div(n, ST);
+  MemP ms;
+  uint64_t* sums = ctx.alloc_t<uint64_t>((size_t)ntiles + 1, ms);
+  tile_sum_kernel<<<(unsigned)ntiles, SB, 0, ctx.stream>>>(in, n, sums);
+  ctx.check_launch("tile_sum_kernel");
+  scan_sums_kernel<<<1, SB, 0, ctx.stream>>>(sums, ntiles);
+  ctx.check_launch("scan_sums_kernel");
+  tile_scan_kernel<<<(unsigned)ntiles, SB, 0, ctx.stream>>>(in, n, sums, out);
+  ctx.check_launch("tile_scan_kernel");
+  copy_total_kernel<<<1, 1, 0, ctx.stream>>>(sums + ntiles, total_dev);
+  ctx.check_launch("copy_total_kernel");
+}
+
 uint64_t scan_u32(Ctx& ctx, const uint32_t* in, uint64_t* out, int64_t n) {
   if (n <= 0) return 0;
   int64_t ntiles = ceil_div(n, ST);

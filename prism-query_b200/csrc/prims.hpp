@@ -8,6 +8,8 @@ namespace prism {
 // Exclusive scan of n u32 values into u64 offsets; returns the total
 // (synchronises the stream to read it).
 uint64_t scan_u32(Ctx& ctx, const uint32_t* in, uint64_t* out, int64_t n);
+// Same without a host round trip: the total is written to *total_dev.
+void scan_u32_async(Ctx& ctx, const uint32_t* in, uint64_t* out, int64_t n, uint64_t* total_dev);
 
 // Ordered positions of the set bits (or unset bits, invert = true) of an
 // n-bit bitmap; *count receives their number.

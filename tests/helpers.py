@@ -32,6 +32,19 @@ def assert_batches_equal(got: pa.RecordBatch, ref: pa.RecordBatch, float_cols=()
         else:
             if pa.types.is_dictionary(a.type):
                 assert a.to_pylist() == b.to_pylist(), f"column {i}"
+            elif _is_float(a.type):
+                # bit-exact, with NaN equal to NaN (pyarrow's equals is not)
+                assert a.null_count == b.null_count, f"column {i} null count"
+                va = np.asarray(a.is_valid()) if a.null_count else np.ones(len(a), bool)
+                vb = np.asarray(b.is_valid()) if b.null_count else np.ones(len(b), bool)
+                assert np.array_equal(va, vb), f"column {i} validity"
+                x = a.to_numpy(zero_copy_only=False)[va]
+                y = b.to_numpy(zero_copy_only=False)[vb]
+                same = (x == y) | (np.isnan(x) & np.isnan(y))
+                assert same.all(), f"column {i} ({got.schema.names[i]}) differs at {np.flatnonzero(~same)[:5]}"
+                sx = np.signbit(x[~np.isnan(x)])
+                sy = np.signbit(y[~np.isnan(y)])
+                assert np.array_equal(sx, sy), f"column {i} signed-zero mismatch"
             else:
                 assert a.equals(b), f"column {i} ({got.schema.names[i]}) differs:\n{a}\n{b}"
 

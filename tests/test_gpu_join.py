@@ -25,6 +25,16 @@ def test_reference_known_answers(ctx, name, jt, rows, cols):
 
 @pytest.mark.parametrize("jt", ALL_TYPES)
 def test_all_join_types_small(ctx, jt):
+    if jt == JoinType.Full:
+        # the unmatched probe row (dept 99) puts a null into the non-nullable
+        # build field dept_name: arrow-rs RecordBatch::try_new rejects that
+        # batch in the reference, and both engines report the Arrow error
+        with pytest.raises(oracle.OracleError) as e1:
+            oracle.hash_join(K.join_probe_side(), K.join_build_side(), K.join_config(jt))
+        with pytest.raises(prism_gpu.PrismError) as e2:
+            prism_gpu.hash_join(K.join_probe_side(), K.join_build_side(), K.join_config(jt))
+        assert e1.value.kind == e2.value.kind == "Arrow"
+        return
     out = prism_gpu.hash_join(K.join_probe_side(), K.join_build_side(), K.join_config(jt))
     ref = oracle.hash_join(K.join_probe_side(), K.join_build_side(), K.join_config(jt))
     assert_batches_equal(out, ref)
