@@ -240,7 +240,7 @@ def main():
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("probe_kernel_c2")
+        traffic = json.load(open(tp)).get("probe_phase_c2")
 
     # e2e: host Arrow batches in pinned memory through the C ABI
     e2e = None
