@@ -274,6 +274,28 @@ int prism_hash_table_build(prism_ctx* ctx, const prism_batch* build,
 int prism_hash_table_probe(prism_ctx* ctx, const prism_hash_table* table,
                            const prism_batch* probe, const int32_t* key_cols,
                            int32_t n_keys, prism_batch** out);
+/* Probe that allocates nothing. No counterpart in the reference: it exists
+ * for callers that may not allocate device memory while they run — e.g. a
+ * host engine that reserved its whole device-memory budget up front and owns
+ * every buffer through its own pool, or a plugin whose host forbids driver
+ * allocations mid-query. The caller passes device pointers: `probe_keys`
+ * (n_probe Int64 keys) and the outputs `out_probe_idx` / `out_build_idx`
+ * (UInt32, room for `out_capacity` matches); results equal
+ * prism_hash_table_probe's, in the same order. The table must have a single
+ * Int64 key column. Scratch is a file-scope device array of 1 MiB that every
+ * GPU loading the library keeps until exit; it bounds n_probe to
+ * 268,435,456 rows (larger inputs are rejected with
+ * PRISM_ERR_INVALID_ARGUMENT). The first call on each device looks up that
+ * array's device address (cudaGetSymbolAddress) with the device current; make
+ * that first call before any stream capture. Every call shares the array and
+ * clears the part it uses; calls that overlap on the GPU race. When more
+ * matches exist than out_capacity, nothing past the capacity is written,
+ * *out_matches receives the full count and the call returns
+ * PRISM_ERR_INVALID_ARGUMENT. */
+int prism_hash_table_probe_noalloc(prism_ctx* ctx, const prism_hash_table* table,
+                                   const int64_t* probe_keys, int64_t n_probe,
+                                   uint32_t* out_probe_idx, uint32_t* out_build_idx,
+                                   int64_t out_capacity, int64_t* out_matches);
 int64_t prism_hash_table_num_rows(const prism_hash_table* table);
 int prism_hash_table_has_duplicates(const prism_hash_table* table);
 void prism_hash_table_free(prism_hash_table* table);

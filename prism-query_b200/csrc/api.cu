@@ -13,11 +13,6 @@
 
 using namespace prism;
 
-struct prism_hash_table {
-  prism_ctx* ctx = nullptr;
-  std::unique_ptr<JoinTable> t;
-};
-
 namespace {
 
 thread_local std::string t_err;  // errors before a context exists

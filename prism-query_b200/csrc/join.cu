@@ -752,4 +752,115 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
   return res;
 }
 
+// ------------------------------------------------ allocation-free probe ----
+// For callers that may not allocate device memory while they run: the
+// single-pass probe with its look-back scratch (one status word per
+// 2048-row tile, the tile counter and the match total) in a file-scope
+// device array instead of a per-call allocation.
+namespace {
+
+constexpr int64_t NOALLOC_MAX_TILES = 131072;  // x 2048 rows = 268,435,456 probe rows
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_MAX_TILES + 32];
+
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+// Device address of g_noalloc_scratch on `device`, looked up once per device
+// with that device current. In host code the symbol's name is only a
+// host-side stand-in and must never be passed to a kernel.
+unsigned long long* noalloc_scratch(int device) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= NOALLOC_MAX_DEVICES) fail(PRISM_ERR_INVALID_ARGUMENT, "device index out of range");
+  if (!g_noalloc_addr[device]) {
+    int cur = -1;
+    PRISM_CUDA(cudaGetDevice(&cur));
+    if (cur != device) PRISM_CUDA(cudaSetDevice(device));
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (cur != device) cudaSetDevice(cur);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      fail(PRISM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    }
+    g_noalloc_addr[device] = static_cast<unsigned long long*>(p);
+  }
+  return g_noalloc_addr[device];
+}
+
+}  // namespace
+
 }  // namespace prism
+
+extern "C" int prism_hash_table_probe_noalloc(prism_ctx* c, const prism_hash_table* tab, const int64_t* probe_keys,
+                                              int64_t n_probe, uint32_t* out_probe_idx, uint32_t* out_build_idx,
+                                              int64_t out_capacity, int64_t* out_matches) {
+  using namespace prism;
+  if (!c) return PRISM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(c->impl.mu);
+  try {
+    Ctx& ctx = c->impl;
+    if (!tab || !tab->t || !out_matches) fail(PRISM_ERR_INVALID_ARGUMENT, "null table or out_matches");
+    const JoinTable& t = *tab->t;
+    if (!t.int64_fast)
+      fail(PRISM_ERR_INVALID_ARGUMENT, "the allocation-free probe needs a table with one Int64 key column");
+    if (n_probe < 0 || out_capacity < 0) fail(PRISM_ERR_INVALID_ARGUMENT, "negative size");
+    int64_t n_tiles = ceil_div(n_probe, PT);
+    if (n_tiles > NOALLOC_MAX_TILES)
+      fail(PRISM_ERR_INVALID_ARGUMENT, "n_probe " + std::to_string(n_probe) +
+                                           " exceeds the allocation-free probe's maximum of " +
+                                           std::to_string(NOALLOC_MAX_TILES * PT) + " rows");
+    if (n_probe > 0 && !probe_keys) fail(PRISM_ERR_INVALID_ARGUMENT, "null probe keys");
+    if (out_capacity > 0 && (!out_probe_idx || !out_build_idx)) fail(PRISM_ERR_INVALID_ARGUMENT, "null outputs");
+    *out_matches = 0;
+    if (n_probe == 0 || t.build.rows == 0) return PRISM_OK;
+
+    unsigned long long* scratch = noalloc_scratch(ctx.device);
+    unsigned long long* status = scratch;
+    unsigned long long* counter = scratch + NOALLOC_MAX_TILES;
+    unsigned long long* total = counter + 1;
+    // the array keeps the previous call's contents: clear what this call uses
+    PRISM_CUDA(cudaMemsetAsync(status, 0, (size_t)n_tiles * 8, ctx.stream));
+    PRISM_CUDA(cudaMemsetAsync(counter, 0, 16, ctx.stream));
+
+    ProbeArgs a{};
+    a.n = n_probe;
+    a.slots = static_cast<const ulonglong2*>(t.slots->ptr);
+    a.shift = 64 - t.log2cap;
+    a.mask = t.capacity - 1;
+    a.cap = t.capacity;
+    a.dup_rows = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+    a.nkeys = 1;
+    a.out_probe = out_probe_idx;
+    a.out_build = out_build_idx;
+    a.ngather = 0;
+    a.out_capacity = (uint64_t)out_capacity;
+    a.tile_status = status;
+    a.tile_counter = counter;
+    a.n_tiles = n_tiles;
+    a.total = total;
+    a.err = ctx.d_err;
+    int grid = (int)std::min<int64_t>(n_tiles, (int64_t)ctx.sm_count * 2);
+    if (t.has_dups)
+      probe_kernel<KeysFast, true, false, true><<<grid, PW * 32, 0, ctx.stream>>>(KeysFast{probe_keys}, a);
+    else
+      probe_kernel<KeysFast, false, false, true><<<grid, PW * 32, 0, ctx.stream>>>(KeysFast{probe_keys}, a);
+    ctx.check_launch("probe_kernel(noalloc)");
+    unsigned long long tot = 0;
+    PRISM_CUDA(cudaMemcpyAsync(&tot, total, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    uint32_t derr = ctx.take_device_errors();
+    if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+    *out_matches = (int64_t)tot;
+    if (derr & DERR_CAPACITY)
+      fail(PRISM_ERR_INVALID_ARGUMENT, "output capacity " + std::to_string(out_capacity) + " is smaller than the " +
+                                           std::to_string(tot) + " matches");
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    c->impl.last_error = f.msg;
+    cudaGetLastError();
+    return f.code;
+  } catch (const std::exception& e) {
+    c->impl.last_error = e.what();
+    return PRISM_ERR_INTERNAL;
+  }
+}

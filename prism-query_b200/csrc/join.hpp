@@ -61,3 +61,9 @@ int64_t match_upper_bound(const JoinTable& t, int64_t probe_rows);
 void check_join_keys(const Batch& probe, const std::vector<int>& pk, const Batch& build, const std::vector<int>& bk);
 
 }  // namespace prism
+
+// The opaque resident-table handle of the C ABI.
+struct prism_hash_table {
+  prism_ctx* ctx = nullptr;
+  std::unique_ptr<prism::JoinTable> t;
+};
