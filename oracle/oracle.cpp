@@ -250,7 +250,7 @@ ColP take_col(const Col& c, const std::vector<int64_t>& idx, const std::string& 
 ColP filter_col(const Col& c, const std::vector<uint8_t>& keep) {
   Builder b = builder_like(c, c.name, c.nullable);
   for (int64_t i = 0; i < c.len; ++i)
-    if (keep[i]) b.push_from(c, i);
+    if (keep[i]) b.push_slot(c, i);
   return b.finish();
 }
 
@@ -1160,16 +1160,20 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
           ob.scale = so;
           __int128 fl = pow10_i128(so - sl), fr = pow10_i128(so - sr);
           for (int64_t i = 0; i < R; ++i) {
-            if (l->null_at(i) || r->null_at(i)) { ob.push_null(); continue; }
+            // null rows carry the wrapped (mod 2^128) result of the raw
+            // slots and never raise
+            bool valid = !l->null_at(i) && !r->null_at(i);
             __int128 a = exact_val(*l, i), c = exact_val(*r, i), out;
             bool ovf = false;
             if (nd.op == PRISM_EXPR_MUL) ovf = __builtin_mul_overflow(a, c, &out);
             else {
               __int128 aa, cc;
-              ovf = __builtin_mul_overflow(a, fl, &aa) || __builtin_mul_overflow(c, fr, &cc);
-              if (!ovf) ovf = nd.op == PRISM_EXPR_ADD ? __builtin_add_overflow(aa, cc, &out)
-                                                      : __builtin_sub_overflow(aa, cc, &out);
+              ovf = __builtin_mul_overflow(a, fl, &aa);
+              ovf = __builtin_mul_overflow(c, fr, &cc) || ovf;
+              ovf = (nd.op == PRISM_EXPR_ADD ? __builtin_add_overflow(aa, cc, &out)
+                                             : __builtin_sub_overflow(aa, cc, &out)) || ovf;
             }
+            if (!valid) { ob.push_raw_null(&out, 16); continue; }
             if (ovf) fail(PRISM_ERR_EXECUTION, "decimal overflow in exact arithmetic");
             ob.push_i128(out);
           }
@@ -1179,8 +1183,9 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
         // filter_project.rs:233-247: cast both to Float64, IEEE arithmetic
         F64Col lv = cast_f64(*l, "arithmetic"), rv = cast_f64(*r, "arithmetic");
         Builder ob(T_F64, "", true);
+        // arrow-arith applies float ops to every slot (binary), so a null
+        // row holds the result of its raw operand slots
         for (int64_t i = 0; i < R; ++i) {
-          if (!lv.valid[i] || !rv.valid[i]) { ob.push_null(); continue; }
           double a = lv.v[i], c = rv.v[i], o = 0;
           switch (nd.op) {
             case PRISM_EXPR_ADD: o = a + c; break;
@@ -1188,7 +1193,8 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
             case PRISM_EXPR_MUL: o = a * c; break;
             case PRISM_EXPR_DIV: o = a / c; break;
           }
-          ob.push_f64(o);
+          if (!lv.valid[i] || !rv.valid[i]) ob.push_raw_null(&o, 8);
+          else ob.push_f64(o);
         }
         st.push_back(ob.finish());
         break;
@@ -1201,8 +1207,9 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
           ob.prec = 38;
           ob.scale = x->ty == T_DEC128 ? x->scale : 0;
           for (int64_t i = 0; i < R; ++i) {
-            if (x->null_at(i)) ob.push_null();
-            else ob.push_i128(-exact_val(*x, i));
+            __int128 v = (__int128)((unsigned __int128)0 - (unsigned __int128)exact_val(*x, i));
+            if (x->null_at(i)) ob.push_raw_null(&v, 16);
+            else ob.push_i128(v);
           }
           st.push_back(ob.finish());
           break;
@@ -1210,8 +1217,9 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
         F64Col v = cast_f64(*x, "negation");
         Builder ob(T_F64, "", true);
         for (int64_t i = 0; i < R; ++i) {
-          if (!v.valid[i]) ob.push_null();
-          else ob.push_f64(-v.v[i]);
+          double o = -v.v[i];
+          if (!v.valid[i]) ob.push_raw_null(&o, 8);
+          else ob.push_f64(o);
         }
         st.push_back(ob.finish());
         break;
@@ -1243,8 +1251,8 @@ ColP eval_expr_range(const Batch& b, const prism_expr& e, int begin, int end, in
           ColP br = cast_to(branches[ci], target);
           Builder zb = builder_like(target, "", true);
           for (int64_t i = 0; i < R; ++i) {
-            if (m.valid[i] && m.val[i]) zb.push_from(*br, i);
-            else zb.push_from(*result, i);
+            if (m.valid[i] && m.val[i]) zb.push_slot(*br, i);
+            else zb.push_slot(*result, i);
           }
           result = zb.finish();
         }

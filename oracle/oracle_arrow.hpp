@@ -161,6 +161,12 @@ struct Builder {
     const uint8_t* b = static_cast<const uint8_t*>(p);
     raw.insert(raw.end(), b, b + w);
   }
+  // a null row whose slot holds `w` raw bytes (arrow compute kernels fill
+  // null slots with the operation applied to the raw operand slots)
+  void push_raw_null(const void* p, int64_t w) {
+    mark(false);
+    push_raw(p, w);
+  }
   void push_null() {
     mark(false);
     Ty t = ty == T_DICT ? idx_ty : ty;
@@ -196,6 +202,28 @@ struct Builder {
     data.insert(data.end(), s.begin(), s.end());
     if ((int64_t)data.size() > INT32_MAX) fail(PRISM_ERR_ARROW, "utf8 column exceeds 2 GiB");
     offs.push_back((int32_t)data.size());
+  }
+  // copy row i of c keeping the raw slot of a null row, as arrow-select's
+  // filter kernels copy the selected values and bytes regardless of
+  // validity (filter_primitive / filter_bytes, arrow 57)
+  void push_slot(const Col& c, int64_t i) {
+    if (!c.null_at(i)) { push_from(c, i); return; }
+    Ty t = c.ty == T_DICT ? c.idx_ty : c.ty;
+    int64_t w = width_of(t);
+    if (t == T_UTF8) {
+      mark(false);
+      std::string_view v = c.sval(i);
+      data.insert(data.end(), v.begin(), v.end());
+      offs.push_back((int32_t)data.size());
+    } else if (t == T_BOOL) {
+      mark(false);
+      raw.push_back((uint8_t)(c.ival(i) ? 1 : 0));
+    } else if (w > 0) {
+      mark(false);
+      push_raw(c.vals + w * (c.off + i), w);
+    } else {
+      push_null();
+    }
   }
   // copy row i of c (same type family) into this builder
   void push_from(const Col& c, int64_t i) {

@@ -745,7 +745,9 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       fail(PRISM_ERR_UNSUPPORTED_AGGREGATION, "unknown aggregate function");
   if (cfg.n_aggs > 32) fail(PRISM_ERR_INVALID_ARGUMENT, "at most 32 aggregates per call");
   if (cfg.n_group_by > MAX_GCOLS) fail(PRISM_ERR_INVALID_ARGUMENT, "at most 8 group-by columns");
-  const bool exact = fused && arith_mode == PRISM_ARITH_EXACT;
+  // EXACT also covers the materialized fallback of the fused call (fused =
+  // false with the caller's mode); plain hash_aggregate passes F64
+  const bool exact = arith_mode == PRISM_ARITH_EXACT;
   int64_t total_rows = 0;
   for (auto* b : batches) total_rows += b->rows;
   bool any_rows = total_rows > 0;
