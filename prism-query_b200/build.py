@@ -18,7 +18,12 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+# --fmad=false: Float64 arithmetic rounds after every operation (no FMA
+# contraction), as the reference computes it
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "--fmad=false",
+         "-I", INCLUDE, "-I", CSRC]
+# device headers embedded into the library for run-time compiled kernels
+JIT_HEADERS = ["common.cuh", "eval.cuh", "agg_device.cuh"]
 
 
 def sources():
@@ -43,6 +48,33 @@ def compile_one(src: str, force: bool, extra) -> str:
     return obj
 
 
+def jit_headers_object(force: bool) -> str:
+    """Embeds JIT_HEADERS as C strings (kJitHeaderNames / kJitHeaderTexts)."""
+    src = os.path.join(BUILD, "jit_headers.cpp")
+    obj = os.path.join(BUILD, "jit_headers.o")
+    hs = [os.path.join(CSRC, h) for h in JIT_HEADERS]
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(h) for h in hs):
+        return obj
+    delim = "PRISMHDR"
+    parts = []
+    for h in hs:
+        text = open(h).read()
+        if f"){delim}\"" in text:
+            raise RuntimeError(f"{h} contains the raw-string delimiter")
+        parts.append(f'R"{delim}({text}){delim}"')
+    names = ", ".join(f'"{h}"' for h in JIT_HEADERS)
+    with open(src, "w") as f:
+        f.write("// generated by build.py: device headers for run-time compiled kernels\n")
+        f.write("namespace prism {\n")
+        f.write(f"extern const int kJitHeaderCount = {len(hs)};\n")
+        f.write(f"extern const char* const kJitHeaderNames[] = {{{names}}};\n")
+        f.write("extern const char* const kJitHeaderTexts[] = {\n" + ",\n".join(parts) + "};\n}\n")
+    r = subprocess.run(["g++", "-O1", "-fPIC", "-c", src, "-o", obj], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"embedding device headers failed:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
 def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     extra = ["-DPRISM_DEBUG=1"] if debug else []
@@ -50,8 +82,9 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
         extra += ["-Xptxas", "-v"]
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         objs = list(ex.map(lambda s: compile_one(s, force, extra), sources()))
+    objs.append(jit_headers_object(force))
     if force or not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", *objs, "-o", OUT, "-lpthread"]
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", *objs, "-o", OUT, "-lpthread", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -25,6 +25,8 @@
 #include <map>
 
 #include "agg.hpp"
+#include "agg_device.cuh"
+#include "jit.hpp"
 #include "prims.hpp"
 
 namespace prism {
@@ -33,138 +35,6 @@ namespace {
 
 constexpr uint64_t GEMPTY = 0xFFFFFFFFFFFFFFFFULL;
 constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
-constexpr int MAX_SRC = 8;
-constexpr int MAX_OPS = 16;
-constexpr int MAX_W = 64;
-constexpr int MAX_GCOLS = 8;
-constexpr int LIMBS = 6;  // f64 window: 6 x 32 bits
-constexpr int WIDE_LIMBS = 68;  // 2^-1074 .. 2^1102
-constexpr int WIDE_LO = -1074;
-
-enum SrcKind : int32_t { S_COL_F64 = 0, S_COL_INT, S_COL_I128, S_EXPR_F64, S_EXPR_I128, S_VALID };
-enum OpKind : int32_t { O_SUM_F64 = 0, O_SUM_INT, O_SUM_DEC, O_MIN, O_MAX, O_NONNULL, O_DISTINCT };
-enum WordKind : int32_t { W_ADD = 0, W_MIN, W_MAX, W_OR };
-
-struct Src {
-  int32_t kind;
-  int32_t col;          // program column slot
-  int32_t begin, end;   // expression nodes
-};
-struct Op {
-  int32_t kind;
-  int32_t src;
-  int32_t word;
-  int32_t lo_exp;       // O_SUM_F64 window bottom exponent
-  int32_t distinct;     // O_DISTINCT: table index
-  int32_t pad;
-};
-
-struct DistinctTable {
-  unsigned long long* slots;  // pairs (a, b)
-  uint64_t mask;
-};
-
-struct AggArgs {
-  int64_t n;
-  uint64_t row_base;
-  const PNode* pn;
-  const ENode* en;
-  const PRange* cl;
-  const DCol* cols;
-  int32_t has_filter;
-  PRange filter;
-  int32_t n_src;
-  Src src[MAX_SRC];
-  int32_t n_ops;
-  Op op[MAX_OPS];
-  int32_t W;
-  unsigned long long winit[MAX_W];
-  int32_t wkind[MAX_W];
-  int32_t skip_nulls;
-  int32_t count_rows;       // maintain word 0 (grouped path)
-  // group identity
-  int32_t n_gcols;
-  int32_t gcol[MAX_GCOLS];
-  int32_t dense;
-  int64_t G;
-  int64_t dstride[MAX_GCOLS];
-  int64_t dnull[MAX_GCOLS];
-  // shared-memory table geometry (hash mode)
-  int32_t ss_log2;
-  int32_t sd;
-  int32_t use_smem;
-  // global table
-  unsigned long long* gkeys;
-  unsigned long long* gfirst;
-  unsigned long long* gacc;
-  uint64_t gmask;
-  int32_t gshift;
-  uint64_t gcap;
-  DistinctTable dt[4];
-  uint32_t* err;
-  int* maxexp;   // per op (O_SUM_F64 overflow diagnosis)
-  // wide mode: Float64 sums over the whole double range (68 limbs from
-  // 2^-1074), global accumulators only; used when a value overflowed the
-  // 192-bit window
-  int32_t wide;
-  int32_t n_wide;
-  unsigned long long* gwide;  // [slot][n_wide][WIDE_LIMBS + 1]
-};
-
-// ------------------------------------------------------------ accumulate --
-
-__device__ __forceinline__ void atom_add(unsigned long long* p, unsigned long long v) {
-  if (v) atomicAdd(p, v);
-}
-
-// Adds v to a 6-limb fixed-point accumulator whose bit 0 weighs 2^lo_exp
-// (acc[6] collects NaN/+inf/-inf flags). Bits below the window are dropped.
-__device__ void add_f64(unsigned long long* acc, double v, int lo_exp, uint32_t* err, int* maxexp, int nl = LIMBS) {
-  uint64_t u = (uint64_t)__double_as_longlong(v);
-  int be = (int)((u >> 52) & 0x7ff);
-  uint64_t m = u & 0xFFFFFFFFFFFFFULL;
-  if (be == 0x7ff) {
-    atomicOr(acc + nl, m ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
-    return;
-  }
-  if (be) m |= 1ULL << 52;
-  else be = 1;
-  if (!m) return;
-  int pos = be - 1075 - lo_exp;
-  if (pos < 0) {
-    if (pos <= -64) return;
-    m >>= -pos;
-    pos = 0;
-    if (!m) return;
-  }
-  int k = pos >> 5, sh = pos & 31;
-  unsigned __int128 x = (unsigned __int128)m << sh;
-  uint32_t p0 = (uint32_t)x, p1 = (uint32_t)(x >> 32), p2 = (uint32_t)(x >> 64);
-  if (k >= nl || (k + 1 >= nl && p1) || (k + 2 >= nl && p2)) {
-    atomicOr(err, DERR_OVERFLOW);
-    atomicMax(maxexp, be);
-    return;
-  }
-  bool neg = u >> 63;
-  unsigned long long q0 = neg ? (unsigned long long)(-(long long)p0) : p0;
-  unsigned long long q1 = neg ? (unsigned long long)(-(long long)p1) : p1;
-  unsigned long long q2 = neg ? (unsigned long long)(-(long long)p2) : p2;
-  atom_add(acc + k, q0);
-  if (k + 1 < nl) atom_add(acc + k + 1, q1);
-  if (k + 2 < nl) atom_add(acc + k + 2, q2);
-}
-
-__device__ __forceinline__ void add_i128_limbs(unsigned long long* acc, __int128 v, int n_limbs) {
-  // n_limbs 32-bit limbs, the top one signed
-  for (int q = 0; q < n_limbs; ++q) {
-    long long part;
-    if (q == n_limbs - 1) part = (long long)(v >> (32 * q));
-    else part = (long long)(uint32_t)(v >> (32 * q));
-    atom_add(acc + q, (unsigned long long)part);
-  }
-}
-
-__device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 struct RowVals {
   double f[MAX_SRC];
@@ -635,6 +505,10 @@ __global__ void distinct_count_kernel(AggArgs a, int table, unsigned long long* 
 // ---------------------------------------------------------------- host ----
 namespace {
 
+// register budget of a generated small-groups kernel's per-thread
+// accumulators: two words per op and group, four with a Float64 SUM present
+bool tiny_fits_registers(int G, int nops, bool f64) { return G * nops * (f64 ? 4 : 2) + G <= 136; }
+
 bool int_like(int t) {
   return t == TY_I8 || t == TY_I16 || t == TY_I32 || t == TY_I64 || t == TY_U8 || t == TY_U16 || t == TY_U32 ||
          t == TY_BOOL;
@@ -1020,6 +894,12 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   A.use_smem = smem > 0 ? 1 : 0;
   PRISM_CUDA(cudaFuncSetAttribute(agg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
 
+  // few dense groups: a generated kernel with per-thread register
+  // accumulators (tiny_body), sized to the exact group and op counts
+  bool any_f64 = false;
+  for (int j = 0; j < A.n_ops; ++j) any_f64 |= A.op[j].kind == O_SUM_F64;
+  bool tiny = dense && G <= 8 && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 &&
+              tiny_fits_registers((int)G, A.n_ops, any_f64) && jit_enabled();
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
   for (int attempt = 0; attempt < 40; ++attempt) {
@@ -1095,7 +975,38 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       a.cl = pg.d_clauses;
       a.cols = pg.d_cols;
       int grid = (int)std::min<int64_t>(ceil_div(b.rows, block), (int64_t)ctx.sm_count * std::max(1, tune.blocks_per_sm));
-      {
+      const void* jk = nullptr;
+      if (tiny) {
+        std::string src = jit_tiny_agg_source(pg, b, a, (int)G, any_f64);
+        if (!src.empty()) jk = jit_get(src, "prism_tiny_agg");
+      }
+      if (jk) {
+        // stage every program column through shared memory when all are
+        // fixed width, null-free and 16-byte aligned
+        a.n_cols = (int)pg.cols.size();
+        a.n_stage = 0;
+        bool stage_ok = a.n_cols <= TINY_MAX_COLS;
+        int off = 0;
+        for (int k = 0; stage_ok && k < a.n_cols; ++k) {
+          const Column& c = *b.cols[pg.cols[k]];
+          int w = width_of(c.type == TY_DICT ? c.index_type : c.type);
+          if (w == 0 || c.validity || (reinterpret_cast<uintptr_t>(c.values) & 15)) stage_ok = false;
+          a.stage_w[k] = w;
+          a.stage_off[k] = off;
+          off += (TINY_T * w + 15) & ~15;
+        }
+        size_t tsmem = 0;
+        if (stage_ok && (size_t)off * TINY_STAGES <= smem_budget) {
+          a.n_stage = a.n_cols;
+          a.stage_bytes = off;
+          tsmem = (size_t)off * TINY_STAGES;
+        }
+        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, TINY_T), (int64_t)ctx.sm_count);
+        PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+        void* params[] = {&a};
+        KernelTimer kt(ctx, "agg_tiny_jit");
+        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, tsmem, ctx.stream));
+      } else {
         KernelTimer kt(ctx, "agg_kernel");
         agg_kernel<<<grid, block, smem, ctx.stream>>>(a);
       }
@@ -1119,6 +1030,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         if (A.op[j].kind == O_SUM_F64) A.op[j].distinct = A.n_wide++;
       A.use_smem = 0;
       smem = 0;
+      tiny = false;
       continue;
     }
     if (derr & DERR_RANGE) fail(PRISM_ERR_EXECUTION, "decimal overflow in exact arithmetic");

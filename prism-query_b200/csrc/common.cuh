@@ -1,8 +1,21 @@
 // common.cuh — shared device types and helpers of the B200 engine.
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// compiled by NVRTC for per-query kernels: no system headers (LP64 types)
+typedef signed char int8_t;
+typedef short int16_t;
+typedef int int32_t;
+typedef long int64_t;
+typedef unsigned char uint8_t;
+typedef unsigned short uint16_t;
+typedef unsigned int uint32_t;
+typedef unsigned long uint64_t;
+typedef unsigned long uintptr_t;
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 namespace prism {
 
@@ -214,6 +227,8 @@ enum DevErr : uint32_t {
   DERR_CAPACITY = 16,
 };
 
+#ifndef __CUDACC_RTC__
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+#endif
 
 }  // namespace prism

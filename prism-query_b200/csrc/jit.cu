@@ -1,0 +1,585 @@
+// jit.cu — run-time generation and NVRTC compilation of per-query kernels.
+//
+// Generated code mirrors the interpreters of eval.cuh node for node:
+//   predicates  eval_pred  (native/prism-executor/src/filter_project.rs:65-123, 346-404)
+//   expressions eval_expr  (filter_project.rs:216-294)
+// with the column types, null-freedom and program shape fixed at generation
+// time. Literal values are read from the device programs once per thread
+// (E::load), so queries that differ only in literals share one compiled
+// kernel. NVRTC is loaded with dlopen on first use; kernels are loaded
+// through the runtime's library API (cudaLibraryLoadData).
+#include "jit.hpp"
+
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <sstream>
+#include <unordered_map>
+#include <vector>
+
+#include "agg_device.cuh"
+#include "plan.hpp"
+
+namespace prism {
+
+// embedded device headers (generated by build.py from csrc/)
+extern const int kJitHeaderCount;
+extern const char* const kJitHeaderNames[];
+extern const char* const kJitHeaderTexts[];
+
+namespace {
+
+struct Nvrtc {
+  decltype(&nvrtcCreateProgram) create = nullptr;
+  decltype(&nvrtcCompileProgram) compile = nullptr;
+  decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+  decltype(&nvrtcGetProgramLog) log = nullptr;
+  decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+  decltype(&nvrtcGetCUBIN) cubin = nullptr;
+  decltype(&nvrtcDestroyProgram) destroy = nullptr;
+  bool ok = false;
+};
+
+Nvrtc load_nvrtc() {
+  Nvrtc n;
+  const char* env = std::getenv("PRISM_JIT");
+  if (env && std::strcmp(env, "0") == 0) return n;
+  void* h = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+  if (!h) h = dlopen("/usr/local/cuda/lib64/libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+  if (!h) return n;
+  n.create = reinterpret_cast<decltype(n.create)>(dlsym(h, "nvrtcCreateProgram"));
+  n.compile = reinterpret_cast<decltype(n.compile)>(dlsym(h, "nvrtcCompileProgram"));
+  n.log_size = reinterpret_cast<decltype(n.log_size)>(dlsym(h, "nvrtcGetProgramLogSize"));
+  n.log = reinterpret_cast<decltype(n.log)>(dlsym(h, "nvrtcGetProgramLog"));
+  n.cubin_size = reinterpret_cast<decltype(n.cubin_size)>(dlsym(h, "nvrtcGetCUBINSize"));
+  n.cubin = reinterpret_cast<decltype(n.cubin)>(dlsym(h, "nvrtcGetCUBIN"));
+  n.destroy = reinterpret_cast<decltype(n.destroy)>(dlsym(h, "nvrtcDestroyProgram"));
+  n.ok = n.create && n.compile && n.log_size && n.log && n.cubin_size && n.cubin && n.destroy;
+  return n;
+}
+
+Nvrtc& nvrtc() {
+  static Nvrtc n = load_nvrtc();
+  return n;
+}
+
+struct Entry {
+  cudaLibrary_t lib = nullptr;
+  std::unordered_map<std::string, cudaKernel_t> kernels;
+};
+
+std::mutex g_mu;
+std::unordered_map<std::string, Entry> g_cache;
+int64_t g_compiles = 0;
+double g_compile_ms = 0;
+
+// ------------------------------------------------------------ generator --
+
+const char* cmp_op(int c) {
+  switch (c) {
+    case C_EQ: return "==";
+    case C_NE: return "!=";
+    case C_LT: return "<";
+    case C_LE: return "<=";
+    case C_GT: return ">";
+    default: return ">=";
+  }
+}
+
+// Magnitude bounds of 128-bit values (exact, saturating): an add, subtract
+// or multiply whose operand bounds keep |result| <= 2^127 - 1 cannot
+// overflow and needs no check.
+struct Mag {
+  unsigned __int128 m = 0;
+  bool unknown = true;
+};
+const unsigned __int128 I128_MAX = ((unsigned __int128)1 << 127) - 1;
+
+Mag mag_of(unsigned __int128 m) {
+  Mag r;
+  r.m = m;
+  r.unknown = false;
+  return r;
+}
+
+// |value| bound of a column read by dcol_i128
+Mag type_mag(int t) {
+  switch (t) {
+    case TY_BOOL: return mag_of(1);
+    case TY_I8: return mag_of(128);
+    case TY_U8: return mag_of(255);
+    case TY_I16: return mag_of(1 << 15);
+    case TY_U16: return mag_of(65535);
+    case TY_I32: case TY_DATE32: return mag_of((unsigned __int128)1 << 31);
+    case TY_U32: return mag_of(((unsigned __int128)1 << 32) - 1);
+    case TY_I64: return mag_of((unsigned __int128)1 << 63);
+    case TY_U64: return mag_of(((unsigned __int128)1 << 64) - 1);
+    default: return Mag{};
+  }
+}
+
+Mag mag_add(Mag a, Mag b) {
+  if (a.unknown || b.unknown) return Mag{};
+  unsigned __int128 s = a.m + b.m;
+  if (s < a.m) return Mag{};
+  return mag_of(s);
+}
+
+Mag mag_mul(Mag a, Mag b) {
+  if ((!a.unknown && a.m == 0) || (!b.unknown && b.m == 0)) return mag_of(0);
+  if (a.unknown || b.unknown) return Mag{};
+  if (a.m > ~(unsigned __int128)0 / b.m) return Mag{};
+  return mag_of(a.m * b.m);
+}
+
+Mag mag_max(Mag a, Mag b) {
+  if (a.unknown || b.unknown) return Mag{};
+  return mag_of(a.m > b.m ? a.m : b.m);
+}
+
+bool mag_fits(Mag a) { return !a.unknown && a.m <= I128_MAX; }
+
+std::string hex64(uint64_t u) {
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "0x%016llxULL", (unsigned long long)u);
+  return buf;
+}
+
+struct Gen {
+  const Program& pg;
+  const Batch& b;
+  std::ostringstream consts;  // Consts fields
+  std::ostringstream load;    // E::load statements
+  std::unordered_map<std::string, bool> have;
+  std::ostringstream out;     // current function body
+  int id = 0;
+  bool ok = true;
+
+  Gen(const Program& p, const Batch& bb) : pg(p), b(bb) {}
+
+  std::string fresh(const char* p) { return p + std::to_string(id++); }
+
+  void konst(const std::string& decl_type, const std::string& name, const std::string& init) {
+    if (have.count(name)) return;
+    have[name] = true;
+    consts << "    " << decl_type << " " << name << ";\n";
+    load << "    K." << name << " = " << init << ";\n";
+  }
+
+  // typed local views of every program column (the optimizer drops unused
+  // ones): a constant type folds the type switches of the dcol_* readers,
+  // and a null validity pointer folds dcol_valid to true
+  void declare_cols() {
+    for (size_t s = 0; s < pg.cols.size(); ++s) {
+      const Column& c = *b.cols[pg.cols[s]];
+      out << "    DCol c" << s << " = cols[" << s << "];\n";
+      out << "    c" << s << ".type = " << c.type << "; c" << s << ".index_type = " << c.index_type << "; c" << s
+          << ".scale = " << c.scale << ";";
+      if (!c.validity) out << " c" << s << ".validity = nullptr;";
+      out << "\n";
+    }
+  }
+
+  std::string col(int slot) {
+    if (slot < 0 || slot >= (int)pg.cols.size()) {
+      ok = false;
+      return "c0";
+    }
+    return "c" + std::to_string(slot);
+  }
+
+  // predicate nodes [begin, begin + len): emits statements, returns the
+  // names of the value bit and the validity bit
+  std::pair<std::string, std::string> pred(int begin, int len) {
+    std::vector<std::pair<std::string, std::string>> st;
+    const std::pair<std::string, std::string> bad{"false", "false"};
+    for (int k = begin; k < begin + len; ++k) {
+      const PNode& nd = pg.pnodes[k];
+      std::string v = fresh("pv"), a = fresh("pa"), K = std::to_string(k);
+      switch (nd.op) {
+        case P_LIT:
+          konst("bool", "pl" + K, "a.pn[" + K + "].i != 0");
+          out << "    bool " << v << " = K.pl" << K << ", " << a << " = true;\n";
+          break;
+        case P_CMP_INT: {
+          std::string c = col(nd.col);
+          konst("int64_t", "pi" + K, "a.pn[" + K + "].i");
+          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
+          out << "    bool " << v << " = dcol_ival(" << c << ", idx) " << cmp_op(nd.cmp) << " K.pi" << K << ";\n";
+          break;
+        }
+        case P_CMP_F64: {
+          std::string c = col(nd.col);
+          konst("int64_t", "pf" + K, "total_key(a.pn[" + K + "].f)");
+          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
+          out << "    bool " << v << " = total_key(static_cast<const double*>(" << c << ".values)[idx]) "
+              << cmp_op(nd.cmp) << " K.pf" << K << ";\n";
+          break;
+        }
+        case P_CMP_STR: case P_LIKE: {
+          std::string c = col(nd.col);
+          konst("const uint8_t*", "ps" + K, "a.pn[" + K + "].s");
+          konst("int32_t", "pn" + K, "a.pn[" + K + "].slen");
+          std::string p = fresh("sp"), n = fresh("sn");
+          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
+          out << "    const uint8_t* " << p << "; int32_t " << n << "; dcol_str(" << c << ", idx, " << p << ", " << n
+              << ");\n";
+          if (nd.op == P_CMP_STR)
+            out << "    bool " << v << " = bytes_cmp(" << p << ", " << n << ", K.ps" << K << ", K.pn" << K << ") "
+                << cmp_op(nd.cmp) << " 0;\n";
+          else
+            out << "    bool " << v << " = like_match(" << p << ", " << n << ", K.ps" << K << ", K.pn" << K << ", "
+                << (nd.cmp != 0 ? "true" : "false") << ");\n";
+          break;
+        }
+        case P_IS_NULL: case P_IS_NOT_NULL: {
+          std::string c = col(nd.col);
+          out << "    bool " << v << " = " << (nd.op == P_IS_NULL ? "!" : "") << "dcol_valid(" << c << ", idx), " << a
+              << " = true;\n";
+          break;
+        }
+        case P_AND: case P_OR: {
+          if (st.size() < 2) { ok = false; return bad; }
+          auto r = st.back(); st.pop_back();
+          auto l = st.back(); st.pop_back();
+          out << "    bool " << v << " = " << l.first << (nd.op == P_AND ? " && " : " || ") << r.first << ", " << a
+              << " = " << l.second << " && " << r.second << ";\n";
+          break;
+        }
+        case P_NOT: {
+          if (st.empty()) { ok = false; return bad; }
+          auto x = st.back(); st.pop_back();
+          out << "    bool " << v << " = !" << x.first << ", " << a << " = " << x.second << ";\n";
+          break;
+        }
+        default:
+          ok = false;
+          return bad;
+      }
+      st.push_back({v, a});
+    }
+    if (st.size() != 1) { ok = false; return bad; }
+    return st.back();
+  }
+
+  struct EV {
+    std::string n;
+    Mag mag;  // bound of |n.i|
+  };
+
+  // expression nodes [begin, end): emits statements, returns the Val
+  // variable; `ovf` names the overflow flag of the enclosing scope
+  std::string expr(int begin, int end, const std::string& ovf) {
+    std::vector<EV> st;
+    for (int k = begin; k < end; ++k) {
+      const ENode& nd = pg.enodes[k];
+      std::string n = fresh("e"), K = std::to_string(k);
+      auto pop = [&]() -> EV {
+        if (st.empty()) { ok = false; return EV{"e_bad", Mag{}}; }
+        EV x = st.back();
+        st.pop_back();
+        return x;
+      };
+      switch (nd.op) {
+        case E_COL_F64: {
+          std::string c = col(nd.col);
+          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = dcol_fval(" << c << ", idx); " << n
+              << ".valid = dcol_valid(" << c << ", idx);\n";
+          st.push_back({n, Mag{}});
+          break;
+        }
+        case E_COL_I128: {
+          std::string c = col(nd.col);
+          const Column& cc = *b.cols[pg.cols[std::max(0, std::min(nd.col, (int)pg.cols.size() - 1))]];
+          int t = cc.type == TY_DICT ? cc.index_type : cc.type;
+          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = dcol_i128(" << c << ", idx); " << n
+              << ".valid = dcol_valid(" << c << ", idx);\n";
+          st.push_back({n, type_mag(t)});
+          break;
+        }
+        case E_LIT_F64:
+          konst("double", "ef" + K, "a.en[" + K + "].f");
+          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = K.ef" << K << "; " << n << ".valid = true;\n";
+          st.push_back({n, Mag{}});
+          break;
+        case E_LIT_I128: {
+          // the bound used is the literal's power-of-two ceiling, which the
+          // source records: literals of one size class share a kernel
+          __int128 v = (__int128)(((unsigned __int128)(uint64_t)nd.hi << 64) | (uint64_t)nd.lo);
+          unsigned __int128 m = v < 0 ? (unsigned __int128)0 - (unsigned __int128)v : (unsigned __int128)v;
+          int bits = 0;
+          while (bits < 127 && ((unsigned __int128)1 << bits) < m) ++bits;
+          konst("__int128", "ei" + K,
+                "(__int128)(((unsigned __int128)(uint64_t)a.en[" + K + "].hi << 64) | (uint64_t)a.en[" + K + "].lo)");
+          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = K.ei" << K << "; " << n
+              << ".valid = true;  // |literal| <= 2^" << bits << "\n";
+          st.push_back({n, mag_of((unsigned __int128)1 << bits)});
+          break;
+        }
+        case E_ADD_F: case E_SUB_F: case E_MUL_F: case E_DIV_F: {
+          EV r = pop(), l = pop();
+          const char* op = nd.op == E_ADD_F ? "+" : nd.op == E_SUB_F ? "-" : nd.op == E_MUL_F ? "*" : "/";
+          out << "    Val " << n << " = " << l.n << "; " << n << ".f = " << l.n << ".f " << op << " " << r.n << ".f; "
+              << n << ".valid = " << l.n << ".valid && " << r.n << ".valid;\n";
+          st.push_back({n, Mag{}});
+          break;
+        }
+        case E_NEG_F: {
+          EV x = pop();
+          out << "    Val " << n << " = " << x.n << "; " << n << ".f = -" << x.n << ".f;\n";
+          st.push_back({n, Mag{}});
+          break;
+        }
+        case E_ADD_I: case E_SUB_I: case E_MUL_I: {
+          EV r = pop(), l = pop();
+          Mag bound = nd.op == E_MUL_I ? mag_mul(l.mag, r.mag) : mag_add(l.mag, r.mag);
+          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".valid = " << l.n << ".valid && " << r.n
+              << ".valid;\n";
+          if (mag_fits(bound)) {
+            // operand ranges rule out a 128-bit overflow: wrapping
+            // arithmetic gives the exact result
+            const char* op = nd.op == E_ADD_I ? "+" : nd.op == E_SUB_I ? "-" : "*";
+            out << "    " << n << ".i = (__int128)((unsigned __int128)" << l.n << ".i " << op << " (unsigned __int128)"
+                << r.n << ".i);\n";
+            st.push_back({n, bound});
+          } else {
+            const char* fn = nd.op == E_ADD_I ? "add_ovf_i128" : nd.op == E_SUB_I ? "sub_ovf_i128" : "mul_ovf_i128";
+            out << "    { __int128 o; if (" << fn << "(" << l.n << ".i, " << r.n << ".i, o) && " << n << ".valid) "
+                << ovf << " = true; " << n << ".i = o; }\n";
+            st.push_back({n, Mag{}});
+          }
+          break;
+        }
+        case E_NEG_I: {
+          EV x = pop();
+          out << "    Val " << n << " = " << x.n << "; " << n
+              << ".i = (__int128)((unsigned __int128)0 - (unsigned __int128)" << x.n << ".i);\n";
+          st.push_back({n, x.mag});
+          break;
+        }
+        case E_I2F: {
+          EV x = pop();
+          double sc = 1.0;
+          for (int q = 0; q < nd.col; ++q) sc *= 10.0;
+          uint64_t u;
+          std::memcpy(&u, &sc, 8);
+          out << "    Val " << n << " = " << x.n << "; " << n << ".f = (double)" << x.n << ".i / __longlong_as_double("
+              << hex64(u) << ");  // 10^" << nd.col << "\n";
+          st.push_back({n, Mag{}});
+          break;
+        }
+        case E_SCALE_I: {
+          EV x = pop();
+          out << "    Val " << n << " = " << x.n << "; { __int128 o; if (mul_ovf_i128(" << x.n << ".i, pow10_i128("
+              << nd.col << "), o) && " << x.n << ".valid) " << ovf << " = true; " << n << ".i = o; }\n";
+          st.push_back({n, Mag{}});
+          break;
+        }
+        case E_F2I: {
+          EV x = pop();
+          out << "    Val " << n << " = " << x.n << "; { double t = trunc(" << x.n
+              << ".f); if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) { " << n
+              << ".valid = false; " << n << ".i = 0; } else { " << n << ".i = (__int128)(long long)t; } }\n";
+          st.push_back({n, mag_of((unsigned __int128)1 << 63)});
+          break;
+        }
+        case E_SELECT: {
+          int nc = nd.col, has_else = nd.a, need = nc + has_else;
+          if ((int)st.size() < need || nc < 0) { ok = false; return "e_bad"; }
+          int base = (int)st.size() - need;
+          Mag bound = mag_of(0);
+          for (int q = base; q < (int)st.size(); ++q) bound = mag_max(bound, st[q].mag);
+          out << "    Val " << n << ";";
+          if (has_else) out << " " << n << " = " << st.back().n << ";\n";
+          else out << " " << n << ".valid = false; " << n << ".i = 0; " << n << ".f = 0;\n";
+          // the first clause that holds wins: evaluate from the last one
+          // backwards, each match overriding
+          for (int ci = nc - 1; ci >= 0; --ci) {
+            if (nd.b + ci < 0 || nd.b + ci >= (int)pg.clauses.size()) { ok = false; return "e_bad"; }
+            const PRange& cl = pg.clauses[nd.b + ci];
+            out << "    {\n";
+            auto pv = pred(cl.begin, cl.len);
+            out << "    if (" << pv.first << " && " << pv.second << ") " << n << " = " << st[base + ci].n
+                << ";\n    }\n";
+          }
+          st.resize(base);
+          st.push_back({n, bound});
+          break;
+        }
+        default:
+          ok = false;
+          return "e_bad";
+      }
+    }
+    if (st.size() != 1) { ok = false; return "e_bad"; }
+    return st.back().n;
+  }
+
+  std::string take() {
+    std::string s = out.str();
+    out.str("");
+    out.clear();
+    return s;
+  }
+};
+
+}  // namespace
+
+bool jit_enabled() { return nvrtc().ok; }
+
+void jit_stats(int64_t* compiles, double* ms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (compiles) *compiles = g_compiles;
+  if (ms) *ms = g_compile_ms;
+}
+
+const void* jit_get(const std::string& source, const char* name) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_cache.find(source);
+  if (it == g_cache.end()) {
+    Nvrtc& N = nvrtc();
+    if (!N.ok) fail(PRISM_ERR_INTERNAL, "run-time kernel compilation is not available (NVRTC not loaded)");
+    auto t0 = std::chrono::steady_clock::now();
+    nvrtcProgram prog;
+    if (N.create(&prog, source.c_str(), "prism_query.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
+        NVRTC_SUCCESS)
+      fail(PRISM_ERR_INTERNAL, "nvrtcCreateProgram failed");
+    // no FMA contraction: generated Float64 arithmetic rounds after every
+    // operation, like the interpreter and the reference
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-int128", "--fmad=false",
+                          "--diag-suppress=550"};
+    nvrtcResult r = N.compile(prog, 5, opts);
+    if (r != NVRTC_SUCCESS) {
+      size_t ls = 0;
+      N.log_size(prog, &ls);
+      std::string log(ls, '\0');
+      if (ls) N.log(prog, &log[0]);
+      N.destroy(&prog);
+      fail(PRISM_ERR_INTERNAL, "run-time kernel compilation failed:\n" + log);
+    }
+    size_t n = 0;
+    N.cubin_size(prog, &n);
+    std::vector<char> cubin(n);
+    N.cubin(prog, cubin.data());
+    N.destroy(&prog);
+    Entry e;
+    PRISM_CUDA(cudaLibraryLoadData(&e.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+    it = g_cache.emplace(source, std::move(e)).first;
+    g_compiles += 1;
+    g_compile_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  auto kt = it->second.kernels.find(name);
+  if (kt == it->second.kernels.end()) {
+    cudaKernel_t k;
+    PRISM_CUDA(cudaLibraryGetKernel(&k, it->second.lib, name));
+    kt = it->second.kernels.emplace(name, k).first;
+  }
+  return reinterpret_cast<const void*>(kt->second);
+}
+
+std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64) {
+  Gen gen(pg, b);
+  // filter
+  gen.declare_cols();
+  if (a.has_filter) {
+    auto p = gen.pred(a.filter.begin, a.filter.len);
+    gen.out << "    return " << p.first << " && " << p.second << ";\n";
+  } else {
+    gen.out << "    return true;\n";
+  }
+  std::string keep = gen.take();
+  // dense group id
+  gen.declare_cols();
+  gen.out << "    int g = 0;\n";
+  for (int k = 0; k < a.n_gcols; ++k) {
+    std::string c = gen.col(a.gcol[k]);
+    gen.out << "    { int64_t code = dcol_valid(" << c << ", idx) ? dcol_ival(" << c << ", idx) : a.dnull[" << k
+            << "]; g += (int)(code * a.dstride[" << k << "]); }\n";
+  }
+  gen.out << "    return g;\n";
+  std::string gid = gen.take();
+  // operands
+  gen.declare_cols();
+  gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
+  std::ostringstream kinds;
+  for (int j = 0; j < a.n_ops; ++j) {
+    const Op& o = a.op[j];
+    if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) return "";
+    kinds << "    if (j == " << j << ") return " << o.kind << ";\n";
+    const Src& sr = a.src[o.src];
+    gen.out << "    " << (j ? "else " : "") << "if (j == " << j << ") {\n";
+    switch (sr.kind) {
+      case S_COL_F64: {
+        std::string c = gen.col(sr.col);
+        gen.out << "    r.f = dcol_fval(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        break;
+      }
+      case S_COL_INT: {
+        std::string c = gen.col(sr.col);
+        gen.out << "    r.i = dcol_ival(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        break;
+      }
+      case S_COL_I128: {
+        std::string c = gen.col(sr.col);
+        gen.out << "    r.i = dcol_i128(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        break;
+      }
+      case S_VALID: {
+        std::string c = gen.col(sr.col);
+        gen.out << "    r.valid = dcol_valid(" << c << ", idx);\n";
+        break;
+      }
+      default: {
+        gen.out << "    bool ovf = false;\n";
+        std::string v = gen.expr(sr.begin, sr.end, "ovf");
+        gen.out << "    r = " << v << ";\n    if (ovf) atomicOr(a.err, DERR_RANGE);\n";
+      }
+    }
+    gen.out << "    }\n";
+  }
+  gen.out << "    return r;\n";
+  std::string value = gen.take();
+  if (!gen.ok) return "";
+
+  std::string consts = gen.consts.str();
+  if (consts.empty()) consts = "    int unused;\n";
+  std::ostringstream s;
+  s << "#include \"agg_device.cuh\"\n"
+       "namespace prism {\n"
+       "struct QueryRow {\n"
+       "  struct Consts {\n"
+    << consts
+    << "  };\n"
+       "  static __device__ __forceinline__ Consts load(const AggArgs& a) {\n    Consts K;\n"
+    << gen.load.str()
+    << "    return K;\n  }\n"
+       "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
+    << keep
+    << "  }\n"
+       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
+    << gid
+    << "  }\n"
+       "  static __device__ __forceinline__ int kind(const AggArgs& a, int j) {\n"
+    << kinds.str()
+    << "    return 0;\n  }\n"
+       "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
+       "int64_t idx) {\n"
+    << value
+    << "  }\n"
+       "};\n"
+       "}  // namespace prism\n"
+       "extern \"C\" __global__ void __launch_bounds__(prism::TINY_BLOCK, 1) prism_tiny_agg(prism::AggArgs a) {\n"
+       "  prism::tiny_body<prism::QueryRow, "
+    << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false")
+    << ">(a);\n"
+       "}\n";
+  return s.str();
+}
+
+}  // namespace prism

@@ -1,0 +1,42 @@
+// jit.hpp — per-query kernels generated at run time and compiled with NVRTC
+// for sm_100a.
+//
+// The ahead-of-time kernels interpret a query's filter and expression
+// programs node by node (eval.cuh); on a scan with few groups that
+// interpretation costs thousands of instructions per row. The generator
+// turns the same typed programs into straight-line CUDA C++ (column types and
+// null-freedom fixed, literals in registers, 128-bit overflow checks only
+// where the operand ranges need them) and instantiates the small-groups
+// kernel body (agg_device.cuh) with it. Results are identical by
+// construction: the generated code calls the same device helpers, in the
+// same order of operations, as the interpreter.
+#pragma once
+
+#include <string>
+
+#include "runtime.hpp"
+
+namespace prism {
+
+struct Program;
+struct AggArgs;
+
+// False when PRISM_JIT=0 is set or NVRTC (libnvrtc.so.12) cannot be loaded;
+// callers then launch the interpreting kernels.
+bool jit_enabled();
+
+// Kernel `name` of `source`, compiled once per process (cached by source
+// text). A compile error is an engine bug: throws PRISM_ERR_INTERNAL with
+// the compiler log.
+const void* jit_get(const std::string& source, const char* name);
+
+// Number of NVRTC compilations so far and their total wall time (ms).
+void jit_stats(int64_t* compiles, double* ms);
+
+// Source of the small-groups aggregation kernel `prism_tiny_agg` for the
+// program `pg` over batch `b` (`a` holds the sources, ops and group columns;
+// g groups, f64 = some Float64 SUM present). Empty when the program uses a
+// construct the generator does not cover.
+std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64);
+
+}  // namespace prism
