@@ -9,6 +9,14 @@ build_payload) for every match in the reference's order. Input rows/s =
 (10M + 100M) / step time. Synthetic, seeded data of the stated shapes.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl prism|reference]
+                  [--workload c2|c1|c3|c4]
+
+--workload picks the other shapes of the path (default c2, the join above):
+  c1  GROUP BY over one 1M-row batch: int64 key over 1,024 values; COUNT,
+      SUM/MIN/MAX(v_i int64), SUM/AVG(v_f float64)
+  c3  fused filter -> project -> aggregate over 100M fact rows (exact int128
+      expressions, GROUP BY two dictionary columns)
+  c4  join (15M unique utf8 build keys) -> GROUP BY over 150M probe rows
 
 value: device-resident inputs (HBM), CUDA-event timed, max over ranks.
 e2e:   the same step through the C ABI with host (pinned) Arrow buffers: H2D of
@@ -37,12 +45,15 @@ METRIC = "join/agg input rows/s"
 WORKLOAD = "inner hash join: 10M unique int64 build keys (+int64 payload) x 100M Zipf(1.1) int64 probe keys (+int32 payload), emit (probe_row_idx, build_payload)"
 FALLBACK_HBM_GBS = 6650.0
 CPU_SAMPLE_PROBE = 10_000_000
+SCALE = 1.0
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4"], default="c2")
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["prism", "reference"], default="prism")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -50,7 +61,10 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale all sizes (profiling captures use a smaller case; bench lines use 1.0)")
     a = ap.parse_args()
-    global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE
+    if a.steps is None:
+        a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10}[a.workload]
+    global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE
+    SCALE = a.scale
     if a.scale != 1.0:
         N_BUILD = int(N_BUILD * a.scale)
         N_PROBE = int(N_PROBE * a.scale)
@@ -167,6 +181,8 @@ def main():
         import datetime
 
         dist.init_process_group("nccl" if args.impl == "prism" else "gloo", timeout=datetime.timedelta(seconds=120))
+    if args.workload != "c2":
+        return run_workload(args, rank, world, local, torch, dist)
     if args.impl == "reference":
         return run_reference(args, rank, world, torch, dist)
 
@@ -297,6 +313,517 @@ def main():
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------- workloads --
+def sc(n):
+    return max(1, int(n * SCALE))
+
+
+def utf8_strings(torch, words, device):
+    """Utf8 values -> (int32 offsets, uint8 data) device tensors."""
+    offs = [0]
+    for w in words:
+        offs.append(offs[-1] + len(w.encode()))
+    data = b"".join(w.encode() for w in words) or b"\0"
+    return (torch.tensor(offs, dtype=torch.int32, device=device),
+            torch.tensor(list(data), dtype=torch.uint8, device=device))
+
+
+def pinned(torch, t):
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t)
+    return h
+
+
+def host_array(torch, pa, t, typ):
+    h = pinned(torch, t)
+    return pa.Array.from_buffers(typ, h.numel(), [None, pa.foreign_buffer(h.data_ptr(), h.numel() * h.element_size(), base=h)])
+
+
+def host_utf8(torch, pa, offs, data, n):
+    ho, hd = pinned(torch, offs), pinned(torch, data)
+    return pa.Array.from_buffers(pa.utf8(), n, [None, pa.foreign_buffer(ho.data_ptr(), ho.numel() * 4, base=ho),
+                                                pa.foreign_buffer(hd.data_ptr(), max(1, hd.numel()), base=hd)])
+
+
+def host_dict(torch, pa, idx, offs, data, n_dict):
+    return pa.DictionaryArray.from_arrays(host_array(torch, pa, idx, pa.int8()), host_utf8(torch, pa, offs, data, n_dict))
+
+
+def oracle_mod():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py
+
+    return oracle_py
+
+
+class C1:
+    """GROUP BY over one 1M-row batch (the reference's CPU-runnable case)."""
+    name = "c1"
+    workload = ("GROUP BY over one 1M-row batch: int64 key uniform over 1,024 values; COUNT, SUM/MIN/MAX(v_i int64), "
+                "SUM/AVG(v_f float64)")
+    dtype = "int64+f64"
+    flush_l2 = True
+
+    def __init__(self, torch, device, ctx, rank):
+        import prism_gpu
+        from prism_gpu import AggExpr, AggFunc, HashAggConfig
+
+        self.torch, self.ctx, self.pg = torch, ctx, prism_gpu
+        n = self.rows = sc(1_000_000)
+        g = torch.Generator(device=device)
+        g.manual_seed(100 + rank)
+        keys = torch.randint(-(2**62), 2**62, (1024,), generator=g, device=device, dtype=torch.int64)
+        self.key = keys[torch.randint(0, 1024, (n,), generator=g, device=device)]
+        self.vi = torch.randint(-1_000_000, 1_000_001, (n,), generator=g, device=device, dtype=torch.int64)
+        self.vf = torch.rand(n, generator=g, device=device, dtype=torch.float64)
+        self.batch = prism_gpu.DeviceBatch.from_device_buffers(
+            [("key", "l", self.key.data_ptr()), ("v_i", "l", self.vi.data_ptr()), ("v_f", "g", self.vf.data_ptr())], n, ctx,
+            device.index)
+        self.cfg = HashAggConfig([0], [AggExpr(0, AggFunc.Count, "count"), AggExpr(1, AggFunc.Sum, "sum_i"),
+                                       AggExpr(1, AggFunc.Min, "min_i"), AggExpr(1, AggFunc.Max, "max_i"),
+                                       AggExpr(2, AggFunc.Sum, "sum_f"), AggExpr(2, AggFunc.Avg, "avg_f")])
+
+    def step(self):
+        out = self.pg.hash_aggregate(self.batch, self.cfg, ctx=self.ctx, as_device=True)
+        out.free()
+
+    def host_batch(self):
+        import pyarrow as pa
+
+        t = self.torch
+        return pa.RecordBatch.from_arrays([host_array(t, pa, self.key, pa.int64()), host_array(t, pa, self.vi, pa.int64()),
+                                           host_array(t, pa, self.vf, pa.float64())], names=["key", "v_i", "v_f"])
+
+    def check(self):
+        from helpers import assert_batches_equal
+
+        hb = self.host_batch()
+        got = self.pg.hash_aggregate(self.batch, self.cfg, ctx=self.ctx)
+        ref = oracle_mod().hash_aggregate(hb, self.cfg, n_threads=1)
+        assert_batches_equal(got, ref, float_cols=(4, 5, 6))
+        return {"groups": got.num_rows, "full_size_check": "bit-exact vs the oracle (Float64 sums within 1e-12)"}
+
+    def roofline(self, kstats):
+        n, ms = kstats.get("agg_kernel", (0, 0.0))
+        return {"kernel": "agg_kernel", "bytes": 24 * self.rows, "ms": ms / max(1, n),
+                "per_unit": "24 B per row (key + v_i + v_f)", "traffic_key": "agg_c1"}
+
+    def e2e_inputs(self):
+        return [self.host_batch()]
+
+    def e2e_step(self, hb):
+        return self.pg.hash_aggregate(hb[0], self.cfg, ctx=self.ctx)
+
+    def cpu_baseline(self, threads):
+        hb = self.host_batch()
+        o = oracle_mod()
+        o.hash_aggregate(hb, self.cfg, n_threads=1)
+        runs, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 5.0:
+            o.hash_aggregate(hb, self.cfg, n_threads=1)
+            runs += 1
+        dt = (time.perf_counter() - t0) / runs
+        return self.rows / dt, 1, (f"the whole {self.rows:,}-row batch, {runs} runs; the reference aggregates one "
+                                   "RecordBatch on one thread (hash_aggregate.rs:217)")
+
+
+def c3_exprs():
+    from prism_gpu import ArithmeticOp, ScalarExpr, ScalarValue
+
+    c = ScalarExpr.ColumnRef
+    L = lambda v: ScalarExpr.Literal(ScalarValue.Int64(v))  # noqa: E731
+    disc = ScalarExpr.BinaryOp(ArithmeticOp.Multiply, c(1), ScalarExpr.BinaryOp(ArithmeticOp.Subtract, L(100), c(2)))
+    charge = ScalarExpr.BinaryOp(ArithmeticOp.Multiply, disc, ScalarExpr.BinaryOp(ArithmeticOp.Add, L(100), c(3)))
+    return [disc, charge]
+
+
+def c3_agg():
+    from prism_gpu import AggExpr, AggFunc, HashAggConfig
+
+    return HashAggConfig([0, 1], [
+        AggExpr(2, AggFunc.Sum, "sum_disc_price"), AggExpr(2, AggFunc.Avg, "avg_disc_price"),
+        AggExpr(3, AggFunc.Sum, "sum_charge"), AggExpr(3, AggFunc.Avg, "avg_charge"), AggExpr(2, AggFunc.Count, "count_order")])
+
+
+class C3:
+    """Fused filter -> project -> aggregate over a 100M-row fact table."""
+    name = "c3"
+    workload = ("fused filter->project->aggregate, 100M rows: ship_day <= 2436; price*(100-discount) and "
+                "price*(100-discount)*(100+tax) exact int128 (price in cents, discount/tax in hundredths); "
+                "GROUP BY (flag, status) utf8 dictionaries: SUM, AVG, COUNT")
+    dtype = "int64->int128"
+    flush_l2 = False
+
+    def __init__(self, torch, device, ctx, rank):
+        import prism_gpu
+        from prism_gpu import Predicate, ScalarValue
+
+        self.torch, self.ctx, self.pg = torch, ctx, prism_gpu
+        n = self.rows = sc(100_000_000)
+        g = torch.Generator(device=device)
+        g.manual_seed(300 + rank)
+        r = lambda lo, hi, dt=torch.int64: torch.randint(lo, hi, (n,), generator=g, device=device, dtype=dt)  # noqa: E731
+        self.cols = {"quantity": r(1, 51), "price": r(90_000, 10_500_001), "discount": r(0, 11), "tax": r(0, 9),
+                     "ship_day": r(0, 2526, torch.int32), "flag": r(0, 3, torch.int8), "status": r(0, 2, torch.int8)}
+        self.fo, self.fd = utf8_strings(torch, ["A", "N", "R"], device)
+        self.so, self.sd = utf8_strings(torch, ["F", "O"], device)
+        c = self.cols
+        self.batch = prism_gpu.DeviceBatch.from_device_buffers([
+            ("quantity", "l", c["quantity"].data_ptr()), ("price", "l", c["price"].data_ptr()),
+            ("discount", "l", c["discount"].data_ptr()), ("tax", "l", c["tax"].data_ptr()),
+            ("ship_day", "i", c["ship_day"].data_ptr()),
+            ("flag", "c", c["flag"].data_ptr(), (self.fo.data_ptr(), self.fd.data_ptr(), 3)),
+            ("status", "c", c["status"].data_ptr(), (self.so.data_ptr(), self.sd.data_ptr(), 2))], n, ctx, device.index)
+        self.pred = Predicate.Le(4, ScalarValue.Int32(2436))
+        self.exprs, self.agg = c3_exprs(), c3_agg()
+
+    def run(self, batches, **kw):
+        return self.pg.filter_project_aggregate(batches, self.pred, [5, 6], self.exprs, self.agg,
+                                                arith_mode=self.pg.ARITH_EXACT, ctx=self.ctx, **kw)
+
+    def step(self):
+        out = self.run([self.batch], as_device=True)
+        out.free()
+
+    def check(self):
+        torch = self.torch
+        got = self.run([self.batch])
+        c = self.cols
+        keep = c["ship_day"] <= 2436
+        gid = c["flag"].to(torch.int64) * 2 + c["status"].to(torch.int64)
+        exp = {}
+        for lo in range(0, self.rows, 1_000_000):  # exact per-group sums, chunked so int64 never overflows
+            sl = slice(lo, lo + 1_000_000)
+            k, gg = keep[sl], gid[sl]
+            disc = c["price"][sl] * (100 - c["discount"][sl])
+            charge = disc * (100 + c["tax"][sl])
+            for q in range(6):
+                m = k & (gg == q)
+                e = exp.setdefault(q, [0, 0, 0])
+                e[0] += int(disc[m].sum().item())
+                e[1] += int(charge[m].sum().item())
+                e[2] += int(m.sum().item())
+        names = {0: ("A", "F"), 1: ("A", "O"), 2: ("N", "F"), 3: ("N", "O"), 4: ("R", "F"), 5: ("R", "O")}
+        cols = [got.column(i).to_pylist() for i in range(got.num_columns)]
+        for row in zip(*cols):
+            q = [k for k, v in names.items() if v == (row[0], row[1])][0]
+            d, ch, cnt = exp[q]
+            assert int(row[2]) == d and int(row[4]) == ch and row[6] == cnt, (row, exp[q])
+        return {"groups": got.num_rows,
+                "full_size_check": "exact int128 SUMs and COUNT per group equal chunked torch int64 sums"}
+
+    def roofline(self, kstats):
+        name = max(("agg_tiny_jit", "agg_kernel"), key=lambda k: kstats.get(k, (0, 0.0))[0])
+        n, ms = kstats.get(name, (0, 0.0))
+        return {"kernel": f"{name} (fused filter + project + aggregate)", "bytes": 30 * self.rows, "ms": ms / max(1, n),
+                "per_unit": "30 B per row (ship_day 4 + price 8 + discount 8 + tax 8 + flag 1 + status 1)",
+                "traffic_key": "agg_c3"}
+
+    def host_batch(self, lo=0, hi=None):
+        import pyarrow as pa
+
+        t, c = self.torch, self.cols
+        hi = self.rows if hi is None else hi
+        sl = slice(lo, hi)
+        arrs = [host_array(t, pa, c[k][sl], pa.int64()) for k in ("quantity", "price", "discount", "tax")]
+        arrs.append(host_array(t, pa, c["ship_day"][sl], pa.int32()))
+        arrs.append(host_dict(t, pa, c["flag"][sl], self.fo, self.fd, 3))
+        arrs.append(host_dict(t, pa, c["status"][sl], self.so, self.sd, 2))
+        schema = pa.schema([pa.field(nm, a.type, nullable=False) for nm, a in
+                            zip(["quantity", "price", "discount", "tax", "ship_day", "flag", "status"], arrs)])
+        return pa.RecordBatch.from_arrays(arrs, schema=schema)
+
+    def e2e_inputs(self):
+        return [self.host_batch()]
+
+    def e2e_step(self, hb):
+        return self.run(hb)
+
+    def cpu_baseline(self, threads):
+        o = oracle_mod()
+        s = min(self.rows, 10_000_000)
+        bs = [self.host_batch(lo, min(s, lo + 1_000_000)) for lo in range(0, s, 1_000_000)]
+        t0 = time.perf_counter()
+        o.filter_project_aggregate(bs, self.pred, [5, 6], self.exprs, self.agg, n_threads=threads)
+        dt = time.perf_counter() - t0
+        return s / dt, threads, (f"first {s:,} rows in 1M-row batches, the reference's Float64 expression semantics "
+                                 f"({dt:.2f} s)")
+
+
+class C4:
+    """Join (unique utf8 build keys) -> GROUP BY over the probe stream."""
+    name = "c4"
+    workload = ("join->aggregate: 15M unique utf8 build keys (8-32 bytes) + int32 group id over 25 values; 150M probe "
+                "rows with keys drawn Zipf(0.8) over the build keys (5% non-matching), float64 amount lognormal(5,1), "
+                "in 10M-row batches; SUM(amount), COUNT GROUP BY group_id")
+    dtype = "utf8+f64"
+    flush_l2 = False
+    BATCH = 10_000_000
+
+    def __init__(self, torch, device, ctx, rank):
+        import prism_gpu
+        from prism_gpu import AggExpr, AggFunc, HashAggConfig
+
+        self.torch, self.ctx, self.pg = torch, ctx, prism_gpu
+        nb, npr = sc(15_000_000), sc(150_000_000)
+        self.nb, self.np_ = nb, npr
+        self.rows = nb + npr
+        g = torch.Generator(device=device)
+        g.manual_seed(400 + rank)
+        lens = torch.randint(8, 33, (nb,), generator=g, device=device, dtype=torch.int64)
+        boffs = torch.zeros(nb + 1, device=device, dtype=torch.int64)
+        torch.cumsum(lens, 0, out=boffs[1:])
+        bdata = torch.randint(97, 123, (int(boffs[-1].item()),), generator=g, device=device, dtype=torch.uint8)
+        idx = torch.arange(nb, device=device, dtype=torch.int64)
+        for k in range(6):  # the first 6 letters spell the row index in base 26: keys are unique
+            bdata[boffs[:-1] + k] = (97 + (idx // 26**k) % 26).to(torch.uint8)
+        self.bo32 = boffs.to(torch.int32)
+        self.bdata = bdata
+        self.gid = torch.randint(0, 25, (nb,), generator=g, device=device, dtype=torch.int32)
+        self.build = prism_gpu.DeviceBatch.from_device_buffers(
+            [("key", "u", (self.bo32.data_ptr(), bdata.data_ptr())), ("group_id", "i", self.gid.data_ptr())], nb, ctx,
+            device.index)
+        # Zipf(0.8) ranks over the build rows through a seeded permutation
+        w = torch.arange(1, nb + 1, device=device, dtype=torch.float64).pow_(-0.8)
+        cdf = torch.cumsum(w, 0)
+        cdf /= cdf[-1].clone()
+        del w
+        perm = torch.randperm(nb, generator=g, device=device)
+        self.batches, self.keep, self.hits = [], [], 0
+        for lo in range(0, npr, self.BATCH):
+            n = min(self.BATCH, npr - lo)
+            u = torch.rand(n, generator=g, device=device, dtype=torch.float64)
+            src = perm[torch.searchsorted(cdf, u, right=True).clamp_(max=nb - 1)]
+            del u
+            plen = lens[src]
+            poffs = torch.zeros(n + 1, device=device, dtype=torch.int64)
+            torch.cumsum(plen, 0, out=poffs[1:])
+            row = torch.repeat_interleave(torch.arange(n, device=device), plen)
+            pos = torch.arange(row.numel(), device=device) - poffs[row]
+            pdata = bdata[boffs[src][row] + pos]
+            del row, pos
+            miss = torch.rand(n, generator=g, device=device) < 0.05
+            pdata[poffs[:-1][miss]] = ord("Z")  # upper case never occurs in build keys
+            self.hits += int(n - miss.sum().item())
+            amount = torch.exp(5.0 + torch.randn(n, generator=g, device=device, dtype=torch.float64))  # lognormal(5, 1)
+            po32 = poffs.to(torch.int32)
+            del poffs, src, plen, miss
+            db = prism_gpu.DeviceBatch.from_device_buffers(
+                [("key", "u", (po32.data_ptr(), pdata.data_ptr())), ("amount", "g", amount.data_ptr())], n, ctx, device.index)
+            self.batches.append(db)
+            self.keep.append((po32, pdata, amount))
+        del cdf, perm
+        self.agg = HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "sum_amount"), AggExpr(1, AggFunc.Count, "cnt")])
+        self.cols = [3, 1]  # group_id (build side), amount (probe side)
+
+    def run(self, probes, build, **kw):
+        return self.pg.join_aggregate(probes, build, [0], [0], self.cols, [], self.agg, ctx=self.ctx, **kw)
+
+    def step(self):
+        out = self.run(self.batches, self.build, as_device=True)
+        out.free()
+
+    def check(self):
+        got = self.run(self.batches, self.build)
+        total = sum(got.column(2).to_pylist())
+        assert total == self.hits, (total, self.hits)
+        return {"groups": got.num_rows, "matches": self.hits,
+                "full_size_check": "COUNT total == probe rows drawn from build keys"}
+
+    def roofline(self, kstats):
+        names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit")
+        ms = sum(kstats.get(k, (0, 0.0))[1] for k in names)
+        steps = max(1, kstats.get("insert_kernel", (1, 0.0))[0])
+        kb = int(self.bo32[-1].item()) + sum(int(k[0][-1].item()) for k in self.keep)
+        nbytes = kb + 8 * self.nb + 12 * self.np_
+        return {"kernel": "insert + probe + aggregation kernels (per step)", "bytes": nbytes, "ms": ms / steps,
+                "per_unit": "build: key bytes + 4 B offset + 4 B group id; probe: key bytes + 4 B offset + 8 B amount",
+                "traffic_key": "join_agg_c4"}
+
+    def host_build(self):
+        import pyarrow as pa
+
+        t = self.torch
+        return pa.RecordBatch.from_arrays([host_utf8(t, pa, self.bo32, self.bdata, self.nb),
+                                           host_array(t, pa, self.gid, pa.int32())], names=["key", "group_id"])
+
+    def host_probe(self, k, rows=None):
+        import pyarrow as pa
+
+        t = self.torch
+        po, pd, am = self.keep[k]
+        n = po.numel() - 1 if rows is None else rows
+        return pa.RecordBatch.from_arrays([host_utf8(t, pa, po[: n + 1], pd, n), host_array(t, pa, am[:n], pa.float64())],
+                                          names=["key", "amount"])
+
+    def e2e_inputs(self):
+        return [self.host_build()] + [self.host_probe(k) for k in range(len(self.keep))]
+
+    def e2e_step(self, hb):
+        return self.run(hb[1:], hb[0])
+
+    def cpu_baseline(self, threads):
+        o = oracle_mod()
+        build = self.host_build()
+        s = min(self.np_, 10_000_000)
+        probes = []
+        for lo in range(0, s, 1_000_000):
+            pb = self.host_probe(lo // self.BATCH)
+            off = lo % self.BATCH
+            probes.append(pb.slice(off, min(1_000_000, s - lo)))
+        t0 = time.perf_counter()
+        o.join_aggregate(probes, build, [0], [0], self.cols, [], self.agg, n_threads=threads)
+        dt = time.perf_counter() - t0
+        return (self.nb + s) / dt, threads, (f"oracle join->aggregate: all {self.nb:,} build rows + the first {s:,} probe "
+                                             f"rows in 1M-row batches ({dt:.2f} s)")
+
+
+WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4}
+
+
+def gpu_index_of(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if vis and vis.split(",")[local].strip().isdigit():
+        return int(vis.split(",")[local])
+    return local
+
+
+def run_workload(args, rank, world, local, torch, dist):
+    Wc = WORKLOAD_CLASSES[args.workload]
+    if args.impl == "reference":
+        if rank != 0:
+            if world > 1:
+                dist.destroy_process_group()
+            return
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(0)
+        import prism_gpu
+
+        W = Wc(torch, dev, prism_gpu.Context(0), 0)
+        threads = os.cpu_count() or 1
+        rates = []
+        for _ in range(max(1, min(args.steps, 3))):
+            r, cores, sample = W.cpu_baseline(threads)
+            rates.append(r)
+        value = sorted(rates)[len(rates) // 2]
+        line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": len(rates),
+                "warmup": args.warmup, "ms_per_step": W.rows / value * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": W.dtype, "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": W.workload, "rows_per_step": W.rows},
+                "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import prism_gpu
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    ctx = prism_gpu.Context(local)
+    stream = torch.cuda.current_stream(device)
+    ctx.set_stream(stream.cuda_stream)
+    W = Wc(torch, device, ctx, rank)
+    torch.cuda.synchronize()
+    for _ in range(max(3, args.warmup)):
+        W.step()
+    extra = {} if args.no_check else W.check()
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32) if W.flush_l2 else None
+
+    ctx.set_profiling(True)
+    launches0 = ctx.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(gpu_index_of(local)) as clocks:
+        time.sleep(0.5)  # let the sampler start before the timed region
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if flush is not None:
+                flush.fill_(float(i))  # evict the inputs from L2 between steps (outside the events)
+            ev[i][0].record(stream)
+            W.step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    launches = ctx.kernel_launches - launches0
+    names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit",
+             "predicate_kernel", "expr_kernel")
+    kstats = {k: ctx.kernel_stats(k) for k in names}
+    ctx.set_profiling(False)
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * W.rows * args.steps / (ms_max / 1e3)
+
+    rf = W.roofline(kstats)
+    peak, peak_kind = peaks()
+    achieved = rf["bytes"] / (rf["ms"] / 1e3) / 1e9 if rf["ms"] else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(rf["traffic_key"])
+
+    e2e = None
+    if args.e2e_steps > 0:
+        hb = W.e2e_inputs()
+        h2d = sum(c.nbytes for b in hb for c in b.columns)
+        out = W.e2e_step(hb)  # warm
+        d2h = sum(c.nbytes for c in out.columns)
+        del out
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            out = W.e2e_step(hb)
+            del out
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.e2e_steps
+        tt = torch.tensor([dt], device=device, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dt = float(tt.item())
+        del hb
+        e2e = {"value": world * W.rows / dt, "unit": "rows/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+               "timing": "host wall clock around the synchronous C-ABI calls: import (H2D from pinned host Arrow "
+                         "buffers), operator, export (D2H)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, sample = W.cpu_baseline(os.cpu_count() or 1)
+        cpu = {"value": rate, "unit": "rows/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": W.dtype,
+            "data": "synthetic (seeded torch generators with the configs' shapes and distributions)",
+            "config": dict({"workload": W.workload, "rows_per_step": W.rows,
+                            "l2": "L2 flushed between steps (256 MB write)" if W.flush_l2 else
+                            "inputs larger than L2, no flush",
+                            "parallelism": f"independent shard per GPU (weak) x{world}"}, **extra),
+            "roofline": {"bound": "hbm", "kernel": rf["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                         "fallback 6650 GB/s",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": rf["bytes"],
+                         "algorithmic_per_unit": rf["per_unit"], "avg_launch_ms": rf["ms"],
+                         "kernel_ms_per_launch": {k: v[1] / v[0] for k, v in kstats.items() if v[0]}},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks.summary(),
         }
         print(json.dumps(line))
     if world > 1:

@@ -205,21 +205,40 @@ class DeviceBatch:
 
     @staticmethod
     def from_device_buffers(columns, num_rows: int, ctx: Optional[Context] = None, device_id: int = 0) -> "DeviceBatch":
-        """Wraps device-resident, null-free fixed-width columns without a copy.
+        """Wraps device-resident, null-free columns without a copy.
 
-        columns: list of (name, arrow_format, device_pointer); the memory must
-        outlive the batch (e.g. torch tensors the caller keeps).
+        columns: list of
+          (name, arrow_format, values_ptr)                 fixed width
+          (name, "u", (offsets_ptr, data_ptr))              Utf8 (int32 offsets)
+          (name, index_format, indices_ptr, (dict_offsets_ptr, dict_data_ptr, dict_len))
+                                                           Utf8 dictionary
+        The memory must outlive the batch (e.g. torch tensors the caller keeps).
         """
         ctx = ctx or default_context()
         keep = []
         n = len(columns)
         child_arrays = (C.POINTER(_abi.ArrowArray) * n)()
         child_schemas = (C.POINTER(_abi.ArrowSchema) * n)()
-        for i, (name, fmt, ptr) in enumerate(columns):
-            bufs = (C.c_void_p * 2)(None, ptr)
-            a = _abi.ArrowArray(num_rows, 0, 0, 2, 0, bufs, None, None)
+        for i, col in enumerate(columns):
+            name, fmt, ptr = col[0], col[1], col[2]
             nm, fm = name.encode(), fmt.encode()
-            s_ = _abi.ArrowSchema(fm, nm, None, 0, 0, None, None)
+            dict_a = dict_s = None
+            if fmt == "u":
+                offs, data = ptr
+                bufs = (C.c_void_p * 3)(None, offs, data)
+                nbuf = 3
+            else:
+                bufs = (C.c_void_p * 2)(None, ptr)
+                nbuf = 2
+                if len(col) > 3:
+                    doffs, ddata, dlen = col[3]
+                    dbufs = (C.c_void_p * 3)(None, doffs, ddata)
+                    da = _abi.ArrowArray(dlen, 0, 0, 3, 0, dbufs, None, None)
+                    ds = _abi.ArrowSchema(b"u", b"", None, 0, 0, None, None)
+                    keep += [dbufs, da, ds]
+                    dict_a, dict_s = C.pointer(da), C.pointer(ds)
+            a = _abi.ArrowArray(num_rows, 0, 0, nbuf, 0, bufs, None, dict_a)
+            s_ = _abi.ArrowSchema(fm, nm, None, 0, 0, None, dict_s)
             keep += [bufs, a, s_, nm, fm]
             child_arrays[i] = C.pointer(a)
             child_schemas[i] = C.pointer(s_)
