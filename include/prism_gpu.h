@@ -235,6 +235,12 @@ uint64_t prism_ctx_kernel_launches(const prism_ctx* ctx);
  * profiling was (re-)enabled. */
 int prism_ctx_set_profiling(prism_ctx* ctx, int enable);
 int prism_ctx_kernel_stats(prism_ctx* ctx, const char* name, uint64_t* launches, double* total_ms);
+/* Per-query kernels compiled at run time (NVRTC, process-wide cache): sets
+ * *enabled (0 when PRISM_JIT=0 or libnvrtc.so.12 is absent; the
+ * interpreting kernels then run), the number of compilations so far and their
+ * summed wall time. No counterpart in the reference (its operators are
+ * compiled Rust). Any pointer may be NULL. */
+int prism_jit_stats(int32_t* enabled, int64_t* compiles, double* total_ms);
 const char* prism_version(void);
 
 /* ------------------------------------------------------------------------ */

@@ -255,8 +255,12 @@ ColP filter_col(const Col& c, const std::vector<uint8_t>& keep) {
 }
 
 // cast of a column to Float64 as arrow_cast::cast does for the aggregate and
-// arithmetic inputs (hash_aggregate.rs:227-245, filter_project.rs:236-238):
-// values are mapped slot by slot (null slots keep their raw value mapped).
+// arithmetic inputs (hash_aggregate.rs:227-245, filter_project.rs:236-238).
+// Null slots: a Float64 column is not cast and keeps its raw slots; the
+// Decimal128 -> Float64 cast maps every slot (unary), so raw slots are
+// mapped too; integer, Float32 and Boolean casts (numeric_cast / unary_opt,
+// cast_bool_to_numeric) write only valid rows into a zeroed buffer, so a
+// null row reads 0.
 struct F64Col {
   std::vector<double> v;
   std::vector<uint8_t> valid;  // 1 = valid
@@ -269,8 +273,8 @@ F64Col cast_f64(const Col& c, const char* what) {
     case T_I8: case T_I16: case T_I32: case T_I64: case T_U8: case T_U16: case T_U32:
     case T_U64: case T_F32: case T_F64: case T_BOOL: case T_DEC128:
       for (int64_t i = 0; i < c.len; ++i) {
-        r.v[i] = c.fval(i);
         r.valid[i] = !c.null_at(i);
+        r.v[i] = (r.valid[i] || c.ty == T_F64 || c.ty == T_DEC128) ? c.fval(i) : 0.0;
       }
       return r;
     case T_NULL:
@@ -1127,8 +1131,11 @@ __int128 pow10_i128(int s) {
 bool exactable(const Col& c) {
   return (is_int_like(c.ty) && c.ty != T_DATE32) || c.ty == T_DEC128 || c.ty == T_BOOL;
 }
+// exact value of row i; a null row of an integer column reads 0 and a
+// Decimal128 keeps its raw slot, as the Float64 cast above treats them
 __int128 exact_val(const Col& c, int64_t i) {
   if (c.ty == T_DEC128) return c.dval(i);
+  if (c.null_at(i)) return 0;
   if (c.ty == T_U64) return (__int128)(uint64_t)c.ival(i);
   return (__int128)c.ival(i);
 }

@@ -46,9 +46,10 @@ __device__ __forceinline__ void load_sources(const AggArgs& a, int64_t row, RowV
   for (int s = 0; s < a.n_src; ++s) {
     const Src& sr = a.src[s];
     switch (sr.kind) {
-      case S_COL_F64: v.f[s] = dcol_fval(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
-      case S_COL_INT: v.i[s] = dcol_ival(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
-      case S_COL_I128: v.i[s] = dcol_i128(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
+      // inputs as arrow's cast to Float64 leaves them (hash_aggregate.rs:227-245)
+      case S_COL_F64: v.f[s] = dcol_fval_cast(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
+      case S_COL_INT: v.i[s] = dcol_ival_cast(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
+      case S_COL_I128: v.i[s] = dcol_i128_cast(a.cols[sr.col], row); v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
       case S_VALID: v.valid[s] = dcol_valid(a.cols[sr.col], row); break;
       case S_EXPR_F64: case S_EXPR_I128: {
         bool ovf = false;
@@ -846,11 +847,18 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         if (b->rows && b->cols[bc]->dict_fingerprint != c.dict_fingerprint) all_dict = false;
     }
     if (all_dict) {
+      // one id per dictionary entry, plus one for null only when some batch
+      // has nulls in the column (so null-free keys stay compact)
+      std::vector<int64_t> card(cfg.n_group_by);
       int64_t prod = 1;
-      for (int bc : gbatch_cols) {
-        int64_t card = ref.cols[bc]->dict->length + 1;
-        if (prod * card > 4096) { prod = -1; break; }
-        prod *= card;
+      for (int k = 0; k < cfg.n_group_by; ++k) {
+        int bc = gbatch_cols[k];
+        bool nulls = false;
+        for (auto* b : batches)
+          if (b->rows && b->cols[bc]->validity) nulls = true;
+        card[k] = ref.cols[bc]->dict->length + (nulls ? 1 : 0);
+        if (card[k] < 1 || prod * card[k] > 4096) { prod = -1; break; }
+        prod *= card[k];
       }
       if (prod > 0) {
         dense = true;
@@ -860,7 +868,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
           const Column& c = *ref.cols[gbatch_cols[k]];
           A.dstride[k] = stride;
           A.dnull[k] = c.dict->length;
-          stride *= c.dict->length + 1;
+          stride *= card[k];
         }
       }
     }

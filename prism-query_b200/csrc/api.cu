@@ -8,6 +8,7 @@
 #include "agg.hpp"
 #include "arrow_io.hpp"
 #include "filter_project.hpp"
+#include "jit.hpp"
 #include "join.hpp"
 #include "prims.hpp"
 
@@ -323,6 +324,12 @@ int prism_ctx_kernel_stats(prism_ctx* c, const char* name, uint64_t* launches, d
       *launches += 1;
     }
   });
+}
+
+int prism_jit_stats(int32_t* enabled, int64_t* compiles, double* total_ms) {
+  if (enabled) *enabled = prism::jit_enabled() ? 1 : 0;
+  prism::jit_stats(compiles, total_ms);
+  return PRISM_OK;
 }
 uint64_t prism_ctx_kernel_launches(const prism_ctx* c) { return c ? c->impl.launches.load() : 0; }
 

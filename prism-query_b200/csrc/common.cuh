@@ -103,6 +103,21 @@ __device__ __forceinline__ __int128 dcol_i128(const DCol& c, int64_t i) {
   return (__int128)dcol_ival(c, i);
 }
 
+// Value of row i as arrow's cast hands it to arithmetic and aggregation:
+// the cast of an integer, Float32 or Boolean column (arrow-rs numeric_cast /
+// unary_opt) writes 0 into the slots of null rows, while a Float64 column
+// (no cast) and the Decimal128 -> Float64 cast (unary) keep the raw slot.
+__device__ __forceinline__ bool keeps_null_slot(const DCol& c) { return c.type == TY_F64 || c.type == TY_DEC128; }
+__device__ __forceinline__ double dcol_fval_cast(const DCol& c, int64_t i) {
+  return (keeps_null_slot(c) || dcol_valid(c, i)) ? dcol_fval(c, i) : 0.0;
+}
+__device__ __forceinline__ int64_t dcol_ival_cast(const DCol& c, int64_t i) {
+  return (keeps_null_slot(c) || dcol_valid(c, i)) ? dcol_ival(c, i) : 0;
+}
+__device__ __forceinline__ __int128 dcol_i128_cast(const DCol& c, int64_t i) {
+  return (keeps_null_slot(c) || dcol_valid(c, i)) ? dcol_i128(c, i) : (__int128)0;
+}
+
 // UTF8 (or dictionary-decoded) bytes of row i.
 __device__ __forceinline__ void dcol_str(const DCol& c, int64_t i, const uint8_t*& p, int32_t& n) {
   if (c.type == TY_DICT) {

@@ -56,7 +56,8 @@ enum EOp : int32_t {
 struct ENode {
   int32_t op;
   int32_t col;        // column index / scale / n_clauses
-  int32_t a;          // E_SELECT: has_else; first clause index in `clauses`
+  int32_t a;          // E_SELECT: has_else; E_COL_*: 1 = keep a null row's raw slot
+                      // (a same-typed IfThen branch, which arrow does not cast)
   int32_t b;          // E_SELECT: first clause
   double f;
   int64_t lo, hi;     // i128 literal
@@ -242,14 +243,14 @@ __device__ inline Val eval_expr(const ENode* nodes, int begin, int end, const PN
     switch (nd.op) {
       case E_COL_F64: {
         const DCol& c = cols[nd.col];
-        st[sp].f = dcol_fval(c, row);
+        st[sp].f = nd.a ? dcol_fval(c, row) : dcol_fval_cast(c, row);
         st[sp].valid = dcol_valid(c, row);
         ++sp;
         break;
       }
       case E_COL_I128: {
         const DCol& c = cols[nd.col];
-        st[sp].i = dcol_i128(c, row);
+        st[sp].i = nd.a ? dcol_i128(c, row) : dcol_i128_cast(c, row);
         st[sp].valid = dcol_valid(c, row);
         ++sp;
         break;
@@ -298,7 +299,9 @@ __device__ inline Val eval_expr(const ENode* nodes, int begin, int end, const PN
       case E_F2I: {
         double x = st[sp - 1].f;
         double t = trunc(x);
-        if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) {
+        if (!st[sp - 1].valid) {
+          st[sp - 1].i = 0;  // a cast leaves 0 in a null row's slot
+        } else if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) {
           st[sp - 1].valid = false;
           st[sp - 1].i = 0;
         } else {

@@ -46,24 +46,28 @@ __global__ void expr_kernel(const ENode* en, int begin, int end, const PNode* pn
       Val v = eval_expr(en, begin, end, pn, cl, cols, i, &ovf);
       if (ovf) atomicOr(err, DERR_RANGE);
       ok = v.valid;
+      // null rows keep the slot the reference leaves there: arithmetic fills
+      // every slot from the operands' slots, casts leave 0, a same-typed
+      // IfThen branch passes its raw slot through
       if (kind == 0) {
-        static_cast<double*>(out)[i] = ok ? v.f : 0.0;
+        static_cast<double*>(out)[i] = v.f;
       } else if (kind == 1) {
-        __int128 x = ok ? v.i : 0;
+        __int128 x = v.i;
         unsigned long long* p = static_cast<unsigned long long*>(out) + 2 * i;
         p[0] = (unsigned long long)x;
         p[1] = (unsigned long long)(x >> 64);
       } else {
-        // arrow safe cast into the target type: out-of-range -> null
+        // arrow safe cast into the target type: out-of-range -> null (slot 0)
         __int128 x;
+        bool rep = true;
         if (from_int) x = v.i;
         else {
           double t = trunc(v.f);
-          if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) ok = false;
-          x = ok ? (__int128)(long long)t : 0;
+          if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) rep = false;
+          x = rep ? (__int128)(long long)t : 0;
         }
         if (out_type == TY_F32) {
-          static_cast<float*>(out)[i] = ok ? (float)(from_int ? (double)v.i : v.f) : 0.f;
+          static_cast<float*>(out)[i] = (float)(from_int ? (double)v.i : v.f);
         } else {
           __int128 lo, hi;
           switch (out_type) {
@@ -77,11 +81,14 @@ __global__ void expr_kernel(const ENode* en, int begin, int end, const PNode* pn
             case TY_BOOL: lo = 0; hi = 1; break;
             default: lo = INT64_MIN; hi = INT64_MAX;
           }
-          if (ok && (x < lo || x > hi)) {
+          if (rep && (x < lo || x > hi)) {
             if (out_type == TY_BOOL) x = x != 0;  // numeric -> bool: non-zero is true
-            else ok = false;
+            else rep = false;
           }
-          if (!ok) x = 0;
+          if (!rep) {
+            x = 0;
+            ok = false;
+          }
           switch (out_type) {
             case TY_I8: case TY_U8: static_cast<int8_t*>(out)[i] = (int8_t)x; break;
             case TY_I16: case TY_U16: static_cast<int16_t*>(out)[i] = (int16_t)x; break;

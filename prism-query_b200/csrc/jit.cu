@@ -165,6 +165,9 @@ struct Gen {
 
   std::string fresh(const char* p) { return p + std::to_string(id++); }
 
+  // every program the plan compiler emits is covered: a miss is an engine bug
+  [[noreturn]] void gen_fail(const char* why) { fail(PRISM_ERR_INTERNAL, std::string("kernel generator: ") + why); }
+
   void konst(const std::string& decl_type, const std::string& name, const std::string& init) {
     if (have.count(name)) return;
     have[name] = true;
@@ -188,7 +191,7 @@ struct Gen {
 
   std::string col(int slot) {
     if (slot < 0 || slot >= (int)pg.cols.size()) {
-      ok = false;
+      gen_fail("column slot out of range");
       return "c0";
     }
     return "c" + std::to_string(slot);
@@ -245,7 +248,7 @@ struct Gen {
           break;
         }
         case P_AND: case P_OR: {
-          if (st.size() < 2) { ok = false; return bad; }
+          if (st.size() < 2) { gen_fail("AND/OR without two operands"); return bad; }
           auto r = st.back(); st.pop_back();
           auto l = st.back(); st.pop_back();
           out << "    bool " << v << " = " << l.first << (nd.op == P_AND ? " && " : " || ") << r.first << ", " << a
@@ -253,18 +256,18 @@ struct Gen {
           break;
         }
         case P_NOT: {
-          if (st.empty()) { ok = false; return bad; }
+          if (st.empty()) { gen_fail("NOT without an operand"); return bad; }
           auto x = st.back(); st.pop_back();
           out << "    bool " << v << " = !" << x.first << ", " << a << " = " << x.second << ";\n";
           break;
         }
         default:
-          ok = false;
+          gen_fail("unknown predicate node");
           return bad;
       }
       st.push_back({v, a});
     }
-    if (st.size() != 1) { ok = false; return bad; }
+    if (st.size() != 1) { gen_fail("predicate leaves more than one value"); return bad; }
     return st.back();
   }
 
@@ -281,7 +284,7 @@ struct Gen {
       const ENode& nd = pg.enodes[k];
       std::string n = fresh("e"), K = std::to_string(k);
       auto pop = [&]() -> EV {
-        if (st.empty()) { ok = false; return EV{"e_bad", Mag{}}; }
+        if (st.empty()) { gen_fail("expression stack underflow"); return EV{"e_bad", Mag{}}; }
         EV x = st.back();
         st.pop_back();
         return x;
@@ -289,8 +292,8 @@ struct Gen {
       switch (nd.op) {
         case E_COL_F64: {
           std::string c = col(nd.col);
-          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = dcol_fval(" << c << ", idx); " << n
-              << ".valid = dcol_valid(" << c << ", idx);\n";
+          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = " << (nd.a ? "dcol_fval(" : "dcol_fval_cast(")
+              << c << ", idx); " << n << ".valid = dcol_valid(" << c << ", idx);\n";
           st.push_back({n, Mag{}});
           break;
         }
@@ -298,8 +301,8 @@ struct Gen {
           std::string c = col(nd.col);
           const Column& cc = *b.cols[pg.cols[std::max(0, std::min(nd.col, (int)pg.cols.size() - 1))]];
           int t = cc.type == TY_DICT ? cc.index_type : cc.type;
-          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = dcol_i128(" << c << ", idx); " << n
-              << ".valid = dcol_valid(" << c << ", idx);\n";
+          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = " << (nd.a ? "dcol_i128(" : "dcol_i128_cast(")
+              << c << ", idx); " << n << ".valid = dcol_valid(" << c << ", idx);\n";
           st.push_back({n, type_mag(t)});
           break;
         }
@@ -383,15 +386,15 @@ struct Gen {
         }
         case E_F2I: {
           EV x = pop();
-          out << "    Val " << n << " = " << x.n << "; { double t = trunc(" << x.n
-              << ".f); if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) { " << n
+          out << "    Val " << n << " = " << x.n << "; { double t = trunc(" << x.n << ".f); if (!" << x.n << ".valid) { "
+              << n << ".i = 0; } else if (!(t >= -9.223372036854775808e18 && t < 9.223372036854775808e18)) { " << n
               << ".valid = false; " << n << ".i = 0; } else { " << n << ".i = (__int128)(long long)t; } }\n";
           st.push_back({n, mag_of((unsigned __int128)1 << 63)});
           break;
         }
         case E_SELECT: {
           int nc = nd.col, has_else = nd.a, need = nc + has_else;
-          if ((int)st.size() < need || nc < 0) { ok = false; return "e_bad"; }
+          if ((int)st.size() < need || nc < 0) { gen_fail("IfThen without its branches"); return "e_bad"; }
           int base = (int)st.size() - need;
           Mag bound = mag_of(0);
           for (int q = base; q < (int)st.size(); ++q) bound = mag_max(bound, st[q].mag);
@@ -401,7 +404,7 @@ struct Gen {
           // the first clause that holds wins: evaluate from the last one
           // backwards, each match overriding
           for (int ci = nc - 1; ci >= 0; --ci) {
-            if (nd.b + ci < 0 || nd.b + ci >= (int)pg.clauses.size()) { ok = false; return "e_bad"; }
+            if (nd.b + ci < 0 || nd.b + ci >= (int)pg.clauses.size()) { gen_fail("IfThen clause out of range"); return "e_bad"; }
             const PRange& cl = pg.clauses[nd.b + ci];
             out << "    {\n";
             auto pv = pred(cl.begin, cl.len);
@@ -413,11 +416,11 @@ struct Gen {
           break;
         }
         default:
-          ok = false;
+          gen_fail("unknown expression node");
           return "e_bad";
       }
     }
-    if (st.size() != 1) { ok = false; return "e_bad"; }
+    if (st.size() != 1) { gen_fail("expression leaves more than one value"); return "e_bad"; }
     return st.back().n;
   }
 
@@ -517,17 +520,17 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     switch (sr.kind) {
       case S_COL_F64: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.f = dcol_fval(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.f = dcol_fval_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
         break;
       }
       case S_COL_INT: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.i = dcol_ival(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.i = dcol_ival_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
         break;
       }
       case S_COL_I128: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.i = dcol_i128(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.i = dcol_i128_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
         break;
       }
       case S_VALID: {

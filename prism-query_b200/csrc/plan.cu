@@ -314,7 +314,11 @@ struct Compiler {
     fail(PRISM_ERR_INVALID_ARGUMENT, "unknown expression op");
   }
 
-  void emit_select(const ETree& t, bool exact, int target) {
+  // raw_slots: the select is a top-level output column of type `target`, so a
+  // branch that is a bare column of that type reaches the output uncast and
+  // keeps its null rows' raw slots (filter_project.rs:277-288: only branches
+  // of another type are cast)
+  void emit_select(const ETree& t, bool exact, int target, bool raw_slots = false) {
     const prism_expr_node& nd = *t.nd;
     if (nd.n_clauses == 0) {
       if (exact) emit_exact(*t.kids.back());
@@ -328,6 +332,7 @@ struct Compiler {
       } else {
         emit_branch_f64(*k, int_target);
       }
+      if (raw_slots && k->nd->op == PRISM_EXPR_COLUMN && arrow_type(*k) == target) p.enodes.back().a = 1;
     }
     int begin = (int)p.clauses.size();
     for (int ci = 0; ci < nd.n_clauses; ++ci) {
@@ -399,12 +404,12 @@ struct Compiler {
         if (target == TY_DICT) fail(PRISM_ERR_ARROW, "Cast error: dictionary IfThen branches are not supported");
         c.begin = (int)p.enodes.size();
         if (target == TY_F64 || target == TY_F32 || target == TY_DEC128) {
-          emit_select(t, false, target);
+          emit_select(t, false, target, /*raw_slots=*/true);
           c.kind = EK_F64;
           c.out_type = TY_F64;
           if (target != TY_F64) { c.kind = EK_CAST; c.out_type = target; }
         } else {
-          emit_select(t, true, target);
+          emit_select(t, true, target, /*raw_slots=*/true);
           c.kind = EK_CAST;
           c.out_type = target;
         }

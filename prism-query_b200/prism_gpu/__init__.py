@@ -73,6 +73,7 @@ def _declare(lib):
     lib.prism_version.restype = C.c_char_p
     lib.prism_ctx_set_profiling.argtypes = [P, I]
     lib.prism_ctx_kernel_stats.argtypes = [P, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    lib.prism_jit_stats.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     lib.prism_batch_import.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_import_device.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_export.argtypes = [P, P, P, P]
@@ -177,6 +178,13 @@ class Context:
 
 
 _default_ctx: Optional[Context] = None
+
+
+def jit_stats():
+    """(enabled, compiles, total compile ms) of the run-time kernel compiler."""
+    e, n, ms = C.c_int32(0), C.c_int64(0), C.c_double(0)
+    lib().prism_jit_stats(C.byref(e), C.byref(n), C.byref(ms))
+    return bool(e.value), int(n.value), float(ms.value)
 
 
 def default_context() -> Context:

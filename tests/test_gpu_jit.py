@@ -140,7 +140,7 @@ def test_generated_kernel_exact(prof, case, nulls):
     pred, exprs = EXACT_CASES[case]
     bs = [table(70_000, 21 + k, nulls) for k in range(2)]
     got, ref, ran = run_both(prof, bs, pred, exprs, ARITH_EXACT)
-    assert ran == len(bs)
+    assert ran == len(bs), (prism_gpu.jit_stats(), prof.kernel_stats("agg_kernel"))
     assert_batches_equal(got, ref, float_cols=float_cols(ref))
 
 
