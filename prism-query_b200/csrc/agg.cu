@@ -506,9 +506,15 @@ __global__ void distinct_count_kernel(AggArgs a, int table, unsigned long long* 
 // ---------------------------------------------------------------- host ----
 namespace {
 
-// register budget of a generated small-groups kernel's per-thread
-// accumulators: two words per op and group, four with a Float64 SUM present
-bool tiny_fits_registers(int G, int nops, bool f64) { return G * nops * (f64 ? 4 : 2) + G <= 136; }
+// register budget of a generated small-groups kernel: it holds TINY_R rows'
+// operands per thread (a 128-bit integer and its null flag for integer sums,
+// a double or key for the others)
+bool tiny_fits_registers(const AggArgs& A) {
+  int regs = 0;
+  for (int j = 0; j < A.n_ops; ++j)
+    regs += TINY_R * (A.op[j].kind == O_SUM_INT || A.op[j].kind == O_SUM_DEC ? 5 : A.op[j].kind == O_NONNULL ? 1 : 3);
+  return regs <= 96;
+}
 
 bool int_like(int t) {
   return t == TY_I8 || t == TY_I16 || t == TY_I32 || t == TY_I64 || t == TY_U8 || t == TY_U16 || t == TY_U32 ||
@@ -907,7 +913,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   bool any_f64 = false;
   for (int j = 0; j < A.n_ops; ++j) any_f64 |= A.op[j].kind == O_SUM_F64;
   bool tiny = dense && G <= 8 && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 &&
-              tiny_fits_registers((int)G, A.n_ops, any_f64) && jit_enabled();
+              tiny_fits_registers(A) && jit_enabled();
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
   for (int attempt = 0; attempt < 40; ++attempt) {
@@ -989,31 +995,12 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         if (!src.empty()) jk = jit_get(src, "prism_tiny_agg");
       }
       if (jk) {
-        // stage every program column through shared memory when all are
-        // fixed width, null-free and 16-byte aligned
         a.n_cols = (int)pg.cols.size();
-        a.n_stage = 0;
-        bool stage_ok = a.n_cols <= TINY_MAX_COLS;
-        int off = 0;
-        for (int k = 0; stage_ok && k < a.n_cols; ++k) {
-          const Column& c = *b.cols[pg.cols[k]];
-          int w = width_of(c.type == TY_DICT ? c.index_type : c.type);
-          if (w == 0 || c.validity || (reinterpret_cast<uintptr_t>(c.values) & 15)) stage_ok = false;
-          a.stage_w[k] = w;
-          a.stage_off[k] = off;
-          off += (TINY_T * w + 15) & ~15;
-        }
-        size_t tsmem = 0;
-        if (stage_ok && (size_t)off * TINY_STAGES <= smem_budget) {
-          a.n_stage = a.n_cols;
-          a.stage_bytes = off;
-          tsmem = (size_t)off * TINY_STAGES;
-        }
-        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, TINY_T), (int64_t)ctx.sm_count);
-        PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)TINY_BLOCK * TINY_R),
+                                           (int64_t)ctx.sm_count * 2);
         void* params[] = {&a};
         KernelTimer kt(ctx, "agg_tiny_jit");
-        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, tsmem, ctx.stream));
+        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, 0, ctx.stream));
       } else {
         KernelTimer kt(ctx, "agg_kernel");
         agg_kernel<<<grid, block, smem, ctx.stream>>>(a);

@@ -71,13 +71,7 @@ struct AggArgs {
   int32_t ss_log2;
   int32_t sd;
   int32_t use_smem;
-  // few dense groups (tiny_body): input tiles staged into shared memory
-  // (every program column fixed width, null-free, 16-byte aligned) or read
-  // in place when n_stage == 0
-  int32_t n_stage;
-  int32_t stage_w[8];
-  int32_t stage_off[8];
-  int32_t stage_bytes;
+  // few dense groups (tiny_body): number of program columns in `cols`
   int32_t n_cols;
   // global table
   unsigned long long* gkeys;
@@ -154,32 +148,25 @@ __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (
 
 // ------------------------------------------------ few dense groups (<= 8) --
 // The kernel body for GROUP BY with at most 8 dense groups (dictionary keys,
-// or none). Each thread keeps its own accumulators for every group in
-// registers: integer-sum partials in int64 that spill exactly into the
-// block's shared 128-bit accumulators when a row would overflow them,
-// double-double Float64 partials, MIN/MAX totalOrder keys and row counts.
-// Rows never contend on shared addresses; at the end each warp reduces with
-// shuffles and one lane per warp merges into the block's and then the global
-// exact accumulators (the same words agg_kernel fills, so the same finalize
-// kernels run). Input tiles stream through a 3-stage shared-memory ring
-// filled by cp.async (16-byte chunks, zero-filled tail), so the loads of the
-// next tiles are in flight while the current one is evaluated.
+// or none). Each warp takes 32 consecutive rows per sub-step, TINY_R
+// sub-steps at a time (coalesced loads of all of them first, so that many
+// bytes are in flight), then folds the rows into the groups with warp-wide
+// reductions: per group a ballot gives the row count, and a butterfly of
+// shuffles sums / min-maxes the operands of the rows in that group. Lane 0
+// keeps the warp's running totals in shared memory (exact 128-bit integer
+// sums, double-double Float64 sums, totalOrder MIN/MAX keys, counts) and
+// merges them into the global accumulators once at the end, into the same
+// words agg_kernel fills, so the same finalize kernels run. Per row the
+// cost is the row's own arithmetic plus a few instructions per group,
+// instead of one read-modify-write per accumulator.
 //
 // E supplies the row logic as straight-line code generated per query
 // (jit.cu): E::Consts / E::load (per-thread constants read once), E::keep
 // (filter), E::gid (dense group id), E::kind (op kind of j), E::value (op
 // j's operand).
-constexpr int TINY_BLOCK = 256;  // 8 warps, up to 255 registers a thread
-constexpr int TINY_T = 2048;     // rows per tile
-constexpr int TINY_STAGES = 3;
-constexpr int TINY_MAX_COLS = 8;
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, int src_bytes) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
+constexpr int TINY_BLOCK = 256;  // 8 warps; two blocks per SM
+constexpr int TINY_R = 4;        // 32-row sub-steps per warp step
+constexpr int TINY_MAX_COLS = 16;
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
@@ -187,228 +174,195 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
   e = (a - (s - bb)) + (b - bb);
 }
 
-// limbs of an integer-sum op: int64 inputs use 2 (low 32 bits, signed rest),
-// 128-bit decimal inputs 4
-__device__ __forceinline__ int int_limbs(int kind) { return kind == O_SUM_INT ? 2 : 4; }
+__device__ __forceinline__ long long warp_sum64(long long x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+  return x;
+}
 
-// One row's contribution to a thread's accumulator of op j in group g.
-template <bool F64>
-__device__ __forceinline__ void tiny_apply(const AggArgs& a, int kind, long long& w0, long long& w1, const Val& v,
-                                           int j, int g, unsigned long long* sacc) {
-  if (a.skip_nulls && !v.valid) return;
-  switch (kind) {
-    case O_SUM_INT: case O_SUM_DEC: {
-      long long x = (long long)v.i;
-      long long r = (long long)((unsigned long long)w0 + (unsigned long long)x);
-      bool fits = (__int128)x == v.i && !(((w0 ^ r) & (x ^ r)) < 0);
-      if (fits) {
-        w0 = r;
-      } else {  // exact spill of partial + value, partial restarts at 0
-        add_i128_limbs(sacc + (g * 8 + j) * 4, (__int128)w0 + v.i, int_limbs(kind));
-        w0 = 0;
-      }
-      break;
-    }
-    case O_SUM_F64:
-      if (F64) {
-        if (!isfinite(v.f)) {  // NaN / inf: flag straight into the global accumulator
-          uint64_t u = (uint64_t)__double_as_longlong(v.f);
-          atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(v.f) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
-          break;
-        }
-        double s, e;
-        two_sum(__longlong_as_double(w0), v.f, s, e);
-        w0 = __double_as_longlong(s);
-        w1 = __double_as_longlong(__longlong_as_double(w1) + e);
-      }
-      break;
-    case O_MIN:
-      if (!isnan(v.f)) w0 = min(w0, (long long)total_key(v.f));
-      break;
-    case O_MAX:
-      if (!isnan(v.f)) w0 = max(w0, (long long)total_key(v.f));
-      break;
-    case O_NONNULL:
-      w0 += v.valid ? 1 : 0;
-      break;
+__device__ __forceinline__ __int128 warp_sum128(__int128 x) {
+  unsigned long long lo = (unsigned long long)x, hi = (unsigned long long)((unsigned __int128)x >> 64);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    unsigned long long olo = __shfl_xor_sync(0xffffffffu, lo, d), ohi = __shfl_xor_sync(0xffffffffu, hi, d);
+    unsigned long long s = lo + olo;
+    hi = hi + ohi + (s < lo ? 1ULL : 0ULL);
+    lo = s;
+  }
+  return (__int128)(((unsigned __int128)hi << 64) | lo);
+}
+
+// double-double sum across the warp (error-free two_sum at every step)
+__device__ __forceinline__ void warp_sum_dd(double& h, double& l) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    double oh = __shfl_xor_sync(0xffffffffu, h, d), ol = __shfl_xor_sync(0xffffffffu, l, d), s, e;
+    two_sum(h, oh, s, e);
+    e += l + ol;
+    h = s + e;
+    l = e - (h - s);
   }
 }
 
-// issues the asynchronous copies of tile t into ring stage `stage` (always
-// commits a group, empty past the last tile, so group counting stays uniform)
-__device__ __forceinline__ void tiny_issue(const AggArgs& a, int64_t t, int stage, int64_t n_tiles,
-                                           unsigned char* ring) {
-  if (t < n_tiles) {
-    int64_t r0 = t * TINY_T;
-    int64_t rows = a.n - r0 < TINY_T ? a.n - r0 : TINY_T;
-    unsigned char* sb = ring + (size_t)stage * a.stage_bytes;
-    for (int k = 0; k < a.n_stage; ++k) {
-      int w = a.stage_w[k];
-      const unsigned char* src = static_cast<const unsigned char*>(a.cols[k].values) + r0 * w;
-      unsigned char* dst = sb + a.stage_off[k];
-      int bytes = (int)(rows * w);
-      int chunks = (bytes + 15) >> 4;
-      for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
-        int rem = bytes - (c << 4);
-        cp_async16(dst + (c << 4), src + (c << 4), rem >= 16 ? 16 : rem);
-      }
-    }
+__device__ __forceinline__ long long warp_minmax64(long long x, bool is_min) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    long long o = __shfl_xor_sync(0xffffffffu, x, d);
+    x = is_min ? min(x, o) : max(x, o);
   }
-  cp_async_commit();
+  return x;
 }
 
-__device__ __forceinline__ long long shfl64(long long x, int d) { return __shfl_xor_sync(0xffffffffu, x, d); }
+// per-warp running totals of one (group, op): integer sums as (lo, hi) of a
+// 128-bit value, Float64 sums as (hi, lo) doubles, MIN/MAX keys and
+// non-null counts in w[0]
+struct TinyAcc {
+  unsigned long long w[2];
+};
 
 template <class E, int G, int NOPS, bool F64>
 __device__ __forceinline__ void tiny_body(const AggArgs& a) {
-  extern __shared__ __align__(16) unsigned char tiny_smem[];
-  __shared__ unsigned long long sfirst[G];
-  __shared__ unsigned long long sacc[G * 8 * 4];  // exact spill-over of integer sums
-  __shared__ DCol shadow[TINY_STAGES][TINY_MAX_COLS];
-  const bool staged = a.n_stage > 0;
-  if (threadIdx.x < G) sfirst[threadIdx.x] = ~0ULL;
-  for (int q = threadIdx.x; q < G * 8 * 4; q += blockDim.x) sacc[q] = 0;
-  if (staged && threadIdx.x < TINY_STAGES * a.n_cols) {
-    int st = threadIdx.x / a.n_cols, k = threadIdx.x % a.n_cols;
-    DCol d = a.cols[k];
-    d.values = tiny_smem + (size_t)st * a.stage_bytes + a.stage_off[k];
-    shadow[st][k] = d;
-  }
-  uint32_t cnt[G];
-  long long w0[G][NOPS], w1[G][F64 ? NOPS : 1];
+  constexpr int WARPS = TINY_BLOCK / 32;
+  __shared__ TinyAcc acc[WARPS][G][NOPS];
+  __shared__ unsigned long long cnt[WARPS][G];
+  __shared__ DCol scols[TINY_MAX_COLS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
+  if (shared_cols && threadIdx.x < a.n_cols) scols[threadIdx.x] = a.cols[threadIdx.x];
+  if (lane == 0) {
 #pragma unroll
-  for (int g = 0; g < G; ++g) {
-    cnt[g] = 0;
-#pragma unroll
-    for (int j = 0; j < NOPS; ++j) {
-      int kind = E::kind(a, j);
-      w0[g][j] = kind == O_MIN ? 0x7fffffffffffffffLL : kind == O_MAX ? (long long)0x8000000000000000ULL : 0LL;
-      if (F64) w1[g][j] = 0;
-    }
-  }
-  uint32_t seen = 0;
-  const typename E::Consts K = E::load(a);
-  __syncthreads();
-
-  const int64_t n_tiles = (a.n + TINY_T - 1) / TINY_T;
-  int64_t my = 0;  // k-th tile of this CTA: blockIdx.x + k * gridDim.x
-  if (staged) {
-    tiny_issue(a, blockIdx.x, 0, n_tiles, tiny_smem);
-    tiny_issue(a, blockIdx.x + gridDim.x, 1, n_tiles, tiny_smem);
-  }
-  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++my) {
-    const int stage = (int)(my % TINY_STAGES);
-    const DCol* cols = a.cols;
-    int64_t r0 = t * TINY_T;
-    int64_t base = r0;  // row index base passed to the row logic
-    if (staged) {
-      tiny_issue(a, t + 2 * (int64_t)gridDim.x, (int)((my + 2) % TINY_STAGES), n_tiles, tiny_smem);
-      cp_async_wait_2();
-      __syncthreads();
-      cols = shadow[stage];
-      base = 0;
-    }
-    int64_t rows = a.n - r0 < TINY_T ? a.n - r0 : TINY_T;
-    for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
-      int64_t idx = base + i;
-      if (!E::keep(a, K, cols, idx)) continue;
-      int gid = E::gid(a, K, cols, idx);
-      if (gid < 0 || gid >= G) {
-        atomicOr(a.err, DERR_RANGE);
-        continue;
-      }
-      uint64_t grow = a.row_base + (uint64_t)(r0 + i);
-#pragma unroll
-      for (int g = 0; g < G; ++g) {
-        if (gid != g) continue;
-        cnt[g] += 1;
-        if (!((seen >> g) & 1u)) {
-          seen |= 1u << g;
-          atomicMin(&sfirst[g], grow);
-        }
-      }
-      // one operand live at a time: evaluate op j's operand, fold it into
-      // the row's group, move on
+    for (int g = 0; g < G; ++g) {
+      cnt[wid][g] = 0;
 #pragma unroll
       for (int j = 0; j < NOPS; ++j) {
-        Val v = E::value(a, K, j, cols, idx);
         int kind = E::kind(a, j);
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-          if (gid == g) tiny_apply<F64>(a, kind, w0[g][j], w1[g][F64 ? j : 0], v, j, g, sacc);
-      }
-    }
-    if (staged) __syncthreads();  // the stage is refilled next iteration
-  }
-  if (staged) asm volatile("cp.async.wait_all;\n" ::: "memory");
-  // warp reduction (integer partials widened to 128 bits), then lane 0
-  // merges into the block's shared accumulators / the global words
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int g = 0; g < G; ++g) {
-    unsigned long long c64 = cnt[g];
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) c64 += (unsigned long long)shfl64((long long)c64, d);
-    unsigned long long* acc = a.gacc + (size_t)g * a.W;
-    if (lane == 0 && a.count_rows) atom_add(acc, c64);
-#pragma unroll
-    for (int j = 0; j < NOPS; ++j) {
-      int kind = E::kind(a, j);
-      unsigned long long* w = acc + a.op[j].word;
-      if (kind == O_SUM_INT || kind == O_SUM_DEC) {
-        long long hi = w0[g][j] < 0 ? -1 : 0, lo = w0[g][j];
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-          long long olo = shfl64(lo, d), ohi = shfl64(hi, d);
-          unsigned __int128 s = (((unsigned __int128)(unsigned long long)hi << 64) | (unsigned long long)lo) +
-                                (((unsigned __int128)(unsigned long long)ohi << 64) | (unsigned long long)olo);
-          lo = (long long)(unsigned long long)s;
-          hi = (long long)(unsigned long long)(s >> 64);
-        }
-        if (lane == 0)
-          add_i128_limbs(sacc + (g * 8 + j) * 4,
-                         (__int128)(((unsigned __int128)(unsigned long long)hi << 64) | (unsigned long long)lo),
-                         int_limbs(kind));
-      } else if (kind == O_SUM_F64) {
-        if (F64) {
-          double h = __longlong_as_double(w0[g][j]), l = __longlong_as_double(w1[g][F64 ? j : 0]);
-#pragma unroll
-          for (int d = 16; d > 0; d >>= 1) {
-            double oh = __shfl_xor_sync(0xffffffffu, h, d), ol = __shfl_xor_sync(0xffffffffu, l, d), s, e;
-            two_sum(h, oh, s, e);
-            e += l + ol;
-            h = s + e;
-            l = e - (h - s);
-          }
-          if (lane == 0) {  // both parts exactly into the fixed-point window
-            add_f64(w, h, a.op[j].lo_exp, a.err, a.maxexp + j);
-            add_f64(w, l, a.op[j].lo_exp, a.err, a.maxexp + j);
-          }
-        }
-      } else {
-        long long v = w0[g][j];
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-          long long o = shfl64(v, d);
-          v = kind == O_MIN ? min(v, o) : kind == O_MAX ? max(v, o) : v + o;
-        }
-        if (lane == 0) {
-          if (kind == O_MIN && v != 0x7fffffffffffffffLL) atomicMin((long long*)w, v);
-          else if (kind == O_MAX && v != (long long)0x8000000000000000ULL) atomicMax((long long*)w, v);
-          else if (kind == O_NONNULL) atom_add(w, (unsigned long long)v);
-        }
+        acc[wid][g][j].w[0] = kind == O_MIN ? 0x7fffffffffffffffULL : kind == O_MAX ? 0x8000000000000000ULL : 0ULL;
+        acc[wid][g][j].w[1] = 0;
       }
     }
   }
   __syncthreads();
-  if (threadIdx.x < G && sfirst[threadIdx.x] != ~0ULL) atomicMin(&a.gfirst[threadIdx.x], sfirst[threadIdx.x]);
-  // the block's exact integer sums into the global limbs
-  for (int q = threadIdx.x; q < G * 8 * 4; q += blockDim.x) {
-    int g = q / 32, j = (q / 4) % 8, limb = q % 4;
-    if (j < NOPS) {
-      int kind = E::kind(a, j);
-      if ((kind == O_SUM_INT || kind == O_SUM_DEC) && limb < int_limbs(kind))
-        atom_add(a.gacc + (size_t)g * a.W + a.op[j].word + limb, sacc[q]);
+  const DCol* cols = shared_cols ? scols : a.cols;
+  const typename E::Consts K = E::load(a);
+  uint32_t seen = 0;  // groups this warp has met (rows arrive in increasing order)
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = gw * 32 * TINY_R; base < a.n; base += nw * 32 * TINY_R) {
+    int gid[TINY_R];
+    Val v[TINY_R][NOPS];
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+      int64_t idx = base + r * 32 + lane;
+      bool keep = idx < a.n && E::keep(a, K, cols, idx);
+      gid[r] = -1;
+      if (keep) {
+        int g = E::gid(a, K, cols, idx);
+        if (g < 0 || g >= G) atomicOr(a.err, DERR_RANGE);
+        else gid[r] = g;
+      }
+#pragma unroll
+      for (int j = 0; j < NOPS; ++j) {
+        if (gid[r] >= 0) {
+          v[r][j] = E::value(a, K, j, cols, idx);
+        } else {
+          v[r][j].i = 0;
+          v[r][j].f = 0;
+          v[r][j].valid = false;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const unsigned m = __ballot_sync(0xffffffffu, gid[r] == g);
+        if (m == 0) continue;  // warp-uniform
+        const bool mine = gid[r] == g;
+        if (lane == 0) {
+          cnt[wid][g] += (unsigned long long)__popc(m);
+          if (!((seen >> g) & 1u)) atomicMin(&a.gfirst[g], a.row_base + (uint64_t)(base + r * 32 + __ffs(m) - 1));
+        }
+        seen |= 1u << g;
+#pragma unroll
+        for (int j = 0; j < NOPS; ++j) {
+          const int kind = E::kind(a, j);
+          const Val& x = v[r][j];
+          const bool use = mine && !(a.skip_nulls && !x.valid);
+          TinyAcc& t = acc[wid][g][j];
+          if (kind == O_SUM_INT || kind == O_SUM_DEC) {
+            __int128 y = use ? x.i : (__int128)0;
+            long long y64 = (long long)y;
+            // 32 values below 2^57 in magnitude sum exactly in 64 bits
+            bool small = (__int128)y64 == y && y64 > -(1LL << 57) && y64 < (1LL << 57);
+            __int128 s = __all_sync(0xffffffffu, small) ? (__int128)warp_sum64(y64) : warp_sum128(y);
+            if (lane == 0) {
+              unsigned __int128 cur = ((unsigned __int128)t.w[1] << 64) | t.w[0];
+              cur += (unsigned __int128)s;
+              t.w[0] = (unsigned long long)cur;
+              t.w[1] = (unsigned long long)(cur >> 64);
+            }
+          } else if (kind == O_SUM_F64) {
+            if (F64) {
+              double y = use ? x.f : 0.0;
+              if (!isfinite(y)) {  // NaN / inf: flag straight into the global accumulator
+                uint64_t u = (uint64_t)__double_as_longlong(y);
+                atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(y) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
+                y = 0.0;
+              }
+              double h = y, l = 0.0;
+              warp_sum_dd(h, l);
+              if (lane == 0) {
+                double th = __longlong_as_double((long long)t.w[0]), tl = __longlong_as_double((long long)t.w[1]);
+                double s1, e1;
+                two_sum(th, h, s1, e1);
+                e1 += tl + l;
+                double nh = s1 + e1;
+                t.w[0] = (unsigned long long)__double_as_longlong(nh);
+                t.w[1] = (unsigned long long)__double_as_longlong(e1 - (nh - s1));
+              }
+            }
+          } else if (kind == O_MIN || kind == O_MAX) {
+            const bool is_min = kind == O_MIN;
+            long long key = (use && !isnan(x.f)) ? (long long)total_key(x.f)
+                                                 : (is_min ? 0x7fffffffffffffffLL : (long long)0x8000000000000000ULL);
+            key = warp_minmax64(key, is_min);
+            if (lane == 0) t.w[0] = (unsigned long long)(is_min ? min((long long)t.w[0], key) : max((long long)t.w[0], key));
+          } else if (kind == O_NONNULL) {
+            unsigned mv = __ballot_sync(0xffffffffu, mine && x.valid);
+            if (lane == 0) t.w[0] += (unsigned long long)__popc(mv);
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  // lane 0 of each warp merges the warp's totals into the global words
+  if (lane == 0) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      unsigned long long* accg = a.gacc + (size_t)g * a.W;
+      if (a.count_rows) atom_add(accg, cnt[wid][g]);
+#pragma unroll
+      for (int j = 0; j < NOPS; ++j) {
+        const int kind = E::kind(a, j);
+        const TinyAcc& t = acc[wid][g][j];
+        unsigned long long* w = accg + a.op[j].word;
+        if (kind == O_SUM_INT || kind == O_SUM_DEC) {
+          __int128 x = (__int128)(((unsigned __int128)t.w[1] << 64) | t.w[0]);
+          add_i128_limbs(w, x, kind == O_SUM_INT ? 2 : 4);
+        } else if (kind == O_SUM_F64) {
+          if (F64) {  // both parts exactly into the fixed-point window
+            add_f64(w, __longlong_as_double((long long)t.w[0]), a.op[j].lo_exp, a.err, a.maxexp + j);
+            add_f64(w, __longlong_as_double((long long)t.w[1]), a.op[j].lo_exp, a.err, a.maxexp + j);
+          }
+        } else if (kind == O_MIN) {
+          if ((long long)t.w[0] != 0x7fffffffffffffffLL) atomicMin((long long*)w, (long long)t.w[0]);
+        } else if (kind == O_MAX) {
+          if ((long long)t.w[0] != (long long)0x8000000000000000ULL) atomicMax((long long*)w, (long long)t.w[0]);
+        } else if (kind == O_NONNULL) {
+          atom_add(w, t.w[0]);
+        }
+      }
     }
   }
 }

@@ -577,7 +577,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << "  }\n"
        "};\n"
        "}  // namespace prism\n"
-       "extern \"C\" __global__ void __launch_bounds__(prism::TINY_BLOCK, 1) prism_tiny_agg(prism::AggArgs a) {\n"
+       "extern \"C\" __global__ void __launch_bounds__(prism::TINY_BLOCK, 2) prism_tiny_agg(prism::AggArgs a) {\n"
        "  prism::tiny_body<prism::QueryRow, "
     << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false")
     << ">(a);\n"
