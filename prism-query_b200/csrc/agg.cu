@@ -516,6 +516,13 @@ bool tiny_fits_registers(const AggArgs& A) {
   return regs <= 96;
 }
 
+// words per group of the small-groups kernel's accumulator columns
+int tiny_group_words(const AggArgs& A) {
+  int nw = 1;
+  for (int j = 0; j < A.n_ops; ++j) nw += tiny_words(A.op[j].kind);
+  return nw;
+}
+
 bool int_like(int t) {
   return t == TY_I8 || t == TY_I16 || t == TY_I32 || t == TY_I64 || t == TY_U8 || t == TY_U16 || t == TY_U32 ||
          t == TY_BOOL;
@@ -913,7 +920,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   bool any_f64 = false;
   for (int j = 0; j < A.n_ops; ++j) any_f64 |= A.op[j].kind == O_SUM_F64;
   bool tiny = dense && G <= 8 && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 &&
-              tiny_fits_registers(A) && jit_enabled();
+              tiny_fits_registers(A) && G * tiny_group_words(A) <= TINY_MAX_WORDS && jit_enabled();
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
   for (int attempt = 0; attempt < 40; ++attempt) {
@@ -996,11 +1003,13 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       }
       if (jk) {
         a.n_cols = (int)pg.cols.size();
-        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)TINY_BLOCK * TINY_R),
+        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)TINY_BLOCK * TINY_R * 8),
                                            (int64_t)ctx.sm_count * 2);
+        size_t tsmem = (size_t)G * tiny_group_words(A) * TINY_BLOCK * 8;
+        PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
         void* params[] = {&a};
         KernelTimer kt(ctx, "agg_tiny_jit");
-        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, 0, ctx.stream));
+        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, tsmem, ctx.stream));
       } else {
         KernelTimer kt(ctx, "agg_kernel");
         agg_kernel<<<grid, block, smem, ctx.stream>>>(a);

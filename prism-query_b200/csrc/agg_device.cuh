@@ -148,25 +148,29 @@ __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (
 
 // ------------------------------------------------ few dense groups (<= 8) --
 // The kernel body for GROUP BY with at most 8 dense groups (dictionary keys,
-// or none). Each warp takes 32 consecutive rows per sub-step, TINY_R
-// sub-steps at a time (coalesced loads of all of them first, so that many
-// bytes are in flight), then folds the rows into the groups with warp-wide
-// reductions: per group a ballot gives the row count, and a butterfly of
-// shuffles sums / min-maxes the operands of the rows in that group. Lane 0
-// keeps the warp's running totals in shared memory (exact 128-bit integer
-// sums, double-double Float64 sums, totalOrder MIN/MAX keys, counts) and
-// merges them into the global accumulators once at the end, into the same
-// words agg_kernel fills, so the same finalize kernels run. Per row the
-// cost is the row's own arithmetic plus a few instructions per group,
-// instead of one read-modify-write per accumulator.
+// or none). Every thread owns a private column of accumulators in shared
+// memory, word w of thread t at tacc[w * TINY_BLOCK + t] (so a warp's
+// accesses never conflict, whatever groups its rows fall in): per group a
+// row count and each op's words (int64 partial of an integer sum, the two
+// doubles of a double-double Float64 sum, a totalOrder MIN/MAX key, a
+// non-null count). A row costs one read-modify-write of its own group's
+// words, independent of the number of groups. An integer partial that would
+// overflow spills exactly into the block's 128-bit accumulators. Threads
+// stride over rows so each warp loads 32 consecutive rows per step, TINY_R
+// steps deep before using them (many loads in flight). At the end the block
+// folds the columns (exact 128-bit integer sums, double-double Float64 sums)
+// and merges them into the global words agg_kernel fills, so the same
+// finalize kernels run.
 //
-// E supplies the row logic as straight-line code generated per query
-// (jit.cu): E::Consts / E::load (per-thread constants read once), E::keep
-// (filter), E::gid (dense group id), E::kind (op kind of j), E::value (op
-// j's operand).
-constexpr int TINY_BLOCK = 256;  // 8 warps; two blocks per SM
-constexpr int TINY_R = 4;        // 32-row sub-steps per warp step
+// E supplies the row logic as code generated per query (jit.cu): E::Consts /
+// E::load (per-thread constants read once), E::keep (filter), E::gid (dense
+// group id), E::value (op j's operand), and the compile-time layout kKind[j]
+// (op kinds), kWord[j] (first word of op j within a group), kNW (words per
+// group, the row count being word 0).
+constexpr int TINY_BLOCK = 256;
+constexpr int TINY_R = 4;        // rows in flight per thread
 constexpr int TINY_MAX_COLS = 16;
+constexpr int TINY_MAX_WORDS = 48;  // G * kNW: 96 KB of accumulators per block
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
@@ -174,88 +178,48 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
   e = (a - (s - bb)) + (b - bb);
 }
 
-__device__ __forceinline__ long long warp_sum64(long long x) {
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
-  return x;
-}
+// words an op occupies in a group's accumulator column
+__host__ __device__ constexpr int tiny_words(int kind) { return kind == O_SUM_F64 ? 2 : 1; }
 
-__device__ __forceinline__ __int128 warp_sum128(__int128 x) {
-  unsigned long long lo = (unsigned long long)x, hi = (unsigned long long)((unsigned __int128)x >> 64);
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    unsigned long long olo = __shfl_xor_sync(0xffffffffu, lo, d), ohi = __shfl_xor_sync(0xffffffffu, hi, d);
-    unsigned long long s = lo + olo;
-    hi = hi + ohi + (s < lo ? 1ULL : 0ULL);
-    lo = s;
-  }
-  return (__int128)(((unsigned __int128)hi << 64) | lo);
+__host__ __device__ constexpr unsigned long long tiny_init(int kind) {
+  return kind == O_MIN ? 0x7fffffffffffffffULL : kind == O_MAX ? 0x8000000000000000ULL : 0ULL;
 }
-
-// double-double sum across the warp (error-free two_sum at every step)
-__device__ __forceinline__ void warp_sum_dd(double& h, double& l) {
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    double oh = __shfl_xor_sync(0xffffffffu, h, d), ol = __shfl_xor_sync(0xffffffffu, l, d), s, e;
-    two_sum(h, oh, s, e);
-    e += l + ol;
-    h = s + e;
-    l = e - (h - s);
-  }
-}
-
-__device__ __forceinline__ long long warp_minmax64(long long x, bool is_min) {
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    long long o = __shfl_xor_sync(0xffffffffu, x, d);
-    x = is_min ? min(x, o) : max(x, o);
-  }
-  return x;
-}
-
-// per-warp running totals of one (group, op): integer sums as (lo, hi) of a
-// 128-bit value, Float64 sums as (hi, lo) doubles, MIN/MAX keys and
-// non-null counts in w[0]
-struct TinyAcc {
-  unsigned long long w[2];
-};
 
 template <class E, int G, int NOPS, bool F64>
 __device__ __forceinline__ void tiny_body(const AggArgs& a) {
-  constexpr int WARPS = TINY_BLOCK / 32;
-  __shared__ TinyAcc acc[WARPS][G][NOPS];
-  __shared__ unsigned long long cnt[WARPS][G];
+  constexpr int NW = E::kNW;
+  extern __shared__ unsigned long long tacc[];  // [G * NW][TINY_BLOCK]
+  __shared__ unsigned long long sfirst[G];
+  __shared__ unsigned long long spill[G][NOPS][4];  // exact overflow of integer partials
   __shared__ DCol scols[TINY_MAX_COLS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = threadIdx.x;
   const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
-  if (shared_cols && threadIdx.x < a.n_cols) scols[threadIdx.x] = a.cols[threadIdx.x];
-  if (lane == 0) {
+  if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
+  if (tid < G) sfirst[tid] = ~0ULL;
+  for (int q = tid; q < G * NOPS * 4; q += TINY_BLOCK) (&spill[0][0][0])[q] = 0;
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-      cnt[wid][g] = 0;
+  for (int g = 0; g < G; ++g) {
+    tacc[(g * NW) * TINY_BLOCK + tid] = 0;
 #pragma unroll
-      for (int j = 0; j < NOPS; ++j) {
-        int kind = E::kind(a, j);
-        acc[wid][g][j].w[0] = kind == O_MIN ? 0x7fffffffffffffffULL : kind == O_MAX ? 0x8000000000000000ULL : 0ULL;
-        acc[wid][g][j].w[1] = 0;
-      }
+    for (int j = 0; j < NOPS; ++j) {
+      tacc[(g * NW + E::kWord[j]) * TINY_BLOCK + tid] = tiny_init(E::kKind[j]);
+      if (tiny_words(E::kKind[j]) == 2) tacc[(g * NW + E::kWord[j] + 1) * TINY_BLOCK + tid] = 0;
     }
   }
   __syncthreads();
   const DCol* cols = shared_cols ? scols : a.cols;
   const typename E::Consts K = E::load(a);
-  uint32_t seen = 0;  // groups this warp has met (rows arrive in increasing order)
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = gw * 32 * TINY_R; base < a.n; base += nw * 32 * TINY_R) {
+  unsigned long long* my = tacc + tid;
+  uint32_t seen = 0;
+  const int64_t stride = (int64_t)gridDim.x * TINY_BLOCK;
+  for (int64_t base = blockIdx.x * (int64_t)TINY_BLOCK + tid; base < a.n; base += stride * TINY_R) {
     int gid[TINY_R];
     Val v[TINY_R][NOPS];
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-      int64_t idx = base + r * 32 + lane;
-      bool keep = idx < a.n && E::keep(a, K, cols, idx);
+      int64_t idx = base + r * stride;
       gid[r] = -1;
-      if (keep) {
+      if (idx < a.n && E::keep(a, K, cols, idx)) {
         int g = E::gid(a, K, cols, idx);
         if (g < 0 || g >= G) atomicOr(a.err, DERR_RANGE);
         else gid[r] = g;
@@ -273,96 +237,101 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-#pragma unroll
-      for (int g = 0; g < G; ++g) {
-        const unsigned m = __ballot_sync(0xffffffffu, gid[r] == g);
-        if (m == 0) continue;  // warp-uniform
-        const bool mine = gid[r] == g;
-        if (lane == 0) {
-          cnt[wid][g] += (unsigned long long)__popc(m);
-          if (!((seen >> g) & 1u)) atomicMin(&a.gfirst[g], a.row_base + (uint64_t)(base + r * 32 + __ffs(m) - 1));
-        }
+      const int g = gid[r];
+      if (g < 0) continue;
+      if (!((seen >> g) & 1u)) {
         seen |= 1u << g;
+        atomicMin(&sfirst[g], a.row_base + (uint64_t)(base + r * stride));
+      }
+      unsigned long long* col = my + (size_t)(g * NW) * TINY_BLOCK;
+      col[0] += 1;
 #pragma unroll
-        for (int j = 0; j < NOPS; ++j) {
-          const int kind = E::kind(a, j);
-          const Val& x = v[r][j];
-          const bool use = mine && !(a.skip_nulls && !x.valid);
-          TinyAcc& t = acc[wid][g][j];
-          if (kind == O_SUM_INT || kind == O_SUM_DEC) {
-            __int128 y = use ? x.i : (__int128)0;
-            long long y64 = (long long)y;
-            // 32 values below 2^57 in magnitude sum exactly in 64 bits
-            bool small = (__int128)y64 == y && y64 > -(1LL << 57) && y64 < (1LL << 57);
-            __int128 s = __all_sync(0xffffffffu, small) ? (__int128)warp_sum64(y64) : warp_sum128(y);
-            if (lane == 0) {
-              unsigned __int128 cur = ((unsigned __int128)t.w[1] << 64) | t.w[0];
-              cur += (unsigned __int128)s;
-              t.w[0] = (unsigned long long)cur;
-              t.w[1] = (unsigned long long)(cur >> 64);
-            }
-          } else if (kind == O_SUM_F64) {
-            if (F64) {
-              double y = use ? x.f : 0.0;
-              if (!isfinite(y)) {  // NaN / inf: flag straight into the global accumulator
-                uint64_t u = (uint64_t)__double_as_longlong(y);
-                atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(y) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
-                y = 0.0;
-              }
-              double h = y, l = 0.0;
-              warp_sum_dd(h, l);
-              if (lane == 0) {
-                double th = __longlong_as_double((long long)t.w[0]), tl = __longlong_as_double((long long)t.w[1]);
-                double s1, e1;
-                two_sum(th, h, s1, e1);
-                e1 += tl + l;
-                double nh = s1 + e1;
-                t.w[0] = (unsigned long long)__double_as_longlong(nh);
-                t.w[1] = (unsigned long long)__double_as_longlong(e1 - (nh - s1));
-              }
-            }
-          } else if (kind == O_MIN || kind == O_MAX) {
-            const bool is_min = kind == O_MIN;
-            long long key = (use && !isnan(x.f)) ? (long long)total_key(x.f)
-                                                 : (is_min ? 0x7fffffffffffffffLL : (long long)0x8000000000000000ULL);
-            key = warp_minmax64(key, is_min);
-            if (lane == 0) t.w[0] = (unsigned long long)(is_min ? min((long long)t.w[0], key) : max((long long)t.w[0], key));
-          } else if (kind == O_NONNULL) {
-            unsigned mv = __ballot_sync(0xffffffffu, mine && x.valid);
-            if (lane == 0) t.w[0] += (unsigned long long)__popc(mv);
+      for (int j = 0; j < NOPS; ++j) {
+        const int kind = E::kKind[j];
+        const Val& x = v[r][j];
+        if (a.skip_nulls && !x.valid) continue;
+        unsigned long long* w = col + (size_t)E::kWord[j] * TINY_BLOCK;
+        if (kind == O_SUM_INT || kind == O_SUM_DEC) {
+          long long x64 = (long long)x.i;
+          long long p = (long long)w[0];
+          long long s = (long long)((unsigned long long)p + (unsigned long long)x64);
+          if ((__int128)x64 == x.i && !(((p ^ s) & (x64 ^ s)) < 0)) {
+            w[0] = (unsigned long long)s;
+          } else {  // exact spill of partial + value; the partial restarts at 0
+            add_i128_limbs(&spill[g][j][0], (__int128)p + x.i, kind == O_SUM_INT ? 2 : 4);
+            w[0] = 0;
           }
+        } else if (kind == O_SUM_F64) {
+          if (F64) {
+            if (!isfinite(x.f)) {  // NaN / inf: flag straight into the global accumulator
+              uint64_t u = (uint64_t)__double_as_longlong(x.f);
+              atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(x.f) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
+            } else {
+              double s, e;
+              two_sum(__longlong_as_double((long long)w[0]), x.f, s, e);
+              w[0] = (unsigned long long)__double_as_longlong(s);
+              w[TINY_BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[TINY_BLOCK]) + e);
+            }
+          }
+        } else if (kind == O_MIN) {
+          if (!isnan(x.f)) w[0] = (unsigned long long)min((long long)w[0], (long long)total_key(x.f));
+        } else if (kind == O_MAX) {
+          if (!isnan(x.f)) w[0] = (unsigned long long)max((long long)w[0], (long long)total_key(x.f));
+        } else if (kind == O_NONNULL) {
+          w[0] += x.valid ? 1ULL : 0ULL;
         }
       }
     }
   }
-  __syncwarp();
-  // lane 0 of each warp merges the warp's totals into the global words
-  if (lane == 0) {
+  __syncthreads();
+  if (tid < G && sfirst[tid] != ~0ULL) atomicMin(&a.gfirst[tid], sfirst[tid]);
+  // fold the thread columns: one item per (group, count or op)
+  for (int q = tid; q < G * (NOPS + 1); q += TINY_BLOCK) {
+    const int g = q / (NOPS + 1), jj = q % (NOPS + 1);
+    unsigned long long* accg = a.gacc + (size_t)g * a.W;
+    const unsigned long long* row = tacc + (size_t)(g * NW) * TINY_BLOCK;
+    if (jj == 0) {
+      unsigned long long c = 0;
+      for (int t = 0; t < TINY_BLOCK; ++t) c += row[t];
+      if (a.count_rows) atom_add(accg, c);
+      continue;
+    }
+    const int j = jj - 1;
+    int kind = 0, word = 0;
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-      unsigned long long* accg = a.gacc + (size_t)g * a.W;
-      if (a.count_rows) atom_add(accg, cnt[wid][g]);
-#pragma unroll
-      for (int j = 0; j < NOPS; ++j) {
-        const int kind = E::kind(a, j);
-        const TinyAcc& t = acc[wid][g][j];
-        unsigned long long* w = accg + a.op[j].word;
-        if (kind == O_SUM_INT || kind == O_SUM_DEC) {
-          __int128 x = (__int128)(((unsigned __int128)t.w[1] << 64) | t.w[0]);
-          add_i128_limbs(w, x, kind == O_SUM_INT ? 2 : 4);
-        } else if (kind == O_SUM_F64) {
-          if (F64) {  // both parts exactly into the fixed-point window
-            add_f64(w, __longlong_as_double((long long)t.w[0]), a.op[j].lo_exp, a.err, a.maxexp + j);
-            add_f64(w, __longlong_as_double((long long)t.w[1]), a.op[j].lo_exp, a.err, a.maxexp + j);
-          }
-        } else if (kind == O_MIN) {
-          if ((long long)t.w[0] != 0x7fffffffffffffffLL) atomicMin((long long*)w, (long long)t.w[0]);
-        } else if (kind == O_MAX) {
-          if ((long long)t.w[0] != (long long)0x8000000000000000ULL) atomicMax((long long*)w, (long long)t.w[0]);
-        } else if (kind == O_NONNULL) {
-          atom_add(w, t.w[0]);
+    for (int k = 0; k < NOPS; ++k)
+      if (k == j) { kind = E::kKind[k]; word = E::kWord[k]; }
+    const unsigned long long* w = row + (size_t)word * TINY_BLOCK;
+    unsigned long long* gw = accg + a.op[j].word;
+    if (kind == O_SUM_INT || kind == O_SUM_DEC) {
+      __int128 s = 0;
+      for (int t = 0; t < TINY_BLOCK; ++t) s += (__int128)(long long)w[t];
+      for (int l = 0; l < 4; ++l) s += (__int128)(long long)spill[g][j][l] << (32 * l);
+      add_i128_limbs(gw, s, kind == O_SUM_INT ? 2 : 4);
+    } else if (kind == O_SUM_F64) {
+      if (F64) {
+        double h = 0, l = 0;
+        for (int t = 0; t < TINY_BLOCK; ++t) {
+          double s1, e1;
+          two_sum(h, __longlong_as_double((long long)w[t]), s1, e1);
+          e1 += l + __longlong_as_double((long long)w[t + TINY_BLOCK]);
+          h = s1 + e1;
+          l = e1 - (h - s1);
         }
+        add_f64(gw, h, a.op[j].lo_exp, a.err, a.maxexp + j);  // both parts exactly into the window
+        add_f64(gw, l, a.op[j].lo_exp, a.err, a.maxexp + j);
       }
+    } else if (kind == O_MIN || kind == O_MAX) {
+      long long m = (long long)tiny_init(kind);
+      for (int t = 0; t < TINY_BLOCK; ++t) m = kind == O_MIN ? min(m, (long long)w[t]) : max(m, (long long)w[t]);
+      if (m != (long long)tiny_init(kind)) {
+        if (kind == O_MIN) atomicMin((long long*)gw, m);
+        else atomicMax((long long*)gw, m);
+      }
+    } else if (kind == O_NONNULL) {
+      unsigned long long c = 0;
+      for (int t = 0; t < TINY_BLOCK; ++t) c += w[t];
+      atom_add(gw, c);
     }
   }
 }

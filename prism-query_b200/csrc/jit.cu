@@ -510,11 +510,14 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   // operands
   gen.declare_cols();
   gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
-  std::ostringstream kinds;
+  std::ostringstream kinds, words;
+  int nw = 1;  // word 0 of a group: its row count
   for (int j = 0; j < a.n_ops; ++j) {
     const Op& o = a.op[j];
     if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) return "";
-    kinds << "    if (j == " << j << ") return " << o.kind << ";\n";
+    kinds << (j ? ", " : "") << o.kind;
+    words << (j ? ", " : "") << nw;
+    nw += tiny_words(o.kind);
     const Src& sr = a.src[o.src];
     gen.out << "    " << (j ? "else " : "") << "if (j == " << j << ") {\n";
     switch (sr.kind) {
@@ -568,9 +571,9 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
     << gid
     << "  }\n"
-       "  static __device__ __forceinline__ int kind(const AggArgs& a, int j) {\n"
-    << kinds.str()
-    << "    return 0;\n  }\n"
+       "  static constexpr int kNW = "
+    << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
+    << a.n_ops << "] = {" << words.str() << "};\n"
        "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "int64_t idx) {\n"
     << value
