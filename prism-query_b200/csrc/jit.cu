@@ -424,6 +424,111 @@ struct Gen {
     return st.back().n;
   }
 
+  // 64-bit fast path of an exact (int128) program: the same values computed
+  // in int64 with an overflow flag per step; exact whenever no step
+  // overflowed (then `ok` stays true). Emits into `out`; returns the names
+  // of the value, validity and ok variables, or false when the program has
+  // a node the fast path does not take (IfThen, Float64 steps, Decimal128 or
+  // UInt64 columns).
+  bool expr_fast64(int begin, int end, std::string& val, std::string& valid, std::string& okv) {
+    struct FV {
+      std::string n, v;
+      Mag mag;
+    };
+    for (int k = begin; k < end; ++k) {
+      int op = pg.enodes[k].op;
+      if (op == E_COL_I128) {
+        const Column& cc = *b.cols[pg.cols[std::max(0, std::min(pg.enodes[k].col, (int)pg.cols.size() - 1))]];
+        int t = cc.type == TY_DICT ? cc.index_type : cc.type;
+        if (t == TY_U64 || type_mag(t).unknown) return false;
+      } else if (op != E_LIT_I128 && op != E_ADD_I && op != E_SUB_I && op != E_MUL_I && op != E_NEG_I &&
+                 !(op == E_SCALE_I && pg.enodes[k].col <= 18)) {
+        return false;
+      }
+    }
+    const unsigned __int128 I64_MAX = ((unsigned __int128)1 << 63) - 1;
+    auto fits64 = [&](Mag m) { return !m.unknown && m.m <= I64_MAX; };
+    okv = fresh("fok");
+    out << "    bool " << okv << " = true;\n";
+    std::vector<FV> st;
+    for (int k = begin; k < end; ++k) {
+      const ENode& nd = pg.enodes[k];
+      std::string n = fresh("f"), vv = fresh("fv"), K = std::to_string(k);
+      switch (nd.op) {
+        case E_COL_I128: {
+          std::string c = col(nd.col);
+          const Column& cc = *b.cols[pg.cols[nd.col]];
+          int t = cc.type == TY_DICT ? cc.index_type : cc.type;
+          out << "    long long " << n << " = " << (nd.a ? "dcol_ival(" : "dcol_ival_cast(") << c << ", idx); bool " << vv
+              << " = dcol_valid(" << c << ", idx);\n";
+          st.push_back({n, vv, type_mag(t)});
+          break;
+        }
+        case E_LIT_I128: {
+          // bound: the literal's power-of-two ceiling, recorded in the source
+          __int128 lv = (__int128)(((unsigned __int128)(uint64_t)nd.hi << 64) | (uint64_t)nd.lo);
+          unsigned __int128 m = lv < 0 ? (unsigned __int128)0 - (unsigned __int128)lv : (unsigned __int128)lv;
+          int bits = 0;
+          while (bits < 127 && ((unsigned __int128)1 << bits) < m) ++bits;
+          konst("__int128", "ei" + K,
+                "(__int128)(((unsigned __int128)(uint64_t)a.en[" + K + "].hi << 64) | (uint64_t)a.en[" + K + "].lo)");
+          out << "    long long " << n << " = (long long)K.ei" << K << "; bool " << vv << " = true; " << okv << " = " << okv
+              << " && (__int128)" << n << " == K.ei" << K << ";  // |literal| <= 2^" << bits << "\n";
+          st.push_back({n, vv, mag_of((unsigned __int128)1 << bits)});
+          break;
+        }
+        case E_ADD_I: case E_SUB_I: case E_MUL_I: {
+          if (st.size() < 2) gen_fail("expression stack underflow");
+          FV r = st.back(); st.pop_back();
+          FV l = st.back(); st.pop_back();
+          Mag bound = nd.op == E_MUL_I ? mag_mul(l.mag, r.mag) : mag_add(l.mag, r.mag);
+          const char* o = nd.op == E_ADD_I ? "+" : nd.op == E_SUB_I ? "-" : "*";
+          out << "    long long " << n << " = (long long)((unsigned long long)" << l.n << " " << o << " (unsigned long long)"
+              << r.n << "); bool " << vv << " = " << l.v << " && " << r.v << ";\n";
+          if (!fits64(bound)) {
+            if (nd.op == E_ADD_I)
+              out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << n << ") & (" << r.n << " ^ " << n
+                  << ")) < 0);\n";
+            else if (nd.op == E_SUB_I)
+              out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
+                  << ")) < 0);\n";
+            else
+              out << "    " << okv << " = " << okv << " && __mul64hi(" << l.n << ", " << r.n << ") == (" << n
+                  << " >> 63);\n";
+            bound = Mag{};
+          }
+          st.push_back({n, vv, bound});
+          break;
+        }
+        case E_NEG_I: {
+          if (st.empty()) gen_fail("expression stack underflow");
+          FV x = st.back(); st.pop_back();
+          out << "    long long " << n << " = (long long)(0ULL - (unsigned long long)" << x.n << "); bool " << vv << " = "
+              << x.v << "; " << okv << " = " << okv << " && " << x.n << " != (long long)0x8000000000000000ULL;\n";
+          st.push_back({n, vv, x.mag});
+          break;
+        }
+        case E_SCALE_I: {
+          if (st.empty()) gen_fail("expression stack underflow");
+          FV x = st.back(); st.pop_back();
+          long long p10 = 1;
+          for (int q = 0; q < nd.col; ++q) p10 *= 10;
+          out << "    long long " << n << " = (long long)((unsigned long long)" << x.n << " * " << p10 << "ULL); bool " << vv
+              << " = " << x.v << "; " << okv << " = " << okv << " && __mul64hi(" << x.n << ", " << p10 << "LL) == (" << n
+              << " >> 63);\n";
+          st.push_back({n, vv, Mag{}});
+          break;
+        }
+        default:
+          gen_fail("unknown expression node");
+      }
+    }
+    if (st.size() != 1) gen_fail("expression leaves more than one value");
+    val = st.back().n;
+    valid = st.back().v;
+    return true;
+  }
+
   std::string take() {
     std::string s = out.str();
     out.str("");
@@ -510,7 +615,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   // operands
   gen.declare_cols();
   gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
-  std::ostringstream kinds, words;
+  std::ostringstream kinds, words, slow;
   int nw = 1;  // word 0 of a group: its row count
   for (int j = 0; j < a.n_ops; ++j) {
     const Op& o = a.op[j];
@@ -542,9 +647,26 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
         break;
       }
       default: {
-        gen.out << "    bool ovf = false;\n";
-        std::string v = gen.expr(sr.begin, sr.end, "ovf");
-        gen.out << "    r = " << v << ";\n    if (ovf) atomicOr(a.err, DERR_RANGE);\n";
+        std::string fval, fvalid, fok;
+        bool fast = sr.kind == S_EXPR_I128 && gen.expr_fast64(sr.begin, sr.end, fval, fvalid, fok);
+        if (fast) {
+          // 64-bit steps first; the 128-bit program (out of line, so it costs
+          // the hot loop no registers) runs only when one of them overflowed
+          gen.out << "    if (" << fok << ") { r.i = (__int128)" << fval << "; r.valid = " << fvalid << "; } else {\n"
+                  << "    r = slow" << j << "(a, K, cols, idx);\n    }\n";
+          std::string body = gen.take();
+          gen.declare_cols();
+          gen.out << "    bool ovf = false;\n";
+          std::string v = gen.expr(sr.begin, sr.end, "ovf");
+          gen.out << "    if (ovf) atomicOr(a.err, DERR_RANGE);\n    return " << v << ";\n";
+          slow << "  static __device__ __noinline__ Val slow" << j
+               << "(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n" << gen.take() << "  }\n";
+          gen.out << body;
+        } else {
+          gen.out << "    bool ovf = false;\n";
+          std::string v = gen.expr(sr.begin, sr.end, "ovf");
+          gen.out << "    r = " << v << ";\n    if (ovf) atomicOr(a.err, DERR_RANGE);\n";
+        }
       }
     }
     gen.out << "    }\n";
@@ -574,7 +696,8 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
-       "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
+    << slow.str()
+    << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "int64_t idx) {\n"
     << value
     << "  }\n"
