@@ -518,7 +518,7 @@ bool tiny_fits_registers(const AggArgs& A) {
 
 // words per group of the small-groups kernel's accumulator columns
 int tiny_group_words(const AggArgs& A) {
-  int nw = 1;
+  int nw = TINY_FIRST_OP_WORD;
   for (int j = 0; j < A.n_ops; ++j) nw += tiny_words(A.op[j].kind);
   return nw;
 }
@@ -920,7 +920,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   bool any_f64 = false;
   for (int j = 0; j < A.n_ops; ++j) any_f64 |= A.op[j].kind == O_SUM_F64;
   bool tiny = dense && G <= 8 && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 &&
-              tiny_fits_registers(A) && G * tiny_group_words(A) <= TINY_MAX_WORDS && jit_enabled();
+              tiny_fits_registers(A) && (G + 1) * tiny_group_words(A) <= TINY_MAX_WORDS && jit_enabled();
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
   for (int attempt = 0; attempt < 40; ++attempt) {
@@ -1005,7 +1005,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         a.n_cols = (int)pg.cols.size();
         int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)TINY_BLOCK * TINY_R * 8),
                                            (int64_t)ctx.sm_count * 2);
-        size_t tsmem = (size_t)G * tiny_group_words(A) * TINY_BLOCK * 8;
+        size_t tsmem = (size_t)(G + 1) * tiny_group_words(A) * TINY_BLOCK * 8;
         PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
         void* params[] = {&a};
         KernelTimer kt(ctx, "agg_tiny_jit");

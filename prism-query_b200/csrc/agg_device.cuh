@@ -149,28 +149,30 @@ __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (
 // ------------------------------------------------ few dense groups (<= 8) --
 // The kernel body for GROUP BY with at most 8 dense groups (dictionary keys,
 // or none). Every thread owns a private column of accumulators in shared
-// memory, word w of thread t at tacc[w * TINY_BLOCK + t] (so a warp's
-// accesses never conflict, whatever groups its rows fall in): per group a
-// row count and each op's words (int64 partial of an integer sum, the two
-// doubles of a double-double Float64 sum, a totalOrder MIN/MAX key, a
-// non-null count). A row costs one read-modify-write of its own group's
-// words, independent of the number of groups. An integer partial that would
-// overflow spills exactly into the block's 128-bit accumulators. Threads
-// stride over rows so each warp loads 32 consecutive rows per step, TINY_R
-// steps deep before using them (many loads in flight). At the end the block
-// folds the columns (exact 128-bit integer sums, double-double Float64 sums)
-// and merges them into the global words agg_kernel fills, so the same
+// memory, word w of thread t at tacc[w * TINY_BLOCK + t] (a warp's accesses
+// never conflict, whatever groups its rows fall in). Per group: word 0 the
+// row count, word 1 the first row seen, then each op's words (int64 partial
+// of an integer sum, the two doubles of a double-double Float64 sum, a
+// totalOrder MIN/MAX key, a non-null count). Slot G takes the rows the
+// filter drops, so the row loop has no data-dependent branches: every row
+// does one read-modify-write of its slot's words. An integer partial that
+// would overflow spills exactly into the block's 128-bit accumulators.
+// Threads stride over the rows so each warp loads 32 consecutive rows per
+// step, TINY_R steps deep before using them (many loads in flight). At the
+// end the block folds the columns (exact 128-bit integer sums, double-double
+// Float64 sums) into the global words agg_kernel fills, so the same
 // finalize kernels run.
 //
 // E supplies the row logic as code generated per query (jit.cu): E::Consts /
 // E::load (per-thread constants read once), E::keep (filter), E::gid (dense
-// group id), E::value (op j's operand), and the compile-time layout kKind[j]
-// (op kinds), kWord[j] (first word of op j within a group), kNW (words per
-// group, the row count being word 0).
+// group id), E::value (op j's operand; `live` = the row counts, so only then
+// may it raise an error), and the compile-time layout kKind[j] (op kinds),
+// kWord[j] (first word of op j in a group), kNW (words per group).
 constexpr int TINY_BLOCK = 256;
 constexpr int TINY_R = 4;        // rows in flight per thread
 constexpr int TINY_MAX_COLS = 16;
-constexpr int TINY_MAX_WORDS = 48;  // G * kNW: 96 KB of accumulators per block
+constexpr int TINY_MAX_WORDS = 48;  // (G + 1) * kNW: 96 KB of accumulators per block
+constexpr int TINY_FIRST_OP_WORD = 2;
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
@@ -188,18 +190,18 @@ __host__ __device__ constexpr unsigned long long tiny_init(int kind) {
 template <class E, int G, int NOPS, bool F64>
 __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   constexpr int NW = E::kNW;
-  extern __shared__ unsigned long long tacc[];  // [G * NW][TINY_BLOCK]
-  __shared__ unsigned long long sfirst[G];
+  constexpr int GS = G + 1;  // slot G: dropped rows
+  extern __shared__ unsigned long long tacc[];  // [GS * NW][TINY_BLOCK]
   __shared__ unsigned long long spill[G][NOPS][4];  // exact overflow of integer partials
   __shared__ DCol scols[TINY_MAX_COLS];
   const int tid = threadIdx.x;
   const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
   if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
-  if (tid < G) sfirst[tid] = ~0ULL;
   for (int q = tid; q < G * NOPS * 4; q += TINY_BLOCK) (&spill[0][0][0])[q] = 0;
 #pragma unroll
-  for (int g = 0; g < G; ++g) {
+  for (int g = 0; g < GS; ++g) {
     tacc[(g * NW) * TINY_BLOCK + tid] = 0;
+    tacc[(g * NW + 1) * TINY_BLOCK + tid] = ~0ULL;
 #pragma unroll
     for (int j = 0; j < NOPS; ++j) {
       tacc[(g * NW + E::kWord[j]) * TINY_BLOCK + tid] = tiny_init(E::kKind[j]);
@@ -210,73 +212,66 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   const DCol* cols = shared_cols ? scols : a.cols;
   const typename E::Consts K = E::load(a);
   unsigned long long* my = tacc + tid;
-  uint32_t seen = 0;
   const int64_t stride = (int64_t)gridDim.x * TINY_BLOCK;
+  const int64_t last = a.n - 1;
   for (int64_t base = blockIdx.x * (int64_t)TINY_BLOCK + tid; base < a.n; base += stride * TINY_R) {
-    int gid[TINY_R];
+    int slot[TINY_R];
     Val v[TINY_R][NOPS];
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-      int64_t idx = base + r * stride;
-      gid[r] = -1;
-      if (idx < a.n && E::keep(a, K, cols, idx)) {
-        int g = E::gid(a, K, cols, idx);
-        if (g < 0 || g >= G) atomicOr(a.err, DERR_RANGE);
-        else gid[r] = g;
-      }
+      int64_t at = base + r * stride;
+      int64_t idx = at < last ? at : last;  // rows past the end read the last row and are dropped
+      bool keep = at <= last && E::keep(a, K, cols, idx);
+      int g = E::gid(a, K, cols, idx);
+      bool bad = keep && (g < 0 || g >= G);
+      if (bad) atomicOr(a.err, DERR_RANGE);
+      slot[r] = (keep && !bad) ? g : G;
 #pragma unroll
-      for (int j = 0; j < NOPS; ++j) {
-        if (gid[r] >= 0) {
-          v[r][j] = E::value(a, K, j, cols, idx);
-        } else {
-          v[r][j].i = 0;
-          v[r][j].f = 0;
-          v[r][j].valid = false;
-        }
-      }
+      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, keep && !bad);
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-      const int g = gid[r];
-      if (g < 0) continue;
-      if (!((seen >> g) & 1u)) {
-        seen |= 1u << g;
-        atomicMin(&sfirst[g], a.row_base + (uint64_t)(base + r * stride));
-      }
+      const int g = slot[r];
       unsigned long long* col = my + (size_t)(g * NW) * TINY_BLOCK;
       col[0] += 1;
+      const unsigned long long row = a.row_base + (uint64_t)(base + r * stride);
+      col[TINY_BLOCK] = min(col[TINY_BLOCK], row);
 #pragma unroll
       for (int j = 0; j < NOPS; ++j) {
         const int kind = E::kKind[j];
         const Val& x = v[r][j];
-        if (a.skip_nulls && !x.valid) continue;
+        const bool use = !(a.skip_nulls && !x.valid);
         unsigned long long* w = col + (size_t)E::kWord[j] * TINY_BLOCK;
         if (kind == O_SUM_INT || kind == O_SUM_DEC) {
-          long long x64 = (long long)x.i;
+          __int128 xi = use ? x.i : (__int128)0;
+          long long x64 = (long long)xi;
           long long p = (long long)w[0];
           long long s = (long long)((unsigned long long)p + (unsigned long long)x64);
-          if ((__int128)x64 == x.i && !(((p ^ s) & (x64 ^ s)) < 0)) {
+          if ((__int128)x64 == xi && !(((p ^ s) & (x64 ^ s)) < 0)) {
             w[0] = (unsigned long long)s;
           } else {  // exact spill of partial + value; the partial restarts at 0
-            add_i128_limbs(&spill[g][j][0], (__int128)p + x.i, kind == O_SUM_INT ? 2 : 4);
+            if (g < G) add_i128_limbs(&spill[g][j][0], (__int128)p + xi, kind == O_SUM_INT ? 2 : 4);
             w[0] = 0;
           }
         } else if (kind == O_SUM_F64) {
           if (F64) {
-            if (!isfinite(x.f)) {  // NaN / inf: flag straight into the global accumulator
-              uint64_t u = (uint64_t)__double_as_longlong(x.f);
-              atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(x.f) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
+            double xf = use ? x.f : 0.0;
+            if (!isfinite(xf)) {  // NaN / inf: flag straight into the global accumulator
+              if (g < G) {
+                uint64_t u = (uint64_t)__double_as_longlong(xf);
+                atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(xf) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
+              }
             } else {
               double s, e;
-              two_sum(__longlong_as_double((long long)w[0]), x.f, s, e);
+              two_sum(__longlong_as_double((long long)w[0]), xf, s, e);
               w[0] = (unsigned long long)__double_as_longlong(s);
               w[TINY_BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[TINY_BLOCK]) + e);
             }
           }
         } else if (kind == O_MIN) {
-          if (!isnan(x.f)) w[0] = (unsigned long long)min((long long)w[0], (long long)total_key(x.f));
+          if (use && !isnan(x.f)) w[0] = (unsigned long long)min((long long)w[0], (long long)total_key(x.f));
         } else if (kind == O_MAX) {
-          if (!isnan(x.f)) w[0] = (unsigned long long)max((long long)w[0], (long long)total_key(x.f));
+          if (use && !isnan(x.f)) w[0] = (unsigned long long)max((long long)w[0], (long long)total_key(x.f));
         } else if (kind == O_NONNULL) {
           w[0] += x.valid ? 1ULL : 0ULL;
         }
@@ -284,10 +279,9 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     }
   }
   __syncthreads();
-  if (tid < G && sfirst[tid] != ~0ULL) atomicMin(&a.gfirst[tid], sfirst[tid]);
-  // fold the thread columns: one item per (group, count or op)
-  for (int q = tid; q < G * (NOPS + 1); q += TINY_BLOCK) {
-    const int g = q / (NOPS + 1), jj = q % (NOPS + 1);
+  // fold the thread columns: one item per (group, count / first row / op)
+  for (int q = tid; q < G * (NOPS + 2); q += TINY_BLOCK) {
+    const int g = q / (NOPS + 2), jj = q % (NOPS + 2);
     unsigned long long* accg = a.gacc + (size_t)g * a.W;
     const unsigned long long* row = tacc + (size_t)(g * NW) * TINY_BLOCK;
     if (jj == 0) {
@@ -296,7 +290,13 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       if (a.count_rows) atom_add(accg, c);
       continue;
     }
-    const int j = jj - 1;
+    if (jj == 1) {
+      unsigned long long f = ~0ULL;
+      for (int t = 0; t < TINY_BLOCK; ++t) f = min(f, row[TINY_BLOCK + t]);
+      if (f != ~0ULL) atomicMin(&a.gfirst[g], f);
+      continue;
+    }
+    const int j = jj - 2;
     int kind = 0, word = 0;
 #pragma unroll
     for (int k = 0; k < NOPS; ++k)

@@ -616,7 +616,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   gen.declare_cols();
   gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
   std::ostringstream kinds, words, slow;
-  int nw = 1;  // word 0 of a group: its row count
+  int nw = TINY_FIRST_OP_WORD;  // words 0, 1 of a group: row count, first row
   for (int j = 0; j < a.n_ops; ++j) {
     const Op& o = a.op[j];
     if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) return "";
@@ -652,20 +652,21 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
         if (fast) {
           // 64-bit steps first; the 128-bit program (out of line, so it costs
           // the hot loop no registers) runs only when one of them overflowed
-          gen.out << "    if (" << fok << ") { r.i = (__int128)" << fval << "; r.valid = " << fvalid << "; } else {\n"
-                  << "    r = slow" << j << "(a, K, cols, idx);\n    }\n";
+          gen.out << "    if (" << fok << " || !live) { r.i = (__int128)" << fval << "; r.valid = " << fvalid << "; } else {\n"
+                  << "    r = slow" << j << "(a, K, cols, idx, live);\n    }\n";
           std::string body = gen.take();
           gen.declare_cols();
           gen.out << "    bool ovf = false;\n";
           std::string v = gen.expr(sr.begin, sr.end, "ovf");
-          gen.out << "    if (ovf) atomicOr(a.err, DERR_RANGE);\n    return " << v << ";\n";
+          gen.out << "    if (ovf && live) atomicOr(a.err, DERR_RANGE);\n    return " << v << ";\n";
           slow << "  static __device__ __noinline__ Val slow" << j
-               << "(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n" << gen.take() << "  }\n";
+               << "(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, bool live) {\n" << gen.take()
+               << "  }\n";
           gen.out << body;
         } else {
           gen.out << "    bool ovf = false;\n";
           std::string v = gen.expr(sr.begin, sr.end, "ovf");
-          gen.out << "    r = " << v << ";\n    if (ovf) atomicOr(a.err, DERR_RANGE);\n";
+          gen.out << "    r = " << v << ";\n    if (ovf && live) atomicOr(a.err, DERR_RANGE);\n";
         }
       }
     }
@@ -698,7 +699,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << a.n_ops << "] = {" << words.str() << "};\n"
     << slow.str()
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "int64_t idx) {\n"
+       "int64_t idx, bool live) {\n"
     << value
     << "  }\n"
        "};\n"
