@@ -1003,13 +1003,16 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       }
       if (jk) {
         a.n_cols = (int)pg.cols.size();
-        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)TINY_BLOCK * TINY_R * 8),
-                                           (int64_t)ctx.sm_count * 2);
-        size_t tsmem = (size_t)(G + 1) * tiny_group_words(A) * TINY_BLOCK * 8;
+        const int words = (int)(G + 1) * tiny_group_words(A), tblock = tiny_block(words);
+        // two blocks per SM (512 threads); fewer for small inputs (each
+        // thread takes at least 8 x TINY_R rows)
+        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)tblock * TINY_R * 8),
+                                           (int64_t)ctx.sm_count * (512 / tblock));
+        size_t tsmem = (size_t)words * tblock * 8;
         PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
         void* params[] = {&a};
         KernelTimer kt(ctx, "agg_tiny_jit");
-        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(TINY_BLOCK), params, tsmem, ctx.stream));
+        PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(tblock), params, tsmem, ctx.stream));
       } else {
         KernelTimer kt(ctx, "agg_kernel");
         agg_kernel<<<grid, block, smem, ctx.stream>>>(a);

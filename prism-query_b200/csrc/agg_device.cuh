@@ -168,10 +168,12 @@ __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (
 // group id), E::value (op j's operand; `live` = the row counts, so only then
 // may it raise an error), and the compile-time layout kKind[j] (op kinds),
 // kWord[j] (first word of op j in a group), kNW (words per group).
-constexpr int TINY_BLOCK = 256;
 constexpr int TINY_R = 4;        // rows in flight per thread
 constexpr int TINY_MAX_COLS = 16;
-constexpr int TINY_MAX_WORDS = 48;  // (G + 1) * kNW: 96 KB of accumulators per block
+// (G + 1) * kNW accumulator words per thread: up to 48 with 256-thread
+// blocks, up to 96 with 128-thread blocks (96 KB of shared memory a block)
+constexpr int TINY_MAX_WORDS = 96;
+__host__ __device__ constexpr int tiny_block(int words) { return words <= 48 ? 256 : 128; }
 constexpr int TINY_FIRST_OP_WORD = 2;
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
@@ -187,34 +189,34 @@ __host__ __device__ constexpr unsigned long long tiny_init(int kind) {
   return kind == O_MIN ? 0x7fffffffffffffffULL : kind == O_MAX ? 0x8000000000000000ULL : 0ULL;
 }
 
-template <class E, int G, int NOPS, bool F64>
+template <class E, int G, int NOPS, bool F64, int BLOCK>
 __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   constexpr int NW = E::kNW;
   constexpr int GS = G + 1;  // slot G: dropped rows
-  extern __shared__ unsigned long long tacc[];  // [GS * NW][TINY_BLOCK]
+  extern __shared__ unsigned long long tacc[];  // [GS * NW][BLOCK]
   __shared__ unsigned long long spill[G][NOPS][4];  // exact overflow of integer partials
   __shared__ DCol scols[TINY_MAX_COLS];
   const int tid = threadIdx.x;
   const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
   if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
-  for (int q = tid; q < G * NOPS * 4; q += TINY_BLOCK) (&spill[0][0][0])[q] = 0;
+  for (int q = tid; q < G * NOPS * 4; q += BLOCK) (&spill[0][0][0])[q] = 0;
 #pragma unroll
   for (int g = 0; g < GS; ++g) {
-    tacc[(g * NW) * TINY_BLOCK + tid] = 0;
-    tacc[(g * NW + 1) * TINY_BLOCK + tid] = ~0ULL;
+    tacc[(g * NW) * BLOCK + tid] = 0;
+    tacc[(g * NW + 1) * BLOCK + tid] = ~0ULL;
 #pragma unroll
     for (int j = 0; j < NOPS; ++j) {
-      tacc[(g * NW + E::kWord[j]) * TINY_BLOCK + tid] = tiny_init(E::kKind[j]);
-      if (tiny_words(E::kKind[j]) == 2) tacc[(g * NW + E::kWord[j] + 1) * TINY_BLOCK + tid] = 0;
+      tacc[(g * NW + E::kWord[j]) * BLOCK + tid] = tiny_init(E::kKind[j]);
+      if (tiny_words(E::kKind[j]) == 2) tacc[(g * NW + E::kWord[j] + 1) * BLOCK + tid] = 0;
     }
   }
   __syncthreads();
   const DCol* cols = shared_cols ? scols : a.cols;
   const typename E::Consts K = E::load(a);
   unsigned long long* my = tacc + tid;
-  const int64_t stride = (int64_t)gridDim.x * TINY_BLOCK;
+  const int64_t stride = (int64_t)gridDim.x * BLOCK;
   const int64_t last = a.n - 1;
-  for (int64_t base = blockIdx.x * (int64_t)TINY_BLOCK + tid; base < a.n; base += stride * TINY_R) {
+  for (int64_t base = blockIdx.x * (int64_t)BLOCK + tid; base < a.n; base += stride * TINY_R) {
     int slot[TINY_R];
     Val v[TINY_R][NOPS];
 #pragma unroll
@@ -232,16 +234,16 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       const int g = slot[r];
-      unsigned long long* col = my + (size_t)(g * NW) * TINY_BLOCK;
+      unsigned long long* col = my + (size_t)(g * NW) * BLOCK;
       col[0] += 1;
       const unsigned long long row = a.row_base + (uint64_t)(base + r * stride);
-      col[TINY_BLOCK] = min(col[TINY_BLOCK], row);
+      col[BLOCK] = min(col[BLOCK], row);
 #pragma unroll
       for (int j = 0; j < NOPS; ++j) {
         const int kind = E::kKind[j];
         const Val& x = v[r][j];
         const bool use = !(a.skip_nulls && !x.valid);
-        unsigned long long* w = col + (size_t)E::kWord[j] * TINY_BLOCK;
+        unsigned long long* w = col + (size_t)E::kWord[j] * BLOCK;
         if (kind == O_SUM_INT || kind == O_SUM_DEC) {
           __int128 xi = use ? x.i : (__int128)0;
           long long x64 = (long long)xi;
@@ -265,7 +267,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
               double s, e;
               two_sum(__longlong_as_double((long long)w[0]), xf, s, e);
               w[0] = (unsigned long long)__double_as_longlong(s);
-              w[TINY_BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[TINY_BLOCK]) + e);
+              w[BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[BLOCK]) + e);
             }
           }
         } else if (kind == O_MIN) {
@@ -280,19 +282,19 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   }
   __syncthreads();
   // fold the thread columns: one item per (group, count / first row / op)
-  for (int q = tid; q < G * (NOPS + 2); q += TINY_BLOCK) {
+  for (int q = tid; q < G * (NOPS + 2); q += BLOCK) {
     const int g = q / (NOPS + 2), jj = q % (NOPS + 2);
     unsigned long long* accg = a.gacc + (size_t)g * a.W;
-    const unsigned long long* row = tacc + (size_t)(g * NW) * TINY_BLOCK;
+    const unsigned long long* row = tacc + (size_t)(g * NW) * BLOCK;
     if (jj == 0) {
       unsigned long long c = 0;
-      for (int t = 0; t < TINY_BLOCK; ++t) c += row[t];
+      for (int t = 0; t < BLOCK; ++t) c += row[t];
       if (a.count_rows) atom_add(accg, c);
       continue;
     }
     if (jj == 1) {
       unsigned long long f = ~0ULL;
-      for (int t = 0; t < TINY_BLOCK; ++t) f = min(f, row[TINY_BLOCK + t]);
+      for (int t = 0; t < BLOCK; ++t) f = min(f, row[BLOCK + t]);
       if (f != ~0ULL) atomicMin(&a.gfirst[g], f);
       continue;
     }
@@ -301,20 +303,20 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 #pragma unroll
     for (int k = 0; k < NOPS; ++k)
       if (k == j) { kind = E::kKind[k]; word = E::kWord[k]; }
-    const unsigned long long* w = row + (size_t)word * TINY_BLOCK;
+    const unsigned long long* w = row + (size_t)word * BLOCK;
     unsigned long long* gw = accg + a.op[j].word;
     if (kind == O_SUM_INT || kind == O_SUM_DEC) {
       __int128 s = 0;
-      for (int t = 0; t < TINY_BLOCK; ++t) s += (__int128)(long long)w[t];
+      for (int t = 0; t < BLOCK; ++t) s += (__int128)(long long)w[t];
       for (int l = 0; l < 4; ++l) s += (__int128)(long long)spill[g][j][l] << (32 * l);
       add_i128_limbs(gw, s, kind == O_SUM_INT ? 2 : 4);
     } else if (kind == O_SUM_F64) {
       if (F64) {
         double h = 0, l = 0;
-        for (int t = 0; t < TINY_BLOCK; ++t) {
+        for (int t = 0; t < BLOCK; ++t) {
           double s1, e1;
           two_sum(h, __longlong_as_double((long long)w[t]), s1, e1);
-          e1 += l + __longlong_as_double((long long)w[t + TINY_BLOCK]);
+          e1 += l + __longlong_as_double((long long)w[t + BLOCK]);
           h = s1 + e1;
           l = e1 - (h - s1);
         }
@@ -323,14 +325,14 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       }
     } else if (kind == O_MIN || kind == O_MAX) {
       long long m = (long long)tiny_init(kind);
-      for (int t = 0; t < TINY_BLOCK; ++t) m = kind == O_MIN ? min(m, (long long)w[t]) : max(m, (long long)w[t]);
+      for (int t = 0; t < BLOCK; ++t) m = kind == O_MIN ? min(m, (long long)w[t]) : max(m, (long long)w[t]);
       if (m != (long long)tiny_init(kind)) {
         if (kind == O_MIN) atomicMin((long long*)gw, m);
         else atomicMax((long long*)gw, m);
       }
     } else if (kind == O_NONNULL) {
       unsigned long long c = 0;
-      for (int t = 0; t < TINY_BLOCK; ++t) c += w[t];
+      for (int t = 0; t < BLOCK; ++t) c += w[t];
       atom_add(gw, c);
     }
   }

@@ -674,6 +674,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   }
   gen.out << "    return r;\n";
   std::string value = gen.take();
+  const int block = tiny_block((g + 1) * nw);
   if (!gen.ok) return "";
 
   std::string consts = gen.consts.str();
@@ -704,9 +705,10 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << "  }\n"
        "};\n"
        "}  // namespace prism\n"
-       "extern \"C\" __global__ void __launch_bounds__(prism::TINY_BLOCK, 2) prism_tiny_agg(prism::AggArgs a) {\n"
+       "extern \"C\" __global__ void __launch_bounds__("
+    << block << ", " << 512 / block << ") prism_tiny_agg(prism::AggArgs a) {\n"
        "  prism::tiny_body<prism::QueryRow, "
-    << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false")
+    << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false") << ", " << block
     << ">(a);\n"
        "}\n";
   return s.str();
