@@ -216,9 +216,13 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   unsigned long long* my = tacc + tid;
   const int64_t stride = (int64_t)gridDim.x * BLOCK;
   const int64_t last = a.n - 1;
+  bool err = false;
   for (int64_t base = blockIdx.x * (int64_t)BLOCK + tid; base < a.n; base += stride * TINY_R) {
     int slot[TINY_R];
+    unsigned flags[TINY_R];
     Val v[TINY_R][NOPS];
+    // phase 1, loads and arithmetic only (no stores, atomics or calls), so
+    // the loads of all TINY_R rows are in flight together
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       int64_t at = base + r * stride;
@@ -226,14 +230,24 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       bool keep = at <= last && E::keep(a, K, cols, idx);
       int g = E::gid(a, K, cols, idx);
       bool bad = keep && (g < 0 || g >= G);
-      if (bad) atomicOr(a.err, DERR_RANGE);
+      err |= bad;
       slot[r] = (keep && !bad) ? g : G;
+      flags[r] = 0;
 #pragma unroll
-      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, keep && !bad);
+      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, flags[r]);
     }
+    // phase 2: the rare 128-bit recomputations, then the accumulators
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       const int g = slot[r];
+      if (g < G && flags[r]) {
+        const int64_t at = base + r * stride;
+#pragma unroll
+        for (int j = 0; j < NOPS; ++j)
+          if ((flags[r] >> (2 * j)) & 1u) v[r][j] = E::slow(a, K, j, cols, at, flags[r]);
+#pragma unroll
+        for (int j = 0; j < NOPS; ++j) err |= ((flags[r] >> (2 * j + 1)) & 1u) != 0;
+      }
       unsigned long long* col = my + (size_t)(g * NW) * BLOCK;
       col[0] += 1;
       const unsigned long long row = a.row_base + (uint64_t)(base + r * stride);
@@ -280,6 +294,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       }
     }
   }
+  if (err) atomicOr(a.err, DERR_RANGE);
   __syncthreads();
   // fold the thread columns: one item per (group, count / first row / op)
   for (int q = tid; q < G * (NOPS + 2); q += BLOCK) {

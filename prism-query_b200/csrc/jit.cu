@@ -650,23 +650,22 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
         std::string fval, fvalid, fok;
         bool fast = sr.kind == S_EXPR_I128 && gen.expr_fast64(sr.begin, sr.end, fval, fvalid, fok);
         if (fast) {
-          // 64-bit steps first; the 128-bit program (out of line, so it costs
-          // the hot loop no registers) runs only when one of them overflowed
-          gen.out << "    if (" << fok << " || !live) { r.i = (__int128)" << fval << "; r.valid = " << fvalid << "; } else {\n"
-                  << "    r = slow" << j << "(a, K, cols, idx, live);\n    }\n";
+          // 64-bit steps here; when one of them overflowed, flag bit 2j asks
+          // the caller for the 128-bit program (out of line in slow(), so it
+          // costs the hot loop no registers and no ordering of its loads)
+          gen.out << "    r.i = (__int128)" << fval << "; r.valid = " << fvalid << "; if (!" << fok << ") flags |= "
+                  << (1u << (2 * j)) << "u;\n";
           std::string body = gen.take();
-          gen.declare_cols();
-          gen.out << "    bool ovf = false;\n";
+          gen.out << "    if (j == " << j << ") {\n    bool ovf = false;\n";
           std::string v = gen.expr(sr.begin, sr.end, "ovf");
-          gen.out << "    if (ovf && live) atomicOr(a.err, DERR_RANGE);\n    return " << v << ";\n";
-          slow << "  static __device__ __noinline__ Val slow" << j
-               << "(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, bool live) {\n" << gen.take()
-               << "  }\n";
+          gen.out << "    if (ovf) flags |= " << (2u << (2 * j)) << "u;\n    return " << v << ";\n    }\n";
+          slow << gen.take();
           gen.out << body;
         } else {
+          // overflow is reported through flag bit 2j+1, never raised here
           gen.out << "    bool ovf = false;\n";
           std::string v = gen.expr(sr.begin, sr.end, "ovf");
-          gen.out << "    r = " << v << ";\n    if (ovf && live) atomicOr(a.err, DERR_RANGE);\n";
+          gen.out << "    r = " << v << ";\n    if (ovf) flags |= " << (2u << (2 * j)) << "u;\n";
         }
       }
     }
@@ -674,6 +673,8 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   }
   gen.out << "    return r;\n";
   std::string value = gen.take();
+  gen.declare_cols();
+  std::string slow_cols = gen.take();
   const int block = tiny_block((g + 1) * nw);
   if (!gen.ok) return "";
 
@@ -698,9 +699,12 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
-    << slow.str()
+    << "  static __device__ __noinline__ Val slow(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
+       "int64_t idx, unsigned& flags) {\n"
+    << slow_cols << slow.str()
+    << "    Val r; r.i = 0; r.f = 0; r.valid = false;\n    return r;\n  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "int64_t idx, bool live) {\n"
+       "int64_t idx, unsigned& flags) {\n"
     << value
     << "  }\n"
        "};\n"
