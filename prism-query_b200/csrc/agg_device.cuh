@@ -182,6 +182,12 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
   e = (a - (s - bb)) + (b - bb);
 }
 
+// result of a generated program's out-of-line 128-bit path
+struct SlowVal {
+  Val v;
+  bool ovf;
+};
+
 // words an op occupies in a group's accumulator column
 __host__ __device__ constexpr int tiny_words(int kind) { return kind == O_SUM_F64 ? 2 : 1; }
 
@@ -244,7 +250,11 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
         const int64_t at = base + r * stride;
 #pragma unroll
         for (int j = 0; j < NOPS; ++j)
-          if ((flags[r] >> (2 * j)) & 1u) v[r][j] = E::slow(a, K, j, cols, at, flags[r]);
+          if ((flags[r] >> (2 * j)) & 1u) {
+            SlowVal sv = E::slow(a, j, cols, at);
+            v[r][j] = sv.v;
+            if (sv.ovf) flags[r] |= 2u << (2 * j);
+          }
 #pragma unroll
         for (int j = 0; j < NOPS; ++j) err |= ((flags[r] >> (2 * j + 1)) & 1u) != 0;
       }

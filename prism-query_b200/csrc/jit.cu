@@ -658,7 +658,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
           std::string body = gen.take();
           gen.out << "    if (j == " << j << ") {\n    bool ovf = false;\n";
           std::string v = gen.expr(sr.begin, sr.end, "ovf");
-          gen.out << "    if (ovf) flags |= " << (2u << (2 * j)) << "u;\n    return " << v << ";\n    }\n";
+          gen.out << "    SlowVal s; s.v = " << v << "; s.ovf = ovf;\n    return s;\n    }\n";
           slow << gen.take();
           gen.out << body;
         } else {
@@ -699,10 +699,10 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
-    << "  static __device__ __noinline__ Val slow(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "int64_t idx, unsigned& flags) {\n"
+    << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, int64_t idx) {\n"
+       "    const Consts K = load(a);\n"
     << slow_cols << slow.str()
-    << "    Val r; r.i = 0; r.f = 0; r.valid = false;\n    return r;\n  }\n"
+    << "    SlowVal s; s.v.i = 0; s.v.f = 0; s.v.valid = false; s.ovf = false;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "int64_t idx, unsigned& flags) {\n"
     << value
