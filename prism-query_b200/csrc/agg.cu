@@ -1004,12 +1004,15 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       if (jk) {
         a.n_cols = (int)pg.cols.size();
         const int words = (int)(G + 1) * tiny_group_words(A), tblock = tiny_block(words);
-        // two blocks per SM (512 threads); fewer for small inputs (each
-        // thread takes at least 8 x TINY_R rows)
-        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)tblock * TINY_R * 8),
-                                           (int64_t)ctx.sm_count * (512 / tblock));
         size_t tsmem = (size_t)words * tblock * 8;
         PRISM_CUDA(cudaFuncSetAttribute(jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+        // as many blocks as fit on every SM at once (registers and shared
+        // memory decide); fewer for small inputs (each thread takes at
+        // least 8 x TINY_R rows)
+        int per_sm = 0;
+        PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jk, tblock, tsmem));
+        int tgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)tblock * TINY_R * 8),
+                                           (int64_t)ctx.sm_count * std::max(1, per_sm));
         void* params[] = {&a};
         KernelTimer kt(ctx, "agg_tiny_jit");
         PRISM_CUDA(cudaLaunchKernel(jk, dim3(tgrid), dim3(tblock), params, tsmem, ctx.stream));

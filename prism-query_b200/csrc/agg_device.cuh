@@ -223,6 +223,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   const int64_t stride = (int64_t)gridDim.x * BLOCK;
   const int64_t last = a.n - 1;
   bool err = false;
+  unsigned seen = 0;  // slots this thread has met (slot G included: harmless)
   for (int64_t base = blockIdx.x * (int64_t)BLOCK + tid; base < a.n; base += stride * TINY_R) {
     int slot[TINY_R];
     unsigned flags[TINY_R];
@@ -260,8 +261,11 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       }
       unsigned long long* col = my + (size_t)(g * NW) * BLOCK;
       col[0] += 1;
-      const unsigned long long row = a.row_base + (uint64_t)(base + r * stride);
-      col[BLOCK] = min(col[BLOCK], row);
+      // a thread meets its rows in increasing order: the first row of a
+      // group is the one seen while its bit is still clear
+      const unsigned bit = 1u << g;
+      if (!(seen & bit)) col[BLOCK] = a.row_base + (uint64_t)(base + r * stride);
+      seen |= bit;
 #pragma unroll
       for (int j = 0; j < NOPS; ++j) {
         const int kind = E::kKind[j];
