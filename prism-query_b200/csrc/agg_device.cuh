@@ -270,7 +270,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       for (int j = 0; j < NOPS; ++j) {
         const int kind = E::kKind[j];
         const Val& x = v[r][j];
-        const bool use = !(a.skip_nulls && !x.valid);
+        const bool use = !(E::kSkipNulls && !x.valid);
         unsigned long long* w = col + (size_t)E::kWord[j] * BLOCK;
         if (kind == O_SUM_INT || kind == O_SUM_DEC) {
           __int128 xi = use ? x.i : (__int128)0;

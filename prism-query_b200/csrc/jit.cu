@@ -492,9 +492,10 @@ struct Gen {
             else if (nd.op == E_SUB_I)
               out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
                   << ")) < 0);\n";
-            else
-              out << "    " << okv << " = " << okv << " && __mul64hi(" << l.n << ", " << r.n << ") == (" << n
-                  << " >> 63);\n";
+            else  // operands inside int32 cannot overflow; only others pay for the high product
+              out << "    if ((unsigned long long)(" << l.n << " + 0x80000000LL) >= 0x100000000ULL || (unsigned long long)("
+                  << r.n << " + 0x80000000LL) >= 0x100000000ULL) " << okv << " = " << okv << " && __mul64hi(" << l.n
+                  << ", " << r.n << ") == (" << n << " >> 63);\n";
             bound = Mag{};
           }
           st.push_back({n, vv, bound});
@@ -696,6 +697,9 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
     << gid
     << "  }\n"
+       "  static constexpr bool kSkipNulls = "
+    << (a.skip_nulls ? "true" : "false")
+    << ";\n"
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
