@@ -228,20 +228,27 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     int slot[TINY_R];
     unsigned flags[TINY_R];
     Val v[TINY_R][NOPS];
-    // phase 1, loads and arithmetic only (no stores, atomics or calls), so
-    // the loads of all TINY_R rows are in flight together
+    typename E::Row rows[TINY_R];
+    // phase 1: the fixed-width columns of all TINY_R rows are loaded first
+    // (straight-line loads, all in flight together), then evaluated with
+    // arithmetic only (no stores, atomics or calls)
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       int64_t at = base + r * stride;
-      int64_t idx = at < last ? at : last;  // rows past the end read the last row and are dropped
-      bool keep = at <= last && E::keep(a, K, cols, idx);
-      int g = E::gid(a, K, cols, idx);
+      rows[r] = E::fetch(cols, at < last ? at : last);  // rows past the end read the last row and are dropped
+    }
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+      int64_t at = base + r * stride;
+      int64_t idx = at < last ? at : last;
+      bool keep = at <= last && E::keep(a, K, cols, idx, rows[r]);
+      int g = E::gid(a, K, cols, idx, rows[r]);
       bool bad = keep && (g < 0 || g >= G);
       err |= bad;
       slot[r] = (keep && !bad) ? g : G;
       flags[r] = 0;
 #pragma unroll
-      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, flags[r]);
+      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, rows[r], flags[r]);
     }
     // phase 2: the rare 128-bit recomputations, then the accumulators
 #pragma unroll

@@ -175,26 +175,87 @@ struct Gen {
     load << "    K." << name << " = " << init << ";\n";
   }
 
-  // typed local views of every program column (the optimizer drops unused
-  // ones): a constant type folds the type switches of the dcol_* readers,
-  // and a null validity pointer folds dcol_valid to true
+  // Fixed-width columns (numbers, Boolean, dictionary indices, decimals)
+  // are fetched for a row up front into a Row of raw register words (one
+  // load each, no control flow, so the loads of several rows overlap); the
+  // typed views below read them from there with the same dcol_* helpers the
+  // interpreter uses (index 0 of the view, a constant type so the type
+  // switches fold). Utf8 columns are read in place at the row index.
+  int col_type(int slot) const { return b.cols[pg.cols[slot]]->type; }
+  bool fetched(int slot) const { return width_of(col_type(slot) == TY_DICT ? TY_I32 : col_type(slot)) > 0 || col_type(slot) == TY_BOOL || col_type(slot) == TY_DICT; }
+  bool nullable(int slot) const { return b.cols[pg.cols[slot]]->validity != nullptr; }
+  std::string ix(int slot) const { return fetched(slot) ? "0" : "idx"; }
+
   void declare_cols() {
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       const Column& c = *b.cols[pg.cols[s]];
+      int t = c.type == TY_BOOL ? TY_U8 : c.type;  // a fetched Boolean is one byte 0 / 1
       out << "    DCol c" << s << " = cols[" << s << "];\n";
-      out << "    c" << s << ".type = " << c.type << "; c" << s << ".index_type = " << c.index_type << "; c" << s
+      out << "    c" << s << ".type = " << t << "; c" << s << ".index_type = " << c.index_type << "; c" << s
           << ".scale = " << c.scale << ";";
-      if (!c.validity) out << " c" << s << ".validity = nullptr;";
+      if (fetched((int)s)) out << " c" << s << ".values = &row.r" << s << "[0]; c" << s << ".validity = nullptr;";
+      else if (!c.validity) out << " c" << s << ".validity = nullptr;";
       out << "\n";
     }
   }
 
   std::string col(int slot) {
-    if (slot < 0 || slot >= (int)pg.cols.size()) {
-      gen_fail("column slot out of range");
-      return "c0";
-    }
+    if (slot < 0 || slot >= (int)pg.cols.size()) gen_fail("column slot out of range");
     return "c" + std::to_string(slot);
+  }
+
+  // validity of the row in column `slot`
+  std::string V(int slot) const {
+    if (fetched(slot)) return nullable(slot) ? "row.m" + std::to_string(slot) : std::string("true");
+    return "dcol_valid(c" + std::to_string(slot) + ", idx)";
+  }
+  // plain reader: fn(view, index)
+  std::string rd(const char* fn, int slot) const {
+    return std::string(fn) + "(c" + std::to_string(slot) + ", " + ix(slot) + ")";
+  }
+  // the dcol_*_cast readers: a null row of a column other than Float64 and
+  // Decimal128 reads 0 (as arrow's casts leave it)
+  std::string rd_cast(const char* fn, const char* zero, int slot) const {
+    int t = col_type(slot);
+    if (t == TY_F64 || t == TY_DEC128 || !nullable(slot)) return rd(fn, slot);
+    return "(" + V(slot) + " ? " + rd(fn, slot) + " : " + zero + ")";
+  }
+
+  // struct Row and fetch(): raw words of every fixed-width program column
+  std::string row_struct() const {
+    std::ostringstream o;
+    o << "  struct Row {\n";
+    bool any = false;
+    for (size_t s = 0; s < pg.cols.size(); ++s) {
+      if (!fetched((int)s)) continue;
+      any = true;
+      o << "    unsigned long long r" << s << "[" << (col_type((int)s) == TY_DEC128 ? 2 : 1) << "];\n";
+      if (nullable((int)s)) o << "    bool m" << s << ";\n";
+    }
+    if (!any) o << "    int unused;\n";
+    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, int64_t idx) {\n    Row w;\n";
+    for (size_t s = 0; s < pg.cols.size(); ++s) {
+      if (!fetched((int)s)) continue;
+      const Column& c = *b.cols[pg.cols[s]];
+      int t = c.type == TY_DICT ? c.index_type : c.type;
+      std::string src = "cols[" + std::to_string(s) + "].values";
+      switch (t == TY_BOOL ? 0 : width_of(t)) {
+        case 0:
+          o << "    w.r" << s << "[0] = (static_cast<const uint8_t*>(" << src << ")[idx >> 3] >> (idx & 7)) & 1;\n";
+          break;
+        case 1: o << "    w.r" << s << "[0] = static_cast<const uint8_t*>(" << src << ")[idx];\n"; break;
+        case 2: o << "    w.r" << s << "[0] = static_cast<const uint16_t*>(" << src << ")[idx];\n"; break;
+        case 4: o << "    w.r" << s << "[0] = static_cast<const uint32_t*>(" << src << ")[idx];\n"; break;
+        case 8: o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[idx];\n"; break;
+        default:
+          o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[2 * idx];\n";
+          o << "    w.r" << s << "[1] = static_cast<const unsigned long long*>(" << src << ")[2 * idx + 1];\n";
+      }
+      if (c.validity)
+        o << "    w.m" << s << " = (cols[" << s << "].validity[idx >> 3] >> (idx & 7)) & 1;\n";
+    }
+    o << "    return w;\n  }\n";
+    return o.str();
   }
 
   // predicate nodes [begin, begin + len): emits statements, returns the
@@ -213,15 +274,15 @@ struct Gen {
         case P_CMP_INT: {
           std::string c = col(nd.col);
           konst("int64_t", "pi" + K, "a.pn[" + K + "].i");
-          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
-          out << "    bool " << v << " = dcol_ival(" << c << ", idx) " << cmp_op(nd.cmp) << " K.pi" << K << ";\n";
+          out << "    bool " << a << " = " << V(nd.col) << ";\n";
+          out << "    bool " << v << " = " << rd("dcol_ival", nd.col) << " " << cmp_op(nd.cmp) << " K.pi" << K << ";\n";
           break;
         }
         case P_CMP_F64: {
           std::string c = col(nd.col);
           konst("int64_t", "pf" + K, "total_key(a.pn[" + K + "].f)");
-          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
-          out << "    bool " << v << " = total_key(static_cast<const double*>(" << c << ".values)[idx]) "
+          out << "    bool " << a << " = " << V(nd.col) << ";\n";
+          out << "    bool " << v << " = total_key(static_cast<const double*>(" << c << ".values)[" << ix(nd.col) << "]) "
               << cmp_op(nd.cmp) << " K.pf" << K << ";\n";
           break;
         }
@@ -230,8 +291,8 @@ struct Gen {
           konst("const uint8_t*", "ps" + K, "a.pn[" + K + "].s");
           konst("int32_t", "pn" + K, "a.pn[" + K + "].slen");
           std::string p = fresh("sp"), n = fresh("sn");
-          out << "    bool " << a << " = dcol_valid(" << c << ", idx);\n";
-          out << "    const uint8_t* " << p << "; int32_t " << n << "; dcol_str(" << c << ", idx, " << p << ", " << n
+          out << "    bool " << a << " = " << V(nd.col) << ";\n";
+          out << "    const uint8_t* " << p << "; int32_t " << n << "; dcol_str(" << c << ", " << ix(nd.col) << ", " << p << ", " << n
               << ");\n";
           if (nd.op == P_CMP_STR)
             out << "    bool " << v << " = bytes_cmp(" << p << ", " << n << ", K.ps" << K << ", K.pn" << K << ") "
@@ -243,7 +304,7 @@ struct Gen {
         }
         case P_IS_NULL: case P_IS_NOT_NULL: {
           std::string c = col(nd.col);
-          out << "    bool " << v << " = " << (nd.op == P_IS_NULL ? "!" : "") << "dcol_valid(" << c << ", idx), " << a
+          out << "    bool " << v << " = " << (nd.op == P_IS_NULL ? "!" : "") << "(" << V(nd.col) << "), " << a
               << " = true;\n";
           break;
         }
@@ -292,8 +353,9 @@ struct Gen {
       switch (nd.op) {
         case E_COL_F64: {
           std::string c = col(nd.col);
-          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = " << (nd.a ? "dcol_fval(" : "dcol_fval_cast(")
-              << c << ", idx); " << n << ".valid = dcol_valid(" << c << ", idx);\n";
+          out << "    Val " << n << "; " << n << ".i = 0; " << n << ".f = "
+              << (nd.a ? rd("dcol_fval", nd.col) : rd_cast("dcol_fval", "0.0", nd.col)) << "; " << n << ".valid = " << V(nd.col)
+              << ";\n";
           st.push_back({n, Mag{}});
           break;
         }
@@ -301,8 +363,9 @@ struct Gen {
           std::string c = col(nd.col);
           const Column& cc = *b.cols[pg.cols[std::max(0, std::min(nd.col, (int)pg.cols.size() - 1))]];
           int t = cc.type == TY_DICT ? cc.index_type : cc.type;
-          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = " << (nd.a ? "dcol_i128(" : "dcol_i128_cast(")
-              << c << ", idx); " << n << ".valid = dcol_valid(" << c << ", idx);\n";
+          out << "    Val " << n << "; " << n << ".f = 0; " << n << ".i = "
+              << (nd.a ? rd("dcol_i128", nd.col) : rd_cast("dcol_i128", "(__int128)0", nd.col)) << "; " << n
+              << ".valid = " << V(nd.col) << ";\n";
           st.push_back({n, type_mag(t)});
           break;
         }
@@ -459,8 +522,8 @@ struct Gen {
           std::string c = col(nd.col);
           const Column& cc = *b.cols[pg.cols[nd.col]];
           int t = cc.type == TY_DICT ? cc.index_type : cc.type;
-          out << "    long long " << n << " = " << (nd.a ? "dcol_ival(" : "dcol_ival_cast(") << c << ", idx); bool " << vv
-              << " = dcol_valid(" << c << ", idx);\n";
+          out << "    long long " << n << " = " << (nd.a ? rd("dcol_ival", nd.col) : rd_cast("dcol_ival", "0LL", nd.col))
+              << "; bool " << vv << " = " << V(nd.col) << ";\n";
           st.push_back({n, vv, type_mag(t)});
           break;
         }
@@ -492,10 +555,9 @@ struct Gen {
             else if (nd.op == E_SUB_I)
               out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
                   << ")) < 0);\n";
-            else  // operands inside int32 cannot overflow; only others pay for the high product
-              out << "    if ((unsigned long long)(" << l.n << " + 0x80000000LL) >= 0x100000000ULL || (unsigned long long)("
-                  << r.n << " + 0x80000000LL) >= 0x100000000ULL) " << okv << " = " << okv << " && __mul64hi(" << l.n
-                  << ", " << r.n << ") == (" << n << " >> 63);\n";
+            else
+              out << "    " << okv << " = " << okv << " && __mul64hi(" << l.n << ", " << r.n << ") == (" << n
+                  << " >> 63);\n";
             bound = Mag{};
           }
           st.push_back({n, vv, bound});
@@ -608,7 +670,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   gen.out << "    int g = 0;\n";
   for (int k = 0; k < a.n_gcols; ++k) {
     std::string c = gen.col(a.gcol[k]);
-    gen.out << "    { int64_t code = dcol_valid(" << c << ", idx) ? dcol_ival(" << c << ", idx) : a.dnull[" << k
+    gen.out << "    { int64_t code = " << gen.V(a.gcol[k]) << " ? " << gen.rd("dcol_ival", a.gcol[k]) << " : a.dnull[" << k
             << "]; g += (int)(code * a.dstride[" << k << "]); }\n";
   }
   gen.out << "    return g;\n";
@@ -629,22 +691,22 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     switch (sr.kind) {
       case S_COL_F64: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.f = dcol_fval_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.f = " << gen.rd_cast("dcol_fval", "0.0", sr.col) << "; r.valid = " << gen.V(sr.col) << ";\n";
         break;
       }
       case S_COL_INT: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.i = dcol_ival_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.i = " << gen.rd_cast("dcol_ival", "0LL", sr.col) << "; r.valid = " << gen.V(sr.col) << ";\n";
         break;
       }
       case S_COL_I128: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.i = dcol_i128_cast(" << c << ", idx); r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.i = " << gen.rd_cast("dcol_i128", "(__int128)0", sr.col) << "; r.valid = " << gen.V(sr.col) << ";\n";
         break;
       }
       case S_VALID: {
         std::string c = gen.col(sr.col);
-        gen.out << "    r.valid = dcol_valid(" << c << ", idx);\n";
+        gen.out << "    r.valid = " << gen.V(sr.col) << ";\n";
         break;
       }
       default: {
@@ -688,13 +750,16 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  struct Consts {\n"
     << consts
     << "  };\n"
-       "  static __device__ __forceinline__ Consts load(const AggArgs& a) {\n    Consts K;\n"
+    << gen.row_struct()
+    << "  static __device__ __forceinline__ Consts load(const AggArgs& a) {\n    Consts K;\n"
     << gen.load.str()
     << "    return K;\n  }\n"
-       "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
+       "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, "
+       "const Row& row) {\n"
     << keep
     << "  }\n"
-       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx) {\n"
+       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, "
+       "const Row& row) {\n"
     << gid
     << "  }\n"
        "  static constexpr bool kSkipNulls = "
@@ -704,11 +769,11 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
     << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, int64_t idx) {\n"
-       "    const Consts K = load(a);\n"
+       "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
     << slow_cols << slow.str()
     << "    SlowVal s; s.v.i = 0; s.v.f = 0; s.v.valid = false; s.ovf = false;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "int64_t idx, unsigned& flags) {\n"
+       "int64_t idx, const Row& row, unsigned& flags) {\n"
     << value
     << "  }\n"
        "};\n"
