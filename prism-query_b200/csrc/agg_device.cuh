@@ -220,11 +220,14 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   const DCol* cols = shared_cols ? scols : a.cols;
   const typename E::Consts K = E::load(a);
   unsigned long long* my = tacc + tid;
-  const int64_t stride = (int64_t)gridDim.x * BLOCK;
-  const int64_t last = a.n - 1;
+  // row indices in E::idx_t: 32-bit when the batch has fewer than 2^31 rows
+  // (cheaper address arithmetic), else 64-bit
+  using I = typename E::idx_t;
+  const I stride = (I)gridDim.x * BLOCK;
+  const I n = (I)a.n, last = n - 1;
   bool err = false;
   unsigned seen = 0;  // slots this thread has met (slot G included: harmless)
-  for (int64_t base = blockIdx.x * (int64_t)BLOCK + tid; base < a.n; base += stride * TINY_R) {
+  for (I base = (I)blockIdx.x * BLOCK + tid; base < n; base += stride * TINY_R) {
     int slot[TINY_R];
     unsigned flags[TINY_R];
     Val v[TINY_R][NOPS];
@@ -234,13 +237,13 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     // arithmetic only (no stores, atomics or calls)
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-      int64_t at = base + r * stride;
+      I at = base + r * stride;
       rows[r] = E::fetch(cols, at < last ? at : last);  // rows past the end read the last row and are dropped
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
-      int64_t at = base + r * stride;
-      int64_t idx = at < last ? at : last;
+      I at = base + r * stride;
+      I idx = at < last ? at : last;
       bool keep = at <= last && E::keep(a, K, cols, idx, rows[r]);
       int g = E::gid(a, K, cols, idx, rows[r]);
       bool bad = keep && (g < 0 || g >= G);
@@ -255,7 +258,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     for (int r = 0; r < TINY_R; ++r) {
       const int g = slot[r];
       if (g < G && flags[r]) {
-        const int64_t at = base + r * stride;
+        const I at = base + r * stride;
 #pragma unroll
         for (int j = 0; j < NOPS; ++j)
           if ((flags[r] >> (2 * j)) & 1u) {
@@ -266,7 +269,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 #pragma unroll
         for (int j = 0; j < NOPS; ++j) err |= ((flags[r] >> (2 * j + 1)) & 1u) != 0;
       }
-      unsigned long long* col = my + (size_t)(g * NW) * BLOCK;
+      unsigned long long* col = my + (g * NW) * BLOCK;
       col[0] += 1;
       // a thread meets its rows in increasing order: the first row of a
       // group is the one seen while its bit is still clear
@@ -278,7 +281,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
         const int kind = E::kKind[j];
         const Val& x = v[r][j];
         const bool use = !(E::kSkipNulls && !x.valid);
-        unsigned long long* w = col + (size_t)E::kWord[j] * BLOCK;
+        unsigned long long* w = col + E::kWord[j] * BLOCK;
         if (kind == O_SUM_INT || kind == O_SUM_DEC) {
           __int128 xi = use ? x.i : (__int128)0;
           long long x64 = (long long)xi;

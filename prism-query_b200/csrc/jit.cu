@@ -233,7 +233,7 @@ struct Gen {
       if (nullable((int)s)) o << "    bool m" << s << ";\n";
     }
     if (!any) o << "    int unused;\n";
-    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, int64_t idx) {\n    Row w;\n";
+    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, idx_t idx) {\n    Row w;\n";
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       if (!fetched((int)s)) continue;
       const Column& c = *b.cols[pg.cols[s]];
@@ -555,9 +555,10 @@ struct Gen {
             else if (nd.op == E_SUB_I)
               out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
                   << ")) < 0);\n";
-            else
-              out << "    " << okv << " = " << okv << " && __mul64hi(" << l.n << ", " << r.n << ") == (" << n
-                  << " >> 63);\n";
+            else  // safe when both factors lie inside int32; other rows take the 128-bit path
+              out << "    " << okv << " = " << okv << " && (unsigned long long)(" << l.n
+                  << " + 0x80000000LL) < 0x100000000ULL && (unsigned long long)(" << r.n
+                  << " + 0x80000000LL) < 0x100000000ULL;\n";
             bound = Mag{};
           }
           st.push_back({n, vv, bound});
@@ -577,8 +578,8 @@ struct Gen {
           long long p10 = 1;
           for (int q = 0; q < nd.col; ++q) p10 *= 10;
           out << "    long long " << n << " = (long long)((unsigned long long)" << x.n << " * " << p10 << "ULL); bool " << vv
-              << " = " << x.v << "; " << okv << " = " << okv << " && __mul64hi(" << x.n << ", " << p10 << "LL) == (" << n
-              << " >> 63);\n";
+              << " = " << x.v << "; " << okv << " = " << okv << " && (" << x.n << " < 0 ? 0ULL - (unsigned long long)" << x.n
+              << " : (unsigned long long)" << x.n << ") <= " << (9223372036854775807LL / p10) << "ULL;\n";
           st.push_back({n, vv, Mag{}});
           break;
         }
@@ -670,8 +671,9 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   gen.out << "    int g = 0;\n";
   for (int k = 0; k < a.n_gcols; ++k) {
     std::string c = gen.col(a.gcol[k]);
-    gen.out << "    { int64_t code = " << gen.V(a.gcol[k]) << " ? " << gen.rd("dcol_ival", a.gcol[k]) << " : a.dnull[" << k
-            << "]; g += (int)(code * a.dstride[" << k << "]); }\n";
+    // the dense id layout (dictionary sizes) is fixed per plan: constants
+    gen.out << "    { int code = " << gen.V(a.gcol[k]) << " ? (int)" << gen.rd("dcol_ival", a.gcol[k]) << " : "
+            << a.dnull[k] << "; g += code * " << a.dstride[k] << "; }\n";
   }
   gen.out << "    return g;\n";
   std::string gid = gen.take();
@@ -747,6 +749,9 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   s << "#include \"agg_device.cuh\"\n"
        "namespace prism {\n"
        "struct QueryRow {\n"
+       "  typedef "
+    << (b.rows < ((int64_t)1 << 31) - ((int64_t)1 << 26) ? "int" : "long long")
+    << " idx_t;  // row index type: 32-bit below 2^31 rows\n"
        "  struct Consts {\n"
     << consts
     << "  };\n"
@@ -754,11 +759,11 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << "  static __device__ __forceinline__ Consts load(const AggArgs& a) {\n    Consts K;\n"
     << gen.load.str()
     << "    return K;\n  }\n"
-       "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, "
+       "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
        "const Row& row) {\n"
     << keep
     << "  }\n"
-       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, int64_t idx, "
+       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
        "const Row& row) {\n"
     << gid
     << "  }\n"
@@ -768,12 +773,12 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n"
-    << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, int64_t idx) {\n"
+    << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
        "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
     << slow_cols << slow.str()
     << "    SlowVal s; s.v.i = 0; s.v.f = 0; s.v.valid = false; s.ovf = false;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "int64_t idx, const Row& row, unsigned& flags) {\n"
+       "idx_t idx, const Row& row, unsigned& flags) {\n"
     << value
     << "  }\n"
        "};\n"

@@ -184,3 +184,21 @@ def test_interpreting_kernel_agrees_without_runtime_compilation():
     assert r.returncode == 0, r.stderr[-3000:]
     stats = json.loads(r.stdout.strip().splitlines()[-1])
     assert stats["jit"] == 0 and stats["interp"] > 0
+
+
+def test_exact_overflow_raises_like_the_oracle(prof):
+    """A 128-bit overflow in a generated exact program raises (64-bit steps
+    overflow first and hand the row to the 128-bit path, which detects it)."""
+    bs = [table(20_000, 8, False)]
+    a4 = bin_(Op.Multiply, bin_(Op.Multiply, c(0), c(0)), bin_(Op.Multiply, c(0), c(0)))
+    agg = HashAggConfig([0], [AggExpr(2, AggFunc.Sum, "s")])
+    with pytest.raises(Exception) as ref_err:
+        oracle.filter_project_aggregate(bs, None, [5, 6], [a4], agg, arith_mode=ARITH_EXACT, n_threads=2)
+    with pytest.raises(prism_gpu.PrismError) as got_err:
+        prism_gpu.filter_project_aggregate(bs, None, [5, 6], [a4], agg, arith_mode=ARITH_EXACT, ctx=prof)
+    assert "overflow" in str(ref_err.value) and "overflow" in str(got_err.value)
+    # rows the filter drops never raise (no row has b > 1000)
+    pred = P.Gt(1, S.Int32(1000))
+    got = prism_gpu.filter_project_aggregate(bs, pred, [5, 6], [a4], agg, arith_mode=ARITH_EXACT, ctx=prof)
+    ref = oracle.filter_project_aggregate(bs, pred, [5, 6], [a4], agg, arith_mode=ARITH_EXACT, n_threads=2)
+    assert got.num_rows == ref.num_rows == 0
