@@ -195,6 +195,54 @@ __host__ __device__ constexpr unsigned long long tiny_init(int kind) {
   return kind == O_MIN ? 0x7fffffffffffffffULL : kind == O_MAX ? 0x8000000000000000ULL : 0ULL;
 }
 
+// one row's contribution to its slot's words; FAST: the ops E::kI64 marks
+// hold values that fit int64 (no 128-bit test)
+template <class E, int G, int NOPS, bool F64, int BLOCK, bool FAST>
+__device__ __forceinline__ void tiny_accumulate(const AggArgs& a, unsigned long long* col, int g, const Val* v,
+                                                unsigned long long (*spill)[NOPS][4]) {
+#pragma unroll
+  for (int j = 0; j < NOPS; ++j) {
+    const int kind = E::kKind[j];
+    const Val& x = v[j];
+    const bool use = !(E::kSkipNulls && !x.valid);
+    unsigned long long* w = col + E::kWord[j] * BLOCK;
+    if (kind == O_SUM_INT || kind == O_SUM_DEC) {
+      const bool narrow = FAST && E::kI64[j];
+      __int128 xi = use ? x.i : (__int128)0;
+      long long x64 = narrow ? (use ? (long long)x.i : 0LL) : (long long)xi;
+      long long p = (long long)w[0];
+      long long s = (long long)((unsigned long long)p + (unsigned long long)x64);
+      if ((narrow || (__int128)x64 == xi) && !(((p ^ s) & (x64 ^ s)) < 0)) {
+        w[0] = (unsigned long long)s;
+      } else {  // exact spill of partial + value; the partial restarts at 0
+        if (g < G) add_i128_limbs(&spill[g][j][0], (__int128)p + (narrow ? (__int128)x64 : xi), kind == O_SUM_INT ? 2 : 4);
+        w[0] = 0;
+      }
+    } else if (kind == O_SUM_F64) {
+      if (F64) {
+        double xf = use ? x.f : 0.0;
+        if (!isfinite(xf)) {  // NaN / inf: flag straight into the global accumulator
+          if (g < G) {
+            uint64_t u = (uint64_t)__double_as_longlong(xf);
+            atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(xf) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
+          }
+        } else {
+          double s, e;
+          two_sum(__longlong_as_double((long long)w[0]), xf, s, e);
+          w[0] = (unsigned long long)__double_as_longlong(s);
+          w[BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[BLOCK]) + e);
+        }
+      }
+    } else if (kind == O_MIN) {
+      if (use && !isnan(x.f)) w[0] = (unsigned long long)min((long long)w[0], (long long)total_key(x.f));
+    } else if (kind == O_MAX) {
+      if (use && !isnan(x.f)) w[0] = (unsigned long long)max((long long)w[0], (long long)total_key(x.f));
+    } else if (kind == O_NONNULL) {
+      w[0] += x.valid ? 1ULL : 0ULL;
+    }
+  }
+}
+
 template <class E, int G, int NOPS, bool F64, int BLOCK>
 __device__ __forceinline__ void tiny_body(const AggArgs& a) {
   constexpr int NW = E::kNW;
@@ -253,12 +301,21 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 #pragma unroll
       for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, rows[r], flags[r]);
     }
-    // phase 2: the rare 128-bit recomputations, then the accumulators
+    // phase 2: the accumulators; rows with a flagged op first get its
+    // 128-bit recomputation and take the general accumulate path, the others
+    // the lean one (ops known to fit int64 there)
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       const int g = slot[r];
+      const I at = base + r * stride;
+      unsigned long long* col = my + (g * NW) * BLOCK;
+      col[0] += 1;
+      // a thread meets its rows in increasing order: the first row of a
+      // group is the one seen while its bit is still clear
+      const unsigned bit = 1u << g;
+      if (!(seen & bit)) col[BLOCK] = a.row_base + (uint64_t)at;
+      seen |= bit;
       if (g < G && flags[r]) {
-        const I at = base + r * stride;
 #pragma unroll
         for (int j = 0; j < NOPS; ++j)
           if ((flags[r] >> (2 * j)) & 1u) {
@@ -268,53 +325,9 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
           }
 #pragma unroll
         for (int j = 0; j < NOPS; ++j) err |= ((flags[r] >> (2 * j + 1)) & 1u) != 0;
-      }
-      unsigned long long* col = my + (g * NW) * BLOCK;
-      col[0] += 1;
-      // a thread meets its rows in increasing order: the first row of a
-      // group is the one seen while its bit is still clear
-      const unsigned bit = 1u << g;
-      if (!(seen & bit)) col[BLOCK] = a.row_base + (uint64_t)(base + r * stride);
-      seen |= bit;
-#pragma unroll
-      for (int j = 0; j < NOPS; ++j) {
-        const int kind = E::kKind[j];
-        const Val& x = v[r][j];
-        const bool use = !(E::kSkipNulls && !x.valid);
-        unsigned long long* w = col + E::kWord[j] * BLOCK;
-        if (kind == O_SUM_INT || kind == O_SUM_DEC) {
-          __int128 xi = use ? x.i : (__int128)0;
-          long long x64 = (long long)xi;
-          long long p = (long long)w[0];
-          long long s = (long long)((unsigned long long)p + (unsigned long long)x64);
-          if ((__int128)x64 == xi && !(((p ^ s) & (x64 ^ s)) < 0)) {
-            w[0] = (unsigned long long)s;
-          } else {  // exact spill of partial + value; the partial restarts at 0
-            if (g < G) add_i128_limbs(&spill[g][j][0], (__int128)p + xi, kind == O_SUM_INT ? 2 : 4);
-            w[0] = 0;
-          }
-        } else if (kind == O_SUM_F64) {
-          if (F64) {
-            double xf = use ? x.f : 0.0;
-            if (!isfinite(xf)) {  // NaN / inf: flag straight into the global accumulator
-              if (g < G) {
-                uint64_t u = (uint64_t)__double_as_longlong(xf);
-                atomicOr(a.gacc + (size_t)g * a.W + a.op[j].word + LIMBS, isnan(xf) ? 1ULL : ((u >> 63) ? 4ULL : 2ULL));
-              }
-            } else {
-              double s, e;
-              two_sum(__longlong_as_double((long long)w[0]), xf, s, e);
-              w[0] = (unsigned long long)__double_as_longlong(s);
-              w[BLOCK] = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)w[BLOCK]) + e);
-            }
-          }
-        } else if (kind == O_MIN) {
-          if (use && !isnan(x.f)) w[0] = (unsigned long long)min((long long)w[0], (long long)total_key(x.f));
-        } else if (kind == O_MAX) {
-          if (use && !isnan(x.f)) w[0] = (unsigned long long)max((long long)w[0], (long long)total_key(x.f));
-        } else if (kind == O_NONNULL) {
-          w[0] += x.valid ? 1ULL : 0ULL;
-        }
+        tiny_accumulate<E, G, NOPS, F64, BLOCK, false>(a, col, g, v[r], spill);
+      } else {
+        tiny_accumulate<E, G, NOPS, F64, BLOCK, true>(a, col, g, v[r], spill);
       }
     }
   }

@@ -556,9 +556,8 @@ struct Gen {
               out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
                   << ")) < 0);\n";
             else  // safe when both factors lie inside int32; other rows take the 128-bit path
-              out << "    " << okv << " = " << okv << " && (unsigned long long)(" << l.n
-                  << " + 0x80000000LL) < 0x100000000ULL && (unsigned long long)(" << r.n
-                  << " + 0x80000000LL) < 0x100000000ULL;\n";
+              out << "    " << okv << " = " << okv << " && (long long)(int)" << l.n << " == " << l.n << " && (long long)(int)"
+                  << r.n << " == " << r.n << ";\n";
             bound = Mag{};
           }
           st.push_back({n, vv, bound});
@@ -680,12 +679,13 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   // operands
   gen.declare_cols();
   gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
-  std::ostringstream kinds, words, slow;
+  std::ostringstream kinds, words, slow, i64;
   int nw = TINY_FIRST_OP_WORD;  // words 0, 1 of a group: row count, first row
   for (int j = 0; j < a.n_ops; ++j) {
     const Op& o = a.op[j];
     if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) return "";
     kinds << (j ? ", " : "") << o.kind;
+    bool narrow = false;  // value fits int64 whenever the row's slow flag is clear
     words << (j ? ", " : "") << nw;
     nw += tiny_words(o.kind);
     const Src& sr = a.src[o.src];
@@ -697,6 +697,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
         break;
       }
       case S_COL_INT: {
+        narrow = true;
         std::string c = gen.col(sr.col);
         gen.out << "    r.i = " << gen.rd_cast("dcol_ival", "0LL", sr.col) << "; r.valid = " << gen.V(sr.col) << ";\n";
         break;
@@ -714,6 +715,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
       default: {
         std::string fval, fvalid, fok;
         bool fast = sr.kind == S_EXPR_I128 && gen.expr_fast64(sr.begin, sr.end, fval, fvalid, fok);
+        narrow = fast;
         if (fast) {
           // 64-bit steps here; when one of them overflowed, flag bit 2j asks
           // the caller for the 128-bit program (out of line in slow(), so it
@@ -735,6 +737,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
       }
     }
     gen.out << "    }\n";
+    i64 << (j ? ", " : "") << (narrow ? "true" : "false");
   }
   gen.out << "    return r;\n";
   std::string value = gen.take();
@@ -772,7 +775,8 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << ";\n"
        "  static constexpr int kNW = "
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
-    << a.n_ops << "] = {" << words.str() << "};\n"
+    << a.n_ops << "] = {" << words.str() << "};\n  static constexpr bool kI64[" << a.n_ops << "] = {" << i64.str()
+    << "};\n"
     << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
        "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
     << slow_cols << slow.str()
