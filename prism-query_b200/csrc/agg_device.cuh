@@ -316,16 +316,16 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       if (!(seen & bit)) col[BLOCK] = a.row_base + (uint64_t)at;
       seen |= bit;
       if (g < G && flags[r]) {
+        // every op of the row recomputed exactly (so the fast path's values
+        // need only their 64-bit form kept)
+        Val w[NOPS];
 #pragma unroll
-        for (int j = 0; j < NOPS; ++j)
-          if ((flags[r] >> (2 * j)) & 1u) {
-            SlowVal sv = E::slow(a, j, cols, at);
-            v[r][j] = sv.v;
-            if (sv.ovf) flags[r] |= 2u << (2 * j);
-          }
-#pragma unroll
-        for (int j = 0; j < NOPS; ++j) err |= ((flags[r] >> (2 * j + 1)) & 1u) != 0;
-        tiny_accumulate<E, G, NOPS, F64, BLOCK, false>(a, col, g, v[r], spill);
+        for (int j = 0; j < NOPS; ++j) {
+          SlowVal sv = E::slow(a, j, cols, at);
+          w[j] = sv.v;
+          err |= sv.ovf;
+        }
+        tiny_accumulate<E, G, NOPS, F64, BLOCK, false>(a, col, g, w, spill);
       } else {
         tiny_accumulate<E, G, NOPS, F64, BLOCK, true>(a, col, g, v[r], spill);
       }

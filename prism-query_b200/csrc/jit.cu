@@ -229,7 +229,12 @@ struct Gen {
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       if (!fetched((int)s)) continue;
       any = true;
-      o << "    unsigned long long r" << s << "[" << (col_type((int)s) == TY_DEC128 ? 2 : 1) << "];\n";
+      const Column& c = *b.cols[pg.cols[s]];
+      int t = c.type == TY_DICT ? c.index_type : c.type;
+      // one 32-bit register for columns of up to 4 bytes (read from its low bytes)
+      if (t == TY_DEC128) o << "    unsigned long long r" << s << "[2];\n";
+      else if (width_of(t) == 8) o << "    unsigned long long r" << s << "[1];\n";
+      else o << "    unsigned int r" << s << "[1];\n";
       if (nullable((int)s)) o << "    bool m" << s << ";\n";
     }
     if (!any) o << "    int unused;\n";
@@ -777,10 +782,13 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
     << a.n_ops << "] = {" << words.str() << "};\n  static constexpr bool kI64[" << a.n_ops << "] = {" << i64.str()
     << "};\n"
-    << "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
+    << "  // every op's exact value, out of line: 128-bit programs for ops with a\n"
+       "  // 64-bit fast path, value() itself for the others\n"
+       "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
        "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
     << slow_cols << slow.str()
-    << "    SlowVal s; s.v.i = 0; s.v.f = 0; s.v.valid = false; s.ovf = false;\n    return s;\n  }\n"
+    << "    unsigned fl = 0;\n    SlowVal s;\n    s.v = value(a, K, j, cols, idx, row, fl);\n"
+       "    s.ovf = ((fl >> (2 * j + 1)) & 1u) != 0;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "idx_t idx, const Row& row, unsigned& flags) {\n"
     << value
