@@ -182,10 +182,6 @@ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e
   e = (a - (s - bb)) + (b - bb);
 }
 
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
 // result of a generated program's out-of-line 128-bit path
 struct SlowVal {
   Val v;
@@ -287,13 +283,6 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
     // phase 1: the fixed-width columns of all TINY_R rows are loaded first
     // (straight-line loads, all in flight together), then evaluated with
     // arithmetic only (no stores, atomics or calls)
-    // the rows of the next step go to L2 now; these rows' loads were
-    // prefetched one step ago
-#pragma unroll
-    for (int r = 0; r < TINY_R; ++r) {
-      I ahead = base + (TINY_R + r) * stride;
-      if (ahead <= last) E::prefetch(cols, ahead);
-    }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       I at = base + r * stride;

@@ -260,17 +260,6 @@ struct Gen {
         o << "    w.m" << s << " = (cols[" << s << "].validity[idx >> 3] >> (idx & 7)) & 1;\n";
     }
     o << "    return w;\n  }\n";
-    // L2 prefetch of a later row's fixed-width values (no registers held)
-    o << "  static __device__ __forceinline__ void prefetch(const DCol* cols, idx_t idx) {\n";
-    for (size_t s = 0; s < pg.cols.size(); ++s) {
-      if (!fetched((int)s)) continue;
-      const Column& c = *b.cols[pg.cols[s]];
-      int t = c.type == TY_DICT ? c.index_type : c.type;
-      if (t == TY_BOOL) continue;
-      o << "    prefetch_l2(static_cast<const unsigned char*>(cols[" << s << "].values) + (size_t)idx * " << width_of(t)
-        << ");\n";
-    }
-    o << "  }\n";
     return o.str();
   }
 
