@@ -164,11 +164,14 @@ __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (
 // finalize kernels run.
 //
 // E supplies the row logic as code generated per query (jit.cu): E::Consts /
-// E::load (per-thread constants read once), E::keep (filter), E::gid (dense
-// group id), E::value (op j's operand; `live` = the row counts, so only then
-// may it raise an error), and the compile-time layout kKind[j] (op kinds),
-// kWord[j] (first word of op j in a group), kNW (words per group).
-constexpr int TINY_R = 4;        // rows in flight per thread
+// E::load (per-thread constants read once), E::Row / E::fetch (a row's
+// fixed-width column words, loaded first), E::keep (filter), E::gid (dense
+// group id), E::values (every op's operand, with per-op flags asking for the
+// exact recomputation E::slow or reporting an overflow), and the
+// compile-time layout kKind[j] (op kinds), kWord[j] (first word of op j in
+// a group), kNW (words per group), kI64[j] (op j's fast value fits int64),
+// kSkipNulls.
+constexpr int TINY_R = 2;        // rows in flight per thread
 constexpr int TINY_MAX_COLS = 16;
 // (G + 1) * kNW accumulator words per thread: up to 48 with 256-thread
 // blocks, up to 96 with 128-thread blocks (96 KB of shared memory a block)
@@ -298,8 +301,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       err |= bad;
       slot[r] = (keep && !bad) ? g : G;
       flags[r] = 0;
-#pragma unroll
-      for (int j = 0; j < NOPS; ++j) v[r][j] = E::value(a, K, j, cols, idx, rows[r], flags[r]);
+      E::values(a, K, cols, idx, rows[r], v[r], flags[r]);
     }
     // phase 2: the accumulators; rows with a flagged op first get its
     // 128-bit recomputation and take the general accumulate path, the others

@@ -493,16 +493,21 @@ struct Gen {
   }
 
   // 64-bit fast path of an exact (int128) program: the same values computed
-  // in int64 with an overflow flag per step; exact whenever no step
-  // overflowed (then `ok` stays true). Emits into `out`; returns the names
-  // of the value, validity and ok variables, or false when the program has
-  // a node the fast path does not take (IfThen, Float64 steps, Decimal128 or
-  // UInt64 columns).
+  // in int64, each step with an "ok" flag (no overflow, and for products
+  // both factors inside int32); exact whenever the root's flag holds.
+  // Emits into `out`; returns the names of the value, validity and ok
+  // variables, or false when the program has a node the fast path does not
+  // take (IfThen, Float64 steps, Decimal128 or UInt64 columns). With `cse`,
+  // subtrees met before in this function (same columns, literal values and
+  // operations) are reused instead of recomputed.
+  struct FV {
+    std::string n, v, ok;
+    Mag mag;
+  };
+  std::unordered_map<std::string, FV> cse_map;
+  bool cse = false;
+
   bool expr_fast64(int begin, int end, std::string& val, std::string& valid, std::string& okv) {
-    struct FV {
-      std::string n, v;
-      Mag mag;
-    };
     for (int k = begin; k < end; ++k) {
       int op = pg.enodes[k].op;
       if (op == E_COL_I128) {
@@ -516,20 +521,43 @@ struct Gen {
     }
     const unsigned __int128 I64_MAX = ((unsigned __int128)1 << 63) - 1;
     auto fits64 = [&](Mag m) { return !m.unknown && m.m <= I64_MAX; };
-    okv = fresh("fok");
-    out << "    bool " << okv << " = true;\n";
-    std::vector<FV> st;
+    auto in32 = [&](const std::string& x) { return "(long long)(int)" + x + " == " + x; };
+    std::vector<std::pair<std::string, FV>> st;  // (signature, value)
     for (int k = begin; k < end; ++k) {
       const ENode& nd = pg.enodes[k];
-      std::string n = fresh("f"), vv = fresh("fv"), K = std::to_string(k);
+      std::string K = std::to_string(k);
+      std::string sig;
+      std::vector<std::pair<std::string, FV>> kids;
+      int arity = (nd.op == E_ADD_I || nd.op == E_SUB_I || nd.op == E_MUL_I) ? 2
+                  : (nd.op == E_NEG_I || nd.op == E_SCALE_I) ? 1 : 0;
+      if ((int)st.size() < arity) gen_fail("expression stack underflow");
+      for (int q = 0; q < arity; ++q) kids.insert(kids.begin(), st.back()), st.pop_back();
+      switch (nd.op) {
+        case E_COL_I128: sig = "c" + std::to_string(nd.col) + (nd.a ? "r" : ""); break;
+        case E_LIT_I128: sig = "l" + std::to_string(nd.lo) + ":" + std::to_string(nd.hi); break;
+        case E_SCALE_I: sig = "s" + std::to_string(nd.col) + "(" + kids[0].first + ")"; break;
+        case E_NEG_I: sig = "n(" + kids[0].first + ")"; break;
+        default: sig = std::to_string(nd.op) + "(" + kids[0].first + "," + kids[1].first + ")";
+      }
+      if (cse) {
+        auto it = cse_map.find(sig);
+        if (it != cse_map.end()) {
+          st.push_back({sig, it->second});
+          continue;
+        }
+      }
+      FV f;
+      f.n = fresh("f");
+      f.v = fresh("fv");
+      f.ok = fresh("fo");
       switch (nd.op) {
         case E_COL_I128: {
           std::string c = col(nd.col);
           const Column& cc = *b.cols[pg.cols[nd.col]];
           int t = cc.type == TY_DICT ? cc.index_type : cc.type;
-          out << "    long long " << n << " = " << (nd.a ? rd("dcol_ival", nd.col) : rd_cast("dcol_ival", "0LL", nd.col))
-              << "; bool " << vv << " = " << V(nd.col) << ";\n";
-          st.push_back({n, vv, type_mag(t)});
+          out << "    long long " << f.n << " = " << (nd.a ? rd("dcol_ival", nd.col) : rd_cast("dcol_ival", "0LL", nd.col))
+              << "; bool " << f.v << " = " << V(nd.col) << "; const bool " << f.ok << " = true;\n";
+          f.mag = type_mag(t);
           break;
         }
         case E_LIT_I128: {
@@ -540,60 +568,61 @@ struct Gen {
           while (bits < 127 && ((unsigned __int128)1 << bits) < m) ++bits;
           konst("__int128", "ei" + K,
                 "(__int128)(((unsigned __int128)(uint64_t)a.en[" + K + "].hi << 64) | (uint64_t)a.en[" + K + "].lo)");
-          out << "    long long " << n << " = (long long)K.ei" << K << "; bool " << vv << " = true; " << okv << " = " << okv
-              << " && (__int128)" << n << " == K.ei" << K << ";  // |literal| <= 2^" << bits << "\n";
-          st.push_back({n, vv, mag_of((unsigned __int128)1 << bits)});
+          out << "    long long " << f.n << " = (long long)K.ei" << K << "; const bool " << f.v << " = true; bool " << f.ok
+              << " = (__int128)" << f.n << " == K.ei" << K << ";  // |literal| <= 2^" << bits << "\n";
+          f.mag = mag_of((unsigned __int128)1 << bits);
           break;
         }
         case E_ADD_I: case E_SUB_I: case E_MUL_I: {
-          if (st.size() < 2) gen_fail("expression stack underflow");
-          FV r = st.back(); st.pop_back();
-          FV l = st.back(); st.pop_back();
+          const FV& l = kids[0].second;
+          const FV& r = kids[1].second;
           Mag bound = nd.op == E_MUL_I ? mag_mul(l.mag, r.mag) : mag_add(l.mag, r.mag);
           const char* o = nd.op == E_ADD_I ? "+" : nd.op == E_SUB_I ? "-" : "*";
-          out << "    long long " << n << " = (long long)((unsigned long long)" << l.n << " " << o << " (unsigned long long)"
-              << r.n << "); bool " << vv << " = " << l.v << " && " << r.v << ";\n";
+          out << "    long long " << f.n << " = (long long)((unsigned long long)" << l.n << " " << o << " (unsigned long long)"
+              << r.n << "); bool " << f.v << " = " << l.v << " && " << r.v << "; bool " << f.ok << " = " << l.ok << " && "
+              << r.ok;
           if (!fits64(bound)) {
             if (nd.op == E_ADD_I)
-              out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << n << ") & (" << r.n << " ^ " << n
-                  << ")) < 0);\n";
+              out << " && !(((" << l.n << " ^ " << f.n << ") & (" << r.n << " ^ " << f.n << ")) < 0)";
             else if (nd.op == E_SUB_I)
-              out << "    " << okv << " = " << okv << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << n
-                  << ")) < 0);\n";
+              out << " && !(((" << l.n << " ^ " << r.n << ") & (" << l.n << " ^ " << f.n << ")) < 0)";
             else  // safe when both factors lie inside int32; other rows take the 128-bit path
-              out << "    " << okv << " = " << okv << " && (long long)(int)" << l.n << " == " << l.n << " && (long long)(int)"
-                  << r.n << " == " << r.n << ";\n";
+              out << " && " << (fits64(l.mag) && l.mag.m <= 0x7fffffff ? "true" : in32(l.n)) << " && "
+                  << (fits64(r.mag) && r.mag.m <= 0x7fffffff ? "true" : in32(r.n));
             bound = Mag{};
           }
-          st.push_back({n, vv, bound});
+          out << ";\n";
+          f.mag = bound;
           break;
         }
         case E_NEG_I: {
-          if (st.empty()) gen_fail("expression stack underflow");
-          FV x = st.back(); st.pop_back();
-          out << "    long long " << n << " = (long long)(0ULL - (unsigned long long)" << x.n << "); bool " << vv << " = "
-              << x.v << "; " << okv << " = " << okv << " && " << x.n << " != (long long)0x8000000000000000ULL;\n";
-          st.push_back({n, vv, x.mag});
+          const FV& x = kids[0].second;
+          out << "    long long " << f.n << " = (long long)(0ULL - (unsigned long long)" << x.n << "); bool " << f.v << " = "
+              << x.v << "; bool " << f.ok << " = " << x.ok << " && " << x.n << " != (long long)0x8000000000000000ULL;\n";
+          f.mag = x.mag;
           break;
         }
         case E_SCALE_I: {
-          if (st.empty()) gen_fail("expression stack underflow");
-          FV x = st.back(); st.pop_back();
+          const FV& x = kids[0].second;
           long long p10 = 1;
           for (int q = 0; q < nd.col; ++q) p10 *= 10;
-          out << "    long long " << n << " = (long long)((unsigned long long)" << x.n << " * " << p10 << "ULL); bool " << vv
-              << " = " << x.v << "; " << okv << " = " << okv << " && (" << x.n << " < 0 ? 0ULL - (unsigned long long)" << x.n
-              << " : (unsigned long long)" << x.n << ") <= " << (9223372036854775807LL / p10) << "ULL;\n";
-          st.push_back({n, vv, Mag{}});
+          out << "    long long " << f.n << " = (long long)((unsigned long long)" << x.n << " * " << p10 << "ULL); bool "
+              << f.v << " = " << x.v << "; bool " << f.ok << " = " << x.ok << " && (" << x.n
+              << " < 0 ? 0ULL - (unsigned long long)" << x.n << " : (unsigned long long)" << x.n
+              << ") <= " << (9223372036854775807LL / p10) << "ULL;\n";
+          f.mag = Mag{};
           break;
         }
         default:
           gen_fail("unknown expression node");
       }
+      if (cse) cse_map[sig] = f;
+      st.push_back({sig, f});
     }
     if (st.size() != 1) gen_fail("expression leaves more than one value");
-    val = st.back().n;
-    valid = st.back().v;
+    val = st.back().second.n;
+    valid = st.back().second.v;
+    okv = st.back().second.ok;
     return true;
   }
 
@@ -746,6 +775,49 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   }
   gen.out << "    return r;\n";
   std::string value = gen.take();
+  // values(): every op of a row in one straight-line body (the hot path);
+  // subtrees shared between ops' 64-bit programs are computed once
+  gen.declare_cols();
+  gen.cse = true;
+  gen.cse_map.clear();
+  for (int j = 0; j < a.n_ops; ++j) {
+    const Src& sr = a.src[a.op[j].src];
+    std::string o = "out[" + std::to_string(j) + "]";
+    switch (sr.kind) {
+      case S_COL_F64:
+        gen.col(sr.col);
+        gen.out << "    " << o << ".i = 0; " << o << ".f = " << gen.rd_cast("dcol_fval", "0.0", sr.col) << "; " << o
+                << ".valid = " << gen.V(sr.col) << ";\n";
+        break;
+      case S_COL_INT:
+        gen.col(sr.col);
+        gen.out << "    " << o << ".f = 0; " << o << ".i = " << gen.rd_cast("dcol_ival", "0LL", sr.col) << "; " << o
+                << ".valid = " << gen.V(sr.col) << ";\n";
+        break;
+      case S_COL_I128:
+        gen.col(sr.col);
+        gen.out << "    " << o << ".f = 0; " << o << ".i = " << gen.rd_cast("dcol_i128", "(__int128)0", sr.col) << "; " << o
+                << ".valid = " << gen.V(sr.col) << ";\n";
+        break;
+      case S_VALID:
+        gen.col(sr.col);
+        gen.out << "    " << o << ".i = 0; " << o << ".f = 0; " << o << ".valid = " << gen.V(sr.col) << ";\n";
+        break;
+      default: {
+        std::string fval, fvalid, fok;
+        if (sr.kind == S_EXPR_I128 && gen.expr_fast64(sr.begin, sr.end, fval, fvalid, fok)) {
+          gen.out << "    " << o << ".f = 0; " << o << ".i = (__int128)" << fval << "; " << o << ".valid = " << fvalid
+                  << "; if (!" << fok << ") flags |= " << (1u << (2 * j)) << "u;\n";
+        } else {
+          gen.out << "    {\n    bool ovf = false;\n";
+          std::string v = gen.expr(sr.begin, sr.end, "ovf");
+          gen.out << "    " << o << " = " << v << ";\n    if (ovf) flags |= " << (2u << (2 * j)) << "u;\n    }\n";
+        }
+      }
+    }
+  }
+  gen.cse = false;
+  std::string values_body = gen.take();
   gen.declare_cols();
   std::string slow_cols = gen.take();
   const int block = tiny_block((g + 1) * nw);
@@ -789,6 +861,9 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << slow_cols << slow.str()
     << "    unsigned fl = 0;\n    SlowVal s;\n    s.v = value(a, K, j, cols, idx, row, fl);\n"
        "    s.ovf = ((fl >> (2 * j + 1)) & 1u) != 0;\n    return s;\n  }\n"
+    << "  static __device__ __forceinline__ void values(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
+       "const Row& row, Val* out, unsigned& flags) {\n"
+    << values_body << "  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "idx_t idx, const Row& row, unsigned& flags) {\n"
     << value
