@@ -397,8 +397,10 @@ class C1:
         import pyarrow as pa
 
         t = self.torch
+        schema = pa.schema([pa.field("key", pa.int64(), nullable=False), pa.field("v_i", pa.int64(), nullable=False),
+                            pa.field("v_f", pa.float64(), nullable=False)])  # as the device batch declares them
         return pa.RecordBatch.from_arrays([host_array(t, pa, self.key, pa.int64()), host_array(t, pa, self.vi, pa.int64()),
-                                           host_array(t, pa, self.vf, pa.float64())], names=["key", "v_i", "v_f"])
+                                           host_array(t, pa, self.vf, pa.float64())], schema=schema)
 
     def check(self):
         from helpers import assert_batches_equal
