@@ -2,6 +2,7 @@
 //
 // Every entry point catches failures and returns a status code (the library
 // never aborts); the message is kept on the context for prism_last_error().
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 
@@ -54,7 +55,13 @@ std::vector<int> ints(const int32_t* p, int n) {
   return std::vector<int>(p, p + std::max(0, n));
 }
 
-JoinTuning join_tuning() { return JoinTuning{}; }
+// PRISM_JOIN_DENSE=0 keeps single Int64 keys in the hash table (dense mode off)
+JoinTuning join_tuning() {
+  JoinTuning t{};
+  const char* d = std::getenv("PRISM_JOIN_DENSE");
+  if (d && std::strcmp(d, "0") == 0) t.dense = false;
+  return t;
+}
 AggTuning agg_tuning() { return AggTuning{}; }
 
 std::string right_name(const Batch& probe, const std::string& nm) {

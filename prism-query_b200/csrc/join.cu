@@ -197,8 +197,13 @@ __global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulo
 }
 
 // ------------------------------------------------------------- the probe --
+constexpr uint32_t NO_MATCH = 0xFFFFFFFFu;
+
 struct ProbeArgs {
   int64_t n;
+  const uint32_t* dense;  // dense mode (see JoinTable), else nullptr
+  int64_t dmin;
+  uint64_t drange;
   const ulonglong2* slots;
   int shift;
   uint64_t mask;
@@ -312,7 +317,23 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
     const int64_t base = tile * PT + warp * (32 * PI);
 
     uint32_t c[PI], v[PI], cand[PI];
-    {
+    if (K::kFast && a.dense != nullptr) {
+      // dense mode: one direct lookup per row
+#pragma unroll
+      for (int it = 0; it < PI; ++it) {
+        int64_t r = base + it * 32 + lane;
+        c[it] = v[it] = cand[it] = 0;
+        if (r < a.n) {
+          uint64_t d = keys.key(r) - (uint64_t)a.dmin;
+          uint32_t row = d < a.drange ? __ldg(a.dense + d) : NO_MATCH;
+          if (row != NO_MATCH) {
+            v[it] = row;
+            cand[it] = 1;
+            c[it] = 1;
+          }
+        }
+      }
+    } else {
       uint64_t key[PI];
       uint64_t s[PI];
       ulonglong2 e[PI];
@@ -423,7 +444,6 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
 constexpr int QB = 256;            // threads per CTA
 constexpr int QI = 8;              // rows per thread
 constexpr int QT = QB * QI;        // rows per tile (2048)
-constexpr uint32_t NO_MATCH = 0xFFFFFFFFu;
 
 __global__ void __launch_bounds__(QB, 3) probe_rows_kernel(const int64_t* __restrict__ keys, int64_t n,
                                                           const ulonglong2* __restrict__ slots, int shift,
@@ -471,6 +491,72 @@ __global__ void __launch_bounds__(QB, 3) probe_rows_kernel(const int64_t* __rest
 #pragma unroll
     for (int w = 0; w < QB / 32; ++w) t += wsum[w];
     tile_cnt[blockIdx.x] = t;
+  }
+}
+
+// dense-mode twin of probe_rows_kernel: row = dense[key - dmin]
+__global__ void __launch_bounds__(QB, 4) probe_rows_dense_kernel(const int64_t* __restrict__ keys, int64_t n,
+                                                                const uint32_t* __restrict__ dense, int64_t dmin,
+                                                                uint64_t drange, uint32_t* __restrict__ rowv,
+                                                                uint32_t* __restrict__ tile_cnt) {
+  const int64_t base = (int64_t)blockIdx.x * QT;
+  uint64_t d[QI];
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    d[it] = r < n ? (uint64_t)__ldg(keys + r) - (uint64_t)dmin : ~0ULL;
+  }
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int it = 0; it < QI; ++it) {
+    int64_t r = base + it * QB + threadIdx.x;
+    uint32_t row = d[it] < drange ? __ldg(dense + d[it]) : NO_MATCH;
+    if (r < n) rowv[r] = row;
+    cnt += (r < n && row != NO_MATCH) ? 1u : 0u;
+  }
+#pragma unroll
+  for (int k = 16; k > 0; k >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, k);
+  __shared__ uint32_t wsum[QB / 32];
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < QB / 32; ++w) t += wsum[w];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+// min / max of the build keys (dense-mode test)
+__global__ void minmax_i64_kernel(const int64_t* __restrict__ keys, int64_t n, long long* mm) {
+  long long lo = 0x7fffffffffffffffLL, hi = (long long)0x8000000000000000ULL;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    long long k = __ldg(keys + i);
+    lo = min(lo, k);
+    hi = max(hi, k);
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(mm, lo);
+    atomicMax(mm + 1, hi);
+  }
+}
+
+__global__ void fill_u32_kernel(uint32_t* p, uint64_t n, uint32_t v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// dense insert: dense[key - dmin] = row; a second row for a key sets *dup
+__global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t dmin, uint32_t* dense,
+                                    uint32_t* dup) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t d = (uint64_t)__ldg(keys + i) - (uint64_t)dmin;
+    if (atomicCAS(dense + d, NO_MATCH, (uint32_t)i) != NO_MATCH) atomicOr(dup, 1u);
   }
 }
 
@@ -555,6 +641,53 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   int64_t n = build.rows;
   if (n >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "build side exceeds 2^32-1 rows");
   t->int64_fast = keys.size() == 1 && build.cols[keys[0]]->type == TY_I64;
+  for (int k : keys) t->key_views.push_back(build.cols[k]->view());
+  t->key_views_dev = ctx.alloc(t->key_views.size() * sizeof(DCol));
+  PRISM_CUDA(cudaMemcpyAsync(t->key_views_dev->ptr, t->key_views.data(), t->key_views.size() * sizeof(DCol),
+                             cudaMemcpyHostToDevice, ctx.stream));
+  if (t->int64_fast && n > 0 && tune.dense) {
+    // dense mode when the keys span a range of at most twice the rows (plus
+    // 4096) and are unique: a direct row index per key value replaces the
+    // hash slots (4 bytes per value of the range instead of 16 per slot at
+    // load factor 0.5, and one dependent load per probe)
+    const int64_t* bk = static_cast<const int64_t*>(build.cols[keys[0]]->values);
+    MemP mmm;
+    long long* mm = ctx.alloc_t<long long>(2, mmm);
+    const long long init[2] = {0x7fffffffffffffffLL, (long long)0x8000000000000000ULL};
+    PRISM_CUDA(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, ctx.stream));
+    minmax_i64_kernel<<<grid_for(ctx, n, 256, 8), 256, 0, ctx.stream>>>(bk, n, mm);
+    ctx.check_launch("minmax_i64_kernel");
+    long long h[2];
+    PRISM_CUDA(cudaMemcpyAsync(h, mm, 16, cudaMemcpyDeviceToHost, ctx.stream));
+    PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+    unsigned __int128 range = (unsigned __int128)((__int128)h[1] - (__int128)h[0]) + 1;
+    if (range <= (unsigned __int128)(2 * n + 4096) && range <= ((unsigned __int128)1 << 28)) {
+      uint64_t r = (uint64_t)range;
+      MemP dense = ctx.alloc(r * 4);
+      uint32_t* dr = static_cast<uint32_t*>(dense->ptr);
+      fill_u32_kernel<<<grid_for(ctx, (int64_t)r, 256, 8), 256, 0, ctx.stream>>>(dr, r, NO_MATCH);
+      ctx.check_launch("fill_u32_kernel");
+      MemP mdf;
+      uint32_t* df = ctx.alloc_t<uint32_t>(1, mdf);
+      PRISM_CUDA(cudaMemsetAsync(df, 0, 4, ctx.stream));
+      {
+        KernelTimer kt(ctx, "insert_kernel");
+        dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, h[0], dr, df);
+      }
+      ctx.check_launch("dense_insert_kernel");
+      uint32_t hdf = 0;
+      PRISM_CUDA(cudaMemcpyAsync(&hdf, df, 4, cudaMemcpyDeviceToHost, ctx.stream));
+      PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+      if (!hdf) {
+        t->dense = true;
+        t->dmin = h[0];
+        t->drange = r;
+        t->dense_rows = dense;
+        return t;
+      }
+      // a repeated key: the hash table below keeps every row
+    }
+  }
   double lf = std::min(0.9, std::max(0.1, tune.load_factor));
   uint64_t cap = next_pow2((uint64_t)std::ceil((double)std::max<int64_t>(n, 1) / lf));
   if (cap < 16) cap = 16;
@@ -565,10 +698,6 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   init_slots_kernel<<<grid_for(ctx, (int64_t)cap + 1, 256), 256, 0, ctx.stream>>>(slots, cap + 1);
   ctx.check_launch("init_slots_kernel");
 
-  for (int k : keys) t->key_views.push_back(build.cols[k]->view());
-  t->key_views_dev = ctx.alloc(t->key_views.size() * sizeof(DCol));
-  PRISM_CUDA(cudaMemcpyAsync(t->key_views_dev->ptr, t->key_views.data(), t->key_views.size() * sizeof(DCol),
-                             cudaMemcpyHostToDevice, ctx.stream));
   MemP mflag;
   uint32_t* dupflag = ctx.alloc_t<uint32_t>(1, mflag);
   PRISM_CUDA(cudaMemsetAsync(dupflag, 0, 4, ctx.stream));
@@ -634,7 +763,10 @@ static void fill_common(Ctx& ctx, const JoinTable& t, const Batch& probe, const 
                         std::vector<DCol>& pviews, MemP& pviews_dev) {
   a = ProbeArgs{};
   a.n = probe.rows;
-  a.slots = static_cast<const ulonglong2*>(t.slots->ptr);
+  a.dense = t.dense ? static_cast<const uint32_t*>(t.dense_rows->ptr) : nullptr;
+  a.dmin = t.dmin;
+  a.drange = t.drange;
+  a.slots = t.slots ? static_cast<const ulonglong2*>(t.slots->ptr) : nullptr;
   a.shift = 64 - t.log2cap;
   a.mask = t.capacity - 1;
   a.cap = t.capacity;
@@ -714,8 +846,11 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     a.err = ctx.d_err;
     {
       KernelTimer kt(ctx, "probe_rows_kernel");
-      probe_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(static_cast<const int64_t*>(probe.cols[keys[0]]->values),
-                                                                  n, a.slots, a.shift, a.mask, a.cap, rowv, tcnt);
+      const int64_t* pk = static_cast<const int64_t*>(probe.cols[keys[0]]->values);
+      if (t.dense)
+        probe_rows_dense_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(pk, n, a.dense, a.dmin, a.drange, rowv, tcnt);
+      else
+        probe_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(pk, n, a.slots, a.shift, a.mask, a.cap, rowv, tcnt);
     }
     ctx.check_launch("probe_rows_kernel");
     scan_u32_async(ctx, tcnt, toff, ntiles, dtot);
@@ -825,7 +960,10 @@ extern "C" int prism_hash_table_probe_noalloc(prism_ctx* c, const prism_hash_tab
 
     ProbeArgs a{};
     a.n = n_probe;
-    a.slots = static_cast<const ulonglong2*>(t.slots->ptr);
+    a.dense = t.dense ? static_cast<const uint32_t*>(t.dense_rows->ptr) : nullptr;
+    a.dmin = t.dmin;
+    a.drange = t.drange;
+    a.slots = t.slots ? static_cast<const ulonglong2*>(t.slots->ptr) : nullptr;
     a.shift = 64 - t.log2cap;
     a.mask = t.capacity - 1;
     a.cap = t.capacity;

@@ -14,6 +14,13 @@ struct JoinTable {
   int log2cap = 0;
   uint64_t capacity = 0;     // power of two (+1 side slot at [capacity])
   MemP slots;                // ulonglong2 per slot: x = key (or row hash), y = cnt << 32 | row
+  // dense mode (single Int64 key, unique keys spanning a range at most about
+  // twice the row count): dense_rows[key - dmin] = build row, or NO_MATCH;
+  // no hash slots are built
+  bool dense = false;
+  int64_t dmin = 0;
+  uint64_t drange = 0;
+  MemP dense_rows;
   bool has_dups = false;     // some slot holds more than one build row
   MemP dup_rows;             // build rows grouped by slot, ascending inside a slot
   int64_t n_dup_rows = 0;
@@ -24,6 +31,7 @@ struct JoinTable {
 struct JoinTuning {
   double load_factor = 0.5;
   int probe_blocks_per_sm = 2;
+  bool dense = true;  // allow dense mode for single Int64 keys
 };
 
 std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,

@@ -172,3 +172,25 @@ def test_join_project_emits_probe_row_and_payload(ctx):
     assert np.array_equal(out.column(1).to_numpy(), build.column(1).to_numpy()[bidx])
     assert np.array_equal(out.column(2).to_numpy(), probe.column(1).to_numpy()[ref.column(0).to_numpy()])
     assert out.schema.names == ["probe_idx", "payload", "x"]
+
+
+@pytest.mark.parametrize("mode", ["1", "0"])
+def test_unique_int64_keys_dense_and_hash_tables(ctx, mode, monkeypatch):
+    """Unique Int64 build keys over a compact range use the dense table
+    (PRISM_JOIN_DENSE unset or 1); the hash table (0) must give the same rows.
+    A repeated key in a compact range falls back to the hash table."""
+    monkeypatch.setenv("PRISM_JOIN_DENSE", mode)
+    cases = [(3000, 20000, 4000, False, False), (3000, 20000, 4000, True, False), (50000, 70000, 60000, False, False),
+             (3000, 9000, 4000, False, True)]
+    for i, (nb, npr, kr, nulls, dup) in enumerate(cases):
+        probe, build = _int_join_batches(40 + i, nb, npr, kr, dup=dup, nulls=nulls)
+        for jt in (JoinType.Inner, JoinType.Left, JoinType.LeftSemi, JoinType.LeftAnti):
+            cfg = HashJoinConfig(jt, build_keys=[0], probe_keys=[0])
+            assert_batches_equal(prism_gpu.hash_join(probe, build, cfg), oracle.hash_join(probe, build, cfg))
+    # a compact range with one key repeated
+    bk = np.arange(1000, dtype=np.int64)
+    bk[500] = 7
+    build = pa.RecordBatch.from_arrays([pa.array(bk), pa.array(np.arange(1000, dtype=np.int64))], names=["k", "v"])
+    probe = pa.RecordBatch.from_arrays([pa.array(np.arange(-3, 1003, dtype=np.int64))], names=["k"])
+    cfg = HashJoinConfig(JoinType.Inner, build_keys=[0], probe_keys=[0])
+    assert_batches_equal(prism_gpu.hash_join(probe, build, cfg), oracle.hash_join(probe, build, cfg))
