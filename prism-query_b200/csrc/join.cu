@@ -586,46 +586,15 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
   }
   __syncthreads();
   const uint64_t off = tile_off[blockIdx.x];
-  uint64_t pos[QI];
-  bool ok[QI];
 #pragma unroll
   for (int it = 0; it < QI; ++it) {
-    pos[it] = off + seg[it][warp] + lpos[it];
-    ok[it] = v[it] != NO_MATCH;
-    if (ok[it] && pos[it] >= a.out_capacity) {
+    if (v[it] == NO_MATCH) continue;
+    uint64_t pos = off + seg[it][warp] + lpos[it];
+    if (pos >= a.out_capacity) {
       atomicOr(a.err, DERR_CAPACITY);
-      ok[it] = false;
+      continue;
     }
-  }
-#pragma unroll
-  for (int it = 0; it < QI; ++it) {
-    if (!ok[it]) continue;
-    if (a.out_probe) a.out_probe[pos[it]] = (uint32_t)(base + it * QB + threadIdx.x);
-    if (a.out_build) a.out_build[pos[it]] = v[it];
-  }
-  // fused gathers: all QI loads of a column are issued before its stores
-  // (the stores could alias the sources for all the compiler knows)
-  for (int g = 0; g < a.ngather; ++g) {
-    const bool bside = a.g_side[g] != 0;
-    if (a.g_width[g] == 8) {
-      const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[g]);
-      unsigned long long val[QI];
-#pragma unroll
-      for (int it = 0; it < QI; ++it)
-        if (ok[it]) val[it] = __ldg(src + (bside ? (int64_t)v[it] : base + it * QB + threadIdx.x));
-#pragma unroll
-      for (int it = 0; it < QI; ++it)
-        if (ok[it]) static_cast<unsigned long long*>(a.g_dst[g])[pos[it]] = val[it];
-    } else {
-      const unsigned int* src = static_cast<const unsigned int*>(a.g_src[g]);
-      unsigned int val[QI];
-#pragma unroll
-      for (int it = 0; it < QI; ++it)
-        if (ok[it]) val[it] = __ldg(src + (bside ? (int64_t)v[it] : base + it * QB + threadIdx.x));
-#pragma unroll
-      for (int it = 0; it < QI; ++it)
-        if (ok[it]) static_cast<unsigned int*>(a.g_dst[g])[pos[it]] = val[it];
-    }
+    emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
   }
 }
 
