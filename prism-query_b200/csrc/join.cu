@@ -494,59 +494,6 @@ __global__ void __launch_bounds__(QB, 3) probe_rows_kernel(const int64_t* __rest
   }
 }
 
-// general keys (multi-column, Utf8, floats ...) of a table without repeated
-// keys: the same sync-free first kernel as probe_rows_kernel, with the row
-// hash for the slot walk and keys_equal verification of the candidate
-__global__ void __launch_bounds__(QB, 3) probe_rows_general_kernel(KeysGeneral keys, int64_t n,
-                                                                  const ulonglong2* __restrict__ slots, int shift,
-                                                                  uint64_t mask, const DCol* bcols,
-                                                                  uint32_t* __restrict__ rowv,
-                                                                  uint32_t* __restrict__ tile_cnt) {
-  const int64_t base = (int64_t)blockIdx.x * QT;
-  uint64_t key[QI], s[QI];
-  ulonglong2 e[QI];
-#pragma unroll
-  for (int it = 0; it < QI; ++it) {
-    int64_t r = base + it * QB + threadIdx.x;
-    key[it] = r < n ? keys.key(r) : EMPTY;
-  }
-#pragma unroll
-  for (int it = 0; it < QI; ++it) {
-    int64_t r = base + it * QB + threadIdx.x;
-    if (r < n) {
-      s[it] = slot_of(key[it], shift);
-      e[it] = __ldg(slots + s[it]);
-    }
-  }
-  uint32_t cnt = 0;
-#pragma unroll
-  for (int it = 0; it < QI; ++it) {
-    int64_t r = base + it * QB + threadIdx.x;
-    if (r >= n) continue;
-    uint64_t steps = 0;
-    while (e[it].x != key[it] && e[it].x != EMPTY && steps <= mask) {
-      s[it] = (s[it] + 1) & mask;
-      e[it] = __ldg(slots + s[it]);
-      ++steps;
-    }
-    bool hit = e[it].x == key[it] && (e[it].y >> 32) != 0 &&
-               rows_equal(keys.cols, bcols, keys.n, r, (int64_t)(uint32_t)e[it].y);
-    rowv[r] = hit ? (uint32_t)e[it].y : NO_MATCH;
-    cnt += hit ? 1u : 0u;
-  }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
-  __shared__ uint32_t wsum[QB / 32];
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-#pragma unroll
-    for (int w = 0; w < QB / 32; ++w) t += wsum[w];
-    tile_cnt[blockIdx.x] = t;
-  }
-}
-
 // dense-mode twin of probe_rows_kernel: row = dense[key - dmin]
 __global__ void __launch_bounds__(QB, 4) probe_rows_dense_kernel(const int64_t* __restrict__ keys, int64_t n,
                                                                 const uint32_t* __restrict__ dense, int64_t dmin,
@@ -888,9 +835,8 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     a.g_dst[g] = gathers[g].dst;
   }
   a.out_capacity = (uint64_t)cap;
-  if (!t.has_dups) {
-    // no repeated keys: probe (one u32 per probe row), scan of tile counts,
-    // ordered emit
+  if (t.int64_fast && !t.has_dups) {
+    // unique Int64 keys: probe, scan of tile counts, ordered emit
     int64_t n = probe.rows, ntiles = ceil_div(n, QT);
     MemP mrow, mcnt, moff, mtot;
     uint32_t* rowv = ctx.alloc_t<uint32_t>((size_t)n, mrow);
@@ -903,11 +849,8 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
       const int64_t* pk = static_cast<const int64_t*>(probe.cols[keys[0]]->values);
       if (t.dense)
         probe_rows_dense_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(pk, n, a.dense, a.dmin, a.drange, rowv, tcnt);
-      else if (t.int64_fast)
-        probe_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(pk, n, a.slots, a.shift, a.mask, a.cap, rowv, tcnt);
       else
-        probe_rows_general_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(KeysGeneral{a.pcols, a.nkeys}, n, a.slots,
-                                                                            a.shift, a.mask, a.bcols, rowv, tcnt);
+        probe_rows_kernel<<<(unsigned)ntiles, QB, 0, ctx.stream>>>(pk, n, a.slots, a.shift, a.mask, a.cap, rowv, tcnt);
     }
     ctx.check_launch("probe_rows_kernel");
     scan_u32_async(ctx, tcnt, toff, ntiles, dtot);
