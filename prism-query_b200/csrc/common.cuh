@@ -143,18 +143,22 @@ __device__ __forceinline__ uint64_t fx_word(uint64_t s, uint64_t w) { return s *
 
 // FxHasher::write over bytes (8-byte little-endian chunks, last one padded),
 // then write_u8(0xff): Rust's `impl Hash for str` into FxHasher.
+// Bytes [0, len) of q as a little-endian word, zero above len (1 <= len <= 8).
+// Reads only the aligned 8-byte words that hold at least one of those bytes
+// (so never a page without a byte of the string): one or two loads instead of
+// len byte loads.
+__device__ __forceinline__ uint64_t str_word(const uint8_t* q, int32_t len) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(q) & 7;
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(q - a);
+  uint64_t x = w[0] >> (8 * a);
+  if ((int32_t)(8 - a) < len) x |= w[1] << (64 - 8 * a);
+  return len >= 8 ? x : (x & ((1ULL << (8 * len)) - 1));
+}
+
 __device__ __forceinline__ uint64_t fx_str(uint64_t s, const uint8_t* p, int32_t n) {
   int32_t i = 0;
-  for (; i + 8 <= n; i += 8) {
-    uint64_t w;
-    memcpy(&w, p + i, 8);
-    s = fx_word(s, w);
-  }
-  if (i < n) {
-    uint64_t w = 0;
-    for (int32_t k = 0; i + k < n; ++k) w |= (uint64_t)p[i + k] << (8 * k);
-    s = fx_word(s, w);
-  }
+  for (; i + 8 <= n; i += 8) s = fx_word(s, str_word(p + i, 8));
+  if (i < n) s = fx_word(s, str_word(p + i, n - i));
   return fx_word(s, 0xff);
 }
 

@@ -57,8 +57,10 @@ __device__ __forceinline__ uint64_t general_hash(const DCol* cols, int n, int64_
 
 __device__ __forceinline__ bool bytes_equal(const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb) {
   if (na != nb) return false;
-  for (int32_t i = 0; i < na; ++i)
-    if (a[i] != b[i]) return false;
+  for (int32_t i = 0; i < na; i += 8) {
+    int32_t len = na - i < 8 ? na - i : 8;
+    if (str_word(a + i, len) != str_word(b + i, len)) return false;
+  }
   return true;
 }
 
