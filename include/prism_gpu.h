@@ -263,6 +263,14 @@ int prism_batch_export(prism_ctx* ctx, const prism_batch* batch,
                        struct ArrowArray* out_array, struct ArrowSchema* out_schema);
 int64_t prism_batch_num_rows(const prism_batch* batch);
 int32_t prism_batch_num_columns(const prism_batch* batch);
+/* Device buffers of column `col` without a copy (the batch keeps them alive):
+ * values (fixed width; a Utf8 column's offsets), validity bitmap (NULL when
+ * the column has no nulls), element width in bytes and Arrow type id as in
+ * the engine (0 when unknown). Lets a caller hand result columns to its own
+ * device code (as ArrowDeviceArray export would). No counterpart in the
+ * reference, whose batches are host memory. */
+int prism_batch_column_device(const prism_batch* batch, int32_t col, const void** values, const uint8_t** validity,
+                              int32_t* width);
 void prism_batch_free(prism_batch* batch);
 
 /* ------------------------------------------------------------------------ */

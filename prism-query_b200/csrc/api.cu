@@ -361,6 +361,15 @@ int prism_batch_export(prism_ctx* c, const prism_batch* b, ArrowArray* a, ArrowS
 
 int64_t prism_batch_num_rows(const prism_batch* b) { return b ? b->impl.rows : -1; }
 int32_t prism_batch_num_columns(const prism_batch* b) { return b ? (int32_t)b->impl.cols.size() : -1; }
+int prism_batch_column_device(const prism_batch* b, int32_t col, const void** values, const uint8_t** validity,
+                              int32_t* width) {
+  if (!b || col < 0 || col >= (int32_t)b->impl.cols.size()) return PRISM_ERR_INVALID_ARGUMENT;
+  const Column& c = *b->impl.cols[col];
+  if (values) *values = c.type == TY_UTF8 ? static_cast<const void*>(c.offsets) : c.values;
+  if (validity) *validity = c.validity;
+  if (width) *width = width_of(c.type == TY_DICT ? c.index_type : c.type);
+  return PRISM_OK;
+}
 void prism_batch_free(prism_batch* b) {
   if (!b) return;
   if (b->ctx) {

@@ -74,6 +74,8 @@ def _declare(lib):
     lib.prism_ctx_set_profiling.argtypes = [P, I]
     lib.prism_ctx_kernel_stats.argtypes = [P, C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     lib.prism_jit_stats.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    lib.prism_batch_column_device.argtypes = [P, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                              C.POINTER(C.c_int32)]
     lib.prism_batch_import.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_import_device.argtypes = [P, P, P, C.POINTER(P)]
     lib.prism_batch_export.argtypes = [P, P, P, P]
@@ -273,6 +275,13 @@ class DeviceBatch:
     def num_columns(self) -> int:
         return int(lib().prism_batch_num_columns(self._h))
 
+    def column_device(self, col: int):
+        """(values pointer, validity pointer or 0, element width) of column
+        `col` in device memory, without a copy; valid while the batch lives."""
+        v, m, w = C.c_void_p(), C.c_void_p(), C.c_int32(0)
+        self.ctx.check(lib().prism_batch_column_device(self._h, col, C.byref(v), C.byref(m), C.byref(w)))
+        return int(v.value or 0), int(m.value or 0), int(w.value)
+
     def to_arrow(self) -> pa.RecordBatch:
         a, s = _abi.ArrowArray(), _abi.ArrowSchema()
         self.ctx.check(lib().prism_batch_export(self.ctx.handle, self._h, C.byref(a), C.byref(s)))
@@ -346,15 +355,20 @@ class HashTable:
             return out
         return out.column(0), out.column(1)
 
-    def join_project(self, probe_batch, probe_key_cols: Sequence[int], out_cols: Sequence[int], as_device=False):
-        db = _dev(probe_batch, self.ctx)
+    def join_project(self, probe_batch, probe_key_cols: Sequence[int], out_cols: Sequence[int], as_device=False,
+                     ctx: Optional[Context] = None):
+        """Probe and gather `out_cols` of the joined schema (PRISM_COL_* for
+        row indices). `ctx` (default: the table's) picks the context, hence
+        the stream, the probe runs on: a resident table serves any context of
+        its device."""
+        ctx = ctx or self.ctx
+        db = _dev(probe_batch, ctx)
         keys = _abi.int_array(probe_key_cols)
         oc = _abi.int_array(out_cols)
         h = C.c_void_p()
-        self.ctx.check(
-            lib().prism_join_project(self.ctx.handle, self._h, db.handle, keys, len(probe_key_cols), oc, len(out_cols), C.byref(h))
-        )
-        return _result(self.ctx, h, as_device)
+        ctx.check(lib().prism_join_project(ctx.handle, self._h, db.handle, keys, len(probe_key_cols), oc, len(out_cols),
+                                           C.byref(h)))
+        return _result(ctx, h, as_device)
 
     @property
     def has_duplicates(self) -> bool:

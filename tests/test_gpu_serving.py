@@ -1,0 +1,73 @@
+"""Serving loop: every request's result is the same served in the mix
+(coalesced with others, on several streams, under admission) as run alone."""
+import numpy as np
+import pytest
+
+from helpers import assert_batches_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(torch, prism_gpu, ctx):
+    from prism_gpu import AggExpr, AggFunc, HashAggConfig, HashTable
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    tables = {}
+    for name, n in (("t0", 200_000), ("t1", 1_300_000)):
+        keys = torch.randperm(n, generator=g, device=dev)
+        pay = torch.randint(-(2**62), 2**62, (n,), generator=g, device=dev)
+        db = prism_gpu.DeviceBatch.from_device_buffers([("k", "l", keys.data_ptr()), ("v", "l", pay.data_ptr())], n, ctx)
+        tables[name] = (HashTable.build(db, [0], ctx), n, keys, pay)
+    kpool = torch.randint(0, 1_600_000, (3_000_000,), generator=g, device=dev)
+    gkeys = torch.randint(-(2**40), 2**40, (64,), generator=g, device=dev)
+    akey = gkeys[torch.randint(0, 64, (3_000_000,), generator=g, device=dev)]
+    avi = torch.randint(-1000, 1000, (3_000_000,), generator=g, device=dev)
+    avf = torch.rand(3_000_000, generator=g, device=dev, dtype=torch.float64)
+    cfg = HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "s"), AggExpr(2, AggFunc.Avg, "a"), AggExpr(1, AggFunc.Count, "n"),
+                              AggExpr(2, AggFunc.Min, "mn")])
+    return tables, kpool, (akey, avi, avf), cfg
+
+
+def test_served_results_equal_alone(ctx):
+    import torch
+
+    import prism_gpu
+    from prism_gpu import serving as S
+
+    tables, kpool, (akey, avi, avf), cfg = _setup(torch, prism_gpu, ctx)
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(60):
+        rows = int(np.exp(rng.uniform(np.log(1000), np.log(600_000))))
+        off = int(rng.integers(0, 3_000_000 - rows))
+        if i % 2:
+            reqs.append(S.ProbeRequest("t0" if i % 4 == 1 else "t1", kpool[off:off + rows]))
+        else:
+            reqs.append(S.AggRequest([("k", "l", akey[off:off + rows]), ("vi", "l", avi[off:off + rows]),
+                                      ("vf", "g", avf[off:off + rows])], cfg))
+    torch.cuda.synchronize()
+    regs = {name: S._Table(t, 1) for name, (t, *_rest) in tables.items()}
+    alone, _ = S.run_plain(reqs, regs, ctx)
+    # alone: probe outputs in full, for an exact comparison
+    alone_rows = {}
+    for i, r in enumerate(reqs):
+        if isinstance(r, S.ProbeRequest):
+            db = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", r.keys.data_ptr())], int(r.keys.numel()), ctx)
+            out = regs[r.table].table.join_project(db, [0], [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 2])
+            alone_rows[i] = (out.column(0).to_numpy(), out.column(1).to_numpy())
+    srv = S.Server(0, budget_bytes=64 << 20, workers=3, coalesce_rows=1 << 17, max_coalesce=16)
+    for name, reg in regs.items():
+        srv.register_table(name, reg.table, 1)
+    futs = [srv.submit(r) for r in reqs]
+    got = [f.result(timeout=300) for f in futs]
+    srv.close()
+    for i, (r, a, b) in enumerate(zip(reqs, alone, got)):
+        if isinstance(r, S.ProbeRequest):
+            assert b.matches == a
+            pr, pay = alone_rows[i]
+            assert np.array_equal(b.probe_rows.cpu().numpy().astype(np.uint32), pr)
+            assert np.array_equal(b.payload.cpu().numpy(), pay)
+        else:
+            assert_batches_equal(b, a, float_cols=(1, 2, 4))

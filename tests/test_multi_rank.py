@@ -6,7 +6,6 @@ groups in the same first-seen order, integer results exact, Float64 within
 rank-ordered concatenation must equal the single-call join."""
 import json
 import os
-import socket
 import sys
 
 import numpy as np
@@ -46,7 +45,7 @@ def _join_data(seed=9):
     return build, probes
 
 
-def _rank_main(rank, world, port, outdir):
+def _rank_main(rank, world, store, outdir):
     for p in (os.path.join(ROOT, "prism-query_b200"), os.path.join(ROOT, "tests"), ROOT):
         sys.path.insert(0, p)
     import torch.distributed as dist
@@ -56,7 +55,7 @@ def _rank_main(rank, world, port, outdir):
     from prism_gpu import AggExpr, AggFunc, HashAggConfig, HashJoinConfig, JoinType, Predicate, ScalarValue
     from prism_gpu import distributed as D
 
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    dist.init_process_group("gloo", init_method=f"file://{store}", rank=rank, world_size=world)
     try:
         data = _data()
         mine = D.shard_batches(data, rank, world)
@@ -109,16 +108,9 @@ def _rank_main(rank, world, port, outdir):
         dist.destroy_process_group()
 
 
-def _free_port():
-    s = socket.socket()
-    s.bind(("127.0.0.1", 0))
-    port = s.getsockname()[1]
-    s.close()
-    return port
-
-
 def test_two_gloo_ranks_merge_partials_and_shard_joins(tmp_path):
-    mp.spawn(_rank_main, args=(WORLD, _free_port(), str(tmp_path)), nprocs=WORLD, join=True)
+    # a file store for the rendezvous: no port to race for
+    mp.spawn(_rank_main, args=(WORLD, str(tmp_path / "pg_store"), str(tmp_path)), nprocs=WORLD, join=True)
     for r in range(WORLD):
         assert json.load(open(tmp_path / f"rank{r}.json"))["ok"]
 
