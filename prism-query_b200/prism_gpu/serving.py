@@ -201,6 +201,8 @@ class Server:
                         results = self._run_probe(ctx, stream, job.reqs)
                     else:
                         results = self._run_agg(ctx, stream, job.reqs)
+                # results are read on other streams: finish this job's work first
+                stream.synchronize()
                 for f, r in zip(job.futs, results):
                     f.set_result(r)
             except BaseException as e:  # every request of the job fails alike
@@ -285,9 +287,19 @@ def _device_tensor(torch, batch, col: int, dtype, n: int, device: int):
     return torch.as_tensor(_CudaArray(ptr, n, typestr, batch), device=f"cuda:{device}")
 
 
-def run_plain(requests, tables: Dict[str, _Table], ctx, device: int = 0, t0: Optional[float] = None):
+def probe_digest(torch, res: ProbeResult):
+    """(matches, sum of probe rows, wrapping sum of payloads): a checksum of a
+    probe result that equals another's when the two hold the same rows."""
+    if res.matches == 0:
+        return (0, 0, 0)
+    return (res.matches, int(res.probe_rows.to(torch.int64).sum().item()), int(res.payload.sum().item()))
+
+
+def run_plain(requests, tables: Dict[str, _Table], ctx, device: int = 0, t0: Optional[float] = None,
+              digest=None):
     """The comparison path: one request at a time, in arrival order, each its
-    own launch on one context; returns (results, completion times)."""
+    own launch on one context; returns (results, completion times). A probe's
+    result is its match count, or digest(index, ProbeResult) when given."""
     from . import PRISM_COL_PROBE_ROW_INDEX, DeviceBatch, hash_aggregate
 
     t0 = time.perf_counter() if t0 is None else t0
@@ -301,7 +313,16 @@ def run_plain(requests, tables: Dict[str, _Table], ctx, device: int = 0, t0: Opt
             n = int(r.keys.numel())
             db = DeviceBatch.from_device_buffers([("key", "l", r.keys.data_ptr())], n, ctx, device)
             res = t.table.join_project(db, [0], [PRISM_COL_PROBE_ROW_INDEX, 1 + t.payload_col], as_device=True, ctx=ctx)
-            out.append(res.num_rows)
+            if digest is None:
+                out.append(res.num_rows)
+            else:
+                import torch
+
+                m = res.num_rows
+                pr = ProbeResult(m, _device_tensor(torch, res, 0, torch.int32, m, device),
+                                 _device_tensor(torch, res, 1, torch.int64, m, device))
+                out.append(digest(len(out), pr))
+                del pr
             res.free()
         else:
             n = int(r.columns[0][2].numel())
