@@ -416,8 +416,9 @@ class C1:
         return {"groups": got.num_rows, "full_size_check": "bit-exact vs the oracle (Float64 sums within 1e-12)"}
 
     def roofline(self, kstats):
-        n, ms = kstats.get("agg_kernel", (0, 0.0))
-        return {"kernel": "agg_kernel", "bytes": 24 * self.rows, "ms": ms / max(1, n),
+        name = "agg_hash_jit" if kstats.get("agg_hash_jit", (0, 0.0))[0] else "agg_kernel"
+        n, ms = kstats.get(name, (0, 0.0))
+        return {"kernel": name, "bytes": 24 * self.rows, "ms": ms / max(1, n),
                 "per_unit": "24 B per row (key + v_i + v_f)", "traffic_key": "agg_c1"}
 
     def e2e_inputs(self):
@@ -643,7 +644,8 @@ class C4:
                 "full_size_check": "COUNT total == probe rows drawn from build keys"}
 
     def roofline(self, kstats):
-        names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit")
+        names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit",
+                 "agg_hash_jit")
         ms = sum(kstats.get(k, (0, 0.0))[1] for k in names)
         steps = max(1, kstats.get("insert_kernel", (1, 0.0))[0])
         kb = int(self.bo32[-1].item()) + sum(int(k[0][-1].item()) for k in self.keep)
@@ -763,7 +765,7 @@ def run_workload(args, rank, world, local, torch, dist):
             dist.barrier()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
-    names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit",
+    names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
              "predicate_kernel", "expr_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
     ctx.set_profiling(False)

@@ -33,9 +33,6 @@ namespace prism {
 
 namespace {
 
-constexpr uint64_t GEMPTY = 0xFFFFFFFFFFFFFFFFULL;
-constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
-
 struct RowVals {
   double f[MAX_SRC];
   __int128 i[MAX_SRC];
@@ -80,7 +77,7 @@ __device__ __forceinline__ void apply_ops(const AggArgs& a, unsigned long long* 
         else
           add_f64(w, v.f[o.src], o.lo_exp, a.err, a.maxexp + j);
         break;
-      case O_SUM_INT: add_i128_limbs(w, v.i[o.src], 2); break;
+      case O_SUM_INT: add_i128_limbs(w, f64_cast_int((long long)v.i[o.src]), 2); break;
       case O_SUM_DEC: add_i128_limbs(w, v.i[o.src], 4); break;
       case O_MIN: {
         double d = v.f[o.src];
@@ -156,23 +153,6 @@ __device__ __forceinline__ int64_t dense_gid(const AggArgs& a, int64_t row) {
   return g;
 }
 
-// global open-addressing insert; returns the slot or -1 when full
-__device__ int64_t ginsert(const AggArgs& a, uint64_t h) {
-  if (h == GEMPTY) return (int64_t)a.gcap;  // side slot
-  uint64_t s = (h * FIB) >> a.gshift;
-  for (uint64_t step = 0; step <= a.gmask; ++step) {
-    unsigned long long cur = *(volatile unsigned long long*)&a.gkeys[s];
-    if (cur == h) return (int64_t)s;
-    if (cur == GEMPTY) {
-      unsigned long long prev = atomicCAS(&a.gkeys[s], GEMPTY, h);
-      if (prev == GEMPTY || prev == h) return (int64_t)s;
-    }
-    s = (s + 1) & a.gmask;
-  }
-  atomicOr(a.err, DERR_TABLE_FULL);
-  return -1;
-}
-
 __device__ int64_t gfind(const AggArgs& a, uint64_t h) {
   if (h == GEMPTY) return (int64_t)a.gcap;
   uint64_t s = (h * FIB) >> a.gshift;
@@ -183,15 +163,6 @@ __device__ int64_t gfind(const AggArgs& a, uint64_t h) {
     s = (s + 1) & a.gmask;
   }
   return -1;
-}
-
-__device__ __forceinline__ void merge_word(unsigned long long* dst, unsigned long long v, int kind) {
-  switch (kind) {
-    case W_ADD: atom_add(dst, v); break;
-    case W_MIN: atomicMin((long long*)dst, (long long)v); break;
-    case W_MAX: atomicMax((long long*)dst, (long long)v); break;
-    case W_OR: if (v) atomicOr(dst, v); break;
-  }
 }
 
 __global__ void fill_words_kernel(unsigned long long* acc, int64_t groups, int W, AggArgs a) {
@@ -921,6 +892,22 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   for (int j = 0; j < A.n_ops; ++j) any_f64 |= A.op[j].kind == O_SUM_F64;
   bool tiny = dense && G <= 8 && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 &&
               tiny_fits_registers(A) && (G + 1) * tiny_group_words(A) <= TINY_MAX_WORDS && jit_enabled();
+  // hashed groups: a generated kernel whose per-block table slots own their
+  // accumulator words (hash_body); the largest power-of-two table up to
+  // 2 x smem_groups slots that fits the block's shared memory
+  int hss_log2 = 0;
+  size_t hsmem = 0;
+  if (!dense && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 && tiny_fits_registers(A) && jit_enabled()) {
+    const size_t hbudget = (size_t)smem_optin - TINY_MAX_COLS * sizeof(DCol) - 1024;
+    for (int l = 12; l >= 8; --l) {
+      if ((1 << l) > 2 * std::max(128, tune.smem_groups)) continue;
+      if (((size_t)(2 + W) * 8 << l) <= hbudget) {
+        hss_log2 = l;
+        hsmem = (size_t)(2 + W) * 8 << l;
+        break;
+      }
+    }
+  }
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
   for (int attempt = 0; attempt < 40; ++attempt) {
@@ -1001,7 +988,23 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         std::string src = jit_tiny_agg_source(pg, b, a, (int)G, any_f64);
         if (!src.empty()) jk = jit_get(src, "prism_tiny_agg");
       }
-      if (jk) {
+      const void* hk = nullptr;
+      if (!jk && hss_log2 && !A.wide) {
+        a.n_cols = (int)pg.cols.size();
+        std::string src = jit_hash_agg_source(pg, b, a);
+        if (!src.empty()) hk = jit_get(src, "prism_hash_agg");
+      }
+      if (hk) {
+        a.ss_log2 = hss_log2;
+        PRISM_CUDA(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        int per_sm = 0;
+        PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, HASH_BLOCK, hsmem));
+        int hgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)HASH_BLOCK * TINY_R * 4),
+                                           (int64_t)ctx.sm_count * std::max(1, per_sm));
+        void* params[] = {&a};
+        KernelTimer kt(ctx, "agg_hash_jit");
+        PRISM_CUDA(cudaLaunchKernel(hk, dim3(hgrid), dim3(HASH_BLOCK), params, hsmem, ctx.stream));
+      } else if (jk) {
         a.n_cols = (int)pg.cols.size();
         const int words = (int)(G + 1) * tiny_group_words(A), tblock = tiny_block(words);
         size_t tsmem = (size_t)words * tblock * 8;

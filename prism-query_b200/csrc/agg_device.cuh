@@ -146,6 +146,49 @@ __device__ __forceinline__ void add_i128_limbs(unsigned long long* acc, __int128
 
 __device__ __forceinline__ int64_t ceil_div_dev(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// An integer SUM operand as the reference sums it: its Float64 cast
+// (hash_aggregate.rs:227-245 casts every input to Float64), as an exact
+// integer. The identity for |v| < 2^53; above, v rounded to nearest even
+// (2^63 - 1 rounds to 2^63, which only the 128-bit form holds).
+__device__ __forceinline__ bool f64_exact_int(long long v) { return v > -(1LL << 53) && v < (1LL << 53); }
+__device__ __forceinline__ __int128 f64_cast_int(long long v) {
+  if (f64_exact_int(v)) return v;
+  const double d = (double)v;
+  if (d >= 9223372036854775808.0) return (__int128)1 << 63;
+  return (__int128)(long long)d;
+}
+
+// ------------------------------------------------- global group table --
+constexpr uint64_t GEMPTY = 0xFFFFFFFFFFFFFFFFULL;  // empty slot (a key hashing to it takes the side slot)
+constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
+
+// global open-addressing insert; returns the slot or -1 when full
+__device__ inline int64_t ginsert(const AggArgs& a, uint64_t h) {
+  if (h == GEMPTY) return (int64_t)a.gcap;  // side slot
+  uint64_t s = (h * FIB) >> a.gshift;
+  for (uint64_t step = 0; step <= a.gmask; ++step) {
+    unsigned long long cur = *(volatile unsigned long long*)&a.gkeys[s];
+    if (cur == h) return (int64_t)s;
+    if (cur == GEMPTY) {
+      unsigned long long prev = atomicCAS(&a.gkeys[s], GEMPTY, h);
+      if (prev == GEMPTY || prev == h) return (int64_t)s;
+    }
+    s = (s + 1) & a.gmask;
+  }
+  atomicOr(a.err, DERR_TABLE_FULL);
+  return -1;
+}
+
+// folds a privatised accumulator word into the global one
+__device__ __forceinline__ void merge_word(unsigned long long* dst, unsigned long long v, int kind) {
+  switch (kind) {
+    case W_ADD: atom_add(dst, v); break;
+    case W_MIN: atomicMin((long long*)dst, (long long)v); break;
+    case W_MAX: atomicMax((long long*)dst, (long long)v); break;
+    case W_OR: if (v) atomicOr(dst, v); break;
+  }
+}
+
 // ------------------------------------------------ few dense groups (<= 8) --
 // The kernel body for GROUP BY with at most 8 dense groups (dictionary keys,
 // or none). Every thread owns a private column of accumulators in shared
@@ -213,12 +256,19 @@ __device__ __forceinline__ void tiny_accumulate(const AggArgs& a, unsigned long 
       const bool narrow = FAST && E::kI64[j];
       __int128 xi = use ? x.i : (__int128)0;
       long long x64 = narrow ? (use ? (long long)x.i : 0LL) : (long long)xi;
+      // integer column: the value's Float64 cast (exact below 2^53: the
+      // partial takes it; else the cast goes through the spill)
+      bool fits = narrow || (__int128)x64 == xi;
+      if (kind == O_SUM_INT && !f64_exact_int(x64)) {
+        xi = f64_cast_int(x64);
+        fits = false;
+      }
       long long p = (long long)w[0];
       long long s = (long long)((unsigned long long)p + (unsigned long long)x64);
-      if ((narrow || (__int128)x64 == xi) && !(((p ^ s) & (x64 ^ s)) < 0)) {
+      if (fits && !(((p ^ s) & (x64 ^ s)) < 0)) {
         w[0] = (unsigned long long)s;
       } else {  // exact spill of partial + value; the partial restarts at 0
-        if (g < G) add_i128_limbs(&spill[g][j][0], (__int128)p + (narrow ? (__int128)x64 : xi), kind == O_SUM_INT ? 2 : 4);
+        if (g < G) add_i128_limbs(&spill[g][j][0], (__int128)p + xi, kind == O_SUM_INT ? 2 : 4);
         w[0] = 0;
       }
     } else if (kind == O_SUM_F64) {
@@ -389,6 +439,180 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
       for (int t = 0; t < BLOCK; ++t) c += w[t];
       atom_add(gw, c);
     }
+  }
+}
+
+// ---------------------------------------------- hashed groups (generated) --
+// The kernel body for GROUP BY over hashed keys. Each block keeps a
+// shared-memory open-addressing table of group hashes (the reference's
+// FxHash identity, hash_aggregate.rs:483-504) whose slot s owns the
+// accumulator words sacc[s * kW ...] in the global word layout (word 0 the
+// row count, then each op's words at E::kWord[j]): a row finds or claims its
+// slot with one compare-and-swap and updates the words with shared-memory
+// atomics. A row whose key finds no slot within HASH_PROBES steps (or
+// hashes to the empty marker) goes to the global table directly. At the end
+// the block resolves each used slot's global slot once and folds its words
+// in, one thread per (slot, word), so a warp's global atomics hit
+// consecutive words. Rows are read TINY_R deep per thread (all loads of a
+// step in flight before any is used), as in tiny_body.
+//
+// E supplies, besides the members tiny_body uses (keep, values, slow, Row,
+// fetch, kKind, kI64, kSkipNulls), E::hash (the key columns' FxHash), kW
+// (words per group, a.W), kWord (op j's first word, a.op[j].word) and
+// kCountRows; initial values and merge kinds of the words are a.winit and
+// a.wkind.
+constexpr int HASH_PROBES = 32;
+constexpr int HASH_BLOCK = 512;
+
+template <class E, int NOPS, bool FAST>
+__device__ __forceinline__ void hash_accumulate(const AggArgs& a, unsigned long long* acc, const Val* v) {
+  if (E::kCountRows) atomicAdd(acc, 1ULL);
+#pragma unroll
+  for (int j = 0; j < NOPS; ++j) {
+    const int kind = E::kKind[j];
+    const Val& x = v[j];
+    if (E::kSkipNulls && !x.valid) continue;
+    unsigned long long* w = acc + E::kWord[j];
+    if (kind == O_SUM_F64) {
+      add_f64(w, x.f, a.op[j].lo_exp, a.err, a.maxexp + j);
+    } else if (kind == O_SUM_INT) {
+      const long long q = (long long)x.i;
+      if (f64_exact_int(q)) {  // two 32-bit limbs of an int64 value, the top one signed
+        atom_add(w, (unsigned long long)(uint32_t)q);
+        atom_add(w + 1, (unsigned long long)(q >> 32));
+      } else {
+        add_i128_limbs(w, f64_cast_int(q), 2);
+      }
+    } else if (kind == O_SUM_DEC) {
+      add_i128_limbs(w, x.i, 4);
+    } else if (kind == O_MIN || kind == O_MAX) {
+      if (!isnan(x.f)) {
+        const long long k = (long long)total_key(x.f);
+        const long long cur = (long long)*(volatile unsigned long long*)w;
+        if (kind == O_MIN ? k < cur : k > cur) {  // most rows do not move the extreme: no atomic
+          if (kind == O_MIN) atomicMin((long long*)w, k);
+          else atomicMax((long long*)w, k);
+        }
+      }
+    } else if (kind == O_NONNULL) {
+      if (x.valid) atomicAdd(w, 1ULL);
+    }
+  }
+}
+
+template <class E, int NOPS, int BLOCK>
+__device__ __forceinline__ void hash_body(const AggArgs& a) {
+  constexpr int W = E::kW;
+  extern __shared__ unsigned long long hsm[];  // skeys[SS] | sfirst[SS] | sacc[SS][W]
+  __shared__ DCol scols[TINY_MAX_COLS];
+  const int tid = threadIdx.x;
+  const int SS = 1 << a.ss_log2;
+  const uint32_t smask = (uint32_t)SS - 1;
+  const int sshift = 64 - a.ss_log2;
+  unsigned long long* skeys = hsm;
+  unsigned long long* sfirst = hsm + SS;
+  unsigned long long* sacc = hsm + 2 * SS;
+  const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
+  if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
+  for (int i = tid; i < SS; i += BLOCK) {
+    skeys[i] = GEMPTY;
+    sfirst[i] = ~0ULL;
+  }
+  for (int i = tid; i < SS * W; i += BLOCK) sacc[i] = a.winit[i % W];
+  __syncthreads();
+  const DCol* cols = shared_cols ? scols : a.cols;
+  const typename E::Consts K = E::load(a);
+  using I = typename E::idx_t;
+  const I stride = (I)gridDim.x * BLOCK;
+  const I n = (I)a.n, last = n - 1;
+  bool err = false;
+  for (I base = (I)blockIdx.x * BLOCK + tid; base < n; base += stride * TINY_R) {
+    typename E::Row rows[TINY_R];
+    bool keep[TINY_R];
+    uint64_t hs[TINY_R];
+    unsigned flags[TINY_R];
+    Val v[TINY_R][NOPS];
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+      I at = base + r * stride;
+      rows[r] = E::fetch(cols, at < last ? at : last);  // rows past the end read the last row and are dropped
+    }
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+      I at = base + r * stride;
+      I idx = at < last ? at : last;
+      keep[r] = at <= last && E::keep(a, K, cols, idx, rows[r]);
+      hs[r] = E::hash(a, K, cols, idx, rows[r]);
+      flags[r] = 0;
+      E::values(a, K, cols, idx, rows[r], v[r], flags[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < TINY_R; ++r) {
+      if (!keep[r]) continue;
+      const I at = base + r * stride;
+      const uint64_t h = hs[r];
+      // find or claim the key's slot
+      int s = -1;
+      if (h != GEMPTY) {
+        uint32_t p = (uint32_t)((h * FIB) >> sshift);
+        for (int step = 0; step < HASH_PROBES; ++step) {
+          unsigned long long cur = *(volatile unsigned long long*)&skeys[p];
+          if (cur == GEMPTY) {
+            cur = atomicCAS(&skeys[p], GEMPTY, h);
+            if (cur == GEMPTY) cur = h;
+          }
+          if (cur == h) {
+            s = (int)p;
+            break;
+          }
+          p = (p + 1) & smask;
+        }
+      }
+      const uint64_t grow = a.row_base + (uint64_t)at;
+      unsigned long long* acc;
+      if (s >= 0) {
+        if (grow < sfirst[s]) atomicMin(&sfirst[s], grow);
+        acc = sacc + (size_t)s * W;
+      } else {
+        const int64_t gs = ginsert(a, h);
+        if (gs < 0) continue;
+        if (grow < a.gfirst[gs]) atomicMin(&a.gfirst[gs], grow);
+        acc = a.gacc + (size_t)gs * W;
+      }
+      if (flags[r]) {
+        // every op of the row recomputed exactly
+        Val w[NOPS];
+#pragma unroll
+        for (int j = 0; j < NOPS; ++j) {
+          SlowVal sv = E::slow(a, j, cols, at);
+          w[j] = sv.v;
+          err |= sv.ovf;
+        }
+        hash_accumulate<E, NOPS, false>(a, acc, w);
+      } else {
+        hash_accumulate<E, NOPS, true>(a, acc, v[r]);
+      }
+    }
+  }
+  if (err) atomicOr(a.err, DERR_RANGE);
+  __syncthreads();
+  // each used slot's global slot, kept in skeys (-1: none)
+  for (int i = tid; i < SS; i += BLOCK) {
+    const unsigned long long k = skeys[i];
+    long long gs = -1;
+    if (k != GEMPTY) {
+      gs = ginsert(a, k);
+      if (gs >= 0) atomicMin(&a.gfirst[gs], sfirst[i]);
+    }
+    skeys[i] = (unsigned long long)gs;
+  }
+  __syncthreads();
+  for (int q = tid; q < SS * W; q += BLOCK) {
+    const int i = q / W, w = q - i * W;
+    const long long gs = (long long)skeys[i];
+    if (gs < 0) continue;
+    const unsigned long long x = sacc[q];
+    if (x != a.winit[w]) merge_word(a.gacc + (size_t)gs * W + w, x, a.wkind[w]);
   }
 }
 

@@ -688,9 +688,17 @@ const void* jit_get(const std::string& source, const char* name) {
   return reinterpret_cast<const void*>(kt->second);
 }
 
-std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64) {
-  Gen gen(pg, b);
-  // filter
+namespace {
+
+// The per-row logic every generated aggregation kernel shares: filter
+// (keep), operands (values, value, slow) and the op kind / fast-path tables.
+struct RowParts {
+  std::string keep, value, values_body, slow, slow_cols, kinds, i64;
+  bool ok = true;
+};
+
+RowParts row_parts(Gen& gen, const AggArgs& a) {
+  RowParts rp;
   gen.declare_cols();
   if (a.has_filter) {
     auto p = gen.pred(a.filter.begin, a.filter.len);
@@ -698,30 +706,19 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   } else {
     gen.out << "    return true;\n";
   }
-  std::string keep = gen.take();
-  // dense group id
-  gen.declare_cols();
-  gen.out << "    int g = 0;\n";
-  for (int k = 0; k < a.n_gcols; ++k) {
-    std::string c = gen.col(a.gcol[k]);
-    // the dense id layout (dictionary sizes) is fixed per plan: constants
-    gen.out << "    { int code = " << gen.V(a.gcol[k]) << " ? (int)" << gen.rd("dcol_ival", a.gcol[k]) << " : "
-            << a.dnull[k] << "; g += code * " << a.dstride[k] << "; }\n";
-  }
-  gen.out << "    return g;\n";
-  std::string gid = gen.take();
+  rp.keep = gen.take();
   // operands
   gen.declare_cols();
   gen.out << "    Val r; r.i = 0; r.f = 0; r.valid = true;\n";
-  std::ostringstream kinds, words, slow, i64;
-  int nw = TINY_FIRST_OP_WORD;  // words 0, 1 of a group: row count, first row
+  std::ostringstream kinds, slow, i64;
   for (int j = 0; j < a.n_ops; ++j) {
     const Op& o = a.op[j];
-    if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) return "";
+    if (o.kind == O_DISTINCT || o.src < 0 || o.src >= a.n_src) {
+      rp.ok = false;
+      return rp;
+    }
     kinds << (j ? ", " : "") << o.kind;
     bool narrow = false;  // value fits int64 whenever the row's slow flag is clear
-    words << (j ? ", " : "") << nw;
-    nw += tiny_words(o.kind);
     const Src& sr = a.src[o.src];
     gen.out << "    " << (j ? "else " : "") << "if (j == " << j << ") {\n";
     switch (sr.kind) {
@@ -774,7 +771,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     i64 << (j ? ", " : "") << (narrow ? "true" : "false");
   }
   gen.out << "    return r;\n";
-  std::string value = gen.take();
+  rp.value = gen.take();
   // values(): every op of a row in one straight-line body (the hot path);
   // subtrees shared between ops' 64-bit programs are computed once
   gen.declare_cols();
@@ -817,12 +814,19 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     }
   }
   gen.cse = false;
-  std::string values_body = gen.take();
+  rp.values_body = gen.take();
   gen.declare_cols();
-  std::string slow_cols = gen.take();
-  const int block = tiny_block((g + 1) * nw);
-  if (!gen.ok) return "";
+  rp.slow_cols = gen.take();
+  rp.slow = slow.str();
+  rp.kinds = kinds.str();
+  rp.i64 = i64.str();
+  rp.ok = gen.ok;
+  return rp;
+}
 
+// struct QueryRow: E of the kernel bodies in agg_device.cuh. `members`
+// adds the body-specific functions and layout constants.
+std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts& rp, const std::string& members) {
   std::string consts = gen.consts.str();
   if (consts.empty()) consts = "    int unused;\n";
   std::ostringstream s;
@@ -841,40 +845,108 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
     << "    return K;\n  }\n"
        "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
        "const Row& row) {\n"
-    << keep
-    << "  }\n"
-       "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
-       "const Row& row) {\n"
-    << gid
-    << "  }\n"
-       "  static constexpr bool kSkipNulls = "
-    << (a.skip_nulls ? "true" : "false")
-    << ";\n"
-       "  static constexpr int kNW = "
-    << nw << ";\n  static constexpr int kKind[" << a.n_ops << "] = {" << kinds.str() << "};\n  static constexpr int kWord["
-    << a.n_ops << "] = {" << words.str() << "};\n  static constexpr bool kI64[" << a.n_ops << "] = {" << i64.str()
-    << "};\n"
+    << rp.keep << "  }\n"
+    << members
+    << "  static constexpr bool kSkipNulls = " << (a.skip_nulls ? "true" : "false") << ";\n"
+    << "  static constexpr int kKind[" << a.n_ops << "] = {" << rp.kinds << "};\n"
+    << "  static constexpr bool kI64[" << a.n_ops << "] = {" << rp.i64 << "};\n"
     << "  // every op's exact value, out of line: 128-bit programs for ops with a\n"
        "  // 64-bit fast path, value() itself for the others\n"
        "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
        "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
-    << slow_cols << slow.str()
+    << rp.slow_cols << rp.slow
     << "    unsigned fl = 0;\n    SlowVal s;\n    s.v = value(a, K, j, cols, idx, row, fl);\n"
        "    s.ovf = ((fl >> (2 * j + 1)) & 1u) != 0;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ void values(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
        "const Row& row, Val* out, unsigned& flags) {\n"
-    << values_body << "  }\n"
+    << rp.values_body << "  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
        "idx_t idx, const Row& row, unsigned& flags) {\n"
-    << value
+    << rp.value
     << "  }\n"
        "};\n"
-       "}  // namespace prism\n"
-       "extern \"C\" __global__ void __launch_bounds__("
-    << block << ", " << 512 / block << ") prism_tiny_agg(prism::AggArgs a) {\n"
+       "}  // namespace prism\n";
+  return s.str();
+}
+
+}  // namespace
+
+std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64) {
+  Gen gen(pg, b);
+  RowParts rp = row_parts(gen, a);
+  if (!rp.ok) return "";
+  // dense group id
+  gen.declare_cols();
+  gen.out << "    int g = 0;\n";
+  for (int k = 0; k < a.n_gcols; ++k) {
+    std::string c = gen.col(a.gcol[k]);
+    // the dense id layout (dictionary sizes) is fixed per plan: constants
+    gen.out << "    { int code = " << gen.V(a.gcol[k]) << " ? (int)" << gen.rd("dcol_ival", a.gcol[k]) << " : "
+            << a.dnull[k] << "; g += code * " << a.dstride[k] << "; }\n";
+  }
+  gen.out << "    return g;\n";
+  std::string gid = gen.take();
+  // tiny layout: words 0, 1 of a group are the row count and first row
+  std::ostringstream words;
+  int nw = TINY_FIRST_OP_WORD;
+  for (int j = 0; j < a.n_ops; ++j) {
+    words << (j ? ", " : "") << nw;
+    nw += tiny_words(a.op[j].kind);
+  }
+  const int block = tiny_block((g + 1) * nw);
+  if (!gen.ok) return "";
+  std::ostringstream m;
+  m << "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
+       "const Row& row) {\n"
+    << gid << "  }\n"
+    << "  static constexpr int kNW = " << nw << ";\n"
+    << "  static constexpr int kWord[" << a.n_ops << "] = {" << words.str() << "};\n";
+  std::ostringstream s;
+  s << query_row(gen, b, a, rp, m.str())
+    << "extern \"C\" __global__ void __launch_bounds__(" << block << ", " << 512 / block << ") prism_tiny_agg(prism::AggArgs a) {\n"
        "  prism::tiny_body<prism::QueryRow, "
-    << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false") << ", " << block
-    << ">(a);\n"
+    << g << ", " << a.n_ops << ", " << (f64 ? "true" : "false") << ", " << block << ">(a);\n"
+       "}\n";
+  return s.str();
+}
+
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a) {
+  Gen gen(pg, b);
+  RowParts rp = row_parts(gen, a);
+  if (!rp.ok) return "";
+  // FxHash of the key columns, as fx_value computes it (common.cuh): fixed
+  // width integer and Float64 keys from the fetched row words, any other
+  // type by fx_value itself on the column
+  gen.declare_cols();
+  gen.out << "    uint64_t h = 0;\n";
+  for (int k = 0; k < a.n_gcols; ++k) {
+    const int slot = a.gcol[k];
+    std::string c = gen.col(slot);
+    const int t = gen.col_type(slot);
+    if (gen.fetched(slot) && (t == TY_I32 || t == TY_I64))
+      gen.out << "    h = " << gen.V(slot) << " ? fx_word(h, (uint64_t)dcol_ival(" << c << ", 0)) : fx_word(h, 0);\n";
+    else if (gen.fetched(slot) && t == TY_F64)
+      gen.out << "    h = " << gen.V(slot) << " ? fx_word(h, (uint64_t)__double_as_longlong(static_cast<const double*>(" << c
+              << ".values)[0])) : fx_word(h, 0);\n";
+    else
+      gen.out << "    h = fx_value(h, cols[" << slot << "], idx);\n";
+  }
+  gen.out << "    return h;\n";
+  std::string hash = gen.take();
+  std::ostringstream words;
+  for (int j = 0; j < a.n_ops; ++j) words << (j ? ", " : "") << a.op[j].word;
+  if (!gen.ok) return "";
+  std::ostringstream m;
+  m << "  static __device__ __forceinline__ uint64_t hash(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
+       "const Row& row) {\n"
+    << hash << "  }\n"
+    << "  static constexpr int kW = " << a.W << ";\n"
+    << "  static constexpr bool kCountRows = " << (a.count_rows ? "true" : "false") << ";\n"
+    << "  static constexpr int kWord[" << a.n_ops << "] = {" << words.str() << "};\n";
+  std::ostringstream s;
+  s << query_row(gen, b, a, rp, m.str())
+    << "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
+       "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", prism::HASH_BLOCK>(a);\n"
        "}\n";
   return s.str();
 }

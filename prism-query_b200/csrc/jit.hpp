@@ -39,4 +39,9 @@ void jit_stats(int64_t* compiles, double* ms);
 // construct the generator does not cover.
 std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64);
 
+// Source of the hashed-groups aggregation kernel `prism_hash_agg` (block
+// size HASH_BLOCK, dynamic shared memory (2 + a.W) * 8 << a.ss_log2 bytes).
+// Empty when the program uses a construct the generator does not cover.
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a);
+
 }  // namespace prism
