@@ -165,6 +165,22 @@ __device__ int64_t gfind(const AggArgs& a, uint64_t h) {
   return -1;
 }
 
+// Every word of a fresh group table: keys empty, first rows unset,
+// accumulators at their initial values, counters zero.
+__global__ void init_table_kernel(AggArgs a, int64_t nslots) {
+  const int64_t words = nslots * a.W;
+  const int64_t n = words > nslots ? words : nslots;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < nslots) {
+      if (a.gkeys) a.gkeys[i] = GEMPTY;
+      a.gfirst[i] = ~0ULL;
+    }
+    if (i < words) a.gacc[i] = a.winit[i % a.W];
+    if (i < MAX_OPS) a.maxexp[i] = 0;
+    if (i == 0 && a.gnew_count) *a.gnew_count = 0;
+  }
+}
+
 __global__ void fill_words_kernel(unsigned long long* acc, int64_t groups, int W, AggArgs a) {
   int64_t n = groups * W;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -313,11 +329,73 @@ __global__ void place_groups_kernel(const unsigned long long* gfirst, const uint
   }
 }
 
-// exact big integer (6 signed 64-bit limb counters, weight 2^(32k + lo_exp))
-// -> correctly rounded double
+// Up to SMALL_GROUPS groups are put in first-seen order by one block: the
+// groups' (first row, slot) pairs sorted in shared memory (bitonic). The
+// candidates are the slots ginsert listed (plus the side slot when used),
+// or, for dense ids, every slot with a row. out[0] = the group count, or
+// ~0 when there are more groups than the block sorts (the general path
+// then orders them).
+constexpr int SMALL_GROUPS = 4096;
+__global__ void __launch_bounds__(1024) small_order_kernel(const unsigned long long* gfirst, const uint32_t* gnew,
+                                                           const unsigned long long* gnew_count, int64_t scan_n,
+                                                           int64_t side, uint32_t* ordered, uint32_t* rows32,
+                                                           unsigned long long* out) {
+  __shared__ unsigned long long key[SMALL_GROUPS];
+  __shared__ unsigned int cnt;
+  const int tid = threadIdx.x;
+  if (gnew) {
+    const unsigned long long listed = *gnew_count;
+    if (listed > (unsigned long long)(SMALL_GROUPS - 1)) {  // one entry left for the side slot
+      if (tid == 0) *out = ~0ULL;
+      return;
+    }
+    for (int i = tid; i < (int)listed; i += blockDim.x) {
+      const uint32_t s = gnew[i];
+      key[i] = (gfirst[s] << 32) | s;
+    }
+    if (tid == 0) {
+      cnt = (unsigned int)listed;
+      if (side >= 0 && gfirst[side] != ~0ULL) key[cnt++] = (gfirst[side] << 32) | (uint64_t)side;
+    }
+  } else {
+    if (tid == 0) cnt = 0;
+    __syncthreads();
+    for (int64_t s = tid; s < scan_n; s += blockDim.x)
+      if (gfirst[s] != ~0ULL) key[atomicAdd(&cnt, 1u)] = (gfirst[s] << 32) | (uint64_t)s;
+  }
+  __syncthreads();
+  const int n = (int)cnt;
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int i = n + tid; i < m; i += blockDim.x) key[i] = ~0ULL;
+  __syncthreads();
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < m; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long x = key[i], y = key[ixj];
+          if ((x > y) == ((i & k) == 0)) {
+            key[i] = y;
+            key[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = tid; i < n; i += blockDim.x) {
+    ordered[i] = (uint32_t)key[i];
+    rows32[i] = (uint32_t)(key[i] >> 32);
+  }
+  if (tid == 0) *out = (unsigned long long)n;
+}
+
+// exact big integer (signed 64-bit counters of 32-bit limbs, weight
+// 2^(32k + lo_exp)) -> correctly rounded double; MAXL bounds n_limbs
+template <int MAXL>
 __device__ double limbs_to_double(const unsigned long long* acc, int n_limbs, int lo_exp) {
   // normalise to 32-bit digits with a signed top
-  uint32_t dig[WIDE_LIMBS + 4];
+  uint32_t dig[MAXL + 3];
   long long carry = 0;
   int nd = n_limbs + 3;
   for (int k = 0; k < nd; ++k) {
@@ -421,14 +499,15 @@ __global__ void finalize_kernel(FinalArgs f) {
             if (fl & 1 || ((fl & 2) && (fl & 4))) r = __longlong_as_double(0x7ff8000000000000LL);
             else if (fl & 2) r = __longlong_as_double(0x7ff0000000000000LL);
             else if (fl & 4) r = __longlong_as_double((long long)0xfff0000000000000ULL);
-            else r = limbs_to_double(w, nl, lo);
+            else if (f.wide) r = limbs_to_double<WIDE_LIMBS>(w, nl, lo);
+            else r = limbs_to_double<LIMBS>(w, nl, lo);
           } else if (op.kind == O_SUM_INT) {
-            r = limbs_to_double(w, 2, 0);
+            r = limbs_to_double<2>(w, 2, 0);
           } else {  // O_SUM_DEC
             rd = limbs_to_i128(w, 4);
             double sc = 1.0;
             for (int q = 0; q < o.dec_scale; ++q) sc *= 10.0;
-            r = limbs_to_double(w, 4, 0) / sc;
+            r = limbs_to_double<4>(w, 4, 0) / sc;
           }
           if (o.func == PRISM_AGG_AVG) r = cnt > 0 ? r / (double)cnt : 0.0;
           break;
@@ -925,16 +1004,13 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       A.gwide = ctx.alloc_t<unsigned long long>(nslots * A.n_wide * (WIDE_LIMBS + 1), mwide);
       PRISM_CUDA(cudaMemsetAsync(A.gwide, 0, nslots * A.n_wide * (WIDE_LIMBS + 1) * 8, ctx.stream));
     }
-    PRISM_CUDA(cudaMemsetAsync(A.maxexp, 0, MAX_OPS * sizeof(int), ctx.stream));
-    int gfill = grid_for(ctx, (int64_t)(nslots * W), 256);
-    if (!dense) {
-      fill_u64_kernel<<<grid_for(ctx, (int64_t)nslots, 256), 256, 0, ctx.stream>>>(A.gkeys, (int64_t)nslots, GEMPTY);
-      ctx.check_launch("fill_u64_kernel(keys)");
-    }
-    fill_u64_kernel<<<grid_for(ctx, (int64_t)nslots, 256), 256, 0, ctx.stream>>>(A.gfirst, (int64_t)nslots, ~0ULL);
-    ctx.check_launch("fill_u64_kernel(first)");
-    fill_words_kernel<<<gfill, 256, 0, ctx.stream>>>(A.gacc, (int64_t)nslots, W, A);
-    ctx.check_launch("fill_words_kernel");
+    // hashed groups: ginsert lists the slots it creates (the small-groups
+    // ordering reads that list instead of scanning the table)
+    MemP mnew, mnewc, msmall;
+    A.gnew = dense ? nullptr : ctx.alloc_t<uint32_t>(nslots, mnew);
+    A.gnew_count = dense ? nullptr : ctx.alloc_t<unsigned long long>(1, mnewc);
+    init_table_kernel<<<grid_for(ctx, (int64_t)(nslots * std::max(W, 1)), 256), 256, 0, ctx.stream>>>(A, (int64_t)nslots);
+    ctx.check_launch("init_table_kernel");
     std::vector<MemP> dmem;
     for (int t = 0; t < P.n_distinct; ++t) {
       if (!dist_log2) dist_log2 = std::max(10, 64 - __builtin_clzll((uint64_t)std::max<int64_t>(total_rows, 1) * 2));
@@ -1026,6 +1102,23 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       ctx.check_launch("agg_kernel");
       row_base += (uint64_t)b.rows;
     }
+    // few groups: ordered by one block now, the count read back together
+    // with the error word (one synchronisation)
+    const bool small_try = total_rows < (int64_t)UINT32_MAX && (!dense || (int64_t)nslots <= SMALL_GROUPS);
+    uint32_t* s_ordered = nullptr;
+    uint32_t* s_rows = nullptr;
+    unsigned long long* s_out = nullptr;
+    MemP mso, msr;
+    if (small_try) {
+      s_ordered = ctx.alloc_t<uint32_t>(SMALL_GROUPS, mso);
+      s_rows = ctx.alloc_t<uint32_t>(SMALL_GROUPS, msr);
+      s_out = ctx.alloc_t<unsigned long long>(1, msmall);
+      small_order_kernel<<<1, 1024, 0, ctx.stream>>>(A.gfirst, A.gnew, A.gnew_count, dense ? (int64_t)nslots : 0,
+                                                     dense ? -1 : (int64_t)gcap, s_ordered, s_rows, s_out);
+      ctx.check_launch("small_order_kernel");
+    }
+    unsigned long long small_n = ~0ULL;
+    if (small_try) PRISM_CUDA(cudaMemcpyAsync(&small_n, s_out, 8, cudaMemcpyDeviceToHost, ctx.stream));
     uint32_t derr = ctx.take_device_errors();
     if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "aggregation wait timed out");
     if (derr & DERR_TABLE_FULL) {
@@ -1059,46 +1152,57 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         ctx.check_launch("distinct_count_kernel");
       }
     }
-    MemP mslots, mcnt;
-    uint32_t* slots = ctx.alloc_t<uint32_t>(nslots, mslots);
-    unsigned long long* counter = ctx.alloc_t<unsigned long long>(1, mcnt);
-    PRISM_CUDA(cudaMemsetAsync(counter, 0, 8, ctx.stream));
-    collect_groups_kernel<<<grid_for(ctx, (int64_t)nslots, 256), 256, 0, ctx.stream>>>(A.gfirst, (int64_t)nslots, slots, counter);
-    ctx.check_launch("collect_groups_kernel");
-    unsigned long long ng = 0;
-    PRISM_CUDA(cudaMemcpyAsync(&ng, counter, 8, cudaMemcpyDeviceToHost, ctx.stream));
-    PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
-    int64_t G_out = (int64_t)ng;
-    // first-seen order: rank of each group's first row among all first rows
-    int64_t nw = ceil_div(total_rows, 32);
-    MemP mbits, mwc, mwo, mord, mof;
-    uint32_t* bits = ctx.alloc_t<uint32_t>((size_t)nw, mbits);
-    uint32_t* wc = ctx.alloc_t<uint32_t>((size_t)nw, mwc);
-    uint64_t* wo = ctx.alloc_t<uint64_t>((size_t)nw, mwo);
-    uint32_t* ordered = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mord);
-    unsigned long long* ofirst = ctx.alloc_t<unsigned long long>((size_t)std::max<int64_t>(G_out, 1), mof);
-    PRISM_CUDA(cudaMemsetAsync(bits, 0, nw * 4, ctx.stream));
-    if (G_out) {
-      mark_first_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(A.gfirst, slots, G_out, bits);
-      ctx.check_launch("mark_first_kernel");
-      word_popc32_kernel<<<grid_for(ctx, nw, 256), 256, 0, ctx.stream>>>(bits, nw, wc);
-      ctx.check_launch("word_popc32_kernel");
-      scan_u32(ctx, wc, wo, nw);
-      place_groups_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(A.gfirst, slots, G_out, bits, wo, ordered, ofirst);
-      ctx.check_launch("place_groups_kernel");
+    int64_t G_out = 0;
+    uint32_t* ordered = nullptr;
+    uint32_t* rows32 = nullptr;  // first row of each output group (u32)
+    MemP mslots, mcnt, mbits, mwc, mwo, mord, mof, mrow;
+    if (small_try && small_n != ~0ULL) {
+      G_out = (int64_t)small_n;
+      ordered = s_ordered;
+      rows32 = s_rows;
+    } else {
+      uint32_t* slots = ctx.alloc_t<uint32_t>(nslots, mslots);
+      unsigned long long* counter = ctx.alloc_t<unsigned long long>(1, mcnt);
+      PRISM_CUDA(cudaMemsetAsync(counter, 0, 8, ctx.stream));
+      collect_groups_kernel<<<grid_for(ctx, (int64_t)nslots, 256), 256, 0, ctx.stream>>>(A.gfirst, (int64_t)nslots, slots,
+                                                                                        counter);
+      ctx.check_launch("collect_groups_kernel");
+      unsigned long long ng = 0;
+      PRISM_CUDA(cudaMemcpyAsync(&ng, counter, 8, cudaMemcpyDeviceToHost, ctx.stream));
+      PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+      G_out = (int64_t)ng;
+      // first-seen order: rank of each group's first row among all first rows
+      int64_t nw = ceil_div(total_rows, 32);
+      uint32_t* bits = ctx.alloc_t<uint32_t>((size_t)nw, mbits);
+      uint32_t* wc = ctx.alloc_t<uint32_t>((size_t)nw, mwc);
+      uint64_t* wo = ctx.alloc_t<uint64_t>((size_t)nw, mwo);
+      ordered = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mord);
+      unsigned long long* ofirst = ctx.alloc_t<unsigned long long>((size_t)std::max<int64_t>(G_out, 1), mof);
+      PRISM_CUDA(cudaMemsetAsync(bits, 0, nw * 4, ctx.stream));
+      if (G_out) {
+        mark_first_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(A.gfirst, slots, G_out, bits);
+        ctx.check_launch("mark_first_kernel");
+        word_popc32_kernel<<<grid_for(ctx, nw, 256), 256, 0, ctx.stream>>>(bits, nw, wc);
+        ctx.check_launch("word_popc32_kernel");
+        scan_u32(ctx, wc, wo, nw);
+        place_groups_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(A.gfirst, slots, G_out, bits, wo, ordered,
+                                                                              ofirst);
+        ctx.check_launch("place_groups_kernel");
+      }
+      if (cfg.n_group_by) {
+        if (total_rows >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "aggregation input exceeds 2^32-1 rows");
+        // narrow the first rows to u32 indices
+        rows32 = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mrow);
+        if (G_out) {
+          narrow_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(ofirst, G_out, rows32);
+          ctx.check_launch("narrow_kernel");
+        }
+      }
     }
     Batch out;
     out.rows = G_out;
     // key columns: gather first rows (keys of multi-batch inputs are concatenated first)
     if (cfg.n_group_by) {
-      MemP mrow;
-      uint32_t* rows32 = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mrow);
-      if (total_rows >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "aggregation input exceeds 2^32-1 rows");
-      // narrow the first rows to u32 indices
-      if (G_out) {
-        narrow_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(ofirst, G_out, rows32);
-        ctx.check_launch("narrow_kernel");
-      }
       for (int k = 0; k < cfg.n_group_by; ++k) {
         int bc = gbatch_cols[k];
         std::vector<const Column*> parts;

@@ -77,6 +77,8 @@ struct AggArgs {
   unsigned long long* gkeys;
   unsigned long long* gfirst;
   unsigned long long* gacc;
+  uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
+  unsigned long long* gnew_count;  // length of gnew
   uint64_t gmask;
   int32_t gshift;
   uint64_t gcap;
@@ -171,7 +173,11 @@ __device__ inline int64_t ginsert(const AggArgs& a, uint64_t h) {
     if (cur == h) return (int64_t)s;
     if (cur == GEMPTY) {
       unsigned long long prev = atomicCAS(&a.gkeys[s], GEMPTY, h);
-      if (prev == GEMPTY || prev == h) return (int64_t)s;
+      if (prev == GEMPTY) {  // created: listed once, by its creator
+        if (a.gnew) a.gnew[atomicAdd(a.gnew_count, 1ULL)] = (uint32_t)s;
+        return (int64_t)s;
+      }
+      if (prev == h) return (int64_t)s;
     }
     s = (s + 1) & a.gmask;
   }
