@@ -412,25 +412,28 @@ __device__ double limbs_to_double(const unsigned long long* acc, int n_limbs, in
       c = t >> 32;
     }
   }
-  int top = -1;
+  int kt = -1;
   for (int k = nd - 1; k >= 0; --k)
-    if (dig[k]) { top = k * 32 + 31 - __clz(dig[k]); break; }
-  if (top < 0) return 0.0;
-  auto bit = [&](int p) -> unsigned long long { return p < 0 ? 0ULL : (dig[p >> 5] >> (p & 31)) & 1u; };
+    if (dig[k]) { kt = k; break; }
+  if (kt < 0) return 0.0;
+  const int sh = __clz(dig[kt]);
+  const int top = kt * 32 + 31 - sh;  // highest set bit
+  // bits [top - 63, top] as m64 (top at bit 63), and whether any bit below is set
+  unsigned __int128 x = ((unsigned __int128)dig[kt] << 64) | ((unsigned __int128)(kt >= 1 ? dig[kt - 1] : 0u) << 32) |
+                        (kt >= 2 ? dig[kt - 2] : 0u);
+  x <<= sh;
+  const unsigned long long m64 = (unsigned long long)(x >> 32);
+  bool below = (uint32_t)x != 0;
+  for (int k = kt - 3; k >= 0 && !below; --k) below = dig[k] != 0;
   double r;
   if (top <= 52) {
-    unsigned long long m = 0;
-    for (int p = top; p >= 0; --p) m = (m << 1) | bit(p);
-    r = scalbn((double)m, lo_exp);
+    r = scalbn((double)(m64 >> (63 - top)), lo_exp);
   } else {
-    unsigned long long m = 0;
-    for (int p = top; p >= top - 52; --p) m = (m << 1) | bit(p);
-    int lo = top - 52;
-    unsigned long long rb = bit(lo - 1);
-    bool sticky = false;
-    for (int p = lo - 2; p >= 0 && !sticky; --p) sticky = bit(p);
-    if (rb && (sticky || (m & 1))) ++m;
-    r = scalbn((double)m, lo + lo_exp);
+    unsigned long long m = m64 >> 11;  // bits [top - 52, top]
+    const bool rb = (m64 >> 10) & 1;   // the bit below them
+    const bool sticky = (m64 & 0x3FF) != 0 || below;
+    if (rb && (sticky || (m & 1))) ++m;  // round half to even
+    r = scalbn((double)m, top - 52 + lo_exp);
   }
   return neg ? -r : r;
 }
