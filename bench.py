@@ -645,7 +645,7 @@ class C4:
 
     def roofline(self, kstats):
         names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit",
-                 "agg_hash_jit")
+                 "agg_hash_jit", "join_agg_jit")
         ms = sum(kstats.get(k, (0, 0.0))[1] for k in names)
         steps = max(1, kstats.get("insert_kernel", (1, 0.0))[0])
         kb = int(self.bo32[-1].item()) + sum(int(k[0][-1].item()) for k in self.keep)
@@ -766,7 +766,7 @@ def run_workload(args, rank, world, local, torch, dist):
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
     names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
-             "predicate_kernel", "expr_kernel")
+             "join_agg_jit", "predicate_kernel", "expr_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
     ctx.set_profiling(False)
     t = torch.tensor([ms], device=device, dtype=torch.float64)

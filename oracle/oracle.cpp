@@ -236,13 +236,17 @@ struct ExactSum {
 // ===================================================== column utilities ====
 ColP take_col(const Col& c, const std::vector<int64_t>& idx, const std::string& name,
               bool nullable) {
-  // arrow compute::take; idx < 0 means a null index.
+  // arrow compute::take; idx < 0 means a null index. A null value at a valid
+  // index keeps its raw slot for fixed-width and Boolean columns (take_native
+  // and take_bits copy the values buffer whatever its validity) and is empty
+  // for Utf8 (take_bytes appends no bytes for it).
   Builder b = builder_like(c, name, nullable);
   b.reserve((int64_t)idx.size());
   for (int64_t i : idx) {
     if (i < 0) { b.push_null(); continue; }
     if (i >= c.len) fail(PRISM_ERR_ARROW, "Out-of-bounds index " + std::to_string(i));
-    b.push_from(c, i);
+    if (c.null_at(i) && c.ty != T_UTF8) b.push_slot(c, i);
+    else b.push_from(c, i);
   }
   return b.finish();
 }
@@ -1358,8 +1362,9 @@ Batch join_aggregate(const std::vector<Batch>& probes, const Batch& build,
 
   std::vector<Batch> partials;
   int n_probe_cols = (int)probes[0].cols.size();
+  Batch empty_projected;  // probe batch 0 joined with no rows
   for (size_t bi = 0; bi < probes.size(); ++bi) {
-    if (mp[bi].empty()) continue;
+    if (mp[bi].empty() && bi != 0) continue;
     // project_join_matches: take referenced joined columns, evaluate exprs
     Batch joined;
     joined.rows = (int64_t)mp[bi].size();
@@ -1395,7 +1400,10 @@ Batch join_aggregate(const std::vector<Batch>& probes, const Batch& build,
         joined.cols[c] = z;
       }
     Batch projected = project_exprs(joined, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64);
-    if (projected.rows == 0) continue;
+    if (projected.rows == 0) {
+      if (bi == 0) empty_projected = projected;
+      continue;
+    }
     partials.push_back(aggregate_batches({projected}, projected.cols, wcfg, 1, false));
   }
   // final merge config: SUM for SUM/COUNT/COUNT_DISTINCT, MIN, MAX
@@ -1410,10 +1418,11 @@ Batch join_aggregate(const std::vector<Batch>& probes, const Batch& build,
   prism_agg_config mcfg{agg.n_group_by, mgb.data(), (int32_t)merge.size(), merge.data()};
   Batch merged;
   if (partials.empty()) {
-    // no matches: the unfused path would aggregate an empty join output
-    Batch out;
-    out.rows = 0;
-    return out;
+    // no matches: the fused executor declines (executor.rs:444-446) and the
+    // unfused plan aggregates the empty projected join output, which
+    // hash_aggregate answers with its empty result (group and aggregate
+    // fields, hash_aggregate.rs:188-203, 506-525)
+    return aggregate_batches({empty_projected}, empty_projected.cols, agg, 1, false);
   }
   merged = aggregate_batches(partials, partials[0].cols, mcfg, n_threads, false);
   // reconstruct

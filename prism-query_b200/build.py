@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "--fmad=false",
          "-I", INCLUDE, "-I", CSRC]
 # device headers embedded into the library for run-time compiled kernels
-JIT_HEADERS = ["common.cuh", "eval.cuh", "agg_device.cuh"]
+JIT_HEADERS = ["common.cuh", "eval.cuh", "join_device.cuh", "agg_device.cuh"]
 
 
 def sources():

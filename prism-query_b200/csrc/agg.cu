@@ -27,6 +27,7 @@
 #include "agg.hpp"
 #include "agg_device.cuh"
 #include "jit.hpp"
+#include "join.hpp"
 #include "prims.hpp"
 
 namespace prism {
@@ -330,17 +331,20 @@ __global__ void place_groups_kernel(const unsigned long long* gfirst, const uint
 }
 
 // Up to SMALL_GROUPS groups are put in first-seen order by one block: the
-// groups' (first row, slot) pairs sorted in shared memory (bitonic). The
-// candidates are the slots ginsert listed (plus the side slot when used),
-// or, for dense ids, every slot with a row. out[0] = the group count, or
-// ~0 when there are more groups than the block sorts (the general path
-// then orders them).
+// groups' (first row, slot) pairs sorted in shared memory (bitonic, 64-bit
+// order keys: a row index, or a fused join's (probe row << 32 | build row)).
+// The candidates are the slots ginsert listed (plus the side slot when
+// used), or, for dense ids, every slot with a row. out[0] = the group count,
+// or ~0 when there are more groups than the block sorts (the general path
+// then orders them). Dynamic shared memory: SMALL_GROUPS * 12 bytes.
 constexpr int SMALL_GROUPS = 4096;
+constexpr size_t SMALL_SMEM = SMALL_GROUPS * 12;
 __global__ void __launch_bounds__(1024) small_order_kernel(const unsigned long long* gfirst, const uint32_t* gnew,
                                                            const unsigned long long* gnew_count, int64_t scan_n,
-                                                           int64_t side, uint32_t* ordered, uint32_t* rows32,
-                                                           unsigned long long* out) {
-  __shared__ unsigned long long key[SMALL_GROUPS];
+                                                           int64_t side, uint32_t* ordered, unsigned long long* firsts,
+                                                           uint32_t* rows32, unsigned long long* out) {
+  extern __shared__ unsigned long long okey[];  // [SMALL_GROUPS] order keys | [SMALL_GROUPS] u32 slots
+  uint32_t* oslot = reinterpret_cast<uint32_t*>(okey + SMALL_GROUPS);
   __shared__ unsigned int cnt;
   const int tid = threadIdx.x;
   if (gnew) {
@@ -351,43 +355,68 @@ __global__ void __launch_bounds__(1024) small_order_kernel(const unsigned long l
     }
     for (int i = tid; i < (int)listed; i += blockDim.x) {
       const uint32_t s = gnew[i];
-      key[i] = (gfirst[s] << 32) | s;
+      okey[i] = gfirst[s];
+      oslot[i] = s;
     }
     if (tid == 0) {
       cnt = (unsigned int)listed;
-      if (side >= 0 && gfirst[side] != ~0ULL) key[cnt++] = (gfirst[side] << 32) | (uint64_t)side;
+      if (side >= 0 && gfirst[side] != ~0ULL) {
+        okey[cnt] = gfirst[side];
+        oslot[cnt] = (uint32_t)side;
+        ++cnt;
+      }
     }
   } else {
     if (tid == 0) cnt = 0;
     __syncthreads();
     for (int64_t s = tid; s < scan_n; s += blockDim.x)
-      if (gfirst[s] != ~0ULL) key[atomicAdd(&cnt, 1u)] = (gfirst[s] << 32) | (uint64_t)s;
+      if (gfirst[s] != ~0ULL) {
+        const unsigned int p = atomicAdd(&cnt, 1u);
+        okey[p] = gfirst[s];
+        oslot[p] = (uint32_t)s;
+      }
   }
   __syncthreads();
   const int n = (int)cnt;
   int m = 1;
   while (m < n) m <<= 1;
-  for (int i = n + tid; i < m; i += blockDim.x) key[i] = ~0ULL;
+  for (int i = n + tid; i < m; i += blockDim.x) {
+    okey[i] = ~0ULL;
+    oslot[i] = 0xFFFFFFFFu;
+  }
   __syncthreads();
+  // order keys are distinct (one first row per group)
   for (int k = 2; k <= m; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int i = tid; i < m; i += blockDim.x) {
         const int ixj = i ^ j;
         if (ixj > i) {
-          const unsigned long long x = key[i], y = key[ixj];
+          const unsigned long long x = okey[i], y = okey[ixj];
           if ((x > y) == ((i & k) == 0)) {
-            key[i] = y;
-            key[ixj] = x;
+            okey[i] = y;
+            okey[ixj] = x;
+            const uint32_t t = oslot[i];
+            oslot[i] = oslot[ixj];
+            oslot[ixj] = t;
           }
         }
       }
       __syncthreads();
     }
   for (int i = tid; i < n; i += blockDim.x) {
-    ordered[i] = (uint32_t)key[i];
-    rows32[i] = (uint32_t)(key[i] >> 32);
+    ordered[i] = oslot[i];
+    firsts[i] = okey[i];
+    rows32[i] = (uint32_t)okey[i];
   }
   if (tid == 0) *out = (unsigned long long)n;
+}
+
+// the probe and build rows of fused-join order keys (probe row << 32 | build row)
+__global__ void split_join_rows_kernel(const unsigned long long* firsts, int64_t n, uint32_t* prow, uint32_t* brow) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    prow[i] = (uint32_t)(firsts[i] >> 32);
+    brow[i] = (uint32_t)firsts[i];
+  }
 }
 
 // exact big integer (signed 64-bit counters of 32-bit limbs, weight
@@ -678,9 +707,46 @@ int result_type(int func) {
 
 }  // namespace
 
-Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_agg_config& cfg,
+Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const prism_agg_config& cfg,
                 const prism_predicate* pred, const int32_t* cols, int n_cols, const prism_expr* exprs,
-                int n_exprs, int arith_mode, bool fused, const AggTuning& tune) {
+                int n_exprs, int arith_mode, bool fused, const AggTuning& tune, const JoinAggSpec* join) {
+  // fused join: each probe batch is seen as the joined batch [probe columns,
+  // build columns] with the probe batch's rows; build-side columns are read
+  // at the matched build row inside the kernel
+  const int n_probe_cols = join ? (int)batches_in.at(0)->cols.size() : -1;
+  auto fused_fail = [](const std::string& why) {
+    fail(PRISM_ERR_INVALID_ARGUMENT, why + " is not supported in the fused path");
+  };
+  std::vector<Batch> joined;
+  std::vector<const Batch*> joined_ptrs;
+  if (join) {
+    if (!fused) fail(PRISM_ERR_INTERNAL, "fused join aggregation without a projection");
+    if (!jit_enabled()) fused_fail("a join without run-time compilation");
+    // build columns named like a probe column are `<name>_right` in the
+    // joined schema, as the joined batch names them (hash_join.rs:436-447)
+    std::vector<ColP> bcols;
+    for (auto& c : join->table->build.cols) {
+      bool clash = false;
+      for (auto& pc : batches_in[0]->cols) clash |= pc->name == c->name;
+      if (!clash) {
+        bcols.push_back(c);
+        continue;
+      }
+      auto r = std::make_shared<Column>(*c);
+      r->name = c->name + "_right";
+      bcols.push_back(r);
+    }
+    joined.reserve(batches_in.size());
+    for (auto* p : batches_in) {
+      Batch v;
+      v.rows = p->rows;
+      v.cols = p->cols;
+      for (auto& c : bcols) v.cols.push_back(c);
+      joined.push_back(std::move(v));
+    }
+    for (auto& v : joined) joined_ptrs.push_back(&v);
+  }
+  const std::vector<const Batch*>& batches = join ? joined_ptrs : batches_in;
   for (int i = 0; i < cfg.n_aggs; ++i)
     if (cfg.aggs[i].func < PRISM_AGG_SUM || cfg.aggs[i].func > PRISM_AGG_COUNT_DISTINCT)
       fail(PRISM_ERR_UNSUPPORTED_AGGREGATION, "unknown aggregate function");
@@ -901,7 +967,11 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   int64_t G = 1;
   std::vector<int> gbatch_cols;
   for (int g = 0; g < cfg.n_group_by; ++g) gbatch_cols.push_back(proj[cfg.group_by[g]].batch_col);
-  if (cfg.n_group_by == 0) {
+  if (join) {
+    // hashed groups (no group columns: every row hashes to one group)
+    for (auto& o : P.outs)
+      if (o.op == -2) fused_fail("COUNT(*) over a join");
+  } else if (cfg.n_group_by == 0) {
     dense = true;
     G = 1;
   } else {
@@ -980,8 +1050,11 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
   int hss_log2 = 0;
   size_t hsmem = 0;
   if (!dense && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 && tiny_fits_registers(A) && jit_enabled()) {
-    const size_t hbudget = (size_t)smem_optin - TINY_MAX_COLS * sizeof(DCol) - 1024;
-    for (int l = 12; l >= 8; --l) {
+    // a fused join waits on dependent loads per row: a smaller table (half
+    // a block's share of the SM) keeps two blocks resident per SM
+    const size_t hbudget = join ? (size_t)smem_optin / 2 - TINY_MAX_COLS * sizeof(DCol) - 1024
+                                : (size_t)smem_optin - TINY_MAX_COLS * sizeof(DCol) - 1024;
+    for (int l = join ? 10 : 12; l >= 8; --l) {
       if ((1 << l) > 2 * std::max(128, tune.smem_groups)) continue;
       if (((size_t)(2 + W) * 8 << l) <= hbudget) {
         hss_log2 = l;
@@ -990,8 +1063,23 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
       }
     }
   }
+  if (join && !hss_log2) fused_fail("this aggregate list over a join");
   uint64_t gcap = dense ? (uint64_t)G : std::max<uint64_t>(1024, next_pow2((uint64_t)std::min<int64_t>(total_rows, 1 << 16) * 2));
   int dist_log2 = 0;
+  // fused join: device views of each probe batch's key columns
+  std::vector<MemP> jpk_mem;
+  std::vector<const DCol*> jpk_dev;
+  if (join) {
+    if (total_rows >= (int64_t)UINT32_MAX) fused_fail("a join over 2^32 probe rows");
+    for (auto* pb : batches_in) {
+      std::vector<DCol> v;
+      for (int k : join->probe_keys) v.push_back(pb->cols.at(k)->view());
+      MemP m = ctx.alloc(v.size() * sizeof(DCol));
+      PRISM_CUDA(cudaMemcpyAsync(m->ptr, v.data(), v.size() * sizeof(DCol), cudaMemcpyHostToDevice, ctx.stream));
+      jpk_dev.push_back(static_cast<const DCol*>(m->ptr));
+      jpk_mem.push_back(m);
+    }
+  }
   for (int attempt = 0; attempt < 40; ++attempt) {
     MemP mkeys, mfirst, macc, mmax;
     uint64_t nslots = dense ? gcap : gcap + 1;
@@ -1068,7 +1156,27 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         if (!src.empty()) jk = jit_get(src, "prism_tiny_agg");
       }
       const void* hk = nullptr;
-      if (!jk && hss_log2 && !A.wide) {
+      if (join) {
+        const JoinTable& t = *join->table;
+        a.join = 1;
+        a.jfast = t.int64_fast ? 1 : 0;
+        a.jslots = t.slots ? static_cast<const ulonglong2*>(t.slots->ptr) : nullptr;
+        a.jshift = 64 - t.log2cap;
+        a.jmask = t.capacity - 1;
+        a.jcap = t.capacity;
+        a.jdup = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+        a.jdense = t.dense ? static_cast<const uint32_t*>(t.dense_rows->ptr) : nullptr;
+        a.jdmin = t.dmin;
+        a.jdrange = t.drange;
+        a.jpk = jpk_dev[&b - &joined[0]];
+        a.jbk = static_cast<const DCol*>(t.key_views_dev->ptr);
+        a.jnkeys = (int)join->probe_keys.size();
+        a.n_cols = (int)pg.cols.size();
+        if (A.wide) fused_fail("a Float64 sum beyond the 192-bit window over a join");
+        std::string src = jit_hash_agg_source(pg, b, a, n_probe_cols);
+        if (src.empty()) fused_fail("this projection over a join");
+        hk = jit_get(src, "prism_join_agg");
+      } else if (!jk && hss_log2 && !A.wide) {
         a.n_cols = (int)pg.cols.size();
         std::string src = jit_hash_agg_source(pg, b, a);
         if (!src.empty()) hk = jit_get(src, "prism_hash_agg");
@@ -1081,7 +1189,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
         int hgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)HASH_BLOCK * TINY_R * 4),
                                            (int64_t)ctx.sm_count * std::max(1, per_sm));
         void* params[] = {&a};
-        KernelTimer kt(ctx, "agg_hash_jit");
+        KernelTimer kt(ctx, join ? "join_agg_jit" : "agg_hash_jit");
         PRISM_CUDA(cudaLaunchKernel(hk, dim3(hgrid), dim3(HASH_BLOCK), params, hsmem, ctx.stream));
       } else if (jk) {
         a.n_cols = (int)pg.cols.size();
@@ -1110,14 +1218,18 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
     const bool small_try = total_rows < (int64_t)UINT32_MAX && (!dense || (int64_t)nslots <= SMALL_GROUPS);
     uint32_t* s_ordered = nullptr;
     uint32_t* s_rows = nullptr;
+    unsigned long long* s_firsts = nullptr;
     unsigned long long* s_out = nullptr;
-    MemP mso, msr;
+    MemP mso, msr, msf;
     if (small_try) {
       s_ordered = ctx.alloc_t<uint32_t>(SMALL_GROUPS, mso);
       s_rows = ctx.alloc_t<uint32_t>(SMALL_GROUPS, msr);
+      s_firsts = ctx.alloc_t<unsigned long long>(SMALL_GROUPS, msf);
       s_out = ctx.alloc_t<unsigned long long>(1, msmall);
-      small_order_kernel<<<1, 1024, 0, ctx.stream>>>(A.gfirst, A.gnew, A.gnew_count, dense ? (int64_t)nslots : 0,
-                                                     dense ? -1 : (int64_t)gcap, s_ordered, s_rows, s_out);
+      PRISM_CUDA(cudaFuncSetAttribute(small_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_SMEM));
+      small_order_kernel<<<1, 1024, SMALL_SMEM, ctx.stream>>>(A.gfirst, A.gnew, A.gnew_count,
+                                                              dense ? (int64_t)nslots : 0, dense ? -1 : (int64_t)gcap,
+                                                              s_ordered, s_firsts, s_rows, s_out);
       ctx.check_launch("small_order_kernel");
     }
     unsigned long long small_n = ~0ULL;
@@ -1159,10 +1271,22 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
     uint32_t* ordered = nullptr;
     uint32_t* rows32 = nullptr;  // first row of each output group (u32)
     MemP mslots, mcnt, mbits, mwc, mwo, mord, mof, mrow;
+    MemP mjp, mjb;
+    uint32_t* jprow = nullptr;  // fused join: first joined row's probe row (global) and build row per group
+    uint32_t* jbrow = nullptr;
+    if (join && !(small_try && small_n != ~0ULL)) fused_fail("more than 4,096 groups over a join");
     if (small_try && small_n != ~0ULL) {
       G_out = (int64_t)small_n;
       ordered = s_ordered;
       rows32 = s_rows;
+      if (join) {
+        jprow = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mjp);
+        jbrow = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(G_out, 1), mjb);
+        if (G_out) {
+          split_join_rows_kernel<<<grid_for(ctx, G_out, 256), 256, 0, ctx.stream>>>(s_firsts, G_out, jprow, jbrow);
+          ctx.check_launch("split_join_rows_kernel");
+        }
+      }
     } else {
       uint32_t* slots = ctx.alloc_t<uint32_t>(nslots, mslots);
       unsigned long long* counter = ctx.alloc_t<unsigned long long>(1, mcnt);
@@ -1208,14 +1332,19 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_
     if (cfg.n_group_by) {
       for (int k = 0; k < cfg.n_group_by; ++k) {
         int bc = gbatch_cols[k];
-        std::vector<const Column*> parts;
-        for (auto* b : batches)
-          if (b->rows) parts.push_back(b->cols[bc].get());
-        ColP keycol;
-        ColP src = parts.size() == 1 ? std::shared_ptr<Column>(std::shared_ptr<Column>{}, const_cast<Column*>(parts[0]))
-                                     : concat_columns(ctx, parts);
         const Column& rc = *ref.cols[bc];
-        keycol = take(ctx, *src, rows32, nullptr, G_out, rc.name, rc.nullable);
+        ColP keycol;
+        if (join && bc >= n_probe_cols) {  // build-side key: read at the build row
+          keycol = take(ctx, *join->table->build.cols[bc - n_probe_cols], jbrow, nullptr, G_out, rc.name, rc.nullable);
+        } else {
+          std::vector<const Column*> parts;
+          for (auto* b : batches)
+            if (b->rows) parts.push_back(b->cols[bc].get());
+          ColP src = parts.size() == 1
+                         ? std::shared_ptr<Column>(std::shared_ptr<Column>{}, const_cast<Column*>(parts[0]))
+                         : concat_columns(ctx, parts);
+          keycol = take(ctx, *src, join ? jprow : rows32, nullptr, G_out, rc.name, rc.nullable);
+        }
         if (fused && cfg.group_by[k] >= n_cols) keycol->name = proj_name(cfg.group_by[k]);
         out.cols.push_back(keycol);
       }

@@ -13,11 +13,25 @@ struct AggTuning {
   int blocks_per_sm = 1;
 };
 
+struct JoinTable;
+
+// A fused join -> aggregate (prism-substrait/src/executor.rs:333-842): the
+// aggregated batches are probe batches joined with `table`'s build side on
+// `probe_keys` inside the aggregation kernel; the projection indexes the
+// joined schema (probe columns, then build columns).
+struct JoinAggSpec {
+  const JoinTable* table = nullptr;
+  std::vector<int> probe_keys;
+};
+
 // Aggregates `batches` (all with one schema). When `pred`/`exprs` are given
 // the aggregate config indexes the projected schema [cols..., expr_i...]
 // and the filter/projection is evaluated inside the aggregation kernel.
+// With `join`, the fused join -> aggregate kernel runs instead (fused must
+// be true); shapes it does not cover fail with PRISM_ERR_INVALID_ARGUMENT
+// and a message naming the fused path, so the caller can materialize.
 Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches, const prism_agg_config& cfg,
                 const prism_predicate* pred, const int32_t* cols, int n_cols, const prism_expr* exprs,
-                int n_exprs, int arith_mode, bool fused, const AggTuning& tune);
+                int n_exprs, int arith_mode, bool fused, const AggTuning& tune, const JoinAggSpec* join = nullptr);
 
 }  // namespace prism

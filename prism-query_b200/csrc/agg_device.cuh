@@ -8,6 +8,7 @@
 #pragma once
 
 #include "eval.cuh"
+#include "join_device.cuh"
 
 namespace prism {
 
@@ -77,6 +78,22 @@ struct AggArgs {
   unsigned long long* gkeys;
   unsigned long long* gfirst;
   unsigned long long* gacc;
+  // fused join (join_body): each probe row looks up the build table and
+  // every matched build row is aggregated as a joined row; the program
+  // columns of the build side are read at the build row
+  int32_t join;
+  int32_t jfast;             // single Int64 key matched by raw value
+  const ulonglong2* jslots;  // {key or row hash, cnt << 32 | row}; [jcap] = side slot
+  int32_t jshift;
+  uint64_t jmask;
+  uint64_t jcap;
+  const uint32_t* jdup;      // build rows of multi-row slots
+  const uint32_t* jdense;    // dense mode: build row per key - jdmin
+  int64_t jdmin;
+  uint64_t jdrange;
+  const DCol* jpk;           // probe key column views
+  const DCol* jbk;           // build key column views
+  int32_t jnkeys;
   uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
   unsigned long long* gnew_count;  // length of gnew
   uint64_t gmask;
@@ -345,19 +362,20 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       I at = base + r * stride;
-      rows[r] = E::fetch(cols, at < last ? at : last);  // rows past the end read the last row and are dropped
+      I idx = at < last ? at : last;
+      rows[r] = E::fetch(cols, idx, idx);  // rows past the end read the last row and are dropped
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       I at = base + r * stride;
       I idx = at < last ? at : last;
-      bool keep = at <= last && E::keep(a, K, cols, idx, rows[r]);
-      int g = E::gid(a, K, cols, idx, rows[r]);
+      bool keep = at <= last && E::keep(a, K, cols, idx, idx, rows[r]);
+      int g = E::gid(a, K, cols, idx, idx, rows[r]);
       bool bad = keep && (g < 0 || g >= G);
       err |= bad;
       slot[r] = (keep && !bad) ? g : G;
       flags[r] = 0;
-      E::values(a, K, cols, idx, rows[r], v[r], flags[r]);
+      E::values(a, K, cols, idx, idx, rows[r], v[r], flags[r]);
     }
     // phase 2: the accumulators; rows with a flagged op first get its
     // 128-bit recomputation and take the general accumulate path, the others
@@ -379,7 +397,7 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
         Val w[NOPS];
 #pragma unroll
         for (int j = 0; j < NOPS; ++j) {
-          SlowVal sv = E::slow(a, j, cols, at);
+          SlowVal sv = E::slow(a, j, cols, at, at);
           w[j] = sv.v;
           err |= sv.ovf;
         }
@@ -506,25 +524,110 @@ __device__ __forceinline__ void hash_accumulate(const AggArgs& a, unsigned long 
   }
 }
 
+// the block's table: skeys[SS] | sfirst[SS] | sacc[SS][kW] in dynamic
+// shared memory
+struct HashTable {
+  unsigned long long* keys;
+  unsigned long long* first;
+  unsigned long long* acc;
+  uint32_t mask;
+  int shift;
+};
+
+template <class E>
+__device__ __forceinline__ HashTable hash_table_init(const AggArgs& a, unsigned long long* smem, int tid, int block) {
+  constexpr int W = E::kW;
+  const int SS = 1 << a.ss_log2;
+  HashTable t{smem, smem + SS, smem + 2 * SS, (uint32_t)SS - 1, 64 - a.ss_log2};
+  for (int i = tid; i < SS; i += block) {
+    t.keys[i] = GEMPTY;
+    t.first[i] = ~0ULL;
+  }
+  for (int i = tid; i < SS * W; i += block) t.acc[i] = a.winit[i % W];
+  return t;
+}
+
+// one (joined) row into its group: find or claim the key's slot, else the
+// global table; `first` orders the rows (first-seen order of the groups)
+template <class E, int NOPS>
+__device__ __forceinline__ void hash_row_update(const AggArgs& a, const HashTable& t, uint64_t h, uint64_t first,
+                                                const Val* v, unsigned flags, const DCol* cols,
+                                                typename E::idx_t idx, typename E::idx_t bidx, bool& err) {
+  constexpr int W = E::kW;
+  int s = -1;
+  if (h != GEMPTY) {
+    uint32_t p = (uint32_t)((h * FIB) >> t.shift);
+    for (int step = 0; step < HASH_PROBES; ++step) {
+      unsigned long long cur = *(volatile unsigned long long*)&t.keys[p];
+      if (cur == GEMPTY) {
+        cur = atomicCAS(&t.keys[p], GEMPTY, h);
+        if (cur == GEMPTY) cur = h;
+      }
+      if (cur == h) {
+        s = (int)p;
+        break;
+      }
+      p = (p + 1) & t.mask;
+    }
+  }
+  unsigned long long* acc;
+  if (s >= 0) {
+    if (first < t.first[s]) atomicMin(&t.first[s], first);
+    acc = t.acc + (size_t)s * W;
+  } else {
+    const int64_t gs = ginsert(a, h);
+    if (gs < 0) return;
+    if (first < a.gfirst[gs]) atomicMin(&a.gfirst[gs], first);
+    acc = a.gacc + (size_t)gs * W;
+  }
+  if (flags) {
+    // every op of the row recomputed exactly
+    Val w[NOPS];
+#pragma unroll
+    for (int j = 0; j < NOPS; ++j) {
+      SlowVal sv = E::slow(a, j, cols, idx, bidx);
+      w[j] = sv.v;
+      err |= sv.ovf;
+    }
+    hash_accumulate<E, NOPS, false>(a, acc, w);
+  } else {
+    hash_accumulate<E, NOPS, true>(a, acc, v);
+  }
+}
+
+// folds the block's table into the global one: each used slot's global slot
+// resolved once (kept in keys, -1: none), then one thread per (slot, word)
+template <class E>
+__device__ __forceinline__ void hash_table_merge(const AggArgs& a, const HashTable& t, int tid, int block) {
+  constexpr int W = E::kW;
+  const int SS = 1 << a.ss_log2;
+  for (int i = tid; i < SS; i += block) {
+    const unsigned long long k = t.keys[i];
+    long long gs = -1;
+    if (k != GEMPTY) {
+      gs = ginsert(a, k);
+      if (gs >= 0) atomicMin(&a.gfirst[gs], t.first[i]);
+    }
+    t.keys[i] = (unsigned long long)gs;
+  }
+  __syncthreads();
+  for (int q = tid; q < SS * W; q += block) {
+    const int i = q / W, w = q - i * W;
+    const long long gs = (long long)t.keys[i];
+    if (gs < 0) continue;
+    const unsigned long long x = t.acc[q];
+    if (x != a.winit[w]) merge_word(a.gacc + (size_t)gs * W + w, x, a.wkind[w]);
+  }
+}
+
 template <class E, int NOPS, int BLOCK>
 __device__ __forceinline__ void hash_body(const AggArgs& a) {
-  constexpr int W = E::kW;
-  extern __shared__ unsigned long long hsm[];  // skeys[SS] | sfirst[SS] | sacc[SS][W]
+  extern __shared__ unsigned long long hsm[];
   __shared__ DCol scols[TINY_MAX_COLS];
   const int tid = threadIdx.x;
-  const int SS = 1 << a.ss_log2;
-  const uint32_t smask = (uint32_t)SS - 1;
-  const int sshift = 64 - a.ss_log2;
-  unsigned long long* skeys = hsm;
-  unsigned long long* sfirst = hsm + SS;
-  unsigned long long* sacc = hsm + 2 * SS;
   const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
   if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
-  for (int i = tid; i < SS; i += BLOCK) {
-    skeys[i] = GEMPTY;
-    sfirst[i] = ~0ULL;
-  }
-  for (int i = tid; i < SS * W; i += BLOCK) sacc[i] = a.winit[i % W];
+  const HashTable t = hash_table_init<E>(a, hsm, tid, BLOCK);
   __syncthreads();
   const DCol* cols = shared_cols ? scols : a.cols;
   const typename E::Consts K = E::load(a);
@@ -541,85 +644,118 @@ __device__ __forceinline__ void hash_body(const AggArgs& a) {
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       I at = base + r * stride;
-      rows[r] = E::fetch(cols, at < last ? at : last);  // rows past the end read the last row and are dropped
+      I idx = at < last ? at : last;
+      rows[r] = E::fetch(cols, idx, idx);  // rows past the end read the last row and are dropped
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       I at = base + r * stride;
       I idx = at < last ? at : last;
-      keep[r] = at <= last && E::keep(a, K, cols, idx, rows[r]);
-      hs[r] = E::hash(a, K, cols, idx, rows[r]);
+      keep[r] = at <= last && E::keep(a, K, cols, idx, idx, rows[r]);
+      hs[r] = E::hash(a, K, cols, idx, idx, rows[r]);
       flags[r] = 0;
-      E::values(a, K, cols, idx, rows[r], v[r], flags[r]);
+      E::values(a, K, cols, idx, idx, rows[r], v[r], flags[r]);
     }
 #pragma unroll
     for (int r = 0; r < TINY_R; ++r) {
       if (!keep[r]) continue;
       const I at = base + r * stride;
-      const uint64_t h = hs[r];
-      // find or claim the key's slot
-      int s = -1;
-      if (h != GEMPTY) {
-        uint32_t p = (uint32_t)((h * FIB) >> sshift);
-        for (int step = 0; step < HASH_PROBES; ++step) {
-          unsigned long long cur = *(volatile unsigned long long*)&skeys[p];
-          if (cur == GEMPTY) {
-            cur = atomicCAS(&skeys[p], GEMPTY, h);
-            if (cur == GEMPTY) cur = h;
-          }
-          if (cur == h) {
-            s = (int)p;
-            break;
-          }
-          p = (p + 1) & smask;
-        }
-      }
-      const uint64_t grow = a.row_base + (uint64_t)at;
-      unsigned long long* acc;
-      if (s >= 0) {
-        if (grow < sfirst[s]) atomicMin(&sfirst[s], grow);
-        acc = sacc + (size_t)s * W;
-      } else {
-        const int64_t gs = ginsert(a, h);
-        if (gs < 0) continue;
-        if (grow < a.gfirst[gs]) atomicMin(&a.gfirst[gs], grow);
-        acc = a.gacc + (size_t)gs * W;
-      }
-      if (flags[r]) {
-        // every op of the row recomputed exactly
-        Val w[NOPS];
+      hash_row_update<E, NOPS>(a, t, hs[r], a.row_base + (uint64_t)at, v[r], flags[r], cols, at, at, err);
+    }
+  }
+  if (err) atomicOr(a.err, DERR_RANGE);
+  __syncthreads();
+  hash_table_merge<E>(a, t, tid, BLOCK);
+}
+
+// The fused join -> aggregate body: one probe row per thread and step
+// (JOIN_R rows in flight), its key looked up in the build table as the probe
+// kernels do (join_device.cuh), and every matched build row, in ascending
+// order, aggregated as the joined row (probe row, build row) into the
+// block's table. The order key of a joined row is
+// (global probe row << 32 | build row), which sorts like the joined rows'
+// positions (probe rows ascending, build rows ascending inside one).
+constexpr int JOIN_R = 2;
+
+template <class E, int NOPS, int BLOCK>
+__device__ __forceinline__ void join_body(const AggArgs& a) {
+  extern __shared__ unsigned long long hsm[];
+  __shared__ DCol scols[TINY_MAX_COLS];
+  const int tid = threadIdx.x;
+  const bool shared_cols = a.n_cols <= TINY_MAX_COLS;
+  if (shared_cols && tid < a.n_cols) scols[tid] = a.cols[tid];
+  const HashTable t = hash_table_init<E>(a, hsm, tid, BLOCK);
+  __syncthreads();
+  const DCol* cols = shared_cols ? scols : a.cols;
+  const typename E::Consts K = E::load(a);
+  using I = typename E::idx_t;
+  const I stride = (I)gridDim.x * BLOCK;
+  const I n = (I)a.n;
+  bool err = false;
+  for (I base = (I)blockIdx.x * BLOCK + tid; base < n; base += stride * JOIN_R) {
+    // the build candidates of JOIN_R probe rows (their lookups in flight together)
+    uint32_t cand[JOIN_R], cnt[JOIN_R];
 #pragma unroll
-        for (int j = 0; j < NOPS; ++j) {
-          SlowVal sv = E::slow(a, j, cols, at);
-          w[j] = sv.v;
-          err |= sv.ovf;
+    for (int r = 0; r < JOIN_R; ++r) {
+      const I idx = base + r * stride;
+      cand[r] = JOIN_NO_MATCH;
+      cnt[r] = 0;
+      if (idx >= n) continue;
+      if (a.jfast) {
+        const uint64_t key = (uint64_t)static_cast<const int64_t*>(a.jpk[0].values)[idx];
+        if (a.jdense) {
+          const uint64_t d = key - (uint64_t)a.jdmin;
+          const uint32_t row = d < a.jdrange ? __ldg(a.jdense + d) : JOIN_NO_MATCH;
+          if (row != JOIN_NO_MATCH) {
+            cand[r] = row;
+            cnt[r] = 1;
+          }
+          continue;
         }
-        hash_accumulate<E, NOPS, false>(a, acc, w);
+        uint64_t s = key == JOIN_EMPTY ? a.jcap : join_slot_of(key, a.jshift);
+        ulonglong2 e = __ldg(a.jslots + s);
+        for (uint64_t steps = 0; e.x != key && e.x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
+          s = (s + 1) & a.jmask;
+          e = __ldg(a.jslots + s);
+        }
+        if (e.x == key) {
+          cand[r] = (uint32_t)e.y;
+          cnt[r] = (uint32_t)(e.y >> 32);
+        }
       } else {
-        hash_accumulate<E, NOPS, true>(a, acc, v[r]);
+        const uint64_t key = join_key_hash(a.jpk, a.jnkeys, idx);
+        uint64_t s = join_slot_of(key, a.jshift);
+        ulonglong2 e = __ldg(a.jslots + s);
+        for (uint64_t steps = 0; e.x != key && e.x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
+          s = (s + 1) & a.jmask;
+          e = __ldg(a.jslots + s);
+        }
+        if (e.x == key) {
+          cand[r] = (uint32_t)e.y;
+          cnt[r] = (uint32_t)(e.y >> 32);
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < JOIN_R; ++r) {
+      const I idx = base + r * stride;
+      for (uint32_t j = 0; j < cnt[r]; ++j) {
+        const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
+        if (!a.jfast && !join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b)) continue;
+        const I bidx = (I)b;
+        const typename E::Row row = E::fetch(cols, idx, bidx);
+        if (!E::keep(a, K, cols, idx, bidx, row)) continue;
+        const uint64_t h = E::hash(a, K, cols, idx, bidx, row);
+        unsigned flags = 0;
+        Val v[NOPS];
+        E::values(a, K, cols, idx, bidx, row, v, flags);
+        hash_row_update<E, NOPS>(a, t, h, ((a.row_base + (uint64_t)idx) << 32) | b, v, flags, cols, idx, bidx, err);
       }
     }
   }
   if (err) atomicOr(a.err, DERR_RANGE);
   __syncthreads();
-  // each used slot's global slot, kept in skeys (-1: none)
-  for (int i = tid; i < SS; i += BLOCK) {
-    const unsigned long long k = skeys[i];
-    long long gs = -1;
-    if (k != GEMPTY) {
-      gs = ginsert(a, k);
-      if (gs >= 0) atomicMin(&a.gfirst[gs], sfirst[i]);
-    }
-    skeys[i] = (unsigned long long)gs;
-  }
-  __syncthreads();
-  for (int q = tid; q < SS * W; q += BLOCK) {
-    const int i = q / W, w = q - i * W;
-    const long long gs = (long long)skeys[i];
-    if (gs < 0) continue;
-    const unsigned long long x = sacc[q];
-    if (x != a.winit[w]) merge_word(a.gacc + (size_t)gs * W + w, x, a.wkind[w]);
-  }
+  hash_table_merge<E>(a, t, tid, BLOCK);
 }
 
 }  // namespace prism

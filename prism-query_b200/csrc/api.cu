@@ -64,6 +64,12 @@ JoinTuning join_tuning() {
 }
 AggTuning agg_tuning() { return AggTuning{}; }
 
+// PRISM_JOIN_AGG_FUSED=0 materializes the joined rows before aggregating
+bool join_agg_fused() {
+  const char* d = std::getenv("PRISM_JOIN_AGG_FUSED");
+  return !(d && std::strcmp(d, "0") == 0);
+}
+
 std::string right_name(const Batch& probe, const std::string& nm) {
   for (auto& c : probe.cols)
     if (c->name == nm) return nm + "_right";
@@ -688,6 +694,22 @@ int prism_join_aggregate(prism_ctx* c, const prism_batch* const* probes, int32_t
           if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
           need[col] = true;
         }
+      }
+    }
+    if (join_agg_fused()) {
+      // one kernel per probe batch: lookup, projection and aggregation of
+      // the joined rows without materializing them
+      std::vector<const Batch*> pbs;
+      for (int i = 0; i < n_probes; ++i) pbs.push_back(&B(probes[i]));
+      JoinAggSpec js;
+      js.table = t.get();
+      js.probe_keys = pk;
+      try {
+        *out = wrap(c, aggregate(x, pbs, *agg, nullptr, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64, true,
+                                 agg_tuning(), &js));
+        return;
+      } catch (const Failure& f) {
+        if (f.code != PRISM_ERR_INVALID_ARGUMENT || f.msg.find("fused path") == std::string::npos) throw;
       }
     }
     std::vector<Batch> projected;

@@ -184,7 +184,11 @@ struct Gen {
   int col_type(int slot) const { return b.cols[pg.cols[slot]]->type; }
   bool fetched(int slot) const { return width_of(col_type(slot) == TY_DICT ? TY_I32 : col_type(slot)) > 0 || col_type(slot) == TY_BOOL || col_type(slot) == TY_DICT; }
   bool nullable(int slot) const { return b.cols[pg.cols[slot]]->validity != nullptr; }
-  std::string ix(int slot) const { return fetched(slot) ? "0" : "idx"; }
+  // the row index a column is read at: build-side columns of a fused join
+  // at the matched build row `bidx`, every other column at `idx`
+  std::vector<char> bside;
+  std::string rix(int slot) const { return slot < (int)bside.size() && bside[slot] ? "bidx" : "idx"; }
+  std::string ix(int slot) const { return fetched(slot) ? "0" : rix(slot); }
 
   void declare_cols() {
     for (size_t s = 0; s < pg.cols.size(); ++s) {
@@ -207,7 +211,7 @@ struct Gen {
   // validity of the row in column `slot`
   std::string V(int slot) const {
     if (fetched(slot)) return nullable(slot) ? "row.m" + std::to_string(slot) : std::string("true");
-    return "dcol_valid(c" + std::to_string(slot) + ", idx)";
+    return "dcol_valid(c" + std::to_string(slot) + ", " + rix(slot) + ")";
   }
   // plain reader: fn(view, index)
   std::string rd(const char* fn, int slot) const {
@@ -238,26 +242,27 @@ struct Gen {
       if (nullable((int)s)) o << "    bool m" << s << ";\n";
     }
     if (!any) o << "    int unused;\n";
-    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, idx_t idx) {\n    Row w;\n";
+    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, idx_t idx, idx_t bidx) {\n    Row w;\n";
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       if (!fetched((int)s)) continue;
       const Column& c = *b.cols[pg.cols[s]];
       int t = c.type == TY_DICT ? c.index_type : c.type;
       std::string src = "cols[" + std::to_string(s) + "].values";
+      const std::string at = rix((int)s);
       switch (t == TY_BOOL ? 0 : width_of(t)) {
         case 0:
-          o << "    w.r" << s << "[0] = (static_cast<const uint8_t*>(" << src << ")[idx >> 3] >> (idx & 7)) & 1;\n";
+          o << "    w.r" << s << "[0] = (static_cast<const uint8_t*>(" << src << ")[" << at << " >> 3] >> (" << at << " & 7)) & 1;\n";
           break;
-        case 1: o << "    w.r" << s << "[0] = static_cast<const uint8_t*>(" << src << ")[idx];\n"; break;
-        case 2: o << "    w.r" << s << "[0] = static_cast<const uint16_t*>(" << src << ")[idx];\n"; break;
-        case 4: o << "    w.r" << s << "[0] = static_cast<const uint32_t*>(" << src << ")[idx];\n"; break;
-        case 8: o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[idx];\n"; break;
+        case 1: o << "    w.r" << s << "[0] = static_cast<const uint8_t*>(" << src << ")[" << at << "];\n"; break;
+        case 2: o << "    w.r" << s << "[0] = static_cast<const uint16_t*>(" << src << ")[" << at << "];\n"; break;
+        case 4: o << "    w.r" << s << "[0] = static_cast<const uint32_t*>(" << src << ")[" << at << "];\n"; break;
+        case 8: o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[" << at << "];\n"; break;
         default:
-          o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[2 * idx];\n";
-          o << "    w.r" << s << "[1] = static_cast<const unsigned long long*>(" << src << ")[2 * idx + 1];\n";
+          o << "    w.r" << s << "[0] = static_cast<const unsigned long long*>(" << src << ")[2 * " << at << "];\n";
+          o << "    w.r" << s << "[1] = static_cast<const unsigned long long*>(" << src << ")[2 * " << at << " + 1];\n";
       }
       if (c.validity)
-        o << "    w.m" << s << " = (cols[" << s << "].validity[idx >> 3] >> (idx & 7)) & 1;\n";
+        o << "    w.m" << s << " = (cols[" << s << "].validity[" << at << " >> 3] >> (" << at << " & 7)) & 1;\n";
     }
     o << "    return w;\n  }\n";
     return o.str();
@@ -827,6 +832,10 @@ RowParts row_parts(Gen& gen, const AggArgs& a) {
 // struct QueryRow: E of the kernel bodies in agg_device.cuh. `members`
 // adds the body-specific functions and layout constants.
 std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts& rp, const std::string& members) {
+  // row indices address the longest column (a joined batch's build side
+  // may be longer than its probe rows)
+  int64_t max_rows = b.rows;
+  for (auto& c : b.cols) max_rows = std::max<int64_t>(max_rows, c->length);
   std::string consts = gen.consts.str();
   if (consts.empty()) consts = "    int unused;\n";
   std::ostringstream s;
@@ -834,7 +843,7 @@ std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts
        "namespace prism {\n"
        "struct QueryRow {\n"
        "  typedef "
-    << (b.rows < ((int64_t)1 << 31) - ((int64_t)1 << 26) ? "int" : "long long")
+    << (max_rows < ((int64_t)1 << 31) - ((int64_t)1 << 26) ? "int" : "long long")
     << " idx_t;  // row index type: 32-bit below 2^31 rows\n"
        "  struct Consts {\n"
     << consts
@@ -844,7 +853,7 @@ std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts
     << gen.load.str()
     << "    return K;\n  }\n"
        "  static __device__ __forceinline__ bool keep(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
-       "const Row& row) {\n"
+       "idx_t bidx, const Row& row) {\n"
     << rp.keep << "  }\n"
     << members
     << "  static constexpr bool kSkipNulls = " << (a.skip_nulls ? "true" : "false") << ";\n"
@@ -852,16 +861,16 @@ std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts
     << "  static constexpr bool kI64[" << a.n_ops << "] = {" << rp.i64 << "};\n"
     << "  // every op's exact value, out of line: 128-bit programs for ops with a\n"
        "  // 64-bit fast path, value() itself for the others\n"
-       "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx) {\n"
-       "    const Consts K = load(a);\n    const Row row = fetch(cols, idx);\n"
+       "  static __device__ __noinline__ SlowVal slow(const AggArgs& a, int j, const DCol* cols, idx_t idx, idx_t bidx) {\n"
+       "    const Consts K = load(a);\n    const Row row = fetch(cols, idx, bidx);\n"
     << rp.slow_cols << rp.slow
-    << "    unsigned fl = 0;\n    SlowVal s;\n    s.v = value(a, K, j, cols, idx, row, fl);\n"
+    << "    unsigned fl = 0;\n    SlowVal s;\n    s.v = value(a, K, j, cols, idx, bidx, row, fl);\n"
        "    s.ovf = ((fl >> (2 * j + 1)) & 1u) != 0;\n    return s;\n  }\n"
     << "  static __device__ __forceinline__ void values(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
-       "const Row& row, Val* out, unsigned& flags) {\n"
+       "idx_t bidx, const Row& row, Val* out, unsigned& flags) {\n"
     << rp.values_body << "  }\n"
     << "  static __device__ __forceinline__ Val value(const AggArgs& a, const Consts& K, int j, const DCol* cols, "
-       "idx_t idx, const Row& row, unsigned& flags) {\n"
+       "idx_t idx, idx_t bidx, const Row& row, unsigned& flags) {\n"
     << rp.value
     << "  }\n"
        "};\n"
@@ -897,7 +906,7 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   if (!gen.ok) return "";
   std::ostringstream m;
   m << "  static __device__ __forceinline__ int gid(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
-       "const Row& row) {\n"
+       "idx_t bidx, const Row& row) {\n"
     << gid << "  }\n"
     << "  static constexpr int kNW = " << nw << ";\n"
     << "  static constexpr int kWord[" << a.n_ops << "] = {" << words.str() << "};\n";
@@ -910,8 +919,10 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   return s.str();
 }
 
-std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a) {
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols) {
   Gen gen(pg, b);
+  if (n_probe_cols >= 0)
+    for (size_t s = 0; s < pg.cols.size(); ++s) gen.bside.push_back(pg.cols[s] >= n_probe_cols ? 1 : 0);
   RowParts rp = row_parts(gen, a);
   if (!rp.ok) return "";
   // FxHash of the key columns, as fx_value computes it (common.cuh): fixed
@@ -929,7 +940,7 @@ std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs
       gen.out << "    h = " << gen.V(slot) << " ? fx_word(h, (uint64_t)__double_as_longlong(static_cast<const double*>(" << c
               << ".values)[0])) : fx_word(h, 0);\n";
     else
-      gen.out << "    h = fx_value(h, cols[" << slot << "], idx);\n";
+      gen.out << "    h = fx_value(h, cols[" << slot << "], " << gen.rix(slot) << ");\n";
   }
   gen.out << "    return h;\n";
   std::string hash = gen.take();
@@ -938,15 +949,18 @@ std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs
   if (!gen.ok) return "";
   std::ostringstream m;
   m << "  static __device__ __forceinline__ uint64_t hash(const AggArgs& a, const Consts& K, const DCol* cols, idx_t idx, "
-       "const Row& row) {\n"
+       "idx_t bidx, const Row& row) {\n"
     << hash << "  }\n"
     << "  static constexpr int kW = " << a.W << ";\n"
     << "  static constexpr bool kCountRows = " << (a.count_rows ? "true" : "false") << ";\n"
     << "  static constexpr int kWord[" << a.n_ops << "] = {" << words.str() << "};\n";
   std::ostringstream s;
   s << query_row(gen, b, a, rp, m.str())
-    << "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
-       "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", prism::HASH_BLOCK>(a);\n"
+    << (n_probe_cols >= 0 ? "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 2) prism_join_agg(prism::AggArgs a) {\n"
+                              "  prism::join_body<prism::QueryRow, "
+                            : "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
+                              "  prism::hash_body<prism::QueryRow, ")
+    << a.n_ops << ", prism::HASH_BLOCK>(a);\n"
        "}\n";
   return s.str();
 }

@@ -41,7 +41,11 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
 
 // Source of the hashed-groups aggregation kernel `prism_hash_agg` (block
 // size HASH_BLOCK, dynamic shared memory (2 + a.W) * 8 << a.ss_log2 bytes).
-// Empty when the program uses a construct the generator does not cover.
-std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a);
+// With n_probe_cols >= 0, `b` is a joined batch (probe columns, then build
+// columns) and the source is the fused join -> aggregate kernel
+// `prism_join_agg` (join_body), reading build-side columns at the matched
+// build row. Empty when the program uses a construct the generator does not
+// cover.
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols = -1);
 
 }  // namespace prism

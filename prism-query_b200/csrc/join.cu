@@ -14,95 +14,21 @@
 // reference's order (probe row ascending, build rows ascending) — no second
 // read of the probe side and no post-sort.
 #include "join.hpp"
+#include "join_device.cuh"
 #include "prims.hpp"
 
 namespace prism {
 
 namespace {
 
-constexpr uint64_t EMPTY = 0x8000000000000000ULL;
+constexpr uint64_t EMPTY = JOIN_EMPTY;
 constexpr uint64_t Y_INIT = 0;  // cnt 0
-constexpr uint64_t FIB = 0x9E3779B97F4A7C15ULL;
 
 constexpr int PW = 16;             // warps per probe CTA
 constexpr int PI = 4;              // rows per lane
 constexpr int PT = PW * 32 * PI;   // rows per tile (2048)
 
-__device__ __forceinline__ uint64_t slot_of(uint64_t k, int shift) { return (k * FIB) >> shift; }
-
-// General-path row hash over the key columns; equal keys hash equal across
-// the two sides (types are checked on the host). Null rows contribute a
-// marker word only, as the reference hashes 0u8 for them (hash_join.rs:394-398).
-__device__ __forceinline__ uint64_t general_hash(const DCol* cols, int n, int64_t row) {
-  uint64_t h = 0x2545F4914F6CDD1DULL;
-  for (int i = 0; i < n; ++i) {
-    const DCol& c = cols[i];
-    uint64_t w;
-    if (!dcol_valid(c, row)) w = 0x6a09e667f3bcc909ULL;
-    else if (c.type == TY_UTF8 || c.type == TY_DICT) {
-      const uint8_t* p;
-      int32_t len;
-      dcol_str(c, row, p, len);
-      w = fx_str(0, p, len);
-    } else if (c.type == TY_F64) w = (uint64_t)__double_as_longlong(static_cast<const double*>(c.values)[row]);
-    else if (c.type == TY_F32) w = (uint64_t)__float_as_uint(static_cast<const float*>(c.values)[row]);
-    else if (c.type == TY_DEC128) {
-      const uint64_t* p = static_cast<const uint64_t*>(c.values) + 2 * row;
-      w = p[0] ^ mix64(p[1]);
-    } else w = (uint64_t)dcol_ival(c, row);
-    h = mix64(h ^ w) + FIB;
-  }
-  return h;
-}
-
-__device__ __forceinline__ bool bytes_equal(const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb) {
-  if (na != nb) return false;
-  for (int32_t i = 0; i < na; i += 8) {
-    int32_t len = na - i < 8 ? na - i : 8;
-    if (str_word(a + i, len) != str_word(b + i, len)) return false;
-  }
-  return true;
-}
-
-// keys_equal (hash_join.rs:628-670) plus the hash precondition: null flags
-// must agree and raw values must be equal; Float64 needs equal bits and `==`.
-__device__ __forceinline__ bool rows_equal(const DCol* pc, const DCol* bc, int n, int64_t pr, int64_t br) {
-  for (int i = 0; i < n; ++i) {
-    const DCol& a = pc[i];
-    const DCol& b = bc[i];
-    if (dcol_valid(a, pr) != dcol_valid(b, br)) return false;
-    switch (a.type) {
-      case TY_UTF8: case TY_DICT: {
-        const uint8_t *x, *y;
-        int32_t nx, ny;
-        dcol_str(a, pr, x, nx);
-        dcol_str(b, br, y, ny);
-        if (!bytes_equal(x, nx, y, ny)) return false;
-        break;
-      }
-      case TY_F64: {
-        double x = static_cast<const double*>(a.values)[pr], y = static_cast<const double*>(b.values)[br];
-        if (!(x == y) || __double_as_longlong(x) != __double_as_longlong(y)) return false;
-        break;
-      }
-      case TY_F32: {
-        float x = static_cast<const float*>(a.values)[pr], y = static_cast<const float*>(b.values)[br];
-        if (!(x == y) || __float_as_uint(x) != __float_as_uint(y)) return false;
-        break;
-      }
-      case TY_DEC128: {
-        const uint64_t* x = static_cast<const uint64_t*>(a.values) + 2 * pr;
-        const uint64_t* y = static_cast<const uint64_t*>(b.values) + 2 * br;
-        if (x[0] != y[0] || x[1] != y[1]) return false;
-        break;
-      }
-      case TY_NULL: break;
-      default:
-        if (dcol_ival(a, pr) != dcol_ival(b, br)) return false;
-    }
-  }
-  return true;
-}
+__device__ __forceinline__ uint64_t slot_of(uint64_t k, int shift) { return join_slot_of(k, shift); }
 
 struct KeysFast {
   static constexpr bool kFast = true;
@@ -113,10 +39,7 @@ struct KeysGeneral {
   static constexpr bool kFast = false;
   const DCol* cols;
   int n;
-  __device__ __forceinline__ uint64_t key(int64_t r) const {
-    uint64_t h = general_hash(cols, n, r);
-    return h == EMPTY ? EMPTY + 1 : h;
-  }
+  __device__ __forceinline__ uint64_t key(int64_t r) const { return join_key_hash(cols, n, r); }
 };
 
 __global__ void init_slots_kernel(ulonglong2* slots, uint64_t n) {
@@ -199,7 +122,7 @@ __global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulo
 }
 
 // ------------------------------------------------------------- the probe --
-constexpr uint32_t NO_MATCH = 0xFFFFFFFFu;
+constexpr uint32_t NO_MATCH = JOIN_NO_MATCH;
 
 struct ProbeArgs {
   int64_t n;
@@ -374,10 +297,10 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         if (!VERIFY) {
           c[it] = DUPS ? cnt : 1u;
         } else if (cnt == 1) {
-          c[it] = rows_equal(a.pcols, a.bcols, a.nkeys, r, v[it]) ? 1u : 0u;
+          c[it] = join_rows_equal(a.pcols, a.bcols, a.nkeys, r, v[it]) ? 1u : 0u;
         } else {
           uint32_t m = 0;
-          for (uint32_t j = 0; j < cnt; ++j) m += rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v[it] + j]) ? 1u : 0u;
+          for (uint32_t j = 0; j < cnt; ++j) m += join_rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v[it] + j]) ? 1u : 0u;
           c[it] = m;
         }
       }
@@ -426,7 +349,7 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         } else {
           for (uint32_t j = 0; j < cand[it]; ++j) {
             uint32_t b = a.dup_rows[v[it] + j];
-            if (VERIFY && !rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
+            if (VERIFY && !join_rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
             emit_one(a, pos++, r, b);
           }
         }

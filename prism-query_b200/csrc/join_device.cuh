@@ -1,0 +1,94 @@
+// join_device.cuh — device-side lookup of the hash join table, shared by
+// the probe kernels (join.cu) and the fused join -> aggregate kernels
+// generated at run time (agg_device.cuh, compiled with NVRTC).
+//
+// Key identity follows hash_join.rs: a single Int64 key is matched by its raw
+// value (validity ignored); any other key list by a 64-bit row hash over the
+// key columns (a null contributes a marker word, as the reference hashes 0u8
+// for it, hash_join.rs:394-398) followed by keys_equal
+// (hash_join.rs:628-670): null flags agree and raw values are equal, Float64
+// by `==` and equal bits.
+#pragma once
+
+#include "common.cuh"
+
+namespace prism {
+
+constexpr uint64_t JOIN_EMPTY = 0x8000000000000000ULL;  // empty slot (an Int64 key equal to it takes the side slot)
+constexpr uint64_t JOIN_FIB = 0x9E3779B97F4A7C15ULL;
+constexpr uint32_t JOIN_NO_MATCH = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint64_t join_slot_of(uint64_t k, int shift) { return (k * JOIN_FIB) >> shift; }
+
+// Row hash over the key columns; equal keys hash equal across the two sides
+// (types are checked on the host).
+__device__ __forceinline__ uint64_t join_key_hash(const DCol* cols, int n, int64_t row) {
+  uint64_t h = 0x2545F4914F6CDD1DULL;
+  for (int i = 0; i < n; ++i) {
+    const DCol& c = cols[i];
+    uint64_t w;
+    if (!dcol_valid(c, row)) w = 0x6a09e667f3bcc909ULL;
+    else if (c.type == TY_UTF8 || c.type == TY_DICT) {
+      const uint8_t* p;
+      int32_t len;
+      dcol_str(c, row, p, len);
+      w = fx_str(0, p, len);
+    } else if (c.type == TY_F64) w = (uint64_t)__double_as_longlong(static_cast<const double*>(c.values)[row]);
+    else if (c.type == TY_F32) w = (uint64_t)__float_as_uint(static_cast<const float*>(c.values)[row]);
+    else if (c.type == TY_DEC128) {
+      const uint64_t* p = static_cast<const uint64_t*>(c.values) + 2 * row;
+      w = p[0] ^ mix64(p[1]);
+    } else w = (uint64_t)dcol_ival(c, row);
+    h = mix64(h ^ w) + JOIN_FIB;
+  }
+  return h == JOIN_EMPTY ? JOIN_EMPTY + 1 : h;  // the empty marker stays free
+}
+
+__device__ __forceinline__ bool join_bytes_equal(const uint8_t* a, int32_t na, const uint8_t* b, int32_t nb) {
+  if (na != nb) return false;
+  for (int32_t i = 0; i < na; i += 8) {
+    int32_t len = na - i < 8 ? na - i : 8;
+    if (str_word(a + i, len) != str_word(b + i, len)) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool join_rows_equal(const DCol* pc, const DCol* bc, int n, int64_t pr, int64_t br) {
+  for (int i = 0; i < n; ++i) {
+    const DCol& a = pc[i];
+    const DCol& b = bc[i];
+    if (dcol_valid(a, pr) != dcol_valid(b, br)) return false;
+    switch (a.type) {
+      case TY_UTF8: case TY_DICT: {
+        const uint8_t *x, *y;
+        int32_t nx, ny;
+        dcol_str(a, pr, x, nx);
+        dcol_str(b, br, y, ny);
+        if (!join_bytes_equal(x, nx, y, ny)) return false;
+        break;
+      }
+      case TY_F64: {
+        double x = static_cast<const double*>(a.values)[pr], y = static_cast<const double*>(b.values)[br];
+        if (!(x == y) || __double_as_longlong(x) != __double_as_longlong(y)) return false;
+        break;
+      }
+      case TY_F32: {
+        float x = static_cast<const float*>(a.values)[pr], y = static_cast<const float*>(b.values)[br];
+        if (!(x == y) || __float_as_uint(x) != __float_as_uint(y)) return false;
+        break;
+      }
+      case TY_DEC128: {
+        const uint64_t* x = static_cast<const uint64_t*>(a.values) + 2 * pr;
+        const uint64_t* y = static_cast<const uint64_t*>(b.values) + 2 * br;
+        if (x[0] != y[0] || x[1] != y[1]) return false;
+        break;
+      }
+      case TY_NULL: break;
+      default:
+        if (dcol_ival(a, pr) != dcol_ival(b, br)) return false;
+    }
+  }
+  return true;
+}
+
+}  // namespace prism
