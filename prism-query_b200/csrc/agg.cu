@@ -1052,9 +1052,9 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
   if (!dense && P.n_distinct == 0 && A.n_ops >= 1 && A.n_ops <= 8 && tiny_fits_registers(A) && jit_enabled()) {
     // a fused join waits on dependent loads per row: a smaller table (half
     // a block's share of the SM) keeps two blocks resident per SM
-    const size_t hbudget = join ? (size_t)smem_optin / 2 - TINY_MAX_COLS * sizeof(DCol) - 1024
+    const size_t hbudget = join ? (size_t)smem_optin / std::max(1, tune.join_min_blocks) - TINY_MAX_COLS * sizeof(DCol) - 1024
                                 : (size_t)smem_optin - TINY_MAX_COLS * sizeof(DCol) - 1024;
-    for (int l = join ? 10 : 12; l >= 8; --l) {
+    for (int l = join ? tune.join_table_log2 : 12; l >= 8; --l) {
       if ((1 << l) > 2 * std::max(128, tune.smem_groups)) continue;
       if (((size_t)(2 + W) * 8 << l) <= hbudget) {
         hss_log2 = l;
@@ -1173,7 +1173,11 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.jnkeys = (int)join->probe_keys.size();
         a.n_cols = (int)pg.cols.size();
         if (A.wide) fused_fail("a Float64 sum beyond the 192-bit window over a join");
-        std::string src = jit_hash_agg_source(pg, b, a, n_probe_cols);
+        JoinKernelShape shape;
+        shape.block = tune.join_block;
+        shape.min_blocks = tune.join_min_blocks;
+        shape.rows = tune.join_rows;
+        std::string src = jit_hash_agg_source(pg, b, a, n_probe_cols, shape);
         if (src.empty()) fused_fail("this projection over a join");
         hk = jit_get(src, "prism_join_agg");
       } else if (!jk && hss_log2 && !A.wide) {
@@ -1185,12 +1189,13 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.ss_log2 = hss_log2;
         PRISM_CUDA(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
         int per_sm = 0;
-        PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, HASH_BLOCK, hsmem));
-        int hgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)HASH_BLOCK * TINY_R * 4),
+        const int hblock = join ? tune.join_block : HASH_BLOCK;
+        PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, hblock, hsmem));
+        int hgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)hblock * TINY_R * 4),
                                            (int64_t)ctx.sm_count * std::max(1, per_sm));
         void* params[] = {&a};
         KernelTimer kt(ctx, join ? "join_agg_jit" : "agg_hash_jit");
-        PRISM_CUDA(cudaLaunchKernel(hk, dim3(hgrid), dim3(HASH_BLOCK), params, hsmem, ctx.stream));
+        PRISM_CUDA(cudaLaunchKernel(hk, dim3(hgrid), dim3(hblock), params, hsmem, ctx.stream));
       } else if (jk) {
         a.n_cols = (int)pg.cols.size();
         const int words = (int)(G + 1) * tiny_group_words(A), tblock = tiny_block(words);

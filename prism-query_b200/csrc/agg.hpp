@@ -11,6 +11,13 @@ struct AggTuning {
   int block = 512;
   int smem_groups = 1024;   // dense accumulator rows per CTA (hash mode)
   int blocks_per_sm = 1;
+  // fused join -> aggregate kernel shape: 3 blocks of 512 threads per SM
+  // (40 registers) and a block table of at most 512 slots, which leaves
+  // most of the SM's 228 KB to L1 for the skewed build-side reads
+  int join_block = 512;
+  int join_min_blocks = 3;
+  int join_rows = 2;
+  int join_table_log2 = 9;
 };
 
 struct JoinTable;

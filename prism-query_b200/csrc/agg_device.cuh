@@ -668,16 +668,16 @@ __device__ __forceinline__ void hash_body(const AggArgs& a) {
   hash_table_merge<E>(a, t, tid, BLOCK);
 }
 
-// The fused join -> aggregate body: one probe row per thread and step
-// (JOIN_R rows in flight), its key looked up in the build table as the probe
-// kernels do (join_device.cuh), and every matched build row, in ascending
-// order, aggregated as the joined row (probe row, build row) into the
-// block's table. The order key of a joined row is
+// The fused join -> aggregate body: R probe rows per thread and step, their
+// keys looked up in the build table as the probe kernels do
+// (join_device.cuh) with all R lookups in flight together, then for every
+// row with one candidate its joined row's fixed-width columns fetched (again
+// R at once) before the keys are compared; every matched build row, in
+// ascending order, is aggregated as the joined row (probe row, build row)
+// into the block's table. The order key of a joined row is
 // (global probe row << 32 | build row), which sorts like the joined rows'
 // positions (probe rows ascending, build rows ascending inside one).
-constexpr int JOIN_R = 2;
-
-template <class E, int NOPS, int BLOCK>
+template <class E, int NOPS, int BLOCK, int R>
 __device__ __forceinline__ void join_body(const AggArgs& a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ DCol scols[TINY_MAX_COLS];
@@ -692,58 +692,68 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
   const I stride = (I)gridDim.x * BLOCK;
   const I n = (I)a.n;
   bool err = false;
-  for (I base = (I)blockIdx.x * BLOCK + tid; base < n; base += stride * JOIN_R) {
-    // the build candidates of JOIN_R probe rows (their lookups in flight together)
-    uint32_t cand[JOIN_R], cnt[JOIN_R];
+  for (I base = (I)blockIdx.x * BLOCK + tid; base < n; base += stride * R) {
+    uint32_t cand[R], cnt[R];
+    uint64_t key[R];
+    ulonglong2 e[R];
+    uint64_t s[R];
 #pragma unroll
-    for (int r = 0; r < JOIN_R; ++r) {
+    for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
-      cand[r] = JOIN_NO_MATCH;
       cnt[r] = 0;
-      if (idx >= n) continue;
-      if (a.jfast) {
-        const uint64_t key = (uint64_t)static_cast<const int64_t*>(a.jpk[0].values)[idx];
-        if (a.jdense) {
-          const uint64_t d = key - (uint64_t)a.jdmin;
-          const uint32_t row = d < a.jdrange ? __ldg(a.jdense + d) : JOIN_NO_MATCH;
-          if (row != JOIN_NO_MATCH) {
-            cand[r] = row;
-            cnt[r] = 1;
-          }
-          continue;
+      cand[r] = JOIN_NO_MATCH;
+      key[r] = 0;
+      if (idx < n)
+        key[r] = a.jfast ? (uint64_t)static_cast<const int64_t*>(a.jpk[0].values)[idx]
+                         : join_key_hash(a.jpk, a.jnkeys, idx);
+    }
+    if (a.jdense) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        const uint64_t d = key[r] - (uint64_t)a.jdmin;
+        const uint32_t row = (idx < n && d < a.jdrange) ? __ldg(a.jdense + d) : JOIN_NO_MATCH;
+        if (row != JOIN_NO_MATCH) {
+          cand[r] = row;
+          cnt[r] = 1;
         }
-        uint64_t s = key == JOIN_EMPTY ? a.jcap : join_slot_of(key, a.jshift);
-        ulonglong2 e = __ldg(a.jslots + s);
-        for (uint64_t steps = 0; e.x != key && e.x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
-          s = (s + 1) & a.jmask;
-          e = __ldg(a.jslots + s);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        s[r] = (a.jfast && key[r] == JOIN_EMPTY) ? a.jcap : join_slot_of(key[r], a.jshift);
+        e[r] = idx < n ? __ldg(a.jslots + s[r]) : make_ulonglong2(JOIN_EMPTY, 0);
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        if (idx >= n) continue;
+        for (uint64_t steps = 0; e[r].x != key[r] && e[r].x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
+          s[r] = (s[r] + 1) & a.jmask;
+          e[r] = __ldg(a.jslots + s[r]);
         }
-        if (e.x == key) {
-          cand[r] = (uint32_t)e.y;
-          cnt[r] = (uint32_t)(e.y >> 32);
-        }
-      } else {
-        const uint64_t key = join_key_hash(a.jpk, a.jnkeys, idx);
-        uint64_t s = join_slot_of(key, a.jshift);
-        ulonglong2 e = __ldg(a.jslots + s);
-        for (uint64_t steps = 0; e.x != key && e.x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
-          s = (s + 1) & a.jmask;
-          e = __ldg(a.jslots + s);
-        }
-        if (e.x == key) {
-          cand[r] = (uint32_t)e.y;
-          cnt[r] = (uint32_t)(e.y >> 32);
+        if (e[r].x == key[r]) {
+          cand[r] = (uint32_t)e[r].y;
+          cnt[r] = (uint32_t)(e[r].y >> 32);
         }
       }
     }
+    // single-candidate rows: the joined rows' columns, all R in flight
+    typename E::Row rows[R];
 #pragma unroll
-    for (int r = 0; r < JOIN_R; ++r) {
+    for (int r = 0; r < R; ++r) {
+      const I idx = base + r * stride;
+      if (cnt[r] == 1) rows[r] = E::fetch(cols, idx, (I)cand[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
       for (uint32_t j = 0; j < cnt[r]; ++j) {
         const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
         if (!a.jfast && !join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b)) continue;
         const I bidx = (I)b;
-        const typename E::Row row = E::fetch(cols, idx, bidx);
+        const typename E::Row row = cnt[r] == 1 ? rows[r] : E::fetch(cols, idx, bidx);
         if (!E::keep(a, K, cols, idx, bidx, row)) continue;
         const uint64_t h = E::hash(a, K, cols, idx, bidx, row);
         unsigned flags = 0;

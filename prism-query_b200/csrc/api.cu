@@ -3,6 +3,7 @@
 // Every entry point catches failures and returns a status code (the library
 // never aborts); the message is kept on the context for prism_last_error().
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <functional>
 
@@ -62,7 +63,22 @@ JoinTuning join_tuning() {
   if (d && std::strcmp(d, "0") == 0) t.dense = false;
   return t;
 }
-AggTuning agg_tuning() { return AggTuning{}; }
+// PRISM_JOIN_AGG_SHAPE=block,min_blocks,rows,table_log2 sets the fused join
+// -> aggregate kernel's shape (block 128-1024 in powers of two, min_blocks
+// 1-8, rows 1, 2, 4 or 8, block table of at most 2^table_log2 slots, 8-12)
+AggTuning agg_tuning() {
+  AggTuning t{};
+  const char* d = std::getenv("PRISM_JOIN_AGG_SHAPE");
+  int b = 0, m = 0, r = 0, l = 0;
+  if (d && std::sscanf(d, "%d,%d,%d,%d", &b, &m, &r, &l) == 4 && (b == 128 || b == 256 || b == 512 || b == 1024) &&
+      m >= 1 && m <= 8 && (r == 1 || r == 2 || r == 4 || r == 8) && l >= 8 && l <= 12) {
+    t.join_block = b;
+    t.join_min_blocks = m;
+    t.join_rows = r;
+    t.join_table_log2 = l;
+  }
+  return t;
+}
 
 // PRISM_JOIN_AGG_FUSED=0 materializes the joined rows before aggregating
 bool join_agg_fused() {

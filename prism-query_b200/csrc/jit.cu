@@ -878,6 +878,18 @@ std::string query_row(Gen& gen, const Batch& b, const AggArgs& a, const RowParts
   return s.str();
 }
 
+std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKernelShape& join) {
+  std::ostringstream k;
+  if (n_probe_cols >= 0)
+    k << "extern \"C\" __global__ void __launch_bounds__(" << join.block << ", " << join.min_blocks
+      << ") prism_join_agg(prism::AggArgs a) {\n  prism::join_body<prism::QueryRow, " << a.n_ops << ", " << join.block
+      << ", " << join.rows << ">(a);\n}\n";
+  else
+    k << "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
+         "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", prism::HASH_BLOCK>(a);\n}\n";
+  return k.str();
+}
+
 }  // namespace
 
 std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64) {
@@ -919,7 +931,8 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
   return s.str();
 }
 
-std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols) {
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols,
+                                const JoinKernelShape& join) {
   Gen gen(pg, b);
   if (n_probe_cols >= 0)
     for (size_t s = 0; s < pg.cols.size(); ++s) gen.bside.push_back(pg.cols[s] >= n_probe_cols ? 1 : 0);
@@ -956,12 +969,7 @@ std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs
     << "  static constexpr int kWord[" << a.n_ops << "] = {" << words.str() << "};\n";
   std::ostringstream s;
   s << query_row(gen, b, a, rp, m.str())
-    << (n_probe_cols >= 0 ? "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 2) prism_join_agg(prism::AggArgs a) {\n"
-                              "  prism::join_body<prism::QueryRow, "
-                            : "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
-                              "  prism::hash_body<prism::QueryRow, ")
-    << a.n_ops << ", prism::HASH_BLOCK>(a);\n"
-       "}\n";
+    << query_row_kernel(a, n_probe_cols, join);
   return s.str();
 }
 

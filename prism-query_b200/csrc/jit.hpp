@@ -46,6 +46,12 @@ std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs
 // `prism_join_agg` (join_body), reading build-side columns at the matched
 // build row. Empty when the program uses a construct the generator does not
 // cover.
-std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols = -1);
+struct JoinKernelShape {
+  int block = 512;      // threads per block
+  int min_blocks = 3;   // blocks kept resident per SM (bounds registers and shared memory)
+  int rows = 2;         // probe rows per thread in flight
+};
+std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols = -1,
+                                const JoinKernelShape& join = JoinKernelShape{});
 
 }  // namespace prism
