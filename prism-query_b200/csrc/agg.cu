@@ -1182,14 +1182,16 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         hk = jit_get(src, "prism_join_agg");
       } else if (!jk && hss_log2 && !A.wide) {
         a.n_cols = (int)pg.cols.size();
-        std::string src = jit_hash_agg_source(pg, b, a);
+        JoinKernelShape shape;
+        shape.hash_block = tune.hash_block;
+        std::string src = jit_hash_agg_source(pg, b, a, -1, shape);
         if (!src.empty()) hk = jit_get(src, "prism_hash_agg");
       }
       if (hk) {
         a.ss_log2 = hss_log2;
         PRISM_CUDA(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
         int per_sm = 0;
-        const int hblock = join ? tune.join_block : HASH_BLOCK;
+        const int hblock = join ? tune.join_block : tune.hash_block;
         PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hk, hblock, hsmem));
         int hgrid = (int)std::min<int64_t>(ceil_div(b.rows, (int64_t)hblock * TINY_R * 4),
                                            (int64_t)ctx.sm_count * std::max(1, per_sm));

@@ -18,6 +18,7 @@ struct AggTuning {
   int join_min_blocks = 3;
   int join_rows = 2;
   int join_table_log2 = 9;
+  int hash_block = 1024;  // threads per block of the hashed-groups kernel (1024: 0.068 ms vs 0.080 at 512 on 1M rows x 1,024 groups)
 };
 
 struct JoinTable;

@@ -486,7 +486,6 @@ __device__ __forceinline__ void tiny_body(const AggArgs& a) {
 // kCountRows; initial values and merge kinds of the words are a.winit and
 // a.wkind.
 constexpr int HASH_PROBES = 32;
-constexpr int HASH_BLOCK = 512;
 
 template <class E, int NOPS, bool FAST>
 __device__ __forceinline__ void hash_accumulate(const AggArgs& a, unsigned long long* acc, const Val* v) {

@@ -77,6 +77,9 @@ AggTuning agg_tuning() {
     t.join_rows = r;
     t.join_table_log2 = l;
   }
+  // PRISM_HASH_AGG_BLOCK=256|512|1024: threads per block of the hashed-groups kernel
+  const char* hb = std::getenv("PRISM_HASH_AGG_BLOCK");
+  if (hb && (std::atoi(hb) == 256 || std::atoi(hb) == 512 || std::atoi(hb) == 1024)) t.hash_block = std::atoi(hb);
   return t;
 }
 

@@ -885,8 +885,8 @@ std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKerne
       << ") prism_join_agg(prism::AggArgs a) {\n  prism::join_body<prism::QueryRow, " << a.n_ops << ", " << join.block
       << ", " << join.rows << ">(a);\n}\n";
   else
-    k << "extern \"C\" __global__ void __launch_bounds__(prism::HASH_BLOCK, 1) prism_hash_agg(prism::AggArgs a) {\n"
-         "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", prism::HASH_BLOCK>(a);\n}\n";
+    k << "extern \"C\" __global__ void __launch_bounds__(" << join.hash_block << ", 1) prism_hash_agg(prism::AggArgs a) {\n"
+         "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", " << join.hash_block << ">(a);\n}\n";
   return k.str();
 }
 

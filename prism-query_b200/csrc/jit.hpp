@@ -40,16 +40,18 @@ void jit_stats(int64_t* compiles, double* ms);
 std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64);
 
 // Source of the hashed-groups aggregation kernel `prism_hash_agg` (block
-// size HASH_BLOCK, dynamic shared memory (2 + a.W) * 8 << a.ss_log2 bytes).
+// size JoinKernelShape::hash_block, dynamic shared memory (2 + a.W) * 8 << a.ss_log2 bytes).
 // With n_probe_cols >= 0, `b` is a joined batch (probe columns, then build
 // columns) and the source is the fused join -> aggregate kernel
 // `prism_join_agg` (join_body), reading build-side columns at the matched
 // build row. Empty when the program uses a construct the generator does not
 // cover.
+constexpr int HASH_BLOCK_DEFAULT = 1024;
 struct JoinKernelShape {
   int block = 512;      // threads per block
   int min_blocks = 3;   // blocks kept resident per SM (bounds registers and shared memory)
   int rows = 2;         // probe rows per thread in flight
+  int hash_block = HASH_BLOCK_DEFAULT;  // threads per block of the hashed-groups kernel (no join)
 };
 std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols = -1,
                                 const JoinKernelShape& join = JoinKernelShape{});
