@@ -8,6 +8,8 @@ over a slice of device-resident rows). The server
   (blocking admission on a byte counter);
 * runs requests concurrently: each worker thread owns a context whose CUDA
   stream is its own, and the C ABI releases the GIL while the GPU works;
+* hands the smallest ready job to the next free worker (shortest job
+  first), so a burst of small requests is not queued behind a large one;
 * coalesces small requests that arrive close together into one launch: small
   probes of one table are concatenated and probed once (each request's
   matches are the range of the output whose probe rows fall in its span —
@@ -97,7 +99,9 @@ class Server:
         self.tables: Dict[str, _Table] = {}
         self._cv = threading.Condition()
         self._inbox: "queue.Queue" = queue.Queue()
-        self._jobs: "queue.Queue" = queue.Queue()
+        self._jobs: "queue.PriorityQueue" = queue.PriorityQueue()  # (rows, seq, job); smallest first
+        self._seq = 0
+        self._seq_lock = threading.Lock()
         self._closed = False
         self._ctxs = []
         self._threads = []
@@ -126,9 +130,16 @@ class Server:
         self._inbox.put(None)
         self._disp.join()
         for _ in self._threads:
-            self._jobs.put(None)
+            self._put(None)
         for t in self._threads:
             t.join()
+
+    def _put(self, job: Optional[_Job]):
+        """Queues a job by its row count (a closing sentinel after every job)."""
+        with self._seq_lock:
+            self._seq += 1
+            seq = self._seq
+        self._jobs.put((float("inf") if job is None else job.rows, seq, job))
 
     # -------------------------------------------------------- dispatcher --
     @staticmethod
@@ -149,14 +160,14 @@ class Server:
                 item = "flush"
             if item is None:
                 for j in pending.values():
-                    self._jobs.put(j)
+                    self._put(j)
                 return
             if item != "flush":
                 req, fut = item
                 n = self._rows(req)
                 kind = "probe" if isinstance(req, ProbeRequest) else "agg"
                 if n >= self.coalesce_rows:
-                    self._jobs.put(_Job([req], [fut], kind, n))
+                    self._put(_Job([req], [fut], kind, n))
                     continue
                 k = self._key(req)
                 j = pending.get(k)
@@ -168,12 +179,12 @@ class Server:
                     j.rows += n
                 j = pending[k]
                 if j.rows >= self.coalesce_rows or len(j.reqs) >= self.max_coalesce:
-                    self._jobs.put(pending.pop(k))
+                    self._put(pending.pop(k))
                 if not self._inbox.empty():
                     continue
             # nothing more waiting: hand over what is pending
             for k in list(pending):
-                self._jobs.put(pending.pop(k))
+                self._put(pending.pop(k))
 
     # ------------------------------------------------------------ worker --
     def _admit(self, nbytes: int):
@@ -190,7 +201,7 @@ class Server:
     def _worker(self, ctx, stream):
         torch = self.torch
         while True:
-            job = self._jobs.get()
+            job = self._jobs.get()[2]
             if job is None:
                 return
             nbytes = _footprint(job)
