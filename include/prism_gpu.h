@@ -24,7 +24,11 @@
  *      exported with prism_batch_export). Operators chain on the device with
  *      no host round trip; build-side hash tables stay resident across probes
  *      (the analogue of the reference's PartitionStore,
- *      native/prism-flight/src/shuffle_writer.rs:42-86).
+ *      native/prism-flight/src/shuffle_writer.rs:42-86). A resident result may
+ *      still be in flight when the call returns: it is ordered on the
+ *      context's stream, so calls on the same context and prism_batch_export
+ *      see it complete; other streams or host readers of its device buffers
+ *      call prism_ctx_synchronize first.
  *
  * Tree-shaped configuration (Predicate, ScalarExpr) crosses as flat arrays of
  * POD nodes in post-order (children before parent).

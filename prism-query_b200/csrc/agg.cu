@@ -1383,7 +1383,8 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
       finalize_kernel<<<grid_for(ctx, G_out, 128), 128, 0, ctx.stream>>>(F);
       ctx.check_launch("finalize_kernel");
     }
-    ctx.sync();
+    // the result is stream-ordered: the export (or the caller's next call on
+    // this context) waits for it, so no synchronisation here
     return out;
   }
   fail(PRISM_ERR_TABLE_FULL, "aggregation table could not be sized");

@@ -4,6 +4,8 @@
 #include <cstdlib>
 #include <string>
 
+#include <map>
+#include <mutex>
 #include "arrow_io.hpp"
 
 namespace prism {
@@ -218,9 +220,70 @@ struct Importer {
 };
 
 // ------------------------------------------------------------------ export --
+// Exported buffers are page-locked host memory from a process-wide pool: a
+// device-to-host copy into pinned memory runs asynchronously at the link's
+// full rate, where pageable memory is staged through a driver buffer. Pinning
+// costs a system call per allocation, so buffers are recycled: an exported
+// array returns its buffers to the pool when the consumer releases it. At
+// most kPinnedCached bytes stay cached; small buffers use malloc.
+class PinnedPool {
+ public:
+  static constexpr size_t kPinnedCached = (size_t)8 << 30;
+  static constexpr size_t kPinnedMin = (size_t)64 << 10;
+  // a pinned buffer of at least `bytes` (its size in *size), or nullptr
+  void* get(size_t bytes, size_t* size) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first <= 2 * bytes) {
+        void* p = it->second;
+        *size = it->first;
+        cached_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    size_t sz = (bytes + ((size_t)1 << 16) - 1) & ~(((size_t)1 << 16) - 1);
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();  // not sticky: fall back to pageable memory
+      return nullptr;
+    }
+    *size = sz;
+    return p;
+  }
+  void put(void* p, size_t size) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (cached_ + size <= kPinnedCached) {
+        free_.emplace(size, p);
+        cached_ += size;
+        return;
+      }
+    }
+    cudaFreeHost(p);
+  }
+
+ private:
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  size_t cached_ = 0;
+};
+
+// never destroyed: exported arrays may be released at any time before exit
+PinnedPool& pinned_pool() {
+  static PinnedPool* pool = new PinnedPool();
+  return *pool;
+}
+
 struct HostBuf {
   void* p = nullptr;
-  ~HostBuf() { free(p); }
+  size_t size = 0;
+  bool pinned = false;
+  ~HostBuf() {
+    if (pinned) pinned_pool().put(p, size);
+    else free(p);
+  }
 };
 struct SchemaPriv {
   std::string format, name;
@@ -307,7 +370,11 @@ struct Exporter {
 
   std::shared_ptr<HostBuf> host(size_t bytes) {
     auto h = std::make_shared<HostBuf>();
-    h->p = malloc(bytes + 16);
+    if (bytes + 16 >= PinnedPool::kPinnedMin) {
+      h->p = pinned_pool().get(bytes + 16, &h->size);
+      h->pinned = h->p != nullptr;
+    }
+    if (!h->p) h->p = malloc(bytes + 16);
     if (!h->p) fail(PRISM_ERR_NO_MEMORY, "host allocation failed");
     return h;
   }
