@@ -907,7 +907,8 @@ def run_c5(args, rank, world, local, torch, dist):
             tn = f"t{int(rng.integers(0, 8))}"
             r = S.ProbeRequest(tn, kpools[tn][off:off + rows], arrival=t)
         reqs.append(r)
-    total_rows = sum(S.Server._rows(r) for r in reqs)
+    total_rows = sum(int(r.keys.numel()) if isinstance(r, S.ProbeRequest) else int(r.columns[0][2].numel())
+                     for r in reqs)
     torch.cuda.synchronize()
     # warm-up: both paths on a few requests (allocator pools, kernel images)
     warm = [S.ProbeRequest(r.table, r.keys) if isinstance(r, S.ProbeRequest) else S.AggRequest(r.columns, r.config)

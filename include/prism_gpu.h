@@ -408,6 +408,53 @@ int prism_join_aggregate(prism_ctx* ctx, const prism_batch* const* probes, int32
                          const prism_agg_config* agg, prism_batch** out);
 
 /* ------------------------------------------------------------------------ */
+/* Serving loop (prism_serve_submit/poll of the design)                       */
+/* ------------------------------------------------------------------------ */
+/* Requests of uneven sizes against resident tables, answered by worker
+ * threads that each own a context and stream: small requests of one shape
+ * that arrive close together share a launch, the smallest ready job goes to
+ * the next free worker, and a job starts only while its device footprint
+ * fits the budget. Every result equals the result of the request run alone.
+ * No counterpart in the reference (its Flight handler runs one operator call
+ * at a time, prism-flight/src/handler.rs; PartitionStore,
+ * shuffle_writer.rs:42-86, is the resident-table analogue).
+ *
+ * Lifetimes: tables, request batches and key buffers stay owned by the
+ * caller and must outlive their requests; result batches belong to the
+ * caller and must be freed (prism_batch_free) before prism_server_destroy.
+ * Key buffers and request batches must be complete on the device when
+ * submitted. Results are complete when poll returns them. */
+typedef struct prism_server prism_server;
+
+/* workers: 1-64 worker threads; budget_bytes: device bytes admitted jobs may
+ * hold at once (0 = 120 GB); requests below coalesce_rows rows may share a
+ * launch with up to max_coalesce - 1 others. */
+int prism_server_create(int32_t device, uint64_t budget_bytes, int32_t workers, int64_t coalesce_rows,
+                        int32_t max_coalesce, prism_server** out);
+/* Registers a resident table (single Int64 key); probes emit
+ * (probe row, build column payload_col). */
+int prism_server_add_table(prism_server* server, const prism_hash_table* table, int32_t payload_col,
+                           int32_t* table_id);
+/* Submits a probe of table_id with n device-resident Int64 keys; the result
+ * batch is [probe_idx (UInt32, rows of `keys`, ascending), payload]. */
+int prism_serve_probe(prism_server* server, int32_t table_id, const int64_t* keys, int64_t n, int64_t* ticket);
+/* Submits hash_aggregate(batch, config) (the config is copied). */
+int prism_serve_aggregate(prism_server* server, const prism_batch* batch, const prism_agg_config* config,
+                          int64_t* ticket);
+/* Waits up to wait_ms (-1: until done, 0: no wait) for a ticket. Returns
+ * PRISM_OK with the result in *out, the request's own error status (message
+ * in prism_server_last_error), or PRISM_ERR_TIMEOUT while it is not done.
+ * A ticket's result is returned once; poll one ticket from one thread. */
+int prism_serve_poll(prism_server* server, int64_t ticket, int32_t wait_ms, prism_batch** out);
+/* Waits up to wait_ms (-1: until one is) for a finished ticket not yet
+ * reported by this call, in completion order; PRISM_ERR_TIMEOUT when none.
+ * (Its result is then taken with prism_serve_poll.) */
+int prism_serve_wait_any(prism_server* server, int32_t wait_ms, int64_t* ticket);
+const char* prism_server_last_error(prism_server* server);
+/* Finishes every submitted request, then stops the workers. */
+void prism_server_destroy(prism_server* server);
+
+/* ------------------------------------------------------------------------ */
 /* Arrow-style wrappers: host batches in, host batch out                     */
 /* ------------------------------------------------------------------------ */
 int prism_hash_join_arrow(prism_ctx* ctx, const struct ArrowArray* probe,

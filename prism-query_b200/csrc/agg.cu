@@ -626,8 +626,6 @@ struct Plan {
   int n_distinct = 0;
 };
 
-ColP concat_columns(Ctx& ctx, const std::vector<const Column*>& parts);
-
 }  // namespace
 
 static __global__ void concat_bits_kernel(const uint8_t* src, int64_t n, int64_t dst_off, uint32_t* dst) {
@@ -645,8 +643,7 @@ static __global__ void concat_offsets_kernel(const int32_t* src, int64_t n, int3
     dst[i] = (int32_t)(src[i] - base + dst_data_off);
 }
 
-namespace {
-
+// Concatenation of one column's parts (same type) into a new column.
 ColP concat_columns(Ctx& ctx, const std::vector<const Column*>& parts) {
   const Column& f = *parts[0];
   int64_t n = 0, bytes = 0;
@@ -700,6 +697,8 @@ ColP concat_columns(Ctx& ctx, const std::vector<const Column*>& parts) {
   }
   return out;
 }
+
+namespace {
 
 int result_type(int func) {
   return (func == PRISM_AGG_COUNT || func == PRISM_AGG_COUNT_DISTINCT) ? TY_I64 : TY_F64;

@@ -36,4 +36,8 @@ void scatter_bits(Ctx& ctx, const uint32_t* idx, int64_t n, uint8_t* bitmap);
 // Device column that repeats a null-free fixed-width value (index arrays).
 ColP u32_column(Ctx& ctx, const std::string& name, MemP mem, uint32_t* ptr, int64_t n);
 
+// The parts of one column (same type; Utf8, dictionary indices, fixed width,
+// validity) concatenated into a new column (agg.cu).
+ColP concat_columns(Ctx& ctx, const std::vector<const Column*>& parts);
+
 }  // namespace prism

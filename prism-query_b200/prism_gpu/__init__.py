@@ -106,6 +106,16 @@ def _declare(lib):
     lib.prism_project_batch_with_exprs.argtypes = [P, P, P, i32, P, i32, i32, C.POINTER(P)]
     lib.prism_filter_project_aggregate.argtypes = [P, P, i32, P, P, i32, P, i32, i32, P, C.POINTER(P)]
     lib.prism_join_aggregate.argtypes = [P, P, i32, P, P, P, i32, P, i32, P, i32, P, C.POINTER(P)]
+    lib.prism_server_create.argtypes = [i32, C.c_uint64, i32, C.c_int64, i32, C.POINTER(P)]
+    lib.prism_server_add_table.argtypes = [P, P, i32, C.POINTER(i32)]
+    lib.prism_serve_probe.argtypes = [P, i32, P, C.c_int64, C.POINTER(C.c_int64)]
+    lib.prism_serve_aggregate.argtypes = [P, P, P, C.POINTER(C.c_int64)]
+    lib.prism_serve_poll.argtypes = [P, C.c_int64, i32, C.POINTER(P)]
+    lib.prism_serve_wait_any.argtypes = [P, i32, C.POINTER(C.c_int64)]
+    lib.prism_server_last_error.argtypes = [P]
+    lib.prism_server_last_error.restype = C.c_char_p
+    lib.prism_server_destroy.argtypes = [P]
+    lib.prism_server_destroy.restype = None
     lib.prism_hash_join_arrow.argtypes = [P, P, P, P, P, P, P, P]
     lib.prism_hash_aggregate_arrow.argtypes = [P, P, P, P, P, P]
     lib.prism_filter_and_project_arrow.argtypes = [P, P, P, P, P, i32, P, P]

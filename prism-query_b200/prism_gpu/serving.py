@@ -1,24 +1,16 @@
 """Serving loop: operator requests of uneven sizes against resident tables.
 
-Requests arrive one by one (a probe of a resident hash table, or a GROUP BY
-over a slice of device-resident rows). The server
-
-* keeps the build-side tables resident (built once, shared by every worker);
-* admits a request only while its device-memory footprint fits the budget
-  (blocking admission on a byte counter);
-* runs requests concurrently: each worker thread owns a context whose CUDA
-  stream is its own, and the C ABI releases the GIL while the GPU works;
-* hands the smallest ready job to the next free worker (shortest job
-  first), so a burst of small requests is not queued behind a large one;
-* coalesces small requests that arrive close together into one launch: small
-  probes of one table are concatenated and probed once (each request's
-  matches are the range of the output whose probe rows fall in its span —
-  the output is in probe-row order); small aggregations with one config are
-  concatenated with a segment-id column added as the first group key, so one
-  aggregation computes every request's groups, split afterwards. Every
-  request's result equals the result of running it alone: the matches are
-  identical and the aggregation is exact and order-independent, its groups
-  in the same first-seen order.
+A thin Python face of the native serving loop (prism_server_* /
+prism_serve_* in include/prism_gpu.h, csrc/serve.cu): requests (a probe of a
+resident hash table with device-resident int64 keys, or a GROUP BY over
+device-resident columns) are submitted from any thread and answered through
+futures. The native server keeps the tables resident, runs jobs on worker
+threads that each own a context and CUDA stream, admits a job only while its
+device footprint fits the budget, hands the smallest ready job to the next
+free worker, and coalesces small requests of one shape that arrive close
+together into one launch (probes of one table concatenated and cut apart by
+probe row; GROUP BYs concatenated with a segment id as the first group key).
+Every result equals the result of running the request alone.
 
 This has no counterpart in the reference (its operators are called one at a
 time by the Flight handler, native/prism-flight/src/handler.rs).
@@ -26,7 +18,6 @@ time by the Flight handler, native/prism-flight/src/handler.rs).
 from __future__ import annotations
 
 import concurrent.futures as cf
-import queue
 import threading
 import time
 from dataclasses import dataclass, field
@@ -62,224 +53,118 @@ class ProbeResult:
 
 
 @dataclass
-class _Job:
-    reqs: List
-    futs: List
-    kind: str
-    rows: int
-
-
-@dataclass
 class _Table:
     table: object        # prism_gpu.HashTable
     payload_col: int     # joined-schema column of the build payload
 
 
-def _footprint(job: _Job) -> int:
-    """Device bytes a job may hold at once: staging copy + probe words + output
-    (probe) or staging + segment ids + group tables (aggregation)."""
-    if job.kind == "probe":
-        return job.rows * (8 + 4 + 12) + (1 << 20)
-    return job.rows * (8 * 3 + 4) + (64 << 20)
-
-
 class Server:
     def __init__(self, device: int = 0, budget_bytes: int = 120 << 30, workers: int = 4,
                  coalesce_rows: int = 1 << 18, max_coalesce: int = 64):
+        import ctypes as C
+
         import torch
 
-        from . import Context
+        from . import Context, lib
 
         self.torch = torch
         self.device = device
-        self.budget = budget_bytes
-        self.in_use = 0
-        self.coalesce_rows = coalesce_rows
-        self.max_coalesce = max_coalesce
-        self.tables: Dict[str, _Table] = {}
-        self._cv = threading.Condition()
-        self._inbox: "queue.Queue" = queue.Queue()
-        self._jobs: "queue.PriorityQueue" = queue.PriorityQueue()  # (rows, seq, job); smallest first
-        self._seq = 0
-        self._seq_lock = threading.Lock()
+        self._C = C
+        self._lib = lib()
+        self._ctx = Context(device)  # imports request batches and exports results
+        self._h = C.c_void_p()
+        rc = self._lib.prism_server_create(device, budget_bytes, workers, coalesce_rows, max_coalesce, C.byref(self._h))
+        if rc:
+            self._raise(rc)
+        self.tables: Dict[str, int] = {}
+        self._lock = threading.Lock()
+        self._pending: Dict[int, tuple] = {}  # ticket -> (future, request, keepalive)
         self._closed = False
-        self._ctxs = []
-        self._threads = []
-        for w in range(workers):
-            ctx = Context(device)
-            stream = torch.cuda.Stream(device=device)
-            ctx.set_stream(stream.cuda_stream)
-            self._ctxs.append((ctx, stream))
-            t = threading.Thread(target=self._worker, args=(ctx, stream), daemon=True)
-            t.start()
-            self._threads.append(t)
-        self._disp = threading.Thread(target=self._dispatch, daemon=True)
-        self._disp.start()
+        self._poller = threading.Thread(target=self._poll, daemon=True)
+        self._poller.start()
+
+    def _raise(self, rc: int):
+        from . import PrismError
+
+        msg = self._lib.prism_server_last_error(self._h) if self._h else b"server creation failed"
+        raise PrismError(rc, (msg or b"").decode())
 
     # ------------------------------------------------------------ public --
     def register_table(self, name: str, table, payload_col: int):
-        self.tables[name] = _Table(table, payload_col)
+        """table: a prism_gpu.HashTable (single Int64 key) the caller keeps
+        alive; probes emit (probe row, build column `payload_col`)."""
+        tid = self._C.c_int32(0)
+        rc = self._lib.prism_server_add_table(self._h, table._h, payload_col, self._C.byref(tid))
+        if rc:
+            self._raise(rc)
+        self.tables[name] = tid.value
 
     def submit(self, req) -> cf.Future:
+        from . import DeviceBatch
+
+        C = self._C
         fut: cf.Future = cf.Future()
-        self._inbox.put((req, fut))
+        ticket = C.c_int64(0)
+        if isinstance(req, ProbeRequest):
+            keys = req.keys.contiguous()
+            keep = keys
+            rc = self._lib.prism_serve_probe(self._h, self.tables[req.table], keys.data_ptr(), int(keys.numel()),
+                                             C.byref(ticket))
+        else:
+            n = int(req.columns[0][2].numel())
+            db = DeviceBatch.from_device_buffers([(nm, f, t.data_ptr()) for nm, f, t in req.columns], n, self._ctx,
+                                                 self.device)
+            cfg = req.config.encode()
+            keep = (db, cfg, [t for _, _, t in req.columns])
+            rc = self._lib.prism_serve_aggregate(self._h, db.handle, C.byref(cfg), C.byref(ticket))
+        if rc:
+            self._raise(rc)
+        with self._lock:
+            self._pending[ticket.value] = (fut, req, keep)
         return fut
 
     def close(self):
-        self._closed = True
-        self._inbox.put(None)
-        self._disp.join()
-        for _ in self._threads:
-            self._put(None)
-        for t in self._threads:
-            t.join()
+        """Finishes every submitted request, then stops the native server."""
+        with self._lock:
+            self._closed = True
+        self._poller.join()
+        self._lib.prism_server_destroy(self._h)
+        self._h = None
 
-    def _put(self, job: Optional[_Job]):
-        """Queues a job by its row count (a closing sentinel after every job)."""
-        with self._seq_lock:
-            self._seq += 1
-            seq = self._seq
-        self._jobs.put((float("inf") if job is None else job.rows, seq, job))
+    # ------------------------------------------------------------ results --
+    def _poll(self):
+        from . import DeviceBatch, PrismError
 
-    # -------------------------------------------------------- dispatcher --
-    @staticmethod
-    def _rows(req) -> int:
-        return int(req.keys.numel()) if isinstance(req, ProbeRequest) else int(req.columns[0][2].numel())
+        PRISM_ERR_TIMEOUT = 10  # include/prism_gpu.h
 
-    def _key(self, req):
-        if isinstance(req, ProbeRequest):
-            return ("probe", req.table)
-        return ("agg", repr(req.config), tuple((n, f) for n, f, _ in req.columns))
-
-    def _dispatch(self):
-        pending: Dict[tuple, _Job] = {}
+        C = self._C
+        t = C.c_int64(0)
         while True:
+            rc = self._lib.prism_serve_wait_any(self._h, 20, C.byref(t))
+            if rc == PRISM_ERR_TIMEOUT:
+                with self._lock:
+                    if self._closed and not self._pending:
+                        return
+                continue
+            out = C.c_void_p()
+            rc = self._lib.prism_serve_poll(self._h, t.value, 0, C.byref(out))
+            with self._lock:
+                fut, req, keep = self._pending.pop(t.value)
+            if rc:
+                msg = self._lib.prism_server_last_error(self._h)
+                fut.set_exception(PrismError(rc, (msg or b"").decode()))
+                continue
+            db = DeviceBatch(self._ctx, out)
             try:
-                item = self._inbox.get(timeout=0.0005 if pending else None)
-            except queue.Empty:
-                item = "flush"
-            if item is None:
-                for j in pending.values():
-                    self._put(j)
-                return
-            if item != "flush":
-                req, fut = item
-                n = self._rows(req)
-                kind = "probe" if isinstance(req, ProbeRequest) else "agg"
-                if n >= self.coalesce_rows:
-                    self._put(_Job([req], [fut], kind, n))
-                    continue
-                k = self._key(req)
-                j = pending.get(k)
-                if j is None:
-                    pending[k] = _Job([req], [fut], kind, n)
+                if isinstance(req, ProbeRequest):
+                    m = db.num_rows
+                    fut.set_result(ProbeResult(m, _device_tensor(self.torch, db, 0, self.torch.int32, m, self.device),
+                                               _device_tensor(self.torch, db, 1, self.torch.int64, m, self.device), db))
                 else:
-                    j.reqs.append(req)
-                    j.futs.append(fut)
-                    j.rows += n
-                j = pending[k]
-                if j.rows >= self.coalesce_rows or len(j.reqs) >= self.max_coalesce:
-                    self._put(pending.pop(k))
-                if not self._inbox.empty():
-                    continue
-            # nothing more waiting: hand over what is pending
-            for k in list(pending):
-                self._put(pending.pop(k))
-
-    # ------------------------------------------------------------ worker --
-    def _admit(self, nbytes: int):
-        with self._cv:
-            while self.in_use > 0 and self.in_use + nbytes > self.budget:
-                self._cv.wait()
-            self.in_use += nbytes
-
-    def _release(self, nbytes: int):
-        with self._cv:
-            self.in_use -= nbytes
-            self._cv.notify_all()
-
-    def _worker(self, ctx, stream):
-        torch = self.torch
-        while True:
-            job = self._jobs.get()[2]
-            if job is None:
-                return
-            nbytes = _footprint(job)
-            self._admit(nbytes)
-            try:
-                with torch.cuda.stream(stream):
-                    if job.kind == "probe":
-                        results = self._run_probe(ctx, stream, job.reqs)
-                    else:
-                        results = self._run_agg(ctx, stream, job.reqs)
-                # results are read on other streams: finish this job's work first
-                stream.synchronize()
-                for f, r in zip(job.futs, results):
-                    f.set_result(r)
-            except BaseException as e:  # every request of the job fails alike
-                for f in job.futs:
-                    if not f.done():
-                        f.set_exception(e)
-            finally:
-                self._release(nbytes)
-
-    def _run_probe(self, ctx, stream, reqs: List[ProbeRequest]) -> List[ProbeResult]:
-        from . import PRISM_COL_PROBE_ROW_INDEX, DeviceBatch
-
-        torch = self.torch
-        t = self.tables[reqs[0].table]
-        keys = reqs[0].keys if len(reqs) == 1 else torch.cat([r.keys for r in reqs])
-        n = int(keys.numel())
-        db = DeviceBatch.from_device_buffers([("key", "l", keys.data_ptr())], n, ctx, self.device)
-        out = t.table.join_project(db, [0], [PRISM_COL_PROBE_ROW_INDEX, 1 + t.payload_col], as_device=True, ctx=ctx)
-        m = out.num_rows
-        prow = _device_tensor(torch, out, 0, torch.int32, m, self.device)
-        pay = _device_tensor(torch, out, 1, torch.int64, m, self.device)
-        if len(reqs) == 1:
-            return [ProbeResult(m, prow, pay, (out, db, keys))]
-        starts = [0]
-        for r in reqs:
-            starts.append(starts[-1] + int(r.keys.numel()))
-        bounds = torch.tensor(starts, dtype=torch.int32, device=keys.device)
-        cut = torch.searchsorted(prow, bounds).cpu().tolist()  # matches are in probe-row order
-        res = []
-        for i in range(len(reqs)):
-            a, b = cut[i], cut[i + 1]
-            res.append(ProbeResult(b - a, prow[a:b] - starts[i], pay[a:b], (out, db, keys)))
-        return res
-
-    def _run_agg(self, ctx, stream, reqs: List[AggRequest]) -> List[pa.RecordBatch]:
-        from . import DeviceBatch, hash_aggregate
-
-        torch = self.torch
-        cfg = reqs[0].config
-        if len(reqs) == 1:
-            cols = reqs[0].columns
-            n = int(cols[0][2].numel())
-            db = DeviceBatch.from_device_buffers([(nm, f, t.data_ptr()) for nm, f, t in cols], n, ctx, self.device)
-            return [hash_aggregate(db, cfg, ctx=ctx)]
-        # one aggregation for all: a segment id as the first group key
-        sizes = [int(r.columns[0][2].numel()) for r in reqs]
-        seg = torch.repeat_interleave(torch.arange(len(reqs), dtype=torch.int32, device=reqs[0].columns[0][2].device),
-                                      torch.tensor(sizes, device=reqs[0].columns[0][2].device))
-        cols = [("__segment", "i", seg)]
-        for c in range(len(reqs[0].columns)):
-            nm, f, _ = reqs[0].columns[c]
-            cols.append((nm, f, torch.cat([r.columns[c][2] for r in reqs])))
-        n = sum(sizes)
-        db = DeviceBatch.from_device_buffers([(nm, f, t.data_ptr()) for nm, f, t in cols], n, ctx, self.device)
-        scfg = HashAggConfig([0] + [g + 1 for g in cfg.group_by],
-                             [AggExpr(a.column + 1, a.func, a.output_name) for a in cfg.aggregates])
-        out = hash_aggregate(db, scfg, ctx=ctx)
-        segs = out.column(0).to_numpy()
-        res = []
-        import numpy as np
-
-        for i in range(len(reqs)):
-            idx = np.nonzero(segs == i)[0]
-            part = out.take(pa.array(idx, type=pa.int64()))
-            res.append(pa.RecordBatch.from_arrays(part.columns[1:], schema=pa.schema(list(part.schema)[1:])))
-        return res
+                    fut.set_result(db.to_arrow())
+                    db.free()
+            except BaseException as e:  # reported on the request's future
+                fut.set_exception(e)
 
 
 class _CudaArray:

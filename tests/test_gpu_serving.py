@@ -1,5 +1,7 @@
-"""Serving loop: every request's result is the same served in the mix
-(coalesced with others, on several streams, under admission) as run alone."""
+"""Serving loop (the native prism_server_* ABI through prism_gpu.serving):
+every request's result is the same served in the mix (coalesced with
+others, on several streams, under admission, smallest job first) as run
+alone; errors come back on the request's future."""
 import numpy as np
 import pytest
 
@@ -71,3 +73,31 @@ def test_served_results_equal_alone(ctx):
             assert np.array_equal(b.payload.cpu().numpy(), pay)
         else:
             assert_batches_equal(b, a, float_cols=(1, 2, 4))
+
+
+def test_global_aggregates_and_errors(ctx):
+    """GROUP BY-less aggregates run alone (never coalesced) and equal the
+    plain call; a probe of an unregistered table fails at submit."""
+    import torch
+
+    import prism_gpu
+    from prism_gpu import AggExpr, AggFunc, HashAggConfig
+    from prism_gpu import serving as S
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(9)
+    v = torch.randint(-1000, 1000, (500_000,), generator=g, device=dev)
+    x = torch.rand(500_000, generator=g, device=dev, dtype=torch.float64)
+    cfg = HashAggConfig([], [AggExpr(0, AggFunc.Sum, "s"), AggExpr(1, AggFunc.Avg, "a"), AggExpr(0, AggFunc.Count, "n")])
+    reqs = [S.AggRequest([("v", "l", v[i * 1000:(i + 1) * 1000 + 7 * i]), ("x", "g", x[i * 1000:(i + 1) * 1000 + 7 * i])], cfg)
+            for i in range(40)]
+    torch.cuda.synchronize()
+    alone, _ = S.run_plain(reqs, {}, ctx)
+    srv = S.Server(0, workers=2, coalesce_rows=1 << 20, max_coalesce=32)
+    got = [f.result(timeout=300) for f in [srv.submit(r) for r in reqs]]
+    with pytest.raises(KeyError):
+        srv.submit(S.ProbeRequest("missing", v[:10]))
+    srv.close()
+    for a, b in zip(alone, got):
+        assert_batches_equal(b, a, float_cols=(0, 1))
