@@ -421,7 +421,9 @@ int prism_join_aggregate(prism_ctx* ctx, const prism_batch* const* probes, int32
  *
  * Lifetimes: tables, request batches and key buffers stay owned by the
  * caller and must outlive their requests; result batches belong to the
- * caller and must be freed (prism_batch_free) before prism_server_destroy.
+ * caller (prism_batch_free) and stay valid after prism_server_destroy, which
+ * therefore retires its worker contexts instead of destroying them (their
+ * streams stay until exit; their unused device memory is released).
  * Key buffers and request batches must be complete on the device when
  * submitted. Results are complete when poll returns them. */
 typedef struct prism_server prism_server;

@@ -5,7 +5,8 @@
 // server keeps the caller's tables resident, runs requests on several worker
 // threads that each own a context and CUDA stream (so their kernels overlap
 // on the device), admits a job only while its device footprint fits the
-// budget, hands the smallest ready job to the next free worker, and coalesces
+// budget, hands the smallest ready job to the next free worker (the oldest
+// one once it has waited 10 ms, so no job starves), and coalesces
 // small requests that arrive close together into one launch:
 //   * small probes of one table are concatenated and probed once; the output
 //     is in probe-row order, so each request's matches are one contiguous
@@ -145,7 +146,8 @@ struct prism_server {
   std::condition_variable cv_inbox, cv_jobs, cv_done, cv_admit;
   std::deque<Request> inbox;
   std::priority_queue<std::pair<JobOrder, int64_t>> order;  // (order, job id)
-  std::map<int64_t, Job> jobs;
+  std::deque<std::pair<int64_t, std::chrono::steady_clock::time_point>> fifo;  // (job id, queued at)
+  std::map<int64_t, Job> jobs;  // queued jobs (ids in order/fifo that are gone here were taken)
   int64_t next_job = 0, next_seq = 0, next_ticket = 1;
   std::map<int64_t, Result> results;
   std::deque<int64_t> completed;  // tickets in completion order (prism_serve_wait_any)
@@ -168,8 +170,27 @@ uint64_t footprint(const Job& j) {
 void push_job(prism_server* s, Job&& j) {  // s->mu held
   int64_t id = s->next_job++;
   s->order.push({JobOrder{j.rows, s->next_seq++}, id});
+  s->fifo.push_back({id, std::chrono::steady_clock::now()});
   s->jobs.emplace(id, std::move(j));
   s->cv_jobs.notify_one();
+}
+
+// The next job: the smallest queued one, unless the oldest has waited longer
+// than kMaxWait (smallest-first alone could starve a large job under a
+// steady stream of small ones). s->mu held, some job queued.
+constexpr auto kMaxWait = std::chrono::milliseconds(10);
+int64_t take_job(prism_server* s) {
+  while (!s->fifo.empty() && !s->jobs.count(s->fifo.front().first)) s->fifo.pop_front();
+  while (!s->order.empty() && !s->jobs.count(s->order.top().second)) s->order.pop();
+  int64_t id;
+  if (!s->fifo.empty() && std::chrono::steady_clock::now() - s->fifo.front().second > kMaxWait) {
+    id = s->fifo.front().first;
+    s->fifo.pop_front();
+  } else {
+    id = s->order.top().second;
+    s->order.pop();
+  }
+  return id;
 }
 
 void finish(prism_server* s, const Request& r, int status, const std::string& msg, prism_batch* out) {
@@ -389,10 +410,9 @@ void work(prism_server* s, prism_ctx* w) {
     Job job;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_jobs.wait(lk, [&] { return !s->order.empty() || s->dispatcher_done; });
-      if (s->order.empty()) return;
-      int64_t id = s->order.top().second;
-      s->order.pop();
+      s->cv_jobs.wait(lk, [&] { return !s->jobs.empty() || s->dispatcher_done; });
+      if (s->jobs.empty()) return;
+      int64_t id = take_job(s);
       job = std::move(s->jobs.at(id));
       s->jobs.erase(id);
     }
@@ -598,7 +618,13 @@ void prism_server_destroy(prism_server* s) {
   for (auto& r : s->results)
     if (r.second.out) prism_batch_free(r.second.out);
   s->results.clear();
-  for (auto* c : s->ctxs) prism_ctx_destroy(c);
+  // results already handed out may outlive the server and free their device
+  // memory through the worker context that allocated it: the contexts are
+  // retired (unused pool memory released), not destroyed
+  for (auto* c : s->ctxs) {
+    cudaStreamSynchronize(c->impl.stream);
+    cudaMemPoolTrimTo(c->impl.pool, 0);
+  }
   delete s;
 }
 

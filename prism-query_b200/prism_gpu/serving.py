@@ -71,7 +71,9 @@ class Server:
         self.device = device
         self._C = C
         self._lib = lib()
-        self._ctx = Context(device)  # imports request batches and exports results
+        self._ctx = Context(device)  # wraps request batches (submit side)
+        self._local = threading.local()  # per completion thread: a context for exports
+        self._Context = Context
         self._h = C.c_void_p()
         rc = self._lib.prism_server_create(device, budget_bytes, workers, coalesce_rows, max_coalesce, C.byref(self._h))
         if rc:
@@ -79,7 +81,11 @@ class Server:
         self.tables: Dict[str, int] = {}
         self._lock = threading.Lock()
         self._pending: Dict[int, tuple] = {}  # ticket -> (future, request, keepalive)
+        self._submitted = 0
         self._closed = False
+        # finished tickets are turned into results (export, tensor views) and
+        # the futures' callbacks run on a pool as wide as the server
+        self._done_pool = cf.ThreadPoolExecutor(max_workers=workers)
         self._poller = threading.Thread(target=self._poll, daemon=True)
         self._poller.start()
 
@@ -108,19 +114,23 @@ class Server:
         if isinstance(req, ProbeRequest):
             keys = req.keys.contiguous()
             keep = keys
-            rc = self._lib.prism_serve_probe(self._h, self.tables[req.table], keys.data_ptr(), int(keys.numel()),
-                                             C.byref(ticket))
+            tid = self.tables[req.table]
         else:
             n = int(req.columns[0][2].numel())
             db = DeviceBatch.from_device_buffers([(nm, f, t.data_ptr()) for nm, f, t in req.columns], n, self._ctx,
                                                  self.device)
             cfg = req.config.encode()
             keep = (db, cfg, [t for _, _, t in req.columns])
-            rc = self._lib.prism_serve_aggregate(self._h, db.handle, C.byref(cfg), C.byref(ticket))
+        with self._lock:  # registered before any completion can look it up
+            if isinstance(req, ProbeRequest):
+                rc = self._lib.prism_serve_probe(self._h, tid, keys.data_ptr(), int(keys.numel()), C.byref(ticket))
+            else:
+                rc = self._lib.prism_serve_aggregate(self._h, db.handle, C.byref(cfg), C.byref(ticket))
+            if rc == 0:
+                self._pending[ticket.value] = (fut, req, keep)
+                self._submitted += 1
         if rc:
             self._raise(rc)
-        with self._lock:
-            self._pending[ticket.value] = (fut, req, keep)
         return fut
 
     def close(self):
@@ -128,43 +138,53 @@ class Server:
         with self._lock:
             self._closed = True
         self._poller.join()
+        self._done_pool.shutdown(wait=True)
         self._lib.prism_server_destroy(self._h)
         self._h = None
 
     # ------------------------------------------------------------ results --
     def _poll(self):
-        from . import DeviceBatch, PrismError
-
         PRISM_ERR_TIMEOUT = 10  # include/prism_gpu.h
 
         C = self._C
         t = C.c_int64(0)
+        taken = 0
         while True:
             rc = self._lib.prism_serve_wait_any(self._h, 20, C.byref(t))
             if rc == PRISM_ERR_TIMEOUT:
                 with self._lock:
-                    if self._closed and not self._pending:
+                    if self._closed and len(self._pending) == 0 and taken == self._submitted:
                         return
                 continue
-            out = C.c_void_p()
-            rc = self._lib.prism_serve_poll(self._h, t.value, 0, C.byref(out))
-            with self._lock:
-                fut, req, keep = self._pending.pop(t.value)
-            if rc:
-                msg = self._lib.prism_server_last_error(self._h)
-                fut.set_exception(PrismError(rc, (msg or b"").decode()))
-                continue
-            db = DeviceBatch(self._ctx, out)
-            try:
-                if isinstance(req, ProbeRequest):
-                    m = db.num_rows
-                    fut.set_result(ProbeResult(m, _device_tensor(self.torch, db, 0, self.torch.int32, m, self.device),
-                                               _device_tensor(self.torch, db, 1, self.torch.int64, m, self.device), db))
-                else:
-                    fut.set_result(db.to_arrow())
-                    db.free()
-            except BaseException as e:  # reported on the request's future
-                fut.set_exception(e)
+            taken += 1
+            self._done_pool.submit(self._complete, t.value)
+
+    def _complete(self, ticket: int):
+        from . import DeviceBatch, PrismError
+
+        C = self._C
+        out = C.c_void_p()
+        rc = self._lib.prism_serve_poll(self._h, ticket, 0, C.byref(out))
+        with self._lock:
+            fut, req, keep = self._pending.pop(ticket)
+        if rc:
+            msg = self._lib.prism_server_last_error(self._h)
+            fut.set_exception(PrismError(rc, (msg or b"").decode()))
+            return
+        ctx = getattr(self._local, "ctx", None)
+        if ctx is None:  # exports of different threads do not queue on one context
+            ctx = self._local.ctx = self._Context(self.device)
+        db = DeviceBatch(ctx, out)
+        try:
+            if isinstance(req, ProbeRequest):
+                m = db.num_rows
+                fut.set_result(ProbeResult(m, _device_tensor(self.torch, db, 0, self.torch.int32, m, self.device),
+                                           _device_tensor(self.torch, db, 1, self.torch.int64, m, self.device), db))
+            else:
+                fut.set_result(db.to_arrow())
+                db.free()
+        except BaseException as e:  # reported on the request's future
+            fut.set_exception(e)
 
 
 class _CudaArray:
