@@ -499,6 +499,21 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
     lpos[it] = __popc(m & ((1u << lane) - 1u));
     if (lane == 0) seg[it][warp] = __popc(m);
   }
+  // one 8-byte gathered column (the probe-row + payload output): every
+  // matched row's value is loaded here, all QI in flight, before the scan
+  // and any store (the stores could alias the source, so the compiler would
+  // not move these loads above them)
+  const bool one8 = a.ngather == 1 && a.g_width[0] == 8;
+  unsigned long long pre[QI];
+  if (one8) {
+    const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[0]);
+    const bool bside = a.g_side[0] != 0;
+#pragma unroll
+    for (int it = 0; it < QI; ++it) {
+      int64_t r = base + it * QB + threadIdx.x;
+      pre[it] = v[it] != NO_MATCH ? __ldg(src + (bside ? (int64_t)v[it] : r)) : 0ULL;
+    }
+  }
   __syncthreads();
   // exclusive offsets of the (item, warp) segments in row order
   if (warp == 0) {
@@ -519,7 +534,13 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
       atomicOr(a.err, DERR_CAPACITY);
       continue;
     }
-    emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
+    if (one8) {
+      if (a.out_probe) a.out_probe[pos] = (uint32_t)(base + it * QB + threadIdx.x);
+      if (a.out_build) a.out_build[pos] = v[it];
+      static_cast<unsigned long long*>(a.g_dst[0])[pos] = pre[it];
+    } else {
+      emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
+    }
   }
 }
 
