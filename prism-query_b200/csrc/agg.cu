@@ -378,6 +378,21 @@ __global__ void __launch_bounds__(1024) small_order_kernel(const unsigned long l
   }
   __syncthreads();
   const int n = (int)cnt;
+  if (n <= (int)blockDim.x) {
+    // up to one key per thread: its rank is the number of smaller keys (the
+    // keys are distinct), every thread reading the same key at once
+    const unsigned long long mine = tid < n ? okey[tid] : 0ULL;
+    const uint32_t slot = tid < n ? oslot[tid] : 0u;
+    int rank = 0;
+    for (int j = 0; j < n; ++j) rank += okey[j] < mine ? 1 : 0;
+    if (tid < n) {
+      ordered[rank] = slot;
+      firsts[rank] = mine;
+      rows32[rank] = (uint32_t)mine;
+    }
+    if (tid == 0) *out = (unsigned long long)n;
+    return;
+  }
   int m = 1;
   while (m < n) m <<= 1;
   for (int i = n + tid; i < m; i += blockDim.x) {
