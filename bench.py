@@ -910,14 +910,18 @@ def run_c5(args, rank, world, local, torch, dist):
     total_rows = sum(int(r.keys.numel()) if isinstance(r, S.ProbeRequest) else int(r.columns[0][2].numel())
                      for r in reqs)
     torch.cuda.synchronize()
-    # warm-up: both paths on a few requests (allocator pools, kernel images)
+    # warm-up (allocator pools, every generated kernel shape, export buffers):
+    # both paths on 20 requests, then the server on a burst of 200 (small
+    # requests of both kinds coalesce, so the coalesced shapes compile here),
+    # twice
     warm = [S.ProbeRequest(r.table, r.keys) if isinstance(r, S.ProbeRequest) else S.AggRequest(r.columns, r.config)
-            for r in reqs[:20]]
-    S.run_plain(warm, regs, ctx, local)
+            for r in reqs[:200]]
+    S.run_plain(warm[:20], regs, ctx, local)
     srv = S.Server(local, budget_bytes=120 << 30, workers=4, coalesce_rows=1 << 18, max_coalesce=64)
     for name, reg in regs.items():
         srv.register_table(name, reg.table, 1)
-    [f.result() for f in [srv.submit(w) for w in warm]]
+    for _ in range(2):
+        [f.result() for f in [srv.submit(w) for w in warm]]
 
     # results: aggregates whole; probes by match count, and every 16th probe by a
     # checksum of its rows (holding every probe's output would not fit in HBM)

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <mutex>
 #include <sstream>
 #include <unordered_map>
@@ -72,9 +73,11 @@ Nvrtc& nvrtc() {
 struct Entry {
   cudaLibrary_t lib = nullptr;
   std::unordered_map<std::string, cudaKernel_t> kernels;
+  bool ready = false;  // false while one thread compiles it (others wait on g_cv)
 };
 
 std::mutex g_mu;
+std::condition_variable g_cv;
 std::unordered_map<std::string, Entry> g_cache;
 int64_t g_compiles = 0;
 double g_compile_ms = 0;
@@ -649,40 +652,68 @@ void jit_stats(int64_t* compiles, double* ms) {
   if (ms) *ms = g_compile_ms;
 }
 
+// Compiles `source` with NVRTC and loads it (no lock held: a compile takes
+// hundreds of milliseconds and must not stall lookups of other kernels).
+static cudaLibrary_t compile_source(const std::string& source) {
+  Nvrtc& N = nvrtc();
+  if (!N.ok) fail(PRISM_ERR_INTERNAL, "run-time kernel compilation is not available (NVRTC not loaded)");
+  nvrtcProgram prog;
+  if (N.create(&prog, source.c_str(), "prism_query.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
+      NVRTC_SUCCESS)
+    fail(PRISM_ERR_INTERNAL, "nvrtcCreateProgram failed");
+  // no FMA contraction: generated Float64 arithmetic rounds after every
+  // operation, like the interpreter and the reference
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-int128", "--fmad=false",
+                        "--diag-suppress=550"};
+  nvrtcResult r = N.compile(prog, 5, opts);
+  if (r != NVRTC_SUCCESS) {
+    size_t ls = 0;
+    N.log_size(prog, &ls);
+    std::string log(ls, '\0');
+    if (ls) N.log(prog, &log[0]);
+    N.destroy(&prog);
+    fail(PRISM_ERR_INTERNAL, "run-time kernel compilation failed:\n" + log);
+  }
+  size_t n = 0;
+  N.cubin_size(prog, &n);
+  std::vector<char> cubin(n);
+  N.cubin(prog, cubin.data());
+  N.destroy(&prog);
+  cudaLibrary_t lib = nullptr;
+  PRISM_CUDA(cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  return lib;
+}
+
 const void* jit_get(const std::string& source, const char* name) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::unique_lock<std::mutex> lk(g_mu);
   auto it = g_cache.find(source);
   if (it == g_cache.end()) {
-    Nvrtc& N = nvrtc();
-    if (!N.ok) fail(PRISM_ERR_INTERNAL, "run-time kernel compilation is not available (NVRTC not loaded)");
+    g_cache.emplace(source, Entry{});  // this thread compiles it
+    lk.unlock();
     auto t0 = std::chrono::steady_clock::now();
-    nvrtcProgram prog;
-    if (N.create(&prog, source.c_str(), "prism_query.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
-        NVRTC_SUCCESS)
-      fail(PRISM_ERR_INTERNAL, "nvrtcCreateProgram failed");
-    // no FMA contraction: generated Float64 arithmetic rounds after every
-    // operation, like the interpreter and the reference
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-int128", "--fmad=false",
-                          "--diag-suppress=550"};
-    nvrtcResult r = N.compile(prog, 5, opts);
-    if (r != NVRTC_SUCCESS) {
-      size_t ls = 0;
-      N.log_size(prog, &ls);
-      std::string log(ls, '\0');
-      if (ls) N.log(prog, &log[0]);
-      N.destroy(&prog);
-      fail(PRISM_ERR_INTERNAL, "run-time kernel compilation failed:\n" + log);
+    cudaLibrary_t lib = nullptr;
+    try {
+      lib = compile_source(source);
+    } catch (...) {
+      lk.lock();
+      g_cache.erase(source);
+      g_cv.notify_all();
+      throw;
     }
-    size_t n = 0;
-    N.cubin_size(prog, &n);
-    std::vector<char> cubin(n);
-    N.cubin(prog, cubin.data());
-    N.destroy(&prog);
-    Entry e;
-    PRISM_CUDA(cudaLibraryLoadData(&e.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
-    it = g_cache.emplace(source, std::move(e)).first;
+    lk.lock();
+    it = g_cache.find(source);
+    it->second.lib = lib;
+    it->second.ready = true;
     g_compiles += 1;
     g_compile_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    g_cv.notify_all();
+  } else if (!it->second.ready) {
+    g_cv.wait(lk, [&] {
+      auto f = g_cache.find(source);
+      return f == g_cache.end() || f->second.ready;
+    });
+    it = g_cache.find(source);
+    if (it == g_cache.end()) fail(PRISM_ERR_INTERNAL, "run-time kernel compilation failed in another thread");
   }
   auto kt = it->second.kernels.find(name);
   if (kt == it->second.kernels.end()) {
