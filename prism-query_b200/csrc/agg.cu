@@ -182,17 +182,6 @@ __global__ void init_table_kernel(AggArgs a, int64_t nslots) {
   }
 }
 
-__global__ void fill_words_kernel(unsigned long long* acc, int64_t groups, int W, AggArgs a) {
-  int64_t n = groups * W;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    acc[i] = a.winit[i % W];
-}
-
-__global__ void fill_u64_kernel(unsigned long long* p, int64_t n, unsigned long long v) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = v;
-}
-
 // The aggregation kernel. Dynamic shared memory (hash mode):
 //   skeys[SS] u64 | sfirst[SD] u64 | skeyof[SD] u64 | sacc[SD*W] u64 | sidx[SS] i32
 // Dense mode: sfirst[G] | sacc[G*W] when G fits, else global atomics only.
