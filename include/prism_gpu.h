@@ -408,6 +408,26 @@ int prism_join_aggregate(prism_ctx* ctx, const prism_batch* const* probes, int32
                          const prism_agg_config* agg, prism_batch** out);
 
 /* ------------------------------------------------------------------------ */
+/* Sort / top-N (native/prism-executor/src/sort.rs)                          */
+/* ------------------------------------------------------------------------ */
+/* SortKey (sort.rs:28-32): SortDirection Asc/Desc, NullOrdering
+ * NullsFirst/NullsLast. */
+typedef struct prism_sort_key {
+  int32_t column;
+  int32_t descending;   /* 0 Asc, 1 Desc */
+  int32_t nulls_first;  /* 1 NullsFirst, 0 NullsLast */
+} prism_sort_key;
+
+/* sort_batch (sort.rs:35-54) with limit < 0, sort_batch_limit (sort.rs:56-78)
+ * with limit >= 0, and topn_single_col (sort.rs:97-146) as a Float64
+ * descending key with a limit: the rows ordered by the keys (most
+ * significant first), integers numerically, floats by IEEE totalOrder,
+ * Utf8 / dictionary values bytewise then by length, Decimal128 numerically;
+ * ties keep the input order. An empty batch or key list returns the batch. */
+int prism_sort_batch(prism_ctx* ctx, const prism_batch* batch, const prism_sort_key* keys, int32_t n_keys,
+                     int64_t limit, prism_batch** out);
+
+/* ------------------------------------------------------------------------ */
 /* Serving loop (prism_serve_submit/poll of the design)                       */
 /* ------------------------------------------------------------------------ */
 /* Requests of uneven sizes against resident tables, answered by worker
@@ -469,6 +489,9 @@ int prism_hash_aggregate_arrow(prism_ctx* ctx, const struct ArrowArray* batch,
                                const struct ArrowSchema* schema,
                                const prism_agg_config* config, struct ArrowArray* out,
                                struct ArrowSchema* out_schema);
+int prism_sort_batch_arrow(prism_ctx* ctx, const struct ArrowArray* batch, const struct ArrowSchema* schema,
+                           const prism_sort_key* keys, int32_t n_keys, int64_t limit, struct ArrowArray* out,
+                           struct ArrowSchema* out_schema);
 int prism_filter_and_project_arrow(prism_ctx* ctx, const struct ArrowArray* batch,
                                    const struct ArrowSchema* schema,
                                    const prism_predicate* predicate, const int32_t* cols,

@@ -19,6 +19,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <functional>
 #include <limits>
 #include <map>
@@ -1454,6 +1455,73 @@ Batch join_aggregate(const std::vector<Batch>& probes, const Batch& build,
   return out;
 }
 
+// ================================================================ sort ====
+// sort_batch / sort_batch_limit (sort.rs:35-78): arrow-ord's
+// lexsort_to_indices with each key's SortOptions, then take. Per key: two
+// nulls are equal; a null sorts before a value with nulls_first, after it
+// otherwise, whatever the direction; values compare ascending, reversed for
+// descending. Value order (arrow-ord compare): integers numerically, floats
+// by total_cmp (IEEE totalOrder), Boolean false < true, Utf8 (and a
+// dictionary's decoded values) bytewise then by length, Decimal128
+// numerically. The reference's sort is unstable (sort_unstable_by, with a
+// partial sort under a limit); this restatement is stable, so ties keep the
+// input order.
+int64_t total_key64(double d) {
+  int64_t i;
+  std::memcpy(&i, &d, 8);
+  return i ^ (int64_t)(((uint64_t)(i >> 63)) >> 1);
+}
+int32_t total_key32(float f) {
+  int32_t i;
+  std::memcpy(&i, &f, 4);
+  return i ^ (int32_t)(((uint32_t)(i >> 31)) >> 1);
+}
+
+int sort_value_cmp(const Col& c, int64_t x, int64_t y) {
+  auto sgn = [](auto a, auto b) { return a < b ? -1 : (b < a ? 1 : 0); };
+  switch (c.ty) {
+    case T_F64: return sgn(total_key64(reinterpret_cast<const double*>(c.vals)[c.off + x]),
+                           total_key64(reinterpret_cast<const double*>(c.vals)[c.off + y]));
+    case T_F32: return sgn(total_key32(reinterpret_cast<const float*>(c.vals)[c.off + x]),
+                           total_key32(reinterpret_cast<const float*>(c.vals)[c.off + y]));
+    case T_U64: return sgn((uint64_t)c.ival(x), (uint64_t)c.ival(y));
+    case T_UTF8: case T_DICT: return sgn(c.sval(x), c.sval(y));
+    case T_DEC128: return sgn(c.dval(x), c.dval(y));
+    default: return sgn(c.ival(x), c.ival(y));
+  }
+}
+
+Batch sort_batch(const Batch& b, const prism_sort_key* keys, int n_keys, int64_t limit) {
+  for (int i = 0; i < n_keys; ++i) {
+    if (keys[i].column < 0 || keys[i].column >= (int)b.cols.size())
+      fail(PRISM_ERR_INVALID_ARGUMENT, "sort column out of range");
+    if (b.cols[keys[i].column]->ty == T_NULL) fail(PRISM_ERR_INVALID_ARGUMENT, "sorting by a null-typed column");
+  }
+  if (b.rows == 0 || n_keys == 0) return b;
+  std::vector<int64_t> idx(b.rows);
+  for (int64_t i = 0; i < b.rows; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) {
+    for (int k = 0; k < n_keys; ++k) {
+      const Col& c = *b.cols[keys[k].column];
+      const bool nx = c.null_at(x), ny = c.null_at(y);
+      if (nx || ny) {
+        if (nx && ny) continue;
+        return nx ? keys[k].nulls_first != 0 : keys[k].nulls_first == 0;
+      }
+      int r = sort_value_cmp(c, x, y);
+      if (r == 0) continue;
+      if (keys[k].descending) r = -r;
+      return r < 0;
+    }
+    return false;
+  });
+  if (limit >= 0 && limit < b.rows) idx.resize((size_t)limit);
+  Batch out;
+  out.rows = (int64_t)idx.size();
+  for (auto& c : b.cols) out.cols.push_back(take_col(*c, idx, c->name, c->nullable));
+  return out;
+}
+
 }  // namespace
 
 // ================================================================ C API ====
@@ -1577,6 +1645,14 @@ int oracle_evaluate_predicate(const ArrowArray* batch, const ArrowSchema* schema
     r.rows = b.rows;
     r.cols = {bool_to_col(m, "mask")};
     export_batch(r, out, out_schema);
+  });
+}
+
+int oracle_sort_batch(const ArrowArray* batch, const ArrowSchema* schema, const prism_sort_key* keys, int n_keys,
+                      int64_t limit, ArrowArray* out, ArrowSchema* out_schema) {
+  return guard([&] {
+    Batch b = import_batch(batch, schema);
+    export_batch(sort_batch(b, keys, n_keys, limit), out, out_schema);
   });
 }
 

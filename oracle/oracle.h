@@ -73,6 +73,10 @@ int oracle_hash_aggregate_batches(const struct ArrowArray* const* batches,
 int oracle_evaluate_predicate(const struct ArrowArray* batch, const struct ArrowSchema* schema,
                               const prism_predicate* predicate, struct ArrowArray* out,
                               struct ArrowSchema* out_schema);
+/* sort_batch / sort_batch_limit (sort.rs:35-78); limit < 0: all rows */
+int oracle_sort_batch(const struct ArrowArray* batch, const struct ArrowSchema* schema,
+                      const prism_sort_key* keys, int n_keys, int64_t limit, struct ArrowArray* out,
+                      struct ArrowSchema* out_schema);
 /* filter_batch (filter_project.rs:126-135); mask = 1-column Boolean batch */
 int oracle_filter_batch(const struct ArrowArray* batch, const struct ArrowSchema* schema,
                         const struct ArrowArray* mask, const struct ArrowSchema* mask_schema,

@@ -13,6 +13,7 @@
 #include "jit.hpp"
 #include "join.hpp"
 #include "prims.hpp"
+#include "sort.hpp"
 
 using namespace prism;
 
@@ -760,7 +761,29 @@ int prism_join_aggregate(prism_ctx* c, const prism_batch* const* probes, int32_t
   });
 }
 
+// ------------------------------------------------------------------ sort --
+int prism_sort_batch(prism_ctx* c, const prism_batch* b, const prism_sort_key* keys, int32_t n_keys, int64_t limit,
+                     prism_batch** out) {
+  return run(c, [&] {
+    if (!out || (n_keys > 0 && !keys) || n_keys < 0) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    *out = wrap(c, sort_batch(c->impl, B(b), keys, n_keys, limit));
+  });
+}
+
 // ------------------------------------------------------- arrow wrappers --
+int prism_sort_batch_arrow(prism_ctx* c, const ArrowArray* batch, const ArrowSchema* s, const prism_sort_key* keys,
+                           int32_t n_keys, int64_t limit, ArrowArray* out, ArrowSchema* os) {
+  return run(c, [&] {
+    prism_batch bw;
+    bw.impl = import_batch(c->impl, batch, s, false);
+    prism_batch* r = nullptr;
+    int rc = prism_sort_batch(c, &bw, keys, n_keys, limit, &r);
+    if (rc) fail(rc, c->impl.last_error);
+    std::unique_ptr<prism_batch> hold(r);
+    export_batch(c->impl, r->impl, out, os);
+  });
+}
+
 int prism_hash_join_arrow(prism_ctx* c, const ArrowArray* probe, const ArrowSchema* ps, const ArrowArray* build,
                           const ArrowSchema* bs, const prism_join_config* cfg, ArrowArray* out, ArrowSchema* os) {
   return run(c, [&] {

@@ -1,0 +1,311 @@
+// sort.cu — sort / top-N of a batch on the device.
+//
+// Replaces sort_batch / sort_batch_limit (native/prism-executor/src/sort.rs:
+// 35-78, arrow's lexsort_to_indices + take) and covers topn_single_col
+// (sort.rs:97-146, a Float64 descending top-N) as a limit. Order per key as
+// arrow's sort options define it: a key's nulls first or last whatever its
+// direction; values ascending or descending; integers numerically, floats by
+// IEEE totalOrder (arrow's total_cmp: -0.0 < +0.0, NaN by sign and payload at
+// the ends), Utf8 / dictionary values bytewise then by length. Ties keep the
+// input order (a stable sort).
+//
+// Method: a stable LSD radix sort of (order word, row) pairs. Every key is
+// encoded, least significant part first, into 64-bit order words whose
+// unsigned order is the key's order — fixed-width values in one word (their
+// width in bits), Utf8 as its length and then big-endian 8-byte chunks of its
+// bytes from last to first, and last the null rank — and each word is sorted
+// 8 bits per pass, the row ids riding along; the next word is encoded by
+// gathering through the rows' current order. A pass is a per-tile digit
+// histogram, one exclusive scan over (digit, tile) and a stable scatter
+// (warp match for ranks inside a warp, per-warp digit counts for ranks
+// across warps, tiles in input order).
+#include <algorithm>
+#include <vector>
+
+#include "prims.hpp"
+#include "runtime.hpp"
+#include "sort.hpp"
+
+namespace prism {
+
+namespace {
+
+constexpr int RB = 256;          // threads per block
+constexpr int RR = 16;           // elements per thread per tile
+constexpr int RT = RB * RR;      // elements per tile
+constexpr int RW = RB / 32;      // warps per block
+
+__global__ void iota_u32_kernel(uint32_t* p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (uint32_t)i;
+}
+
+__global__ void __launch_bounds__(RB) radix_hist_kernel(const uint64_t* __restrict__ k, int64_t n, int shift,
+                                                         uint32_t mask, uint32_t* counts, int64_t ntiles) {
+  __shared__ uint32_t h[256];
+  const int tid = threadIdx.x;
+  h[tid] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * RT;
+#pragma unroll 4
+  for (int r = 0; r < RR; ++r) {
+    const int64_t i = base + r * RB + tid;
+    if (i < n) atomicAdd(&h[(uint32_t)(k[i] >> shift) & mask], 1u);
+  }
+  __syncthreads();
+  counts[(int64_t)tid * ntiles + blockIdx.x] = h[tid];
+}
+
+__global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin, int64_t n, int shift,
+                                                            uint32_t mask, const uint64_t* __restrict__ offsets,
+                                                            int64_t ntiles, uint64_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout) {
+  __shared__ uint32_t run[256];      // elements of each digit this tile has placed
+  __shared__ uint32_t wc[RW][256];   // this round: each warp's count per digit
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  run[tid] = 0;
+#pragma unroll
+  for (int w = 0; w < RW; ++w) wc[w][tid] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * RT;
+  for (int r = 0; r < RR; ++r) {
+    const int64_t i = base + r * RB + tid;
+    const bool valid = i < n;
+    uint64_t key = 0;
+    uint32_t val = 0, d = 256u;  // 256: no element
+    if (valid) {
+      key = kin[i];
+      val = vin[i];
+      d = (uint32_t)(key >> shift) & mask;
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank == 0) wc[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t before = run[d];
+      for (int w = 0; w < warp; ++w) before += wc[w][d];
+      const uint64_t pos = offsets[(int64_t)d * ntiles + blockIdx.x] + before + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < RW; ++w) {
+      s += wc[w][tid];
+      wc[w][tid] = 0;
+    }
+    run[tid] += s;
+    __syncthreads();
+  }
+}
+
+// order word of a fixed-width key value (its `bits` low bits); a null row's
+// word is 0 so that nulls tie (their order is decided by the null rank pass)
+__device__ __forceinline__ uint64_t fixed_word(const DCol& c, int64_t row, int bits, bool desc) {
+  if (!dcol_valid(c, row)) return 0;
+  uint64_t u;
+  switch (c.type) {
+    case TY_BOOL: case TY_U8: case TY_U16: case TY_U32: case TY_U64: u = (uint64_t)dcol_ival(c, row); break;
+    case TY_I8: case TY_I16: case TY_I32: case TY_DATE32: case TY_I64:
+      u = (uint64_t)dcol_ival(c, row) ^ (1ULL << (bits - 1));
+      break;
+    case TY_F64: u = (uint64_t)total_key(static_cast<const double*>(c.values)[row]) ^ (1ULL << 63); break;
+    case TY_F32: {
+      int32_t i = __float_as_int(static_cast<const float*>(c.values)[row]);
+      i ^= (int32_t)(((uint32_t)(i >> 31)) >> 1);
+      u = (uint64_t)(uint32_t)i ^ (1ULL << 31);
+      break;
+    }
+    default: u = 0;
+  }
+  const uint64_t m = bits == 64 ? ~0ULL : ((1ULL << bits) - 1);
+  u &= m;
+  return desc ? (~u & m) : u;
+}
+
+__global__ void encode_fixed_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t n, int bits, int desc,
+                                    uint64_t* __restrict__ k) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    k[i] = fixed_word(c, rows[i], bits, desc != 0);
+}
+
+// Decimal128 as two words: low 64 bits, then the high word with the sign flipped
+__global__ void encode_dec_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t n, int high, int desc,
+                                  uint64_t* __restrict__ k) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = rows[i];
+    uint64_t u = 0;
+    if (dcol_valid(c, row)) {
+      const uint64_t* p = static_cast<const uint64_t*>(c.values) + 2 * row;
+      u = high ? (p[1] ^ (1ULL << 63)) : p[0];
+      if (desc) u = ~u;
+    }
+    k[i] = u;
+  }
+}
+
+// Utf8 / dictionary value: word `w` = big-endian bytes [8w, 8w + 8) padded
+// with zeros, or (w < 0) the length
+__global__ void encode_str_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t n, int w, int desc,
+                                  uint64_t* __restrict__ k) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = rows[i];
+    uint64_t u = 0;
+    if (dcol_valid(c, row)) {
+      const uint8_t* p;
+      int32_t len;
+      dcol_str(c, row, p, len);
+      if (w < 0) {
+        u = (uint32_t)len;
+        if (desc) u = ~u & 0xFFFFFFFFULL;
+      } else {
+        const int32_t at = 8 * w;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) u = (u << 8) | (at + b < len ? p[at + b] : 0u);
+        if (desc) u = ~u;
+      }
+    }
+    k[i] = u;
+  }
+}
+
+__global__ void encode_null_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t n, int nulls_first,
+                                   uint64_t* __restrict__ k) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const bool valid = dcol_valid(c, rows[i]);
+    k[i] = nulls_first ? (valid ? 1 : 0) : (valid ? 0 : 1);
+  }
+}
+
+__global__ void max_len_kernel(DCol c, int64_t n, unsigned int* out) {
+  unsigned int m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t* p;
+    int32_t len;
+    dcol_str(c, i, p, len);
+    m = max(m, (unsigned int)len);
+  }
+  for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, d));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+struct Sorter {
+  Ctx& ctx;
+  int64_t n, ntiles;
+  uint64_t *ka, *kb;
+  uint32_t *va, *vb;
+  uint32_t* counts;
+  uint64_t* offsets;
+  uint64_t* total;
+  MemP mka, mkb, mva, mvb, mc, mo, mt;
+  int64_t passes = 0;
+
+  Sorter(Ctx& c, int64_t rows) : ctx(c), n(rows), ntiles(ceil_div(rows, (int64_t)RT)) {
+    ka = ctx.alloc_t<uint64_t>((size_t)n, mka);
+    kb = ctx.alloc_t<uint64_t>((size_t)n, mkb);
+    va = ctx.alloc_t<uint32_t>((size_t)n, mva);
+    vb = ctx.alloc_t<uint32_t>((size_t)n, mvb);
+    counts = ctx.alloc_t<uint32_t>((size_t)ntiles * 256, mc);
+    offsets = ctx.alloc_t<uint64_t>((size_t)ntiles * 256, mo);
+    total = ctx.alloc_t<uint64_t>(1, mt);
+    iota_u32_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(va, n);
+    ctx.check_launch("iota_u32_kernel");
+  }
+  int grid() const { return grid_for(ctx, n, 256); }
+  // stable sort of (ka, va) by the low `bits` bits of ka, 8 per pass
+  void sort_word(int bits) {
+    for (int shift = 0; shift < bits; shift += 8) {
+      const int w = std::min(8, bits - shift);
+      const uint32_t mask = (1u << w) - 1u;
+      radix_hist_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(ka, n, shift, mask, counts, ntiles);
+      ctx.check_launch("radix_hist_kernel");
+      scan_u32_async(ctx, counts, offsets, ntiles * 256, total);
+      {
+        KernelTimer kt(ctx, "radix_scatter_kernel");
+        radix_scatter_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(ka, va, n, shift, mask, offsets, ntiles, kb, vb);
+      }
+      ctx.check_launch("radix_scatter_kernel");
+      std::swap(ka, kb);
+      std::swap(va, vb);
+      ++passes;
+    }
+  }
+};
+
+int key_bits(int type) {
+  switch (type) {
+    case TY_BOOL: return 1;
+    case TY_I8: case TY_U8: return 8;
+    case TY_I16: case TY_U16: return 16;
+    case TY_I32: case TY_U32: case TY_F32: case TY_DATE32: return 32;
+    case TY_I64: case TY_U64: case TY_F64: return 64;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+Batch sort_batch(Ctx& ctx, const Batch& b, const prism_sort_key* keys, int n_keys, int64_t limit) {
+  for (int i = 0; i < n_keys; ++i) {
+    if (keys[i].column < 0 || keys[i].column >= (int)b.cols.size())
+      fail(PRISM_ERR_INVALID_ARGUMENT, "sort column out of range");
+    const int t = b.cols[keys[i].column]->type;
+    if (t == TY_NULL) fail(PRISM_ERR_INVALID_ARGUMENT, "sorting by a null-typed column");
+  }
+  if (b.rows == 0 || n_keys == 0) return b;  // sort.rs:36-38: the batch as it is
+  if (b.rows >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "sort input exceeds 2^32-1 rows");
+  const int64_t n = b.rows;
+  Sorter s(ctx, n);
+  // keys from the least significant (last) to the most significant (first)
+  for (int ki = n_keys - 1; ki >= 0; --ki) {
+    const Column& col = *b.cols[keys[ki].column];
+    const DCol c = col.view();
+    const int desc = keys[ki].descending ? 1 : 0;
+    if (col.type == TY_UTF8 || col.type == TY_DICT) {
+      MemP mm;
+      unsigned int* dmax = ctx.alloc_t<unsigned int>(1, mm);
+      PRISM_CUDA(cudaMemsetAsync(dmax, 0, 4, ctx.stream));
+      max_len_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, n, dmax);
+      ctx.check_launch("max_len_kernel");
+      unsigned int maxlen = 0;
+      PRISM_CUDA(cudaMemcpyAsync(&maxlen, dmax, 4, cudaMemcpyDeviceToHost, ctx.stream));
+      ctx.sync();
+      encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, -1, desc, s.ka);
+      ctx.check_launch("encode_str_kernel");
+      s.sort_word(32);
+      for (int w = (int)((maxlen + 7) / 8) - 1; w >= 0; --w) {
+        encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, w, desc, s.ka);
+        ctx.check_launch("encode_str_kernel");
+        s.sort_word(64);
+      }
+    } else if (col.type == TY_DEC128) {
+      for (int high = 0; high < 2; ++high) {
+        encode_dec_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, high, desc, s.ka);
+        ctx.check_launch("encode_dec_kernel");
+        s.sort_word(64);
+      }
+    } else {
+      const int bits = key_bits(col.type);
+      if (!bits) fail(PRISM_ERR_INVALID_ARGUMENT, "unsupported sort key type");
+      encode_fixed_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, bits, desc, s.ka);
+      ctx.check_launch("encode_fixed_kernel");
+      s.sort_word(bits);
+    }
+    if (col.validity) {
+      encode_null_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, keys[ki].nulls_first ? 1 : 0, s.ka);
+      ctx.check_launch("encode_null_kernel");
+      s.sort_word(1);
+    }
+  }
+  const int64_t m = limit >= 0 ? std::min(limit, n) : n;
+  Batch out;
+  out.rows = m;
+  for (auto& c : b.cols) out.cols.push_back(take(ctx, *c, s.va, nullptr, m, c->name, c->nullable));
+  return out;  // stream-ordered: the sort buffers are freed after the gathers
+
+}
+
+}  // namespace prism

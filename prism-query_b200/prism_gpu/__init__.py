@@ -30,9 +30,13 @@ from .config import (  # noqa: F401  (re-exported API)
     HashJoinConfig,
     JoinType,
     Predicate,
+    NullOrdering,
     ScalarExpr,
     ScalarValue,
+    SortDirection,
+    SortKey,
     encode_exprs,
+    encode_sort_keys,
 )
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -106,6 +110,8 @@ def _declare(lib):
     lib.prism_project_batch_with_exprs.argtypes = [P, P, P, i32, P, i32, i32, C.POINTER(P)]
     lib.prism_filter_project_aggregate.argtypes = [P, P, i32, P, P, i32, P, i32, i32, P, C.POINTER(P)]
     lib.prism_join_aggregate.argtypes = [P, P, i32, P, P, P, i32, P, i32, P, i32, P, C.POINTER(P)]
+    lib.prism_sort_batch.argtypes = [P, P, P, i32, C.c_int64, C.POINTER(P)]
+    lib.prism_sort_batch_arrow.argtypes = [P, P, P, P, i32, C.c_int64, P, P]
     lib.prism_server_create.argtypes = [i32, C.c_uint64, i32, C.c_int64, i32, C.POINTER(P)]
     lib.prism_server_add_table.argtypes = [P, P, i32, C.POINTER(i32)]
     lib.prism_serve_probe.argtypes = [P, i32, P, C.c_int64, C.POINTER(C.c_int64)]
@@ -467,6 +473,20 @@ def evaluate_predicate(batch, predicate: Predicate, ctx: Optional[Context] = Non
     h = C.c_void_p()
     ctx.check(lib().prism_evaluate_predicate(ctx.handle, d.handle, C.byref(p), C.byref(h)))
     return DeviceBatch(ctx, h).to_arrow().column(0)
+
+
+def sort_batch(batch, keys: Sequence[SortKey], limit: Optional[int] = None, ctx: Optional[Context] = None,
+               as_device=False):
+    """sort_batch / sort_batch_limit (sort.rs:35-78): the rows ordered by
+    `keys` (most significant first), the first `limit` of them when given.
+    topn_single_col (sort.rs:97-146) is a Float64 Desc key with a limit."""
+    ctx = ctx or default_context()
+    d = _dev(batch, ctx)
+    k = encode_sort_keys(keys)
+    h = C.c_void_p()
+    ctx.check(lib().prism_sort_batch(ctx.handle, d.handle, k, len(keys), -1 if limit is None else int(limit),
+                                     C.byref(h)))
+    return _result(ctx, h, as_device)
 
 
 def filter_batch(batch, mask, ctx: Optional[Context] = None, as_device=False):

@@ -132,6 +132,10 @@ class prism_agg_expr(C.Structure):
     _fields_ = [("column", C.c_int32), ("func", C.c_int32), ("output_name", C.c_char_p)]
 
 
+class prism_sort_key(C.Structure):
+    _fields_ = [("column", C.c_int32), ("descending", C.c_int32), ("nulls_first", C.c_int32)]
+
+
 class prism_agg_config(C.Structure):
     _fields_ = [
         ("n_group_by", C.c_int32),

@@ -42,6 +42,35 @@ class HashJoinConfig:
         return cfg
 
 
+class SortDirection(enum.IntEnum):
+    """SortDirection (sort.rs:13-17)."""
+    Asc = 0
+    Desc = 1
+
+
+class NullOrdering(enum.IntEnum):
+    """NullOrdering (sort.rs:20-24)."""
+    NullsFirst = 0
+    NullsLast = 1
+
+
+@dataclass
+class SortKey:
+    """SortKey (sort.rs:27-32)."""
+    column: int
+    direction: SortDirection = SortDirection.Asc
+    nulls: NullOrdering = NullOrdering.NullsLast
+
+
+def encode_sort_keys(keys):
+    arr = (_abi.prism_sort_key * max(1, len(keys)))()
+    for i, k in enumerate(keys):
+        arr[i].column = k.column
+        arr[i].descending = 1 if k.direction == SortDirection.Desc else 0
+        arr[i].nulls_first = 1 if k.nulls == NullOrdering.NullsFirst else 0
+    return arr
+
+
 class AggFunc(enum.IntEnum):
     Sum = 0
     Count = 1

@@ -12,6 +12,9 @@ import pyarrow as pa
 
 from prism_gpu.config import (
     AggExpr,
+    NullOrdering,
+    SortDirection,
+    SortKey,
     AggFunc,
     ArithmeticOp,
     HashAggConfig,
@@ -233,3 +236,22 @@ MERGE_CONFIG = HashAggConfig(
 )
 # after reconstruct: F=(130, 3, 130/3), O=(50, 1, 50), P=(70, 2, 35)
 MERGE_EXPECTED = {"F": (130.0, 3, 130.0 / 3.0), "O": (50.0, 1, 50.0), "P": (70.0, 2, 35.0)}
+
+
+# ---------------------------------------------------------------- sort -----
+# native/prism-executor/src/sort.rs:238-253 (test_batch)
+def sort_test_batch() -> pa.RecordBatch:
+    schema = pa.schema([pa.field("name", pa.utf8(), nullable=False), pa.field("age", pa.int64(), nullable=False),
+                        pa.field("score", pa.float64(), nullable=False)])
+    return pa.RecordBatch.from_arrays(
+        [pa.array(["Charlie", "Alice", "Bob", "Dave", "Eve"]), pa.array([30, 25, 25, 35, 28], pa.int64()),
+         pa.array([85.5, 92.0, 88.0, 76.0, 92.0])], schema=schema)
+
+
+# sort.rs:255-266 test_sort_by_name_asc: names[0] == "Alice", names[4] == "Eve"
+SORT_BY_NAME_ASC = [SortKey(0, SortDirection.Asc, NullOrdering.NullsLast)]
+# sort.rs:268-279 test_sort_by_score_desc_limit: 3 rows, scores[0] == 92.0
+SORT_BY_SCORE_DESC = [SortKey(2, SortDirection.Desc, NullOrdering.NullsLast)]
+# sort.rs:281-299 test_multi_key_sort: ages[0] == 25, scores[0] == 92.0
+SORT_MULTI_KEY = [SortKey(1, SortDirection.Asc, NullOrdering.NullsLast),
+                  SortKey(2, SortDirection.Desc, NullOrdering.NullsLast)]

@@ -24,7 +24,9 @@ from prism_gpu.config import (  # noqa: E402
     HashJoinConfig,
     Predicate,
     ScalarExpr,
+    SortKey,
     encode_exprs,
+    encode_sort_keys,
 )
 
 ORACLE_DIR = os.path.join(ROOT, "oracle")
@@ -149,6 +151,15 @@ def evaluate_predicate(batch: pa.RecordBatch, predicate: Predicate) -> pa.Array:
     a, s = _out()
     _check(lib().oracle_evaluate_predicate(e.array_ptr, e.schema_ptr, C.byref(p), C.byref(a), C.byref(s)))
     return _take(a, s).column(0)
+
+
+def sort_batch(batch: pa.RecordBatch, keys: Sequence[SortKey], limit: Optional[int] = None) -> pa.RecordBatch:
+    e = _abi.ExportedBatch(batch)
+    k = encode_sort_keys(keys)
+    a, s = _out()
+    _check(lib().oracle_sort_batch(e.array_ptr, e.schema_ptr, k, len(keys), C.c_int64(-1 if limit is None else limit),
+                                   C.byref(a), C.byref(s)))
+    return _take(a, s)
 
 
 def filter_batch(batch: pa.RecordBatch, mask: pa.Array) -> pa.RecordBatch:
