@@ -51,7 +51,7 @@ SCALE = 1.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "sort", "topn"], default="c2")
     ap.add_argument("--requests", type=int, default=10_000, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="c5: Poisson arrival rate (requests/s)")
     ap.add_argument("--steps", type=int, default=None)
@@ -64,7 +64,7 @@ def parse():
                     help="scale all sizes (profiling captures use a smaller case; bench lines use 1.0)")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1}[a.workload]
+        a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1, "sort": 10, "topn": 10}[a.workload]
     global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE
     SCALE = a.scale
     if a.scale != 1.0:
@@ -197,7 +197,11 @@ def main():
     bk, bp, pk, pp = gen_c2(torch, device, seed=1234 + rank)
     torch.cuda.synchronize()
     ctx = prism_gpu.Context(local)
-    stream = torch.cuda.current_stream(device)
+    # one created stream for torch's work, the events and the library (the
+    # default stream's handle 0 would give the library its own stream, which
+    # events on the default stream do not bracket)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     build_db = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", bk.data_ptr()), ("payload", "l", bp.data_ptr())], N_BUILD, ctx, local)
     probe_db = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", pk.data_ptr()), ("payload", "i", pp.data_ptr())], N_PROBE, ctx, local)
@@ -692,7 +696,90 @@ class C4:
                                              f"rows in 1M-row batches ({dt:.2f} s)")
 
 
-WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4}
+class SortW:
+    """ORDER BY a Float64 key over 100M rows (sort.rs:35-78), full or top-N."""
+    name = "sort"
+    dtype = "f64 key, int64 payload"
+    flush_l2 = False
+
+    def __init__(self, torch, device, ctx, rank, limit=None):
+        import prism_gpu
+        from prism_gpu import NullOrdering, SortDirection, SortKey
+
+        self.torch, self.ctx, self.pg = torch, ctx, prism_gpu
+        n = self.rows = sc(100_000_000)
+        self.limit = limit
+        g = torch.Generator(device=device)
+        g.manual_seed(600 + rank)
+        self.key = torch.randn(n, generator=g, device=device, dtype=torch.float64)
+        self.row = torch.arange(n, device=device, dtype=torch.int64)
+        self.batch = prism_gpu.DeviceBatch.from_device_buffers(
+            [("x", "g", self.key.data_ptr()), ("row", "l", self.row.data_ptr())], n, ctx, device.index)
+        self.keys = [SortKey(0, SortDirection.Desc, NullOrdering.NullsLast)]
+        self.workload = (f"ORDER BY x DESC{'' if limit is None else f' LIMIT {limit}'} over {n:,} rows (x float64 "
+                         "normal(0,1), row int64): stable LSD radix sort, 8 passes of 8 bits, then the gather")
+
+    def step(self):
+        self.pg.sort_batch(self.batch, self.keys, limit=self.limit, ctx=self.ctx, as_device=True).free()
+
+    def check(self):
+        t = self.torch
+        got = self.pg.sort_batch(self.batch, self.keys, limit=self.limit, ctx=self.ctx, as_device=True)
+        m = got.num_rows
+        self.ctx.synchronize()
+        ptr, _, _ = got.column_device(1)
+        rows = t.as_tensor(_DevView(ptr, m), device=self.key.device).clone()
+        got.free()
+        exp = t.sort(self.key, descending=True, stable=True).indices[:m]
+        assert t.equal(rows, exp), "row order differs from torch's stable descending sort"
+        return {"full_size_check": "row order equals torch.sort(descending, stable) at full size"}
+
+    def roofline(self, kstats):
+        n, ms = kstats.get("radix_scatter_kernel", (0, 0.0))
+        return {"kernel": "radix_scatter_kernel (one radix pass)", "bytes": 24 * self.rows, "ms": ms / max(1, n),
+                "per_unit": "24 B per row per pass (8-byte order word + 4-byte row id, read and written)",
+                "traffic_key": "sort_pass"}
+
+    def host_batch(self):
+        import pyarrow as pa
+
+        t = self.torch
+        schema = pa.schema([pa.field("x", pa.float64(), nullable=False), pa.field("row", pa.int64(), nullable=False)])
+        return pa.RecordBatch.from_arrays([host_array(t, pa, self.key, pa.float64()), host_array(t, pa, self.row, pa.int64())],
+                                          schema=schema)
+
+    def e2e_inputs(self):
+        return [self.host_batch()]
+
+    def e2e_step(self, hb):
+        return self.pg.sort_batch(hb[0], self.keys, limit=self.limit, ctx=self.ctx)
+
+    def cpu_baseline(self, threads):
+        o = oracle_mod()
+        s = min(self.rows, 10_000_000)
+        hb = self.host_batch().slice(0, s)
+        t0 = time.perf_counter()
+        o.sort_batch(hb, self.keys, limit=self.limit)
+        dt = time.perf_counter() - t0
+        return s / dt, 1, (f"oracle stable sort of the first {s:,} rows on one thread (the reference sorts one "
+                           f"RecordBatch with arrow's lexsort on one thread, sort.rs:35-54) ({dt:.2f} s)")
+
+
+class _DevView:
+    """__cuda_array_interface__ over an int64 device column another object owns."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False), "version": 3}
+
+
+class TopNW(SortW):
+    name = "topn"
+
+    def __init__(self, torch, device, ctx, rank):
+        super().__init__(torch, device, ctx, rank, limit=100)
+
+
+WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4, "sort": SortW, "topn": TopNW}
 
 
 def gpu_index_of(local):
@@ -737,7 +824,11 @@ def run_workload(args, rank, world, local, torch, dist):
 
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     ctx = prism_gpu.Context(local)
-    stream = torch.cuda.current_stream(device)
+    # one created stream for torch's work, the events and the library (the
+    # default stream's handle 0 would give the library its own stream, which
+    # events on the default stream do not bracket)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     W = Wc(torch, device, ctx, rank)
     torch.cuda.synchronize()
@@ -766,7 +857,7 @@ def run_workload(args, rank, world, local, torch, dist):
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
     names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
-             "join_agg_jit", "predicate_kernel", "expr_kernel")
+             "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
     ctx.set_profiling(False)
     t = torch.tensor([ms], device=device, dtype=torch.float64)
@@ -871,7 +962,8 @@ def run_c5(args, rank, world, local, torch, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = prism_gpu.Context(local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     g = torch.Generator(device=dev)
     g.manual_seed(500 + rank)

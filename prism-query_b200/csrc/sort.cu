@@ -56,27 +56,56 @@ __global__ void __launch_bounds__(RB) radix_hist_kernel(const uint64_t* __restri
   counts[(int64_t)tid * ntiles + blockIdx.x] = h[tid];
 }
 
+// Stable scatter of one tile: every element's rank inside the tile's
+// digit-ordered sequence is computed in tile order (rounds of RB elements:
+// warp match for ranks inside a warp, per-warp digit counts across warps),
+// the tile is staged in shared memory in that order, and then written out
+// with consecutive threads on consecutive positions, so each digit's run of
+// the tile lands as one contiguous (coalesced) stretch of the output.
+// Dynamic shared memory: RT keys + RT row ids.
+constexpr size_t SCATTER_SMEM = (size_t)RT * (8 + 4);
 __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __restrict__ kin,
                                                             const uint32_t* __restrict__ vin, int64_t n, int shift,
-                                                            uint32_t mask, const uint64_t* __restrict__ offsets,
-                                                            int64_t ntiles, uint64_t* __restrict__ kout,
-                                                            uint32_t* __restrict__ vout) {
+                                                            uint32_t mask, const uint32_t* __restrict__ counts,
+                                                            const uint64_t* __restrict__ offsets, int64_t ntiles,
+                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+  extern __shared__ unsigned long long stage[];  // [RT] keys | [RT] row ids
+  uint64_t* sk = reinterpret_cast<uint64_t*>(stage);
+  uint32_t* sv = reinterpret_cast<uint32_t*>(stage + RT);
+  __shared__ uint32_t start[256];    // tile-local start of each digit's run
   __shared__ uint32_t run[256];      // elements of each digit this tile has placed
   __shared__ uint32_t wc[RW][256];   // this round: each warp's count per digit
+  __shared__ uint32_t total[RW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  run[tid] = 0;
+  const int64_t base = (int64_t)blockIdx.x * RT;
+  const int count = (int)min((int64_t)RT, n - base);
+  // tile-local digit starts: exclusive scan of this tile's digit counts
 #pragma unroll
   for (int w = 0; w < RW; ++w) wc[w][tid] = 0;
+  {
+    const uint32_t x = counts[(int64_t)tid * ntiles + blockIdx.x];
+    uint32_t incl = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    if (lane == 31) total[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += total[w];
+    start[tid] = before + incl - x;
+    run[tid] = 0;
+  }
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * RT;
   for (int r = 0; r < RR; ++r) {
-    const int64_t i = base + r * RB + tid;
-    const bool valid = i < n;
+    const int e = r * RB + tid;
+    const bool valid = e < count;
     uint64_t key = 0;
     uint32_t val = 0, d = 256u;  // 256: no element
     if (valid) {
-      key = kin[i];
-      val = vin[i];
+      key = kin[base + e];
+      val = vin[base + e];
       d = (uint32_t)(key >> shift) & mask;
     }
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -86,9 +115,9 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
     if (valid) {
       uint32_t before = run[d];
       for (int w = 0; w < warp; ++w) before += wc[w][d];
-      const uint64_t pos = offsets[(int64_t)d * ntiles + blockIdx.x] + before + rank;
-      kout[pos] = key;
-      vout[pos] = val;
+      const uint32_t at = start[d] + before + rank;
+      sk[at] = key;
+      sv[at] = val;
     }
     __syncthreads();
     uint32_t s = 0;
@@ -99,6 +128,15 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
     }
     run[tid] += s;
     __syncthreads();
+  }
+  // staged element j belongs to digit d(j); its output position is the
+  // digit's global offset for this tile plus its rank inside the digit's run
+  for (int j = tid; j < count; j += RB) {
+    const uint64_t key = sk[j];
+    const uint32_t d = (uint32_t)(key >> shift) & mask;
+    const uint64_t pos = offsets[(int64_t)d * ntiles + blockIdx.x] + (uint32_t)(j - start[d]);
+    kout[pos] = key;
+    vout[pos] = sv[j];
   }
 }
 
@@ -213,6 +251,7 @@ struct Sorter {
     total = ctx.alloc_t<uint64_t>(1, mt);
     iota_u32_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(va, n);
     ctx.check_launch("iota_u32_kernel");
+    PRISM_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SCATTER_SMEM));
   }
   int grid() const { return grid_for(ctx, n, 256); }
   // stable sort of (ka, va) by the low `bits` bits of ka, 8 per pass
@@ -225,7 +264,8 @@ struct Sorter {
       scan_u32_async(ctx, counts, offsets, ntiles * 256, total);
       {
         KernelTimer kt(ctx, "radix_scatter_kernel");
-        radix_scatter_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(ka, va, n, shift, mask, offsets, ntiles, kb, vb);
+        radix_scatter_kernel<<<(unsigned)ntiles, RB, SCATTER_SMEM, ctx.stream>>>(ka, va, n, shift, mask, counts, offsets,
+                                                                                  ntiles, kb, vb);
       }
       ctx.check_launch("radix_scatter_kernel");
       std::swap(ka, kb);
