@@ -777,6 +777,14 @@ class TopNW(SortW):
 
     def __init__(self, torch, device, ctx, rank):
         super().__init__(torch, device, ctx, rank, limit=100)
+        self.workload = (f"ORDER BY x DESC LIMIT 100 over {self.rows:,} rows (x float64 normal(0,1), row int64): "
+                         "radix select (a digit histogram of every row, then of the narrowed rows), stable sort of "
+                         "the survivors, gather")
+
+    def roofline(self, kstats):
+        n, ms = kstats.get("select_hist_kernel", (0, 0.0))
+        return {"kernel": "select_hist_kernel (first level: every row's top digit)", "bytes": 8 * self.rows,
+                "ms": ms / max(1, n), "per_unit": "8 B per row (the Float64 key read once)", "traffic_key": "topn_select"}
 
 
 WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4, "sort": SortW, "topn": TopNW}
@@ -857,7 +865,7 @@ def run_workload(args, rank, world, local, torch, dist):
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
     names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
-             "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel")
+             "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel", "select_hist_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
     ctx.set_profiling(False)
     t = torch.tensor([ms], device=device, dtype=torch.float64)

@@ -230,6 +230,55 @@ __global__ void max_len_kernel(DCol c, int64_t n, unsigned int* out) {
   if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+// ---------------------------------------------------- top-N selection --
+// One fixed-width key: its order word with the null rank above the value
+// bits (`bits` value bits, `nb` = 1 when the column has nulls).
+__device__ __forceinline__ uint64_t select_word(const DCol& c, int64_t row, int bits, bool desc, int nb,
+                                                bool nulls_first) {
+  uint64_t w = fixed_word(c, row, bits, desc);
+  if (nb) {
+    const bool valid = dcol_valid(c, row);
+    w |= (uint64_t)(nulls_first ? valid : !valid) << bits;
+  }
+  return w;
+}
+
+// digit (w >> shift) & 255 of the rows whose word above the digit equals `prefix`
+__global__ void select_hist_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t m, int bits, int desc, int nb,
+                                   int nulls_first, int shift, int top, uint64_t prefix, uint32_t* hist) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = rows ? rows[i] : i;
+    const uint64_t w = select_word(c, row, bits, desc != 0, nb, nulls_first != 0);
+    if (top || (w >> (shift + 8)) == prefix) atomicAdd(&h[(w >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+// bit i set when row i's word above `shift` is at most `bound` (kept)
+__global__ void select_flags_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t m, int bits, int desc, int nb,
+                                    int nulls_first, int shift, uint64_t bound, uint32_t* words) {
+  const int64_t nw = (m + 31) / 32;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nw * 32; i += (int64_t)gridDim.x * blockDim.x) {
+    bool keep = false;
+    if (i < m) {
+      const int64_t row = rows ? rows[i] : i;
+      keep = (select_word(c, row, bits, desc != 0, nb, nulls_first != 0) >> shift) <= bound;
+    }
+    const uint32_t b = __ballot_sync(0xffffffffu, keep);
+    if ((threadIdx.x & 31) == 0) words[i >> 5] = b;
+  }
+}
+
+__global__ void gather_rows_kernel(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ idx, int64_t m,
+                                   uint32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = rows ? rows[idx[i]] : idx[i];
+}
+
 struct Sorter {
   Ctx& ctx;
   int64_t n, ntiles;
@@ -241,7 +290,8 @@ struct Sorter {
   MemP mka, mkb, mva, mvb, mc, mo, mt;
   int64_t passes = 0;
 
-  Sorter(Ctx& c, int64_t rows) : ctx(c), n(rows), ntiles(ceil_div(rows, (int64_t)RT)) {
+  // rows to sort: `init` (ordered, n entries) or, when null, 0..n-1
+  Sorter(Ctx& c, int64_t rows, const uint32_t* init = nullptr) : ctx(c), n(rows), ntiles(ceil_div(rows, (int64_t)RT)) {
     ka = ctx.alloc_t<uint64_t>((size_t)n, mka);
     kb = ctx.alloc_t<uint64_t>((size_t)n, mkb);
     va = ctx.alloc_t<uint32_t>((size_t)n, mva);
@@ -249,8 +299,12 @@ struct Sorter {
     counts = ctx.alloc_t<uint32_t>((size_t)ntiles * 256, mc);
     offsets = ctx.alloc_t<uint64_t>((size_t)ntiles * 256, mo);
     total = ctx.alloc_t<uint64_t>(1, mt);
-    iota_u32_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(va, n);
-    ctx.check_launch("iota_u32_kernel");
+    if (init) {
+      PRISM_CUDA(cudaMemcpyAsync(va, init, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+    } else {
+      iota_u32_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(va, n);
+      ctx.check_launch("iota_u32_kernel");
+    }
     PRISM_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SCATTER_SMEM));
   }
   int grid() const { return grid_for(ctx, n, 256); }
@@ -298,7 +352,65 @@ Batch sort_batch(Ctx& ctx, const Batch& b, const prism_sort_key* keys, int n_key
   if (b.rows == 0 || n_keys == 0) return b;  // sort.rs:36-38: the batch as it is
   if (b.rows >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "sort input exceeds 2^32-1 rows");
   const int64_t n = b.rows;
-  Sorter s(ctx, n);
+  // top-N of one fixed-width key: radix select narrows the rows to those
+  // whose order word is at most the limit-th smallest (ordered compaction,
+  // so ties keep their input order), and only those are sorted
+  MemP msel;
+  const uint32_t* sel = nullptr;
+  int64_t m = n;
+  if (n_keys == 1 && limit >= 0 && limit <= n / 4) {
+    const Column& col = *b.cols[keys[0].column];
+    const int bits = key_bits(col.type);
+    const int nb = col.validity ? 1 : 0;
+    if (bits && bits + nb <= 64) {
+      const DCol c = col.view();
+      const int desc = keys[0].descending ? 1 : 0, nf = keys[0].nulls_first ? 1 : 0;
+      const int total_bits = bits + nb;
+      MemP mh, mw;
+      uint32_t* hist = ctx.alloc_t<uint32_t>(256, mh);
+      uint64_t prefix = 0, below = 0;
+      for (int shift = ((total_bits - 1) / 8) * 8; shift >= 0 && m > std::max<int64_t>(65536, 2 * limit); shift -= 8) {
+        PRISM_CUDA(cudaMemsetAsync(hist, 0, 256 * 4, ctx.stream));
+        const bool top = shift + 8 >= 64;
+        {
+          KernelTimer kt(ctx, sel ? "select_hist_kernel(narrowed)" : "select_hist_kernel");  // the first reads every row
+          select_hist_kernel<<<grid_for(ctx, m, 256), 256, 0, ctx.stream>>>(c, sel, m, bits, desc, nb, nf, shift,
+                                                                            top ? 1 : 0, prefix, hist);
+        }
+        ctx.check_launch("select_hist_kernel");
+        std::vector<uint32_t> h(256);
+        PRISM_CUDA(cudaMemcpyAsync(h.data(), hist, 256 * 4, cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        int dig = 0;
+        uint64_t cum = below;
+        for (; dig < 256; ++dig) {
+          if (cum + h[dig] >= (uint64_t)std::max<int64_t>(limit, 1)) break;
+          cum += h[dig];
+        }
+        if (dig == 256) dig = 255;
+        below = cum;
+        prefix = (prefix << 8) | (uint64_t)dig;
+        // keep the rows whose word down to this digit is at most the prefix
+        uint32_t* words = ctx.alloc_t<uint32_t>((size_t)((m + 31) / 32 + 1), mw);
+        select_flags_kernel<<<grid_for(ctx, m, 256), 256, 0, ctx.stream>>>(c, sel, m, bits, desc, nb, nf, shift, prefix,
+                                                                           words);
+        ctx.check_launch("select_flags_kernel");
+        int64_t kept = 0;
+        MemP idx = compact_bits(ctx, reinterpret_cast<const uint8_t*>(words), m, false, &kept);
+        MemP mnext;
+        uint32_t* next = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(kept, 1), mnext);
+        if (kept) {
+          gather_rows_kernel<<<grid_for(ctx, kept, 256), 256, 0, ctx.stream>>>(sel, static_cast<const uint32_t*>(idx->ptr),
+                                                                               kept, next);
+          ctx.check_launch("gather_rows_kernel");
+        }
+        msel = mnext;
+        sel = next;
+        m = kept;
+      }
+    }
+  }
+  Sorter s(ctx, m, sel);
   // keys from the least significant (last) to the most significant (first)
   for (int ki = n_keys - 1; ki >= 0; --ki) {
     const Column& col = *b.cols[keys[ki].column];
@@ -308,42 +420,42 @@ Batch sort_batch(Ctx& ctx, const Batch& b, const prism_sort_key* keys, int n_key
       MemP mm;
       unsigned int* dmax = ctx.alloc_t<unsigned int>(1, mm);
       PRISM_CUDA(cudaMemsetAsync(dmax, 0, 4, ctx.stream));
-      max_len_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, n, dmax);
+      max_len_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(c, n, dmax);
       ctx.check_launch("max_len_kernel");
       unsigned int maxlen = 0;
       PRISM_CUDA(cudaMemcpyAsync(&maxlen, dmax, 4, cudaMemcpyDeviceToHost, ctx.stream));
       ctx.sync();
-      encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, -1, desc, s.ka);
+      encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, m, -1, desc, s.ka);
       ctx.check_launch("encode_str_kernel");
       s.sort_word(32);
       for (int w = (int)((maxlen + 7) / 8) - 1; w >= 0; --w) {
-        encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, w, desc, s.ka);
+        encode_str_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, m, w, desc, s.ka);
         ctx.check_launch("encode_str_kernel");
         s.sort_word(64);
       }
     } else if (col.type == TY_DEC128) {
       for (int high = 0; high < 2; ++high) {
-        encode_dec_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, high, desc, s.ka);
+        encode_dec_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, m, high, desc, s.ka);
         ctx.check_launch("encode_dec_kernel");
         s.sort_word(64);
       }
     } else {
       const int bits = key_bits(col.type);
       if (!bits) fail(PRISM_ERR_INVALID_ARGUMENT, "unsupported sort key type");
-      encode_fixed_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, bits, desc, s.ka);
+      encode_fixed_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, m, bits, desc, s.ka);
       ctx.check_launch("encode_fixed_kernel");
       s.sort_word(bits);
     }
     if (col.validity) {
-      encode_null_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, n, keys[ki].nulls_first ? 1 : 0, s.ka);
+      encode_null_kernel<<<s.grid(), 256, 0, ctx.stream>>>(c, s.va, m, keys[ki].nulls_first ? 1 : 0, s.ka);
       ctx.check_launch("encode_null_kernel");
       s.sort_word(1);
     }
   }
-  const int64_t m = limit >= 0 ? std::min(limit, n) : n;
+  const int64_t outn = limit >= 0 ? std::min(limit, m) : m;
   Batch out;
-  out.rows = m;
-  for (auto& c : b.cols) out.cols.push_back(take(ctx, *c, s.va, nullptr, m, c->name, c->nullable));
+  out.rows = outn;
+  for (auto& c : b.cols) out.cols.push_back(take(ctx, *c, s.va, nullptr, outn, c->name, c->nullable));
   return out;  // stream-ordered: the sort buffers are freed after the gathers
 
 }

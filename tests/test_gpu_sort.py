@@ -118,3 +118,29 @@ def test_reference_known_answers(ctx):
     assert top.num_rows == 3 and top.column(2)[0].as_py() == 92.0
     multi = prism_gpu.sort_batch(b, K.SORT_MULTI_KEY, ctx=ctx)
     assert multi.column(1)[0].as_py() == 25 and multi.column(2)[0].as_py() == 92.0
+
+
+@pytest.mark.parametrize("kind", ["f64", "i32_nulls", "u8_nulls", "f32_desc_nulls_first", "bool", "i64_ties"])
+@pytest.mark.parametrize("limit", [0, 1, 100, 5000])
+def test_top_n_select(ctx, kind, limit):
+    """Top-N of one fixed-width key over 1.5M rows: the radix-select path
+    (rows narrowed before the sort) gives the oracle's rows, ties included."""
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    n = 1_500_000
+    if kind == "f64":
+        col, key = pa.array(rng.normal(0, 1, n)), SortKey(0, D.Desc, N.NullsLast)
+    elif kind == "i32_nulls":
+        col, key = pa.array(rng.integers(-1000, 1000, n).astype(np.int32), mask=rng.random(n) < 0.2), SortKey(0, D.Asc, N.NullsFirst)
+    elif kind == "u8_nulls":
+        col, key = pa.array(rng.integers(0, 256, n).astype(np.uint8), mask=rng.random(n) < 0.01), SortKey(0, D.Desc, N.NullsLast)
+    elif kind == "f32_desc_nulls_first":
+        col, key = pa.array(rng.normal(0, 1, n).astype(np.float32), mask=rng.random(n) < 0.001), SortKey(0, D.Desc, N.NullsFirst)
+    elif kind == "bool":
+        col, key = pa.array(rng.random(n) < 0.001), SortKey(0, D.Desc, N.NullsLast)
+    else:
+        col, key = pa.array(rng.integers(0, 3, n)), SortKey(0, D.Asc, N.NullsLast)
+    b = pa.RecordBatch.from_arrays([col, pa.array(np.arange(n))], names=["k", "row"])
+    got = prism_gpu.sort_batch(b, [key], limit=limit, ctx=ctx)
+    ref = oracle.sort_batch(b, [key], limit=limit)
+    assert got.num_rows == ref.num_rows == limit
+    assert got.column(1).equals(ref.column(1))
