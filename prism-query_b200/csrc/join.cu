@@ -429,14 +429,16 @@ __global__ void __launch_bounds__(QB, 4) probe_rows_dense_kernel(const int64_t* 
 #pragma unroll
   for (int it = 0; it < QI; ++it) {
     int64_t r = base + it * QB + threadIdx.x;
-    d[it] = r < n ? (uint64_t)__ldg(keys + r) - (uint64_t)dmin : ~0ULL;
+    // the key and row-word streams are touched once: evict-first loads and
+    // stores, so they do not push the dense table out of L2
+    d[it] = r < n ? (uint64_t)__ldcs(keys + r) - (uint64_t)dmin : ~0ULL;
   }
   uint32_t cnt = 0;
 #pragma unroll
   for (int it = 0; it < QI; ++it) {
     int64_t r = base + it * QB + threadIdx.x;
     uint32_t row = d[it] < drange ? __ldg(dense + d[it]) : NO_MATCH;
-    if (r < n) rowv[r] = row;
+    if (r < n) __stcs(rowv + r, row);
     cnt += (r < n && row != NO_MATCH) ? 1u : 0u;
   }
 #pragma unroll
@@ -494,7 +496,7 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
 #pragma unroll
   for (int it = 0; it < QI; ++it) {
     int64_t r = base + it * QB + threadIdx.x;
-    v[it] = r < n ? __ldg(rowv + r) : NO_MATCH;
+    v[it] = r < n ? __ldcs(rowv + r) : NO_MATCH;
     uint32_t m = __ballot_sync(0xffffffffu, v[it] != NO_MATCH);
     lpos[it] = __popc(m & ((1u << lane) - 1u));
     if (lane == 0) seg[it][warp] = __popc(m);
@@ -534,10 +536,10 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
       atomicOr(a.err, DERR_CAPACITY);
       continue;
     }
-    if (one8) {
-      if (a.out_probe) a.out_probe[pos] = (uint32_t)(base + it * QB + threadIdx.x);
-      if (a.out_build) a.out_build[pos] = v[it];
-      static_cast<unsigned long long*>(a.g_dst[0])[pos] = pre[it];
+    if (one8) {  // output streams: evict-first stores
+      if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(base + it * QB + threadIdx.x));
+      if (a.out_build) __stcs(a.out_build + pos, v[it]);
+      __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it]);
     } else {
       emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
     }
