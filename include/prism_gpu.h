@@ -428,6 +428,55 @@ int prism_sort_batch(prism_ctx* ctx, const prism_batch* batch, const prism_sort_
                      int64_t limit, prism_batch** out);
 
 /* ------------------------------------------------------------------------ */
+/* Distributed aggregation: the exchange step                               */
+/* (native/prism-bench/src/handler.rs:270-344)                              */
+/* ------------------------------------------------------------------------ */
+/* The reference runs the aggregation on every worker with AVG expanded into
+ * SUM + COUNT, ships each worker's partial batch to a reducer over Flight,
+ * and merges there. The replacement: each GPU computes its partial with
+ * prism_hash_aggregate_batches (or the fused paths) under the expanded
+ * config, packs it into one device buffer, the buffers are all-gathered
+ * (ncclAllGather over NVLink; pad every rank's buffer to the largest size),
+ * and every rank unpacks them and merges on the GPU.
+ *
+ * expand_worker_aggregates (handler.rs:397-428): writes the worker
+ * aggregate list of `original` (AVG -> SUM then COUNT of its column, every
+ * other aggregate unchanged, output names "agg_<i>" with process lifetime)
+ * into out_aggs (room for 2 * original->n_aggs entries); *n_out = its
+ * length. Group-by columns are unchanged. Host-only; no context needed. */
+int prism_expand_worker_aggregates(const prism_agg_config* original, prism_agg_expr* out_aggs,
+                                   int32_t capacity, int32_t* n_out);
+
+/* Bytes prism_batch_pack writes for `batch` (a multiple of 16). */
+int prism_batch_packed_size(const prism_batch* batch, uint64_t* size);
+
+/* Writes `batch` (header + every buffer, 16-byte aligned) into the device
+ * buffer device_dst of `capacity` bytes, stream-ordered on the context's
+ * stream: synchronise it (or order on it) before a collective reads the
+ * buffer. No counterpart in the reference (Flight IPC encoding,
+ * handler.rs:570-624). */
+int prism_batch_pack(prism_ctx* ctx, const prism_batch* batch, void* device_dst, uint64_t capacity);
+
+/* Reads a packed batch from device memory [device_src, device_src + size)
+ * into a new device batch that owns a copy of the payload (the source may be
+ * reused once this returns). Checks the header and every buffer range
+ * against `size`; synchronises the context's stream. */
+int prism_batch_unpack(prism_ctx* ctx, const void* device_src, uint64_t size, prism_batch** out);
+
+/* The reducer merge (handler.rs:327-344): hash_aggregate_batches over the
+ * partials (in the given order: the reference puts the reducer's own first,
+ * then its peers) with build_final_merge_config (handler.rs:430-457: SUM for
+ * SUM / COUNT / COUNT DISTINCT partials, MIN / MAX for MIN / MAX), then
+ * reconstruct_original_aggregate_batch (handler.rs:459-530): the group
+ * columns, then per original aggregate COUNT / COUNT DISTINCT as Int64, AVG
+ * as SUM / COUNT (0 when the count is 0), SUM / MIN / MAX as Float64, a null
+ * read as 0. Every partial has original->n_group_by group columns followed by
+ * the expanded worker aggregates. COUNT DISTINCT merges by summing the
+ * workers' distinct counts, as the reference does. */
+int prism_merge_partial_aggregates(prism_ctx* ctx, const prism_batch* const* partials, int32_t n_partials,
+                                   const prism_agg_config* original, prism_batch** out);
+
+/* ------------------------------------------------------------------------ */
 /* Serving loop (prism_serve_submit/poll of the design)                       */
 /* ------------------------------------------------------------------------ */
 /* Requests of uneven sizes against resident tables, answered by worker

@@ -12,8 +12,8 @@
 
 namespace prism {
 
-constexpr int MAX_SRC = 8;
-constexpr int MAX_OPS = 16;
+constexpr int MAX_SRC = 16;
+constexpr int MAX_OPS = 24;
 constexpr int MAX_W = 64;
 constexpr int MAX_GCOLS = 8;
 constexpr int LIMBS = 6;  // f64 window: 6 x 32 bits

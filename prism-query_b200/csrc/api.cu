@@ -9,6 +9,7 @@
 
 #include "agg.hpp"
 #include "arrow_io.hpp"
+#include "exchange.hpp"
 #include "filter_project.hpp"
 #include "jit.hpp"
 #include "join.hpp"
@@ -767,6 +768,55 @@ int prism_sort_batch(prism_ctx* c, const prism_batch* b, const prism_sort_key* k
   return run(c, [&] {
     if (!out || (n_keys > 0 && !keys) || n_keys < 0) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
     *out = wrap(c, sort_batch(c->impl, B(b), keys, n_keys, limit));
+  });
+}
+
+// ------------------------------------------- distributed aggregation --
+int prism_expand_worker_aggregates(const prism_agg_config* original, prism_agg_expr* out_aggs, int32_t capacity,
+                                   int32_t* n_out) {
+  try {
+    if (!original || !n_out) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/output");
+    const WorkerAggs w = expand_worker_aggregates(*original);
+    *n_out = (int32_t)w.aggs.size();
+    if ((int32_t)w.aggs.size() > capacity || (!out_aggs && !w.aggs.empty()))
+      fail(PRISM_ERR_INVALID_ARGUMENT, "worker aggregate list longer than the output capacity");
+    for (size_t i = 0; i < w.aggs.size(); ++i) out_aggs[i] = w.aggs[i];
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+int prism_batch_packed_size(const prism_batch* b, uint64_t* size) {
+  try {
+    if (!size) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    *size = packed_size(B(b));
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+int prism_batch_pack(prism_ctx* c, const prism_batch* b, void* dst, uint64_t capacity) {
+  return run(c, [&] { pack_batch(c->impl, B(b), dst, capacity); });
+}
+
+int prism_batch_unpack(prism_ctx* c, const void* src, uint64_t size, prism_batch** out) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    *out = wrap(c, unpack_batch(c->impl, src, size));
+  });
+}
+
+int prism_merge_partial_aggregates(prism_ctx* c, const prism_batch* const* partials, int32_t n,
+                                   const prism_agg_config* original, prism_batch** out) {
+  return run(c, [&] {
+    if (!original || !out || n < 0 || (n > 0 && !partials)) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/partials/output");
+    std::vector<const Batch*> ps;
+    for (int i = 0; i < n; ++i) ps.push_back(&B(partials[i]));
+    *out = wrap(c, merge_partial_aggregates(c->impl, ps, *original, agg_tuning()));
   });
 }
 

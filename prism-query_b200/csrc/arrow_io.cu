@@ -404,7 +404,12 @@ struct Exporter {
       if (c.type == TY_UTF8) {
         auto ob = host((size_t)(n + 1) * 4);
         auto db = host((size_t)c.data_bytes);
-        d2h(ob->p, c.offsets, (size_t)(n + 1) * 4);
+        if (c.offsets) {
+          d2h(ob->p, c.offsets, (size_t)(n + 1) * 4);
+        } else {  // an empty result column built without buffers
+          if (n) fail(PRISM_ERR_INTERNAL, "Utf8 column without offsets");
+          std::memset(ob->p, 0, 4);
+        }
         d2h(db->p, c.data, (size_t)c.data_bytes);
         rebase_offs.push_back({static_cast<int32_t*>(ob->p), {n, c.data_base}});
         p->bufs.push_back(ob);

@@ -17,7 +17,8 @@
 // Every result equals the result of running the request alone.
 //
 // The reference has no serving loop; its analogue is the Flight action
-// handler answering one operator call at a time (prism-flight/src/handler.rs,
+// handler answering one operator call at a time (prism-flight/src/shuffle_writer.rs:294-349
+// calling prism-bench/src/handler.rs:78,
 // with PartitionStore as the resident-table registry,
 // shuffle_writer.rs:42-86).
 #include <algorithm>

@@ -122,6 +122,11 @@ def _declare(lib):
     lib.prism_server_last_error.restype = C.c_char_p
     lib.prism_server_destroy.argtypes = [P]
     lib.prism_server_destroy.restype = None
+    lib.prism_expand_worker_aggregates.argtypes = [P, P, i32, C.POINTER(i32)]
+    lib.prism_batch_packed_size.argtypes = [P, C.POINTER(C.c_uint64)]
+    lib.prism_batch_pack.argtypes = [P, P, P, C.c_uint64]
+    lib.prism_batch_unpack.argtypes = [P, P, C.c_uint64, C.POINTER(P)]
+    lib.prism_merge_partial_aggregates.argtypes = [P, P, i32, P, C.POINTER(P)]
     lib.prism_hash_join_arrow.argtypes = [P, P, P, P, P, P, P, P]
     lib.prism_hash_aggregate_arrow.argtypes = [P, P, P, P, P, P]
     lib.prism_filter_and_project_arrow.argtypes = [P, P, P, P, P, i32, P, P]
@@ -298,6 +303,27 @@ class DeviceBatch:
         self.ctx.check(lib().prism_batch_column_device(self._h, col, C.byref(v), C.byref(m), C.byref(w)))
         return int(v.value or 0), int(m.value or 0), int(w.value)
 
+    def packed_size(self) -> int:
+        """Bytes of this batch in the packed form (prism_batch_pack)."""
+        n = C.c_uint64(0)
+        rc = lib().prism_batch_packed_size(self._h, C.byref(n))
+        if rc:
+            raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+        return int(n.value)
+
+    def pack_into(self, device_ptr: int, capacity: int):
+        """Writes the packed batch to device memory at `device_ptr`
+        (stream-ordered on the context's stream)."""
+        self.ctx.check(lib().prism_batch_pack(self.ctx.handle, self._h, C.c_void_p(device_ptr), capacity))
+
+    @staticmethod
+    def unpack(device_ptr: int, size: int, ctx: Optional[Context] = None) -> "DeviceBatch":
+        """A batch read from a packed device buffer (the payload is copied)."""
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        ctx.check(lib().prism_batch_unpack(ctx.handle, C.c_void_p(device_ptr), size, C.byref(h)))
+        return DeviceBatch(ctx, h)
+
     def to_arrow(self) -> pa.RecordBatch:
         a, s = _abi.ArrowArray(), _abi.ArrowSchema()
         self.ctx.check(lib().prism_batch_export(self.ctx.handle, self._h, C.byref(a), C.byref(s)))
@@ -459,6 +485,34 @@ def hash_aggregate(batch, config: HashAggConfig, ctx: Optional[Context] = None, 
     cfg = config.encode()
     h = C.c_void_p()
     ctx.check(lib().prism_hash_aggregate(ctx.handle, d.handle, C.byref(cfg), C.byref(h)))
+    return _result(ctx, h, as_device)
+
+
+def expand_worker_aggregates(config: HashAggConfig) -> HashAggConfig:
+    """The worker-side config of a distributed aggregation
+    (expand_worker_aggregates, prism-bench/src/handler.rs:397-428): AVG
+    becomes SUM then COUNT of its column, every other aggregate stays; the
+    outputs are named agg_<i>."""
+    cfg = config.encode()
+    out = (_abi.prism_agg_expr * max(1, 2 * len(config.aggregates)))()
+    n = C.c_int32(0)
+    rc = lib().prism_expand_worker_aggregates(C.byref(cfg), out, 2 * len(config.aggregates), C.byref(n))
+    if rc:
+        raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+    aggs = [AggExpr(out[i].column, AggFunc(out[i].func), out[i].output_name.decode()) for i in range(n.value)]
+    return HashAggConfig(list(config.group_by), aggs)
+
+
+def merge_partial_aggregates(partials, config: HashAggConfig, ctx: Optional[Context] = None, as_device=False):
+    """The reducer merge of per-worker partial aggregates
+    (prism-bench/src/handler.rs:327-344) on the GPU: `partials` (Arrow or
+    device batches, reducer's own first) are outputs of
+    expand_worker_aggregates(config); the result has config's columns."""
+    ctx = ctx or default_context()
+    ds = [_dev(b, ctx) for b in partials]
+    cfg = config.encode()
+    h = C.c_void_p()
+    ctx.check(lib().prism_merge_partial_aggregates(ctx.handle, _ptrs(ds), len(ds), C.byref(cfg), C.byref(h)))
     return _result(ctx, h, as_device)
 
 

@@ -2,35 +2,30 @@
 
 The path shards without a data-path collective except one exchange step:
 
-* Aggregation: the input rows are split into contiguous shards in rank order;
-  every rank aggregates its shard on its own GPU into partial states (SUM,
-  COUNT, MIN/MAX with their counts); one all-gather exchanges the partial
-  tables (a few KB per rank at low cardinality); every rank merges them
-  (SUM and COUNT add, MIN/MAX over the partials that saw rows, AVG = SUM /
-  COUNT). This is the decomposition of the reference's distributed partial
-  aggregation (native/prism-flight/src/handler.rs:397-457 merging per-worker
-  partials; prism-substrait/src/executor.rs:710-774 for the fused join).
-  Because shards are contiguous and merged in rank order, the merged groups
-  come out in the same first-seen order as a single-GPU call.
+* Aggregation follows the reference's distributed aggregation
+  (native/prism-bench/src/handler.rs:270-344): the input rows are split into
+  contiguous shards in rank order; every rank aggregates its shard on its own
+  GPU under the worker config (expand_worker_aggregates: AVG -> SUM + COUNT);
+  the partial tables are exchanged by one all-gather and merged on the GPU by
+  the reducer's rule (hash aggregation of the partials with SUM / MIN / MAX,
+  then the original aggregates rebuilt). Between GPUs the exchange is one
+  NCCL all-gather of packed device buffers (prism_batch_pack /
+  prism_batch_unpack), so partial tables never leave HBM; over gloo (the CPU
+  tests) it is an all-gather of Arrow IPC bytes. The partials are merged in
+  the reducer's order (its own first, then the others in rank order), the
+  same on every rank, so every rank returns the reducer's result.
 * Joins: the build side is broadcast (every rank holds a replica) and each
   rank probes its own probe shard; the shards' outputs concatenated in rank
   order are the single-GPU output.
-
-The exchange runs on whatever backend the process group has: NCCL between
-GPUs, gloo in the CPU tests. The merge of the partial tables is host work on
-at most (groups x ranks) rows; the rows themselves are aggregated and joined
-on the GPU by the functions of this package.
 """
 from __future__ import annotations
 
 import io
-import struct
-from dataclasses import dataclass
 from typing import Callable, List, Optional, Sequence, Tuple
 
 import pyarrow as pa
 
-from .config import AggExpr, AggFunc, HashAggConfig
+from .config import HashAggConfig
 
 
 def shard_range(n: int, rank: int, world: int) -> Tuple[int, int]:
@@ -57,92 +52,12 @@ def shard_batches(batches: Sequence[pa.RecordBatch], rank: int, world: int) -> L
     return out
 
 
-@dataclass
-class _Part:
-    """How output aggregate i is rebuilt from the partial columns."""
-    func: AggFunc
-    value: int  # partial column of SUM / MIN / MAX
-    count: int  # partial column of the matching COUNT
-
-
-def partial_config(cfg: HashAggConfig) -> Tuple[HashAggConfig, List[_Part]]:
-    """The per-rank aggregation whose outputs merge exactly into `cfg`'s.
-
-    Output columns of the partial call: the group keys, then for every
-    aggregate of `cfg` its partial value and a COUNT of the same column
-    (the count decides AVG and whether a MIN/MAX partial saw rows).
-    COUNT DISTINCT does not decompose into partial results and is rejected.
-    """
-    aggs, parts = [], []
-    nk = len(cfg.group_by)
-    for i, a in enumerate(cfg.aggregates):
-        if a.func == AggFunc.CountDistinct:
-            raise ValueError("COUNT DISTINCT cannot be merged from per-rank partial results")
-        val_func = {AggFunc.Sum: AggFunc.Sum, AggFunc.Avg: AggFunc.Sum, AggFunc.Count: AggFunc.Count,
-                    AggFunc.Min: AggFunc.Min, AggFunc.Max: AggFunc.Max}[a.func]
-        aggs.append(AggExpr(a.column, val_func, f"p{i}_v"))
-        aggs.append(AggExpr(a.column, AggFunc.Count, f"p{i}_n"))
-        parts.append(_Part(a.func, nk + 2 * i, nk + 2 * i + 1))
-    return HashAggConfig(list(cfg.group_by), aggs), parts
-
-
-def _key_identity(col: pa.ChunkedArray, i: int):
-    """Group identity of a key value as the reference's FxHash sees it
-    (hash_aggregate.rs:492-504): a null numeric key hashes like 0, floats by
-    their bits (so -0.0 and +0.0 differ, and a null joins +0.0), other values
-    by value."""
-    v = col[i].as_py()
-    if pa.types.is_floating(col.type):
-        return ("f", 0 if v is None else struct.unpack("<q", struct.pack("<d", float(v)))[0])
-    if v is None and (pa.types.is_integer(col.type) or pa.types.is_boolean(col.type) or pa.types.is_date(col.type)):
-        return ("v", 0)
-    if isinstance(v, bool):
-        return ("v", int(v))
-    return ("v", v)
-
-
-def merge_partials(parts: Sequence[pa.RecordBatch], cfg: HashAggConfig, plan: List[_Part]) -> pa.RecordBatch:
-    """Merges partial tables (in rank order) into `cfg`'s output."""
-    parts = [p for p in parts if p is not None]
-    t = pa.Table.from_batches(parts) if parts else None
-    nk = len(cfg.group_by)
-    order, rows = [], {}
-    n = t.num_rows if t is not None else 0
-    keycols = [t.column(k) for k in range(nk)] if t is not None else []
-    vals = [t.column(j).to_pylist() for j in range(nk, t.num_columns)] if t is not None else []
-    for r in range(n):
-        ident = tuple(_key_identity(c, r) for c in keycols)
-        if ident not in rows:
-            rows[ident] = [r, []]
-            order.append(ident)
-        rows[ident][1].append(r)
-    out_cols, out_fields = [], []
-    for k in range(nk):
-        first = [rows[g][0] for g in order]
-        arr = t.column(k).take(pa.array(first, type=pa.int64())) if first else t.column(k).slice(0, 0)
-        out_cols.append(arr.combine_chunks() if isinstance(arr, pa.ChunkedArray) else arr)
-        out_fields.append(t.schema.field(k))
-    for i, (a, p) in enumerate(zip(cfg.aggregates, plan)):
-        v, c = vals[p.value - nk] if vals else [], vals[p.count - nk] if vals else []
-        res = []
-        for g in order:
-            rs = rows[g][1]
-            cnt = sum(c[r] for r in rs)
-            if a.func == AggFunc.Count:
-                res.append(int(sum(v[r] for r in rs)))
-            elif a.func == AggFunc.Sum:
-                res.append(float(sum(v[r] for r in rs)))
-            elif a.func == AggFunc.Avg:
-                res.append(float(sum(v[r] for r in rs)) / cnt if cnt else 0.0)
-            else:
-                seen = [v[r] for r in rs if c[r] > 0]
-                res.append((min(seen) if a.func == AggFunc.Min else max(seen)) if seen else 0.0)
-        typ = pa.int64() if a.func == AggFunc.Count else pa.float64()
-        out_cols.append(pa.array(res, type=typ))
-        out_fields.append(pa.field(a.output_name, typ))
-    if t is None:
-        raise ValueError("no partial results")
-    return pa.RecordBatch.from_arrays(out_cols, schema=pa.schema(out_fields))
+def reducer_order(world: int, reducer: int = 0) -> List[int]:
+    """Ranks in the order the reducer merges their partials: its own first,
+    then its peers by index (handler.rs:314-319)."""
+    if not 0 <= reducer < world:
+        raise ValueError("reducer out of range")
+    return [reducer] + [r for r in range(world) if r != reducer]
 
 
 def _to_bytes(batch: pa.RecordBatch) -> bytes:
@@ -168,6 +83,47 @@ def all_gather_batches(batch: pa.RecordBatch, group=None) -> List[pa.RecordBatch
     return [_from_bytes(b) for b in got]
 
 
+def all_gather_device_batches(batch, group=None) -> list:
+    """Every rank's device batch, in rank order, as device batches on this
+    rank's GPU: the batch is packed into one device buffer, the packed sizes
+    are all-gathered, every buffer is padded to the largest and one
+    all-gather moves them (NCCL over NVLink); each rank's piece is unpacked."""
+    import torch
+    import torch.distributed as dist
+
+    from . import DeviceBatch
+
+    world = dist.get_world_size(group)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    size = batch.packed_size()
+    sizes = torch.zeros(world, dtype=torch.int64, device=dev)
+    dist.all_gather_into_tensor(sizes, torch.tensor([size], dtype=torch.int64, device=dev), group=group)
+    host_sizes = [int(x) for x in sizes.tolist()]
+    cap = max(host_sizes)  # packed sizes are multiples of 16: every piece stays aligned
+    send = torch.empty(cap, dtype=torch.uint8, device=dev)
+    batch.pack_into(send.data_ptr(), cap)
+    batch.ctx.synchronize()
+    recv = torch.empty(world * cap, dtype=torch.uint8, device=dev)
+    dist.all_gather_into_tensor(recv, send, group=group)
+    torch.cuda.current_stream().synchronize()
+    return [DeviceBatch.unpack(recv.data_ptr() + r * cap, host_sizes[r], ctx=batch.ctx) for r in range(world)]
+
+
+def gather_partials(part, group=None, reducer: int = 0) -> list:
+    """Every rank's partial aggregate in the reducer's merge order: device
+    batches over an NCCL group, Arrow batches otherwise."""
+    import torch.distributed as dist
+
+    from . import DeviceBatch
+
+    world = dist.get_world_size(group)
+    if isinstance(part, DeviceBatch) and dist.get_backend(group) == "nccl":
+        every = all_gather_device_batches(part, group)
+    else:
+        every = all_gather_batches(part.to_arrow() if isinstance(part, DeviceBatch) else part, group)
+    return [every[r] for r in reducer_order(world, reducer)]
+
+
 def broadcast_batch(batch: Optional[pa.RecordBatch], src: int = 0, group=None) -> pa.RecordBatch:
     """`src`'s batch on every rank (one broadcast of Arrow IPC bytes)."""
     import torch.distributed as dist
@@ -177,49 +133,63 @@ def broadcast_batch(batch: Optional[pa.RecordBatch], src: int = 0, group=None) -
     return _from_bytes(obj[0])
 
 
-def sharded_hash_aggregate(local_batches: Sequence, cfg: HashAggConfig, group=None,
-                           local: Optional[Callable] = None, **kw) -> pa.RecordBatch:
-    """hash_aggregate_batches over the union of every rank's shard.
+def _merge(parts, cfg: HashAggConfig, merge: Optional[Callable], kw) -> pa.RecordBatch:
+    if merge:
+        return merge(parts, cfg)
+    from . import merge_partial_aggregates
 
-    local(batches, partial_cfg) computes this rank's partial table; by default
-    the GPU `hash_aggregate_batches` of this package (keyword arguments such as
-    `ctx` are passed on).
+    return merge_partial_aggregates(parts, cfg, **kw)
+
+
+def sharded_hash_aggregate(local_batches: Sequence, cfg: HashAggConfig, group=None, local: Optional[Callable] = None,
+                           merge: Optional[Callable] = None, reducer: int = 0, **kw) -> pa.RecordBatch:
+    """hash_aggregate_batches over the union of every rank's shard, as the
+    reference's distributed aggregation computes it.
+
+    local(batches, worker_cfg) computes this rank's partial table (default:
+    this package's GPU hash_aggregate_batches, kept in device memory);
+    merge(partials, cfg) merges them (default: the GPU merge). Keyword
+    arguments such as `ctx` are passed on to the defaults.
     """
-    from . import hash_aggregate_batches
+    from . import expand_worker_aggregates, hash_aggregate_batches
 
-    pcfg, plan = partial_config(cfg)
-    part = local(local_batches, pcfg) if local else hash_aggregate_batches(local_batches, pcfg, **kw)
-    return merge_partials(all_gather_batches(part, group), cfg, plan)
+    wcfg = expand_worker_aggregates(cfg)
+    part = local(local_batches, wcfg) if local else hash_aggregate_batches(local_batches, wcfg, as_device=True, **kw)
+    return _merge(gather_partials(part, group, reducer), cfg, merge, kw)
 
 
 def sharded_filter_project_aggregate(local_batches: Sequence, predicate, column_indices, expressions,
                                      cfg: HashAggConfig, group=None, local: Optional[Callable] = None,
-                                     **kw) -> pa.RecordBatch:
+                                     merge: Optional[Callable] = None, reducer: int = 0, **kw) -> pa.RecordBatch:
     """filter_project_aggregate over the union of every rank's shard."""
-    from . import filter_project_aggregate
+    from . import expand_worker_aggregates, filter_project_aggregate
 
-    pcfg, plan = partial_config(cfg)
+    wcfg = expand_worker_aggregates(cfg)
     if local:
-        part = local(local_batches, predicate, column_indices, expressions, pcfg)
+        part = local(local_batches, predicate, column_indices, expressions, wcfg)
     else:
-        part = filter_project_aggregate(local_batches, predicate, column_indices, expressions, pcfg, **kw)
-    return merge_partials(all_gather_batches(part, group), cfg, plan)
+        part = filter_project_aggregate(local_batches, predicate, column_indices, expressions, wcfg,
+                                        as_device=True, **kw)
+    return _merge(gather_partials(part, group, reducer), cfg, merge, kw)
 
 
 def sharded_join_aggregate(local_probes: Sequence, build: Optional[pa.RecordBatch], probe_keys, build_keys,
                            column_indices, expressions, cfg: HashAggConfig, group=None, src: int = 0,
-                           local: Optional[Callable] = None, **kw) -> pa.RecordBatch:
+                           local: Optional[Callable] = None, merge: Optional[Callable] = None, reducer: int = 0,
+                           **kw) -> pa.RecordBatch:
     """join_aggregate with the build side broadcast from `src` and the probe
-    rows sharded: partial aggregates per rank, merged after one all-gather."""
-    from . import join_aggregate
+    rows sharded: partial aggregates per rank, merged after one all-gather
+    (prism-substrait/src/executor.rs:333-842 on each worker)."""
+    from . import expand_worker_aggregates, join_aggregate
 
     build = broadcast_batch(build, src=src, group=group)
-    pcfg, plan = partial_config(cfg)
+    wcfg = expand_worker_aggregates(cfg)
     if local:
-        part = local(local_probes, build, probe_keys, build_keys, column_indices, expressions, pcfg)
+        part = local(local_probes, build, probe_keys, build_keys, column_indices, expressions, wcfg)
     else:
-        part = join_aggregate(local_probes, build, probe_keys, build_keys, column_indices, expressions, pcfg, **kw)
-    return merge_partials(all_gather_batches(part, group), cfg, plan)
+        part = join_aggregate(local_probes, build, probe_keys, build_keys, column_indices, expressions, wcfg,
+                              as_device=True, **kw)
+    return _merge(gather_partials(part, group, reducer), cfg, merge, kw)
 
 
 def sharded_hash_join(local_probe: pa.RecordBatch, build: Optional[pa.RecordBatch], config, group=None, src: int = 0,

@@ -13,7 +13,8 @@ probe row; GROUP BYs concatenated with a segment id as the first group key).
 Every result equals the result of running the request alone.
 
 This has no counterpart in the reference (its operators are called one at a
-time by the Flight handler, native/prism-flight/src/handler.rs).
+time by the Flight action handler, native/prism-flight/src/shuffle_writer.rs:294-349,
+which calls QueryHandler::execute, native/prism-bench/src/handler.rs:78).
 """
 from __future__ import annotations
 

@@ -234,6 +234,11 @@ MERGE_CONFIG = HashAggConfig(
         AggExpr(4, AggFunc.Sum, "agg_3"),
     ],
 )
+# the original aggregates of that test (handler.rs:1379-1395): SUM, COUNT, AVG of column 1
+MERGE_ORIGINAL = HashAggConfig(
+    group_by=[0],
+    aggregates=[AggExpr(1, AggFunc.Sum, "agg_0"), AggExpr(1, AggFunc.Count, "agg_1"), AggExpr(1, AggFunc.Avg, "agg_2")],
+)
 # after reconstruct: F=(130, 3, 130/3), O=(50, 1, 50), P=(70, 2, 35)
 MERGE_EXPECTED = {"F": (130.0, 3, 130.0 / 3.0), "O": (50.0, 1, 50.0), "P": (70.0, 2, 35.0)}
 

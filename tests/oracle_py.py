@@ -20,6 +20,8 @@ sys.path.insert(0, os.path.join(ROOT, "prism-query_b200"))
 from prism_gpu import _abi  # noqa: E402
 from prism_gpu.config import (  # noqa: E402
     ARITH_F64,
+    AggExpr,
+    AggFunc,
     HashAggConfig,
     HashJoinConfig,
     Predicate,
@@ -221,6 +223,73 @@ def join_aggregate(probes: List[pa.RecordBatch], build: pa.RecordBatch, probe_ke
     a, s = _out()
     _check(lib().oracle_join_aggregate(_ptr_array(eps), eps[0].schema_ptr, len(probes), eb.array_ptr, eb.schema_ptr, pk, bk, len(probe_keys), c, len(cols), ex, len(exprs), C.byref(cfg), n_threads, C.byref(a), C.byref(s)))
     return _take(a, s)
+
+
+# ------------------------------------------- distributed aggregation merge --
+def expand_worker_aggregates(config: HashAggConfig):
+    """expand_worker_aggregates (prism-bench/src/handler.rs:397-428):
+    (worker config, per original aggregate the worker indices it maps to)."""
+    aggs, mapping = [], []
+    for a in config.aggregates:
+        if a.func == AggFunc.Avg:
+            i = len(aggs)
+            aggs += [AggExpr(a.column, AggFunc.Sum, f"agg_{i}"), AggExpr(a.column, AggFunc.Count, f"agg_{i + 1}")]
+            mapping.append([i, i + 1])
+        else:
+            mapping.append([len(aggs)])
+            aggs.append(AggExpr(a.column, a.func, f"agg_{len(aggs)}"))
+    return HashAggConfig(list(config.group_by), aggs), mapping
+
+
+def _final_merge_config(nk: int, worker: HashAggConfig) -> HashAggConfig:
+    """build_final_merge_config (handler.rs:430-457)."""
+    def f(func):
+        return func if func in (AggFunc.Min, AggFunc.Max) else AggFunc.Sum
+    return HashAggConfig(list(range(nk)), [AggExpr(nk + i, f(a.func), a.output_name)
+                                           for i, a in enumerate(worker.aggregates)])
+
+
+def _as_f64(v) -> float:  # numeric_value_as_f64 (handler.rs:533-550): null reads 0
+    return 0.0 if v is None else float(v)
+
+
+def _as_i64(v) -> int:  # numeric_value_as_i64 (handler.rs:552-568): f64 `as i64` saturates, NaN -> 0
+    if v is None:
+        return 0
+    if isinstance(v, float):
+        if v != v:
+            return 0
+        if v >= 2.0 ** 63:
+            return 2 ** 63 - 1
+        if v <= -(2.0 ** 63):
+            return -(2 ** 63)
+        return int(v)
+    return int(v)
+
+
+def merge_partial_aggregates(partials: List[pa.RecordBatch], config: HashAggConfig, n_threads: int = DEFAULT_THREADS):
+    """The reducer (handler.rs:327-344): hash_aggregate_batches over the
+    partials with the final merge config, then
+    reconstruct_original_aggregate_batch (handler.rs:459-530)."""
+    nk = len(config.group_by)
+    worker, mapping = expand_worker_aggregates(config)
+    schema = partials[0].schema if partials else None
+    merged = hash_aggregate_batches(list(partials), _final_merge_config(nk, worker), n_threads, schema=schema)
+    cols = [merged.column(k) for k in range(nk)]
+    fields = [merged.schema.field(k) for k in range(nk)]
+    for a, m in zip(config.aggregates, mapping):
+        src = merged.column(nk + m[0]).to_pylist()
+        if a.func in (AggFunc.Count, AggFunc.CountDistinct):
+            arr = pa.array([_as_i64(v) for v in src], type=pa.int64())
+        elif a.func == AggFunc.Avg:
+            cnt = merged.column(nk + m[1]).to_pylist()
+            arr = pa.array([_as_f64(s) / _as_f64(c) if _as_f64(c) > 0 else 0.0 for s, c in zip(src, cnt)],
+                           type=pa.float64())
+        else:
+            arr = pa.array([_as_f64(v) for v in src], type=pa.float64())
+        cols.append(arr)
+        fields.append(pa.field(a.output_name, arr.type, True))
+    return pa.RecordBatch.from_arrays(cols, schema=pa.schema(fields))
 
 
 def exact_sum_f64(values) -> float:

@@ -1,9 +1,13 @@
 """Multi-rank host logic on CPU: two gloo ranks shard the rows, compute their
-partial tables (with the oracle standing in for each rank's GPU), exchange
-them, merge, and must reproduce the single-call result of the oracle — same
+partial tables under the reference's worker config (with the oracle standing
+in for each rank's GPU), exchange them, and merge them by the reference's
+reducer rule (the oracle's restatement of prism-bench/src/handler.rs:327-344).
+The merged result must reproduce the single-call result of the oracle — same
 groups in the same first-seen order, integer results exact, Float64 within
-1e-12. Joins: the build side is broadcast and the probe sharded; the
-rank-ordered concatenation must equal the single-call join."""
+1e-12 — where the decomposition is exact (no COUNT DISTINCT, no group whose
+values are all null on one rank). Joins: the build side is broadcast and the
+probe sharded; the rank-ordered concatenation must equal the single-call
+join."""
 import json
 import os
 import sys
@@ -63,20 +67,27 @@ def _rank_main(rank, world, store, outdir):
         # grouped: int key with nulls (null and 0 share a group, as in the reference)
         cfg = HashAggConfig([0], [AggExpr(1, F.Sum, "s"), AggExpr(1, F.Count, "n"), AggExpr(2, F.Avg, "a"),
                                   AggExpr(1, F.Min, "mn"), AggExpr(2, F.Max, "mx"), AggExpr(2, F.Sum, "sf")])
-        got = D.sharded_hash_aggregate(mine, cfg, local=lambda b, c: oracle.hash_aggregate_batches(b, c, n_threads=1))
+        local = lambda b, c: oracle.hash_aggregate_batches(b, c, n_threads=1)  # noqa: E731
+        merge = lambda p, c: oracle.merge_partial_aggregates(p, c, n_threads=1)  # noqa: E731
+        got = D.sharded_hash_aggregate(mine, cfg, local=local, merge=merge)
         ref = oracle.hash_aggregate_batches(data, cfg, n_threads=1)
         assert_batches_equal(got, ref, float_cols=(1, 3, 4, 5, 6))
+        # reducer 1 merges its own partial first: its groups lead
+        got1 = D.sharded_hash_aggregate(mine, cfg, local=local, merge=merge, reducer=1)
+        wcfg, _ = oracle.expand_worker_aggregates(cfg)
+        shards = [oracle.hash_aggregate_batches(D.shard_batches(data, r, world), wcfg, n_threads=1) for r in (1, 0)]
+        assert_batches_equal(got1, oracle.merge_partial_aggregates(shards, cfg, n_threads=1), float_cols=(1, 3, 4, 5, 6))
         # global (no GROUP BY): nulls skipped
         gcfg = HashAggConfig([], [AggExpr(1, F.Sum, "s"), AggExpr(1, F.Count, "n"), AggExpr(1, F.Avg, "a"),
                                   AggExpr(1, F.Min, "mn"), AggExpr(2, F.Max, "mx")])
-        got = D.sharded_hash_aggregate(mine, gcfg, local=lambda b, c: oracle.hash_aggregate_batches(b, c, n_threads=1))
+        got = D.sharded_hash_aggregate(mine, gcfg, local=local, merge=merge)
         ref = oracle.hash_aggregate_batches(data, gcfg, n_threads=1)
         assert_batches_equal(got, ref, float_cols=(0, 2, 3, 4))
         # fused filter -> project -> aggregate, GROUP BY a dictionary column
         pred = Predicate.Le(4, ScalarValue.Int32(2000))
         fcfg = HashAggConfig([0], [AggExpr(1, F.Sum, "s"), AggExpr(2, F.Avg, "a"), AggExpr(1, F.Count, "n")])
         got = D.sharded_filter_project_aggregate(
-            mine, pred, [3, 1, 2], [], fcfg,
+            mine, pred, [3, 1, 2], [], fcfg, merge=merge,
             local=lambda b, p, c, e, g: oracle.filter_project_aggregate(b, p, c, e, g, n_threads=1))
         ref = oracle.filter_project_aggregate(data, pred, [3, 1, 2], [], fcfg, n_threads=1)
         assert_batches_equal(got, ref, float_cols=(1, 2))
@@ -84,7 +95,7 @@ def _rank_main(rank, world, store, outdir):
         build, probes = _join_data()
         jcfg = HashAggConfig([0], [AggExpr(1, F.Sum, "s"), AggExpr(1, F.Count, "n")])
         got = D.sharded_join_aggregate(D.shard_batches(probes, rank, world), build if rank == 0 else None, [0], [0],
-                                       [3, 1], [], jcfg,
+                                       [3, 1], [], jcfg, merge=merge,
                                        local=lambda p, b, pk, bk, c, e, g: oracle.join_aggregate(p, b, pk, bk, c, e, g, n_threads=1))
         ref = oracle.join_aggregate(probes, build, [0], [0], [3, 1], [], jcfg, n_threads=1)
         assert_batches_equal(got, ref, float_cols=(1,))

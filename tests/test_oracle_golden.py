@@ -111,6 +111,33 @@ def test_distributed_partial_merge():
     assert rows == K.MERGE_EXPECTED
 
 
+def test_reducer_merge_reconstructs_original_aggregates():
+    """handler.rs:1378-1460 through the oracle's restatement of the whole
+    reducer (final merge config, hash aggregation, reconstruct)."""
+    out = oracle.merge_partial_aggregates(K.partial_batches(), K.MERGE_ORIGINAL)
+    assert out.schema.types == [pa.utf8(), pa.float64(), pa.int64(), pa.float64()]
+    rows = {r["status"]: (r["agg_0"], r["agg_1"], r["agg_2"]) for r in out.to_pylist()}
+    assert rows == K.MERGE_EXPECTED
+
+
+def test_worker_aggregate_expansion_matches_oracle():
+    """prism_expand_worker_aggregates (host-only C entry point) against the
+    oracle's restatement of expand_worker_aggregates (handler.rs:397-428)."""
+    import prism_gpu
+    from prism_gpu import AggExpr, AggFunc, HashAggConfig
+
+    F = AggFunc
+    cfg = HashAggConfig([2, 0], [AggExpr(1, F.Avg, "a"), AggExpr(3, F.Min, "b"), AggExpr(1, F.CountDistinct, "c"),
+                                 AggExpr(4, F.Avg, "d"), AggExpr(0, F.Count, "e"), AggExpr(5, F.Max, "f")])
+    got = prism_gpu.expand_worker_aggregates(cfg)
+    ref, mapping = oracle.expand_worker_aggregates(cfg)
+    assert got == ref
+    assert mapping == [[0, 1], [2], [3], [4, 5], [6], [7]]
+    assert [a.output_name for a in got.aggregates] == [f"agg_{i}" for i in range(8)]
+    assert prism_gpu.expand_worker_aggregates(K.MERGE_ORIGINAL).aggregates == [
+        AggExpr(1, F.Sum, "agg_0"), AggExpr(1, F.Count, "agg_1"), AggExpr(1, F.Sum, "agg_2"), AggExpr(1, F.Count, "agg_3")]
+
+
 def test_like_pipeline_count():
     # native/prism-executor/tests/integration.rs:302-340: '%coast%' matches 40,000 of 100K
     regions = ["east_coast", "west_coast", "central", "north_west", "south_east"]
