@@ -428,6 +428,50 @@ int prism_sort_batch(prism_ctx* ctx, const prism_batch* batch, const prism_sort_
                      int64_t limit, prism_batch** out);
 
 /* ------------------------------------------------------------------------ */
+/* Parquet scan (native/prism-executor/src/parquet_scan.rs)                 */
+/* ------------------------------------------------------------------------ */
+/* ParquetScanConfig (parquet_scan.rs:29-50), without target_schema. */
+typedef struct prism_parquet_scan_config {
+  const char* const* uris;        /* local paths or file:// URIs: a file, or a directory scanned for *.parquet */
+  int32_t n_uris;
+  const prism_predicate* predicate; /* NULL: no row-group skipping */
+  const int32_t* projection;      /* NULL: all columns */
+  int32_t n_projection;
+  int64_t batch_size;             /* rows per output batch (> 0) */
+  int32_t skip_expand;
+} prism_parquet_scan_config;
+
+typedef struct prism_parquet_scan_stats {
+  int64_t files, row_groups, row_groups_skipped, pages, compressed_bytes, decoded_bytes;
+} prism_parquet_scan_stats;
+
+/* parquet_scan (parquet_scan.rs:55-168): the files of every URI (sorted
+ * within a URI), their row groups minus those whose statistics rule the
+ * predicate out (row_group_might_match, parquet_scan.rs:355-469), the
+ * projected columns (ProjectionMask::roots: valid indices in file order; none
+ * valid reads all), decoded on the GPU into device batches of at most
+ * batch_size rows that never span row groups; with a projection shorter than
+ * the schema and skip_expand == 0 the batches are expanded back to the first
+ * file's schema with all-null columns (expand_projected_batches,
+ * parquet_scan.rs:471-526). *out is a library-allocated array of *n_out
+ * batches (free each with prism_batch_free, the array with prism_free_array);
+ * stats may be NULL. The GPU decoder reads flat schemas of BOOLEAN, INT32,
+ * DATE, INT64, FLOAT, DOUBLE and UTF8 byte-array columns, PLAIN and dictionary
+ * encodings, data pages V1 and V2, UNCOMPRESSED or SNAPPY chunks; other files
+ * fail with PRISM_ERR_INVALID_ARGUMENT, unreadable or malformed ones with
+ * PRISM_ERR_INTERNAL (the reference's PrismError::Internal). */
+int prism_parquet_scan(prism_ctx* ctx, const prism_parquet_scan_config* config, prism_batch*** out, int32_t* n_out,
+                       prism_parquet_scan_stats* stats);
+
+/* parquet_row_count (parquet_scan.rs:240-266): rows of the row groups the
+ * predicate (NULL: none) might match, from the footers alone. */
+int prism_parquet_row_count(const char* const* uris, int32_t n_uris, const prism_predicate* predicate,
+                            int64_t* count);
+
+/* Frees an array the library allocated (not the batches in it). */
+void prism_free_array(void* array);
+
+/* ------------------------------------------------------------------------ */
 /* Distributed aggregation: the exchange step                               */
 /* (native/prism-bench/src/handler.rs:270-344)                              */
 /* ------------------------------------------------------------------------ */

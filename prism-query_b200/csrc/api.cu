@@ -10,6 +10,7 @@
 #include "agg.hpp"
 #include "arrow_io.hpp"
 #include "exchange.hpp"
+#include "parquet.hpp"
 #include "filter_project.hpp"
 #include "jit.hpp"
 #include "join.hpp"
@@ -770,6 +771,57 @@ int prism_sort_batch(prism_ctx* c, const prism_batch* b, const prism_sort_key* k
     *out = wrap(c, sort_batch(c->impl, B(b), keys, n_keys, limit));
   });
 }
+
+// ---------------------------------------------------------------- parquet --
+int prism_parquet_scan(prism_ctx* c, const prism_parquet_scan_config* cfg, prism_batch*** out, int32_t* n_out,
+                       prism_parquet_scan_stats* stats) {
+  return run(c, [&] {
+    if (!cfg || !out || !n_out || (cfg->n_uris > 0 && !cfg->uris) || cfg->n_uris < 0 ||
+        (cfg->n_projection > 0 && !cfg->projection) || cfg->n_projection < 0)
+      fail(PRISM_ERR_INVALID_ARGUMENT, "null scan config/output");
+    *out = nullptr;
+    *n_out = 0;
+    ParquetScanArgs a;
+    for (int i = 0; i < cfg->n_uris; ++i) {
+      if (!cfg->uris[i]) fail(PRISM_ERR_INVALID_ARGUMENT, "null URI");
+      a.uris.push_back(cfg->uris[i]);
+    }
+    a.predicate = cfg->predicate;
+    a.has_projection = cfg->projection != nullptr;
+    if (a.has_projection) a.projection.assign(cfg->projection, cfg->projection + cfg->n_projection);
+    a.batch_size = cfg->batch_size;
+    a.skip_expand = cfg->skip_expand != 0;
+    ParquetScanStats st;
+    std::vector<Batch> bs = parquet_scan(c->impl, a, &st);
+    if (stats) *stats = {st.files, st.row_groups, st.row_groups_skipped, st.pages, st.compressed_bytes, st.decoded_bytes};
+    auto** arr = static_cast<prism_batch**>(std::malloc(sizeof(prism_batch*) * std::max<size_t>(bs.size(), 1)));
+    if (!arr) fail(PRISM_ERR_NO_MEMORY, "host allocation failed");
+    for (size_t i = 0; i < bs.size(); ++i) arr[i] = wrap(c, std::move(bs[i]));
+    *out = arr;
+    *n_out = (int32_t)bs.size();
+  });
+}
+
+int prism_parquet_row_count(const char* const* uris, int32_t n, const prism_predicate* pred, int64_t* count) {
+  try {
+    if (!count || n < 0 || (n > 0 && !uris)) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    std::vector<std::string> u;
+    for (int i = 0; i < n; ++i) {
+      if (!uris[i]) fail(PRISM_ERR_INVALID_ARGUMENT, "null URI");
+      u.push_back(uris[i]);
+    }
+    *count = parquet_row_count(u, pred);
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  } catch (const std::exception& e) {
+    t_err = e.what();
+    return PRISM_ERR_INTERNAL;
+  }
+}
+
+void prism_free_array(void* a) { std::free(a); }
 
 // ------------------------------------------- distributed aggregation --
 int prism_expand_worker_aggregates(const prism_agg_config* original, prism_agg_expr* out_aggs, int32_t capacity,

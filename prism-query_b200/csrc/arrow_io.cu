@@ -276,6 +276,13 @@ PinnedPool& pinned_pool() {
   return *pool;
 }
 
+}  // namespace
+
+void* pinned_get(size_t bytes, size_t* size) { return pinned_pool().get(bytes, size); }
+void pinned_put(void* p, size_t size) { pinned_pool().put(p, size); }
+
+namespace {
+
 struct HostBuf {
   void* p = nullptr;
   size_t size = 0;

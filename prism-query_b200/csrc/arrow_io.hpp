@@ -12,4 +12,9 @@ Batch import_device_batch(Ctx& ctx, const ArrowDeviceArray* a, const ArrowSchema
 // Copies a device batch into freshly allocated host buffers (caller releases).
 void export_batch(Ctx& ctx, const Batch& b, ArrowArray* a, ArrowSchema* s);
 
+// Page-locked host staging from the process-wide recycling pool: a buffer of
+// at least `bytes` (its size in *size), or nullptr when pinning fails.
+void* pinned_get(size_t bytes, size_t* size);
+void pinned_put(void* p, size_t size);
+
 }  // namespace prism

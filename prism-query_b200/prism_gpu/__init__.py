@@ -122,6 +122,10 @@ def _declare(lib):
     lib.prism_server_last_error.restype = C.c_char_p
     lib.prism_server_destroy.argtypes = [P]
     lib.prism_server_destroy.restype = None
+    lib.prism_parquet_scan.argtypes = [P, P, C.POINTER(C.POINTER(P)), C.POINTER(i32), P]
+    lib.prism_parquet_row_count.argtypes = [P, i32, P, C.POINTER(C.c_int64)]
+    lib.prism_free_array.argtypes = [P]
+    lib.prism_free_array.restype = None
     lib.prism_expand_worker_aggregates.argtypes = [P, P, i32, C.POINTER(i32)]
     lib.prism_batch_packed_size.argtypes = [P, C.POINTER(C.c_uint64)]
     lib.prism_batch_pack.argtypes = [P, P, P, C.c_uint64]
@@ -486,6 +490,52 @@ def hash_aggregate(batch, config: HashAggConfig, ctx: Optional[Context] = None, 
     h = C.c_void_p()
     ctx.check(lib().prism_hash_aggregate(ctx.handle, d.handle, C.byref(cfg), C.byref(h)))
     return _result(ctx, h, as_device)
+
+
+# ------------------------------------------------------------ parquet ----
+
+
+def _uri_array(uris: Sequence[str]):
+    enc = [os.fspath(u).encode() for u in uris]
+    arr = (C.c_char_p * max(1, len(enc)))(*enc)
+    return arr, enc
+
+
+def parquet_scan(uris: Sequence[str], predicate: Optional[Predicate] = None, projection: Optional[Sequence[int]] = None,
+                 batch_size: int = 8192, skip_expand: bool = False, ctx: Optional[Context] = None, as_device=False,
+                 with_stats=False):
+    """parquet_scan (parquet_scan.rs:55-168), decoded on the GPU: a list of
+    batches (Arrow, or DeviceBatch with as_device); with_stats also returns
+    the scan's counters (files, row groups read / skipped, pages, bytes)."""
+    ctx = ctx or default_context()
+    arr, keep = _uri_array(uris)
+    pred = predicate.encode() if predicate is not None else None
+    proj = _abi.int_array(list(projection)) if projection is not None else None
+    cfg = _abi.prism_parquet_scan_config(arr, len(keep), C.cast(C.byref(pred), C.c_void_p) if pred is not None else None,
+                                         proj, len(projection) if projection is not None else 0, batch_size,
+                                         1 if skip_expand else 0)
+    out = C.POINTER(C.c_void_p)()
+    n = C.c_int32(0)
+    st = _abi.prism_parquet_scan_stats()
+    ctx.check(lib().prism_parquet_scan(ctx.handle, C.byref(cfg), C.byref(out), C.byref(n), C.byref(st)))
+    try:
+        res = [_result(ctx, C.c_void_p(out[i]), as_device) for i in range(n.value)]
+    finally:
+        lib().prism_free_array(C.cast(out, C.c_void_p))
+    if with_stats:
+        return res, {f: getattr(st, f) for f, _ in st._fields_}
+    return res
+
+
+def parquet_row_count(uris: Sequence[str], predicate: Optional[Predicate] = None) -> int:
+    """parquet_row_count (parquet_scan.rs:240-266), from the footers alone."""
+    arr, keep = _uri_array(uris)
+    pred = predicate.encode() if predicate is not None else None
+    n = C.c_int64(0)
+    rc = lib().prism_parquet_row_count(arr, len(keep), C.byref(pred) if pred is not None else None, C.byref(n))
+    if rc:
+        raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+    return int(n.value)
 
 
 def expand_worker_aggregates(config: HashAggConfig) -> HashAggConfig:

@@ -132,6 +132,23 @@ class prism_agg_expr(C.Structure):
     _fields_ = [("column", C.c_int32), ("func", C.c_int32), ("output_name", C.c_char_p)]
 
 
+class prism_parquet_scan_config(C.Structure):
+    _fields_ = [
+        ("uris", C.POINTER(C.c_char_p)),
+        ("n_uris", C.c_int32),
+        ("predicate", C.c_void_p),
+        ("projection", C.POINTER(C.c_int32)),
+        ("n_projection", C.c_int32),
+        ("batch_size", C.c_int64),
+        ("skip_expand", C.c_int32),
+    ]
+
+
+class prism_parquet_scan_stats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("files", "row_groups", "row_groups_skipped", "pages", "compressed_bytes",
+                                          "decoded_bytes")]
+
+
 class prism_sort_key(C.Structure):
     _fields_ = [("column", C.c_int32), ("descending", C.c_int32), ("nulls_first", C.c_int32)]
 

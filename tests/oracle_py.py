@@ -292,6 +292,120 @@ def merge_partial_aggregates(partials: List[pa.RecordBatch], config: HashAggConf
     return pa.RecordBatch.from_arrays(cols, schema=pa.schema(fields))
 
 
+# ------------------------------------------------------------- parquet ----
+# The reference reads Parquet with the `parquet` crate 57.3.0 (arrow-rs),
+# absent from the reference's sources; its decoding is checked here against
+# pyarrow's reader (Arrow C++, an independent implementation of the same
+# format), while the scan's own logic (file listing, row-group skipping,
+# projection, batching, expansion) is restated from parquet_scan.rs.
+def list_parquet_files(uri: str) -> List[str]:
+    """list_files (object_source.rs:74-103): every *.parquet below a
+    directory, or the file itself; sorted."""
+    path = uri[7:] if uri.startswith("file://") else uri
+    if os.path.isfile(path):
+        return [path] if path.endswith(".parquet") else []
+    out = []
+    for root, _dirs, files in os.walk(path):
+        out += [os.path.join(root, f) for f in files if f.endswith(".parquet")]
+    return sorted(out)
+
+
+def _check_range(v, mn, mx, op) -> bool:  # check_range / check_range_str (parquet_scan.rs:449-467)
+    return {"Eq": lambda: mn <= v <= mx, "Lt": lambda: mn < v, "Le": lambda: mn <= v,
+            "Gt": lambda: mx > v, "Ge": lambda: mx >= v}[op]()
+
+
+# (physical type, scalar kind) -> the bounds a missing min / max defaults to
+_NUMERIC_STATS = {("INT64", 1): (-2.0 ** 63, 2.0 ** 63 - 1), ("INT32", 0): (-2.0 ** 31, 2.0 ** 31 - 1),
+                  ("DOUBLE", 2): (-1.7976931348623157e308, 1.7976931348623157e308)}
+
+
+def _stats_might_match(pred, rg, schema_names) -> bool:
+    """col_stats_might_match / stats_might_match (parquet_scan.rs:387-447)."""
+    if pred.column >= len(schema_names):
+        return True
+    name = schema_names[pred.column]
+    col = next((rg.column(i) for i in range(rg.num_columns) if rg.column(i).path_in_schema.split(".")[-1] == name), None)
+    if col is None or col.statistics is None:
+        return True
+    st, phys, v = col.statistics, col.physical_type, pred.value
+    key = (phys, v.kind)
+    if key in _NUMERIC_STATS:
+        lo, hi = _NUMERIC_STATS[key]
+        mn = float(st.min_raw) if st.has_min_max else lo
+        mx = float(st.max_raw) if st.has_min_max else hi
+        return _check_range(float(v.value), mn, mx, pred.op)
+    if phys == "BYTE_ARRAY" and v.kind == 3:
+        if not st.has_min_max:
+            return True
+
+        def lossy(x):
+            return (x if isinstance(x, bytes) else str(x).encode()).decode("utf-8", "replace").encode()
+        return _check_range(v.value.encode(), lossy(st.min_raw), lossy(st.max_raw), pred.op)
+    return True
+
+
+def row_group_might_match(pred, rg, schema_names) -> bool:
+    """row_group_might_match (parquet_scan.rs:355-377)."""
+    if pred is None:
+        return True
+    if pred.op == "Literal":
+        return bool(pred.value)
+    if pred.op in ("Eq", "Lt", "Le", "Gt", "Ge"):
+        return _stats_might_match(pred, rg, schema_names)
+    if pred.op == "And":
+        return all(row_group_might_match(c, rg, schema_names) for c in pred.children)
+    if pred.op == "Or":
+        return any(row_group_might_match(c, rg, schema_names) for c in pred.children)
+    return True
+
+
+def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, skip_expand: bool = False):
+    """parquet_scan (parquet_scan.rs:55-168) with pyarrow decoding each row group."""
+    import pyarrow.parquet as pq
+
+    files = []
+    for u in uris:
+        fs = list_parquet_files(u)
+        if not fs:
+            raise OracleError(7, f"no .parquet files found at {u}")
+        files += fs
+    if not files:
+        return []
+    full = pq.ParquetFile(files[0]).schema_arrow
+    out = []
+    for f in files:
+        pf = pq.ParquetFile(f)
+        names = pf.schema_arrow.names
+        cols = sorted({c for c in (projection or []) if 0 <= c < len(names)}) or list(range(len(names)))
+        for g in range(pf.metadata.num_row_groups):
+            if predicate is not None and not row_group_might_match(predicate, pf.metadata.row_group(g), names):
+                continue
+            t = pf.read_row_group(g, columns=[names[c] for c in cols])
+            for s in range(0, t.num_rows, batch_size):
+                piece = t.slice(s, batch_size).combine_chunks()
+                if piece.num_rows:
+                    out.append(piece.to_batches()[0])
+    if not skip_expand and projection is not None and len(projection) < len(full):
+        pmap = {}
+        for bi, oi in enumerate(projection):
+            if 0 <= oi < len(full):
+                pmap[oi] = bi
+        exp = []
+        for b in out:
+            arrays, fields = [], []
+            for i, fld in enumerate(full):
+                if i in pmap:
+                    arrays.append(b.column(pmap[i]))
+                    fields.append(fld)
+                else:
+                    arrays.append(pa.nulls(b.num_rows, fld.type))
+                    fields.append(pa.field(fld.name, fld.type, True))
+            exp.append(pa.RecordBatch.from_arrays(arrays, schema=pa.schema(fields)))
+        out = exp
+    return out
+
+
 def exact_sum_f64(values) -> float:
     import numpy as np
 
