@@ -51,7 +51,7 @@ SCALE = 1.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "sort", "topn"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "sort", "topn", "parquet"], default="c2")
     ap.add_argument("--requests", type=int, default=10_000, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="c5: Poisson arrival rate (requests/s)")
     ap.add_argument("--steps", type=int, default=None)
@@ -787,7 +787,97 @@ class TopNW(SortW):
                 "ms": ms / max(1, n), "per_unit": "8 B per row (the Float64 key read once)", "traffic_key": "topn_select"}
 
 
-WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4, "sort": SortW, "topn": TopNW}
+class ParquetW:
+    """Parquet scan (parquet_scan.rs:55-168) of a lineitem-shaped file, decoded
+    on the GPU from column chunks kept compressed in HBM."""
+    name = "parquet"
+    metric = "parquet scan rows/s"
+    dtype = "i32/i64/f64/utf8 (decoded Arrow)"
+    flush_l2 = False
+
+    def __init__(self, torch, device, ctx, rank):
+        import tempfile
+
+        import numpy as np
+        import pyarrow as pa
+        import pyarrow.parquet as pq
+
+        import prism_gpu
+
+        self.torch, self.ctx, self.pg, self.pq = torch, ctx, prism_gpu, pq
+        n = self.rows = sc(30_000_000)
+        rng = np.random.default_rng(700 + rank)
+        flags, status = np.array(["A", "N", "R"]), np.array(["F", "O"])
+        t = pa.table({
+            "l_orderkey": pa.array(np.sort(rng.integers(1, 6_000_000 * 4, n))),
+            "l_quantity": pa.array(rng.integers(1, 51, n).astype(np.int64)),
+            "l_extendedprice": pa.array(np.round(rng.uniform(900.0, 105_000.0, n), 2)),
+            "l_discount": pa.array(rng.integers(0, 11, n) / 100.0),
+            "l_tax": pa.array(rng.integers(0, 9, n) / 100.0),
+            "l_returnflag": pa.array(flags[rng.integers(0, 3, n)]),
+            "l_linestatus": pa.array(status[rng.integers(0, 2, n)]),
+            "l_shipdate": pa.array(rng.integers(8036, 10562, n).astype(np.int32), type=pa.date32()),
+        })
+        self.dir = tempfile.mkdtemp(prefix=f"prism_bench_pq{rank}_")
+        self.path = os.path.join(self.dir, "lineitem.parquet")
+        pq.write_table(t, self.path, compression="snappy", row_group_size=1 << 20)
+        self.table = t
+        self.prep = prism_gpu.ParquetPrepared([self.path], ctx=ctx, batch_size=1 << 20)
+        self.file_bytes = os.path.getsize(self.path)
+        self.decoded = int(t.nbytes)
+        self.workload = (f"Parquet scan of a lineitem-shaped file: {n:,} rows x 8 columns (orderkey, quantity, "
+                         "extendedprice, discount, tax, returnflag, linestatus, shipdate), written by pyarrow with its "
+                         f"defaults (SNAPPY, dictionary pages with PLAIN fallback, 1 MiB pages), 1Mi-row row groups; "
+                         f"{self.file_bytes / 1e6:.0f} MB on disk, {self.decoded / 1e6:.0f} MB decoded; timed: the "
+                         "GPU decode of the column chunks held compressed in HBM into device batches")
+
+    def step(self):
+        for b in self.prep.decode(as_device=True):
+            b.free()
+
+    def check(self):
+        got = self.pa_table(self.prep.decode())
+        assert got.equals(self.table), "decoded table differs from the written one"
+        return {"full_size_check": "decoded table equals the written table (every value and null)",
+                "file_bytes": self.file_bytes, "compressed_bytes_in_hbm": self.prep.compressed_bytes}
+
+    @staticmethod
+    def pa_table(batches):
+        import pyarrow as pa
+
+        return pa.Table.from_batches(batches)
+
+    def roofline(self, kstats):
+        n, ms = kstats.get("pq_page_kernel", (0, 0.0))
+        st = self.prep.decode(with_stats=True)[1] if not hasattr(self, "_st") else self._st
+        self._st = st
+        return {"kernel": "pq_page_kernel (levels, dictionary indices and PLAIN values of every page)",
+                "bytes": st["inflated_bytes"] + st["decoded_bytes"], "ms": ms / max(1, n),
+                "per_unit": "the inflated page bytes read + the decoded Arrow bytes written, per scan",
+                "traffic_key": "parquet_page"}
+
+    e2e_timing = ("host wall clock around prism_parquet_scan of the file (page cache warm): footer, pread of the "
+                  "column chunks into pinned staging, one H2D, GPU decode, export of the batches to host Arrow (D2H)")
+
+    def e2e_inputs(self):
+        return [self.path]
+
+    def h2d_bytes(self, _inputs):
+        return self.prep.compressed_bytes
+
+    def e2e_step(self, inputs):
+        return self.pa_table(self.pg.parquet_scan(inputs, batch_size=1 << 20, ctx=self.ctx))
+
+    def cpu_baseline(self, threads):
+        t0 = time.perf_counter()
+        tb = self.pq.read_table(self.path, use_threads=True)
+        dt = time.perf_counter() - t0
+        return tb.num_rows / dt, threads, (f"pyarrow {__import__('pyarrow').__version__} (Arrow C++) read_table of the "
+                                          f"whole file on {threads} threads, page cache warm ({dt:.2f} s); the "
+                                          "reference's arrow-rs parquet reader is not buildable here")
+
+
+WORKLOAD_CLASSES = {"c1": C1, "c3": C3, "c4": C4, "sort": SortW, "topn": TopNW, "parquet": ParquetW}
 
 
 def gpu_index_of(local):
@@ -815,7 +905,7 @@ def run_workload(args, rank, world, local, torch, dist):
             r, cores, sample = W.cpu_baseline(threads)
             rates.append(r)
         value = sorted(rates)[len(rates) // 2]
-        line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": len(rates),
+        line = {"metric": getattr(W, "metric", METRIC), "value": value, "unit": "rows/s", "n_gpus": world, "steps": len(rates),
                 "warmup": args.warmup, "ms_per_step": W.rows / value * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": W.dtype, "data": "synthetic (seeded)", "impl": "reference",
                 "config": {"workload": W.workload, "rows_per_step": W.rows},
@@ -865,7 +955,8 @@ def run_workload(args, rank, world, local, torch, dist):
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
     names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
-             "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel", "select_hist_kernel")
+             "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel", "select_hist_kernel",
+             "pq_snappy_kernel", "pq_page_kernel", "pq_copy_kernel", "pq_dict_kernel", "pq_positions_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
     ctx.set_profiling(False)
     t = torch.tensor([ms], device=device, dtype=torch.float64)
@@ -885,7 +976,7 @@ def run_workload(args, rank, world, local, torch, dist):
     e2e = None
     if args.e2e_steps > 0:
         hb = W.e2e_inputs()
-        h2d = sum(c.nbytes for b in hb for c in b.columns)
+        h2d = W.h2d_bytes(hb) if hasattr(W, "h2d_bytes") else sum(c.nbytes for b in hb for c in b.columns)
         out = W.e2e_step(hb)  # warm
         d2h = sum(c.nbytes for c in out.columns)
         del out
@@ -905,8 +996,8 @@ def run_workload(args, rank, world, local, torch, dist):
         del hb
         e2e = {"value": world * W.rows / dt, "unit": "rows/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
-               "timing": "host wall clock around the synchronous C-ABI calls: import (H2D from pinned host Arrow "
-                         "buffers), operator, export (D2H)"}
+               "timing": getattr(W, "e2e_timing", "host wall clock around the synchronous C-ABI calls: import (H2D "
+                                 "from pinned host Arrow buffers), operator, export (D2H)")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -915,7 +1006,7 @@ def run_workload(args, rank, world, local, torch, dist):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "metric": getattr(W, "metric", METRIC), "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": W.dtype,
             "data": "synthetic (seeded torch generators with the configs' shapes and distributions)",

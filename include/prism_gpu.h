@@ -442,7 +442,10 @@ typedef struct prism_parquet_scan_config {
 } prism_parquet_scan_config;
 
 typedef struct prism_parquet_scan_stats {
-  int64_t files, row_groups, row_groups_skipped, pages, compressed_bytes, decoded_bytes;
+  int64_t files, row_groups, row_groups_skipped, pages;
+  int64_t compressed_bytes;  /* column-chunk bytes read (staged to the device) */
+  int64_t inflated_bytes;    /* page bytes after decompression (compressed pages only) */
+  int64_t decoded_bytes;     /* Arrow bytes produced: values, offsets and string data */
 } prism_parquet_scan_stats;
 
 /* parquet_scan (parquet_scan.rs:55-168): the files of every URI (sorted
@@ -462,6 +465,22 @@ typedef struct prism_parquet_scan_stats {
  * PRISM_ERR_INTERNAL (the reference's PrismError::Internal). */
 int prism_parquet_scan(prism_ctx* ctx, const prism_parquet_scan_config* config, prism_batch*** out, int32_t* n_out,
                        prism_parquet_scan_stats* stats);
+
+/* The scan in two steps, for tables kept in HBM still compressed (a
+ * compressed table takes a fraction of its decoded size in the 180 GB):
+ * prism_parquet_prepare reads every selected column chunk (the same file,
+ * row-group and column selection as prism_parquet_scan) into device memory
+ * and walks its page headers; prism_parquet_decode decodes the prepared
+ * chunks on the GPU into batches, as often as called (each call returns new
+ * batches, as prism_parquet_scan would). No counterpart in the reference. */
+typedef struct prism_parquet_prepared prism_parquet_prepared;
+int prism_parquet_prepare(prism_ctx* ctx, const prism_parquet_scan_config* config, prism_parquet_prepared** out,
+                          prism_parquet_scan_stats* stats);
+int prism_parquet_decode(prism_ctx* ctx, const prism_parquet_prepared* prepared, prism_batch*** out, int32_t* n_out,
+                         prism_parquet_scan_stats* stats);
+int64_t prism_parquet_prepared_rows(const prism_parquet_prepared* prepared);
+int64_t prism_parquet_prepared_bytes(const prism_parquet_prepared* prepared);
+void prism_parquet_prepared_free(prism_parquet_prepared* prepared);
 
 /* parquet_row_count (parquet_scan.rs:240-266): rows of the row groups the
  * predicate (NULL: none) might match, from the footers alone. */

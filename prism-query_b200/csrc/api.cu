@@ -773,14 +773,10 @@ int prism_sort_batch(prism_ctx* c, const prism_batch* b, const prism_sort_key* k
 }
 
 // ---------------------------------------------------------------- parquet --
-int prism_parquet_scan(prism_ctx* c, const prism_parquet_scan_config* cfg, prism_batch*** out, int32_t* n_out,
-                       prism_parquet_scan_stats* stats) {
-  return run(c, [&] {
-    if (!cfg || !out || !n_out || (cfg->n_uris > 0 && !cfg->uris) || cfg->n_uris < 0 ||
+static ParquetScanArgs scan_args(const prism_parquet_scan_config* cfg) {
+    if (!cfg || (cfg->n_uris > 0 && !cfg->uris) || cfg->n_uris < 0 ||
         (cfg->n_projection > 0 && !cfg->projection) || cfg->n_projection < 0)
-      fail(PRISM_ERR_INVALID_ARGUMENT, "null scan config/output");
-    *out = nullptr;
-    *n_out = 0;
+      fail(PRISM_ERR_INVALID_ARGUMENT, "null scan config");
     ParquetScanArgs a;
     for (int i = 0; i < cfg->n_uris; ++i) {
       if (!cfg->uris[i]) fail(PRISM_ERR_INVALID_ARGUMENT, "null URI");
@@ -791,16 +787,67 @@ int prism_parquet_scan(prism_ctx* c, const prism_parquet_scan_config* cfg, prism
     if (a.has_projection) a.projection.assign(cfg->projection, cfg->projection + cfg->n_projection);
     a.batch_size = cfg->batch_size;
     a.skip_expand = cfg->skip_expand != 0;
+    return a;
+}
+
+static void batch_array(prism_ctx* c, std::vector<Batch>& bs, prism_batch*** out, int32_t* n_out) {
+  auto** arr = static_cast<prism_batch**>(std::malloc(sizeof(prism_batch*) * std::max<size_t>(bs.size(), 1)));
+  if (!arr) fail(PRISM_ERR_NO_MEMORY, "host allocation failed");
+  for (size_t i = 0; i < bs.size(); ++i) arr[i] = wrap(c, std::move(bs[i]));
+  *out = arr;
+  *n_out = (int32_t)bs.size();
+}
+
+static void put_stats(const ParquetScanStats& st, prism_parquet_scan_stats* stats) {
+  if (stats)
+    *stats = {st.files, st.row_groups, st.row_groups_skipped, st.pages, st.compressed_bytes, st.inflated_bytes,
+              st.decoded_bytes};
+}
+
+int prism_parquet_scan(prism_ctx* c, const prism_parquet_scan_config* cfg, prism_batch*** out, int32_t* n_out,
+                       prism_parquet_scan_stats* stats) {
+  return run(c, [&] {
+    if (!out || !n_out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    *n_out = 0;
     ParquetScanStats st;
-    std::vector<Batch> bs = parquet_scan(c->impl, a, &st);
-    if (stats) *stats = {st.files, st.row_groups, st.row_groups_skipped, st.pages, st.compressed_bytes, st.decoded_bytes};
-    auto** arr = static_cast<prism_batch**>(std::malloc(sizeof(prism_batch*) * std::max<size_t>(bs.size(), 1)));
-    if (!arr) fail(PRISM_ERR_NO_MEMORY, "host allocation failed");
-    for (size_t i = 0; i < bs.size(); ++i) arr[i] = wrap(c, std::move(bs[i]));
-    *out = arr;
-    *n_out = (int32_t)bs.size();
+    std::vector<Batch> bs = parquet_scan(c->impl, scan_args(cfg), &st);
+    put_stats(st, stats);
+    batch_array(c, bs, out, n_out);
   });
 }
+
+struct prism_parquet_prepared {
+  std::shared_ptr<prism::ParquetPrepared> impl;
+};
+
+int prism_parquet_prepare(prism_ctx* c, const prism_parquet_scan_config* cfg, prism_parquet_prepared** out,
+                          prism_parquet_scan_stats* stats) {
+  return run(c, [&] {
+    if (!out) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    ParquetScanStats st;
+    auto p = parquet_prepare(c->impl, scan_args(cfg), &st);
+    put_stats(st, stats);
+    *out = new prism_parquet_prepared{std::move(p)};
+  });
+}
+
+int prism_parquet_decode(prism_ctx* c, const prism_parquet_prepared* p, prism_batch*** out, int32_t* n_out,
+                         prism_parquet_scan_stats* stats) {
+  return run(c, [&] {
+    if (!p || !out || !n_out) fail(PRISM_ERR_INVALID_ARGUMENT, "null prepared scan/output");
+    *out = nullptr;
+    *n_out = 0;
+    ParquetScanStats st;
+    std::vector<Batch> bs = parquet_decode(c->impl, *p->impl, &st);
+    put_stats(st, stats);
+    batch_array(c, bs, out, n_out);
+  });
+}
+
+int64_t prism_parquet_prepared_rows(const prism_parquet_prepared* p) { return p ? parquet_prepared_rows(*p->impl) : -1; }
+int64_t prism_parquet_prepared_bytes(const prism_parquet_prepared* p) { return p ? parquet_prepared_bytes(*p->impl) : -1; }
+void prism_parquet_prepared_free(prism_parquet_prepared* p) { delete p; }
 
 int prism_parquet_row_count(const char* const* uris, int32_t n, const prism_predicate* pred, int64_t* count) {
   try {

@@ -80,103 +80,133 @@ struct SnappyJob {
 // ---------------------------------------------------------------- snappy --
 // The Snappy format: a varint of the uncompressed length, then elements whose
 // tag's low two bits select a literal (length in the tag, or in 1-4 following
-// bytes when the tag says 60-63), or a copy of (length, offset) with a 1-, 2-
-// or 4-byte offset. One lane parses each tag; the warp copies its bytes (a
-// copy whose offset is shorter than its length repeats the last `offset`
-// bytes, which every lane can compute from bytes already written).
-__global__ void pq_snappy_kernel(const SnappyJob* jobs, int n, uint32_t* err) {
+// bytes when the tag says 60-63), or a copy of (length <= 64, offset) with a
+// 1-, 2- or 4-byte offset. One warp inflates one stream: lane 0 parses up to
+// SNAP_CMDS elements into a command queue in shared memory, then the warp
+// executes them in order, its lanes moving the bytes. The last SNAP_RING
+// output bytes are mirrored in a shared-memory ring, so a copy (its source
+// window [op - offset, op) stays intact while it writes at most 64 bytes)
+// reads shared memory unless its offset reaches past the ring.
+constexpr int SNAP_WARPS = 8;
+constexpr int SNAP_RING = 16384;  // power of two
+constexpr int SNAP_CMDS = 32;
+
+struct SnapCmd {
+  int32_t len;
+  int32_t off;  // 0: literal
+  int64_t src;  // literal: input offset
+};
+
+__global__ void __launch_bounds__(32 * SNAP_WARPS) pq_snappy_kernel(const SnappyJob* jobs, int n, uint32_t* err) {
+  extern __shared__ __align__(16) uint8_t snap_smem[];
+  __shared__ SnapCmd cmds[SNAP_WARPS][SNAP_CMDS];
+  __shared__ int32_t ncmd[SNAP_WARPS];
+  __shared__ int32_t state[SNAP_WARPS];  // 0 running, 1 done, 2 malformed
+  __shared__ int64_t in_pos[SNAP_WARPS];
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (warp >= n) return;
-  const SnappyJob J = jobs[warp];
-  const uint8_t* ip = J.src;
-  const uint8_t* const iend = J.src + J.src_len;
+  const int w = threadIdx.x >> 5;
+  const int job = blockIdx.x * SNAP_WARPS + w;
+  if (job >= n) return;
+  const SnappyJob J = jobs[job];
+  uint8_t* const ring = snap_smem + (size_t)w * SNAP_RING;
+  const uint8_t* const in = J.src;
+  const int64_t in_len = J.src_len;
   uint8_t* const dst = J.dst;
-  bool ok = true;
-  // preamble
-  uint32_t ulen = 0;
+  const int64_t out_len = J.dst_len;
   if (lane == 0) {
-    for (int s = 0; s < 35; s += 7) {
-      if (ip >= iend) { ok = false; break; }
-      const uint8_t b = *ip++;
+    uint32_t ulen = 0;
+    int64_t ip = 0;
+    bool ok = true;
+    for (int s = 0;; s += 7) {
+      if (ip >= in_len || s > 28) { ok = false; break; }
+      const uint8_t b = in[ip++];
       ulen |= (uint32_t)(b & 0x7f) << s;
       if (!(b & 0x80)) break;
     }
-    if (ulen != (uint32_t)J.dst_len) ok = false;
+    if (ulen != (uint32_t)out_len) ok = false;
+    state[w] = ok ? 0 : 2;
+    in_pos[w] = ip;
   }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  unsigned long long ipv = __shfl_sync(0xffffffffu, (unsigned long long)ip, 0);
-  ip = reinterpret_cast<const uint8_t*>(ipv);
+  __syncwarp();
   int64_t op = 0;
-  while (ok && ip < iend) {
-    int kind = 0;  // 0 literal, 1 copy
-    int64_t len = 0, off = 0;
-    unsigned long long lit = 0;
-    bool good = true;
-    if (lane == 0) {
-      const uint8_t tag = *ip++;
-      const int t = tag & 3;
-      if (t == 0) {
-        len = (tag >> 2) + 1;
-        if (len > 60) {
-          const int nb = (int)len - 60;
-          if (iend - ip < nb) good = false;
-          else {
+  for (;;) {
+    const int run_state = state[w];
+    __syncwarp();  // every lane has read the state before lane 0 rewrites it
+    if (run_state != 0) break;
+    if (lane == 0) {  // parse up to SNAP_CMDS elements
+      int64_t ip = in_pos[w];
+      int64_t o = op;
+      int k = 0;
+      int st = 0;
+      while (k < SNAP_CMDS) {
+        if (ip >= in_len) { st = 1; break; }
+        const uint8_t tag = in[ip++];
+        const int t = tag & 3;
+        int64_t len, off = 0, src = 0;
+        if (t == 0) {
+          len = (tag >> 2) + 1;
+          if (len > 60) {
+            const int nb = (int)len - 60;
+            if (in_len - ip < nb) { st = 2; break; }
             uint32_t v = 0;
-            for (int k = 0; k < nb; ++k) v |= (uint32_t)ip[k] << (8 * k);
+            for (int q = 0; q < nb; ++q) v |= (uint32_t)in[ip + q] << (8 * q);
             ip += nb;
             len = (int64_t)v + 1;
           }
+          if (in_len - ip < len) { st = 2; break; }
+          src = ip;
+          ip += len;
+        } else {
+          const int nb = t == 1 ? 1 : (t == 2 ? 2 : 4);
+          if (in_len - ip < nb) { st = 2; break; }
+          if (t == 1) {
+            len = ((tag >> 2) & 7) + 4;
+            off = ((int64_t)(tag >> 5) << 8) | in[ip];
+          } else {
+            len = (tag >> 2) + 1;
+            off = 0;
+            for (int q = 0; q < nb; ++q) off |= (int64_t)in[ip + q] << (8 * q);
+          }
+          ip += nb;
+          if (off <= 0 || off > o) { st = 2; break; }
         }
-        lit = (unsigned long long)ip;
-        if (good && (iend - ip) < len) good = false;
-        ip += good ? len : 0;
-      } else if (t == 1) {
-        kind = 1;
-        if (iend - ip < 1) good = false;
-        else {
-          len = ((tag >> 2) & 7) + 4;
-          off = ((int64_t)(tag >> 5) << 8) | ip[0];
-          ip += 1;
+        if (o + len > out_len || len > 0x7fffffff) { st = 2; break; }
+        cmds[w][k] = SnapCmd{(int32_t)len, (int32_t)off, src};
+        o += len;
+        ++k;
+      }
+      ncmd[w] = k;
+      in_pos[w] = ip;
+      state[w] = st;
+    }
+    __syncwarp();
+    const int k_end = ncmd[w];
+    for (int k = 0; k < k_end; ++k) {
+      const SnapCmd c = cmds[w][k];
+      if (c.off == 0) {
+        for (int64_t i = lane; i < c.len; i += 32) {
+          const uint8_t b = in[c.src + i];
+          dst[op + i] = b;
+          ring[(op + i) & (SNAP_RING - 1)] = b;
         }
-      } else if (t == 2) {
-        kind = 1;
-        if (iend - ip < 2) good = false;
-        else {
-          len = (tag >> 2) + 1;
-          off = (int64_t)ip[0] | ((int64_t)ip[1] << 8);
-          ip += 2;
+      } else if (c.off <= SNAP_RING - 64) {
+        for (int i = lane; i < c.len; i += 32) {
+          const uint8_t b = ring[(op - c.off + (i % c.off)) & (SNAP_RING - 1)];
+          dst[op + i] = b;
+          ring[(op + i) & (SNAP_RING - 1)] = b;
         }
       } else {
-        kind = 1;
-        if (iend - ip < 4) good = false;
-        else {
-          len = (tag >> 2) + 1;
-          off = (int64_t)ip[0] | ((int64_t)ip[1] << 8) | ((int64_t)ip[2] << 16) | ((int64_t)ip[3] << 24);
-          ip += 4;
+        for (int i = lane; i < c.len; i += 32) {
+          const uint8_t b = dst[op - c.off + (i % c.off)];
+          dst[op + i] = b;
+          ring[(op + i) & (SNAP_RING - 1)] = b;
         }
       }
-      if (good && op + len > J.dst_len) good = false;
-      if (good && kind == 1 && (off <= 0 || off > op)) good = false;
+      op += c.len;
+      __syncwarp();
     }
-    good = __shfl_sync(0xffffffffu, good, 0);
-    if (!good) { ok = false; break; }
-    kind = __shfl_sync(0xffffffffu, kind, 0);
-    len = __shfl_sync(0xffffffffu, len, 0);
-    off = __shfl_sync(0xffffffffu, off, 0);
-    lit = __shfl_sync(0xffffffffu, lit, 0);
-    ipv = __shfl_sync(0xffffffffu, (unsigned long long)ip, 0);
-    ip = reinterpret_cast<const uint8_t*>(ipv);
-    if (kind == 0) {
-      const uint8_t* s = reinterpret_cast<const uint8_t*>(lit);
-      for (int64_t i = lane; i < len; i += 32) dst[op + i] = s[i];
-    } else {
-      for (int64_t i = lane; i < len; i += 32) dst[op + i] = dst[op - off + (i % off)];
-    }
-    op += len;
-    __syncwarp();
   }
-  if (lane == 0 && (!ok || op != J.dst_len)) atomicOr(err, DERR_CORRUPT);
+  if (lane == 0 && (state[w] != 1 || op != out_len)) atomicOr(err, DERR_CORRUPT);
 }
 
 // ------------------------------------------------------- hybrid streams --
@@ -790,14 +820,47 @@ struct RgOut {  // one row group's decoded columns
 
 int fixed_width(int32_t ty) { return ty == TY_BOOL ? 0 : width_of(ty); }
 
-// Decodes the selected row groups of one file into device columns.
-std::vector<RgOut> decode_file(Ctx& ctx, const std::string& path, FileHandle& fh, const FileMeta& m,
-                               const std::vector<int>& rgs, const std::vector<ColPlan>& plan, ParquetScanStats* stats) {
-  std::vector<RgOut> res;
-  if (rgs.empty()) return res;
-  // 1. column chunk ranges
-  struct Chunk { int rg, c; int64_t file_off, len; size_t host_off; int codec; int ptype; };
+struct Chunk {  // one column chunk of one selected row group
+  int rg, c;
+  int64_t file_off, len;
+  size_t host_off;  // offset in the staging buffer and in the device copy
+  int codec, ptype;
+};
+
+struct PendingJob {  // a Snappy stream to inflate: kind 0 a data page, 1 a dictionary
+  size_t chunk_src;
+  int32_t src_len, dst_len;
+  int kind, idx;
+};
+
+// One file's selected column chunks resident in HBM (still compressed), with
+// the page tables that the decode kernels need.
+struct PreparedFile {
+  std::string path;
+  FileMeta meta;
+  std::vector<int> rgs;
+  std::vector<ColPlan> plan;
   std::vector<Chunk> chunks;
+  MemP raw_mem;
+  std::vector<PqPage> pages;  // bodies of compressed pages are filled in per decode
+  std::vector<PqDict> dicts;
+  std::vector<PendingJob> pend;
+  std::vector<int32_t> plain_utf8;
+  int64_t pos_total = 0;
+  size_t unc_total = 0;
+  int64_t staged = 0;
+};
+
+// Reads the selected chunks of one file into HBM and walks their pages.
+PreparedFile prepare_file(Ctx& ctx, const std::string& path, FileHandle& fh, const FileMeta& m,
+                          const std::vector<int>& rgs, const std::vector<ColPlan>& plan, ParquetScanStats* stats) {
+  PreparedFile P;
+  P.path = path;
+  P.meta = m;
+  P.rgs = rgs;
+  P.plan = plan;
+  // 1. column chunk ranges
+  std::vector<Chunk>& chunks = P.chunks;
   size_t staged = 0;
   for (int g : rgs) {
     const RowGroup& R = m.row_groups[g];
@@ -835,26 +898,20 @@ std::vector<RgOut> decode_file(Ctx& ctx, const std::string& path, FileHandle& fh
     }
   } pin_hold{pinned, hsize, ctx.stream};
   for (const Chunk& ch : chunks) read_at(fh.fd, host + ch.host_off, (size_t)ch.len, ch.file_off, path);
-  MemP raw_mem = ctx.alloc(std::max<size_t>(staged, 16));
-  uint8_t* raw = static_cast<uint8_t*>(raw_mem->ptr);
+  P.raw_mem = ctx.alloc(std::max<size_t>(staged, 16));
+  uint8_t* raw = static_cast<uint8_t*>(P.raw_mem->ptr);
   PRISM_CUDA(cudaMemcpyAsync(raw, host, staged, cudaMemcpyHostToDevice, ctx.stream));
-  if (stats) stats->compressed_bytes += (int64_t)staged;
+  P.staged = (int64_t)staged;
 
   // 3. page headers (host) -> pages, dictionaries, decompression jobs
-  std::vector<PqPage> pages;
-  std::vector<PqDict> dicts;
-  std::vector<SnappyJob> jobs;
-  std::vector<int32_t> plain_utf8;
-  int64_t pos_total = 0;
-  size_t unc_total = 0;
-  struct PendingJob { size_t chunk_src; int32_t src_len; int32_t dst_len; int kind; int idx; };  // kind 0 page, 1 dict
-  std::vector<PendingJob> pend;
-  std::vector<int> out_of_chunk(chunks.size());
-  res.resize(rgs.size());
-  std::vector<std::vector<int64_t>> rg_rows_seen(rgs.size(), std::vector<int64_t>(plan.size(), 0));
+  std::vector<PqPage>& pages = P.pages;
+  std::vector<PqDict>& dicts = P.dicts;
+  std::vector<int32_t>& plain_utf8 = P.plain_utf8;
+  int64_t& pos_total = P.pos_total;
+  size_t& unc_total = P.unc_total;
+  std::vector<PendingJob>& pend = P.pend;
   for (size_t ci = 0; ci < chunks.size(); ++ci) {
     const Chunk& ch = chunks[ci];
-    const int rgi = (int)(std::find(rgs.begin(), rgs.end(), ch.rg) - rgs.begin());
     const ColPlan& cp = plan[ch.c];
     int dict_slot = -1;
     int64_t pos = 0, row = 0;
@@ -934,14 +991,36 @@ std::vector<RgOut> decode_file(Ctx& ctx, const std::string& path, FileHandle& fh
       pos = data_at + h.compressed;
     }
     if (row != want_rows) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": column chunk rows differ from its row group");
-    rg_rows_seen[rgi][ch.c] = row;
   }
-  if (stats) stats->pages += (int64_t)pages.size();
+  (void)stats;
+  ctx.sync();  // the staging buffer goes back to the pool on return
+  return P;
+}
+
+// Decodes a prepared file into device columns, one RgOut per row group.
+std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanStats* stats) {
+  const std::string& path = P.path;
+  const FileMeta& m = P.meta;
+  const std::vector<int>& rgs = P.rgs;
+  const std::vector<ColPlan>& plan = P.plan;
+  const std::vector<Chunk>& chunks = P.chunks;
+  uint8_t* raw = static_cast<uint8_t*>(P.raw_mem->ptr);
+  std::vector<PqPage> pages = P.pages;
+  std::vector<PqDict> dicts = P.dicts;
+  const std::vector<int32_t>& plain_utf8 = P.plain_utf8;
+  const int64_t pos_total = P.pos_total;
+  std::vector<SnappyJob> jobs;
+  std::vector<RgOut> res(rgs.size());
+  if (stats) {
+    stats->pages += (int64_t)pages.size();
+    stats->compressed_bytes += P.staged;
+    for (const PendingJob& j : P.pend) stats->inflated_bytes += j.dst_len;
+  }
   // decompression targets
-  MemP unc_mem = ctx.alloc(std::max<size_t>(unc_total, 16));
+  MemP unc_mem = ctx.alloc(std::max<size_t>(P.unc_total, 16));
   uint8_t* unc = static_cast<uint8_t*>(unc_mem->ptr);
   size_t uo = 0;
-  for (const PendingJob& j : pend) {
+  for (const PendingJob& j : P.pend) {
     if (j.dst_len < 0 || j.src_len < 0) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": negative page size");
     uint8_t* dst = unc + uo;
     uo += (size_t)((j.dst_len + 15) & ~15);
@@ -1017,9 +1096,13 @@ std::vector<RgOut> decode_file(Ctx& ctx, const std::string& path, FileHandle& fh
   if (!jobs.empty()) {
     auto* dj = static_cast<SnappyJob*>(upload(jobs.data(), jobs.size() * sizeof(SnappyJob), jobs_mem));
     KernelTimer kt(ctx, "pq_snappy_kernel");
-    const int warps_per_block = 4;
-    pq_snappy_kernel<<<(unsigned)((jobs.size() + warps_per_block - 1) / warps_per_block), 32 * warps_per_block, 0,
-                       ctx.stream>>>(dj, (int)jobs.size(), err);
+    static const bool attr = [] {
+      return cudaFuncSetAttribute(pq_snappy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SNAP_WARPS * SNAP_RING) == cudaSuccess;
+    }();
+    if (!attr) fail(PRISM_ERR_CUDA, "cannot reserve shared memory for pq_snappy_kernel");
+    pq_snappy_kernel<<<(unsigned)((jobs.size() + SNAP_WARPS - 1) / SNAP_WARPS), 32 * SNAP_WARPS,
+                       SNAP_WARPS * SNAP_RING, ctx.stream>>>(dj, (int)jobs.size(), err);
     ctx.note_launch();
     ctx.check_launch("pq_snappy_kernel");
   }
@@ -1155,7 +1238,6 @@ std::vector<RgOut> decode_file(Ctx& ctx, const std::string& path, FileHandle& fh
     if (stats) stats->decoded_bytes += cp.type == TY_UTF8 ? 0 : (cp.type == TY_BOOL ? (n + 7) / 8 : n * width_of(cp.type));
     res[gi].cols[ch.c] = c;
   }
-  (void)rg_rows_seen;
   return res;
 }
 
@@ -1246,9 +1328,18 @@ int64_t parquet_row_count(const std::vector<std::string>& uris, const prism_pred
   return total;
 }
 
-std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats) {
-  std::vector<Batch> out;
-  if (args.uris.empty()) return out;
+struct ParquetPrepared {
+  ParquetScanArgs args;
+  std::vector<Leaf> full;  // the first file's schema
+  std::vector<PreparedFile> files;
+  int64_t rows = 0;
+};
+
+std::shared_ptr<ParquetPrepared> parquet_prepare(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats) {
+  auto P = std::make_shared<ParquetPrepared>();
+  P->args = args;
+  P->args.predicate = nullptr;  // used here only: the caller's predicate need not outlive this call
+  if (args.uris.empty()) return P;
   if (args.batch_size <= 0) fail(PRISM_ERR_INVALID_ARGUMENT, "batch_size must be positive");
   std::vector<std::string> files;
   for (const auto& uri : args.uris) {
@@ -1257,13 +1348,11 @@ std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetSc
     files.insert(files.end(), fs.begin(), fs.end());
   }
   const bool has_pred = args.predicate && args.predicate->n_nodes > 0;
-  std::vector<Leaf> full;  // the first file's schema
-  std::vector<std::pair<int32_t, bool>> full_types;
   for (size_t fi = 0; fi < files.size(); ++fi) {
     const std::string& path = files[fi];
     FileHandle fh;
     const FileMeta m = read_meta(path, fh);
-    if (fi == 0) full = m.leaves;
+    if (fi == 0) P->full = m.leaves;
     if (stats) {
       stats->files += 1;
       stats->row_groups += (int64_t)m.row_groups.size();
@@ -1296,22 +1385,44 @@ std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetSc
                                              "INT64, FLOAT, DOUBLE and UTF8 BYTE_ARRAY columns are read)");
       plan.push_back({c, ty, l.repetition == 1});
     }
-    std::vector<RgOut> rg_out = decode_file(ctx, path, fh, m, rgs, plan, stats);
+    P->files.push_back(prepare_file(ctx, path, fh, m, rgs, plan, stats));
+    for (int g : rgs) P->rows += m.row_groups[g].num_rows;
+  }
+  return P;
+}
+
+int64_t parquet_prepared_rows(const ParquetPrepared& P) { return P.rows; }
+int64_t parquet_prepared_bytes(const ParquetPrepared& P) {
+  int64_t b = 0;
+  for (const auto& f : P.files) b += f.staged;
+  return b;
+}
+
+std::vector<Batch> parquet_decode(Ctx& ctx, const ParquetPrepared& P, ParquetScanStats* stats) {
+  const ParquetScanArgs& args = P.args;
+  std::vector<Batch> out;
+  for (const PreparedFile& F : P.files) {
+    const std::vector<ColPlan>& plan = F.plan;
+    std::vector<RgOut> rg_out = decode_prepared(ctx, F, stats);
     // batches of at most batch_size rows, per row group
     for (RgOut& R : rg_out) {
       // Utf8 slice bounds need the row group's offsets at the cut points
       std::vector<int64_t> cuts;
       for (int64_t s = 0; s < R.rows; s += args.batch_size) cuts.push_back(s);
       std::vector<std::vector<int64_t>> bounds(plan.size());
+      bool fetched = false;
+      std::vector<std::vector<int32_t>> hb(plan.size());
       for (size_t c = 0; c < plan.size(); ++c) {
         if (plan[c].type != TY_UTF8 || cuts.size() <= 1) continue;
-        std::vector<int32_t> h(cuts.size() + 1);
+        hb[c].resize(cuts.size() + 1);
         for (size_t k = 0; k < cuts.size(); ++k)
-          PRISM_CUDA(cudaMemcpyAsync(&h[k], R.cols[c]->offsets + cuts[k], 4, cudaMemcpyDeviceToHost, ctx.stream));
-        PRISM_CUDA(cudaMemcpyAsync(&h[cuts.size()], R.cols[c]->offsets + R.rows, 4, cudaMemcpyDeviceToHost, ctx.stream));
-        ctx.sync();
-        bounds[c].assign(h.begin(), h.end());
+          PRISM_CUDA(cudaMemcpyAsync(&hb[c][k], R.cols[c]->offsets + cuts[k], 4, cudaMemcpyDeviceToHost, ctx.stream));
+        PRISM_CUDA(cudaMemcpyAsync(&hb[c][cuts.size()], R.cols[c]->offsets + R.rows, 4, cudaMemcpyDeviceToHost,
+                                   ctx.stream));
+        fetched = true;
       }
+      if (fetched) ctx.sync();
+      for (size_t c = 0; c < plan.size(); ++c) bounds[c].assign(hb[c].begin(), hb[c].end());
       for (size_t k = 0; k < cuts.size(); ++k) {
         const int64_t s = cuts[k], n = std::min(args.batch_size, R.rows - s);
         Batch b;
@@ -1326,6 +1437,7 @@ std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetSc
     }
   }
   // expand_projected_batches (parquet_scan.rs:471-526)
+  const std::vector<Leaf>& full = P.full;
   if (!args.skip_expand && args.has_projection && args.projection.size() < full.size()) {
     std::vector<int> proj_map(full.size(), -1);
     for (size_t bi = 0; bi < args.projection.size(); ++bi) {
@@ -1353,6 +1465,11 @@ std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetSc
     }
   }
   return out;
+}
+
+std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats) {
+  const auto P = parquet_prepare(ctx, args, stats);
+  return parquet_decode(ctx, *P, stats);
 }
 
 }  // namespace prism

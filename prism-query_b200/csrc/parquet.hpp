@@ -11,6 +11,7 @@
 // Encodings.md) and the Snappy format description.
 #pragma once
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -108,11 +109,20 @@ struct ParquetScanArgs {
 
 struct ParquetScanStats {
   int64_t files = 0, row_groups = 0, row_groups_skipped = 0, pages = 0;
-  int64_t compressed_bytes = 0, decoded_bytes = 0;
+  int64_t compressed_bytes = 0, inflated_bytes = 0, decoded_bytes = 0;
 };
 
-// parquet_scan (parquet_scan.rs:55-168) into device batches.
+// parquet_scan (parquet_scan.rs:55-168) into device batches: prepare, then decode.
 std::vector<Batch> parquet_scan(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats);
+
+// The scan in two steps: the selected column chunks of every file read and
+// kept in HBM still compressed (with their page tables), then decoded on the
+// GPU as often as asked.
+struct ParquetPrepared;
+std::shared_ptr<ParquetPrepared> parquet_prepare(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats);
+std::vector<Batch> parquet_decode(Ctx& ctx, const ParquetPrepared& p, ParquetScanStats* stats);
+int64_t parquet_prepared_rows(const ParquetPrepared& p);
+int64_t parquet_prepared_bytes(const ParquetPrepared& p);
 // parquet_row_count (parquet_scan.rs:240-266): rows of the row groups the
 // predicate might match, from the footers alone.
 int64_t parquet_row_count(const std::vector<std::string>& uris, const prism_predicate* predicate);

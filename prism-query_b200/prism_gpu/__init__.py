@@ -124,6 +124,14 @@ def _declare(lib):
     lib.prism_server_destroy.restype = None
     lib.prism_parquet_scan.argtypes = [P, P, C.POINTER(C.POINTER(P)), C.POINTER(i32), P]
     lib.prism_parquet_row_count.argtypes = [P, i32, P, C.POINTER(C.c_int64)]
+    lib.prism_parquet_prepare.argtypes = [P, P, C.POINTER(P), P]
+    lib.prism_parquet_decode.argtypes = [P, P, C.POINTER(C.POINTER(P)), C.POINTER(i32), P]
+    lib.prism_parquet_prepared_rows.argtypes = [P]
+    lib.prism_parquet_prepared_rows.restype = C.c_int64
+    lib.prism_parquet_prepared_bytes.argtypes = [P]
+    lib.prism_parquet_prepared_bytes.restype = C.c_int64
+    lib.prism_parquet_prepared_free.argtypes = [P]
+    lib.prism_parquet_prepared_free.restype = None
     lib.prism_free_array.argtypes = [P]
     lib.prism_free_array.restype = None
     lib.prism_expand_worker_aggregates.argtypes = [P, P, i32, C.POINTER(i32)]
@@ -501,6 +509,28 @@ def _uri_array(uris: Sequence[str]):
     return arr, enc
 
 
+def _scan_config(uris, predicate, projection, batch_size, skip_expand):
+    arr, keep = _uri_array(uris)
+    pred = predicate.encode() if predicate is not None else None
+    proj = _abi.int_array(list(projection)) if projection is not None else None
+    cfg = _abi.prism_parquet_scan_config(arr, len(keep), C.cast(C.pointer(pred), C.c_void_p) if pred is not None else None,
+                                         proj, len(projection) if projection is not None else 0, batch_size,
+                                         1 if skip_expand else 0)
+    cfg._keep = (arr, keep, pred, proj)
+    return cfg
+
+
+def _batch_list(ctx, out, n, as_device):
+    try:
+        return [_result(ctx, C.c_void_p(out[i]), as_device) for i in range(n.value)]
+    finally:
+        lib().prism_free_array(C.cast(out, C.c_void_p))
+
+
+def _stats_dict(st):
+    return {f: getattr(st, f) for f, _ in st._fields_}
+
+
 def parquet_scan(uris: Sequence[str], predicate: Optional[Predicate] = None, projection: Optional[Sequence[int]] = None,
                  batch_size: int = 8192, skip_expand: bool = False, ctx: Optional[Context] = None, as_device=False,
                  with_stats=False):
@@ -508,23 +538,56 @@ def parquet_scan(uris: Sequence[str], predicate: Optional[Predicate] = None, pro
     batches (Arrow, or DeviceBatch with as_device); with_stats also returns
     the scan's counters (files, row groups read / skipped, pages, bytes)."""
     ctx = ctx or default_context()
-    arr, keep = _uri_array(uris)
-    pred = predicate.encode() if predicate is not None else None
-    proj = _abi.int_array(list(projection)) if projection is not None else None
-    cfg = _abi.prism_parquet_scan_config(arr, len(keep), C.cast(C.byref(pred), C.c_void_p) if pred is not None else None,
-                                         proj, len(projection) if projection is not None else 0, batch_size,
-                                         1 if skip_expand else 0)
+    cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand)
     out = C.POINTER(C.c_void_p)()
     n = C.c_int32(0)
     st = _abi.prism_parquet_scan_stats()
     ctx.check(lib().prism_parquet_scan(ctx.handle, C.byref(cfg), C.byref(out), C.byref(n), C.byref(st)))
-    try:
-        res = [_result(ctx, C.c_void_p(out[i]), as_device) for i in range(n.value)]
-    finally:
-        lib().prism_free_array(C.cast(out, C.c_void_p))
-    if with_stats:
-        return res, {f: getattr(st, f) for f, _ in st._fields_}
-    return res
+    res = _batch_list(ctx, out, n, as_device)
+    return (res, _stats_dict(st)) if with_stats else res
+
+
+class ParquetPrepared:
+    """A Parquet scan's column chunks kept in HBM still compressed
+    (prism_parquet_prepare); decode() runs the GPU decoder over them."""
+
+    def __init__(self, uris: Sequence[str], predicate: Optional[Predicate] = None,
+                 projection: Optional[Sequence[int]] = None, batch_size: int = 8192, skip_expand: bool = False,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand)
+        h = C.c_void_p()
+        st = _abi.prism_parquet_scan_stats()
+        self.ctx.check(lib().prism_parquet_prepare(self.ctx.handle, C.byref(cfg), C.byref(h), C.byref(st)))
+        self._h = h
+        self.stats = _stats_dict(st)
+
+    @property
+    def num_rows(self) -> int:
+        return int(lib().prism_parquet_prepared_rows(self._h))
+
+    @property
+    def compressed_bytes(self) -> int:
+        return int(lib().prism_parquet_prepared_bytes(self._h))
+
+    def decode(self, as_device=False, with_stats=False):
+        out = C.POINTER(C.c_void_p)()
+        n = C.c_int32(0)
+        st = _abi.prism_parquet_scan_stats()
+        self.ctx.check(lib().prism_parquet_decode(self.ctx.handle, self._h, C.byref(out), C.byref(n), C.byref(st)))
+        res = _batch_list(self.ctx, out, n, as_device)
+        return (res, _stats_dict(st)) if with_stats else res
+
+    def free(self):
+        if self._h:
+            lib().prism_parquet_prepared_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def parquet_row_count(uris: Sequence[str], predicate: Optional[Predicate] = None) -> int:

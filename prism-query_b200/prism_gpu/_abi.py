@@ -146,7 +146,7 @@ class prism_parquet_scan_config(C.Structure):
 
 class prism_parquet_scan_stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("files", "row_groups", "row_groups_skipped", "pages", "compressed_bytes",
-                                          "decoded_bytes")]
+                                          "inflated_bytes", "decoded_bytes")]
 
 
 class prism_sort_key(C.Structure):

@@ -171,3 +171,21 @@ def test_unsupported_and_malformed(ctx, tmp_path):
     with pytest.raises(prism_gpu.PrismError):
         prism_gpu.parquet_scan([str(tmp_path / "nothing-here")], ctx=ctx)
     assert os.path.exists(good)
+
+
+def test_prepared_decode_repeats_the_scan(ctx, tmp_path):
+    """prism_parquet_prepare keeps the compressed chunks in HBM; every decode
+    returns what prism_parquet_scan returns."""
+    t = PF.typed_table(40_000, seed=12)
+    path = str(tmp_path / "prep.parquet")
+    pq.write_table(t, path, row_group_size=9_000, compression="snappy")
+    pred = Predicate.Ge(9, ScalarValue.Int64(10_000))
+    prep = prism_gpu.ParquetPrepared([path], pred, projection=[3, 6, 9], batch_size=4096, ctx=ctx)
+    assert prep.num_rows == 40_000 - 9_000 and prep.stats["row_groups_skipped"] == 1
+    assert prep.compressed_bytes > 0
+    ref = oracle.parquet_scan([path], pred, projection=[3, 6, 9], batch_size=4096)
+    for _ in range(2):
+        got, st = prep.decode(with_stats=True)
+        _same(got, ref)
+        assert st["decoded_bytes"] > 0 and st["inflated_bytes"] > 0
+    prep.free()
