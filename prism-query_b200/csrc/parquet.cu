@@ -20,7 +20,9 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
 
 #include "arrow_io.hpp"
 #include "parquet.hpp"
@@ -75,34 +77,40 @@ struct SnappyJob {
   uint8_t* dst;
   int32_t src_len;
   int32_t dst_len;
+  int32_t preamble;    // the job starts its stream (reads the length varint)
+  int32_t stream_len;  // the stream's uncompressed length
 };
 
 // ---------------------------------------------------------------- snappy --
 // The Snappy format: a varint of the uncompressed length, then elements whose
 // tag's low two bits select a literal (length in the tag, or in 1-4 following
 // bytes when the tag says 60-63), or a copy of (length <= 64, offset) with a
-// 1-, 2- or 4-byte offset. One warp inflates one stream: lane 0 parses up to
-// SNAP_CMDS elements into a command queue in shared memory, then the warp
-// executes them in order, its lanes moving the bytes. The last SNAP_RING
-// output bytes are mirrored in a shared-memory ring, so a copy (its source
-// window [op - offset, op) stays intact while it writes at most 64 bytes)
-// reads shared memory unless its offset reaches past the ring.
+// 1-, 2- or 4-byte offset.
+//
+// A stream longer than 64 KB is cut on the host (snappy_segments) at the 64 KB
+// output boundaries that no later copy reaches back across (the reference
+// compressor works in independent 64 KB blocks, so every boundary qualifies
+// for its streams), and each segment is a job. One warp inflates one job, a
+// batch of elements at a time:
+//   1. the warp loads 64 input bytes; every lane decodes the element that
+//      would start at its byte (its header is within the window);
+//   2. a shuffle walk from lane 0 follows the real element starts (up to 32,
+//      until the batch writes SNAP_SPAN bytes or meets a literal longer than
+//      64 bytes, which gets a batch of its own);
+//   3. literals and copies whose source lies before the batch run in
+//      parallel, one lane per element; copies that read the batch's own
+//      output then run in order, the warp's lanes over their bytes.
+// The last SNAP_RING output bytes are mirrored in shared memory for copies
+// with offsets up to SNAP_RING_REACH; longer ones read the output in HBM.
 constexpr int SNAP_WARPS = 8;
-constexpr int SNAP_RING = 16384;  // power of two
-constexpr int SNAP_CMDS = 32;
-
-struct SnapCmd {
-  int32_t len;
-  int32_t off;  // 0: literal
-  int64_t src;  // literal: input offset
-};
+constexpr int SNAP_RING = 8192;  // power of two
+constexpr int SNAP_SPAN = 1024;
+constexpr int SNAP_RING_REACH = SNAP_RING - 2 * SNAP_SPAN;
+constexpr int64_t SNAP_BLOCK = 65536;
 
 __global__ void __launch_bounds__(32 * SNAP_WARPS) pq_snappy_kernel(const SnappyJob* jobs, int n, uint32_t* err) {
   extern __shared__ __align__(16) uint8_t snap_smem[];
-  __shared__ SnapCmd cmds[SNAP_WARPS][SNAP_CMDS];
-  __shared__ int32_t ncmd[SNAP_WARPS];
-  __shared__ int32_t state[SNAP_WARPS];  // 0 running, 1 done, 2 malformed
-  __shared__ int64_t in_pos[SNAP_WARPS];
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const int job = blockIdx.x * SNAP_WARPS + w;
@@ -113,100 +121,141 @@ __global__ void __launch_bounds__(32 * SNAP_WARPS) pq_snappy_kernel(const Snappy
   const int64_t in_len = J.src_len;
   uint8_t* const dst = J.dst;
   const int64_t out_len = J.dst_len;
-  if (lane == 0) {
+  bool bad = false;
+  int64_t ip = 0;
+  if (J.preamble) {
     uint32_t ulen = 0;
-    int64_t ip = 0;
-    bool ok = true;
-    for (int s = 0;; s += 7) {
-      if (ip >= in_len || s > 28) { ok = false; break; }
-      const uint8_t b = in[ip++];
+    int s = 0;
+    for (;; s += 7) {
+      if (ip >= in_len || s > 28) { bad = true; break; }
+      const uint8_t b = in[ip++];  // every lane reads the same bytes
       ulen |= (uint32_t)(b & 0x7f) << s;
       if (!(b & 0x80)) break;
     }
-    if (ulen != (uint32_t)out_len) ok = false;
-    state[w] = ok ? 0 : 2;
-    in_pos[w] = ip;
+    if (ulen != (uint32_t)J.stream_len) bad = true;
   }
-  __syncwarp();
   int64_t op = 0;
-  for (;;) {
-    const int run_state = state[w];
-    __syncwarp();  // every lane has read the state before lane 0 rewrites it
-    if (run_state != 0) break;
-    if (lane == 0) {  // parse up to SNAP_CMDS elements
-      int64_t ip = in_pos[w];
-      int64_t o = op;
-      int k = 0;
-      int st = 0;
-      while (k < SNAP_CMDS) {
-        if (ip >= in_len) { st = 1; break; }
-        const uint8_t tag = in[ip++];
-        const int t = tag & 3;
-        int64_t len, off = 0, src = 0;
-        if (t == 0) {
-          len = (tag >> 2) + 1;
-          if (len > 60) {
-            const int nb = (int)len - 60;
-            if (in_len - ip < nb) { st = 2; break; }
-            uint32_t v = 0;
-            for (int q = 0; q < nb; ++q) v |= (uint32_t)in[ip + q] << (8 * q);
-            ip += nb;
-            len = (int64_t)v + 1;
-          }
-          if (in_len - ip < len) { st = 2; break; }
-          src = ip;
-          ip += len;
-        } else {
-          const int nb = t == 1 ? 1 : (t == 2 ? 2 : 4);
-          if (in_len - ip < nb) { st = 2; break; }
-          if (t == 1) {
-            len = ((tag >> 2) & 7) + 4;
-            off = ((int64_t)(tag >> 5) << 8) | in[ip];
-          } else {
-            len = (tag >> 2) + 1;
-            off = 0;
-            for (int q = 0; q < nb; ++q) off |= (int64_t)in[ip + q] << (8 * q);
-          }
-          ip += nb;
-          if (off <= 0 || off > o) { st = 2; break; }
-        }
-        if (o + len > out_len || len > 0x7fffffff) { st = 2; break; }
-        cmds[w][k] = SnapCmd{(int32_t)len, (int32_t)off, src};
-        o += len;
-        ++k;
+  while (!bad && ip < in_len) {
+    const int64_t base = ip;
+    const uint32_t b0 = base + lane < in_len ? in[base + lane] : 0u;
+    const uint32_t b1 = base + 32 + lane < in_len ? in[base + 32 + lane] : 0u;
+    uint32_t nb[5];
+    nb[0] = b0;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) {
+      const uint32_t x = __shfl_down_sync(FULL, b0, k);
+      const uint32_t y = __shfl_sync(FULL, b1, (lane + k) & 31);
+      nb[k] = lane + k < 32 ? x : y;
+    }
+    // the element that would start at this lane's byte
+    const uint32_t tag = nb[0];
+    const int t = tag & 3;
+    int64_t len, elen_in;
+    uint32_t off = 0;
+    if (t == 0) {
+      const int l = (int)(tag >> 2);
+      if (l < 60) {
+        len = l + 1;
+        elen_in = 1 + len;
+      } else {
+        const int nbytes = l - 59;
+        uint32_t v = 0;
+        for (int q = 0; q < nbytes; ++q) v |= nb[1 + q] << (8 * q);
+        len = (int64_t)v + 1;
+        elen_in = 1 + nbytes + len;
       }
-      ncmd[w] = k;
-      in_pos[w] = ip;
-      state[w] = st;
+    } else if (t == 1) {
+      len = ((tag >> 2) & 7) + 4;
+      off = ((tag >> 5) << 8) | nb[1];
+      elen_in = 2;
+    } else if (t == 2) {
+      len = (tag >> 2) + 1;
+      off = nb[1] | (nb[2] << 8);
+      elen_in = 3;
+    } else {
+      len = (tag >> 2) + 1;
+      off = nb[1] | (nb[2] << 8) | (nb[3] << 16) | (nb[4] << 24);
+      elen_in = 5;
+    }
+    // walk the real element starts (uniform across the warp)
+    int64_t pos = 0, o = op;
+    int cnt = 0;
+    int64_t my_o = -1;
+    while (cnt < 32 && pos < 32 && base + pos < in_len) {
+      const int src_lane = (int)pos;
+      const int64_t e_in = __shfl_sync(FULL, elen_in, src_lane);
+      const int64_t e_len = __shfl_sync(FULL, len, src_lane);
+      const int e_t = __shfl_sync(FULL, t, src_lane);
+      const bool long_lit = e_t == 0 && e_len > 64;
+      if (cnt > 0 && long_lit) break;
+      if (lane == src_lane) my_o = o;
+      o += e_len;
+      pos += e_in;
+      ++cnt;
+      if (long_lit || o - op >= SNAP_SPAN) break;
+    }
+    const bool mine = my_o >= 0;
+    // element checks: inside the input, inside the output, copies after the job's start
+    bool ok = true;
+    if (mine) {
+      if (base + lane + elen_in > in_len || my_o + len > out_len) ok = false;
+      if (t != 0 && (off == 0 || (int64_t)off > my_o)) ok = false;
+    }
+    if (__any_sync(FULL, !ok)) {
+      bad = true;
+      break;
+    }
+    const int64_t batch_end = o;
+    const bool first_long = cnt == 1 && __shfl_sync(FULL, (int)(t == 0 && len > 64), 0);
+    // 3a. independent elements, one lane each
+    const bool indep_copy = mine && t != 0 && my_o - (int64_t)off + (len < (int64_t)off ? len : (int64_t)off) <= op;
+    if (mine && t == 0 && len <= 64) {
+      const uint8_t* src = in + base + lane + (elen_in - len);
+      for (int i = 0; i < (int)len; ++i) {
+        const uint8_t v = src[i];
+        dst[my_o + i] = v;
+        ring[(my_o + i) & (SNAP_RING - 1)] = v;
+      }
+    } else if (indep_copy) {
+      const bool near = off <= (uint32_t)SNAP_RING_REACH;
+      for (int i = 0; i < (int)len; ++i) {
+        const int64_t p = my_o - off + (i % off);
+        const uint8_t v = near ? ring[p & (SNAP_RING - 1)] : dst[p];
+        dst[my_o + i] = v;
+        ring[(my_o + i) & (SNAP_RING - 1)] = v;
+      }
     }
     __syncwarp();
-    const int k_end = ncmd[w];
-    for (int k = 0; k < k_end; ++k) {
-      const SnapCmd c = cmds[w][k];
-      if (c.off == 0) {
-        for (int64_t i = lane; i < c.len; i += 32) {
-          const uint8_t b = in[c.src + i];
-          dst[op + i] = b;
-          ring[(op + i) & (SNAP_RING - 1)] = b;
-        }
-      } else if (c.off <= SNAP_RING - 64) {
-        for (int i = lane; i < c.len; i += 32) {
-          const uint8_t b = ring[(op - c.off + (i % c.off)) & (SNAP_RING - 1)];
-          dst[op + i] = b;
-          ring[(op + i) & (SNAP_RING - 1)] = b;
-        }
-      } else {
-        for (int i = lane; i < c.len; i += 32) {
-          const uint8_t b = dst[op - c.off + (i % c.off)];
-          dst[op + i] = b;
-          ring[(op + i) & (SNAP_RING - 1)] = b;
-        }
+    if (first_long) {  // one long literal: the warp copies it
+      const int64_t L = __shfl_sync(FULL, len, 0);
+      const int64_t so = base + __shfl_sync(FULL, elen_in, 0) - L;
+      for (int64_t i = lane; i < L; i += 32) {
+        const uint8_t v = in[so + i];
+        dst[op + i] = v;
+        ring[(op + i) & (SNAP_RING - 1)] = v;
       }
-      op += c.len;
       __syncwarp();
     }
+    // 3b. copies that read this batch's output, in order
+    unsigned dep = __ballot_sync(FULL, mine && t != 0 && !indep_copy);
+    while (dep) {
+      const int sl = __ffs(dep) - 1;
+      dep &= dep - 1;
+      const int64_t eo = __shfl_sync(FULL, my_o, sl);
+      const uint32_t eoff = __shfl_sync(FULL, off, sl);
+      const int el = (int)__shfl_sync(FULL, len, sl);
+      for (int i = lane; i < el; i += 32) {
+        const int64_t p = eo - eoff + (i % eoff);
+        const uint8_t v = ring[p & (SNAP_RING - 1)];
+        dst[eo + i] = v;
+        ring[(eo + i) & (SNAP_RING - 1)] = v;
+      }
+      __syncwarp();
+    }
+    op = batch_end;
+    ip = base + pos;
   }
-  if (lane == 0 && (state[w] != 1 || op != out_len)) atomicOr(err, DERR_CORRUPT);
+  if (lane == 0 && (bad || op != out_len || ip != in_len)) atomicOr(err, DERR_CORRUPT);
 }
 
 // ------------------------------------------------------- hybrid streams --
@@ -607,6 +656,67 @@ __global__ void pq_slice_bits_kernel(const uint32_t* src, int64_t start, int64_t
 }
 
 // ------------------------------------------------------------ host side --
+struct SnapSeg {
+  int64_t in_off;
+  int64_t out_off;
+};
+
+// The points a Snappy stream can be cut at: element starts on 64 KB output
+// boundaries that no later copy reaches back across. Empty when the stream
+// is malformed (it is then inflated whole, and the kernel reports it).
+std::vector<SnapSeg> snappy_segments(const uint8_t* p, int64_t n, int64_t out_len) {
+  std::vector<SnapSeg> segs;
+  int64_t ip = 0;
+  uint64_t ulen = 0;
+  for (int s = 0;; s += 7) {
+    if (ip >= n || s > 28) return {};
+    const uint8_t b = p[ip++];
+    ulen |= (uint64_t)(b & 0x7f) << s;
+    if (!(b & 0x80)) break;
+  }
+  if ((int64_t)ulen != out_len) return {};
+  segs.push_back({0, 0});
+  int64_t op = 0;
+  while (ip < n) {
+    if (op > 0 && op % SNAP_BLOCK == 0 && segs.back().out_off != op) segs.push_back({ip, op});
+    const uint8_t tag = p[ip++];
+    const int t = tag & 3;
+    int64_t len;
+    if (t == 0) {
+      len = (tag >> 2) + 1;
+      if (len > 60) {
+        const int nb = (int)len - 60;
+        if (n - ip < nb) return {};
+        uint32_t v = 0;
+        for (int q = 0; q < nb; ++q) v |= (uint32_t)p[ip + q] << (8 * q);
+        ip += nb;
+        len = (int64_t)v + 1;
+      }
+      if (n - ip < len) return {};
+      ip += len;
+    } else {
+      const int nb = t == 1 ? 1 : (t == 2 ? 2 : 4);
+      if (n - ip < nb) return {};
+      int64_t off;
+      if (t == 1) {
+        len = ((tag >> 2) & 7) + 4;
+        off = ((int64_t)(tag >> 5) << 8) | p[ip];
+      } else {
+        len = (tag >> 2) + 1;
+        off = 0;
+        for (int q = 0; q < nb; ++q) off |= (int64_t)p[ip + q] << (8 * q);
+      }
+      ip += nb;
+      if (off <= 0 || off > op) return {};
+      while (segs.size() > 1 && op - off < segs.back().out_off) segs.pop_back();
+    }
+    op += len;
+    if (op > out_len) return {};
+  }
+  if (op != out_len) return {};
+  return segs;
+}
+
 struct FileHandle {
   int fd = -1;
   ~FileHandle() {
@@ -845,6 +955,7 @@ struct PreparedFile {
   std::vector<PqPage> pages;  // bodies of compressed pages are filled in per decode
   std::vector<PqDict> dicts;
   std::vector<PendingJob> pend;
+  std::vector<std::vector<SnapSeg>> segs;  // per pending stream: its cut points (empty: whole)
   std::vector<int32_t> plain_utf8;
   int64_t pos_total = 0;
   size_t unc_total = 0;
@@ -992,6 +1103,25 @@ PreparedFile prepare_file(Ctx& ctx, const std::string& path, FileHandle& fh, con
     }
     if (row != want_rows) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": column chunk rows differ from its row group");
   }
+  // cut points of the long Snappy streams, on every core
+  P.segs.resize(pend.size());
+  {
+    std::vector<size_t> longs;
+    for (size_t j = 0; j < pend.size(); ++j)
+      if (pend[j].dst_len > SNAP_BLOCK) longs.push_back(j);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+      for (size_t k; (k = next.fetch_add(1)) < longs.size();) {
+        const PendingJob& pj = pend[longs[k]];
+        P.segs[longs[k]] = snappy_segments(host + pj.chunk_src, pj.src_len, pj.dst_len);
+      }
+    };
+    const unsigned nt = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 32u);
+    std::vector<std::thread> pool;
+    for (unsigned q = 1; q < nt && q < longs.size(); ++q) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+  }
   (void)stats;
   ctx.sync();  // the staging buffer goes back to the pool on return
   return P;
@@ -1020,14 +1150,27 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
   MemP unc_mem = ctx.alloc(std::max<size_t>(P.unc_total, 16));
   uint8_t* unc = static_cast<uint8_t*>(unc_mem->ptr);
   size_t uo = 0;
-  for (const PendingJob& j : P.pend) {
+  for (size_t pj = 0; pj < P.pend.size(); ++pj) {
+    const PendingJob& j = P.pend[pj];
     if (j.dst_len < 0 || j.src_len < 0) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": negative page size");
     uint8_t* dst = unc + uo;
     uo += (size_t)((j.dst_len + 15) & ~15);
-    jobs.push_back({raw + j.chunk_src, dst, j.src_len, j.dst_len});
+    const std::vector<SnapSeg>& sg = P.segs[pj];
+    if (sg.size() < 2) {
+      jobs.push_back({raw + j.chunk_src, dst, j.src_len, j.dst_len, 1, j.dst_len});
+    } else {
+      for (size_t q = 0; q < sg.size(); ++q) {
+        const int64_t in_end = q + 1 < sg.size() ? sg[q + 1].in_off : j.src_len;
+        const int64_t out_end = q + 1 < sg.size() ? sg[q + 1].out_off : j.dst_len;
+        jobs.push_back({raw + j.chunk_src + sg[q].in_off, dst + sg[q].out_off, (int32_t)(in_end - sg[q].in_off),
+                        (int32_t)(out_end - sg[q].out_off), q == 0 ? 1 : 0, j.dst_len});
+      }
+    }
     if (j.kind == 0) pages[j.idx].body = dst;
     else dicts[j.idx].body = dst;
   }
+  // longest jobs first: the tail of the launch is the shortest work
+  std::stable_sort(jobs.begin(), jobs.end(), [](const SnappyJob& a, const SnappyJob& b) { return a.dst_len > b.dst_len; });
 
   // 4. outputs: one carve per file
   std::vector<PqOut> outs(chunks.size());

@@ -189,3 +189,25 @@ def test_prepared_decode_repeats_the_scan(ctx, tmp_path):
         _same(got, ref)
         assert st["decoded_bytes"] > 0 and st["inflated_bytes"] > 0
     prep.free()
+
+
+@pytest.mark.parametrize("version", ["1.0", "2.0"])
+def test_long_snappy_streams(ctx, tmp_path, version):
+    """Pages and dictionaries far longer than one 64 KB Snappy block (the
+    streams are cut at block boundaries and inflated in parallel): sorted
+    int64 (short copies reaching back 8 bytes), random bytes (long literals),
+    long runs (overlapping copies), a 1 MB dictionary page."""
+    rng = np.random.default_rng(77)
+    n = 400_000
+    t = pa.table({
+        "sorted": pa.array(np.sort(rng.integers(0, 10**9, n))),
+        "noise": pa.array(rng.random(n)),
+        "runs": pa.array(np.repeat(rng.integers(0, 5, n // 1000), 1000)),
+        "words": pa.array(np.array([f"w{i:06d}" for i in range(60_000)])[rng.integers(0, 60_000, n)]),
+    })
+    path = str(tmp_path / "long.parquet")
+    pq.write_table(t, path, row_group_size=n, data_page_size=4 << 20, compression="snappy", data_page_version=version,
+                   write_batch_size=n)
+    got, st = prism_gpu.parquet_scan([path], batch_size=1 << 20, ctx=ctx, with_stats=True)
+    _same(got, oracle.parquet_scan([path], batch_size=1 << 20))
+    assert st["inflated_bytes"] > 4 * 65536
