@@ -472,7 +472,10 @@ int prism_parquet_scan(prism_ctx* ctx, const prism_parquet_scan_config* config, 
  * row-group and column selection as prism_parquet_scan) into device memory
  * and walks its page headers; prism_parquet_decode decodes the prepared
  * chunks on the GPU into batches, as often as called (each call returns new
- * batches, as prism_parquet_scan would). No counterpart in the reference. */
+ * batches, as prism_parquet_scan would), on the context that prepared them
+ * (their inflate buffer is reused, in that context's stream order). A
+ * prepared scan holds the compressed chunks plus that buffer (the inflated
+ * page bytes). No counterpart in the reference. */
 typedef struct prism_parquet_prepared prism_parquet_prepared;
 int prism_parquet_prepare(prism_ctx* ctx, const prism_parquet_scan_config* config, prism_parquet_prepared** out,
                           prism_parquet_scan_stats* stats);

@@ -960,6 +960,10 @@ struct PreparedFile {
   int64_t pos_total = 0;
   size_t unc_total = 0;
   int64_t staged = 0;
+  int64_t inflated = 0;
+  // device side, built once: the inflate target and the kernels' tables
+  MemP unc_mem, jobs_dev, pages_dev, dicts_dev, list_dev, dstarts_mem, dlens_mem;
+  int64_t n_jobs = 0;
 };
 
 // Reads the selected chunks of one file into HBM and walks their pages.
@@ -1122,6 +1126,54 @@ PreparedFile prepare_file(Ctx& ctx, const std::string& path, FileHandle& fh, con
     work();
     for (auto& th : pool) th.join();
   }
+  // inflate targets and Snappy jobs (segments of long streams), longest first
+  P.unc_mem = ctx.alloc(std::max<size_t>(unc_total, 16));
+  uint8_t* unc = static_cast<uint8_t*>(P.unc_mem->ptr);
+  std::vector<SnappyJob> jobs;
+  size_t uo = 0;
+  for (size_t pj = 0; pj < pend.size(); ++pj) {
+    const PendingJob& j = pend[pj];
+    if (j.dst_len < 0 || j.src_len < 0) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": negative page size");
+    uint8_t* dstp = unc + uo;
+    uo += (size_t)((j.dst_len + 15) & ~15);
+    P.inflated += j.dst_len;
+    const std::vector<SnapSeg>& sg = P.segs[pj];
+    if (sg.size() < 2) {
+      jobs.push_back({raw + j.chunk_src, dstp, j.src_len, j.dst_len, 1, j.dst_len});
+    } else {
+      for (size_t q = 0; q < sg.size(); ++q) {
+        const int64_t in_end = q + 1 < sg.size() ? sg[q + 1].in_off : j.src_len;
+        const int64_t out_end = q + 1 < sg.size() ? sg[q + 1].out_off : j.dst_len;
+        jobs.push_back({raw + j.chunk_src + sg[q].in_off, dstp + sg[q].out_off, (int32_t)(in_end - sg[q].in_off),
+                        (int32_t)(out_end - sg[q].out_off), q == 0 ? 1 : 0, j.dst_len});
+      }
+    }
+    if (j.kind == 0) pages[j.idx].body = dstp;
+    else dicts[j.idx].body = dstp;
+  }
+  std::stable_sort(jobs.begin(), jobs.end(), [](const SnappyJob& a, const SnappyJob& b) { return a.dst_len > b.dst_len; });
+  P.n_jobs = (int64_t)jobs.size();
+  // byte-array dictionaries: room for their value starts / lengths
+  int64_t dict_slots = 0;
+  for (auto& d : dicts)
+    if (d.type == TY_UTF8) dict_slots += d.count;
+  uint32_t* ds = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(dict_slots, 1), P.dstarts_mem);
+  uint32_t* dl = ctx.alloc_t<uint32_t>((size_t)std::max<int64_t>(dict_slots, 1), P.dlens_mem);
+  int64_t at = 0;
+  for (auto& d : dicts)
+    if (d.type == TY_UTF8) {
+      d.starts = ds + at;
+      d.lens = dl + at;
+      at += d.count;
+    }
+  auto upload = [&](const void* src, size_t bytes, MemP& hold) {
+    hold = ctx.alloc(std::max<size_t>(bytes, 16));
+    if (bytes) PRISM_CUDA(cudaMemcpyAsync(hold->ptr, src, bytes, cudaMemcpyHostToDevice, ctx.stream));
+  };
+  upload(jobs.data(), jobs.size() * sizeof(SnappyJob), P.jobs_dev);
+  upload(pages.data(), pages.size() * sizeof(PqPage), P.pages_dev);
+  upload(dicts.data(), dicts.size() * sizeof(PqDict), P.dicts_dev);
+  upload(plain_utf8.data(), plain_utf8.size() * 4, P.list_dev);
   (void)stats;
   ctx.sync();  // the staging buffer goes back to the pool on return
   return P;
@@ -1134,43 +1186,16 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
   const std::vector<int>& rgs = P.rgs;
   const std::vector<ColPlan>& plan = P.plan;
   const std::vector<Chunk>& chunks = P.chunks;
-  uint8_t* raw = static_cast<uint8_t*>(P.raw_mem->ptr);
-  std::vector<PqPage> pages = P.pages;
-  std::vector<PqDict> dicts = P.dicts;
+  const std::vector<PqPage>& pages = P.pages;
+  const std::vector<PqDict>& dicts = P.dicts;
   const std::vector<int32_t>& plain_utf8 = P.plain_utf8;
   const int64_t pos_total = P.pos_total;
-  std::vector<SnappyJob> jobs;
   std::vector<RgOut> res(rgs.size());
   if (stats) {
     stats->pages += (int64_t)pages.size();
     stats->compressed_bytes += P.staged;
-    for (const PendingJob& j : P.pend) stats->inflated_bytes += j.dst_len;
+    stats->inflated_bytes += P.inflated;
   }
-  // decompression targets
-  MemP unc_mem = ctx.alloc(std::max<size_t>(P.unc_total, 16));
-  uint8_t* unc = static_cast<uint8_t*>(unc_mem->ptr);
-  size_t uo = 0;
-  for (size_t pj = 0; pj < P.pend.size(); ++pj) {
-    const PendingJob& j = P.pend[pj];
-    if (j.dst_len < 0 || j.src_len < 0) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": negative page size");
-    uint8_t* dst = unc + uo;
-    uo += (size_t)((j.dst_len + 15) & ~15);
-    const std::vector<SnapSeg>& sg = P.segs[pj];
-    if (sg.size() < 2) {
-      jobs.push_back({raw + j.chunk_src, dst, j.src_len, j.dst_len, 1, j.dst_len});
-    } else {
-      for (size_t q = 0; q < sg.size(); ++q) {
-        const int64_t in_end = q + 1 < sg.size() ? sg[q + 1].in_off : j.src_len;
-        const int64_t out_end = q + 1 < sg.size() ? sg[q + 1].out_off : j.dst_len;
-        jobs.push_back({raw + j.chunk_src + sg[q].in_off, dst + sg[q].out_off, (int32_t)(in_end - sg[q].in_off),
-                        (int32_t)(out_end - sg[q].out_off), q == 0 ? 1 : 0, j.dst_len});
-      }
-    }
-    if (j.kind == 0) pages[j.idx].body = dst;
-    else dicts[j.idx].body = dst;
-  }
-  // longest jobs first: the tail of the launch is the shortest work
-  std::stable_sort(jobs.begin(), jobs.end(), [](const SnappyJob& a, const SnappyJob& b) { return a.dst_len > b.dst_len; });
 
   // 4. outputs: one carve per file
   std::vector<PqOut> outs(chunks.size());
@@ -1235,51 +1260,34 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     if (bytes) PRISM_CUDA(cudaMemcpyAsync(hold->ptr, src, bytes, cudaMemcpyHostToDevice, ctx.stream));
     return hold->ptr;
   };
-  MemP jobs_mem, dicts_mem, pages_mem, outs_mem, list_mem;
-  if (!jobs.empty()) {
-    auto* dj = static_cast<SnappyJob*>(upload(jobs.data(), jobs.size() * sizeof(SnappyJob), jobs_mem));
+  MemP outs_mem, list_mem;
+  if (P.n_jobs) {
     KernelTimer kt(ctx, "pq_snappy_kernel");
     static const bool attr = [] {
       return cudaFuncSetAttribute(pq_snappy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   SNAP_WARPS * SNAP_RING) == cudaSuccess;
     }();
     if (!attr) fail(PRISM_ERR_CUDA, "cannot reserve shared memory for pq_snappy_kernel");
-    pq_snappy_kernel<<<(unsigned)((jobs.size() + SNAP_WARPS - 1) / SNAP_WARPS), 32 * SNAP_WARPS,
-                       SNAP_WARPS * SNAP_RING, ctx.stream>>>(dj, (int)jobs.size(), err);
+    pq_snappy_kernel<<<(unsigned)((P.n_jobs + SNAP_WARPS - 1) / SNAP_WARPS), 32 * SNAP_WARPS, SNAP_WARPS * SNAP_RING,
+                       ctx.stream>>>(static_cast<const SnappyJob*>(P.jobs_dev->ptr), (int)P.n_jobs, err);
     ctx.note_launch();
     ctx.check_launch("pq_snappy_kernel");
   }
-  // dictionaries of byte arrays: starts / lengths
-  MemP dstarts_mem, dlens_mem;
-  {
-    int64_t dict_slots = 0;
-    for (auto& d : dicts)
-      if (d.type == TY_UTF8) dict_slots += d.count;
-    uint32_t* ds = dict_slots ? ctx.alloc_t<uint32_t>((size_t)dict_slots, dstarts_mem) : nullptr;
-    uint32_t* dl = dict_slots ? ctx.alloc_t<uint32_t>((size_t)dict_slots, dlens_mem) : nullptr;
-    int64_t at = 0;
-    for (auto& d : dicts)
-      if (d.type == TY_UTF8) {
-        d.starts = ds + at;
-        d.lens = dl + at;
-        at += d.count;
-      }
-  }
-  PqDict* ddicts = static_cast<PqDict*>(upload(dicts.data(), dicts.size() * sizeof(PqDict), dicts_mem));
+  PqDict* ddicts = static_cast<PqDict*>(P.dicts_dev->ptr);
   if (!dicts.empty()) {
     KernelTimer kt(ctx, "pq_dict_kernel");
     pq_dict_kernel<<<(unsigned)((dicts.size() + 127) / 128), 128, 0, ctx.stream>>>(ddicts, (int)dicts.size(), err);
     ctx.note_launch();
     ctx.check_launch("pq_dict_kernel");
   }
-  PqPage* dpages = static_cast<PqPage*>(upload(pages.data(), pages.size() * sizeof(PqPage), pages_mem));
+  PqPage* dpages = static_cast<PqPage*>(P.pages_dev->ptr);
   PqOut* douts = static_cast<PqOut*>(upload(outs.data(), outs.size() * sizeof(PqOut), outs_mem));
   MemP pstart_mem, plen_mem, pfound_mem;
   uint32_t* pstarts = pos_total ? ctx.alloc_t<uint32_t>((size_t)pos_total, pstart_mem) : nullptr;
   uint32_t* plens = pos_total ? ctx.alloc_t<uint32_t>((size_t)pos_total, plen_mem) : nullptr;
   int32_t* pfound = ctx.alloc_t<int32_t>(std::max<size_t>(pages.size(), 1), pfound_mem);
   if (!plain_utf8.empty()) {
-    auto* dl = static_cast<int32_t*>(upload(plain_utf8.data(), plain_utf8.size() * 4, list_mem));
+    auto* dl = static_cast<int32_t*>(P.list_dev->ptr);
     KernelTimer kt(ctx, "pq_positions_kernel");
     pq_positions_kernel<<<(unsigned)((plain_utf8.size() + 127) / 128), 128, 0, ctx.stream>>>(
         dpages, dl, (int)plain_utf8.size(), pstarts, plens, pfound, err);
@@ -1472,6 +1480,7 @@ int64_t parquet_row_count(const std::vector<std::string>& uris, const prism_pred
 }
 
 struct ParquetPrepared {
+  const Ctx* owner = nullptr;  // decodes run on the preparing context's stream (they share the inflate buffer)
   ParquetScanArgs args;
   std::vector<Leaf> full;  // the first file's schema
   std::vector<PreparedFile> files;
@@ -1480,6 +1489,7 @@ struct ParquetPrepared {
 
 std::shared_ptr<ParquetPrepared> parquet_prepare(Ctx& ctx, const ParquetScanArgs& args, ParquetScanStats* stats) {
   auto P = std::make_shared<ParquetPrepared>();
+  P->owner = &ctx;
   P->args = args;
   P->args.predicate = nullptr;  // used here only: the caller's predicate need not outlive this call
   if (args.uris.empty()) return P;
@@ -1542,6 +1552,7 @@ int64_t parquet_prepared_bytes(const ParquetPrepared& P) {
 }
 
 std::vector<Batch> parquet_decode(Ctx& ctx, const ParquetPrepared& P, ParquetScanStats* stats) {
+  if (P.owner != &ctx) fail(PRISM_ERR_INVALID_ARGUMENT, "a prepared Parquet scan decodes on the context that prepared it");
   const ParquetScanArgs& args = P.args;
   std::vector<Batch> out;
   for (const PreparedFile& F : P.files) {
