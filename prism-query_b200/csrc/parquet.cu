@@ -547,8 +547,10 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
         const int w = (r - lo) >> 5, b = (r - lo) & 31;
         const int64_t row = pg.out_row + r;
         const uint32_t word = s_word[w];
-        if (!((word >> b) & 1)) {
+        if (!((word >> b) & 1)) {  // a null row: zero length / zero value
           if (pg.type == TY_UTF8) O.lens[row] = 0;
+          else if (pg.type == TY_I64 || pg.type == TY_F64) static_cast<unsigned long long*>(O.values)[row] = 0;
+          else static_cast<uint32_t*>(O.values)[row] = 0;
           continue;
         }
         const int32_t j = jbase + (int32_t)s_pre[w] + __popc(word & ((1u << b) - 1));
@@ -625,9 +627,14 @@ __global__ void pq_copy_kernel(const unsigned long long* srcs, const uint32_t* l
     const uint32_t L = r < n ? lens[r] : 0;
     const unsigned long long s = r < n ? srcs[r] : 0;
     const unsigned long long d = r < n ? g[r] : 0;
+    if (L <= 16) {  // short strings: each lane its own row
+      const uint8_t* sp = reinterpret_cast<const uint8_t*>(s);
+      uint8_t* dp = data + d;
+      for (uint32_t i = 0; i < L; ++i) dp[i] = sp[i];
+    }
     for (int k = 0; k < 32; ++k) {
       const uint32_t Lk = __shfl_sync(0xffffffffu, L, k);
-      if (!Lk) continue;
+      if (Lk <= 16) continue;
       const uint8_t* sp = reinterpret_cast<const uint8_t*>(__shfl_sync(0xffffffffu, s, k));
       uint8_t* dp = data + __shfl_sync(0xffffffffu, d, k);
       for (uint32_t i = lane; i < Lk; i += 32) dp[i] = sp[i];
@@ -1228,18 +1235,21 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
   std::vector<SegView> segs;
   std::vector<int> seg_of_chunk(chunks.size(), -1);
   int64_t urow = 0;
+  // bitmaps (validity, boolean values) first, zeroed by one memset: the page
+  // kernel ORs bits into them; fixed-width values are written for every row
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    const ColPlan& cp = plan[chunks[ci].c];
+    const int64_t n = m.row_groups[chunks[ci].rg].num_rows;
+    if (cp.optional) outs[ci].valid = static_cast<uint32_t*>(cv.take(words(n)));
+    if (cp.type == TY_BOOL) outs[ci].values = cv.take(words(n));
+  }
+  if (cv.used) PRISM_CUDA(cudaMemsetAsync(cv.base, 0, cv.used, ctx.stream));
   for (size_t ci = 0; ci < chunks.size(); ++ci) {
     const Chunk& ch = chunks[ci];
     const ColPlan& cp = plan[ch.c];
     const int64_t n = m.row_groups[ch.rg].num_rows;
     PqOut& o = outs[ci];
-    if (cp.optional) {
-      o.valid = static_cast<uint32_t*>(cv.take(words(n)));
-      PRISM_CUDA(cudaMemsetAsync(o.valid, 0, words(n), ctx.stream));
-    }
     if (cp.type == TY_BOOL) {
-      o.values = cv.take(words(n));
-      PRISM_CUDA(cudaMemsetAsync(o.values, 0, words(n), ctx.stream));
     } else if (cp.type == TY_UTF8) {
       o.lens = ulens + urow;
       o.srcs = usrcs + urow;
@@ -1247,9 +1257,7 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
       segs.push_back({urow, 0, n});
       urow += n + 1;
     } else {
-      const size_t b = (size_t)std::max<int64_t>(n, 1) * width_of(cp.type);
-      o.values = cv.take(b);
-      if (cp.optional) PRISM_CUDA(cudaMemsetAsync(o.values, 0, b, ctx.stream));
+      o.values = cv.take((size_t)std::max<int64_t>(n, 1) * width_of(cp.type));
     }
   }
 
