@@ -305,7 +305,7 @@ def main():
             },
             "roofline": {
                 "bound": "hbm",
-                "kernel": "probe phase (probe_rows_kernel + emit_rows_kernel)",
+                "kernel": "probe phase (" + " + ".join(k for k, v in kstats.items() if v[0]) + ")",
                 "kernel_ms_per_launch": {k: (v[1] / v[0] if v[0] else None) for k, v in kstats.items()},
                 "achieved": achieved,
                 "peak": peak,

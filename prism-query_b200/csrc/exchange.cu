@@ -356,7 +356,6 @@ Batch merge_partial_aggregates(Ctx& ctx, const std::vector<const Batch*>& partia
     const DCol cnt = kind == RB_AVG ? merged.cols[nk + w.map[2 * i + 1]]->view() : src;
     if (n > 0) {
       rebuild_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(kind, src, cnt, col->values, n);
-      ctx.note_launch();
       ctx.check_launch("rebuild_kernel");
     }
     out.cols.push_back(col);

@@ -1278,14 +1278,12 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     if (!attr) fail(PRISM_ERR_CUDA, "cannot reserve shared memory for pq_snappy_kernel");
     pq_snappy_kernel<<<(unsigned)((P.n_jobs + SNAP_WARPS - 1) / SNAP_WARPS), 32 * SNAP_WARPS, SNAP_WARPS * SNAP_RING,
                        ctx.stream>>>(static_cast<const SnappyJob*>(P.jobs_dev->ptr), (int)P.n_jobs, err);
-    ctx.note_launch();
     ctx.check_launch("pq_snappy_kernel");
   }
   PqDict* ddicts = static_cast<PqDict*>(P.dicts_dev->ptr);
   if (!dicts.empty()) {
     KernelTimer kt(ctx, "pq_dict_kernel");
     pq_dict_kernel<<<(unsigned)((dicts.size() + 127) / 128), 128, 0, ctx.stream>>>(ddicts, (int)dicts.size(), err);
-    ctx.note_launch();
     ctx.check_launch("pq_dict_kernel");
   }
   PqPage* dpages = static_cast<PqPage*>(P.pages_dev->ptr);
@@ -1299,14 +1297,12 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     KernelTimer kt(ctx, "pq_positions_kernel");
     pq_positions_kernel<<<(unsigned)((plain_utf8.size() + 127) / 128), 128, 0, ctx.stream>>>(
         dpages, dl, (int)plain_utf8.size(), pstarts, plens, pfound, err);
-    ctx.note_launch();
     ctx.check_launch("pq_positions_kernel");
   }
   if (!pages.empty()) {
     KernelTimer kt(ctx, "pq_page_kernel");
     pq_page_kernel<<<(unsigned)pages.size(), PQ_THREADS, 0, ctx.stream>>>(dpages, douts, ddicts, pstarts, plens, pfound,
                                                                           err);
-    ctx.note_launch();
     ctx.check_launch("pq_page_kernel");
   }
   // 6. Utf8: offsets and bytes
@@ -1328,7 +1324,6 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     auto* dat = static_cast<int64_t*>(upload(at.data(), at.size() * 8, at_mem));
     unsigned long long* gb = ctx.alloc_t<unsigned long long>(at.size(), gb_mem);
     pq_gather_u64_kernel<<<(unsigned)((at.size() + 127) / 128), 128, 0, ctx.stream>>>(ug, dat, (int)at.size(), gb);
-    ctx.note_launch();
     ctx.check_launch("pq_gather_u64_kernel");
     seg_bounds.resize(at.size() + 1);
     PRISM_CUDA(cudaMemcpyAsync(seg_bounds.data(), gb, at.size() * 8, cudaMemcpyDeviceToHost, ctx.stream));
@@ -1348,12 +1343,10 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     MemP seg_mem;
     auto* dsegs = static_cast<SegView*>(upload(segs.data(), segs.size() * sizeof(SegView), seg_mem));
     pq_seg_offsets_kernel<<<dim3(64, (unsigned)segs.size()), 256, 0, ctx.stream>>>(ug, dsegs, (int)segs.size(), offs);
-    ctx.note_launch();
     ctx.check_launch("pq_seg_offsets_kernel");
     {
       KernelTimer kt(ctx, "pq_copy_kernel");
       pq_copy_kernel<<<grid_for(ctx, (utf8_rows + 7) / 8, 256), 256, 0, ctx.stream>>>(usrcs, ulens, ug, utf8_rows, data);
-      ctx.note_launch();
       ctx.check_launch("pq_copy_kernel");
     }
     for (size_t ci = 0; ci < chunks.size(); ++ci) {
@@ -1414,7 +1407,6 @@ ColP slice_column(Ctx& ctx, const ColP& c, int64_t start, int64_t n, const std::
       uint32_t* dst = ctx.alloc_t<uint32_t>((size_t)((n + 31) / 32 + 1), m);
       pq_slice_bits_kernel<<<grid_for(ctx, (n + 31) / 32, 256), 256, 0, ctx.stream>>>(
           reinterpret_cast<const uint32_t*>(c->validity), start, n, dst);
-      ctx.note_launch();
       ctx.check_launch("pq_slice_bits_kernel");
       s->validity = reinterpret_cast<uint8_t*>(dst);
       s->owners.push_back(m);
@@ -1425,7 +1417,6 @@ ColP slice_column(Ctx& ctx, const ColP& c, int64_t start, int64_t n, const std::
     uint32_t* dst = ctx.alloc_t<uint32_t>((size_t)((n + 31) / 32 + 1), m);
     pq_slice_bits_kernel<<<grid_for(ctx, (n + 31) / 32, 256), 256, 0, ctx.stream>>>(
         static_cast<const uint32_t*>(c->values), start, n, dst);
-    ctx.note_launch();
     ctx.check_launch("pq_slice_bits_kernel");
     s->values = dst;
     s->owners.push_back(m);
