@@ -699,6 +699,7 @@ class C4:
 class SortW:
     """ORDER BY a Float64 key over 100M rows (sort.rs:35-78), full or top-N."""
     name = "sort"
+    metric = "sort input rows/s"
     dtype = "f64 key, int64 payload"
     flush_l2 = False
 

@@ -76,9 +76,19 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
   __shared__ uint32_t run[256];      // elements of each digit this tile has placed
   __shared__ uint32_t wc[RW][256];   // this round: each warp's count per digit
   __shared__ uint32_t total[RW];
+  __shared__ unsigned long long goff[256];  // the digit's global offset for this tile, minus its tile-local start
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t base = (int64_t)blockIdx.x * RT;
   const int count = (int)min((int64_t)RT, n - base);
+  // all of this thread's elements in flight at once, before the first barrier
+  uint64_t keys[RR];
+  uint32_t vals[RR];
+#pragma unroll
+  for (int r = 0; r < RR; ++r) {
+    const int e = r * RB + tid;
+    keys[r] = e < count ? kin[base + e] : 0;
+    vals[r] = e < count ? vin[base + e] : 0;
+  }
   // tile-local digit starts: exclusive scan of this tile's digit counts
 #pragma unroll
   for (int w = 0; w < RW; ++w) wc[w][tid] = 0;
@@ -96,18 +106,16 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
     for (int w = 0; w < warp; ++w) before += total[w];
     start[tid] = before + incl - x;
     run[tid] = 0;
+    goff[tid] = offsets[(int64_t)tid * ntiles + blockIdx.x] - (before + incl - x);
   }
   __syncthreads();
+#pragma unroll
   for (int r = 0; r < RR; ++r) {
     const int e = r * RB + tid;
     const bool valid = e < count;
-    uint64_t key = 0;
-    uint32_t val = 0, d = 256u;  // 256: no element
-    if (valid) {
-      key = kin[base + e];
-      val = vin[base + e];
-      d = (uint32_t)(key >> shift) & mask;
-    }
+    const uint64_t key = keys[r];
+    const uint32_t val = vals[r];
+    const uint32_t d = valid ? (uint32_t)(key >> shift) & mask : 256u;  // 256: no element
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
     if (valid && rank == 0) wc[warp][d] = __popc(peers);
@@ -134,7 +142,7 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
   for (int j = tid; j < count; j += RB) {
     const uint64_t key = sk[j];
     const uint32_t d = (uint32_t)(key >> shift) & mask;
-    const uint64_t pos = offsets[(int64_t)d * ntiles + blockIdx.x] + (uint32_t)(j - start[d]);
+    const uint64_t pos = goff[d] + (uint64_t)j;
     kout[pos] = key;
     vout[pos] = sv[j];
   }
