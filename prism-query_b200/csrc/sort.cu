@@ -47,11 +47,15 @@ __global__ void __launch_bounds__(RB) radix_hist_kernel(const uint64_t* __restri
   h[tid] = 0;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * RT;
-#pragma unroll 4
+  uint64_t w[RR];  // every load in flight before the first atomic
+#pragma unroll
   for (int r = 0; r < RR; ++r) {
     const int64_t i = base + r * RB + tid;
-    if (i < n) atomicAdd(&h[(uint32_t)(k[i] >> shift) & mask], 1u);
+    w[r] = i < n ? k[i] : 0;
   }
+#pragma unroll
+  for (int r = 0; r < RR; ++r)
+    if (base + r * RB + tid < n) atomicAdd(&h[(uint32_t)(w[r] >> shift) & mask], 1u);
   __syncthreads();
   counts[(int64_t)tid * ntiles + blockIdx.x] = h[tid];
 }
@@ -170,6 +174,36 @@ __device__ __forceinline__ uint64_t fixed_word(const DCol& c, int64_t row, int b
   const uint64_t m = bits == 64 ? ~0ULL : ((1ULL << bits) - 1);
   u &= m;
   return desc ? (~u & m) : u;
+}
+
+// The inverse of fixed_word for a key without nulls: a sorted column's values
+// straight from its sorted order words (a sequential pass instead of a
+// gather through the row ids).
+__global__ void decode_fixed_kernel(const uint64_t* __restrict__ k, int64_t n, int type, int bits, int desc,
+                                    void* __restrict__ out) {
+  const uint64_t m = bits == 64 ? ~0ULL : ((1ULL << bits) - 1);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t u = k[i] & m;
+    if (desc) u = ~u & m;
+    switch (type) {
+      case TY_U8: static_cast<uint8_t*>(out)[i] = (uint8_t)u; break;
+      case TY_U16: static_cast<uint16_t*>(out)[i] = (uint16_t)u; break;
+      case TY_U32: static_cast<uint32_t*>(out)[i] = (uint32_t)u; break;
+      case TY_U64: static_cast<uint64_t*>(out)[i] = u; break;
+      case TY_I8: static_cast<uint8_t*>(out)[i] = (uint8_t)(u ^ (1ULL << 7)); break;
+      case TY_I16: static_cast<uint16_t*>(out)[i] = (uint16_t)(u ^ (1ULL << 15)); break;
+      case TY_I32: case TY_DATE32: static_cast<uint32_t*>(out)[i] = (uint32_t)(u ^ (1ULL << 31)); break;
+      case TY_I64: static_cast<uint64_t*>(out)[i] = u ^ (1ULL << 63); break;
+      case TY_F64: static_cast<double*>(out)[i] = from_total_key((int64_t)(u ^ (1ULL << 63))); break;
+      case TY_F32: {
+        int32_t x = (int32_t)(uint32_t)(u ^ (1ULL << 31));
+        x ^= (int32_t)(((uint32_t)(x >> 31)) >> 1);
+        static_cast<int32_t*>(out)[i] = x;
+        break;
+      }
+      default: break;
+    }
+  }
 }
 
 __global__ void encode_fixed_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t n, int bits, int desc,
@@ -463,7 +497,25 @@ Batch sort_batch(Ctx& ctx, const Batch& b, const prism_sort_key* keys, int n_key
   const int64_t outn = limit >= 0 ? std::min(limit, m) : m;
   Batch out;
   out.rows = outn;
-  for (auto& c : b.cols) out.cols.push_back(take(ctx, *c, s.va, nullptr, outn, c->name, c->nullable));
+  // the most significant key, fixed width without nulls: its sorted order
+  // words (the last word sorted) decode back into the output column
+  const Column& k0 = *b.cols[keys[0].column];
+  const bool decode_k0 = !k0.validity && k0.type != TY_BOOL && key_bits(k0.type) > 0;
+  for (size_t ci = 0; ci < b.cols.size(); ++ci) {
+    const auto& c = b.cols[ci];
+    if (decode_k0 && (int)ci == keys[0].column) {
+      ColP d = make_column(ctx, c->type, c->name, outn, false);
+      d->nullable = c->nullable;
+      if (outn) {
+        decode_fixed_kernel<<<grid_for(ctx, outn, 256), 256, 0, ctx.stream>>>(s.ka, outn, c->type, key_bits(c->type),
+                                                                              keys[0].descending ? 1 : 0, d->values);
+        ctx.check_launch("decode_fixed_kernel");
+      }
+      out.cols.push_back(d);
+      continue;
+    }
+    out.cols.push_back(take(ctx, *c, s.va, nullptr, outn, c->name, c->nullable));
+  }
   return out;  // stream-ordered: the sort buffers are freed after the gathers
 
 }
