@@ -64,7 +64,7 @@ def parse():
                     help="scale all sizes (profiling captures use a smaller case; bench lines use 1.0)")
     a = ap.parse_args()
     if a.steps is None:
-        a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1, "sort": 10, "topn": 10}[a.workload]
+        a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1, "sort": 10, "topn": 10, "parquet": 10}[a.workload]
     global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE
     SCALE = a.scale
     if a.scale != 1.0:
