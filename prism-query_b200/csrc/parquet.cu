@@ -473,11 +473,15 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
   const PqDict* D = pg.dict >= 0 ? dicts + pg.dict : nullptr;
   int32_t jbase = 0;
   bool bad = false;
+  // Each round: warp 0 alone parses the level runs, builds the round's 32
+  // validity words, scans their populations and parses the index runs (warp
+  // barriers only); then every thread writes values. Two block barriers.
   for (int32_t lo = 0; lo < pg.rows; lo += PQ_CHUNK) {
     const int32_t hi = min(lo + PQ_CHUNK, pg.rows);
     const int nw = (hi - lo + 31) >> 5;
+    if (tid < 32) {
     if (pg.optional && tid == 0) fill_runs(def_runs, dc, lo, hi);
-    __syncthreads();
+    __syncwarp();
     // validity words of this round (definition level 1 = present)
     if (tid < nw) {
       const int32_t r0 = lo + 32 * tid;
@@ -500,8 +504,8 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
         if (sh && (w >> (32 - sh))) atomicOr(O.valid + (bit >> 5) + 1, w >> (32 - sh));
       }
     }
-    __syncthreads();
-    if (tid < 32) {  // exclusive scan of the words' populations
+    __syncwarp();
+    {  // exclusive scan of the words' populations
       const uint32_t c = tid < nw ? __popc(s_word[tid]) : 0;
       uint32_t x = c;
       for (int d = 1; d < 32; d <<= 1) {
@@ -509,12 +513,13 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
         if (tid >= d) x += y;
       }
       s_pre[tid] = x - c;
-      if (tid == 31) s_total = (int32_t)x;
+      const int32_t tot = (int32_t)__shfl_sync(0xffffffffu, x, 31);
+      if (tid == 0) {
+        s_total = tot;
+        if (pg.enc == PE_DICT || pg.enc == PE_RLE_BOOL) fill_runs(idx_runs, ic, jbase, jbase + tot);
+      }
     }
-    __syncthreads();
-    const int32_t total = s_total;
-    if ((pg.enc == PE_DICT || pg.enc == PE_RLE_BOOL) && tid == 0) fill_runs(idx_runs, ic, jbase, jbase + total);
-    __syncthreads();
+    __syncwarp();
     if (pg.type == TY_BOOL) {
       // bits: one thread per word of 32 rows
       if (tid < nw) {
@@ -542,7 +547,10 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
           if (sh && (out >> (32 - sh))) atomicOr(ov + (bit >> 5) + 1, out >> (32 - sh));
         }
       }
-    } else {
+    }
+    }  // warp 0
+    __syncthreads();
+    if (pg.type != TY_BOOL) {
       for (int32_t r = lo + tid; r < hi; r += PQ_THREADS) {
         const int w = (r - lo) >> 5, b = (r - lo) & 31;
         const int64_t row = pg.out_row + r;
@@ -591,8 +599,8 @@ __global__ void __launch_bounds__(PQ_THREADS) pq_page_kernel(const PqPage* pages
         }
       }
     }
-    jbase += total;
-    __syncthreads();
+    jbase += s_total;
+    __syncthreads();  // warp 0 rewrites the round's words and runs next
   }
   if (tid == 0 && (dc.bad || ic.bad)) bad = true;
   if (bad) atomicOr(err, DERR_CORRUPT);
