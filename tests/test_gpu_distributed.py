@@ -109,7 +109,7 @@ def _merge_data(n=400_000, seed=11):
     ], names=["k", "v", "x", "cust", "flag"])]
 
 
-CONFIGS = {
+AGG_CASES = {
     "int_key_all_funcs": HashAggConfig([0], [AggExpr(1, F.Sum, "s"), AggExpr(1, F.Count, "n"), AggExpr(2, F.Avg, "a"),
                                             AggExpr(1, F.Min, "mn"), AggExpr(2, F.Max, "mx"),
                                             AggExpr(3, F.CountDistinct, "cd")]),
@@ -125,12 +125,12 @@ CONFIGS = {
 
 
 @pytest.mark.parametrize("world", [2, 4])
-@pytest.mark.parametrize("name", sorted(CONFIGS))
+@pytest.mark.parametrize("name", sorted(AGG_CASES))
 def test_sharded_merge_matches_reducer(ctx, name, world):
     """World partials computed on the GPU, packed as an all-gather leaves
     them, unpacked and merged on the GPU: the oracle reducer's result over
     the oracle's partials (bit-exact keys and counts, Float64 within 1e-12)."""
-    cfg = CONFIGS[name]
+    cfg = AGG_CASES[name]
     data = _merge_data()
     wcfg = prism_gpu.expand_worker_aggregates(cfg)
     parts = [prism_gpu.hash_aggregate_batches(D.shard_batches(data, r, world), wcfg, ctx=ctx, as_device=True)
@@ -151,7 +151,7 @@ def test_sharded_merge_matches_reducer(ctx, name, world):
 
 def test_reducer_order(ctx):
     """Reducer 2 of 3 merges its own partial first: its groups lead."""
-    cfg = CONFIGS["utf8_key"]
+    cfg = AGG_CASES["utf8_key"]
     data = _merge_data(n=30_000, seed=5)
     wcfg = prism_gpu.expand_worker_aggregates(cfg)
     parts = [prism_gpu.hash_aggregate_batches(D.shard_batches(data, r, 3), wcfg, ctx=ctx) for r in range(3)]
@@ -164,18 +164,18 @@ def test_reducer_order(ctx):
 
 
 def test_merge_errors(ctx):
-    cfg = CONFIGS["two_keys"]
+    cfg = AGG_CASES["two_keys"]
     with pytest.raises(prism_gpu.PrismError):  # partial without the worker columns
         prism_gpu.merge_partial_aggregates([_merge_data(n=100)[0]], cfg, ctx=ctx)
     with pytest.raises(prism_gpu.PrismError):  # the reducer always has its own partial
-        prism_gpu.merge_partial_aggregates([], CONFIGS["utf8_key"], ctx=ctx)
-    wcfg = prism_gpu.expand_worker_aggregates(CONFIGS["utf8_key"])
+        prism_gpu.merge_partial_aggregates([], AGG_CASES["utf8_key"], ctx=ctx)
+    wcfg = prism_gpu.expand_worker_aggregates(AGG_CASES["utf8_key"])
     empty = [_merge_data(n=100)[0].slice(0, 0)]
     part = prism_gpu.hash_aggregate_batches(empty, wcfg, ctx=ctx)
-    ocfg, _ = oracle.expand_worker_aggregates(CONFIGS["utf8_key"])
+    ocfg, _ = oracle.expand_worker_aggregates(AGG_CASES["utf8_key"])
     assert_batches_equal(part, oracle.hash_aggregate_batches(empty, ocfg))
-    got = prism_gpu.merge_partial_aggregates([part, part], CONFIGS["utf8_key"], ctx=ctx)
-    assert_batches_equal(got, oracle.merge_partial_aggregates([part, part], CONFIGS["utf8_key"]))
+    got = prism_gpu.merge_partial_aggregates([part, part], AGG_CASES["utf8_key"], ctx=ctx)
+    assert_batches_equal(got, oracle.merge_partial_aggregates([part, part], AGG_CASES["utf8_key"]))
 
 
 def test_nccl_group_of_one(ctx, tmp_path):
@@ -188,7 +188,7 @@ def test_nccl_group_of_one(ctx, tmp_path):
     dist.init_process_group("nccl", init_method=f"file://{tmp_path / 'store'}", rank=0, world_size=1)
     try:
         data = _merge_data(n=50_000, seed=2)
-        for cfg in (CONFIGS["int_key_all_funcs"], CONFIGS["global"]):
+        for cfg in (AGG_CASES["int_key_all_funcs"], AGG_CASES["global"]):
             got = D.sharded_hash_aggregate(data, cfg, ctx=ctx)
             ocfg, _ = oracle.expand_worker_aggregates(cfg)
             ref = oracle.merge_partial_aggregates([oracle.hash_aggregate_batches(data, ocfg)], cfg)
