@@ -1318,6 +1318,8 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
   std::vector<unsigned long long> seg_bounds;
   std::vector<int32_t*> utf8_offs(chunks.size(), nullptr);
   std::vector<uint8_t*> utf8_data(chunks.size(), nullptr);
+  bool errors_read = false;  // read with the Utf8 segment bounds (one synchronisation)
+  uint32_t derr_early = 0;
   if (utf8_rows) {
     MemP tot_mem;
     unsigned long long* tot = ctx.alloc_t<unsigned long long>(1, tot_mem);
@@ -1336,7 +1338,16 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     seg_bounds.resize(at.size() + 1);
     PRISM_CUDA(cudaMemcpyAsync(seg_bounds.data(), gb, at.size() * 8, cudaMemcpyDeviceToHost, ctx.stream));
     PRISM_CUDA(cudaMemcpyAsync(&seg_bounds[at.size()], tot, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    // the error word rides along: the kernels after this point report none
+    PRISM_CUDA(cudaMemcpyAsync(ctx.h_err, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
+    errors_read = true;
+    derr_early = *ctx.h_err;
+    if (derr_early) {
+      PRISM_CUDA(cudaMemsetAsync(ctx.d_err, 0, sizeof(uint32_t), ctx.stream));
+      if (derr_early & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": malformed page data");
+      fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": device error " + std::to_string(derr_early));
+    }
     const unsigned long long total_bytes = seg_bounds[at.size()];
     for (size_t s = 0; s < segs.size(); ++s)
       if (seg_bounds[2 * s + 1] - seg_bounds[2 * s] > 0x7fffffffULL)
@@ -1365,7 +1376,7 @@ std::vector<RgOut> decode_prepared(Ctx& ctx, const PreparedFile& P, ParquetScanS
     }
     if (stats) stats->decoded_bytes += (int64_t)total_bytes + (int64_t)utf8_rows * 4;
   }
-  const uint32_t derr = ctx.take_device_errors();
+  const uint32_t derr = errors_read ? derr_early : ctx.take_device_errors();
   if (derr & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": malformed page data");
   if (derr) fail(PRISM_ERR_INTERNAL, "parquet read " + path + ": device error " + std::to_string(derr));
 
