@@ -288,16 +288,23 @@ __device__ __forceinline__ uint64_t select_word(const DCol& c, int64_t row, int 
 // digit (w >> shift) & 255 of the rows whose word above the digit equals `prefix`
 __global__ void select_hist_kernel(DCol c, const uint32_t* __restrict__ rows, int64_t m, int bits, int desc, int nb,
                                    int nulls_first, int shift, int top, uint64_t prefix, uint32_t* hist) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+  // one histogram per warp: a key's top digits take few values (a Float64's
+  // sign and exponent), so a block-wide histogram serialises on them
+  __shared__ uint32_t h[8][256];
+  const int wv = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) h[q][threadIdx.x] = 0;
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = rows ? rows[i] : i;
     const uint64_t w = select_word(c, row, bits, desc != 0, nb, nulls_first != 0);
-    if (top || (w >> (shift + 8)) == prefix) atomicAdd(&h[(w >> shift) & 255], 1u);
+    if (top || (w >> (shift + 8)) == prefix) atomicAdd(&h[wv][(w >> shift) & 255], 1u);
   }
   __syncthreads();
-  if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+  uint32_t t = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) t += h[q][threadIdx.x];
+  if (t) atomicAdd(&hist[threadIdx.x], t);
 }
 
 // bit i set when row i's word above `shift` is at most `bound` (kept)
