@@ -60,9 +60,21 @@ def parse():
     ap.add_argument("--impl", choices=["prism", "reference"], default="prism")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--join-table", choices=["auto", "hash"], default="auto",
+                    help="c2: 'auto' lets the library pick (a dense row table for the permutation keys), 'hash' "
+                         "forces the open-addressing hash table")
+    ap.add_argument("--partition", choices=["auto", "on", "off"], default="auto",
+                    help="c2 with --join-table hash: the radix-partitioned build and probe (auto: once the hash slots "
+                         "outgrow L2)")
+    ap.add_argument("--ordered", action="store_true",
+                    help="c2: emit matches in the reference's probe order (default: as a multiset, one-pass probe)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale all sizes (profiling captures use a smaller case; bench lines use 1.0)")
     a = ap.parse_args()
+    if a.join_table == "hash":
+        os.environ["PRISM_JOIN_DENSE"] = "0"  # read by the library at every table build
+    if a.partition != "auto":
+        os.environ["PRISM_JOIN_PARTITION"] = "1" if a.partition == "on" else "0"
     if a.steps is None:
         a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1, "sort": 10, "topn": 10, "parquet": 10}[a.workload]
     global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE
@@ -171,6 +183,40 @@ def cpu_baseline(bk, bp, pk, threads):
     return (len(bk) + len(pk)) / dt, dt, m
 
 
+def check_c2_sample(torch, prism_gpu, ctx, build_db, bk, bp, pk, out_cols, any_order):
+    """The step's output for the first 10M probe rows against the oracle's
+    probe (hash_join.rs:143-200) + payload take: the (probe_row, payload)
+    pairs as ordered pairs (multiset: sorted by probe row, unique build keys
+    give each probe row at most one match; probe order: as emitted)."""
+    import numpy as np
+    import pyarrow as pa
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as oracle
+
+    s = min(CPU_SAMPLE_PROBE, N_PROBE)
+    hb = pa.RecordBatch.from_arrays([pa.array(bk.cpu().numpy()), pa.array(bp.cpu().numpy())], names=["key", "payload"])
+    hpk = pk[:s].cpu().numpy()
+    probes = [pa.RecordBatch.from_arrays([pa.array(hpk[i : i + 1_000_000])], names=["key"]) for i in range(0, s, 1_000_000)]
+    t0 = time.perf_counter()
+    pm = oracle.probe_matches_chunked(probes, hb, [0], [0], n_threads=os.cpu_count() or 1)
+    ref_rows = np.concatenate([m.column(0).to_numpy().astype(np.int64) + 1_000_000 * i for i, m in enumerate(pm)])
+    ref_pay = hb.column(1).to_numpy()[np.concatenate([m.column(1).to_numpy() for m in pm]).astype(np.int64)]
+    dt = time.perf_counter() - t0
+    sample = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", pk.data_ptr())], s, ctx, pk.device.index)
+    t = prism_gpu.HashTable.build(build_db, [0], ctx)
+    got = t.join_project(sample, [0], [out_cols[0], 2], any_order=any_order)
+    t.free()
+    rows = got.column(0).to_numpy().astype(np.int64)
+    pay = got.column(1).to_numpy()
+    if any_order:
+        o = np.argsort(rows, kind="stable")
+        rows, pay = rows[o], pay[o]
+    assert np.array_equal(rows, ref_rows) and np.array_equal(pay, ref_pay), "(probe_row, payload) pairs differ from the oracle"
+    return (f"the first {s:,} probe rows' {len(rows):,} (probe_row, payload) pairs equal the oracle's "
+            f"({'as a multiset' if any_order else 'in order'}; oracle {dt:.1f} s)")
+
+
 def main():
     args = parse()
     import torch
@@ -206,10 +252,14 @@ def main():
     build_db = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", bk.data_ptr()), ("payload", "l", bp.data_ptr())], N_BUILD, ctx, local)
     probe_db = prism_gpu.DeviceBatch.from_device_buffers([("key", "l", pk.data_ptr()), ("payload", "i", pp.data_ptr())], N_PROBE, ctx, local)
     OUT = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 3]
+    any_order = not args.ordered
+    layout = []
 
     def step():
         t = prism_gpu.HashTable.build(build_db, [0], ctx)
-        out = t.join_project(probe_db, [0], OUT, as_device=True)
+        if not layout:
+            layout.append(t.layout)
+        out = t.join_project(probe_db, [0], OUT, as_device=True, any_order=any_order)
         m = out.num_rows
         out.free()
         t.free()
@@ -219,6 +269,7 @@ def main():
         matches = step()
     expected = int((pk < N_BUILD).sum().item())
     assert matches == expected, f"match count {matches} != {expected}"
+    check = None if args.no_check else check_c2_sample(torch, prism_gpu, ctx, build_db, bk, bp, pk, OUT, any_order)
 
     gpu_index = local
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
@@ -241,10 +292,13 @@ def main():
             dist.barrier()
     ms = start.elapsed_time(stop)
     launches = ctx.kernel_launches - launches0
-    # the probe phase: probe_rows_kernel + emit_rows_kernel (unique int64
-    # keys) or the single-pass probe_kernel (duplicate / general keys)
-    kstats = {k: ctx.kernel_stats(k) for k in ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel")}
-    n_probe_launch = max(kstats["probe_rows_kernel"][0], kstats["probe_kernel"][0])
+    # the probe phase: the one-pass probe_emit_any_kernel (matches as a
+    # multiset), probe_rows_kernel + emit_rows_kernel (probe order, unique
+    # int64 keys) or the single-pass probe_kernel (duplicate / general keys)
+    kstats = {k: ctx.kernel_stats(k) for k in ("probe_partition_hist_kernel", "probe_partition_scatter_kernel",
+                                               "probe_emit_any_kernel", "probe_rows_kernel", "emit_rows_kernel",
+                                               "probe_kernel")}
+    n_probe_launch = max(kstats["probe_emit_any_kernel"][0], kstats["probe_rows_kernel"][0], kstats["probe_kernel"][0])
     probe_ms = sum(v[1] for v in kstats.values())
     n_ins, ins_ms = ctx.kernel_stats("insert_kernel")
     ctx.set_profiling(False)
@@ -299,7 +353,12 @@ def main():
                 "workload": WORKLOAD,
                 "build_rows": N_BUILD,
                 "probe_rows": N_PROBE,
+                "table": layout[0],
+                "probe_path": ("radix-partitioned (keys reordered by the top 8 bits of their slot hash, then probed)"
+                               if kstats["probe_partition_scatter_kernel"][0] else "streamed (probe order)"),
+                "order": "any (matches as a multiset)" if any_order else "probe order (the reference's)",
                 "matches_per_step": matches,
+                "check": check,
                 "l2": "inputs larger than L2 (1.76 GB per step), no flush",
                 "parallelism": f"replicated build, probe sharded (weak) x{world}",
             },
@@ -1212,11 +1271,14 @@ def run_e2e(args, torch, prism_gpu, ctx, bk, bp, pk, world, dist, device, rows_p
     h2d = sum(c.nbytes for c in hb.columns) + sum(c.nbytes for c in hp.columns)
     out_cols = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 2]  # probe (key) | build (key_right, payload)
 
+    any_order = not args.ordered
+
     def step():
+        # build side up and built; the probe batch streams through the C ABI
+        # in chunks whose uploads, probes and downloads overlap
         b = prism_gpu.DeviceBatch.from_arrow(hb, ctx)
-        p = prism_gpu.DeviceBatch.from_arrow(hp, ctx)
         t = prism_gpu.HashTable.build(b, [0], ctx)
-        out = t.join_project(p, [0], out_cols)
+        out = t.join_project_arrow(hp, [0], out_cols, any_order=any_order)
         t.free()
         return out
 
@@ -1237,7 +1299,10 @@ def run_e2e(args, torch, prism_gpu, ctx, bk, bp, pk, world, dist, device, rows_p
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     dt = float(tt.item())
     return {"value": world * rows_per_rank / dt, "unit": "rows/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": dt * 1e3, "timing": "host wall clock around synchronous C-ABI calls (import H2D, build, probe, export D2H)"}
+            "ms_per_step": dt * 1e3,
+            "timing": ("host wall clock around the C-ABI calls of a step: build batch import (H2D) and table build, "
+                       "then prism_join_project_arrow on the host probe batch (8M-row chunks: H2D, probe and D2H "
+                       "of neighbouring chunks overlap), result in host memory")}
 
 
 def run_reference(args, rank, world, torch, dist):

@@ -307,15 +307,23 @@ int prism_hash_table_probe(prism_ctx* ctx, const prism_hash_table* table,
  * array's device address (cudaGetSymbolAddress) with the device current; make
  * that first call before any stream capture. Every call shares the array and
  * clears the part it uses; calls that overlap on the GPU race. When more
- * matches exist than out_capacity, nothing past the capacity is written,
- * *out_matches receives the full count and the call returns
- * PRISM_ERR_INVALID_ARGUMENT. */
+ * matches exist than out_capacity, the first out_capacity matches (in the
+ * order above, also when a probe row's matches straddle the capacity) are
+ * written and nothing past them, *out_matches receives the full count and
+ * the call returns PRISM_ERR_INVALID_ARGUMENT. */
 int prism_hash_table_probe_noalloc(prism_ctx* ctx, const prism_hash_table* table,
                                    const int64_t* probe_keys, int64_t n_probe,
                                    uint32_t* out_probe_idx, uint32_t* out_build_idx,
                                    int64_t out_capacity, int64_t* out_matches);
 int64_t prism_hash_table_num_rows(const prism_hash_table* table);
 int prism_hash_table_has_duplicates(const prism_hash_table* table);
+/* How the table is laid out in HBM (no reference counterpart; the Rust
+ * HashTable is one hashbrown map per partition): PRISM_TABLE_HASH
+ * (open-addressing slots), PRISM_TABLE_DENSE (a direct row per key value,
+ * chosen for unique Int64 keys over a compact range); -1 for a null table. */
+#define PRISM_TABLE_HASH 0
+#define PRISM_TABLE_DENSE 1
+int prism_hash_table_layout(const prism_hash_table* table);
 void prism_hash_table_free(prism_hash_table* table);
 
 /* Fused probe + gather: emits the selected columns of the inner join of
@@ -327,6 +335,16 @@ int prism_join_project(prism_ctx* ctx, const prism_hash_table* table,
                        const prism_batch* probe, const int32_t* probe_keys,
                        int32_t n_keys, const int32_t* out_cols, int32_t n_out,
                        prism_batch** out);
+/* prism_join_project with flags. PRISM_JOIN_ANY_ORDER: the caller takes the
+ * matches as a multiset (the executor's fused join -> aggregate consumes
+ * them that way, executor.rs:474-551): runs of consecutive probe rows come in
+ * any order, rows ascending inside a run, so the probe needs one pass and no
+ * ordering step. The set of output rows is the same as without the flag. */
+#define PRISM_JOIN_ANY_ORDER 1u
+int prism_join_project_ex(prism_ctx* ctx, const prism_hash_table* table,
+                          const prism_batch* probe, const int32_t* probe_keys,
+                          int32_t n_keys, const int32_t* out_cols, int32_t n_out,
+                          uint32_t flags, prism_batch** out);
 
 /* hash_join (hash_join.rs:312-365). */
 int prism_hash_join(prism_ctx* ctx, const prism_batch* probe, const prism_batch* build,
@@ -604,6 +622,19 @@ int prism_hash_aggregate_arrow(prism_ctx* ctx, const struct ArrowArray* batch,
                                const struct ArrowSchema* schema,
                                const prism_agg_config* config, struct ArrowArray* out,
                                struct ArrowSchema* out_schema);
+/* prism_join_project_ex with a host probe batch and a host result (what
+ * prism-jni would call per probe batch against a resident build table).
+ * With unique Int64 build keys and fixed-width, null-free probe key and
+ * gathered columns the probe streams through in chunks of 8M rows: chunk
+ * i+1's upload, chunk i's probe and chunk i-1's download overlap on the
+ * link's two directions; the output lands in page-locked host buffers.
+ * Other inputs take one upload, the probe, one download. Results equal
+ * prism_join_project_ex's for the same flags. */
+int prism_join_project_arrow(prism_ctx* ctx, const prism_hash_table* table,
+                             const struct ArrowArray* probe, const struct ArrowSchema* probe_schema,
+                             const int32_t* probe_keys, int32_t n_keys, const int32_t* out_cols,
+                             int32_t n_out, uint32_t flags, struct ArrowArray* out,
+                             struct ArrowSchema* out_schema);
 int prism_sort_batch_arrow(prism_ctx* ctx, const struct ArrowArray* batch, const struct ArrowSchema* schema,
                            const prism_sort_key* keys, int32_t n_keys, int64_t limit, struct ArrowArray* out,
                            struct ArrowSchema* out_schema);

@@ -761,6 +761,10 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
   int64_t total_rows = 0;
   for (auto* b : batches) total_rows += b->rows;
   bool any_rows = total_rows > 0;
+  // the accumulators are signed 64-bit counters of 32-bit limbs, added to
+  // without carry normalisation: exact for up to 2^31 - 1 rows per call
+  if (total_rows > (int64_t)INT32_MAX)
+    fail(PRISM_ERR_INVALID_ARGUMENT, "aggregation input exceeds 2^31-1 rows per call");
 
   // projected schema description
   std::vector<ProjCol> proj;
@@ -1074,6 +1078,13 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
   std::vector<const DCol*> jpk_dev;
   if (join) {
     if (total_rows >= (int64_t)UINT32_MAX) fused_fail("a join over 2^32 probe rows");
+    if (join->table->has_dups) {
+      // repeated build keys: a probe row can join several build rows, so
+      // bound the joined rows (not the probe rows) by the accumulators' limit
+      int64_t joined = 0;
+      for (auto* pb : batches_in) joined += probe_count(ctx, *join->table, *pb, join->probe_keys, JoinTuning{});
+      if (joined > (int64_t)INT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "aggregation input exceeds 2^31-1 joined rows per call");
+    }
     for (auto* pb : batches_in) {
       std::vector<DCol> v;
       for (int k : join->probe_keys) v.push_back(pb->cols.at(k)->view());

@@ -117,7 +117,9 @@ __device__ __forceinline__ void atom_add(unsigned long long* p, unsigned long lo
 }
 
 // Adds v to a 6-limb fixed-point accumulator whose bit 0 weighs 2^lo_exp
-// (acc[6] collects NaN/+inf/-inf flags). Bits below the window are dropped.
+// (acc[6] collects NaN/+inf/-inf flags). A value with set bits above or
+// below the window raises DERR_OVERFLOW (the caller reruns over the wide
+// window from 2^-1074, which holds every double exactly), so no bit is lost.
 __device__ inline void add_f64(unsigned long long* acc, double v, int lo_exp, uint32_t* err, int* maxexp, int nl = LIMBS) {
   uint64_t u = (uint64_t)__double_as_longlong(v);
   int be = (int)((u >> 52) & 0x7ff);
@@ -131,10 +133,13 @@ __device__ inline void add_f64(unsigned long long* acc, double v, int lo_exp, ui
   if (!m) return;
   int pos = be - 1075 - lo_exp;
   if (pos < 0) {
-    if (pos <= -64) return;
+    // set bits below 2^lo_exp: the window cannot hold the value exactly
+    if (pos <= -64 || (m & ((1ULL << -pos) - 1))) {
+      atomicOr(err, DERR_OVERFLOW);
+      return;
+    }
     m >>= -pos;
     pos = 0;
-    if (!m) return;
   }
   int k = pos >> 5, sh = pos & 31;
   unsigned __int128 x = (unsigned __int128)m << sh;

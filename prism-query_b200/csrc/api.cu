@@ -2,6 +2,7 @@
 //
 // Every entry point catches failures and returns a status code (the library
 // never aborts); the message is kept on the context for prism_last_error().
+#include <algorithm>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
@@ -60,10 +61,14 @@ std::vector<int> ints(const int32_t* p, int n) {
 }
 
 // PRISM_JOIN_DENSE=0 keeps single Int64 keys in the hash table (dense mode off)
+// PRISM_JOIN_PARTITION=0|1 turns the radix-partitioned build / probe off or
+// on (default: on once the hash slots outgrow L2)
 JoinTuning join_tuning() {
   JoinTuning t{};
   const char* d = std::getenv("PRISM_JOIN_DENSE");
   if (d && std::strcmp(d, "0") == 0) t.dense = false;
+  const char* p = std::getenv("PRISM_JOIN_PARTITION");
+  if (p && (std::strcmp(p, "0") == 0 || std::strcmp(p, "1") == 0)) t.partition = p[0] - '0';
   return t;
 }
 // PRISM_JOIN_AGG_SHAPE=block,min_blocks,rows,table_log2 sets the fused join
@@ -269,6 +274,70 @@ std::string joined_name(const Batch& probe, const Batch& build, int col) {
   return right_name(probe, build.cols[col - np]->name);
 }
 
+// join_project: probe `probe` against `t` and gather `oc` of the joined
+// schema (probe columns, then build columns; PRISM_COL_* for row indices).
+Batch join_project_impl(Ctx& x, const JoinTable& t, const Batch& probe, const std::vector<int>& pk,
+                        const std::vector<int>& oc, uint32_t flags) {
+  if (flags & ~(uint32_t)PRISM_JOIN_ANY_ORDER) fail(PRISM_ERR_INVALID_ARGUMENT, "unknown join_project flags");
+  const Batch& build = t.build;
+  int np = (int)probe.cols.size(), nb = (int)build.cols.size();
+  for (int col : oc)
+    if (col < PRISM_COL_BUILD_ROW_INDEX || col >= np + nb) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+  // gather fixed-width null-free columns inside the probe kernel
+  bool fusable = (int)oc.size() <= 6;
+  int n_gather = 0;
+  for (int col : oc) {
+    if (col < 0) continue;
+    const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+    int w = width_of(src.type);
+    if (src.validity || (w != 4 && w != 8) || src.type == TY_DICT) fusable = false;
+    ++n_gather;
+  }
+  if (n_gather > 4) fusable = false;
+  int64_t cap = match_upper_bound(t, probe.rows);
+  if (cap < 0) cap = probe_count(x, t, probe, pk, join_tuning());
+  bool want_p = !fusable, want_b = !fusable;
+  for (int col : oc) {
+    if (col == PRISM_COL_PROBE_ROW_INDEX) want_p = true;
+    if (col == PRISM_COL_BUILD_ROW_INDEX) want_b = true;
+  }
+  std::vector<ProbeGather> gathers;
+  std::vector<ColP> gcols;
+  if (fusable) {
+    for (int col : oc) {
+      if (col < 0) continue;
+      const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+      ColP dst = make_column(x, src.type, joined_name(probe, build, col), cap, false);
+      dst->nullable = src.nullable;
+      dst->precision = src.precision;
+      dst->scale = src.scale;
+      gathers.push_back({col < np ? 0 : 1, src.values, width_of(src.type), dst->values});
+      gcols.push_back(dst);
+    }
+  }
+  ProbeResult r = probe_join_table(x, t, probe, pk, want_p, want_b, gathers, cap, join_tuning(),
+                                   (flags & PRISM_JOIN_ANY_ORDER) != 0);
+  Batch res;
+  res.rows = r.matches;
+  size_t gi = 0;
+  for (int col : oc) {
+    if (col == PRISM_COL_PROBE_ROW_INDEX) {
+      res.cols.push_back(u32_column(x, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
+    } else if (col == PRISM_COL_BUILD_ROW_INDEX) {
+      res.cols.push_back(u32_column(x, "build_idx", r.build_idx, static_cast<uint32_t*>(r.build_idx->ptr), r.matches));
+    } else if (fusable) {
+      ColP g = gcols[gi++];
+      g->length = r.matches;
+      res.cols.push_back(g);
+    } else {
+      const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
+      const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
+      res.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(probe, build, col), src.nullable));
+    }
+  }
+  return res;
+}
+
 }  // namespace
 
 extern "C" {
@@ -296,6 +365,9 @@ int prism_ctx_create(int device, uint64_t budget, prism_ctx** out) {
     PRISM_CUDA(cudaMemGetInfo(&free_b, &total_b));
     x.budget = budget ? budget : (uint64_t)(free_b * 0.9);
     PRISM_CUDA(cudaDeviceGetAttribute(&x.sm_count, cudaDevAttrMultiProcessorCount, device));
+    int l2 = 0;
+    PRISM_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+    if (l2 > 0) x.l2_bytes = l2;
     PRISM_CUDA(cudaMalloc(&x.d_err, 64));
     PRISM_CUDA(cudaMemset(x.d_err, 0, 64));
     PRISM_CUDA(cudaMallocHost(&x.h_err, 64));
@@ -440,6 +512,10 @@ int prism_hash_table_probe(prism_ctx* c, const prism_hash_table* t, const prism_
 
 int64_t prism_hash_table_num_rows(const prism_hash_table* t) { return t ? t->t->build.rows : -1; }
 int prism_hash_table_has_duplicates(const prism_hash_table* t) { return t && t->t->has_dups ? 1 : 0; }
+int prism_hash_table_layout(const prism_hash_table* t) {
+  if (!t || !t->t) return -1;
+  return t->t->dense ? PRISM_TABLE_DENSE : PRISM_TABLE_HASH;
+}
 void prism_hash_table_free(prism_hash_table* t) {
   if (!t) return;
   if (t->ctx) {
@@ -452,69 +528,186 @@ void prism_hash_table_free(prism_hash_table* t) {
 
 int prism_join_project(prism_ctx* c, const prism_hash_table* tab, const prism_batch* probe_b, const int32_t* probe_keys,
                        int32_t n_keys, const int32_t* out_cols, int32_t n_out, prism_batch** out) {
+  return prism_join_project_ex(c, tab, probe_b, probe_keys, n_keys, out_cols, n_out, 0u, out);
+}
+
+int prism_join_project_ex(prism_ctx* c, const prism_hash_table* tab, const prism_batch* probe_b,
+                          const int32_t* probe_keys, int32_t n_keys, const int32_t* out_cols, int32_t n_out,
+                          uint32_t flags, prism_batch** out) {
   return run(c, [&] {
-    if (!tab || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
+    if (!tab || !tab->t || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
+    Batch res = join_project_impl(c->impl, *tab->t, B(probe_b), ints(probe_keys, n_keys), ints(out_cols, n_out), flags);
+    c->impl.sync();
+    *out = wrap(c, std::move(res));
+  });
+}
+
+int prism_join_project_arrow(prism_ctx* c, const prism_hash_table* tab, const ArrowArray* probe_a,
+                             const ArrowSchema* probe_s, const int32_t* probe_keys, int32_t n_keys,
+                             const int32_t* out_cols, int32_t n_out, uint32_t flags, ArrowArray* out,
+                             ArrowSchema* out_schema) {
+  return run(c, [&] {
+    if (!tab || !tab->t || !out || !out_schema) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
     Ctx& x = c->impl;
     const JoinTable& t = *tab->t;
-    const Batch& probe = B(probe_b);
-    const Batch& build = t.build;
     std::vector<int> pk = ints(probe_keys, n_keys), oc = ints(out_cols, n_out);
-    int np = (int)probe.cols.size(), nb = (int)build.cols.size();
+    std::vector<HostView> hv = host_view(probe_a, probe_s);
+    const int np = (int)hv.size(), nb = (int)t.build.cols.size();
+    const int64_t n = probe_a->length;
     for (int col : oc)
       if (col < PRISM_COL_BUILD_ROW_INDEX || col >= np + nb) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
-    // gather fixed-width null-free columns inside the probe kernel
-    bool fusable = (int)oc.size() <= 6;
+    // Streamed when every match has one row (unique Int64 build keys) and the
+    // probe key and every gathered column are fixed-width without nulls:
+    // the probe rows go up in chunks, and chunk i+1's upload, chunk i's probe
+    // and chunk i-1's download run at once (uploads and downloads use the
+    // link's two directions). Anything else: one upload, probe, download.
+    bool stream = t.int64_fast && !t.has_dups && pk.size() == 1 && pk[0] >= 0 && pk[0] < np &&
+                  hv[pk[0]].meta->type == TY_I64 && hv[pk[0]].values && oc.size() <= 6;
     int n_gather = 0;
     for (int col : oc) {
       if (col < 0) continue;
-      const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
-      int w = width_of(src.type);
-      if (src.validity || (w != 4 && w != 8) || src.type == TY_DICT) fusable = false;
       ++n_gather;
-    }
-    if (n_gather > 4) fusable = false;
-    int64_t cap = match_upper_bound(t, probe.rows);
-    if (cap < 0) cap = probe_count(x, t, probe, pk, join_tuning());
-    bool want_p = !fusable, want_b = !fusable;
-    for (int col : oc) {
-      if (col == PRISM_COL_PROBE_ROW_INDEX) want_p = true;
-      if (col == PRISM_COL_BUILD_ROW_INDEX) want_b = true;
-    }
-    std::vector<ProbeGather> gathers;
-    std::vector<ColP> gcols;
-    if (fusable) {
-      for (int col : oc) {
-        if (col < 0) continue;
-        const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
-        ColP dst = make_column(x, src.type, joined_name(probe, build, col), cap, false);
-        dst->nullable = src.nullable;
-        dst->precision = src.precision;
-        dst->scale = src.scale;
-        gathers.push_back({col < np ? 0 : 1, src.values, width_of(src.type), dst->values});
-        gcols.push_back(dst);
-      }
-    }
-    ProbeResult r = probe_join_table(x, t, probe, pk, want_p, want_b, gathers, cap, join_tuning());
-    Batch res;
-    res.rows = r.matches;
-    size_t gi = 0;
-    for (int col : oc) {
-      if (col == PRISM_COL_PROBE_ROW_INDEX) {
-        res.cols.push_back(u32_column(x, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
-      } else if (col == PRISM_COL_BUILD_ROW_INDEX) {
-        res.cols.push_back(u32_column(x, "build_idx", r.build_idx, static_cast<uint32_t*>(r.build_idx->ptr), r.matches));
-      } else if (fusable) {
-        ColP g = gcols[gi++];
-        g->length = r.matches;
-        res.cols.push_back(g);
+      if (col < np) {
+        const HostView& h = hv[col];
+        const int w = width_of(h.meta->type);
+        if (!h.values || h.null_count != 0 || (w != 4 && w != 8) || h.meta->type == TY_DICT) stream = false;
       } else {
-        const Column& src = col < np ? *probe.cols[col] : *build.cols[col - np];
-        const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
-        res.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(probe, build, col), src.nullable));
+        const Column& src = *t.build.cols[col - np];
+        const int w = width_of(src.type);
+        if (src.validity || (w != 4 && w != 8) || src.type == TY_DICT) stream = false;
       }
     }
-    x.sync();
-    *out = wrap(c, std::move(res));
+    if (n_gather > 4) stream = false;
+    if (!stream || n == 0) {
+      Batch probe = import_batch(x, probe_a, probe_s, false);
+      Batch res = join_project_impl(x, t, probe, pk, oc, flags);
+      export_batch(x, res, out, out_schema);
+      return;
+    }
+    Batch pmeta;  // the probe schema (metadata only)
+    pmeta.rows = n;
+    for (auto& h : hv) pmeta.cols.push_back(h.meta);
+    check_join_keys(pmeta, pk, t.build, t.key_cols);
+    const bool any = (flags & PRISM_JOIN_ANY_ORDER) != 0;
+    if (flags & ~(uint32_t)PRISM_JOIN_ANY_ORDER) fail(PRISM_ERR_INVALID_ARGUMENT, "unknown join_project flags");
+    constexpr int64_t CH = (int64_t)1 << 23;  // probe rows per chunk (a multiple of every probe tile)
+    const int64_t nchunks = (n + CH - 1) / CH;
+    // probe columns to upload (the key first), with their staging slots
+    std::vector<int> up{pk[0]};
+    for (int col : oc)
+      if (col >= 0 && col < np && std::find(up.begin(), up.end(), col) == up.end()) up.push_back(col);
+    std::vector<MemP> in_mem[2];
+    for (int sl = 0; sl < 2; ++sl)
+      for (int col : up) in_mem[sl].push_back(x.alloc((size_t)std::min(CH, n) * width_of(hv[col].meta->type) + 16));
+    // outputs: host columns sized for every probe row, device staging per slot
+    std::vector<HostOutCol> hcols;
+    std::vector<int> ow;
+    for (int col : oc) {
+      ColP m = std::make_shared<Column>();
+      if (col == PRISM_COL_PROBE_ROW_INDEX || col == PRISM_COL_BUILD_ROW_INDEX) {
+        m->type = TY_U32;
+        m->name = col == PRISM_COL_PROBE_ROW_INDEX ? "probe_idx" : "build_idx";
+        m->nullable = false;
+      } else {
+        const Column& src = col < np ? *hv[col].meta : *t.build.cols[col - np];
+        m->type = src.type;
+        m->name = joined_name(pmeta, t.build, col);
+        m->nullable = src.nullable;
+        m->precision = src.precision;
+        m->scale = src.scale;
+      }
+      ow.push_back(width_of(m->type));
+      hcols.push_back(host_out_column(m, (size_t)n * ow.back()));
+    }
+    std::vector<MemP> out_mem[2];
+    for (int sl = 0; sl < 2; ++sl)
+      for (size_t k = 0; k < oc.size(); ++k)
+        if (oc[k] >= 0) out_mem[sl].push_back(x.alloc((size_t)std::min(CH, n) * ow[k] + 16));
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[2] = {}, ev_used[2] = {}, ev_probed[2] = {}, ev_out[2] = {};
+    ProbeResult held[2];
+    auto cleanup = [&] {
+      if (s_in) cudaStreamSynchronize(s_in);
+      if (s_out) cudaStreamSynchronize(s_out);
+      cudaStreamSynchronize(x.stream);
+      for (auto* e : {ev_in, ev_used, ev_probed, ev_out})
+        for (int sl = 0; sl < 2; ++sl)
+          if (e[sl]) cudaEventDestroy(e[sl]);
+      if (s_in) cudaStreamDestroy(s_in);
+      if (s_out) cudaStreamDestroy(s_out);
+    };
+    int64_t total = 0;
+    try {
+      PRISM_CUDA(cudaStreamCreateWithFlags(&s_in, cudaStreamNonBlocking));
+      PRISM_CUDA(cudaStreamCreateWithFlags(&s_out, cudaStreamNonBlocking));
+      for (auto* e : {ev_in, ev_used, ev_probed, ev_out})
+        for (int sl = 0; sl < 2; ++sl) PRISM_CUDA(cudaEventCreateWithFlags(&e[sl], cudaEventDisableTiming));
+      // the staging and output buffers were allocated on the context's stream
+      PRISM_CUDA(cudaEventRecord(ev_used[0], x.stream));
+      PRISM_CUDA(cudaStreamWaitEvent(s_in, ev_used[0], 0));
+      auto upload = [&](int64_t i) {
+        const int sl = (int)(i & 1);
+        const int64_t lo = i * CH, rows = std::min(CH, n - lo);
+        if (i >= 2) PRISM_CUDA(cudaStreamWaitEvent(s_in, ev_used[sl], 0));  // chunk i-2's probe read the slot
+        for (size_t u = 0; u < up.size(); ++u) {
+          const int w = width_of(hv[up[u]].meta->type);
+          PRISM_CUDA(cudaMemcpyAsync(in_mem[sl][u]->ptr, static_cast<const uint8_t*>(hv[up[u]].values) + lo * w,
+                                     (size_t)rows * w, cudaMemcpyHostToDevice, s_in));
+        }
+        PRISM_CUDA(cudaEventRecord(ev_in[sl], s_in));
+      };
+      upload(0);
+      for (int64_t i = 0; i < nchunks; ++i) {
+        const int sl = (int)(i & 1);
+        const int64_t lo = i * CH, rows = std::min(CH, n - lo);
+        if (i + 1 < nchunks) upload(i + 1);
+        PRISM_CUDA(cudaStreamWaitEvent(x.stream, ev_in[sl], 0));
+        if (i >= 2) PRISM_CUDA(cudaStreamWaitEvent(x.stream, ev_out[sl], 0));  // chunk i-2's download left the slot
+        held[sl] = ProbeResult{};  // chunk i-2's index arrays: freed after its download (ordered above)
+        Batch chunk;
+        chunk.rows = rows;
+        for (int j = 0; j < np; ++j) {
+          auto col = std::make_shared<Column>(*hv[j].meta);
+          col->length = rows;
+          auto it = std::find(up.begin(), up.end(), j);
+          col->values = it == up.end() ? nullptr : in_mem[sl][it - up.begin()]->ptr;
+          chunk.cols.push_back(col);
+        }
+        std::vector<ProbeGather> gathers;
+        bool want_p = false, want_b = false;
+        size_t g = 0;
+        for (int col : oc) {
+          if (col == PRISM_COL_PROBE_ROW_INDEX) want_p = true;
+          else if (col == PRISM_COL_BUILD_ROW_INDEX) want_b = true;
+          else {
+            const Column& src = col < np ? *chunk.cols[col] : *t.build.cols[col - np];
+            gathers.push_back({col < np ? 0 : 1, src.values, width_of(src.type), out_mem[sl][g++]->ptr});
+          }
+        }
+        held[sl] = probe_join_table(x, t, chunk, pk, want_p, want_b, gathers, rows, join_tuning(), any, lo);
+        const int64_t m = held[sl].matches;
+        PRISM_CUDA(cudaEventRecord(ev_used[sl], x.stream));
+        PRISM_CUDA(cudaEventRecord(ev_probed[sl], x.stream));
+        PRISM_CUDA(cudaStreamWaitEvent(s_out, ev_probed[sl], 0));
+        g = 0;
+        for (size_t k = 0; k < oc.size(); ++k) {
+          const void* src = oc[k] == PRISM_COL_PROBE_ROW_INDEX   ? held[sl].probe_idx->ptr
+                            : oc[k] == PRISM_COL_BUILD_ROW_INDEX ? held[sl].build_idx->ptr
+                                                                 : out_mem[sl][g++]->ptr;
+          if (m)
+            PRISM_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(hcols[k].values) + (size_t)total * ow[k], src,
+                                       (size_t)m * ow[k], cudaMemcpyDeviceToHost, s_out));
+        }
+        PRISM_CUDA(cudaEventRecord(ev_out[sl], s_out));
+        total += m;
+      }
+      PRISM_CUDA(cudaStreamSynchronize(s_out));
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+    export_host_columns(hcols, total, out, out_schema);
   });
 }
 

@@ -617,6 +617,91 @@ Batch import_device_batch(Ctx& ctx, const ArrowDeviceArray* a, const ArrowSchema
   return import_batch(ctx, &a->array, s, dev);
 }
 
+std::vector<HostView> host_view(const ArrowArray* a, const ArrowSchema* s) {
+  if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null ArrowArray/ArrowSchema");
+  if (!s->format || std::string(s->format) != "+s")
+    fail(PRISM_ERR_ARROW, "a RecordBatch must be exported as a struct array (format '+s')");
+  if (a->n_children != s->n_children) fail(PRISM_ERR_ARROW, "array/schema child count mismatch");
+  std::vector<HostView> v;
+  for (int64_t i = 0; i < s->n_children; ++i) {
+    const ArrowArray* ca = a->children[i];
+    const ArrowSchema* cs = s->children[i];
+    HostView h;
+    h.meta = std::make_shared<Column>();
+    Column& c = *h.meta;
+    c.name = cs->name ? cs->name : "";
+    c.nullable = (cs->flags & ARROW_FLAG_NULLABLE) != 0;
+    c.length = a->length;
+    int32_t t, prec = 38, scale = 0;
+    if (!parse_format(cs->format, t, prec, scale))
+      fail(PRISM_ERR_ARROW, std::string("unsupported arrow format '") + (cs->format ? cs->format : "") + "'");
+    c.type = cs->dictionary ? TY_DICT : t;
+    c.precision = prec;
+    c.scale = scale;
+    h.null_count = ca->null_count;
+    const int w = width_of(t);
+    if (!cs->dictionary && t != TY_UTF8 && t != TY_BOOL && t != TY_NULL && w > 0 && ca->n_buffers >= 2 && ca->buffers[1])
+      h.values = static_cast<const uint8_t*>(ca->buffers[1]) + (ca->offset + a->offset) * w;
+    v.push_back(h);
+  }
+  return v;
+}
+
+HostOutCol host_out_column(ColP meta, size_t bytes) {
+  auto h = std::make_shared<HostBuf>();
+  if (bytes + 16 >= PinnedPool::kPinnedMin) {
+    h->p = pinned_pool().get(bytes + 16, &h->size);
+    h->pinned = h->p != nullptr;
+  }
+  if (!h->p) h->p = malloc(bytes + 16);
+  if (!h->p) fail(PRISM_ERR_NO_MEMORY, "host allocation failed");
+  HostOutCol c;
+  c.meta = std::move(meta);
+  c.values = h->p;
+  c.hold = h;
+  return c;
+}
+
+void export_host_columns(const std::vector<HostOutCol>& cols, int64_t rows, ArrowArray* a, ArrowSchema* s) {
+  if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null output ArrowArray/ArrowSchema");
+  auto* ap = new ArrayPriv();
+  ap->ptrs = {nullptr};
+  auto* sp = new SchemaPriv();
+  sp->format = "+s";
+  for (auto& c : cols) {
+    auto* p = new ArrayPriv();
+    auto* ca = new ArrowArray();
+    *ca = ArrowArray{};
+    ca->length = rows;
+    ca->null_count = 0;
+    p->bufs.push_back(std::static_pointer_cast<HostBuf>(c.hold));
+    p->ptrs = {nullptr, c.values};
+    ca->n_buffers = 2;
+    ca->buffers = p->ptrs.data();
+    ca->release = release_array;
+    ca->private_data = p;
+    ap->children.push_back(ca);
+    auto* cs = new ArrowSchema();
+    export_schema_col(*c.meta, cs);
+    sp->children.push_back(cs);
+  }
+  *s = ArrowSchema{};
+  s->format = sp->format.c_str();
+  s->name = sp->name.c_str();
+  s->n_children = (int64_t)sp->children.size();
+  s->children = sp->children.data();
+  s->release = release_schema;
+  s->private_data = sp;
+  *a = ArrowArray{};
+  a->length = rows;
+  a->n_buffers = 1;
+  a->buffers = ap->ptrs.data();
+  a->n_children = (int64_t)ap->children.size();
+  a->children = ap->children.data();
+  a->release = release_array;
+  a->private_data = ap;
+}
+
 void export_batch(Ctx& ctx, const Batch& b, ArrowArray* a, ArrowSchema* s) {
   if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null output ArrowArray/ArrowSchema");
   for (auto& c : b.cols)

@@ -16,6 +16,7 @@
 #include "join.hpp"
 #include "join_device.cuh"
 #include "prims.hpp"
+#include "sort.hpp"
 
 namespace prism {
 
@@ -42,16 +43,32 @@ struct KeysGeneral {
   __device__ __forceinline__ uint64_t key(int64_t r) const { return join_key_hash(cols, n, r); }
 };
 
+// The radix-partitioned build and probe (single Int64 key, hash slots): on
+// when the tuning asks for it, or by default (partition < 0) once the slots
+// outgrow L2 — then a stretch of tiles in partition order touches one
+// 1/2^bits slice of the table, which stays in L2.
+bool use_partitioned(const Ctx& ctx, const JoinTable& t, const JoinTuning& tune) {
+  if (t.dense || !t.int64_fast || t.capacity == 0) return false;
+  if (tune.partition >= 0) return tune.partition > 0;
+  return (t.capacity + 1) * sizeof(ulonglong2) > (uint64_t)ctx.l2_bytes;
+}
+int partition_bits(const JoinTable& t, const JoinTuning& tune) {
+  const int b = tune.partition_bits > 0 ? tune.partition_bits : 8;
+  return std::max(1, std::min(std::min(b, 8), t.log2cap));
+}
+
 __global__ void init_slots_kernel(ulonglong2* slots, uint64_t n) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     slots[i] = make_ulonglong2(EMPTY, Y_INIT);
 }
 
+// rowmap: the build row of element i (radix-partitioned build), or null (row i)
 template <class K>
 __global__ void insert_kernel(K keys, int64_t n, ulonglong2* slots, int shift, uint64_t mask, uint64_t cap,
-                              uint32_t* dupflag, uint32_t* err) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t k = keys.key(i);
+                              uint32_t* dupflag, uint32_t* err, const uint32_t* __restrict__ rowmap) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = keys.key(e);
+    const int64_t i = rowmap ? (int64_t)rowmap[e] : e;
     uint64_t s;
     bool winner = false;
     if (K::kFast && k == EMPTY) {
@@ -150,6 +167,8 @@ struct ProbeArgs {
   int64_t n_tiles;
   unsigned long long* total;
   uint32_t* err;
+  int any_order;  // tiles reserve their output by one atomicAdd on *total, no look-back
+  int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
 };
 
 constexpr unsigned long long FLAG_A = 1ULL << 62;
@@ -212,7 +231,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan32(uint32_t x) {
 }
 
 __device__ __forceinline__ void emit_one(const ProbeArgs& a, uint64_t pos, int64_t prow, uint32_t brow) {
-  if (a.out_probe) a.out_probe[pos] = (uint32_t)prow;
+  if (a.out_probe) a.out_probe[pos] = (uint32_t)(prow + a.row_base);
   if (a.out_build) a.out_build[pos] = brow;
 #pragma unroll
   for (int g = 0; g < 4; ++g) {
@@ -321,7 +340,9 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
       uint32_t incl = warp_incl_scan32(wv);
       uint32_t tile_total = __shfl_sync(0xffffffffu, incl, 31);
       if (lane < PW) s_wexcl[lane] = incl - wv;
-      if (EMIT) {
+      if (EMIT && a.any_order) {
+        if (lane == 0) s_excl = tile_total ? atomicAdd(a.total, (unsigned long long)tile_total) : 0ULL;
+      } else if (EMIT) {
         unsigned long long ex = warp_lookback(a.tile_status, tile, tile_total, a.err);
         if (lane == 0) {
           s_excl = ex;
@@ -340,14 +361,13 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         if (!c[it]) continue;
         int64_t r = base + it * 32 + lane;
         uint64_t pos = wbase + lex[it];
-        if (pos + c[it] > a.out_capacity) {
-          atomicOr(a.err, DERR_CAPACITY);
-          continue;
-        }
+        // a short output keeps the prefix of the matches that fits
+        if (pos + c[it] > a.out_capacity) atomicOr(a.err, DERR_CAPACITY);
+        if (pos >= a.out_capacity) continue;
         if ((!DUPS && !VERIFY) || cand[it] == 1) {
           emit_one(a, pos, r, v[it]);
         } else {
-          for (uint32_t j = 0; j < cand[it]; ++j) {
+          for (uint32_t j = 0; j < cand[it] && pos < a.out_capacity; ++j) {
             uint32_t b = a.dup_rows[v[it] + j];
             if (VERIFY && !join_rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
             emit_one(a, pos++, r, b);
@@ -537,11 +557,157 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
       continue;
     }
     if (one8) {  // output streams: evict-first stores
-      if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(base + it * QB + threadIdx.x));
+      if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(a.row_base + base + it * QB + threadIdx.x));
       if (a.out_build) __stcs(a.out_build + pos, v[it]);
       __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it]);
     } else {
       emit_one(a, pos, base + it * QB + threadIdx.x, v[it]);
+    }
+  }
+}
+
+// ------------------------------------------ unique int64 keys, any order --
+// One pass when the caller takes the matches as a multiset (the fused
+// join -> aggregate and join_project with PRISM_JOIN_ANY_ORDER): each CTA
+// loads its 2048 probe keys with 16-byte vector loads, looks them up (dense
+// row or hash slot walk), loads every matched row's gathered values, ranks
+// its matches in row order with warp ballots and one warp scan, reserves its
+// output segment with ONE atomicAdd and writes the segment contiguously. No
+// row words go back to HBM and no CTA waits on another; segments land in
+// whatever order the CTAs reserve them.
+constexpr int AB = 256;            // threads per CTA
+constexpr int AV = 4;              // 16-byte key loads per thread (2 rows each)
+constexpr int AT = AB * AV * 2;    // rows per tile (2048)
+
+// PART: the keys come in radix-partition order (kpart, with each key's probe
+// row in prow): a tile's keys share their top hash bits, so its slot loads
+// stay inside one slice of the table (the partitioned probe of a table
+// larger than L2).
+template <bool DENSE, bool VEC, bool PART>
+__global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
+                                                                const uint32_t* __restrict__ prow, int64_t n,
+                                                                ProbeArgs a) {
+  __shared__ uint32_t seg[AV * (AB / 32)];
+  __shared__ unsigned long long s_off;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * AT;
+  // positions of this thread: base + 2 * (it * AB + threadIdx.x) + {0, 1}
+  uint64_t key[AV][2];
+  int64_t row[AV][2];  // probe row of each position
+#pragma unroll
+  for (int it = 0; it < AV; ++it) {
+    const int64_t q = base + 2 * (it * AB + threadIdx.x);
+    if (VEC && q + 1 < n) {
+      // streamed once: evict-first, so the table and payload stay in L2
+      const longlong2 kv = __ldcs(reinterpret_cast<const longlong2*>(keys + q));
+      key[it][0] = (uint64_t)kv.x;
+      key[it][1] = (uint64_t)kv.y;
+      if (PART) {
+        const uint2 rv = __ldcs(reinterpret_cast<const uint2*>(prow + q));
+        row[it][0] = rv.x;
+        row[it][1] = rv.y;
+      }
+    } else {
+      key[it][0] = q < n ? (uint64_t)__ldcs(keys + q) : 0;
+      key[it][1] = q + 1 < n ? (uint64_t)__ldcs(keys + q + 1) : 0;
+      if (PART) {
+        row[it][0] = q < n ? __ldcs(prow + q) : 0;
+        row[it][1] = q + 1 < n ? __ldcs(prow + q + 1) : 0;
+      }
+    }
+    if (!PART) {
+      row[it][0] = q;
+      row[it][1] = q + 1;
+    }
+  }
+  uint32_t brow[AV][2];
+  if (DENSE) {
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
+        const uint64_t d = key[it][j] - (uint64_t)a.dmin;
+        brow[it][j] = (q < n && d < a.drange) ? __ldg(a.dense + d) : NO_MATCH;
+      }
+  } else {
+    uint64_t s[AV][2];
+    ulonglong2 e[AV][2];
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
+        s[it][j] = key[it][j] == EMPTY ? a.cap : slot_of(key[it][j], a.shift);
+        e[it][j] = q < n ? __ldg(a.slots + s[it][j]) : make_ulonglong2(EMPTY, 0);
+      }
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
+        uint64_t steps = 0;
+        while (e[it][j].x != key[it][j] && e[it][j].x != EMPTY && steps <= a.mask) {
+          s[it][j] = (s[it][j] + 1) & a.mask;
+          e[it][j] = __ldg(a.slots + s[it][j]);
+          ++steps;
+        }
+        const bool hit = q < n && e[it][j].x == key[it][j] && (e[it][j].y >> 32) != 0;
+        brow[it][j] = hit ? (uint32_t)e[it][j].y : NO_MATCH;
+      }
+  }
+  // one 8-byte gathered column (probe row + payload): its values loaded now,
+  // all in flight before the ranking
+  const bool one8 = a.ngather == 1 && a.g_width[0] == 8;
+  unsigned long long pre[AV][2];
+  if (one8) {
+    const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[0]);
+    const bool bside = a.g_side[0] != 0;
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        pre[it][j] = brow[it][j] != NO_MATCH ? __ldg(src + (bside ? (int64_t)brow[it][j] : row[it][j])) : 0ULL;
+  }
+  // rank in position order: (it, warp, lane, j)
+  uint32_t lpos[AV];
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int it = 0; it < AV; ++it) {
+    const uint32_t m0 = __ballot_sync(0xffffffffu, brow[it][0] != NO_MATCH);
+    const uint32_t m1 = __ballot_sync(0xffffffffu, brow[it][1] != NO_MATCH);
+    lpos[it] = __popc(m0 & lt) + __popc(m1 & lt);
+    if (lane == 0) seg[it * (AB / 32) + warp] = __popc(m0) + __popc(m1);
+  }
+  __syncthreads();
+  if (warp == 0) {  // AV * 8 = 32 segments: one warp scan
+    const uint32_t x = seg[lane];
+    const uint32_t incl = warp_incl_scan32(x);
+    seg[lane] = incl - x;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) s_off = total ? atomicAdd(a.total, (unsigned long long)total) : 0ULL;
+  }
+  __syncthreads();
+  const unsigned long long off = s_off;
+#pragma unroll
+  for (int it = 0; it < AV; ++it) {
+    uint64_t pos = off + seg[it * (AB / 32) + warp] + lpos[it];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (brow[it][j] == NO_MATCH) continue;
+      const int64_t r = row[it][j];
+      if (pos >= a.out_capacity) {
+        atomicOr(a.err, DERR_CAPACITY);
+        continue;
+      }
+      if (one8) {
+        if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(a.row_base + r));
+        if (a.out_build) __stcs(a.out_build + pos, brow[it][j]);
+        __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it][j]);
+      } else {
+        emit_one(a, pos, r, brow[it][j]);
+      }
+      ++pos;
     }
   }
 }
@@ -653,13 +819,28 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   uint64_t mask = cap - 1;
   if (n > 0) {
     int g = grid_for(ctx, n, 256, 16);
-    KernelTimer kt(ctx, "insert_kernel");
-    if (t->int64_fast) {
-      KeysFast kf{static_cast<const int64_t*>(build.cols[keys[0]]->values)};
-      insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err);
+    if (t->int64_fast && use_partitioned(ctx, *t, tune)) {
+      // radix-partitioned build: the keys in the order of the top bits of
+      // their slot hash, so the inserts of a stretch of CTAs hit one slice
+      // of the table (in L2) instead of the whole table at random
+      const int bits = partition_bits(*t, tune);
+      MemP mk, mr;
+      uint64_t* kpart = ctx.alloc_t<uint64_t>((size_t)n, mk);
+      uint32_t* rpart = ctx.alloc_t<uint32_t>((size_t)n, mr);
+      radix_partition(ctx, static_cast<const uint64_t*>(build.cols[keys[0]]->values), n, JOIN_FIB, 64 - bits, bits,
+                      kpart, rpart, "build_partition_hist_kernel", "build_partition_scatter_kernel");
+      KernelTimer kt(ctx, "insert_kernel");
+      KeysFast kf{reinterpret_cast<const int64_t*>(kpart)};
+      insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err, rpart);
     } else {
-      KeysGeneral kg{static_cast<const DCol*>(t->key_views_dev->ptr), (int)keys.size()};
-      insert_kernel<<<g, 256, 0, ctx.stream>>>(kg, n, slots, shift, mask, cap, dupflag, ctx.d_err);
+      KernelTimer kt(ctx, "insert_kernel");
+      if (t->int64_fast) {
+        KeysFast kf{static_cast<const int64_t*>(build.cols[keys[0]]->values)};
+        insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err, nullptr);
+      } else {
+        KeysGeneral kg{static_cast<const DCol*>(t->key_views_dev->ptr), (int)keys.size()};
+        insert_kernel<<<g, 256, 0, ctx.stream>>>(kg, n, slots, shift, mask, cap, dupflag, ctx.d_err, nullptr);
+      }
     }
     ctx.check_launch("insert_kernel");
   }
@@ -757,7 +938,7 @@ int64_t probe_count(Ctx& ctx, const JoinTable& t, const Batch& probe, const std:
 
 ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
                              bool want_probe_idx, bool want_build_idx, std::vector<ProbeGather>& gathers,
-                             int64_t gather_capacity, const JoinTuning& tune) {
+                             int64_t gather_capacity, const JoinTuning& tune, bool any_order, int64_t row_base) {
   check_join_keys(probe, keys, t.build, t.key_cols);
   ProbeResult res;
   if (gathers.size() > 4) fail(PRISM_ERR_INTERNAL, "at most 4 fused gathers");
@@ -783,6 +964,46 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     a.g_dst[g] = gathers[g].dst;
   }
   a.out_capacity = (uint64_t)cap;
+  a.row_base = row_base;
+  if (any_order && t.int64_fast && !t.has_dups) {
+    // unique Int64 keys, matches as a multiset: one pass, one atomicAdd per tile
+    MemP mtot;
+    a.total = ctx.alloc_t<unsigned long long>(1, mtot);
+    PRISM_CUDA(cudaMemsetAsync(a.total, 0, 8, ctx.stream));
+    const int64_t n = probe.rows;
+    const int64_t* pk = static_cast<const int64_t*>(probe.cols[keys[0]]->values);
+    const bool vec = (reinterpret_cast<uintptr_t>(pk) & 15) == 0;
+    const unsigned grid = (unsigned)ceil_div(n, AT);
+    if (!t.dense && use_partitioned(ctx, t, tune)) {
+      // radix-partitioned probe: the keys reordered by the top bits of their
+      // slot hash, so each tile probes one slice of the table
+      MemP mk, mr;
+      uint64_t* kpart = ctx.alloc_t<uint64_t>((size_t)n, mk);
+      uint32_t* rpart = ctx.alloc_t<uint32_t>((size_t)n, mr);
+      const int bits = partition_bits(t, tune);
+      radix_partition(ctx, reinterpret_cast<const uint64_t*>(pk), n, JOIN_FIB, 64 - bits, bits, kpart, rpart,
+                      "probe_partition_hist_kernel", "probe_partition_scatter_kernel");
+      KernelTimer kt(ctx, "probe_emit_any_kernel");
+      probe_emit_any_kernel<false, true, true><<<grid, AB, 0, ctx.stream>>>(reinterpret_cast<const int64_t*>(kpart),
+                                                                             rpart, n, a);
+    } else {
+      KernelTimer kt(ctx, "probe_emit_any_kernel");
+      if (t.dense)
+        vec ? probe_emit_any_kernel<true, true, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a)
+            : probe_emit_any_kernel<true, false, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
+      else
+        vec ? probe_emit_any_kernel<false, true, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a)
+            : probe_emit_any_kernel<false, false, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
+    }
+    ctx.check_launch("probe_emit_any_kernel");
+    unsigned long long total = 0;
+    PRISM_CUDA(cudaMemcpyAsync(&total, a.total, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    uint32_t derr = ctx.take_device_errors();
+    if (derr & DERR_CAPACITY) fail(PRISM_ERR_INTERNAL, "probe output capacity exceeded");
+    res.matches = (int64_t)total;
+    return res;
+  }
+  a.any_order = any_order ? 1 : 0;
   if (t.int64_fast && !t.has_dups) {
     // unique Int64 keys: probe, scan of tile counts, ordered emit
     int64_t n = probe.rows, ntiles = ceil_div(n, QT);

@@ -32,6 +32,10 @@ struct JoinTuning {
   double load_factor = 0.5;
   int probe_blocks_per_sm = 2;
   bool dense = true;  // allow dense mode for single Int64 keys
+  // radix-partitioned build / probe of hash slots (single Int64 key): -1 once
+  // the slots outgrow L2, 0 never, 1 always; 2^partition_bits partitions
+  int partition = -1;
+  int partition_bits = 8;
 };
 
 std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,
@@ -53,11 +57,16 @@ struct ProbeResult {
 
 // Probes `probe` (key columns `keys`, types checked against the table) and
 // emits matches in the reference's order: probe rows ascending, build rows
-// ascending within a probe row. Fused gathers write into caller buffers of
+// ascending within a probe row. With `any_order` the matches come as a
+// multiset (tiles of consecutive probe rows in any order, rows ascending
+// inside a tile), which needs neither look-back nor a second pass.
+// `row_base` is added to the emitted probe row indices (the probe batch is
+// rows [row_base, row_base + probe.rows) of a larger one). Fused gathers write into caller buffers of
 // `gather_capacity` rows (must be >= the match count; use probe_count first).
 ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,
                              bool want_probe_idx, bool want_build_idx, std::vector<ProbeGather>& gathers,
-                             int64_t gather_capacity, const JoinTuning& tune);
+                             int64_t gather_capacity, const JoinTuning& tune, bool any_order = false,
+                             int64_t row_base = 0);
 
 // Number of matches of `probe` against the table (no output).
 int64_t probe_count(Ctx& ctx, const JoinTable& t, const Batch& probe, const std::vector<int>& keys,

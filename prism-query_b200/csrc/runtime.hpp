@@ -85,6 +85,7 @@ struct Ctx {
   std::recursive_mutex mu;
   std::string last_error;
   int sm_count = 148;
+  int64_t l2_bytes = 126LL << 20;  // the device's L2 size
   uint32_t* d_err = nullptr;  // device error flags (one word)
   uint32_t* h_err = nullptr;  // pinned mirror
   // per-kernel CUDA-event timing (off unless enabled)

@@ -40,8 +40,15 @@ __global__ void iota_u32_kernel(uint32_t* p, int64_t n) {
     p[i] = (uint32_t)i;
 }
 
+// digit of an element: bits [shift, shift + log2(mask + 1)) of key * mul
+// (mul = 1 sorts by the key; an odd multiplier partitions by hash bits)
+__device__ __forceinline__ uint32_t radix_digit(uint64_t key, uint64_t mul, int shift, uint32_t mask) {
+  return (uint32_t)((key * mul) >> shift) & mask;
+}
+
 __global__ void __launch_bounds__(RB) radix_hist_kernel(const uint64_t* __restrict__ k, int64_t n, int shift,
-                                                         uint32_t mask, uint32_t* counts, int64_t ntiles) {
+                                                         uint32_t mask, uint32_t* counts, int64_t ntiles,
+                                                         uint64_t mul) {
   __shared__ uint32_t h[256];
   const int tid = threadIdx.x;
   h[tid] = 0;
@@ -55,7 +62,7 @@ __global__ void __launch_bounds__(RB) radix_hist_kernel(const uint64_t* __restri
   }
 #pragma unroll
   for (int r = 0; r < RR; ++r)
-    if (base + r * RB + tid < n) atomicAdd(&h[(uint32_t)(w[r] >> shift) & mask], 1u);
+    if (base + r * RB + tid < n) atomicAdd(&h[radix_digit(w[r], mul, shift, mask)], 1u);
   __syncthreads();
   counts[(int64_t)tid * ntiles + blockIdx.x] = h[tid];
 }
@@ -72,7 +79,8 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
                                                             const uint32_t* __restrict__ vin, int64_t n, int shift,
                                                             uint32_t mask, const uint32_t* __restrict__ counts,
                                                             const uint64_t* __restrict__ offsets, int64_t ntiles,
-                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                            uint64_t mul) {
   extern __shared__ unsigned long long stage[];  // [RT] keys | [RT] row ids
   uint64_t* sk = reinterpret_cast<uint64_t*>(stage);
   uint32_t* sv = reinterpret_cast<uint32_t*>(stage + RT);
@@ -91,7 +99,7 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
   for (int r = 0; r < RR; ++r) {
     const int e = r * RB + tid;
     keys[r] = e < count ? kin[base + e] : 0;
-    vals[r] = e < count ? vin[base + e] : 0;
+    vals[r] = e < count ? (vin ? vin[base + e] : (uint32_t)(base + e)) : 0;  // no vin: the element's index
   }
   // tile-local digit starts: exclusive scan of this tile's digit counts
 #pragma unroll
@@ -119,7 +127,7 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
     const bool valid = e < count;
     const uint64_t key = keys[r];
     const uint32_t val = vals[r];
-    const uint32_t d = valid ? (uint32_t)(key >> shift) & mask : 256u;  // 256: no element
+    const uint32_t d = valid ? radix_digit(key, mul, shift, mask) : 256u;  // 256: no element
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
     if (valid && rank == 0) wc[warp][d] = __popc(peers);
@@ -145,7 +153,7 @@ __global__ void __launch_bounds__(RB) radix_scatter_kernel(const uint64_t* __res
   // digit's global offset for this tile plus its rank inside the digit's run
   for (int j = tid; j < count; j += RB) {
     const uint64_t key = sk[j];
-    const uint32_t d = (uint32_t)(key >> shift) & mask;
+    const uint32_t d = radix_digit(key, mul, shift, mask);
     const uint64_t pos = goff[d] + (uint64_t)j;
     kout[pos] = key;
     vout[pos] = sv[j];
@@ -362,13 +370,13 @@ struct Sorter {
     for (int shift = 0; shift < bits; shift += 8) {
       const int w = std::min(8, bits - shift);
       const uint32_t mask = (1u << w) - 1u;
-      radix_hist_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(ka, n, shift, mask, counts, ntiles);
+      radix_hist_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(ka, n, shift, mask, counts, ntiles, 1ULL);
       ctx.check_launch("radix_hist_kernel");
       scan_u32_async(ctx, counts, offsets, ntiles * 256, total);
       {
         KernelTimer kt(ctx, "radix_scatter_kernel");
         radix_scatter_kernel<<<(unsigned)ntiles, RB, SCATTER_SMEM, ctx.stream>>>(ka, va, n, shift, mask, counts, offsets,
-                                                                                  ntiles, kb, vb);
+                                                                                  ntiles, kb, vb, 1ULL);
       }
       ctx.check_launch("radix_scatter_kernel");
       std::swap(ka, kb);
@@ -525,6 +533,39 @@ Batch sort_batch(Ctx& ctx, const Batch& b, const prism_sort_key* keys, int n_key
   }
   return out;  // stream-ordered: the sort buffers are freed after the gathers
 
+}
+
+// Radix partition of 64-bit keys (with their positions 0..n-1) by the digit
+// bits [shift, shift + bits) of key * mul, bits <= 8: one pass of the sort's
+// machinery — per-tile digit histograms, one scan over (digit, tile), and a
+// scatter that ranks each tile in order, stages it in shared memory and
+// writes every digit's run of the tile contiguously. Output: the keys and
+// their original positions in partition order, positions ascending inside a
+// partition (stable).
+void radix_partition(Ctx& ctx, const uint64_t* keys, int64_t n, uint64_t mul, int shift, int bits,
+                     uint64_t* kout, uint32_t* pos_out, const char* hist_name, const char* scatter_name) {
+  if (n <= 0) return;
+  if (bits < 1 || bits > 8) fail(PRISM_ERR_INTERNAL, "radix partition digit of 1..8 bits");
+  if (n >= (int64_t)UINT32_MAX) fail(PRISM_ERR_INVALID_ARGUMENT, "radix partition of 2^32 rows or more");
+  const int64_t ntiles = ceil_div(n, (int64_t)RT);
+  const uint32_t mask = (1u << bits) - 1u;
+  MemP mc, mo, mt;
+  uint32_t* counts = ctx.alloc_t<uint32_t>((size_t)ntiles * 256, mc);
+  uint64_t* offsets = ctx.alloc_t<uint64_t>((size_t)ntiles * 256, mo);
+  uint64_t* total = ctx.alloc_t<uint64_t>(1, mt);
+  {
+    KernelTimer kt(ctx, hist_name);
+    radix_hist_kernel<<<(unsigned)ntiles, RB, 0, ctx.stream>>>(keys, n, shift, mask, counts, ntiles, mul);
+  }
+  ctx.check_launch("radix_hist_kernel(partition)");
+  scan_u32_async(ctx, counts, offsets, ntiles * 256, total);
+  PRISM_CUDA(cudaFuncSetAttribute(radix_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SCATTER_SMEM));
+  {
+    KernelTimer kt(ctx, scatter_name);
+    radix_scatter_kernel<<<(unsigned)ntiles, RB, SCATTER_SMEM, ctx.stream>>>(keys, nullptr, n, shift, mask, counts,
+                                                                              offsets, ntiles, kout, pos_out, mul);
+  }
+  ctx.check_launch("radix_scatter_kernel(partition)");
 }
 
 }  // namespace prism

@@ -43,6 +43,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PRISM_GPU_LIB", os.path.join(PKG_DIR, "libprism_gpu.so"))
 
 PRISM_COL_PROBE_ROW_INDEX = -1
+PRISM_JOIN_ANY_ORDER = 1  # prism_join_project_ex flag: matches as a multiset
 PRISM_COL_BUILD_ROW_INDEX = -2
 
 
@@ -94,9 +95,12 @@ def _declare(lib):
     lib.prism_hash_table_num_rows.argtypes = [P]
     lib.prism_hash_table_num_rows.restype = C.c_int64
     lib.prism_hash_table_has_duplicates.argtypes = [P]
+    lib.prism_hash_table_layout.argtypes = [P]
     lib.prism_hash_table_free.argtypes = [P]
     lib.prism_hash_table_free.restype = None
     lib.prism_join_project.argtypes = [P, P, P, P, i32, P, i32, C.POINTER(P)]
+    lib.prism_join_project_ex.argtypes = [P, P, P, P, i32, P, i32, C.c_uint32, C.POINTER(P)]
+    lib.prism_join_project_arrow.argtypes = [P, P, P, P, P, i32, P, i32, C.c_uint32, P, P]
     lib.prism_hash_join.argtypes = [P, P, P, P, C.POINTER(P)]
     lib.prism_probe_matches_chunked.argtypes = [P, P, i32, P, P, P, i32, P]
     lib.prism_hash_join_probe_chunked.argtypes = [P, P, i32, P, P, P, C.POINTER(i32)]
@@ -410,23 +414,46 @@ class HashTable:
         return out.column(0), out.column(1)
 
     def join_project(self, probe_batch, probe_key_cols: Sequence[int], out_cols: Sequence[int], as_device=False,
-                     ctx: Optional[Context] = None):
+                     ctx: Optional[Context] = None, any_order: bool = False):
         """Probe and gather `out_cols` of the joined schema (PRISM_COL_* for
         row indices). `ctx` (default: the table's) picks the context, hence
         the stream, the probe runs on: a resident table serves any context of
-        its device."""
+        its device. `any_order`: the matches as a multiset (one-pass probe)."""
         ctx = ctx or self.ctx
         db = _dev(probe_batch, ctx)
         keys = _abi.int_array(probe_key_cols)
         oc = _abi.int_array(out_cols)
         h = C.c_void_p()
-        ctx.check(lib().prism_join_project(ctx.handle, self._h, db.handle, keys, len(probe_key_cols), oc, len(out_cols),
-                                           C.byref(h)))
+        ctx.check(lib().prism_join_project_ex(ctx.handle, self._h, db.handle, keys, len(probe_key_cols), oc,
+                                              len(out_cols), PRISM_JOIN_ANY_ORDER if any_order else 0, C.byref(h)))
         return _result(ctx, h, as_device)
+
+    def join_project_arrow(self, probe_batch: pa.RecordBatch, probe_key_cols: Sequence[int], out_cols: Sequence[int],
+                           any_order: bool = False, ctx: Optional[Context] = None) -> pa.RecordBatch:
+        """join_project with a host probe batch and a host result, through
+        prism_join_project_arrow (streamed in chunks: uploads, probes and
+        downloads overlap)."""
+        ctx = ctx or self.ctx
+        e = _abi.ExportedBatch(probe_batch)
+        keys = _abi.int_array(probe_key_cols)
+        oc = _abi.int_array(out_cols)
+        a, s = _abi.ArrowArray(), _abi.ArrowSchema()
+        try:
+            ctx.check(lib().prism_join_project_arrow(ctx.handle, self._h, e.array_ptr, e.schema_ptr, keys,
+                                                     len(probe_key_cols), oc, len(out_cols),
+                                                     PRISM_JOIN_ANY_ORDER if any_order else 0, C.byref(a), C.byref(s)))
+        finally:
+            e.release()
+        return _abi.import_batch(a, s)
 
     @property
     def has_duplicates(self) -> bool:
         return bool(lib().prism_hash_table_has_duplicates(self._h))
+
+    @property
+    def layout(self) -> str:
+        """'hash' (open-addressing slots) or 'dense' (a row per key value)."""
+        return {0: "hash", 1: "dense"}.get(lib().prism_hash_table_layout(self._h), "unknown")
 
     def free(self):
         if self._h:

@@ -2,7 +2,9 @@
 
 Each case builds the same input batches as the cited reference test and
 records the result the reference asserts. The GPU path and the CPU oracle are
-both checked against them (tests/test_oracle_golden.py, tests/test_gpu_parity.py).
+both checked against them (tests/test_oracle_golden.py for the oracle;
+tests/test_gpu_join.py, test_gpu_agg.py, test_gpu_filter_project.py,
+test_gpu_fused.py, test_gpu_sort.py and test_gpu_distributed.py on the GPU).
 No values here are invented: where the reference asserts only a shape (row or
 column count) the case asserts only that shape.
 """

@@ -159,3 +159,40 @@ def test_deterministic_across_runs(ctx):
     first = prism_gpu.hash_aggregate(b, cfg)
     for _ in range(3):
         assert prism_gpu.hash_aggregate(b, cfg).equals(first)
+
+
+@pytest.mark.parametrize("scale", [1e-40, 1e-30, 3e-39])
+def test_float_sums_below_the_window_bottom(ctx, scale):
+    """Groups whose values all lie near or below 2^-128 (no large value in the
+    call): every mantissa bit counts, so SUM / AVG stay within 1e-12 of the
+    reference's sequential sums (and equal the correctly rounded exact sum)."""
+    rng = np.random.default_rng(int(-np.log10(scale)))
+    n = 20_000
+    g = rng.integers(0, 13, n)
+    v = rng.random(n) * scale
+    b = pa.RecordBatch.from_arrays([pa.array(g), pa.array(v)], names=["g", "v"])
+    cfg = HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "s"), AggExpr(1, AggFunc.Avg, "a"), AggExpr(1, AggFunc.Count, "c")])
+    got = prism_gpu.hash_aggregate(b, cfg)
+    assert_batches_equal(got, oracle.hash_aggregate(b, cfg), float_cols=(1, 2))
+    keys = got.column(0).to_numpy()
+    exact = np.array([oracle.exact_sum_f64(v[g == k]) for k in keys])
+    assert np.array_equal(got.column(1).to_numpy(), exact)
+    # the same values under a dictionary key (few dense groups) and globally
+    d = pa.DictionaryArray.from_arrays(pa.array((g % 3).astype(np.int8)), pa.array(["x", "y", "z"]))
+    bd = pa.RecordBatch.from_arrays([d, pa.array(v)], names=["d", "v"])
+    assert_batches_equal(prism_gpu.hash_aggregate(bd, cfg), oracle.hash_aggregate(bd, cfg), float_cols=(1, 2))
+    gcfg = HashAggConfig([], [AggExpr(1, AggFunc.Sum, "s"), AggExpr(1, AggFunc.Avg, "a")])
+    assert_batches_equal(prism_gpu.hash_aggregate(b, gcfg), oracle.hash_aggregate(b, gcfg), float_cols=(0, 1))
+
+
+def test_float_sum_mixed_tiny_and_unit_values(ctx):
+    """A value near 1e-30 beside values near 1: the sum keeps the tiny value's
+    contribution exactly as the correctly rounded sum does."""
+    v = np.array([1e-30, 1.0, 2.5e-31, 0.75, 1e-40, 3.0], dtype=np.float64)
+    g = np.array([0, 0, 1, 1, 2, 2], dtype=np.int64)
+    b = pa.RecordBatch.from_arrays([pa.array(g), pa.array(v)], names=["g", "v"])
+    cfg = HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "s")])
+    got = prism_gpu.hash_aggregate(b, cfg)
+    assert_batches_equal(got, oracle.hash_aggregate(b, cfg), float_cols=(1,))
+    exact = np.array([oracle.exact_sum_f64(v[g == k]) for k in got.column(0).to_numpy()])
+    assert np.array_equal(got.column(1).to_numpy(), exact)

@@ -174,12 +174,14 @@ def test_join_project_emits_probe_row_and_payload(ctx):
     assert out.schema.names == ["probe_idx", "payload", "x"]
 
 
-@pytest.mark.parametrize("mode", ["1", "0"])
+@pytest.mark.parametrize("mode", ["1", "0", "0p"])
 def test_unique_int64_keys_dense_and_hash_tables(ctx, mode, monkeypatch):
     """Unique Int64 build keys over a compact range use the dense table
-    (PRISM_JOIN_DENSE unset or 1); the hash table (0) must give the same rows.
-    A repeated key in a compact range falls back to the hash table."""
-    monkeypatch.setenv("PRISM_JOIN_DENSE", mode)
+    (PRISM_JOIN_DENSE unset or 1); the hash table (0), also built by the
+    radix-partitioned insert (0p), must give the same rows. A repeated key in
+    a compact range falls back to the hash table."""
+    monkeypatch.setenv("PRISM_JOIN_DENSE", mode[0])
+    monkeypatch.setenv("PRISM_JOIN_PARTITION", "1" if mode == "0p" else "0")
     cases = [(3000, 20000, 4000, False, False), (3000, 20000, 4000, True, False), (50000, 70000, 60000, False, False),
              (3000, 9000, 4000, False, True)]
     for i, (nb, npr, kr, nulls, dup) in enumerate(cases):
@@ -194,3 +196,91 @@ def test_unique_int64_keys_dense_and_hash_tables(ctx, mode, monkeypatch):
     probe = pa.RecordBatch.from_arrays([pa.array(np.arange(-3, 1003, dtype=np.int64))], names=["k"])
     cfg = HashJoinConfig(JoinType.Inner, build_keys=[0], probe_keys=[0])
     assert_batches_equal(prism_gpu.hash_join(probe, build, cfg), oracle.hash_join(probe, build, cfg))
+
+
+def _sorted_pairs(out, ncols):
+    cols = [out.column(i).to_numpy() for i in range(ncols)]
+    order = np.lexsort(cols[::-1])
+    return [c[order] for c in cols]
+
+
+@pytest.mark.parametrize("mode", ["dense", "hash", "partitioned"])
+@pytest.mark.parametrize("case", ["unique", "dup", "utf8", "sliced", "tiles"])
+def test_join_project_any_order_is_the_same_multiset(ctx, mode, case, monkeypatch):
+    """PRISM_JOIN_ANY_ORDER: the same (probe_row, build_row, gathered
+    columns) rows as the probe-order output, compared after sorting — on the
+    one-pass unique-key kernel (dense table, hash table, and the hash table
+    with the radix-partitioned build and probe; aligned and unaligned key
+    columns, ragged tiles) and on the single-pass probe with repeated or Utf8
+    keys."""
+    monkeypatch.setenv("PRISM_JOIN_DENSE", "1" if mode == "dense" else "0")
+    monkeypatch.setenv("PRISM_JOIN_PARTITION", "1" if mode == "partitioned" else "0")
+    keys = [0]
+    if case == "utf8":
+        rng = np.random.default_rng(61)
+        words = [f"w{i:05d}" + "y" * (i % 23) for i in range(3000)]
+        build = pa.RecordBatch.from_arrays([pa.array([words[i] for i in rng.permutation(3000)[:2500]]),
+                                            pa.array(rng.integers(0, 1 << 40, 2500))], names=["s", "v"])
+        probe = pa.RecordBatch.from_arrays([pa.array([words[i] for i in rng.integers(0, 3000, 40000)]),
+                                            pa.array(rng.integers(0, 9, 40000))], names=["s", "z"])
+    elif case == "tiles":
+        probe, build = _int_join_batches(62, 4000, 2048 * 7 + 1, 5000)
+    else:
+        probe, build = _int_join_batches(63, 20000, 150000, 26000, dup=case == "dup")
+        if case == "sliced":
+            probe, build = probe.slice(1, 140001), build.slice(3, 19000)
+    table = HashTable.build(build, keys)
+    oc = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, prism_gpu.PRISM_COL_BUILD_ROW_INDEX, probe.num_columns + 1]
+    ordered = table.join_project(probe, keys, oc)
+    anyo = table.join_project(probe, keys, oc, any_order=True)
+    assert anyo.num_rows == ordered.num_rows
+    for a, b in zip(_sorted_pairs(anyo, 3), _sorted_pairs(ordered, 3)):
+        assert np.array_equal(a, b)
+    # only the probe row and one 8-byte payload: the fast emit of the one-pass kernel
+    oc2 = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, probe.num_columns + 1]
+    a2 = _sorted_pairs(table.join_project(probe, keys, oc2, any_order=True), 2)
+    o2 = _sorted_pairs(table.join_project(probe, keys, oc2), 2)
+    for a, b in zip(a2, o2):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("any_order", [False, True])
+def test_join_project_arrow_streamed_equals_device_path(ctx, any_order):
+    """prism_join_project_arrow (host batch in, host batch out) streams the
+    probe in 8M-row chunks; its rows equal the device-path join_project's:
+    the same rows in the same order (probe order), or the same multiset."""
+    rng = np.random.default_rng(71)
+    nb, npr = 300_000, 2 * (1 << 23) + 12_345  # three chunks, the last one ragged
+    build = pa.RecordBatch.from_arrays([pa.array(rng.permutation(nb).astype(np.int64)),
+                                        pa.array(rng.integers(-(2**62), 2**62, nb))], names=["k", "payload"])
+    probe = pa.RecordBatch.from_arrays([pa.array(rng.integers(-5, int(nb * 1.25), npr).astype(np.int64)),
+                                        pa.array(rng.integers(0, 1000, npr).astype(np.int32))], names=["k", "x"])
+    table = HashTable.build(build, [0])
+    oc = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 3, 1, prism_gpu.PRISM_COL_BUILD_ROW_INDEX]
+    got = table.join_project_arrow(probe, [0], oc, any_order=any_order)
+    ref = table.join_project(probe, [0], oc)
+    assert got.schema.names == ref.schema.names == ["probe_idx", "payload", "x", "build_idx"]
+    assert got.num_rows == ref.num_rows
+    if any_order:
+        g, r = _sorted_pairs(got, 4), _sorted_pairs(ref, 4)
+        for a, b in zip(g, r):
+            assert np.array_equal(a, b)
+    else:
+        assert got.equals(ref)
+    # a sliced probe batch (non-zero offset) takes the same streamed path
+    sl = probe.slice(1_000_003, 9_000_000)
+    assert table.join_project_arrow(sl, [0], oc).equals(table.join_project(sl, [0], oc))
+
+
+def test_join_project_arrow_other_inputs_take_one_pass(ctx):
+    """Repeated build keys, nullable gathered columns or Utf8 keys: one
+    upload, probe and download, with the same result as the device path."""
+    probe, build = _int_join_batches(72, 5000, 60000, 6000, dup=True, nulls=True)
+    table = HashTable.build(build, [0])
+    oc = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 3, 4]
+    assert table.join_project_arrow(probe, [0], oc).equals(table.join_project(probe, [0], oc))
+    probe, build = _int_join_batches(73, 5000, 60000, 6000, nulls=True)
+    table = HashTable.build(build, [0])
+    assert table.join_project_arrow(probe, [0], oc).equals(table.join_project(probe, [0], oc))
+    empty = probe.slice(0, 0)
+    assert table.join_project_arrow(empty, [0], oc).num_rows == 0

@@ -71,11 +71,12 @@ def test_noalloc_probe_equals_allocating_probe(dup):
         assert np.array_equal(got_b, ref_b)
 
 
-def test_noalloc_probe_rejects_sizes_and_short_outputs():
+@pytest.mark.parametrize("dup", [False, True])
+def test_noalloc_probe_rejects_sizes_and_short_outputs(dup):
     import torch
 
     ctx = prism_gpu.default_context()
-    build, pkeys = _inputs(False, seed=3)
+    build, pkeys = _inputs(dup, seed=3)
     table = prism_gpu.HashTable.build(build, [0], ctx)
     f = _noalloc()
     keys_dev = torch.from_numpy(pkeys).to("cuda")
@@ -85,11 +86,16 @@ def test_noalloc_probe_rejects_sizes_and_short_outputs():
     rc = f(ctx.handle, table._h, keys_dev.data_ptr(), MAX_ROWS + 1, out.data_ptr(), out.data_ptr(), 16, C.byref(m))
     assert rc == 3
     assert b"maximum" in prism_gpu.lib().prism_last_error(ctx.handle)
-    # too small an output: nothing past the capacity, the full count reported
-    ref_p, _ = table.probe(pa.RecordBatch.from_arrays([pa.array(pkeys)], names=["k"]), [0])
-    out_p = torch.empty(100, dtype=torch.int32, device="cuda")
-    out_b = torch.empty(100, dtype=torch.int32, device="cuda")
-    torch.cuda.synchronize()
-    rc = f(ctx.handle, table._h, keys_dev.data_ptr(), len(pkeys), out_p.data_ptr(), out_b.data_ptr(), 100, C.byref(m))
-    assert rc == 3 and m.value == len(ref_p)
-    assert np.array_equal(out_p.cpu().numpy().view(np.uint32), ref_p.to_numpy()[:100])
+    # too small an output: the prefix of the matches that fits (with repeated
+    # keys, a probe row's matches may straddle the capacity), nothing past it,
+    # the full count reported
+    ref_p, ref_b = table.probe(pa.RecordBatch.from_arrays([pa.array(pkeys)], names=["k"]), [0])
+    for cap in (100, 101, 1003):
+        out_p = torch.full((cap + 8,), -7, dtype=torch.int32, device="cuda")
+        out_b = torch.full((cap + 8,), -7, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        rc = f(ctx.handle, table._h, keys_dev.data_ptr(), len(pkeys), out_p.data_ptr(), out_b.data_ptr(), cap, C.byref(m))
+        assert rc == 3 and m.value == len(ref_p)
+        assert np.array_equal(out_p[:cap].cpu().numpy().view(np.uint32), ref_p.to_numpy()[:cap])
+        assert np.array_equal(out_b[:cap].cpu().numpy().view(np.uint32), ref_b.to_numpy()[:cap])
+        assert (out_p[cap:].cpu().numpy() == -7).all() and (out_b[cap:].cpu().numpy() == -7).all()
