@@ -546,6 +546,16 @@ int prism_batch_pack(prism_ctx* ctx, const prism_batch* batch, void* device_dst,
  * reused once this returns). Checks the header and every buffer range
  * against `size`; synchronises the context's stream. */
 int prism_batch_unpack(prism_ctx* ctx, const void* device_src, uint64_t size, prism_batch** out);
+/* The same packed format on the host, for exchanges whose transport is host
+ * memory (a gloo or TCP group, a file): a host struct array packed into host
+ * memory, and a host packed buffer read back into a host struct array (the
+ * result owns a copy). No device or context is needed; a packed buffer made
+ * by either side unpacks on either side. */
+int prism_arrow_packed_size(const struct ArrowArray* batch, const struct ArrowSchema* schema, uint64_t* size);
+int prism_arrow_pack(const struct ArrowArray* batch, const struct ArrowSchema* schema, void* host_dst,
+                     uint64_t capacity);
+int prism_arrow_unpack(const void* host_src, uint64_t size, struct ArrowArray* out,
+                       struct ArrowSchema* out_schema);
 
 /* The reducer merge (handler.rs:327-344): hash_aggregate_batches over the
  * partials (in the given order: the reference puts the reducer's own first,

@@ -1102,6 +1102,44 @@ int prism_batch_unpack(prism_ctx* c, const void* src, uint64_t size, prism_batch
   });
 }
 
+int prism_arrow_packed_size(const ArrowArray* a, const ArrowSchema* s, uint64_t* size) {
+  try {
+    if (!size) fail(PRISM_ERR_INVALID_ARGUMENT, "null output");
+    std::vector<std::shared_ptr<std::vector<uint8_t>>> keep;
+    *size = packed_size(host_batch(a, s, keep));
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+int prism_arrow_pack(const ArrowArray* a, const ArrowSchema* s, void* dst, uint64_t capacity) {
+  try {
+    std::vector<std::shared_ptr<std::vector<uint8_t>>> keep;
+    pack_host(host_batch(a, s, keep), dst, capacity);
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+int prism_arrow_unpack(const void* src, uint64_t size, ArrowArray* out, ArrowSchema* out_schema) {
+  try {
+    std::shared_ptr<std::vector<uint8_t>> payload;
+    Batch b = unpack_host(src, size, payload);
+    export_host_batch(b, payload, out, out_schema);
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    t_err = "host allocation failed";
+    return PRISM_ERR_NO_MEMORY;
+  }
+}
+
 int prism_merge_partial_aggregates(prism_ctx* c, const prism_batch* const* partials, int32_t n,
                                    const prism_agg_config* original, prism_batch** out) {
   return run(c, [&] {

@@ -447,6 +447,7 @@ void release_schema(ArrowSchema* s) {
 }
 struct ArrayPriv {
   std::vector<std::shared_ptr<HostBuf>> bufs;
+  std::vector<std::shared_ptr<void>> holds;  // other owners of the buffers (host_batch exports)
   std::vector<const void*> ptrs;
   std::vector<ArrowArray*> children;
   ArrowArray* dict = nullptr;
@@ -615,6 +616,147 @@ Batch import_device_batch(Ctx& ctx, const ArrowDeviceArray* a, const ArrowSchema
     fail(PRISM_ERR_INVALID_ARGUMENT, "device array lives on another device");
   if (dev && a->sync_event) PRISM_CUDA(cudaStreamWaitEvent(ctx.stream, *static_cast<cudaEvent_t*>(a->sync_event), 0));
   return import_batch(ctx, &a->array, s, dev);
+}
+
+
+// ------------------------------------------------------- host-side batches --
+namespace {
+
+// bits [off, off + n) of `in`, realigned to bit 0
+std::vector<uint8_t> realign_bits_host(const uint8_t* in, int64_t off, int64_t n) {
+  const int64_t nbytes = (n + 7) / 8;
+  std::vector<uint8_t> out((size_t)nbytes + 1, 0);
+  const int sh = (int)(off & 7);
+  const uint8_t* b = in + (off >> 3);
+  const int64_t src_bytes = ((off & 7) + n + 7) / 8;  // bytes of `in` that hold the bits
+  for (int64_t j = 0; j < nbytes; ++j) {
+    const uint32_t lo = b[j];
+    const uint32_t hi = j + 1 < src_bytes ? b[j + 1] : 0u;
+    out[(size_t)j] = (uint8_t)(((hi << 8) | lo) >> sh);
+  }
+  return out;
+}
+
+ColP host_column(const ArrowArray* a, const ArrowSchema* s, int64_t extra_off, int64_t len,
+                 std::vector<std::shared_ptr<std::vector<uint8_t>>>& keep) {
+  auto c = std::make_shared<Column>();
+  c->name = s->name ? s->name : "";
+  c->nullable = (s->flags & ARROW_FLAG_NULLABLE) != 0;
+  c->length = len;
+  int32_t t, prec = 38, scale = 0;
+  if (!parse_format(s->format, t, prec, scale))
+    fail(PRISM_ERR_ARROW, std::string("unsupported arrow format '") + (s->format ? s->format : "") + "'");
+  c->precision = prec;
+  c->scale = scale;
+  const int64_t off = a->offset + extra_off;
+  if (s->dictionary) {
+    c->type = TY_DICT;
+    c->index_type = t;
+    c->dict = host_column(a->dictionary, s->dictionary, 0, a->dictionary->length, keep);
+    if (c->dict->type != TY_UTF8) fail(PRISM_ERR_ARROW, "only Utf8 dictionaries are supported");
+  } else {
+    c->type = t;
+  }
+  if (t == TY_NULL) return c;
+  auto bits = [&](const void* src) -> uint8_t* {
+    const uint8_t* b = static_cast<const uint8_t*>(src);
+    if ((off & 7) == 0) return const_cast<uint8_t*>(b + (off >> 3));
+    keep.push_back(std::make_shared<std::vector<uint8_t>>(realign_bits_host(b, off, len)));
+    return keep.back()->data();
+  };
+  if (a->null_count != 0 && a->buffers[0]) c->validity = bits(a->buffers[0]);
+  if (c->type == TY_UTF8) {
+    const int32_t* offs = static_cast<const int32_t*>(a->buffers[1]);
+    c->offsets = const_cast<int32_t*>(offs + off);
+    c->data_base = offs[off];
+    c->data_bytes = offs[off + len] - offs[off];
+    c->data = const_cast<uint8_t*>(static_cast<const uint8_t*>(a->buffers[2])) + c->data_base;
+  } else if (c->type == TY_BOOL) {
+    c->values = bits(a->buffers[1]);
+  } else {
+    const int w = width_of(c->type == TY_DICT ? c->index_type : c->type);
+    c->values = const_cast<uint8_t*>(static_cast<const uint8_t*>(a->buffers[1]) + off * w);
+  }
+  return c;
+}
+
+void host_array_col(const Column& c, ArrowArray* a, const std::shared_ptr<void>& hold) {
+  auto* p = new ArrayPriv();
+  p->holds.push_back(hold);
+  *a = ArrowArray{};
+  a->length = c.length;
+  const int64_t n = c.length;
+  if (c.type == TY_NULL) {
+    a->null_count = n;
+    a->n_buffers = 0;
+  } else {
+    a->null_count = c.validity ? -1 : 0;
+    p->ptrs.push_back(c.validity);
+    if (c.type == TY_UTF8) {
+      // offsets rebased to the column's first byte
+      auto o = std::make_shared<std::vector<int32_t>>((size_t)n + 1, 0);
+      if (c.offsets)
+        for (int64_t i = 0; i <= n; ++i) (*o)[(size_t)i] = c.offsets[i] - c.data_base;
+      p->holds.push_back(o);
+      p->ptrs.push_back(o->data());
+      p->ptrs.push_back(c.data ? c.data : reinterpret_cast<uint8_t*>(o->data()));
+    } else {
+      p->ptrs.push_back(c.values);
+    }
+    a->n_buffers = (int64_t)p->ptrs.size();
+    a->buffers = p->ptrs.data();
+  }
+  if (c.type == TY_DICT) {
+    p->dict = new ArrowArray();
+    host_array_col(*c.dict, p->dict, hold);
+    a->dictionary = p->dict;
+  }
+  a->release = release_array;
+  a->private_data = p;
+}
+
+}  // namespace
+
+Batch host_batch(const ArrowArray* a, const ArrowSchema* s, std::vector<std::shared_ptr<std::vector<uint8_t>>>& keep) {
+  if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null ArrowArray/ArrowSchema");
+  if (!s->format || std::string(s->format) != "+s")
+    fail(PRISM_ERR_ARROW, "a RecordBatch must be exported as a struct array (format '+s')");
+  if (a->n_children != s->n_children) fail(PRISM_ERR_ARROW, "array/schema child count mismatch");
+  Batch b;
+  b.rows = a->length;
+  for (int64_t i = 0; i < s->n_children; ++i) b.cols.push_back(host_column(a->children[i], s->children[i], a->offset, a->length, keep));
+  return b;
+}
+
+void export_host_batch(const Batch& b, const std::shared_ptr<void>& hold, ArrowArray* a, ArrowSchema* s) {
+  if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null output ArrowArray/ArrowSchema");
+  auto* ap = new ArrayPriv();
+  ap->ptrs = {nullptr};
+  auto* sp = new SchemaPriv();
+  sp->format = "+s";
+  for (auto& c : b.cols) {
+    auto* ca = new ArrowArray();
+    host_array_col(*c, ca, hold);
+    ap->children.push_back(ca);
+    auto* cs = new ArrowSchema();
+    export_schema_col(*c, cs);
+    sp->children.push_back(cs);
+  }
+  *s = ArrowSchema{};
+  s->format = sp->format.c_str();
+  s->name = sp->name.c_str();
+  s->n_children = (int64_t)sp->children.size();
+  s->children = sp->children.data();
+  s->release = release_schema;
+  s->private_data = sp;
+  *a = ArrowArray{};
+  a->length = b.rows;
+  a->n_buffers = 1;
+  a->buffers = ap->ptrs.data();
+  a->n_children = (int64_t)ap->children.size();
+  a->children = ap->children.data();
+  a->release = release_array;
+  a->private_data = ap;
 }
 
 std::vector<HostView> host_view(const ArrowArray* a, const ArrowSchema* s) {

@@ -35,6 +35,13 @@ std::vector<HostView> host_view(const ArrowArray* a, const ArrowSchema* s);
 // back to the pool by the consumer's release callback).
 void export_host_columns(const std::vector<HostOutCol>& cols, int64_t rows, ArrowArray* a, ArrowSchema* s);
 
+// A host struct array as a Batch whose column pointers are HOST pointers
+// (no copy; bitmaps not starting on a byte boundary are realigned into
+// `keep`). For host-side code only (the packed exchange format on the host).
+Batch host_batch(const ArrowArray* a, const ArrowSchema* s, std::vector<std::shared_ptr<std::vector<uint8_t>>>& keep);
+// Exports a Batch of HOST pointers (kept alive by `hold`) as a struct array.
+void export_host_batch(const Batch& b, const std::shared_ptr<void>& hold, ArrowArray* a, ArrowSchema* s);
+
 // Page-locked host staging from the process-wide recycling pool: a buffer of
 // at least `bytes` (its size in *size), or nullptr when pinning fails.
 void* pinned_get(size_t bytes, size_t* size);

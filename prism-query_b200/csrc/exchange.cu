@@ -236,29 +236,21 @@ void pack_batch(Ctx& ctx, const Batch& b, void* dst, uint64_t capacity) {
     PRISM_CUDA(cudaMemcpyAsync(d + p.first, p.second.src, p.second.bytes, cudaMemcpyDeviceToDevice, ctx.stream));
 }
 
-Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size) {
-  if (!src) fail(PRISM_ERR_INVALID_ARGUMENT, "null packed buffer");
-  if (size < sizeof(PackHead)) fail(PRISM_ERR_INVALID_ARGUMENT, "packed buffer shorter than its header");
-  PackHead head{};
-  PRISM_CUDA(cudaMemcpyAsync(&head, src, sizeof head, cudaMemcpyDeviceToHost, ctx.stream));
-  ctx.sync();
+namespace {
+
+void check_head(const PackHead& head, uint64_t size) {
   if (head.magic != PACK_MAGIC) fail(PRISM_ERR_INVALID_ARGUMENT, "not a packed batch");
   if (head.header_bytes < sizeof head || head.header_bytes > head.total_bytes || head.total_bytes > size ||
       head.n_entries < head.n_cols || head.n_cols < 0 || head.rows < 0 ||
       (uint64_t)head.n_entries > (head.header_bytes - sizeof head) / sizeof(PackEntry))
     fail(PRISM_ERR_INVALID_ARGUMENT, "packed batch header out of range");
-  std::vector<uint8_t> h(head.header_bytes);
-  PRISM_CUDA(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, ctx.stream));
+}
+
+// The columns described by a packed header `h` (host bytes), with every
+// buffer at payload + (offset - header_bytes); `hold` (if any) owns the payload.
+Batch parse_packed(const PackHead& head, const std::vector<uint8_t>& h, uint8_t* payload, const MemP& hold) {
   std::vector<PackEntry> ents((size_t)head.n_entries);
   std::memcpy(ents.data(), h.data() + sizeof head, ents.size() * sizeof(PackEntry));
-  // one owned copy of the payload; columns point into it
-  const uint64_t payload = head.total_bytes - head.header_bytes;
-  MemP hold = ctx.alloc(std::max<uint64_t>(payload, 16));
-  uint8_t* copy = static_cast<uint8_t*>(hold->ptr);  // packed offset off lives at copy + (off - header_bytes)
-  if (payload)
-    PRISM_CUDA(cudaMemcpyAsync(hold->ptr, static_cast<const uint8_t*>(src) + head.header_bytes, payload,
-                               cudaMemcpyDeviceToDevice, ctx.stream));
-  ctx.sync();
   uint64_t p = sizeof head + ents.size() * sizeof(PackEntry);
   std::vector<ColP> all;
   Batch out;
@@ -293,7 +285,7 @@ Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size) {
       if (e.off[k] < head.header_bytes || e.off[k] % 16 || e.off[k] > head.total_bytes ||
           sz[k] > head.total_bytes - e.off[k])
         fail(PRISM_ERR_INVALID_ARGUMENT, "packed buffer out of range");
-      at[k] = copy + (e.off[k] - head.header_bytes);
+      at[k] = payload + (e.off[k] - head.header_bytes);
     }
     const bool fixed = e.type != TY_UTF8 && e.type != TY_NULL;
     if ((fixed && !at[1] && e.length > 0) || (e.type == TY_UTF8 && !at[2] && e.length > 0))
@@ -302,7 +294,7 @@ Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size) {
     c->values = at[1];
     c->offsets = static_cast<int32_t*>(at[2]);
     c->data = static_cast<uint8_t*>(at[3]);
-    c->owners.push_back(hold);
+    if (hold) c->owners.push_back(hold);
     if (e.parent >= 0) {
       if (e.parent >= (int32_t)all.size() || all[e.parent]->type != TY_DICT || all[e.parent]->dict)
         fail(PRISM_ERR_INVALID_ARGUMENT, "packed dictionary entry out of order");
@@ -318,6 +310,51 @@ Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size) {
     if (c->type == TY_DICT && !c->dict) fail(PRISM_ERR_INVALID_ARGUMENT, "packed dictionary without values");
   }
   return out;
+}
+
+}  // namespace
+
+Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size) {
+  if (!src) fail(PRISM_ERR_INVALID_ARGUMENT, "null packed buffer");
+  if (size < sizeof(PackHead)) fail(PRISM_ERR_INVALID_ARGUMENT, "packed buffer shorter than its header");
+  PackHead head{};
+  PRISM_CUDA(cudaMemcpyAsync(&head, src, sizeof head, cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.sync();
+  check_head(head, size);
+  std::vector<uint8_t> h(head.header_bytes);
+  PRISM_CUDA(cudaMemcpyAsync(h.data(), src, h.size(), cudaMemcpyDeviceToHost, ctx.stream));
+  // one owned copy of the payload; columns point into it
+  const uint64_t payload = head.total_bytes - head.header_bytes;
+  MemP hold = ctx.alloc(std::max<uint64_t>(payload, 16));
+  if (payload)
+    PRISM_CUDA(cudaMemcpyAsync(hold->ptr, static_cast<const uint8_t*>(src) + head.header_bytes, payload,
+                               cudaMemcpyDeviceToDevice, ctx.stream));
+  ctx.sync();
+  return parse_packed(head, h, static_cast<uint8_t*>(hold->ptr), hold);
+}
+
+void pack_host(const Batch& b, void* dst, uint64_t capacity) {
+  const Layout L = layout_of(b);
+  if (!dst) fail(PRISM_ERR_INVALID_ARGUMENT, "null pack destination");
+  if (capacity < L.total) fail(PRISM_ERR_INVALID_ARGUMENT, "pack destination smaller than the packed size");
+  const std::vector<uint8_t> h = header_bytes(b, L);
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  std::memcpy(d, h.data(), h.size());
+  std::memset(d + h.size(), 0, L.total - h.size());  // padding between buffers is defined
+  for (const auto& p : L.pieces) std::memcpy(d + p.first, p.second.src, p.second.bytes);
+}
+
+Batch unpack_host(const void* src, uint64_t size, std::shared_ptr<std::vector<uint8_t>>& payload) {
+  if (!src) fail(PRISM_ERR_INVALID_ARGUMENT, "null packed buffer");
+  if (size < sizeof(PackHead)) fail(PRISM_ERR_INVALID_ARGUMENT, "packed buffer shorter than its header");
+  PackHead head{};
+  std::memcpy(&head, src, sizeof head);
+  check_head(head, size);
+  std::vector<uint8_t> h(static_cast<const uint8_t*>(src), static_cast<const uint8_t*>(src) + head.header_bytes);
+  payload = std::make_shared<std::vector<uint8_t>>(
+      static_cast<const uint8_t*>(src) + head.header_bytes, static_cast<const uint8_t*>(src) + head.total_bytes);
+  if (payload->empty()) payload->resize(16);
+  return parse_packed(head, h, payload->data(), nullptr);
 }
 
 Batch merge_partial_aggregates(Ctx& ctx, const std::vector<const Batch*>& partials, const prism_agg_config& original,

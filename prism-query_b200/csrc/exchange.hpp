@@ -30,6 +30,11 @@ void pack_batch(Ctx& ctx, const Batch& b, void* dst, uint64_t capacity);
 // a copy of the payload. Synchronises the context's stream (the header is
 // read on the host).
 Batch unpack_batch(Ctx& ctx, const void* src, uint64_t size);
+// The same format on the host: a Batch of HOST pointers (host_batch) packed
+// into host memory, and a host packed buffer read back (columns point into
+// `payload`, a copy this call makes). No device is involved.
+void pack_host(const Batch& b, void* dst, uint64_t capacity);
+Batch unpack_host(const void* src, uint64_t size, std::shared_ptr<std::vector<uint8_t>>& payload);
 
 // The reducer merge: hash aggregation of the partials with the final merge
 // configuration (handler.rs:430-457), then the original aggregates rebuilt

@@ -142,6 +142,9 @@ def _declare(lib):
     lib.prism_batch_packed_size.argtypes = [P, C.POINTER(C.c_uint64)]
     lib.prism_batch_pack.argtypes = [P, P, P, C.c_uint64]
     lib.prism_batch_unpack.argtypes = [P, P, C.c_uint64, C.POINTER(P)]
+    lib.prism_arrow_packed_size.argtypes = [P, P, C.POINTER(C.c_uint64)]
+    lib.prism_arrow_pack.argtypes = [P, P, P, C.c_uint64]
+    lib.prism_arrow_unpack.argtypes = [P, C.c_uint64, P, P]
     lib.prism_merge_partial_aggregates.argtypes = [P, P, i32, P, C.POINTER(P)]
     lib.prism_hash_join_arrow.argtypes = [P, P, P, P, P, P, P, P]
     lib.prism_hash_aggregate_arrow.argtypes = [P, P, P, P, P, P]
@@ -641,6 +644,41 @@ def expand_worker_aggregates(config: HashAggConfig) -> HashAggConfig:
         raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
     aggs = [AggExpr(out[i].column, AggFunc(out[i].func), out[i].output_name.decode()) for i in range(n.value)]
     return HashAggConfig(list(config.group_by), aggs)
+
+
+def pack_arrow(batch: pa.RecordBatch) -> bytearray:
+    """A host batch in the packed exchange format (prism_arrow_pack): the
+    same bytes prism_batch_pack writes for the batch on a device."""
+    e = _abi.ExportedBatch(batch)
+    try:
+        n = C.c_uint64(0)
+        rc = lib().prism_arrow_packed_size(e.array_ptr, e.schema_ptr, C.byref(n))
+        if rc:
+            raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+        buf = bytearray(int(n.value))
+        cbuf = (C.c_char * len(buf)).from_buffer(buf)
+        rc = lib().prism_arrow_pack(e.array_ptr, e.schema_ptr, C.addressof(cbuf), len(buf))
+        if rc:
+            raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+        del cbuf
+        return buf
+    finally:
+        e.release()
+
+
+def unpack_arrow(data) -> pa.RecordBatch:
+    """A packed batch (host bytes, from either pack) as a host batch
+    (prism_arrow_unpack; the result owns a copy)."""
+    mv = memoryview(data).cast("B")
+    if mv.readonly:
+        mv = memoryview(bytearray(mv))
+    cbuf = (C.c_char * len(mv)).from_buffer(mv)
+    a, s = _abi.ArrowArray(), _abi.ArrowSchema()
+    rc = lib().prism_arrow_unpack(C.addressof(cbuf), len(mv), C.byref(a), C.byref(s))
+    del cbuf
+    if rc:
+        raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+    return _abi.import_batch(a, s)
 
 
 def merge_partial_aggregates(partials, config: HashAggConfig, ctx: Optional[Context] = None, as_device=False):

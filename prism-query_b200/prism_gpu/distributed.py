@@ -11,16 +11,17 @@ The path shards without a data-path collective except one exchange step:
   then the original aggregates rebuilt). Between GPUs the exchange is one
   NCCL all-gather of packed device buffers (prism_batch_pack /
   prism_batch_unpack), so partial tables never leave HBM; over gloo (the CPU
-  tests) it is an all-gather of Arrow IPC bytes. The partials are merged in
+  tests) it is an all-gather of the same packed format built on the host
+  (prism_arrow_pack / prism_arrow_unpack). The partials are merged in
   the reducer's order (its own first, then the others in rank order), the
   same on every rank, so every rank returns the reducer's result.
-* Joins: the build side is broadcast (every rank holds a replica) and each
+* Joins: the build side is broadcast in the packed format (one NCCL
+  broadcast of the device buffer; every rank holds a replica in HBM) and each
   rank probes its own probe shard; the shards' outputs concatenated in rank
   order are the single-GPU output.
 """
 from __future__ import annotations
 
-import io
 from typing import Callable, List, Optional, Sequence, Tuple
 
 import pyarrow as pa
@@ -60,27 +61,34 @@ def reducer_order(world: int, reducer: int = 0) -> List[int]:
     return [reducer] + [r for r in range(world) if r != reducer]
 
 
-def _to_bytes(batch: pa.RecordBatch) -> bytes:
-    sink = io.BytesIO()
-    with pa.ipc.new_stream(sink, batch.schema) as w:
-        w.write_batch(batch)
-    return sink.getvalue()
-
-
-def _from_bytes(b: bytes) -> pa.RecordBatch:
-    with pa.ipc.open_stream(io.BytesIO(b)) as r:
-        batches = list(r)
-    return batches[0] if batches else None
-
-
-def all_gather_batches(batch: pa.RecordBatch, group=None) -> List[pa.RecordBatch]:
-    """Every rank's batch, in rank order (one all-gather of Arrow IPC bytes)."""
+def _gather_bytes(data: bytes, group=None) -> List[bytes]:
+    """Every rank's bytes, in rank order, over a host (gloo) group: the sizes
+    are all-gathered, every buffer is padded to the largest and one
+    all-gather moves them (the same steps as the device exchange)."""
+    import torch
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
-    got: List[Optional[bytes]] = [None] * world
-    dist.all_gather_object(got, _to_bytes(batch), group=group)
-    return [_from_bytes(b) for b in got]
+    sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    dist.all_gather(sizes, torch.tensor([len(data)], dtype=torch.int64), group=group)
+    host_sizes = [int(x.item()) for x in sizes]
+    cap = max(max(host_sizes), 1)
+    send = torch.zeros(cap, dtype=torch.uint8)
+    if data:
+        send[: len(data)] = torch.frombuffer(bytearray(data), dtype=torch.uint8)
+    recv = [torch.empty(cap, dtype=torch.uint8) for _ in range(world)]
+    dist.all_gather(recv, send, group=group)
+    return [recv[r][: host_sizes[r]].numpy().tobytes() for r in range(world)]
+
+
+def all_gather_batches(batch: pa.RecordBatch, group=None) -> List[pa.RecordBatch]:
+    """Every rank's batch, in rank order, over a host (gloo) group: each rank
+    packs its batch in the library's exchange format (prism_arrow_pack), the
+    packed buffers are all-gathered, and each piece is unpacked
+    (prism_arrow_unpack)."""
+    from . import pack_arrow, unpack_arrow
+
+    return [unpack_arrow(b) for b in _gather_bytes(bytes(pack_arrow(batch)), group)]
 
 
 def all_gather_device_batches(batch, group=None) -> list:
@@ -124,13 +132,48 @@ def gather_partials(part, group=None, reducer: int = 0) -> list:
     return [every[r] for r in reducer_order(world, reducer)]
 
 
-def broadcast_batch(batch: Optional[pa.RecordBatch], src: int = 0, group=None) -> pa.RecordBatch:
-    """`src`'s batch on every rank (one broadcast of Arrow IPC bytes)."""
+def broadcast_batch(batch, src: int = 0, group=None, ctx=None):
+    """`src`'s batch on every rank (the build side of a sharded join,
+    replacing the concatenated build broadcast of
+    prism-substrait/src/executor.rs:222-232).
+
+    Over an NCCL group the batch travels in HBM: `src` packs it into one
+    device buffer (prism_batch_pack; a host batch is imported first), the
+    packed size and then the buffer go out in one broadcast each, and every
+    rank unpacks its copy (prism_batch_unpack); the result is a DeviceBatch.
+    Over a host (gloo) group the packed bytes are built and read on the host
+    (prism_arrow_pack / prism_arrow_unpack); the result is a host batch."""
+    import torch
     import torch.distributed as dist
 
-    obj = [_to_bytes(batch) if dist.get_rank(group) == src else None]
-    dist.broadcast_object_list(obj, src=src, group=group)
-    return _from_bytes(obj[0])
+    from . import DeviceBatch, default_context, pack_arrow, unpack_arrow
+
+    me = dist.get_rank(group)
+    if dist.get_backend(group) == "nccl":
+        ctx = ctx or default_context()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        size = torch.zeros(1, dtype=torch.int64, device=dev)
+        db = None
+        if me == src:
+            db = batch if isinstance(batch, DeviceBatch) else DeviceBatch.from_arrow(batch, ctx)
+            size.fill_(db.packed_size())
+        dist.broadcast(size, src=src, group=group)
+        n = int(size.item())
+        buf = torch.empty(max(n, 16), dtype=torch.uint8, device=dev)
+        if me == src:
+            db.pack_into(buf.data_ptr(), buf.numel())
+            db.ctx.synchronize()
+        dist.broadcast(buf, src=src, group=group)
+        torch.cuda.current_stream().synchronize()
+        return DeviceBatch.unpack(buf.data_ptr(), n, ctx=ctx)
+    data = bytes(pack_arrow(batch)) if me == src else b""
+    size = torch.tensor([len(data)], dtype=torch.int64)
+    dist.broadcast(size, src=src, group=group)
+    buf = torch.zeros(max(int(size.item()), 1), dtype=torch.uint8)
+    if me == src and data:
+        buf[: len(data)] = torch.frombuffer(bytearray(data), dtype=torch.uint8)
+    dist.broadcast(buf, src=src, group=group)
+    return unpack_arrow(buf[: int(size.item())].numpy().tobytes())
 
 
 def _merge(parts, cfg: HashAggConfig, merge: Optional[Callable], kw) -> pa.RecordBatch:

@@ -12,7 +12,7 @@ import oracle_py as oracle
 import prism_gpu
 from golden import reference_kat as K
 from helpers import assert_batches_equal
-from prism_gpu import AggExpr, AggFunc, DeviceBatch, HashAggConfig
+from prism_gpu import AggExpr, AggFunc, DeviceBatch, HashAggConfig, HashJoinConfig, JoinType
 from prism_gpu import distributed as D
 
 pytestmark = pytest.mark.gpu
@@ -195,5 +195,21 @@ def test_nccl_group_of_one(ctx, tmp_path):
             nk = len(cfg.group_by)
             floats = tuple(nk + i for i, a in enumerate(cfg.aggregates) if a.func in (F.Sum, F.Avg, F.Min, F.Max))
             assert_batches_equal(got, ref, float_cols=floats)
+        # sharded join -> aggregate and join: the build side broadcast as one
+        # packed device buffer (NCCL), unpacked into HBM
+        rng = np.random.default_rng(12)
+        build = pa.RecordBatch.from_arrays([pa.array(rng.permutation(4000).astype(np.int64)),
+                                            pa.array(rng.integers(0, 25, 4000).astype(np.int32)),
+                                            pa.array([f"b{i % 31}" for i in range(4000)])], names=["key", "gid", "tag"])
+        probes = [pa.RecordBatch.from_arrays([pa.array(rng.integers(-50, 4500, 30_000)), pa.array(rng.lognormal(5, 1, 30_000))],
+                                             names=["key", "amount"]) for _ in range(2)]
+        jcfg = HashAggConfig([0], [AggExpr(1, F.Sum, "s"), AggExpr(1, F.Count, "n")])
+        got = D.sharded_join_aggregate(probes, build, [0], [0], [3, 1], [], jcfg, ctx=ctx)
+        assert_batches_equal(got, oracle.join_aggregate(probes, build, [0], [0], [3, 1], [], jcfg), float_cols=(1,))
+        jc = HashJoinConfig(JoinType.Inner, build_keys=[0], probe_keys=[0])
+        got = D.sharded_hash_join(probes[0], build, jc, ctx=ctx)
+        assert_batches_equal(got, oracle.hash_join(probes[0], build, jc))
+        bb = D.broadcast_batch(build, ctx=ctx)
+        assert bb.to_arrow().equals(build)
     finally:
         dist.destroy_process_group()

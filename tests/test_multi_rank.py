@@ -1,7 +1,11 @@
 """Multi-rank host logic on CPU: two gloo ranks shard the rows, compute their
 partial tables under the reference's worker config (with the oracle standing
-in for each rank's GPU), exchange them, and merge them by the reference's
-reducer rule (the oracle's restatement of prism-bench/src/handler.rs:327-344).
+in for each rank's GPU), exchange them through the library's own exchange
+(each partial packed by prism_arrow_pack in the format prism_batch_pack
+writes on a GPU, the packed sizes and buffers all-gathered, each piece
+unpacked by prism_arrow_unpack; the join build side broadcast the same way),
+and merge them by the reference's reducer rule (the oracle's restatement of
+prism-bench/src/handler.rs:327-344).
 The merged result must reproduce the single-call result of the oracle — same
 groups in the same first-seen order, integer results exact, Float64 within
 1e-12 — where the decomposition is exact (no COUNT DISTINCT, no group whose
@@ -113,6 +117,14 @@ def _rank_main(rank, world, store, outdir):
                 keys = [(n, "ascending") for n in ref.schema.names]
                 got, ref = got.sort_by(keys), ref.sort_by(keys)
             assert_batches_equal(got.combine_chunks().to_batches()[0], ref.combine_chunks().to_batches()[0])
+        # the exchange itself: every rank's packed batch comes back bit-exact
+        # (nulls, a sliced Utf8 column, dictionaries) in rank order
+        b = data[rank].slice(11 * rank + 3, 5_000)
+        every = D.all_gather_batches(b)
+        for r in range(world):
+            assert every[r].equals(data[r].slice(11 * r + 3, 5_000))
+        bb = D.broadcast_batch(build if rank == 1 else None, src=1)
+        assert bb.equals(build)
         with open(os.path.join(outdir, f"rank{rank}.json"), "w") as f:
             json.dump({"ok": True}, f)
     finally:
