@@ -620,6 +620,53 @@ const char* prism_server_last_error(prism_server* server);
 void prism_server_destroy(prism_server* server);
 
 /* ------------------------------------------------------------------------ */
+/* Autotuner and the per-shape tuning table                                  */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference, whose one knob on this path is the
+ * compile-time HASH_PARTITIONS = 64 (hash_join.rs:43). Each prism_tune_* call
+ * times candidate settings of one operator on the caller's data (CUDA
+ * events, median of repeated runs after a warm-up), records the fastest for
+ * the input's shape class in the process-wide tuning table, and reports
+ * every candidate in *result (may be NULL). Later calls of that shape class
+ * use the record; settings given through the environment (PRISM_JOIN_DENSE,
+ * PRISM_JOIN_PARTITION, PRISM_JOIN_AGG_SHAPE, PRISM_HASH_AGG_BLOCK) take
+ * precedence. Shape classes: joins and join -> aggregates by key kind
+ * (single Int64 or general) and log2 of the build rows; hashed-groups
+ * aggregation by log2 of the input rows. The table is loaded from the file
+ * named by PRISM_TUNING_FILE at first use, and saved / loaded explicitly
+ * below (a text file, one record per line). */
+#define PRISM_TUNE_MAX_CANDIDATES 16
+typedef struct prism_tune_result {
+  int32_t n_candidates;
+  int32_t best;                                /* index of the fastest */
+  double ms[PRISM_TUNE_MAX_CANDIDATES];        /* median time of each candidate */
+  char desc[PRISM_TUNE_MAX_CANDIDATES][64];    /* each candidate's settings */
+} prism_tune_result;
+/* Join table layout (dense rows / hash slots), load factor and the
+ * radix-partitioned build + probe (off, 2^8 or 2^6 partitions), timed as a
+ * table build plus one probe (flags: PRISM_JOIN_ANY_ORDER as the calls to
+ * be tuned will pass it). */
+int prism_tune_join(prism_ctx* ctx, const prism_batch* build, const prism_batch* probe, const int32_t* build_keys,
+                    const int32_t* probe_keys, int32_t n_keys, uint32_t flags, prism_tune_result* result);
+/* The fused join -> aggregate kernel's shape (threads per block, blocks per
+ * SM, probe rows in flight, group-table slots), timed as whole
+ * prism_join_aggregate calls with these arguments. */
+int prism_tune_join_aggregate(prism_ctx* ctx, const prism_batch* const* probes, int32_t n_probes,
+                              const prism_batch* build, const int32_t* probe_keys, const int32_t* build_keys,
+                              int32_t n_keys, const int32_t* cols, int32_t n_cols, const prism_expr* exprs,
+                              int32_t n_exprs, const prism_agg_config* agg, prism_tune_result* result);
+/* The hashed-groups aggregation kernel's block size, timed as whole
+ * prism_hash_aggregate_batches calls. */
+int prism_tune_hash_aggregate(prism_ctx* ctx, const prism_batch* const* batches, int32_t n_batches,
+                              const prism_agg_config* config, prism_tune_result* result);
+int prism_tuning_save(const char* path);
+int prism_tuning_load(const char* path);  /* merges the file's records into the table */
+void prism_tuning_clear(void);
+/* The table in its file format: copies at most capacity - 1 bytes and a NUL;
+ * returns the full length. */
+int64_t prism_tuning_dump(char* buf, int64_t capacity);
+
+/* ------------------------------------------------------------------------ */
 /* Arrow-style wrappers: host batches in, host batch out                     */
 /* ------------------------------------------------------------------------ */
 int prism_hash_join_arrow(prism_ctx* ctx, const struct ArrowArray* probe,

@@ -19,6 +19,9 @@ struct AggTuning {
   int join_rows = 2;
   int join_table_log2 = 9;
   int hash_block = 1024;  // threads per block of the hashed-groups kernel (1024: 0.068 ms vs 0.080 at 512 on 1M rows x 1,024 groups)
+  // fields the environment set (the tuning table leaves them alone)
+  enum : uint32_t { FIX_JOIN_SHAPE = 1, FIX_HASH_BLOCK = 2 };
+  uint32_t fixed = 0;
 };
 
 struct JoinTable;

@@ -17,6 +17,7 @@
 #include "join.hpp"
 #include "prims.hpp"
 #include "sort.hpp"
+#include "tuning.hpp"
 
 using namespace prism;
 
@@ -66,11 +67,25 @@ std::vector<int> ints(const int32_t* p, int n) {
 JoinTuning join_tuning() {
   JoinTuning t{};
   const char* d = std::getenv("PRISM_JOIN_DENSE");
-  if (d && std::strcmp(d, "0") == 0) t.dense = false;
+  if (d && (std::strcmp(d, "0") == 0 || std::strcmp(d, "1") == 0)) {
+    t.dense = d[0] == '1';
+    t.fixed |= JoinTuning::FIX_DENSE;
+  }
   const char* p = std::getenv("PRISM_JOIN_PARTITION");
-  if (p && (std::strcmp(p, "0") == 0 || std::strcmp(p, "1") == 0)) t.partition = p[0] - '0';
+  if (p && (std::strcmp(p, "0") == 0 || std::strcmp(p, "1") == 0)) {
+    t.partition = p[0] - '0';
+    t.fixed |= JoinTuning::FIX_PARTITION;
+  }
   return t;
 }
+// the environment's settings, then the tuning table's record for the build
+// side's shape class
+JoinTuning join_tuning_for(const Batch& build, const std::vector<int>& keys) {
+  JoinTuning t = join_tuning();
+  apply_join_tuning(join_shape(build, keys), t);
+  return t;
+}
+JoinTuning join_tuning_for(const JoinTable& t) { return join_tuning_for(t.build, t.key_cols); }
 // PRISM_JOIN_AGG_SHAPE=block,min_blocks,rows,table_log2 sets the fused join
 // -> aggregate kernel's shape (block 128-1024 in powers of two, min_blocks
 // 1-8, rows 1, 2, 4 or 8, block table of at most 2^table_log2 slots, 8-12)
@@ -84,11 +99,26 @@ AggTuning agg_tuning() {
     t.join_min_blocks = m;
     t.join_rows = r;
     t.join_table_log2 = l;
+    t.fixed |= AggTuning::FIX_JOIN_SHAPE;
   }
   // PRISM_HASH_AGG_BLOCK=256|512|1024: threads per block of the hashed-groups kernel
   const char* hb = std::getenv("PRISM_HASH_AGG_BLOCK");
-  if (hb && (std::atoi(hb) == 256 || std::atoi(hb) == 512 || std::atoi(hb) == 1024)) t.hash_block = std::atoi(hb);
+  if (hb && (std::atoi(hb) == 256 || std::atoi(hb) == 512 || std::atoi(hb) == 1024)) {
+    t.hash_block = std::atoi(hb);
+    t.fixed |= AggTuning::FIX_HASH_BLOCK;
+  }
   return t;
+}
+// the environment's settings, then the tuning table's record for `rows` input rows
+AggTuning agg_tuning_for(int64_t rows) {
+  AggTuning t = agg_tuning();
+  apply_agg_tuning(rows, t);
+  return t;
+}
+int64_t total_rows(const std::vector<const Batch*>& bs) {
+  int64_t n = 0;
+  for (auto* b : bs) n += b->rows;
+  return n;
 }
 
 // PRISM_JOIN_AGG_FUSED=0 materializes the joined rows before aggregating
@@ -191,7 +221,7 @@ MemP matched_bits(Ctx& ctx, const uint32_t* idx, int64_t n_idx, int64_t n_rows) 
 Batch join_one(Ctx& ctx, const Batch& probe, const Batch& build, const JoinTable& t, const std::vector<int>& pk,
                int join_type, bool chunked) {
   std::vector<ProbeGather> none;
-  ProbeResult pr = probe_join_table(ctx, t, probe, pk, true, true, none, -1, join_tuning());
+  ProbeResult pr = probe_join_table(ctx, t, probe, pk, true, true, none, -1, join_tuning_for(t));
   int64_t n = pr.matches;
   IndexVec pi = as_vec(pr.probe_idx, n), bi = as_vec(pr.build_idx, n);
   switch (join_type) {
@@ -295,7 +325,7 @@ Batch join_project_impl(Ctx& x, const JoinTable& t, const Batch& probe, const st
   }
   if (n_gather > 4) fusable = false;
   int64_t cap = match_upper_bound(t, probe.rows);
-  if (cap < 0) cap = probe_count(x, t, probe, pk, join_tuning());
+  if (cap < 0) cap = probe_count(x, t, probe, pk, join_tuning_for(t));
   bool want_p = !fusable, want_b = !fusable;
   for (int col : oc) {
     if (col == PRISM_COL_PROBE_ROW_INDEX) want_p = true;
@@ -315,7 +345,7 @@ Batch join_project_impl(Ctx& x, const JoinTable& t, const Batch& probe, const st
       gcols.push_back(dst);
     }
   }
-  ProbeResult r = probe_join_table(x, t, probe, pk, want_p, want_b, gathers, cap, join_tuning(),
+  ProbeResult r = probe_join_table(x, t, probe, pk, want_p, want_b, gathers, cap, join_tuning_for(t),
                                    (flags & PRISM_JOIN_ANY_ORDER) != 0);
   Batch res;
   res.rows = r.matches;
@@ -336,6 +366,79 @@ Batch join_project_impl(Ctx& x, const JoinTable& t, const Batch& probe, const st
     }
   }
   return res;
+}
+
+// try_execute_fused_join_aggregate (executor.rs:333-458): the fused kernel
+// (lookup, projection and aggregation of the joined rows in one kernel per
+// probe batch) under `tune`, or the materialising path for shapes it does not
+// take.
+Batch join_aggregate_impl(Ctx& x, const std::vector<const Batch*>& probes, const Batch& bb, const std::vector<int>& pk,
+                          const std::vector<int>& bk, const int32_t* cols, int32_t n_cols, const prism_expr* exprs,
+                          int32_t n_exprs, const prism_agg_config* agg, const AggTuning& tune) {
+  for (const Batch* p : probes) check_join_keys(*p, pk, bb, bk);
+  auto t = build_join_table(x, bb, bk, join_tuning_for(bb, bk));
+  // joined columns referenced by the projection (executor.rs:474-551)
+  const Batch& p0 = *probes[0];
+  int np = (int)p0.cols.size(), total = np + (int)bb.cols.size();
+  std::vector<bool> need(total, false);
+  for (int i = 0; i < n_cols; ++i) {
+    if (cols[i] < 0 || cols[i] >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+    need[cols[i]] = true;
+  }
+  for (int e = 0; e < n_exprs; ++e) {
+    for (int k = 0; k < exprs[e].n_nodes; ++k)
+      if (exprs[e].nodes[k].op == PRISM_EXPR_COLUMN) {
+        int col = exprs[e].nodes[k].column;
+        if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+        need[col] = true;
+      }
+    for (int k = 0; k < exprs[e].n_preds; ++k) {
+      int op = exprs[e].preds[k].op;
+      if (op != PRISM_PRED_LITERAL && op != PRISM_PRED_AND && op != PRISM_PRED_OR && op != PRISM_PRED_NOT) {
+        int col = exprs[e].preds[k].column;
+        if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
+        need[col] = true;
+      }
+    }
+  }
+  if (join_agg_fused()) {
+    // one kernel per probe batch: lookup, projection and aggregation of
+    // the joined rows without materializing them
+    JoinAggSpec js;
+    js.table = t.get();
+    js.probe_keys = pk;
+    try {
+      return aggregate(x, probes, *agg, nullptr, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64, true, tune, &js);
+    } catch (const Failure& f) {
+      if (f.code != PRISM_ERR_INVALID_ARGUMENT || f.msg.find("fused path") == std::string::npos) throw;
+    }
+  }
+  std::vector<Batch> projected;
+  for (const Batch* pbp : probes) {
+    const Batch& pb = *pbp;
+    std::vector<ProbeGather> none;
+    ProbeResult r = probe_join_table(x, *t, pb, pk, true, true, none, -1, join_tuning_for(*t));
+    if (r.matches == 0 && !projected.empty()) continue;
+    Batch joined;
+    joined.rows = r.matches;
+    for (int col = 0; col < total; ++col) {
+      if (!need[col]) {
+        auto z = std::make_shared<Column>();
+        z->type = TY_NULL;
+        z->length = r.matches;
+        joined.cols.push_back(z);
+        continue;
+      }
+      const Column& src = col < np ? *pb.cols[col] : *bb.cols[col - np];
+      const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
+      joined.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(pb, bb, col), src.nullable));
+    }
+    projected.push_back(project_with_exprs(x, joined, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64));
+  }
+  std::vector<const Batch*> ps;
+  for (auto& p : projected)
+    if (p.rows > 0 || projected.size() == 1) ps.push_back(&p);
+  return aggregate(x, ps, *agg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, agg_tuning_for(total_rows(ps)));
 }
 
 }  // namespace
@@ -487,7 +590,8 @@ int prism_hash_table_build(prism_ctx* c, const prism_batch* build, const int32_t
     auto* h = new prism_hash_table();
     h->ctx = c;
     try {
-      h->t = build_join_table(c->impl, B(build), ints(keys, n), join_tuning());
+      const std::vector<int> kv = ints(keys, n);
+      h->t = build_join_table(c->impl, B(build), kv, join_tuning_for(B(build), kv));
     } catch (...) {
       delete h;
       throw;
@@ -501,7 +605,7 @@ int prism_hash_table_probe(prism_ctx* c, const prism_hash_table* t, const prism_
   return run(c, [&] {
     if (!t || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null table/output");
     std::vector<ProbeGather> none;
-    ProbeResult r = probe_join_table(c->impl, *t->t, B(probe), ints(keys, n), true, true, none, -1, join_tuning());
+    ProbeResult r = probe_join_table(c->impl, *t->t, B(probe), ints(keys, n), true, true, none, -1, join_tuning_for(*t->t));
     Batch b;
     b.rows = r.matches;
     b.cols.push_back(u32_column(c->impl, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
@@ -684,7 +788,7 @@ int prism_join_project_arrow(prism_ctx* c, const prism_hash_table* tab, const Ar
             gathers.push_back({col < np ? 0 : 1, src.values, width_of(src.type), out_mem[sl][g++]->ptr});
           }
         }
-        held[sl] = probe_join_table(x, t, chunk, pk, want_p, want_b, gathers, rows, join_tuning(), any, lo);
+        held[sl] = probe_join_table(x, t, chunk, pk, want_p, want_b, gathers, rows, join_tuning_for(t), any, lo);
         const int64_t m = held[sl].matches;
         PRISM_CUDA(cudaEventRecord(ev_used[sl], x.stream));
         PRISM_CUDA(cudaEventRecord(ev_probed[sl], x.stream));
@@ -717,7 +821,7 @@ int prism_hash_join(prism_ctx* c, const prism_batch* probe, const prism_batch* b
     if (!cfg || !out) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/output");
     std::vector<int> pk = ints(cfg->probe_keys, cfg->n_keys), bk = ints(cfg->build_keys, cfg->n_keys);
     check_join_keys(B(probe), pk, B(build), bk);
-    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning_for(B(build), bk));
     Batch r = join_one(c->impl, B(probe), B(build), *t, pk, cfg->join_type, false);
     c->impl.sync();
     *out = wrap(c, std::move(r));
@@ -730,12 +834,12 @@ int prism_probe_matches_chunked(prism_ctx* c, const prism_batch* const* probes, 
     if (!out || (n_probes > 0 && !probes)) fail(PRISM_ERR_INVALID_ARGUMENT, "null probes/output");
     std::vector<int> pk = ints(probe_keys, n_keys), bk = ints(build_keys, n_keys);
     for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, B(build), bk);
-    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning_for(B(build), bk));
     std::vector<prism_batch*> res;
     try {
       for (int i = 0; i < n_probes; ++i) {
         std::vector<ProbeGather> none;
-        ProbeResult r = probe_join_table(c->impl, *t, B(probes[i]), pk, true, true, none, -1, join_tuning());
+        ProbeResult r = probe_join_table(c->impl, *t, B(probes[i]), pk, true, true, none, -1, join_tuning_for(*t));
         Batch b;
         b.rows = r.matches;
         b.cols.push_back(u32_column(c->impl, "probe_idx", r.probe_idx, static_cast<uint32_t*>(r.probe_idx->ptr), r.matches));
@@ -757,7 +861,7 @@ int prism_hash_join_probe_chunked(prism_ctx* c, const prism_batch* const* probes
     if (!cfg || !out || !n_out) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/output");
     std::vector<int> pk = ints(cfg->probe_keys, cfg->n_keys), bk = ints(cfg->build_keys, cfg->n_keys);
     for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, B(build), bk);
-    auto t = build_join_table(c->impl, B(build), bk, join_tuning());
+    auto t = build_join_table(c->impl, B(build), bk, join_tuning_for(B(build), bk));
     std::vector<prism_batch*> res;
     try {
       for (int i = 0; i < n_probes; ++i) {
@@ -781,7 +885,8 @@ int prism_hash_aggregate_batches(prism_ctx* c, const prism_batch* const* batches
     if (!cfg || !out || (n > 0 && !batches)) fail(PRISM_ERR_INVALID_ARGUMENT, "null config/batches/output");
     std::vector<const Batch*> bs;
     for (int i = 0; i < n; ++i) bs.push_back(&B(batches[i]));
-    *out = wrap(c, aggregate(c->impl, bs, *cfg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, agg_tuning()));
+    *out = wrap(c, aggregate(c->impl, bs, *cfg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false,
+                             agg_tuning_for(total_rows(bs))));
   });
 }
 
@@ -855,7 +960,7 @@ int prism_filter_project_aggregate(prism_ctx* c, const prism_batch* const* batch
     std::vector<const Batch*> bs;
     for (int i = 0; i < n; ++i) bs.push_back(&B(batches[i]));
     try {
-      *out = wrap(c, aggregate(c->impl, bs, *agg, p, cols, n_cols, exprs, n_exprs, mode, true, agg_tuning()));
+      *out = wrap(c, aggregate(c->impl, bs, *agg, p, cols, n_cols, exprs, n_exprs, mode, true, agg_tuning_for(total_rows(bs))));
       return;
     } catch (const Failure& f) {
       if (f.code != PRISM_ERR_INVALID_ARGUMENT || f.msg.find("fused path") == std::string::npos) throw;
@@ -872,7 +977,7 @@ int prism_filter_project_aggregate(prism_ctx* c, const prism_batch* const* batch
     }
     std::vector<const Batch*> ms;
     for (auto& m : mats) ms.push_back(&m);
-    *out = wrap(c, aggregate(c->impl, ms, *agg, nullptr, nullptr, 0, nullptr, 0, mode, false, agg_tuning()));
+    *out = wrap(c, aggregate(c->impl, ms, *agg, nullptr, nullptr, 0, nullptr, 0, mode, false, agg_tuning_for(total_rows(ms))));
   });
 }
 
@@ -882,78 +987,217 @@ int prism_join_aggregate(prism_ctx* c, const prism_batch* const* probes, int32_t
                          prism_batch** out) {
   return run(c, [&] {
     if (!agg || !out || n_probes <= 0 || !probes) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    std::vector<int> pk = ints(probe_keys, n_keys), bk = ints(build_keys, n_keys);
+    std::vector<const Batch*> pbs;
+    for (int i = 0; i < n_probes; ++i) pbs.push_back(&B(probes[i]));
+    const Batch& bb = B(build);
+    AggTuning tune = agg_tuning();
+    apply_join_agg_tuning(join_shape(bb, bk), tune);
+    *out = wrap(c, join_aggregate_impl(c->impl, pbs, bb, pk, bk, cols, n_cols, exprs, n_exprs, agg, tune));
+  });
+}
+
+// ----------------------------------------------------------- autotuner --
+namespace {
+
+// Times `fn` on the context's stream with CUDA events: one warm-up run, then
+// the median of `reps` runs (milliseconds).
+double time_ms(Ctx& x, int reps, const std::function<void()>& fn) {
+  fn();
+  x.sync();
+  cudaEvent_t a, b;
+  PRISM_CUDA(cudaEventCreate(&a));
+  PRISM_CUDA(cudaEventCreate(&b));
+  std::vector<double> t;
+  for (int i = 0; i < reps; ++i) {
+    PRISM_CUDA(cudaEventRecord(a, x.stream));
+    fn();
+    PRISM_CUDA(cudaEventRecord(b, x.stream));
+    PRISM_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    PRISM_CUDA(cudaEventElapsedTime(&ms, a, b));
+    t.push_back(ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::sort(t.begin(), t.end());
+  return t[t.size() / 2];
+}
+
+void put_result(prism_tune_result* r, const std::vector<std::string>& desc, const std::vector<double>& ms, int best) {
+  if (!r) return;
+  *r = prism_tune_result{};
+  r->n_candidates = (int32_t)std::min<size_t>(desc.size(), PRISM_TUNE_MAX_CANDIDATES);
+  r->best = best;
+  for (int i = 0; i < r->n_candidates; ++i) {
+    r->ms[i] = ms[i];
+    std::snprintf(r->desc[i], sizeof r->desc[i], "%s", desc[i].c_str());
+  }
+}
+
+std::string join_desc(const JoinTuning& t) {
+  char b[64];
+  if (t.dense) std::snprintf(b, sizeof b, "dense rows");
+  else if (t.partition > 0) std::snprintf(b, sizeof b, "hash lf=%.2f partitioned 2^%d", t.load_factor, t.partition_bits);
+  else std::snprintf(b, sizeof b, "hash lf=%.2f streamed", t.load_factor);
+  return b;
+}
+
+}  // namespace
+
+int prism_tune_join(prism_ctx* c, const prism_batch* build, const prism_batch* probe, const int32_t* build_keys,
+                    const int32_t* probe_keys, int32_t n_keys, uint32_t flags, prism_tune_result* result) {
+  return run(c, [&] {
+    if (flags & ~(uint32_t)PRISM_JOIN_ANY_ORDER) fail(PRISM_ERR_INVALID_ARGUMENT, "unknown join flags");
+    Ctx& x = c->impl;
+    const Batch& bb = B(build);
+    const Batch& pb = B(probe);
+    std::vector<int> bk = ints(build_keys, n_keys), pk = ints(probe_keys, n_keys);
+    check_join_keys(pb, pk, bb, bk);
+    const JoinShape shape = join_shape(bb, bk);
+    const bool any = (flags & PRISM_JOIN_ANY_ORDER) != 0;
+    // candidates: the dense row table (unique compact Int64 keys), hash slots
+    // at two load factors, and for Int64 keys the radix-partitioned build and
+    // probe at two fan-outs
+    std::vector<JoinTuning> cand;
+    auto mk = [](bool dense, double lf, int part, int bits) {
+      JoinTuning t;
+      t.dense = dense;
+      t.load_factor = lf;
+      t.partition = part;
+      t.partition_bits = bits;
+      return t;
+    };
+    if (shape.key_kind == 0) cand.push_back(mk(true, 0.5, 0, 8));
+    for (double lf : {0.5, 0.7}) {
+      cand.push_back(mk(false, lf, 0, 8));
+      if (shape.key_kind == 0 && any) {
+        cand.push_back(mk(false, lf, 1, 8));
+        cand.push_back(mk(false, lf, 1, 6));
+      }
+    }
+    std::vector<double> ms;
+    std::vector<std::string> desc;
+    std::vector<JoinTuning> kept;
+    int best = -1;
+    for (const JoinTuning& jt : cand) {
+      bool dense_taken = false;
+      const double t = time_ms(x, 3, [&] {
+        auto tab = build_join_table(x, bb, bk, jt);
+        dense_taken = tab->dense;
+        std::vector<ProbeGather> none;
+        probe_join_table(x, *tab, pb, pk, true, true, none, -1, jt, any);
+      });
+      if (jt.dense && !dense_taken) continue;  // the keys do not allow the dense table
+      ms.push_back(t);
+      desc.push_back(join_desc(jt));
+      kept.push_back(jt);
+      if (best < 0 || t < ms[best]) best = (int)ms.size() - 1;
+    }
+    record_join_tuning(shape, kept[best]);
+    put_result(result, desc, ms, best);
+  });
+}
+
+int prism_tune_join_aggregate(prism_ctx* c, const prism_batch* const* probes, int32_t n_probes, const prism_batch* build,
+                              const int32_t* probe_keys, const int32_t* build_keys, int32_t n_keys, const int32_t* cols,
+                              int32_t n_cols, const prism_expr* exprs, int32_t n_exprs, const prism_agg_config* agg,
+                              prism_tune_result* result) {
+  return run(c, [&] {
+    if (!agg || n_probes <= 0 || !probes) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
     Ctx& x = c->impl;
     std::vector<int> pk = ints(probe_keys, n_keys), bk = ints(build_keys, n_keys);
+    std::vector<const Batch*> pbs;
+    for (int i = 0; i < n_probes; ++i) pbs.push_back(&B(probes[i]));
     const Batch& bb = B(build);
-    for (int i = 0; i < n_probes; ++i) check_join_keys(B(probes[i]), pk, bb, bk);
-    auto t = build_join_table(x, bb, bk, join_tuning());
-    // joined columns referenced by the projection (executor.rs:474-551)
-    const Batch& p0 = B(probes[0]);
-    int np = (int)p0.cols.size(), total = np + (int)bb.cols.size();
-    std::vector<bool> need(total, false);
-    for (int i = 0; i < n_cols; ++i) {
-      if (cols[i] < 0 || cols[i] >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
-      need[cols[i]] = true;
+    // fused kernel shapes: (threads per block, blocks per SM, probe rows in
+    // flight per thread, log2 of the block's group-table slots)
+    const int shapes[][4] = {{512, 3, 2, 9}, {512, 2, 2, 10}, {1024, 1, 2, 9}, {256, 6, 2, 9},
+                             {512, 4, 1, 9}, {512, 3, 4, 9},  {256, 4, 4, 9},  {1024, 2, 1, 8}};
+    std::vector<double> ms;
+    std::vector<std::string> desc;
+    std::vector<AggTuning> tried;
+    int best = -1;
+    for (auto& sh : shapes) {
+      AggTuning t = agg_tuning();
+      t.join_block = sh[0];
+      t.join_min_blocks = sh[1];
+      t.join_rows = sh[2];
+      t.join_table_log2 = sh[3];
+      const double v = time_ms(x, 2, [&] {
+        join_aggregate_impl(x, pbs, bb, pk, bk, cols, n_cols, exprs, n_exprs, agg, t);
+      });
+      char d[64];
+      std::snprintf(d, sizeof d, "block %d x %d/SM, %d rows, 2^%d slots", sh[0], sh[1], sh[2], sh[3]);
+      ms.push_back(v);
+      desc.push_back(d);
+      tried.push_back(t);
+      if (best < 0 || v < ms[best]) best = (int)ms.size() - 1;
     }
-    for (int e = 0; e < n_exprs; ++e) {
-      for (int k = 0; k < exprs[e].n_nodes; ++k)
-        if (exprs[e].nodes[k].op == PRISM_EXPR_COLUMN) {
-          int col = exprs[e].nodes[k].column;
-          if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
-          need[col] = true;
-        }
-      for (int k = 0; k < exprs[e].n_preds; ++k) {
-        int op = exprs[e].preds[k].op;
-        if (op != PRISM_PRED_LITERAL && op != PRISM_PRED_AND && op != PRISM_PRED_OR && op != PRISM_PRED_NOT) {
-          int col = exprs[e].preds[k].column;
-          if (col < 0 || col >= total) fail(PRISM_ERR_INVALID_ARGUMENT, "joined column out of range");
-          need[col] = true;
-        }
-      }
-    }
-    if (join_agg_fused()) {
-      // one kernel per probe batch: lookup, projection and aggregation of
-      // the joined rows without materializing them
-      std::vector<const Batch*> pbs;
-      for (int i = 0; i < n_probes; ++i) pbs.push_back(&B(probes[i]));
-      JoinAggSpec js;
-      js.table = t.get();
-      js.probe_keys = pk;
-      try {
-        *out = wrap(c, aggregate(x, pbs, *agg, nullptr, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64, true,
-                                 agg_tuning(), &js));
-        return;
-      } catch (const Failure& f) {
-        if (f.code != PRISM_ERR_INVALID_ARGUMENT || f.msg.find("fused path") == std::string::npos) throw;
-      }
-    }
-    std::vector<Batch> projected;
-    for (int i = 0; i < n_probes; ++i) {
-      const Batch& pb = B(probes[i]);
-      std::vector<ProbeGather> none;
-      ProbeResult r = probe_join_table(x, *t, pb, pk, true, true, none, -1, join_tuning());
-      if (r.matches == 0 && !projected.empty()) continue;
-      Batch joined;
-      joined.rows = r.matches;
-      for (int col = 0; col < total; ++col) {
-        if (!need[col]) {
-          auto z = std::make_shared<Column>();
-          z->type = TY_NULL;
-          z->length = r.matches;
-          joined.cols.push_back(z);
-          continue;
-        }
-        const Column& src = col < np ? *pb.cols[col] : *bb.cols[col - np];
-        const uint32_t* idx = static_cast<const uint32_t*>(col < np ? r.probe_idx->ptr : r.build_idx->ptr);
-        joined.cols.push_back(take(x, src, idx, nullptr, r.matches, joined_name(pb, bb, col), src.nullable));
-      }
-      projected.push_back(project_with_exprs(x, joined, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64));
-    }
-    std::vector<const Batch*> ps;
-    for (auto& p : projected)
-      if (p.rows > 0 || projected.size() == 1) ps.push_back(&p);
-    *out = wrap(c, aggregate(x, ps, *agg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, agg_tuning()));
+    record_join_agg_tuning(join_shape(bb, bk), tried[best]);
+    put_result(result, desc, ms, best);
   });
+}
+
+int prism_tune_hash_aggregate(prism_ctx* c, const prism_batch* const* batches, int32_t n, const prism_agg_config* cfg,
+                              prism_tune_result* result) {
+  return run(c, [&] {
+    if (!cfg || n < 0 || (n > 0 && !batches)) fail(PRISM_ERR_INVALID_ARGUMENT, "null arguments");
+    Ctx& x = c->impl;
+    std::vector<const Batch*> bs;
+    for (int i = 0; i < n; ++i) bs.push_back(&B(batches[i]));
+    std::vector<double> ms;
+    std::vector<std::string> desc;
+    std::vector<AggTuning> tried;
+    int best = -1;
+    for (int block : {256, 512, 1024}) {
+      AggTuning t = agg_tuning();
+      t.hash_block = block;
+      const double v = time_ms(x, 3, [&] {
+        aggregate(x, bs, *cfg, nullptr, nullptr, 0, nullptr, 0, PRISM_ARITH_F64, false, t);
+      });
+      ms.push_back(v);
+      desc.push_back("hashed groups block " + std::to_string(block));
+      tried.push_back(t);
+      if (best < 0 || v < ms[best]) best = (int)ms.size() - 1;
+    }
+    record_agg_tuning(total_rows(bs), tried[best]);
+    put_result(result, desc, ms, best);
+  });
+}
+
+int prism_tuning_save(const char* path) {
+  try {
+    if (!path) fail(PRISM_ERR_INVALID_ARGUMENT, "null path");
+    tuning_save(path);
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+int prism_tuning_load(const char* path) {
+  try {
+    if (!path) fail(PRISM_ERR_INVALID_ARGUMENT, "null path");
+    tuning_load(path);
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    t_err = f.msg;
+    return f.code;
+  }
+}
+
+void prism_tuning_clear(void) { tuning_clear(); }
+
+int64_t prism_tuning_dump(char* buf, int64_t capacity) {
+  const std::string d = tuning_dump();
+  if (buf && capacity > 0) {
+    const size_t n = std::min<size_t>(d.size(), (size_t)capacity - 1);
+    std::memcpy(buf, d.data(), n);
+    buf[n] = 0;
+  }
+  return (int64_t)d.size();
 }
 
 // ------------------------------------------------------------------ sort --

@@ -36,6 +36,9 @@ struct JoinTuning {
   // the slots outgrow L2, 0 never, 1 always; 2^partition_bits partitions
   int partition = -1;
   int partition_bits = 8;
+  // fields the environment set (the tuning table leaves them alone)
+  enum : uint32_t { FIX_DENSE = 1, FIX_PARTITION = 2, FIX_LOAD = 4 };
+  uint32_t fixed = 0;
 };
 
 std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,

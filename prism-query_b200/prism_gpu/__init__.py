@@ -145,6 +145,15 @@ def _declare(lib):
     lib.prism_arrow_packed_size.argtypes = [P, P, C.POINTER(C.c_uint64)]
     lib.prism_arrow_pack.argtypes = [P, P, P, C.c_uint64]
     lib.prism_arrow_unpack.argtypes = [P, C.c_uint64, P, P]
+    lib.prism_tune_join.argtypes = [P, P, P, P, P, i32, C.c_uint32, P]
+    lib.prism_tune_join_aggregate.argtypes = [P, P, i32, P, P, P, i32, P, i32, P, i32, P, P]
+    lib.prism_tune_hash_aggregate.argtypes = [P, P, i32, P, P]
+    lib.prism_tuning_save.argtypes = [C.c_char_p]
+    lib.prism_tuning_load.argtypes = [C.c_char_p]
+    lib.prism_tuning_clear.argtypes = []
+    lib.prism_tuning_clear.restype = None
+    lib.prism_tuning_dump.argtypes = [C.c_char_p, C.c_int64]
+    lib.prism_tuning_dump.restype = C.c_int64
     lib.prism_merge_partial_aggregates.argtypes = [P, P, i32, P, C.POINTER(P)]
     lib.prism_hash_join_arrow.argtypes = [P, P, P, P, P, P, P, P]
     lib.prism_hash_aggregate_arrow.argtypes = [P, P, P, P, P, P]
@@ -812,3 +821,66 @@ def join_aggregate(probe_batches, build_batch, probe_keys, build_keys, column_in
         )
     )
     return _result(ctx, h, as_device)
+
+
+# ------------------------------------------------------------- autotuner ----
+def tune_join(build_batch, probe_batch, build_keys: Sequence[int], probe_keys: Sequence[int], any_order: bool = False,
+              ctx: Optional[Context] = None) -> dict:
+    """Times the join table settings on this build / probe pair and records
+    the fastest for the build side's shape class (prism_tune_join)."""
+    ctx = ctx or default_context()
+    b, p = _dev(build_batch, ctx), _dev(probe_batch, ctx)
+    r = _abi.TuneResult()
+    ctx.check(lib().prism_tune_join(ctx.handle, b.handle, p.handle, _abi.int_array(build_keys), _abi.int_array(probe_keys),
+                                    len(build_keys), PRISM_JOIN_ANY_ORDER if any_order else 0, C.byref(r)))
+    return r.as_dict()
+
+
+def tune_join_aggregate(probe_batches, build_batch, probe_keys, build_keys, column_indices: Sequence[int],
+                        expressions: Sequence[ScalarExpr], agg: HashAggConfig, ctx: Optional[Context] = None) -> dict:
+    """Times the fused join -> aggregate kernel shapes on these inputs and
+    records the fastest for the build side's shape class."""
+    ctx = ctx or default_context()
+    ps = [_dev(b, ctx) for b in probe_batches]
+    b = _dev(build_batch, ctx)
+    cfg = agg.encode()
+    r = _abi.TuneResult()
+    ctx.check(lib().prism_tune_join_aggregate(
+        ctx.handle, _ptrs(ps), len(ps), b.handle, _abi.int_array(probe_keys), _abi.int_array(build_keys), len(probe_keys),
+        _abi.int_array(column_indices), len(column_indices), encode_exprs(expressions), len(expressions), C.byref(cfg),
+        C.byref(r)))
+    return r.as_dict()
+
+
+def tune_hash_aggregate(batches, config: HashAggConfig, ctx: Optional[Context] = None) -> dict:
+    """Times the hashed-groups kernel's block sizes on these batches and
+    records the fastest for their row-count class."""
+    ctx = ctx or default_context()
+    ds = [_dev(b, ctx) for b in batches]
+    cfg = config.encode()
+    r = _abi.TuneResult()
+    ctx.check(lib().prism_tune_hash_aggregate(ctx.handle, _ptrs(ds), len(ds), C.byref(cfg), C.byref(r)))
+    return r.as_dict()
+
+
+def tuning_save(path: str):
+    rc = lib().prism_tuning_save(path.encode())
+    if rc:
+        raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+
+
+def tuning_load(path: str):
+    rc = lib().prism_tuning_load(path.encode())
+    if rc:
+        raise PrismError(rc, (lib().prism_last_error(None) or b"").decode())
+
+
+def tuning_clear():
+    lib().prism_tuning_clear()
+
+
+def tuning_dump() -> str:
+    n = lib().prism_tuning_dump(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().prism_tuning_dump(buf, n + 1)
+    return buf.value.decode()

@@ -212,3 +212,17 @@ def int_array(values):
     values = list(values)
     arr = (C.c_int32 * max(1, len(values)))(*values)
     return arr
+
+
+TUNE_MAX = 16
+
+
+class TuneResult(C.Structure):
+    """prism_tune_result (include/prism_gpu.h)."""
+
+    _fields_ = [("n_candidates", C.c_int32), ("best", C.c_int32), ("ms", C.c_double * TUNE_MAX),
+                ("desc", (C.c_char * 64) * TUNE_MAX)]
+
+    def as_dict(self):
+        cands = [{"settings": self.desc[i].value.decode(), "ms": self.ms[i]} for i in range(self.n_candidates)]
+        return {"candidates": cands, "best": cands[self.best] if cands else None}
