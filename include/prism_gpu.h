@@ -603,6 +603,26 @@ int prism_server_add_table(prism_server* server, const prism_hash_table* table, 
 /* Submits a probe of table_id with n device-resident Int64 keys; the result
  * batch is [probe_idx (UInt32, rows of `keys`, ascending), payload]. */
 int prism_serve_probe(prism_server* server, int32_t table_id, const int64_t* keys, int64_t n, int64_t* ticket);
+/* The device work queue (no counterpart in the reference): with enable != 0,
+ * probes of registered tables with unique Int64 keys and a fixed-width,
+ * null-free payload, of at most max_rows rows (0: any), no longer go to the
+ * worker threads: their descriptors go into a ring in device memory, and ONE
+ * persistent kernel (ctas_per_sm CTAs per SM, 1 or 2; 0: 2) drains it tile
+ * by tile (2,048 probe rows), requests of different tables and sizes sharing
+ * the launch; a host thread reports each request when its last tile is done.
+ * Their matches come as a multiset: runs of consecutive probe rows in any
+ * order, rows ascending inside a run. Every wait of the kernel is bounded:
+ * idle CTAs exit after a few milliseconds (the kernel is relaunched when work
+ * arrives), and a CTA that waits wait_limit_ms (0: 1000) for a request's
+ * descriptor gives up, every request then in flight fails with
+ * PRISM_ERR_TIMEOUT, and the queue is reset and stays usable. enable = 0
+ * sends new probes back to the workers. */
+int prism_server_set_device_queue(prism_server* server, int32_t enable, int64_t max_rows, int32_t ctas_per_sm,
+                                  int32_t wait_limit_ms);
+/* Failure injection for tests of the bounded wait above: publishes a request
+ * whose descriptor is never written; its ticket (and every request in flight
+ * with it) fails with PRISM_ERR_TIMEOUT after wait_limit_ms. */
+int prism_server_inject_unready(prism_server* server, int64_t* ticket);
 /* Submits hash_aggregate(batch, config) (the config is copied). */
 int prism_serve_aggregate(prism_server* server, const prism_batch* batch, const prism_agg_config* config,
                           int64_t* ticket);

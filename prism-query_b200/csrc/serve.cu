@@ -35,6 +35,7 @@
 #include "join.hpp"
 #include "prims.hpp"
 #include "prism_gpu.h"
+#include "queue.hpp"
 #include "runtime.hpp"
 
 using namespace prism;
@@ -131,6 +132,14 @@ struct TableRef {
   const prism_hash_table* table;
   int32_t payload_col;  // build column emitted with the probe row
   bool coalesce;        // payload null-free and fixed width: results can be views
+  int queue_id = -1;    // index on the device queue, or -1
+};
+
+// a probe in flight on the device queue
+struct Queued {
+  Request req;
+  MemP prow, pay;
+  uint64_t footprint = 0;
 };
 
 }  // namespace
@@ -156,6 +165,14 @@ struct prism_server {
   uint64_t in_use = 0;
   bool closing = false, dispatcher_done = false;
   std::string last_error;
+  // the device work queue (prism_server_set_device_queue): eligible probes
+  // are drained by one persistent kernel; a host thread reports completions
+  prism_ctx* qctx = nullptr;
+  std::unique_ptr<DeviceQueue> queue;
+  int64_t queue_max_rows = 0;
+  std::map<int64_t, Queued> queued;  // queue seq -> request
+  std::thread qthread;
+  bool qstop = false;
 };
 
 namespace {
@@ -454,6 +471,122 @@ void work(prism_server* s, prism_ctx* w) {
   }
 }
 
+// Reports the device queue's finished requests: each result is a batch of
+// views into the request's own output buffers.
+void queue_loop(prism_server* s) {
+  cudaSetDevice(s->device);
+  int quiet = 0;
+  for (;;) {
+    int got = 0;
+    try {
+      got = s->queue->poll([&](int64_t seq, int status, int64_t matches) {
+        Queued q;
+        {
+          std::lock_guard<std::mutex> lk(s->mu);
+          auto it = s->queued.find(seq);
+          if (it == s->queued.end()) return;
+          q = std::move(it->second);
+          s->queued.erase(it);
+        }
+        prism_batch* out = nullptr;
+        std::string msg;
+        if (status == PRISM_OK) {
+          const TableRef& tb = s->tables[q.req.table];
+          const Column& pay = *tb.table->t->build.cols[tb.payload_col];
+          Batch b;
+          b.rows = matches;
+          auto c0 = std::make_shared<Column>();
+          c0->type = TY_U32;
+          c0->name = "probe_idx";
+          c0->nullable = false;
+          c0->length = matches;
+          c0->values = q.prow->ptr;
+          c0->owners = {q.prow};
+          auto c1 = std::make_shared<Column>();
+          c1->type = pay.type;
+          c1->name = pay.name;
+          c1->nullable = pay.nullable;
+          c1->precision = pay.precision;
+          c1->scale = pay.scale;
+          c1->length = matches;
+          c1->values = q.pay->ptr;
+          c1->owners = {q.pay};
+          b.cols = {c0, c1};
+          out = new prism_batch();
+          out->impl = std::move(b);
+          out->ctx = s->qctx;
+        } else {
+          msg = "device queue: a wait in the persistent kernel ran out";
+        }
+        finish(s, q.req, status, msg, out);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use -= q.footprint;
+        s->cv_admit.notify_all();
+      });
+    } catch (const Failure& f) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->last_error = f.msg;
+    }
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->qstop && s->queued.empty()) return;
+    }
+    if (got) {
+      quiet = 0;
+      continue;
+    }
+    // spin briefly after activity, then sleep in short steps
+    if (++quiet < 2000) std::this_thread::yield();
+    else std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+// Queues an eligible probe on the device queue (admission by the outputs'
+// footprint, outputs from the queue context's pool). Returns false when the
+// probe should take the worker path.
+bool queue_probe(prism_server* s, Request& r, int64_t* ticket) {
+  int qid;
+  int w;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->queue || s->closing || r.rows <= 0 || r.rows > s->queue_max_rows) return false;
+    qid = s->tables[r.table].queue_id;
+    if (qid < 0) return false;
+    const TableRef& tb = s->tables[r.table];
+    w = width_of(tb.table->t->build.cols[tb.payload_col]->type);
+  }
+  const uint64_t fp = (uint64_t)r.rows * (4 + (uint64_t)w) + 512;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_admit.wait(lk, [&] { return s->in_use == 0 || s->in_use + fp <= s->budget; });
+    s->in_use += fp;
+    r.ticket = s->next_ticket++;
+    s->results[r.ticket] = Result{};
+  }
+  Queued q;
+  try {
+    Ctx& x = s->qctx->impl;
+    {
+      std::lock_guard<std::recursive_mutex> lk(x.mu);
+      q.prow = x.alloc((size_t)r.rows * 4);
+      q.pay = x.alloc((size_t)r.rows * w);
+      x.sync();  // the outputs exist before the kernel may write them
+    }
+    q.req = r;
+    q.footprint = fp;
+    std::lock_guard<std::mutex> lk(s->mu);  // registered before its completion can be reported
+    const int64_t seq = s->queue->submit(qid, r.keys, r.rows, static_cast<uint32_t*>(q.prow->ptr), q.pay->ptr);
+    s->queued.emplace(seq, std::move(q));
+  } catch (const Failure& f) {
+    finish(s, r, f.code, f.msg, nullptr);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= fp;
+    s->cv_admit.notify_all();
+  }
+  *ticket = r.ticket;
+  return true;
+}
+
 std::string agg_shape(const prism_batch* b, const prism_agg_config* cfg) {
   if (cfg->n_group_by == 0) return "";  // a global aggregate must run alone (grouped semantics differ)
   std::string k = "agg";
@@ -520,7 +653,16 @@ int prism_server_add_table(prism_server* s, const prism_hash_table* table, int32
   const int w = width_of(p.type);
   const bool coalesce = !p.validity && (w == 4 || w == 8) && p.type != TY_DICT;
   std::lock_guard<std::mutex> lk(s->mu);
-  s->tables.push_back({table, payload_col, coalesce});
+  TableRef ref{table, payload_col, coalesce, -1};
+  if (s->queue && coalesce && table->t->int64_fast && !table->t->has_dups) {
+    try {
+      ref.queue_id = s->queue->add_table(*table->t, p);
+    } catch (const Failure& f) {
+      s->last_error = f.msg;
+      return f.code;
+    }
+  }
+  s->tables.push_back(ref);
   *table_id = (int32_t)s->tables.size() - 1;
   return PRISM_OK;
 }
@@ -542,7 +684,60 @@ int prism_serve_probe(prism_server* s, int32_t table_id, const int64_t* keys, in
   r.table = table_id;
   r.keys = keys;
   r.rows = n;
+  if (queue_probe(s, r, ticket)) return PRISM_OK;
   return submit(s, std::move(r), ticket);
+}
+
+int prism_server_set_device_queue(prism_server* s, int32_t enable, int64_t max_rows, int32_t ctas_per_sm,
+                                  int32_t wait_limit_ms) {
+  if (!s || max_rows < 0 || ctas_per_sm < 0 || wait_limit_ms < 0) return PRISM_ERR_INVALID_ARGUMENT;
+  if (!enable) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->queue_max_rows = 0;  // new probes take the worker path; the queue drains
+    return PRISM_OK;
+  }
+  try {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->queue) {
+      int rc = prism_ctx_create(s->device, 0, &s->qctx);
+      if (rc) fail(rc, "device queue context");
+      s->queue = std::make_unique<DeviceQueue>(s->qctx->impl, ctas_per_sm ? ctas_per_sm : 2,
+                                               (int64_t)(wait_limit_ms ? wait_limit_ms : 1000) * 1000);
+      for (auto& tb : s->tables)
+        if (tb.coalesce && tb.table->t->int64_fast && !tb.table->t->has_dups)
+          tb.queue_id = s->queue->add_table(*tb.table->t, *tb.table->t->build.cols[tb.payload_col]);
+      s->qthread = std::thread(queue_loop, s);
+    }
+    s->queue_max_rows = max_rows ? max_rows : (int64_t)UINT32_MAX - 1;
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    s->last_error = f.msg;
+    return f.code;
+  }
+}
+
+int prism_server_inject_unready(prism_server* s, int64_t* ticket) {
+  if (!s || !ticket) return PRISM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->queue) {
+    s->last_error = "the device queue is not enabled";
+    return PRISM_ERR_INVALID_ARGUMENT;
+  }
+  try {
+    Request r;
+    r.ticket = s->next_ticket++;
+    r.kind = 0;
+    s->results[r.ticket] = Result{};
+    Queued q;
+    q.req = r;
+    const int64_t seq = s->queue->submit_unready(1);
+    s->queued.emplace(seq, std::move(q));
+    *ticket = r.ticket;
+    return PRISM_OK;
+  } catch (const Failure& f) {
+    s->last_error = f.msg;
+    return f.code;
+  }
 }
 
 int prism_serve_aggregate(prism_server* s, const prism_batch* batch, const prism_agg_config* cfg, int64_t* ticket) {
@@ -616,6 +811,14 @@ void prism_server_destroy(prism_server* s) {
   }
   s->dispatcher.join();
   for (auto& t : s->threads) t.join();
+  if (s->queue) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->qstop = true;
+    }
+    s->qthread.join();  // after every queued request is reported
+    s->queue.reset();   // stops the persistent kernel
+  }
   for (auto& r : s->results)
     if (r.second.out) prism_batch_free(r.second.out);
   s->results.clear();
@@ -625,6 +828,10 @@ void prism_server_destroy(prism_server* s) {
   for (auto* c : s->ctxs) {
     cudaStreamSynchronize(c->impl.stream);
     cudaMemPoolTrimTo(c->impl.pool, 0);
+  }
+  if (s->qctx) {
+    cudaStreamSynchronize(s->qctx->impl.stream);
+    cudaMemPoolTrimTo(s->qctx->impl.pool, 0);
   }
   delete s;
 }

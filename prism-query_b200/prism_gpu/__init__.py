@@ -146,6 +146,8 @@ def _declare(lib):
     lib.prism_arrow_pack.argtypes = [P, P, P, C.c_uint64]
     lib.prism_arrow_unpack.argtypes = [P, C.c_uint64, P, P]
     lib.prism_tune_join.argtypes = [P, P, P, P, P, i32, C.c_uint32, P]
+    lib.prism_server_set_device_queue.argtypes = [P, i32, C.c_int64, i32, i32]
+    lib.prism_server_inject_unready.argtypes = [P, C.POINTER(C.c_int64)]
     lib.prism_tune_join_aggregate.argtypes = [P, P, i32, P, P, P, i32, P, i32, P, i32, P, P]
     lib.prism_tune_hash_aggregate.argtypes = [P, P, i32, P, P]
     lib.prism_tuning_save.argtypes = [C.c_char_p]

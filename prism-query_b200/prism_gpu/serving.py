@@ -61,7 +61,8 @@ class _Table:
 
 class Server:
     def __init__(self, device: int = 0, budget_bytes: int = 120 << 30, workers: int = 4,
-                 coalesce_rows: int = 1 << 18, max_coalesce: int = 64):
+                 coalesce_rows: int = 1 << 18, max_coalesce: int = 64, device_queue: bool = False,
+                 queue_max_rows: int = 0, queue_ctas_per_sm: int = 0, queue_wait_limit_ms: int = 0):
         import ctypes as C
 
         import torch
@@ -79,6 +80,12 @@ class Server:
         rc = self._lib.prism_server_create(device, budget_bytes, workers, coalesce_rows, max_coalesce, C.byref(self._h))
         if rc:
             self._raise(rc)
+        if device_queue:
+            # eligible probes drained by the persistent kernel (matches as a multiset)
+            rc = self._lib.prism_server_set_device_queue(self._h, 1, queue_max_rows, queue_ctas_per_sm,
+                                                         queue_wait_limit_ms)
+            if rc:
+                self._raise(rc)
         self.tables: Dict[str, int] = {}
         self._lock = threading.Lock()
         self._pending: Dict[int, tuple] = {}  # ticket -> (future, request, keepalive)
@@ -129,6 +136,21 @@ class Server:
                 rc = self._lib.prism_serve_aggregate(self._h, db.handle, C.byref(cfg), C.byref(ticket))
             if rc == 0:
                 self._pending[ticket.value] = (fut, req, keep)
+                self._submitted += 1
+        if rc:
+            self._raise(rc)
+        return fut
+
+    def inject_unready(self) -> cf.Future:
+        """Failure injection (tests): a queued request whose descriptor never
+        arrives; its future fails with Timeout once the kernel's wait runs out."""
+        C = self._C
+        fut: cf.Future = cf.Future()
+        ticket = C.c_int64(0)
+        with self._lock:
+            rc = self._lib.prism_server_inject_unready(self._h, C.byref(ticket))
+            if rc == 0:
+                self._pending[ticket.value] = (fut, None, None)
                 self._submitted += 1
         if rc:
             self._raise(rc)
