@@ -448,7 +448,7 @@ int prism_sort_batch(prism_ctx* ctx, const prism_batch* batch, const prism_sort_
 /* ------------------------------------------------------------------------ */
 /* Parquet scan (native/prism-executor/src/parquet_scan.rs)                 */
 /* ------------------------------------------------------------------------ */
-/* ParquetScanConfig (parquet_scan.rs:29-50), without target_schema. */
+/* ParquetScanConfig (parquet_scan.rs:29-50). */
 typedef struct prism_parquet_scan_config {
   const char* const* uris;        /* local paths or file:// URIs: a file, or a directory scanned for *.parquet */
   int32_t n_uris;
@@ -457,6 +457,16 @@ typedef struct prism_parquet_scan_config {
   int32_t n_projection;
   int64_t batch_size;             /* rows per output batch (> 0) */
   int32_t skip_expand;
+  /* target_schema (parquet_scan.rs:45-50, NULL: none): a struct schema. A
+   * scan without a projection adapts every batch to it (adapt_batch_to_schema,
+   * parquet_scan.rs:306-339): the target's fields in its order, matched by
+   * name; a column of another type cast as arrow's safe cast does (a value
+   * the target cannot hold becomes null; the GPU casts between numeric,
+   * Boolean and Date32 types, others fail with PRISM_ERR_INTERNAL); a missing
+   * column all null; a non-nullable field holding a null fails. With a
+   * projection the batches stay file-native and are expanded to the target
+   * schema instead of the first file's. */
+  const struct ArrowSchema* target_schema;
 } prism_parquet_scan_config;
 
 typedef struct prism_parquet_scan_stats {

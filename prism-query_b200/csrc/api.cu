@@ -1224,6 +1224,22 @@ static ParquetScanArgs scan_args(const prism_parquet_scan_config* cfg) {
     if (a.has_projection) a.projection.assign(cfg->projection, cfg->projection + cfg->n_projection);
     a.batch_size = cfg->batch_size;
     a.skip_expand = cfg->skip_expand != 0;
+    if (cfg->target_schema) {
+      // ParquetScanConfig.target_schema (parquet_scan.rs:45-50): a struct schema
+      const ArrowSchema* ts = cfg->target_schema;
+      if (!ts->format || std::string(ts->format) != "+s" || (ts->n_children > 0 && !ts->children))
+        fail(PRISM_ERR_INVALID_ARGUMENT, "target_schema must be a struct schema (format '+s')");
+      a.has_target = true;
+      for (int64_t i = 0; i < ts->n_children; ++i) {
+        const ArrowSchema* f = ts->children[i];
+        TargetField t;
+        t.name = f->name ? f->name : "";
+        t.nullable = (f->flags & ARROW_FLAG_NULLABLE) != 0;
+        if (f->dictionary || !arrow_format_type(f->format, t.type, t.precision, t.scale) || t.type == TY_NULL)
+          fail(PRISM_ERR_INVALID_ARGUMENT, "target_schema field '" + t.name + "' has a type the engine does not hold");
+        a.target.push_back(t);
+      }
+    }
     return a;
 }
 

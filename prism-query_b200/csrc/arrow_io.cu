@@ -759,6 +759,10 @@ void export_host_batch(const Batch& b, const std::shared_ptr<void>& hold, ArrowA
   a->private_data = ap;
 }
 
+bool arrow_format_type(const char* format, int32_t& type, int32_t& precision, int32_t& scale) {
+  return parse_format(format, type, precision, scale);
+}
+
 std::vector<HostView> host_view(const ArrowArray* a, const ArrowSchema* s) {
   if (!a || !s) fail(PRISM_ERR_INVALID_ARGUMENT, "null ArrowArray/ArrowSchema");
   if (!s->format || std::string(s->format) != "+s")

@@ -35,6 +35,10 @@ std::vector<HostView> host_view(const ArrowArray* a, const ArrowSchema* s);
 // back to the pool by the consumer's release callback).
 void export_host_columns(const std::vector<HostOutCol>& cols, int64_t rows, ArrowArray* a, ArrowSchema* s);
 
+// The engine type of an Arrow format string (TY_*; decimal precision /
+// scale for "d:p,s"); false when unsupported.
+bool arrow_format_type(const char* format, int32_t& type, int32_t& precision, int32_t& scale);
+
 // A host struct array as a Batch whose column pointers are HOST pointers
 // (no copy; bitmaps not starting on a byte boundary are realigned into
 // `keep`). For host-side code only (the packed exchange format on the host).

@@ -1497,6 +1497,205 @@ int64_t parquet_row_count(const std::vector<std::string>& uris, const prism_pred
   return total;
 }
 
+// ------------------------------------------------- target schema (casts) --
+// arrow_cast::cast with the default CastOptions { safe: true } between the
+// numeric, boolean and Date32 types: a value the target cannot hold becomes
+// null (integer range, float to integer out of range or NaN, truncating
+// toward zero otherwise), Float64 -> Float32 rounds, booleans are 0 / 1 and
+// a number casts to `value != 0`.
+namespace {
+
+__device__ __forceinline__ bool cast_is_float(int t) { return t == TY_F32 || t == TY_F64; }
+
+__device__ __forceinline__ void int_range(int t, long long& lo, unsigned long long& hi) {
+  switch (t) {
+    case TY_I8: lo = -128; hi = 127; break;
+    case TY_I16: lo = -32768; hi = 32767; break;
+    case TY_I32: case TY_DATE32: lo = -2147483648LL; hi = 2147483647ULL; break;
+    case TY_I64: lo = (long long)0x8000000000000000ULL; hi = 0x7FFFFFFFFFFFFFFFULL; break;
+    case TY_U8: lo = 0; hi = 255; break;
+    case TY_U16: lo = 0; hi = 65535; break;
+    case TY_U32: lo = 0; hi = 4294967295ULL; break;
+    default: lo = 0; hi = 0xFFFFFFFFFFFFFFFFULL; break;  // TY_U64
+  }
+}
+
+__device__ __forceinline__ void store_int(void* out, int t, int64_t i, unsigned long long v) {
+  switch (width_of(t)) {
+    case 1: static_cast<uint8_t*>(out)[i] = (uint8_t)v; break;
+    case 2: static_cast<uint16_t*>(out)[i] = (uint16_t)v; break;
+    case 4: static_cast<uint32_t*>(out)[i] = (uint32_t)v; break;
+    default: static_cast<unsigned long long*>(out)[i] = v; break;
+  }
+}
+
+// one thread per 32 rows (one validity word)
+__global__ void cast_column_kernel(DCol src, int32_t dst_type, void* out, uint32_t* out_valid, int64_t n) {
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w * 32 < n; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t word = 0;
+    for (int k = 0; k < 32; ++k) {
+      const int64_t i = w * 32 + k;
+      if (i >= n) break;
+      bool ok = dcol_valid(src, i);
+      // the source value as a double, or as a 64-bit integer with its sign
+      bool sf = cast_is_float(src.type);
+      double d = 0;
+      long long si = 0;
+      unsigned long long ui = 0;
+      bool neg = false;
+      if (ok) {
+        if (src.type == TY_F64) d = static_cast<const double*>(src.values)[i];
+        else if (src.type == TY_F32) d = (double)static_cast<const float*>(src.values)[i];
+        else if (src.type == TY_BOOL) ui = (static_cast<const uint8_t*>(src.values)[i >> 3] >> (i & 7)) & 1;
+        else if (src.type == TY_U64) ui = static_cast<const unsigned long long*>(src.values)[i];
+        else {
+          si = dcol_ival(src, i);
+          neg = si < 0;
+          ui = (unsigned long long)si;
+        }
+      }
+      if (ok) {
+        if (dst_type == TY_BOOL) {
+          const bool b = sf ? d != 0.0 : ui != 0;
+          if (b) atomicOr(reinterpret_cast<unsigned int*>(out) + (i >> 5), 1u << (i & 31));
+        } else if (cast_is_float(dst_type)) {
+          const double v = sf ? d : (neg ? (double)si : (double)ui);
+          if (dst_type == TY_F64) static_cast<double*>(out)[i] = v;
+          else static_cast<float*>(out)[i] = sf && src.type == TY_F32 ? static_cast<const float*>(src.values)[i]
+                                                                      : (float)(sf ? d : (neg ? (float)si : (float)ui));
+        } else {
+          long long lo;
+          unsigned long long hi;
+          int_range(dst_type, lo, hi);
+          if (sf) {
+            // truncate toward zero; out of range (or NaN) -> null
+            const double t = trunc(d);
+            const double flo = (double)lo, fhi_p1 = hi == 0xFFFFFFFFFFFFFFFFULL ? 18446744073709551616.0
+                                                    : hi == 0x7FFFFFFFFFFFFFFFULL ? 9223372036854775808.0
+                                                                                  : (double)hi + 1.0;
+            ok = t == t && t >= flo && t < fhi_p1;
+            if (ok) store_int(out, dst_type, i, t < 0 ? (unsigned long long)(long long)t : (unsigned long long)t);
+          } else if (neg) {
+            ok = si >= lo;
+            if (ok) store_int(out, dst_type, i, (unsigned long long)si);
+          } else {
+            ok = ui <= hi;
+            if (ok) store_int(out, dst_type, i, ui);
+          }
+        }
+      }
+      if (ok) word |= 1u << k;
+    }
+    out_valid[w] = word;
+  }
+}
+
+bool castable(int32_t from, int32_t to) {
+  auto num = [](int32_t t) {
+    return t == TY_BOOL || t == TY_I8 || t == TY_I16 || t == TY_I32 || t == TY_I64 || t == TY_U8 || t == TY_U16 ||
+           t == TY_U32 || t == TY_U64 || t == TY_F32 || t == TY_F64 || t == TY_DATE32;
+  };
+  if (!num(from) || !num(to)) return false;
+  // Date32 casts to and from the integers only (as arrow does)
+  if ((from == TY_DATE32 || to == TY_DATE32) && (from == TY_F32 || from == TY_F64 || to == TY_F32 ||
+                                                 to == TY_F64 || from == TY_BOOL || to == TY_BOOL))
+    return false;
+  return true;
+}
+
+std::string type_text(int32_t t) {
+  static const char* names[] = {"Null", "Boolean", "Int8", "Int16", "Int32", "Int64", "UInt8", "UInt16", "UInt32",
+                                "UInt64", "Float32", "Float64", "Date32", "Utf8", "Decimal128", "Dictionary"};
+  return t >= 0 && t < (int)(sizeof names / sizeof *names) ? names[t] : "type " + std::to_string(t);
+}
+
+__global__ void null_count_kernel(const uint32_t* valid, int64_t n, unsigned long long* out) {
+  unsigned long long c = 0;
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w * 32 < n; w += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t rem = n - w * 32;
+    const uint32_t m = rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
+    c += __popc(~valid[w] & m);
+  }
+  if (c) atomicAdd(out, c);
+}
+
+// nulls in the first n rows of a column (0 without a validity bitmap)
+int64_t count_nulls(Ctx& ctx, const Column& c, int64_t n) {
+  if (!c.validity || n == 0) return 0;
+  if (c.type == TY_NULL) return n;
+  MemP m;
+  unsigned long long* d = ctx.alloc_t<unsigned long long>(1, m);
+  PRISM_CUDA(cudaMemsetAsync(d, 0, 8, ctx.stream));
+  // bitmaps start at bit 0 and are padded to 32-bit words
+  null_count_kernel<<<grid_for(ctx, (n + 31) / 32, 256), 256, 0, ctx.stream>>>(reinterpret_cast<const uint32_t*>(c.validity), n, d);
+  ctx.check_launch("null_count_kernel");
+  unsigned long long h = 0;
+  PRISM_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.sync();
+  return (int64_t)h;
+}
+
+ColP cast_column(Ctx& ctx, const Column& src, const TargetField& f, int64_t n) {
+  if (!castable(src.type, f.type))
+    fail(PRISM_ERR_INTERNAL, "adapt_batch_to_schema: cannot cast column '" + f.name + "' from " + type_text(src.type) +
+                                 " to " + type_text(f.type) + " (the GPU scan casts between numeric, Boolean and Date32 types)");
+  auto c = std::make_shared<Column>();
+  c->type = f.type;
+  c->name = f.name;
+  c->nullable = f.nullable;
+  c->length = n;
+  const size_t words = (size_t)((n + 31) / 32 + 1);
+  MemP mv = ctx.alloc(words * 4);
+  c->validity = static_cast<uint8_t*>(mv->ptr);
+  c->owners.push_back(mv);
+  MemP vals = ctx.alloc(f.type == TY_BOOL ? words * 4 : (size_t)std::max<int64_t>(n, 1) * width_of(f.type));
+  PRISM_CUDA(cudaMemsetAsync(vals->ptr, 0, f.type == TY_BOOL ? words * 4 : (size_t)std::max<int64_t>(n, 1) * width_of(f.type),
+                             ctx.stream));
+  c->values = vals->ptr;
+  c->owners.push_back(vals);
+  if (n > 0) {
+    cast_column_kernel<<<grid_for(ctx, (n + 31) / 32, 256), 256, 0, ctx.stream>>>(src.view(), f.type, vals->ptr,
+                                                                                   reinterpret_cast<uint32_t*>(mv->ptr), n);
+    ctx.check_launch("cast_column_kernel");
+  }
+  return c;
+}
+
+// adapt_batch_to_schema (parquet_scan.rs:306-339): the target's fields in
+// its order, by name; a different type cast, a missing column all null; a
+// non-nullable field holding a null fails as RecordBatch::try_new does.
+Batch adapt_batch(Ctx& ctx, const Batch& b, const std::vector<TargetField>& target) {
+  Batch out;
+  out.rows = b.rows;
+  for (const TargetField& f : target) {
+    const Column* src = nullptr;
+    for (auto& c : b.cols)
+      if (c->name == f.name) {
+        src = c.get();
+        break;
+      }
+    ColP col;
+    if (!src) {
+      col = null_column(ctx, f.name, f.type, b.rows);
+      col->precision = f.precision;
+      col->scale = f.scale;
+    } else if (src->type == f.type && (f.type != TY_DEC128 || (src->precision == f.precision && src->scale == f.scale))) {
+      col = std::make_shared<Column>(*src);
+      col->name = f.name;
+      col->nullable = f.nullable;
+    } else {
+      col = cast_column(ctx, *src, f, b.rows);
+    }
+    if (!f.nullable && count_nulls(ctx, *col, b.rows) > 0)
+      fail(PRISM_ERR_INTERNAL, "adapt_batch_to_schema: Invalid argument error: Column '" + f.name +
+                                   "' is declared as non-nullable but contains null values");
+    out.cols.push_back(col);
+  }
+  return out;
+}
+
+}  // namespace
+
 struct ParquetPrepared {
   const Ctx* owner = nullptr;  // decodes run on the preparing context's stream (they share the inflate buffer)
   ParquetScanArgs args;
@@ -1608,8 +1807,24 @@ std::vector<Batch> parquet_decode(Ctx& ctx, const ParquetPrepared& P, ParquetSca
       }
     }
   }
-  // expand_projected_batches (parquet_scan.rs:471-526)
-  const std::vector<Leaf>& full = P.full;
+  // the target schema adapts full scans (with a projection the batches stay
+  // file-native, parquet_scan.rs:226-236)
+  if (args.has_target && !args.has_projection)
+    for (Batch& b : out) b = adapt_batch(ctx, b, args.target);
+  // expand_projected_batches (parquet_scan.rs:471-526) to the target schema
+  // when one is given, else to the first file's
+  std::vector<TargetField> full;
+  if (args.has_target) {
+    full = args.target;
+  } else {
+    for (const Leaf& l : P.full) {
+      TargetField f;
+      f.name = l.name;
+      f.type = arrow_type_of(l);
+      f.nullable = l.repetition != 0;
+      full.push_back(f);
+    }
+  }
   if (!args.skip_expand && args.has_projection && args.projection.size() < full.size()) {
     std::vector<int> proj_map(full.size(), -1);
     for (size_t bi = 0; bi < args.projection.size(); ++bi) {
@@ -1620,13 +1835,19 @@ std::vector<Batch> parquet_decode(Ctx& ctx, const ParquetPrepared& P, ParquetSca
       Batch e;
       e.rows = b.rows;
       for (size_t i = 0; i < full.size(); ++i) {
-        const int32_t ty = arrow_type_of(full[i]);
+        const int32_t ty = full[i].type;
         if (proj_map[i] >= 0) {
           if (proj_map[i] >= (int)b.cols.size())
             fail(PRISM_ERR_INTERNAL, "expand batch: projection index past the batch's columns");
           const ColP& src = b.cols[proj_map[i]];
           if (src->type != ty) fail(PRISM_ERR_INTERNAL, "expand batch: column types differ from the schema");
-          e.cols.push_back(src);
+          if (!full[i].nullable && count_nulls(ctx, *src, b.rows) > 0)
+            fail(PRISM_ERR_INTERNAL, "expand batch: Invalid argument error: Column '" + full[i].name +
+                                         "' is declared as non-nullable but contains null values");
+          auto c = std::make_shared<Column>(*src);  // the schema's field: its name and nullability
+          c->name = full[i].name;
+          c->nullable = full[i].nullable;
+          e.cols.push_back(c);
         } else {
           if (ty == TY_NULL)
             fail(PRISM_ERR_INVALID_ARGUMENT, "parquet: column '" + full[i].name + "' has a type the GPU decoder does not read");

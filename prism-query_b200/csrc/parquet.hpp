@@ -98,6 +98,14 @@ int32_t arrow_type_of(const Leaf& l);
 
 }  // namespace pq
 
+// A field of ParquetScanConfig.target_schema (parquet_scan.rs:45-50).
+struct TargetField {
+  std::string name;
+  int32_t type = TY_NULL;
+  bool nullable = true;
+  int32_t precision = 38, scale = 0;
+};
+
 struct ParquetScanArgs {
   std::vector<std::string> uris;
   const prism_predicate* predicate = nullptr;
@@ -105,6 +113,8 @@ struct ParquetScanArgs {
   std::vector<int32_t> projection;
   int64_t batch_size = 8192;
   bool skip_expand = false;
+  bool has_target = false;
+  std::vector<TargetField> target;
 };
 
 struct ParquetScanStats {

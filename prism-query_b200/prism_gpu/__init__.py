@@ -550,14 +550,17 @@ def _uri_array(uris: Sequence[str]):
     return arr, enc
 
 
-def _scan_config(uris, predicate, projection, batch_size, skip_expand):
+def _scan_config(uris, predicate, projection, batch_size, skip_expand, target_schema=None):
     arr, keep = _uri_array(uris)
     pred = predicate.encode() if predicate is not None else None
     proj = _abi.int_array(list(projection)) if projection is not None else None
+    ts = None
+    if target_schema is not None:  # exported through the C Data Interface (released with the config)
+        ts = _abi.ExportedSchema(target_schema)
     cfg = _abi.prism_parquet_scan_config(arr, len(keep), C.cast(C.pointer(pred), C.c_void_p) if pred is not None else None,
                                          proj, len(projection) if projection is not None else 0, batch_size,
-                                         1 if skip_expand else 0)
-    cfg._keep = (arr, keep, pred, proj)
+                                         1 if skip_expand else 0, C.cast(ts.schema_ptr, C.c_void_p) if ts else None)
+    cfg._keep = (arr, keep, pred, proj, ts)
     return cfg
 
 
@@ -574,12 +577,13 @@ def _stats_dict(st):
 
 def parquet_scan(uris: Sequence[str], predicate: Optional[Predicate] = None, projection: Optional[Sequence[int]] = None,
                  batch_size: int = 8192, skip_expand: bool = False, ctx: Optional[Context] = None, as_device=False,
-                 with_stats=False):
+                 with_stats=False, target_schema: Optional[pa.Schema] = None):
     """parquet_scan (parquet_scan.rs:55-168), decoded on the GPU: a list of
     batches (Arrow, or DeviceBatch with as_device); with_stats also returns
-    the scan's counters (files, row groups read / skipped, pages, bytes)."""
+    the scan's counters (files, row groups read / skipped, pages, bytes).
+    target_schema: ParquetScanConfig.target_schema (schema evolution)."""
     ctx = ctx or default_context()
-    cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand)
+    cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand, target_schema)
     out = C.POINTER(C.c_void_p)()
     n = C.c_int32(0)
     st = _abi.prism_parquet_scan_stats()
@@ -594,9 +598,9 @@ class ParquetPrepared:
 
     def __init__(self, uris: Sequence[str], predicate: Optional[Predicate] = None,
                  projection: Optional[Sequence[int]] = None, batch_size: int = 8192, skip_expand: bool = False,
-                 ctx: Optional[Context] = None):
+                 ctx: Optional[Context] = None, target_schema: Optional[pa.Schema] = None):
         self.ctx = ctx or default_context()
-        cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand)
+        cfg = _scan_config(uris, predicate, projection, batch_size, skip_expand, target_schema)
         h = C.c_void_p()
         st = _abi.prism_parquet_scan_stats()
         self.ctx.check(lib().prism_parquet_prepare(self.ctx.handle, C.byref(cfg), C.byref(h), C.byref(st)))

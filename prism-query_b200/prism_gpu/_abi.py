@@ -96,6 +96,25 @@ class ExportedBatch:
             pass
 
 
+class ExportedSchema:
+    """A pyarrow Schema exported through the C Data Interface (as a struct)."""
+
+    def __init__(self, schema: pa.Schema):
+        self.schema = ArrowSchema()
+        schema._export_to_c(C.addressof(self.schema))
+
+    @property
+    def schema_ptr(self):
+        return C.pointer(self.schema)
+
+    def __del__(self):
+        try:
+            if self.schema.release:
+                self.schema.release(C.pointer(self.schema))
+        except Exception:
+            pass
+
+
 def import_batch(array: ArrowArray, schema: ArrowSchema) -> pa.RecordBatch:
     """Moves an exported struct array (callee-produced) into pyarrow."""
     return pa.RecordBatch._import_from_c(C.addressof(array), C.addressof(schema))
@@ -141,6 +160,7 @@ class prism_parquet_scan_config(C.Structure):
         ("n_projection", C.c_int32),
         ("batch_size", C.c_int64),
         ("skip_expand", C.c_int32),
+        ("target_schema", C.c_void_p),
     ]
 
 

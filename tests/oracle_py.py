@@ -360,7 +360,80 @@ def row_group_might_match(pred, rg, schema_names) -> bool:
     return True
 
 
-def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, skip_expand: bool = False):
+_INT_RANGE = {pa.int8(): (-2**7, 2**7 - 1), pa.int16(): (-2**15, 2**15 - 1), pa.int32(): (-2**31, 2**31 - 1),
+              pa.int64(): (-2**63, 2**63 - 1), pa.uint8(): (0, 2**8 - 1), pa.uint16(): (0, 2**16 - 1),
+              pa.uint32(): (0, 2**32 - 1), pa.uint64(): (0, 2**64 - 1), pa.date32(): (-2**31, 2**31 - 1)}
+
+
+def cast_safe(arr: pa.Array, typ: pa.DataType) -> pa.Array:
+    """arrow_cast::cast with the default CastOptions { safe: true } (arrow-rs
+    57.3.0, restated) between numeric, Boolean and Date32 types: a value the
+    target cannot hold becomes null (integer range; a float truncated toward
+    zero, NaN or out of range -> null), Float64 -> Float32 rounds, Boolean
+    is 0 / 1, a number casts to Boolean as value != 0. Date32 casts to and
+    from the integers only."""
+    import numpy as np
+
+    if arr.type == typ:
+        return arr
+    src = arr.type
+    numeric = lambda t: pa.types.is_integer(t) or pa.types.is_floating(t) or pa.types.is_boolean(t) or t == pa.date32()  # noqa: E731
+    bad_date = (src == pa.date32() or typ == pa.date32()) and (
+        pa.types.is_floating(src) or pa.types.is_floating(typ) or pa.types.is_boolean(src) or pa.types.is_boolean(typ))
+    if not (numeric(src) and numeric(typ)) or bad_date:
+        raise OracleError(7, f"adapt_batch_to_schema: cannot cast from {src} to {typ}")
+    valid = np.asarray(arr.is_valid()) if arr.null_count else np.ones(len(arr), bool)
+    if pa.types.is_boolean(src):
+        vals = np.asarray(arr.fill_null(False).to_numpy(zero_copy_only=False)).astype(np.int64)
+        is_f = False
+    elif src == pa.date32():
+        vals = np.asarray(arr.cast(pa.int32()).fill_null(0).to_numpy(zero_copy_only=False)).astype(np.int64)
+        is_f = False
+    else:
+        vals = np.asarray(arr.fill_null(0).to_numpy(zero_copy_only=False))
+        is_f = pa.types.is_floating(src)
+    if pa.types.is_boolean(typ):
+        out = vals != 0
+        return pa.array(out, type=typ, mask=~valid)
+    if pa.types.is_floating(typ):
+        out = vals.astype(np.float64 if typ == pa.float64() else np.float32)
+        return pa.array(out, type=typ, mask=~valid)
+    lo, hi = _INT_RANGE[typ]
+    if is_f:
+        v = vals.astype(np.float64)
+        with np.errstate(invalid="ignore"):
+            t = np.trunc(v)
+            ok = ~np.isnan(t) & (t >= float(lo)) & (t < float(hi) + 1.0)
+        iv = [int(x) if k else 0 for x, k in zip(t.tolist(), ok.tolist())]
+    else:
+        iv = [int(x) for x in vals.tolist()]
+        ok = np.array([lo <= x <= hi for x in iv], dtype=bool) if len(iv) else np.zeros(0, bool)
+        iv = [x if k else 0 for x, k in zip(iv, ok.tolist())]
+    keep = valid & ok
+    if typ == pa.date32():
+        return pa.array(np.array(iv, dtype=np.int32), type=pa.int32(), mask=~keep).cast(pa.date32())
+    return pa.array(iv, type=typ, mask=~keep)
+
+
+def adapt_batch_to_schema(batch: pa.RecordBatch, target: pa.Schema) -> pa.RecordBatch:
+    """adapt_batch_to_schema (parquet_scan.rs:306-339): the target's fields in
+    its order, by name; another type cast (cast_safe), a missing column all
+    null; RecordBatch::try_new rejects nulls in a non-nullable field."""
+    cols = []
+    for f in target:
+        if f.name in batch.schema.names:
+            c = batch.column(batch.schema.get_field_index(f.name))
+            c = cast_safe(c, f.type)
+        else:
+            c = pa.nulls(batch.num_rows, f.type)
+        if not f.nullable and c.null_count:
+            raise OracleError(7, f"adapt_batch_to_schema: Column '{f.name}' is declared as non-nullable but contains null values")
+        cols.append(c)
+    return pa.RecordBatch.from_arrays(cols, schema=target)
+
+
+def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, skip_expand: bool = False,
+                 target_schema: pa.Schema = None):
     """parquet_scan (parquet_scan.rs:55-168) with pyarrow decoding each row group."""
     import pyarrow.parquet as pq
 
@@ -372,7 +445,7 @@ def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, 
         files += fs
     if not files:
         return []
-    full = pq.ParquetFile(files[0]).schema_arrow
+    full = target_schema if target_schema is not None else pq.ParquetFile(files[0]).schema_arrow
     out = []
     for f in files:
         pf = pq.ParquetFile(f)
@@ -385,7 +458,10 @@ def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, 
             for s in range(0, t.num_rows, batch_size):
                 piece = t.slice(s, batch_size).combine_chunks()
                 if piece.num_rows:
-                    out.append(piece.to_batches()[0])
+                    b = piece.to_batches()[0]
+                    if target_schema is not None and projection is None:  # full scans only (parquet_scan.rs:226-236)
+                        b = adapt_batch_to_schema(b, target_schema)
+                    out.append(b)
     if not skip_expand and projection is not None and len(projection) < len(full):
         pmap = {}
         for bi, oi in enumerate(projection):
@@ -396,7 +472,12 @@ def parquet_scan(uris, predicate=None, projection=None, batch_size: int = 8192, 
             arrays, fields = [], []
             for i, fld in enumerate(full):
                 if i in pmap:
-                    arrays.append(b.column(pmap[i]))
+                    c = b.column(pmap[i])
+                    if c.type != fld.type:
+                        raise OracleError(7, "expand batch: column types differ from the schema")
+                    if not fld.nullable and c.null_count:
+                        raise OracleError(7, f"expand batch: Column '{fld.name}' is declared as non-nullable but contains null values")
+                    arrays.append(c)
                     fields.append(fld)
                 else:
                     arrays.append(pa.nulls(b.num_rows, fld.type))

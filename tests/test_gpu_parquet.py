@@ -211,3 +211,63 @@ def test_long_snappy_streams(ctx, tmp_path, version):
     got, st = prism_gpu.parquet_scan([path], batch_size=1 << 20, ctx=ctx, with_stats=True)
     _same(got, oracle.parquet_scan([path], batch_size=1 << 20))
     assert st["inflated_bytes"] > 4 * 65536
+
+
+def _evolved_files(tmp_path):
+    """Two files of one table whose schema evolved: `id` widened from int32
+    to int64, `v` from float32 to float64, `name` dropped, `extra` added."""
+    rng = np.random.default_rng(77)
+    d = tmp_path / "evolved"
+    d.mkdir()
+    n1, n2 = 30_000, 25_000
+    t1 = pa.table({"id": pa.array(rng.integers(-2**31, 2**31 - 1, n1).astype(np.int32)),
+                   "name": pa.array([f"n{i % 113}" for i in range(n1)]),
+                   "v": pa.array(rng.standard_normal(n1).astype(np.float32), mask=rng.random(n1) < 0.1)})
+    big = rng.integers(-2**40, 2**40, n2)
+    big[::7] = rng.integers(-30_000, 30_000, len(big[::7]))
+    t2 = pa.table({"id": pa.array(big), "v": pa.array(rng.standard_normal(n2) * 1e6),
+                   "extra": pa.array(rng.integers(0, 10, n2).astype(np.int32), mask=rng.random(n2) < 0.3)})
+    pq.write_table(t1, d / "a.parquet", row_group_size=8_000)
+    pq.write_table(t2, d / "b.parquet", row_group_size=10_000)
+    return str(d)
+
+
+def test_target_schema_adapts_evolved_files(ctx, tmp_path):
+    """ParquetScanConfig.target_schema (parquet_scan.rs:45-50, 306-339): every
+    batch of a full scan comes out in the target's fields, order and types:
+    widening casts, a narrowing cast whose overflowing values become null,
+    float to integer (truncated; NaN / out of range -> null), a missing column
+    all null, an extra column dropped."""
+    d = _evolved_files(tmp_path)
+    target = pa.schema([pa.field("v", pa.float64()), pa.field("id", pa.int64(), nullable=False),
+                        pa.field("extra", pa.int64()), pa.field("missing", pa.date32()),
+                        pa.field("name", pa.utf8())])
+    got = prism_gpu.parquet_scan([d], batch_size=7_000, target_schema=target)
+    ref = oracle.parquet_scan([d], batch_size=7_000, target_schema=target)
+    _same(got, ref)
+    assert all(b.schema == target for b in got)
+    narrow = pa.schema([pa.field("id", pa.int16()), pa.field("v", pa.int32()), pa.field("extra", pa.bool_())])
+    got = prism_gpu.parquet_scan([d], batch_size=9_000, target_schema=narrow)
+    _same(got, oracle.parquet_scan([d], batch_size=9_000, target_schema=narrow))
+    assert sum(b.column(0).null_count for b in got) > 0  # overflowing ids became null
+
+
+def test_target_schema_errors_and_projection(ctx, tmp_path):
+    """A non-nullable target field that receives nulls fails (as
+    RecordBatch::try_new does), a cast outside the numeric types fails; with
+    a projection the batches stay file-native and expand to the target."""
+    d = _evolved_files(tmp_path)
+    with pytest.raises(prism_gpu.PrismError) as e:
+        prism_gpu.parquet_scan([d], target_schema=pa.schema([pa.field("extra", pa.int32(), nullable=False)]))
+    assert e.value.kind == "Internal"
+    with pytest.raises(oracle.OracleError):
+        oracle.parquet_scan([d], target_schema=pa.schema([pa.field("extra", pa.int32(), nullable=False)]))
+    with pytest.raises(prism_gpu.PrismError) as e:
+        prism_gpu.parquet_scan([d], target_schema=pa.schema([pa.field("name", pa.int32())]))
+    assert e.value.kind == "Internal"
+    f = os.path.join(d, "b.parquet")
+    target = pa.schema([pa.field("id", pa.int64()), pa.field("v", pa.float64()), pa.field("extra", pa.int32()),
+                        pa.field("later", pa.utf8())])
+    got = prism_gpu.parquet_scan([f], projection=[1], batch_size=6_000, target_schema=target)
+    _same(got, oracle.parquet_scan([f], projection=[1], batch_size=6_000, target_schema=target))
+    assert got[0].schema.names == ["id", "v", "extra", "later"]
