@@ -1184,6 +1184,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.jdrange = t.drange;
         a.jpk = jpk_dev[&b - &joined[0]];
         a.jbk = static_cast<const DCol*>(t.key_views_dev->ptr);
+        a.jkrec = t.key_records ? static_cast<const ulonglong2*>(t.key_records->ptr) : nullptr;
         a.jnkeys = (int)join->probe_keys.size();
         a.n_cols = (int)pg.cols.size();
         if (A.wide) fused_fail("a Float64 sum beyond the 192-bit window over a join");

@@ -93,6 +93,7 @@ struct AggArgs {
   uint64_t jdrange;
   const DCol* jpk;           // probe key column views
   const DCol* jbk;           // build key column views
+  const ulonglong2* jkrec;   // packed build keys (single Utf8 key), or null
   int32_t jnkeys;
   uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
   unsigned long long* gnew_count;  // length of gnew
@@ -750,12 +751,25 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
       const I idx = base + r * stride;
       if (cnt[r] == 1) rows[r] = E::fetch(cols, idx, (I)cand[r]);
     }
+    // packed build keys: every single-candidate row's key compared up front
+    // (the R record loads in flight together, beside the fetches above)
+    bool keq[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const I idx = base + r * stride;
+      keq[r] = !a.jfast && a.jkrec && cnt[r] == 1 ? join_rec_equal(a.jpk[0], idx, a.jkrec, cand[r]) : true;
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
       for (uint32_t j = 0; j < cnt[r]; ++j) {
         const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
-        if (!a.jfast && !join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b)) continue;
+        if (!a.jfast) {
+          const bool eq = cnt[r] == 1 && a.jkrec ? keq[r]
+                          : a.jkrec              ? join_rec_equal(a.jpk[0], idx, a.jkrec, b)
+                                                 : join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b);
+          if (!eq) continue;
+        }
         const I bidx = (I)b;
         const typename E::Row row = cnt[r] == 1 ? rows[r] : E::fetch(cols, idx, bidx);
         if (!E::keep(a, K, cols, idx, bidx, row)) continue;

@@ -71,6 +71,9 @@ JoinTuning join_tuning() {
     t.dense = d[0] == '1';
     t.fixed |= JoinTuning::FIX_DENSE;
   }
+  // PRISM_JOIN_KEY_RECORDS=0: Utf8 keys compared through the build column, not packed records
+  const char* kr = std::getenv("PRISM_JOIN_KEY_RECORDS");
+  if (kr && std::strcmp(kr, "0") == 0) t.key_records = false;
   const char* p = std::getenv("PRISM_JOIN_PARTITION");
   if (p && (std::strcmp(p, "0") == 0 || std::strcmp(p, "1") == 0)) {
     t.partition = p[0] - '0';

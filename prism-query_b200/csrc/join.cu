@@ -127,6 +127,32 @@ __global__ void gather_u32_kernel(const uint32_t* src, const uint32_t* idx, int6
     dst[i] = src[idx[i]];
 }
 
+// One 64-byte record per build row of a single Utf8 key column (see
+// join_device.cuh): length word (bit 63: null), then the raw bytes, zero
+// padded; a key longer than JOIN_KREC_MAX bytes sets *too_long (the caller
+// then drops the records).
+__global__ void pack_key_records_kernel(DCol c, int64_t n, ulonglong2* __restrict__ rec, uint32_t* too_long) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t* p;
+    int32_t len;
+    dcol_str(c, i, p, len);
+    if (len > JOIN_KREC_MAX) {
+      atomicOr(too_long, 1u);
+      continue;
+    }
+    uint64_t w[8];
+    w[0] = (uint64_t)(uint32_t)len | (dcol_valid(c, i) ? 0ULL : JOIN_KREC_NULL);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const int32_t o = 8 * k;
+      w[k + 1] = o < len ? str_word(p + o, len - o < 8 ? len - o : 8) : 0ULL;
+    }
+    ulonglong2* r = rec + (size_t)i * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] = make_ulonglong2(w[2 * k], w[2 * k + 1]);
+  }
+}
+
 // sorted_slot[i] starts a segment -> slots[slot].row = i (cnt unchanged)
 __global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulonglong2* slots) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -169,6 +195,7 @@ struct ProbeArgs {
   uint32_t* err;
   int any_order;  // tiles reserve their output by one atomicAdd on *total, no look-back
   int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
+  const ulonglong2* krec;  // packed build keys (single Utf8 key), or null
 };
 
 constexpr unsigned long long FLAG_A = 1ULL << 62;
@@ -316,10 +343,14 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         if (!VERIFY) {
           c[it] = DUPS ? cnt : 1u;
         } else if (cnt == 1) {
-          c[it] = join_rows_equal(a.pcols, a.bcols, a.nkeys, r, v[it]) ? 1u : 0u;
+          c[it] = (a.krec ? join_rec_equal(a.pcols[0], r, a.krec, v[it]) : join_rows_equal(a.pcols, a.bcols, a.nkeys, r, v[it]))
+                      ? 1u : 0u;
         } else {
           uint32_t m = 0;
-          for (uint32_t j = 0; j < cnt; ++j) m += join_rows_equal(a.pcols, a.bcols, a.nkeys, r, a.dup_rows[v[it] + j]) ? 1u : 0u;
+          for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t b = a.dup_rows[v[it] + j];
+            m += (a.krec ? join_rec_equal(a.pcols[0], r, a.krec, b) : join_rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) ? 1u : 0u;
+          }
           c[it] = m;
         }
       }
@@ -369,7 +400,9 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         } else {
           for (uint32_t j = 0; j < cand[it] && pos < a.out_capacity; ++j) {
             uint32_t b = a.dup_rows[v[it] + j];
-            if (VERIFY && !join_rows_equal(a.pcols, a.bcols, a.nkeys, r, b)) continue;
+            if (VERIFY && !(a.krec ? join_rec_equal(a.pcols[0], r, a.krec, b)
+                                   : join_rows_equal(a.pcols, a.bcols, a.nkeys, r, b)))
+              continue;
             emit_one(a, pos++, r, b);
           }
         }
@@ -844,9 +877,23 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
     }
     ctx.check_launch("insert_kernel");
   }
-  uint32_t hdup = 0;
+  // packed build keys for a single Utf8 key column
+  MemP mlong, mrec;
+  uint32_t* too_long = nullptr;
+  if (tune.key_records && keys.size() == 1 && build.cols[keys[0]]->type == TY_UTF8 && n > 0) {
+    too_long = ctx.alloc_t<uint32_t>(1, mlong);
+    PRISM_CUDA(cudaMemsetAsync(too_long, 0, 4, ctx.stream));
+    mrec = ctx.alloc((size_t)n * 64);
+    KernelTimer kt(ctx, "pack_key_records_kernel");
+    pack_key_records_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(
+        t->key_views[0], n, static_cast<ulonglong2*>(mrec->ptr), too_long);
+    ctx.check_launch("pack_key_records_kernel");
+  }
+  uint32_t hdup = 0, hlong = 0;
   PRISM_CUDA(cudaMemcpyAsync(&hdup, dupflag, 4, cudaMemcpyDeviceToHost, ctx.stream));
+  if (too_long) PRISM_CUDA(cudaMemcpyAsync(&hlong, too_long, 4, cudaMemcpyDeviceToHost, ctx.stream));
   uint32_t derr = ctx.take_device_errors();
+  if (too_long && !hlong) t->key_records = mrec;
   if (derr & DERR_TABLE_FULL) fail(PRISM_ERR_TABLE_FULL, "join hash table full");
   t->has_dups = hdup != 0;
   if (t->has_dups) {
@@ -900,6 +947,7 @@ static void fill_common(Ctx& ctx, const JoinTable& t, const Batch& probe, const 
   a.mask = t.capacity - 1;
   a.cap = t.capacity;
   a.dup_rows = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+  a.krec = t.key_records ? static_cast<const ulonglong2*>(t.key_records->ptr) : nullptr;
   a.nkeys = (int)keys.size();
   a.err = ctx.d_err;
   a.bcols = static_cast<const DCol*>(t.key_views_dev->ptr);

@@ -26,6 +26,9 @@ struct JoinTable {
   int64_t n_dup_rows = 0;
   std::vector<DCol> key_views;
   MemP key_views_dev;
+  // packed build keys (single Utf8 key of at most JOIN_KREC_MAX bytes per
+  // row): 64-byte records per build row, see join_device.cuh
+  MemP key_records;
 };
 
 struct JoinTuning {
@@ -36,6 +39,7 @@ struct JoinTuning {
   // the slots outgrow L2, 0 never, 1 always; 2^partition_bits partitions
   int partition = -1;
   int partition_bits = 8;
+  bool key_records = true;  // packed build keys for a single Utf8 key column
   // fields the environment set (the tuning table leaves them alone)
   enum : uint32_t { FIX_DENSE = 1, FIX_PARTITION = 2, FIX_LOAD = 4 };
   uint32_t fixed = 0;

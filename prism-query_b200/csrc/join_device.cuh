@@ -91,4 +91,40 @@ __device__ __forceinline__ bool join_rows_equal(const DCol* pc, const DCol* bc, 
   return true;
 }
 
+// Packed build keys of a single Utf8 key column: one 64-byte record per
+// build row, word 0 = the key's byte length, bit 63 set for a null key, and
+// words 1..7 its raw bytes zero-padded (keys of at most 56 bytes; longer
+// ones keep the column). A probe compares against one aligned record (its
+// first 32 bytes unless the key is longer than 24 bytes) instead of the
+// build offsets and then the bytes they point to: one dependent load less.
+// The comparison is keys_equal's (hash_join.rs:628-670): null flags agree
+// and the raw bytes are equal.
+constexpr uint64_t JOIN_KREC_NULL = 1ULL << 63;
+constexpr int JOIN_KREC_MAX = 56;
+
+__device__ __forceinline__ bool join_rec_equal(const DCol& pc, int64_t pr, const ulonglong2* __restrict__ rec,
+                                               uint32_t row) {
+  const ulonglong2* r = rec + (size_t)row * 4;
+  const ulonglong2 h0 = __ldg(r), h1 = __ldg(r + 1);
+  const uint8_t* p;
+  int32_t n;
+  dcol_str(pc, pr, p, n);
+  const uint64_t want = (uint64_t)(uint32_t)n | (dcol_valid(pc, pr) ? 0ULL : JOIN_KREC_NULL);
+  if (want != h0.x) return false;
+  uint64_t w[7] = {h0.y, h1.x, h1.y, 0, 0, 0, 0};
+  if (n > 24) {
+    const ulonglong2 h2 = __ldg(r + 2), h3 = __ldg(r + 3);
+    w[3] = h2.x;
+    w[4] = h2.y;
+    w[5] = h3.x;
+    w[6] = h3.y;
+  }
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const int32_t i = 8 * k;
+    if (i < n && str_word(p + i, n - i < 8 ? n - i : 8) != w[k]) return false;
+  }
+  return true;
+}
+
 }  // namespace prism

@@ -284,3 +284,36 @@ def test_join_project_arrow_other_inputs_take_one_pass(ctx):
     assert table.join_project_arrow(probe, [0], oc).equals(table.join_project(probe, [0], oc))
     empty = probe.slice(0, 0)
     assert table.join_project_arrow(empty, [0], oc).num_rows == 0
+
+
+@pytest.mark.parametrize("records", ["1", "0"])
+@pytest.mark.parametrize("case", ["short", "long", "dup_nulls"])
+def test_utf8_keys_packed_records_and_column_compare(ctx, records, case, monkeypatch):
+    """Single Utf8 join keys compared through the packed 64-byte build key
+    records (keys of at most 56 bytes) or through the build column
+    (PRISM_JOIN_KEY_RECORDS=0, or a longer key anywhere): the same joins and
+    join -> aggregates as the oracle, with empty strings, nulls (matched by
+    keys_equal's null-flag rule) and repeated build keys."""
+    monkeypatch.setenv("PRISM_JOIN_KEY_RECORDS", records)
+    rng = np.random.default_rng(81)
+    nb = 6000
+    if case == "long":
+        words = [f"k{i}" + "L" * (60 if i == 17 else i % 50) for i in range(nb)]  # one key of 62 bytes
+    else:
+        words = [("" if i == 0 else f"k{i:05d}" + "s" * (i % 48)) for i in range(nb)]
+    bidx = rng.integers(0, nb, nb) if case == "dup_nulls" else rng.permutation(nb)
+    bmask = (rng.random(nb) < 0.05) if case == "dup_nulls" else None
+    build = pa.RecordBatch.from_arrays([pa.array([words[i] for i in bidx], mask=bmask),
+                                        pa.array(rng.integers(0, 25, nb).astype(np.int32))], names=["k", "g"])
+    pidx = rng.integers(0, nb + 500, 50_000)
+    pw = [words[i] if i < nb else f"miss{i}" for i in pidx]
+    pmask = (rng.random(50_000) < 0.03) if case == "dup_nulls" else None
+    probe = pa.RecordBatch.from_arrays([pa.array(pw, mask=pmask), pa.array(rng.lognormal(3, 1, 50_000))],
+                                       names=["k", "amount"])
+    for jt in (JoinType.Inner, JoinType.Left, JoinType.LeftSemi):
+        cfg = HashJoinConfig(jt, build_keys=[0], probe_keys=[0])
+        assert_batches_equal(prism_gpu.hash_join(probe, build, cfg), oracle.hash_join(probe, build, cfg))
+    agg = prism_gpu.HashAggConfig([0], [prism_gpu.AggExpr(1, prism_gpu.AggFunc.Sum, "s"),
+                                        prism_gpu.AggExpr(1, prism_gpu.AggFunc.Count, "n")])
+    got = prism_gpu.join_aggregate([probe], build, [0], [0], [3, 1], [], agg)
+    assert_batches_equal(got, oracle.join_aggregate([probe], build, [0], [0], [3, 1], [], agg), float_cols=(1,))
