@@ -1074,7 +1074,7 @@ int prism_tune_join(prism_ctx* c, const prism_batch* build, const prism_batch* p
     if (shape.key_kind == 0) cand.push_back(mk(true, 0.5, 0, 8));
     for (double lf : {0.5, 0.7}) {
       cand.push_back(mk(false, lf, 0, 8));
-      if (shape.key_kind == 0 && any) {
+      if (shape.key_kind == 1 || any) {  // general keys: the partitioned build alone
         cand.push_back(mk(false, lf, 1, 8));
         cand.push_back(mk(false, lf, 1, 6));
       }

@@ -42,13 +42,24 @@ struct KeysGeneral {
   int n;
   __device__ __forceinline__ uint64_t key(int64_t r) const { return join_key_hash(cols, n, r); }
 };
+// row hashes computed beforehand (the radix-partitioned build of general keys)
+struct KeysHashed {
+  static constexpr bool kFast = false;
+  const uint64_t* h;
+  __device__ __forceinline__ uint64_t key(int64_t r) const { return __ldg(h + r); }
+};
+
+__global__ void row_hash_kernel(const DCol* cols, int n, int64_t rows, uint64_t* __restrict__ h) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x)
+    h[i] = join_key_hash(cols, n, i);
+}
 
 // The radix-partitioned build and probe (single Int64 key, hash slots): on
 // when the tuning asks for it, or by default (partition < 0) once the slots
 // outgrow L2 — then a stretch of tiles in partition order touches one
 // 1/2^bits slice of the table, which stays in L2.
 bool use_partitioned(const Ctx& ctx, const JoinTable& t, const JoinTuning& tune) {
-  if (t.dense || !t.int64_fast || t.capacity == 0) return false;
+  if (t.dense || t.capacity == 0) return false;
   if (tune.partition >= 0) return tune.partition > 0;
   return (t.capacity + 1) * sizeof(ulonglong2) > (uint64_t)ctx.l2_bytes;
 }
@@ -852,19 +863,33 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   uint64_t mask = cap - 1;
   if (n > 0) {
     int g = grid_for(ctx, n, 256, 16);
-    if (t->int64_fast && use_partitioned(ctx, *t, tune)) {
-      // radix-partitioned build: the keys in the order of the top bits of
-      // their slot hash, so the inserts of a stretch of CTAs hit one slice
-      // of the table (in L2) instead of the whole table at random
+    if (use_partitioned(ctx, *t, tune)) {
+      // radix-partitioned build: the keys (general keys: their row hashes)
+      // in the order of the top bits of their slot hash, so the inserts of a
+      // stretch of CTAs hit one slice of the table (in L2) instead of the
+      // whole table at random
       const int bits = partition_bits(*t, tune);
-      MemP mk, mr;
+      MemP mk, mr, mh;
       uint64_t* kpart = ctx.alloc_t<uint64_t>((size_t)n, mk);
       uint32_t* rpart = ctx.alloc_t<uint32_t>((size_t)n, mr);
-      radix_partition(ctx, static_cast<const uint64_t*>(build.cols[keys[0]]->values), n, JOIN_FIB, 64 - bits, bits,
-                      kpart, rpart, "build_partition_hist_kernel", "build_partition_scatter_kernel");
+      const uint64_t* src = static_cast<const uint64_t*>(build.cols[keys[0]]->values);
+      if (!t->int64_fast) {
+        uint64_t* h = ctx.alloc_t<uint64_t>((size_t)n, mh);
+        row_hash_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(
+            static_cast<const DCol*>(t->key_views_dev->ptr), (int)keys.size(), n, h);
+        ctx.check_launch("row_hash_kernel");
+        src = h;
+      }
+      radix_partition(ctx, src, n, JOIN_FIB, 64 - bits, bits, kpart, rpart, "build_partition_hist_kernel",
+                      "build_partition_scatter_kernel");
       KernelTimer kt(ctx, "insert_kernel");
-      KeysFast kf{reinterpret_cast<const int64_t*>(kpart)};
-      insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err, rpart);
+      if (t->int64_fast) {
+        KeysFast kf{reinterpret_cast<const int64_t*>(kpart)};
+        insert_kernel<<<g, 256, 0, ctx.stream>>>(kf, n, slots, shift, mask, cap, dupflag, ctx.d_err, rpart);
+      } else {
+        KeysHashed kh{kpart};
+        insert_kernel<<<g, 256, 0, ctx.stream>>>(kh, n, slots, shift, mask, cap, dupflag, ctx.d_err, rpart);
+      }
     } else {
       KernelTimer kt(ctx, "insert_kernel");
       if (t->int64_fast) {

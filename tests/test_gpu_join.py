@@ -286,7 +286,7 @@ def test_join_project_arrow_other_inputs_take_one_pass(ctx):
     assert table.join_project_arrow(empty, [0], oc).num_rows == 0
 
 
-@pytest.mark.parametrize("records", ["1", "0"])
+@pytest.mark.parametrize("records", ["1", "0", "1p"])
 @pytest.mark.parametrize("case", ["short", "long", "dup_nulls"])
 def test_utf8_keys_packed_records_and_column_compare(ctx, records, case, monkeypatch):
     """Single Utf8 join keys compared through the packed 64-byte build key
@@ -294,7 +294,9 @@ def test_utf8_keys_packed_records_and_column_compare(ctx, records, case, monkeyp
     (PRISM_JOIN_KEY_RECORDS=0, or a longer key anywhere): the same joins and
     join -> aggregates as the oracle, with empty strings, nulls (matched by
     keys_equal's null-flag rule) and repeated build keys."""
-    monkeypatch.setenv("PRISM_JOIN_KEY_RECORDS", records)
+    monkeypatch.setenv("PRISM_JOIN_KEY_RECORDS", records[0])
+    # "1p": the radix-partitioned build (row hashes partitioned, then inserted)
+    monkeypatch.setenv("PRISM_JOIN_PARTITION", "1" if records == "1p" else "0")
     rng = np.random.default_rng(81)
     nb = 6000
     if case == "long":
