@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--partition", choices=["auto", "on", "off"], default="auto",
                     help="c2 with --join-table hash: the radix-partitioned build and probe (auto: once the hash slots "
                          "outgrow L2)")
+    ap.add_argument("--tune", action="store_true",
+                    help="c2 / c4 / c1: run the autotuner on the workload's own inputs first; the timed steps use "
+                         "its recorded choice (reported under config.tuning)")
     ap.add_argument("--ordered", action="store_true",
                     help="c2: emit matches in the reference's probe order (default: as a multiset, one-pass probe)")
     ap.add_argument("--scale", type=float, default=1.0,
@@ -267,6 +270,9 @@ def main():
         t.free()
         return m
 
+    tuning = None
+    if args.tune:
+        tuning = prism_gpu.tune_join(build_db, probe_db, [0], [0], any_order=any_order, ctx=ctx)
     for _ in range(max(3, args.warmup)):
         matches = step()
     expected = int((pk < N_BUILD).sum().item())
@@ -361,6 +367,7 @@ def main():
                 "order": "any (matches as a multiset)" if any_order else "probe order (the reference's)",
                 "matches_per_step": matches,
                 "check": check,
+                "tuning": tuning,
                 "l2": "inputs larger than L2 (1.76 GB per step), no flush",
                 "parallelism": f"replicated build, probe sharded (weak) x{world}",
             },
@@ -461,6 +468,9 @@ class C1:
     def step(self):
         out = self.pg.hash_aggregate(self.batch, self.cfg, ctx=self.ctx, as_device=True)
         out.free()
+
+    def tune(self):
+        return self.pg.tune_hash_aggregate([self.batch], self.cfg, ctx=self.ctx)
 
     def host_batch(self):
         import pyarrow as pa
@@ -697,6 +707,9 @@ class C4:
     def run(self, probes, build, **kw):
         return self.pg.join_aggregate(probes, build, [0], [0], self.cols, [], self.agg, ctx=self.ctx, **kw)
 
+    def tune(self):
+        return self.pg.tune_join_aggregate(self.batches, self.build, [0], [0], self.cols, [], self.agg, ctx=self.ctx)
+
     def step(self):
         out = self.run(self.batches, self.build, as_device=True)
         out.free()
@@ -709,7 +722,8 @@ class C4:
                 "full_size_check": "COUNT total == probe rows drawn from build keys"}
 
     def roofline(self, kstats):
-        names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit",
+        names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "pack_key_records_kernel",
+                 "build_partition_hist_kernel", "build_partition_scatter_kernel", "agg_kernel", "agg_tiny_jit",
                  "agg_hash_jit", "join_agg_jit")
         ms = sum(kstats.get(k, (0, 0.0))[1] for k in names)
         steps = max(1, kstats.get("insert_kernel", (1, 0.0))[0])
@@ -992,9 +1006,12 @@ def run_workload(args, rank, world, local, torch, dist):
     ctx.set_stream(stream.cuda_stream)
     W = Wc(torch, device, ctx, rank)
     torch.cuda.synchronize()
+    tuning = W.tune() if args.tune and hasattr(W, "tune") else None
     for _ in range(max(3, args.warmup)):
         W.step()
     extra = {} if args.no_check else W.check()
+    if tuning is not None:
+        extra["tuning"] = tuning
     flush = torch.empty(256 * 1024 * 1024 // 4, device=device, dtype=torch.float32) if W.flush_l2 else None
 
     ctx.set_profiling(True)
@@ -1016,7 +1033,8 @@ def run_workload(args, rank, world, local, torch, dist):
             dist.barrier()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
-    names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
+    names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "pack_key_records_kernel",
+             "build_partition_hist_kernel", "build_partition_scatter_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
              "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel", "select_hist_kernel",
              "pq_snappy_kernel", "pq_page_kernel", "pq_copy_kernel", "pq_dict_kernel", "pq_positions_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}
