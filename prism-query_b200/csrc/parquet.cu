@@ -1609,12 +1609,14 @@ std::string type_text(int32_t t) {
   return t >= 0 && t < (int)(sizeof names / sizeof *names) ? names[t] : "type " + std::to_string(t);
 }
 
-__global__ void null_count_kernel(const uint32_t* valid, int64_t n, unsigned long long* out) {
+// byte loads: a batch sliced off a row group points its bitmap at any byte
+// (only a byte boundary is guaranteed), so no wider loads
+__global__ void null_count_kernel(const uint8_t* valid, int64_t n, unsigned long long* out) {
   unsigned long long c = 0;
-  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w * 32 < n; w += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t rem = n - w * 32;
-    const uint32_t m = rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
-    c += __popc(~valid[w] & m);
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b * 8 < n; b += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t rem = n - b * 8;
+    const uint32_t m = rem >= 8 ? 0xFFu : ((1u << rem) - 1u);
+    c += __popc(~(uint32_t)valid[b] & m);
   }
   if (c) atomicAdd(out, c);
 }
@@ -1626,8 +1628,8 @@ int64_t count_nulls(Ctx& ctx, const Column& c, int64_t n) {
   MemP m;
   unsigned long long* d = ctx.alloc_t<unsigned long long>(1, m);
   PRISM_CUDA(cudaMemsetAsync(d, 0, 8, ctx.stream));
-  // bitmaps start at bit 0 and are padded to 32-bit words
-  null_count_kernel<<<grid_for(ctx, (n + 31) / 32, 256), 256, 0, ctx.stream>>>(reinterpret_cast<const uint32_t*>(c.validity), n, d);
+  // bitmaps start at bit 0 of their first byte
+  null_count_kernel<<<grid_for(ctx, (n + 7) / 8, 256), 256, 0, ctx.stream>>>(c.validity, n, d);
   ctx.check_launch("null_count_kernel");
   unsigned long long h = 0;
   PRISM_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, ctx.stream));
