@@ -551,12 +551,33 @@ __global__ void fill_u32_kernel(uint32_t* p, uint64_t n, uint32_t v) {
     p[i] = v;
 }
 
-// dense insert: dense[key - dmin] = row; a second row for a key sets *dup
-__global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n, int64_t dmin, uint32_t* dense,
-                                    uint32_t* dup) {
+// The key range the min / max kernel found, or ~0 when it is cap or wider.
+__device__ __forceinline__ uint64_t dense_range(const long long* mm, uint64_t cap) {
+  const uint64_t diff = (uint64_t)mm[1] - (uint64_t)mm[0];  // max >= min: the build has rows
+  return diff < cap ? diff + 1 : ~0ULL;
+}
+
+// NO_MATCH over the first `range` entries (nothing when the range is too wide)
+__global__ void fill_dense_kernel(uint32_t* dense, uint64_t cap, const long long* mm) {
+  const uint64_t r = dense_range(mm, cap);
+  if (r == ~0ULL) return;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < r; i += (uint64_t)gridDim.x * blockDim.x)
+    dense[i] = NO_MATCH;
+}
+
+// dense insert: dense[key - min] = row; a second row for a key sets flag 1,
+// a range of cap or more sets flag 2 (no insert)
+__global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n, const long long* mm, uint64_t cap,
+                                    uint32_t* dense, uint32_t* flag) {
+  const uint64_t r = dense_range(mm, cap);
+  if (r == ~0ULL) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flag, 2u);
+    return;
+  }
+  const uint64_t dmin = (uint64_t)mm[0];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t d = (uint64_t)__ldg(keys + i) - (uint64_t)dmin;
-    if (atomicCAS(dense + d, NO_MATCH, (uint32_t)i) != NO_MATCH) atomicOr(dup, 1u);
+    uint64_t d = (uint64_t)__ldg(keys + i) - dmin;
+    if (atomicCAS(dense + d, NO_MATCH, (uint32_t)i) != NO_MATCH) atomicOr(flag, 1u);
   }
 }
 
@@ -823,42 +844,40 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
     // hash slots (4 bytes per value of the range instead of 16 per slot at
     // load factor 0.5, and one dependent load per probe)
     const int64_t* bk = static_cast<const int64_t*>(build.cols[keys[0]]->values);
-    MemP mmm;
+    // one host synchronisation: the array is sized for the widest range the
+    // dense mode takes; the fill and the inserts read the range the min / max
+    // kernel left on the device, and give up (flag 2) when it is wider
+    const uint64_t dcap = (uint64_t)std::min<int64_t>(2 * n + 4096, (int64_t)1 << 28);
+    MemP mmm, mdf;
     long long* mm = ctx.alloc_t<long long>(2, mmm);
+    uint32_t* df = ctx.alloc_t<uint32_t>(1, mdf);
     const long long init[2] = {0x7fffffffffffffffLL, (long long)0x8000000000000000ULL};
     PRISM_CUDA(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, ctx.stream));
+    PRISM_CUDA(cudaMemsetAsync(df, 0, 4, ctx.stream));
     minmax_i64_kernel<<<grid_for(ctx, n, 256, 8), 256, 0, ctx.stream>>>(bk, n, mm);
     ctx.check_launch("minmax_i64_kernel");
-    long long h[2];
-    PRISM_CUDA(cudaMemcpyAsync(h, mm, 16, cudaMemcpyDeviceToHost, ctx.stream));
-    PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
-    unsigned __int128 range = (unsigned __int128)((__int128)h[1] - (__int128)h[0]) + 1;
-    if (range <= (unsigned __int128)(2 * n + 4096) && range <= ((unsigned __int128)1 << 28)) {
-      uint64_t r = (uint64_t)range;
-      MemP dense = ctx.alloc(r * 4);
-      uint32_t* dr = static_cast<uint32_t*>(dense->ptr);
-      fill_u32_kernel<<<grid_for(ctx, (int64_t)r, 256, 8), 256, 0, ctx.stream>>>(dr, r, NO_MATCH);
-      ctx.check_launch("fill_u32_kernel");
-      MemP mdf;
-      uint32_t* df = ctx.alloc_t<uint32_t>(1, mdf);
-      PRISM_CUDA(cudaMemsetAsync(df, 0, 4, ctx.stream));
-      {
-        KernelTimer kt(ctx, "insert_kernel");
-        dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, h[0], dr, df);
-      }
-      ctx.check_launch("dense_insert_kernel");
-      uint32_t hdf = 0;
-      PRISM_CUDA(cudaMemcpyAsync(&hdf, df, 4, cudaMemcpyDeviceToHost, ctx.stream));
-      PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
-      if (!hdf) {
-        t->dense = true;
-        t->dmin = h[0];
-        t->drange = r;
-        t->dense_rows = dense;
-        return t;
-      }
-      // a repeated key: the hash table below keeps every row
+    MemP dense = ctx.alloc(dcap * 4);
+    uint32_t* dr = static_cast<uint32_t*>(dense->ptr);
+    fill_dense_kernel<<<grid_for(ctx, (int64_t)dcap, 256, 8), 256, 0, ctx.stream>>>(dr, dcap, mm);
+    ctx.check_launch("fill_dense_kernel");
+    {
+      KernelTimer kt(ctx, "insert_kernel");
+      dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, mm, dcap, dr, df);
     }
+    ctx.check_launch("dense_insert_kernel");
+    long long h[2];
+    uint32_t hdf = 0;
+    PRISM_CUDA(cudaMemcpyAsync(h, mm, 16, cudaMemcpyDeviceToHost, ctx.stream));
+    PRISM_CUDA(cudaMemcpyAsync(&hdf, df, 4, cudaMemcpyDeviceToHost, ctx.stream));
+    PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (!hdf) {
+      t->dense = true;
+      t->dmin = h[0];
+      t->drange = (uint64_t)h[1] - (uint64_t)h[0] + 1;
+      t->dense_rows = dense;
+      return t;
+    }
+    // a repeated key (flag 1) or a range too wide (flag 2): hash slots
   }
   double lf = std::min(0.9, std::max(0.1, tune.load_factor));
   uint64_t cap = next_pow2((uint64_t)std::ceil((double)std::max<int64_t>(n, 1) / lf));
