@@ -617,12 +617,13 @@ int prism_serve_probe(prism_server* server, int32_t table_id, const int64_t* key
  * probes of registered tables with unique Int64 keys and a fixed-width,
  * null-free payload, of at most max_rows rows (0: any), no longer go to the
  * worker threads: their descriptors go into a ring in device memory, and ONE
- * persistent kernel (ctas_per_sm CTAs per SM, 1 or 2; 0: 2) drains it tile
+ * persistent kernel (ctas_per_sm CTAs per SM, 1 or 2; 0: 1, which leaves
+ * room beside it for a GROUP BY kernel's block on every SM) drains it tile
  * by tile (2,048 probe rows), requests of different tables and sizes sharing
  * the launch; a host thread reports each request when its last tile is done.
  * Their matches come as a multiset: runs of consecutive probe rows in any
  * order, rows ascending inside a run. Every wait of the kernel is bounded:
- * idle CTAs exit after a few milliseconds (the kernel is relaunched when work
+ * idle CTAs exit after about 0.1 ms (the kernel is relaunched when work
  * arrives), and a CTA that waits wait_limit_ms (0: 1000) for a request's
  * descriptor gives up, every request then in flight fails with
  * PRISM_ERR_TIMEOUT, and the queue is reset and stays usable. enable = 0

@@ -206,7 +206,6 @@ struct ProbeArgs {
   uint32_t* err;
   int any_order;  // tiles reserve their output by one atomicAdd on *total, no look-back
   int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
-  const unsigned long long* inl_pay;  // dense tables: the gathered build column by key value, or null
   const ulonglong2* krec;  // packed build keys (single Utf8 key), or null
 };
 
@@ -519,14 +518,6 @@ __global__ void __launch_bounds__(QB, 4) probe_rows_dense_kernel(const int64_t* 
   }
 }
 
-// inl[key - dmin] = the build row's value of an 8-byte column (dense tables,
-// unique keys: every build row owns its key's entry)
-__global__ void dense_inline_kernel(const int64_t* __restrict__ keys, const unsigned long long* __restrict__ src,
-                                    int64_t n, int64_t dmin, unsigned long long* __restrict__ inl) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    inl[(uint64_t)__ldg(keys + i) - (uint64_t)dmin] = __ldg(src + i);
-}
-
 // min / max of the build keys (dense-mode test)
 __global__ void minmax_i64_kernel(const int64_t* __restrict__ keys, int64_t n, long long* mm) {
   long long lo = 0x7fffffffffffffffLL, hi = (long long)0x8000000000000000ULL;
@@ -657,10 +648,7 @@ constexpr int AT = AB * AV * 2;    // rows per tile (2048)
 // row in prow): a tile's keys share their top hash bits, so its slot loads
 // stay inside one slice of the table (the partitioned probe of a table
 // larger than L2).
-// INL (dense tables): the one gathered build column is read from a copy
-// laid out by key value (a.inl_pay[key - dmin]), loaded beside the dense row
-// instead of after it: one dependent load per probe row instead of two.
-template <bool DENSE, bool VEC, bool PART, bool INL = false>
+template <bool DENSE, bool VEC, bool PART>
 __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
                                                                 const uint32_t* __restrict__ prow, int64_t n,
                                                                 ProbeArgs a) {
@@ -706,9 +694,7 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
       for (int j = 0; j < 2; ++j) {
         const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
         const uint64_t d = key[it][j] - (uint64_t)a.dmin;
-        const bool in = q < n && d < a.drange;
-        brow[it][j] = in ? __ldg(a.dense + d) : NO_MATCH;
-        if (INL) pre[it][j] = in ? __ldg(a.inl_pay + d) : 0ULL;
+        brow[it][j] = (q < n && d < a.drange) ? __ldg(a.dense + d) : NO_MATCH;
       }
   } else {
     uint64_t s[AV][2];
@@ -738,8 +724,8 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   }
   // one 8-byte gathered column (probe row + payload): its values loaded now,
   // all in flight before the ranking
-  const bool one8 = INL || (a.ngather == 1 && a.g_width[0] == 8);
-  if (one8 && !INL) {
+  const bool one8 = a.ngather == 1 && a.g_width[0] == 8;
+  if (one8) {
     const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[0]);
     const bool bside = a.g_side[0] != 0;
 #pragma unroll
@@ -1092,24 +1078,6 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
       KernelTimer kt(ctx, "probe_emit_any_kernel");
       probe_emit_any_kernel<false, true, true><<<grid, AB, 0, ctx.stream>>>(reinterpret_cast<const int64_t*>(kpart),
                                                                              rpart, n, a);
-    } else if (t.dense && !want_build_idx && gathers.size() == 1 && gathers[0].side == 1 && gathers[0].width == 8 &&
-               n >= 2 * t.build.rows && (reinterpret_cast<uintptr_t>(gathers[0].src) & 7) == 0) {
-      // a long probe emitting one 8-byte build column: lay that column out by
-      // key value first (one pass over the build rows), so each probe row's
-      // payload load no longer waits for its dense row
-      MemP minl;
-      unsigned long long* inl = ctx.alloc_t<unsigned long long>((size_t)t.drange, minl);
-      {
-        KernelTimer kt(ctx, "dense_inline_kernel");
-        dense_inline_kernel<<<grid_for(ctx, t.build.rows, 256, 16), 256, 0, ctx.stream>>>(
-            static_cast<const int64_t*>(t.build.cols[t.key_cols[0]]->values),
-            static_cast<const unsigned long long*>(gathers[0].src), t.build.rows, t.dmin, inl);
-      }
-      ctx.check_launch("dense_inline_kernel");
-      a.inl_pay = inl;
-      KernelTimer kt(ctx, "probe_emit_any_kernel");
-      vec ? probe_emit_any_kernel<true, true, false, true><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a)
-          : probe_emit_any_kernel<true, false, false, true><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
     } else {
       KernelTimer kt(ctx, "probe_emit_any_kernel");
       if (t.dense)

@@ -348,9 +348,10 @@ void DeviceQueue::ensure_running() {
     if (e != cudaSuccess) fail(PRISM_ERR_CUDA, std::string("device queue kernel: ") + cudaGetErrorString(e));
   }
   const unsigned long long first = pending_.empty() ? (unsigned long long)next_seq_ : (unsigned long long)pending_.begin()->first;
-  // idle checks of 2 us after the first 32: an exit after ~4 ms without work
+  // idle checks of 2 us after the first 32: an exit after ~0.1 ms without
+  // work, so idle CTAs do not hold SMs the workers' kernels could use
   queue_probe_kernel<<<grid_, QB, 0, kstream_>>>(d_ctl_, d_ring_, d_slots_, d_done_, d_status_, d_tables_, first,
-                                                   2048u, wait_limit_);
+                                                   80u, wait_limit_);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) fail(PRISM_ERR_CUDA, std::string("device queue kernel launch: ") + cudaGetErrorString(e));
   ctx_.note_launch();

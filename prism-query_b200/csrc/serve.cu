@@ -701,7 +701,7 @@ int prism_server_set_device_queue(prism_server* s, int32_t enable, int64_t max_r
     if (!s->queue) {
       int rc = prism_ctx_create(s->device, 0, &s->qctx);
       if (rc) fail(rc, "device queue context");
-      s->queue = std::make_unique<DeviceQueue>(s->qctx->impl, ctas_per_sm ? ctas_per_sm : 2,
+      s->queue = std::make_unique<DeviceQueue>(s->qctx->impl, ctas_per_sm ? ctas_per_sm : 1,
                                                (int64_t)(wait_limit_ms ? wait_limit_ms : 1000) * 1000);
       for (auto& tb : s->tables)
         if (tb.coalesce && tb.table->t->int64_fast && !tb.table->t->has_dups)
