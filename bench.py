@@ -46,6 +46,7 @@ WORKLOAD = "inner hash join: 10M unique int64 build keys (+int64 payload) x 100M
 FALLBACK_HBM_GBS = 6650.0
 CPU_SAMPLE_PROBE = 10_000_000
 SCALE = 1.0
+PROBE_DIST = "zipf"
 
 
 def parse():
@@ -68,6 +69,9 @@ def parse():
     ap.add_argument("--partition", choices=["auto", "on", "off"], default="auto",
                     help="c2 with --join-table hash: the radix-partitioned build and probe (auto: once the hash slots "
                          "outgrow L2)")
+    ap.add_argument("--probe-dist", choices=["zipf", "uniform"], default="zipf",
+                    help="c2: probe keys Zipf(1.1) through a permutation (the workload) or uniform over the same "
+                         "12.5M ranks (a side case without skew: every probe of a table larger than L2 misses it)")
     ap.add_argument("--tune", action="store_true",
                     help="c2 / c4 / c1: run the autotuner on the workload's own inputs first; the timed steps use "
                          "its recorded choice (reported under config.tuning)")
@@ -82,8 +86,11 @@ def parse():
         os.environ["PRISM_JOIN_PARTITION"] = "1" if a.partition == "on" else "0"
     if a.steps is None:
         a.steps = {"c1": 500, "c2": 200, "c3": 60, "c4": 10, "c5": 1, "sort": 10, "topn": 10, "parquet": 10}[a.workload]
-    global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE
+    global N_BUILD, N_PROBE, ZIPF_RANKS, CPU_SAMPLE_PROBE, SCALE, PROBE_DIST, WORKLOAD
     SCALE = a.scale
+    PROBE_DIST = a.probe_dist
+    if PROBE_DIST == "uniform":
+        WORKLOAD = WORKLOAD.replace("Zipf(1.1) int64 probe keys", "uniform int64 probe keys (over 12.5M key values)")
     if a.scale != 1.0:
         N_BUILD = int(N_BUILD * a.scale)
         N_PROBE = int(N_PROBE * a.scale)
@@ -114,7 +121,11 @@ def gen_c2(torch, device, seed):
     pkeys = torch.empty(N_PROBE, device=device, dtype=torch.int64)
     chunk = 20_000_000
     for lo in range(0, N_PROBE, chunk):
-        u = torch.rand(min(chunk, N_PROBE - lo), generator=g, device=device, dtype=torch.float64)
+        m = min(chunk, N_PROBE - lo)
+        if PROBE_DIST == "uniform":
+            pkeys[lo : lo + m] = torch.randint(0, ZIPF_RANKS, (m,), generator=g, device=device, dtype=torch.int64)
+            continue
+        u = torch.rand(m, generator=g, device=device, dtype=torch.float64)
         r = torch.searchsorted(cdf, u, right=True).clamp_(max=ZIPF_RANKS - 1)
         pkeys[lo : lo + len(u)] = sigma[r]
         del u, r
@@ -356,7 +367,8 @@ def main():
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "int64",
-            "data": "synthetic (seeded: permutation build keys, Zipf(1.1) probe ranks through a seeded permutation)",
+            "data": ("synthetic (seeded: permutation build keys, Zipf(1.1) probe ranks through a seeded permutation)"
+                     if PROBE_DIST == "zipf" else "synthetic (seeded: permutation build keys, uniform probe keys)"),
             "config": {
                 "workload": WORKLOAD,
                 "build_rows": N_BUILD,
