@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "sort", "topn", "parquet"], default="c2")
     ap.add_argument("--requests", type=int, default=10_000, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="c5: Poisson arrival rate (requests/s)")
+    ap.add_argument("--queue-ctas", type=int, default=0, help="c5: persistent kernel CTAs per SM (0: the library's default)")
     ap.add_argument("--no-device-queue", action="store_true",
                     help="c5: probes on the worker threads instead of the persistent kernel's device queue")
     ap.add_argument("--steps", type=int, default=None)
@@ -1201,7 +1202,7 @@ def run_c5(args, rank, world, local, torch, dist):
             for r in reqs[:200]]
     S.run_plain(warm[:20], regs, ctx, local)
     srv = S.Server(local, budget_bytes=120 << 30, workers=4, coalesce_rows=1 << 18, max_coalesce=64,
-                   device_queue=not args.no_device_queue)
+                   device_queue=not args.no_device_queue, queue_ctas_per_sm=args.queue_ctas)
     for name, reg in regs.items():
         srv.register_table(name, reg.table, 1)
     for _ in range(2):

@@ -276,12 +276,18 @@ __global__ void __launch_bounds__(QB, 4) queue_probe_kernel(QCtl* ctl, const QIt
 
 }  // namespace
 
-DeviceQueue::DeviceQueue(Ctx& ctx, int ctas_per_sm, int64_t wait_limit_us) : ctx_(ctx) {
+DeviceQueue::DeviceQueue(Ctx& ctx, int ctas_per_sm, int64_t wait_limit_us, int64_t idle_us) : ctx_(ctx) {
   PRISM_CUDA(cudaSetDevice(ctx.device));
   grid_ = ctx.sm_count * std::max(1, std::min(ctas_per_sm, 2));
   wait_limit_ = (uint32_t)std::max<int64_t>(1, std::min<int64_t>(wait_limit_us, 60LL * 1000 * 1000));
+  // idle checks: 32 of ~0.2 us, then ~2 us each
+  idle_limit_ = 32u + (uint32_t)std::max<int64_t>(0, std::min<int64_t>(idle_us, 1000000) / 2);
   PRISM_CUDA(cudaStreamCreateWithFlags(&qstream_, cudaStreamNonBlocking));
-  PRISM_CUDA(cudaStreamCreateWithFlags(&kstream_, cudaStreamNonBlocking));
+  // the persistent kernel's stream at the highest priority: its CTAs are
+  // placed before the workers' pending blocks as SMs free up
+  int lo = 0, hi = 0;
+  PRISM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  PRISM_CUDA(cudaStreamCreateWithPriority(&kstream_, cudaStreamNonBlocking, hi));
   PRISM_CUDA(cudaMalloc(&d_ring_, sizeof(QItem) * kRing));
   PRISM_CUDA(cudaMalloc(&d_ctl_, sizeof(QCtl)));
   PRISM_CUDA(cudaMalloc(&d_slots_, sizeof(QSlot) * kRing));
@@ -348,10 +354,10 @@ void DeviceQueue::ensure_running() {
     if (e != cudaSuccess) fail(PRISM_ERR_CUDA, std::string("device queue kernel: ") + cudaGetErrorString(e));
   }
   const unsigned long long first = pending_.empty() ? (unsigned long long)next_seq_ : (unsigned long long)pending_.begin()->first;
-  // idle checks of 2 us after the first 32: an exit after ~0.1 ms without
-  // work, so idle CTAs do not hold SMs the workers' kernels could use
+  // idle CTAs exit (after idle_limit_ checks) so they do not hold SMs the
+  // workers' kernels could use
   queue_probe_kernel<<<grid_, QB, 0, kstream_>>>(d_ctl_, d_ring_, d_slots_, d_done_, d_status_, d_tables_, first,
-                                                   80u, wait_limit_);
+                                                   idle_limit_, wait_limit_);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) fail(PRISM_ERR_CUDA, std::string("device queue kernel launch: ") + cudaGetErrorString(e));
   ctx_.note_launch();

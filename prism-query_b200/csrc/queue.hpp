@@ -44,7 +44,8 @@ class DeviceQueue {
   static constexpr int kRing = 4096;  // requests in flight at most
 
   // ctx: the context whose pool holds the outputs (kept alive by the caller)
-  DeviceQueue(Ctx& ctx, int ctas_per_sm, int64_t wait_limit_us);
+  // idle_us: a CTA with nothing to claim exits after about this long
+  DeviceQueue(Ctx& ctx, int ctas_per_sm, int64_t wait_limit_us, int64_t idle_us = 100);
   ~DeviceQueue();
 
   // Registers a resident table (single Int64 key, no repeated keys) and its
@@ -72,6 +73,7 @@ class DeviceQueue {
   Ctx& ctx_;
   int grid_ = 0;
   uint32_t wait_limit_ = 0;
+  uint32_t idle_limit_ = 0;
   std::mutex mu_;
   cudaStream_t qstream_ = nullptr;  // descriptor / publish copies
   cudaStream_t kstream_ = nullptr;  // the persistent kernel

@@ -22,6 +22,7 @@
 // with PartitionStore as the resident-table registry,
 // shuffle_writer.rs:42-86).
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -701,8 +702,12 @@ int prism_server_set_device_queue(prism_server* s, int32_t enable, int64_t max_r
     if (!s->queue) {
       int rc = prism_ctx_create(s->device, 0, &s->qctx);
       if (rc) fail(rc, "device queue context");
+      // PRISM_QUEUE_IDLE_US: how long an idle CTA of the persistent kernel
+      // waits for work before it exits (default 100)
+      const char* iu = std::getenv("PRISM_QUEUE_IDLE_US");
+      const int64_t idle_us = iu ? std::max<int64_t>(0, std::atoll(iu)) : 100;
       s->queue = std::make_unique<DeviceQueue>(s->qctx->impl, ctas_per_sm ? ctas_per_sm : 1,
-                                               (int64_t)(wait_limit_ms ? wait_limit_ms : 1000) * 1000);
+                                               (int64_t)(wait_limit_ms ? wait_limit_ms : 1000) * 1000, idle_us);
       for (auto& tb : s->tables)
         if (tb.coalesce && tb.table->t->int64_fast && !tb.table->t->has_dups)
           tb.queue_id = s->queue->add_table(*tb.table->t, *tb.table->t->build.cols[tb.payload_col]);
