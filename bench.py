@@ -56,8 +56,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=10_000, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="c5: Poisson arrival rate (requests/s)")
     ap.add_argument("--queue-ctas", type=int, default=0, help="c5: persistent kernel CTAs per SM (0: the library's default)")
-    ap.add_argument("--no-device-queue", action="store_true",
-                    help="c5: probes on the worker threads instead of the persistent kernel's device queue")
+    ap.add_argument("--device-queue", action="store_true",
+                    help="c5: probes drained by the persistent kernel's device work queue instead of the workers")
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--warmup", type=int, default=5)
@@ -1202,7 +1202,7 @@ def run_c5(args, rank, world, local, torch, dist):
             for r in reqs[:200]]
     S.run_plain(warm[:20], regs, ctx, local)
     srv = S.Server(local, budget_bytes=120 << 30, workers=4, coalesce_rows=1 << 18, max_coalesce=64,
-                   device_queue=not args.no_device_queue, queue_ctas_per_sm=args.queue_ctas)
+                   device_queue=args.device_queue, queue_ctas_per_sm=args.queue_ctas)
     for name, reg in regs.items():
         srv.register_table(name, reg.table, 1)
     for _ in range(2):
@@ -1270,7 +1270,7 @@ def run_c5(args, rank, world, local, torch, dist):
                                    "C2-style probe of 8 resident tables (1M-10M keys), rows log-uniform 8K-16M",
                        "total_rows": total_rows, "budget_bytes": 120 << 30, "workers": 4,
                        "device_queue": ("probes drained by one persistent kernel from a device work queue"
-                                        if not args.no_device_queue else "off (probes on the worker threads)"),
+                                        if args.device_queue else "off (probes on the worker threads)"),
                        "l2": "request slices of 16M-row pools; most requests exceed L2"},
             "served": ss, "plain_per_call": sp,
             "throughput_ratio": ss["rows_per_s"] / sp["rows_per_s"], "p99_ratio": ss["p99_ms"] / sp["p99_ms"],

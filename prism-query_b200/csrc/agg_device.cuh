@@ -506,7 +506,11 @@ __device__ __forceinline__ void hash_accumulate(const AggArgs& a, unsigned long 
       add_f64(w, x.f, a.op[j].lo_exp, a.err, a.maxexp + j);
     } else if (kind == O_SUM_INT) {
       const long long q = (long long)x.i;
-      if (f64_exact_int(q)) {  // two 32-bit limbs of an int64 value, the top one signed
+      if (q >= -(1LL << 32) && q < (1LL << 32)) {
+        // one signed add into the low limb's counter: with at most 2^31 rows
+        // per call its magnitude stays below 2^63
+        atom_add(w, (unsigned long long)q);
+      } else if (f64_exact_int(q)) {  // two 32-bit limbs of an int64 value, the top one signed
         atom_add(w, (unsigned long long)(uint32_t)q);
         atom_add(w + 1, (unsigned long long)(q >> 32));
       } else {

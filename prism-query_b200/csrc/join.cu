@@ -654,13 +654,6 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
                                                                 ProbeArgs a) {
   __shared__ uint32_t seg[AV * (AB / 32)];
   __shared__ unsigned long long s_off;
-  __shared__ uint32_t s_total;
-  // the common output (probe row, build row, one 8-byte column) staged in
-  // rank order, so the segment goes out with consecutive threads on
-  // consecutive rows (each store instruction fills whole sectors)
-  __shared__ uint32_t st_p[AT];
-  __shared__ uint32_t st_b[AT];
-  __shared__ unsigned long long st_v[AT];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * AT;
   // positions of this thread: base + 2 * (it * AB + threadIdx.x) + {0, 1}
@@ -757,41 +750,10 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
     const uint32_t incl = warp_incl_scan32(x);
     seg[lane] = incl - x;
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (lane == 0) {
-      s_off = total ? atomicAdd(a.total, (unsigned long long)total) : 0ULL;
-      s_total = total;
-    }
+    if (lane == 0) s_off = total ? atomicAdd(a.total, (unsigned long long)total) : 0ULL;
   }
   __syncthreads();
   const unsigned long long off = s_off;
-  if (one8) {
-#pragma unroll
-    for (int it = 0; it < AV; ++it) {
-      uint32_t lp = seg[it * (AB / 32) + warp] + lpos[it];
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        if (brow[it][j] == NO_MATCH) continue;
-        st_p[lp] = (uint32_t)(a.row_base + row[it][j]);
-        st_b[lp] = brow[it][j];
-        st_v[lp] = pre[it][j];
-        ++lp;
-      }
-    }
-    __syncthreads();
-    const uint32_t total = s_total;
-    unsigned long long* gv = static_cast<unsigned long long*>(a.g_dst[0]);
-    for (uint32_t i = threadIdx.x; i < total; i += AB) {
-      const uint64_t pos = off + i;
-      if (pos >= a.out_capacity) {
-        atomicOr(a.err, DERR_CAPACITY);
-        break;
-      }
-      if (a.out_probe) __stcs(a.out_probe + pos, st_p[i]);
-      if (a.out_build) __stcs(a.out_build + pos, st_b[i]);
-      __stcs(gv + pos, st_v[i]);
-    }
-    return;
-  }
 #pragma unroll
   for (int it = 0; it < AV; ++it) {
     uint64_t pos = off + seg[it * (AB / 32) + warp] + lpos[it];
@@ -803,7 +765,13 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
         atomicOr(a.err, DERR_CAPACITY);
         continue;
       }
-      emit_one(a, pos, r, brow[it][j]);
+      if (one8) {
+        if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(a.row_base + r));
+        if (a.out_build) __stcs(a.out_build + pos, brow[it][j]);
+        __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it][j]);
+      } else {
+        emit_one(a, pos, r, brow[it][j]);
+      }
       ++pos;
     }
   }
