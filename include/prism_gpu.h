@@ -337,9 +337,10 @@ int prism_join_project(prism_ctx* ctx, const prism_hash_table* table,
                        prism_batch** out);
 /* prism_join_project with flags. PRISM_JOIN_ANY_ORDER: the caller takes the
  * matches as a multiset (the executor's fused join -> aggregate consumes
- * them that way, executor.rs:474-551): runs of consecutive probe rows come in
- * any order, rows ascending inside a run, so the probe needs one pass and no
- * ordering step. The set of output rows is the same as without the flag. */
+ * them that way, executor.rs:474-551): the matches come in no particular
+ * order (each 2,048-row tile's matches form one contiguous run of the output),
+ * so the probe needs one pass and no ordering step. The set of output rows is
+ * the same as without the flag. */
 #define PRISM_JOIN_ANY_ORDER 1u
 int prism_join_project_ex(prism_ctx* ctx, const prism_hash_table* table,
                           const prism_batch* probe, const int32_t* probe_keys,

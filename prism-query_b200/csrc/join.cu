@@ -636,8 +636,9 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
 // join -> aggregate and join_project with PRISM_JOIN_ANY_ORDER): each CTA
 // loads its 2048 probe keys with 16-byte vector loads, looks them up (dense
 // row or hash slot walk), loads every matched row's gathered values, ranks
-// its matches in row order with warp ballots and one warp scan, reserves its
-// output segment with ONE atomicAdd and writes the segment contiguously. No
+// its matches with warp ballots and two warp scans (ordered so that each
+// store instruction of a warp covers one contiguous run), reserves its
+// output segment with ONE atomicAdd and writes the segment. No
 // row words go back to HBM and no CTA waits on another; segments land in
 // whatever order the CTAs reserve them.
 constexpr int AB = 256;            // threads per CTA
@@ -652,7 +653,7 @@ template <bool DENSE, bool VEC, bool PART>
 __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
                                                                 const uint32_t* __restrict__ prow, int64_t n,
                                                                 ProbeArgs a) {
-  __shared__ uint32_t seg[AV * (AB / 32)];
+  __shared__ uint32_t seg[2 * AV * (AB / 32)];
   __shared__ unsigned long long s_off;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * AT;
@@ -734,32 +735,38 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
       for (int j = 0; j < 2; ++j)
         pre[it][j] = brow[it][j] != NO_MATCH ? __ldg(src + (bside ? (int64_t)brow[it][j] : row[it][j])) : 0ULL;
   }
-  // rank in position order: (it, warp, lane, j)
-  uint32_t lpos[AV];
+  // rank as (it, j, warp, lane): the matches of one (it, j) of a warp take
+  // consecutive positions, so each store instruction covers one contiguous
+  // run (whole sectors) instead of every other position
+  uint32_t lpos[AV][2];
   const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int it = 0; it < AV; ++it) {
-    const uint32_t m0 = __ballot_sync(0xffffffffu, brow[it][0] != NO_MATCH);
-    const uint32_t m1 = __ballot_sync(0xffffffffu, brow[it][1] != NO_MATCH);
-    lpos[it] = __popc(m0 & lt) + __popc(m1 & lt);
-    if (lane == 0) seg[it * (AB / 32) + warp] = __popc(m0) + __popc(m1);
-  }
+  for (int it = 0; it < AV; ++it)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t m = __ballot_sync(0xffffffffu, brow[it][j] != NO_MATCH);
+      lpos[it][j] = __popc(m & lt);
+      if (lane == 0) seg[(it * 2 + j) * (AB / 32) + warp] = __popc(m);
+    }
   __syncthreads();
-  if (warp == 0) {  // AV * 8 = 32 segments: one warp scan
-    const uint32_t x = seg[lane];
-    const uint32_t incl = warp_incl_scan32(x);
-    seg[lane] = incl - x;
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (warp == 0) {  // 2 * AV * 8 = 64 segments: two scans of one warp
+    const uint32_t x0 = seg[lane], x1 = seg[32 + lane];
+    const uint32_t i0 = warp_incl_scan32(x0);
+    const uint32_t t0 = __shfl_sync(0xffffffffu, i0, 31);
+    const uint32_t i1 = warp_incl_scan32(x1) + t0;
+    seg[lane] = i0 - x0;
+    seg[32 + lane] = i1 - x1;
+    const uint32_t total = __shfl_sync(0xffffffffu, i1, 31);
     if (lane == 0) s_off = total ? atomicAdd(a.total, (unsigned long long)total) : 0ULL;
   }
   __syncthreads();
   const unsigned long long off = s_off;
 #pragma unroll
-  for (int it = 0; it < AV; ++it) {
-    uint64_t pos = off + seg[it * (AB / 32) + warp] + lpos[it];
+  for (int it = 0; it < AV; ++it)
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       if (brow[it][j] == NO_MATCH) continue;
+      const uint64_t pos = off + seg[(it * 2 + j) * (AB / 32) + warp] + lpos[it][j];
       const int64_t r = row[it][j];
       if (pos >= a.out_capacity) {
         atomicOr(a.err, DERR_CAPACITY);
@@ -772,9 +779,7 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
       } else {
         emit_one(a, pos, r, brow[it][j]);
       }
-      ++pos;
     }
-  }
 }
 
 template <class K, bool EMIT>

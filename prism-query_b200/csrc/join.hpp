@@ -65,8 +65,8 @@ struct ProbeResult {
 // Probes `probe` (key columns `keys`, types checked against the table) and
 // emits matches in the reference's order: probe rows ascending, build rows
 // ascending within a probe row. With `any_order` the matches come as a
-// multiset (tiles of consecutive probe rows in any order, rows ascending
-// inside a tile), which needs neither look-back nor a second pass.
+// multiset (in no particular order), which needs neither look-back nor a
+// second pass.
 // `row_base` is added to the emitted probe row indices (the probe batch is
 // rows [row_base, row_base + probe.rows) of a larger one). Fused gathers write into caller buffers of
 // `gather_capacity` rows (must be >= the match count; use probe_count first).
