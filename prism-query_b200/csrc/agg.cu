@@ -1185,6 +1185,12 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.jpk = jpk_dev[&b - &joined[0]];
         a.jbk = static_cast<const DCol*>(t.key_views_dev->ptr);
         a.jkrec = t.key_records ? static_cast<const ulonglong2*>(t.key_records->ptr) : nullptr;
+        // the entries' lookup reads the probe key's bytes directly: a Utf8
+        // (not dictionary) probe key
+        const bool ent = t.key_entries && join->probe_keys.size() == 1 &&
+                         b.cols[join->probe_keys[0]]->type == TY_UTF8;
+        a.jent = ent ? static_cast<const ulonglong2*>(t.key_entries->ptr) : nullptr;
+        a.jent_col = ent && t.entry_col >= 0 ? n_probe_cols + t.entry_col : -1;
         a.jnkeys = (int)join->probe_keys.size();
         a.n_cols = (int)pg.cols.size();
         if (A.wide) fused_fail("a Float64 sum beyond the 192-bit window over a join");

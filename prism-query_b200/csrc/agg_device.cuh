@@ -94,6 +94,8 @@ struct AggArgs {
   const DCol* jpk;           // probe key column views
   const DCol* jbk;           // build key column views
   const ulonglong2* jkrec;   // packed build keys (single Utf8 key), or null
+  const ulonglong2* jent;    // slot entries (single Utf8 key), or null
+  int32_t jent_col;          // joined column whose value the entries carry, or -1
   int32_t jnkeys;
   uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
   unsigned long long* gnew_count;  // length of gnew
@@ -686,7 +688,7 @@ __device__ __forceinline__ void hash_body(const AggArgs& a) {
 // into the block's table. The order key of a joined row is
 // (global probe row << 32 | build row), which sorts like the joined rows'
 // positions (probe rows ascending, build rows ascending inside one).
-template <class E, int NOPS, int BLOCK, int R>
+template <class E, int NOPS, int BLOCK, int R, bool ENT>
 __device__ __forceinline__ void join_body(const AggArgs& a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ DCol scols[TINY_MAX_COLS];
@@ -706,17 +708,69 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
     uint64_t key[R];
     ulonglong2 e[R];
     uint64_t s[R];
+    // slot entries (a single Utf8 probe key): the key's words read once,
+    // hashed, then compared against the 64-byte entry; keq / inl hold each
+    // single-row slot's comparison and inlined build value
+    JoinKeyWords kw[ENT ? R : 1];
+    bool kw_ok[ENT ? R : 1];
+    bool keq[R];
+    unsigned long long inl[ENT ? R : 1];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
       cnt[r] = 0;
       cand[r] = JOIN_NO_MATCH;
       key[r] = 0;
-      if (idx < n)
+      keq[r] = true;
+      if constexpr (ENT) {
+        kw_ok[r] = idx < n && join_key_words(a.jpk[0], idx, kw[r]);
+        if (kw_ok[r]) key[r] = join_words_hash(kw[r]);
+        else if (idx < n) key[r] = join_key_hash(a.jpk, a.jnkeys, idx);
+      } else if (idx < n) {
         key[r] = a.jfast ? (uint64_t)static_cast<const int64_t*>(a.jpk[0].values)[idx]
                          : join_key_hash(a.jpk, a.jnkeys, idx);
+      }
     }
-    if (a.jdense) {
+    if constexpr (ENT) {
+      ulonglong2 e1[R], e2[R], e3[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        s[r] = join_slot_of(key[r], a.jshift);
+        e[r] = make_ulonglong2(JOIN_EMPTY, 0);
+        if (idx < n) {
+          const ulonglong2* p = a.jent + 4 * s[r];
+          e[r] = __ldg(p);
+          e1[r] = __ldg(p + 1);
+          e2[r] = __ldg(p + 2);
+          e3[r] = __ldg(p + 3);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        inl[r] = 0;
+        if (idx >= n) continue;
+        for (uint64_t steps = 0; e[r].x != key[r] && e[r].x != JOIN_EMPTY && steps <= a.jmask; ++steps) {
+          s[r] = (s[r] + 1) & a.jmask;
+          const ulonglong2* p = a.jent + 4 * s[r];
+          e[r] = __ldg(p);
+          e1[r] = __ldg(p + 1);
+          e2[r] = __ldg(p + 2);
+          e3[r] = __ldg(p + 3);
+        }
+        if (e[r].x == key[r]) {
+          cand[r] = (uint32_t)e[r].y;
+          cnt[r] = (uint32_t)(e[r].y >> 32);
+          if (cnt[r] == 1) {
+            // a long key on either side: compared against the columns
+            keq[r] = kw_ok[r] && !(e1[r].x & JOIN_ENT_LONG) ? join_words_equal(kw[r], e1[r], e2[r], e3[r])
+                                                             : join_rows_equal(a.jpk, a.jbk, 1, idx, cand[r]);
+            inl[r] = e3[r].y;
+          }
+        }
+      }
+    } else if (a.jdense) {
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const I idx = base + r * stride;
@@ -753,15 +807,19 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
-      if (cnt[r] == 1) rows[r] = E::fetch(cols, idx, (I)cand[r]);
+      if (cnt[r] == 1) {
+        if constexpr (ENT) rows[r] = E::fetch(cols, idx, (I)cand[r], inl[r], true);
+        else rows[r] = E::fetch(cols, idx, (I)cand[r]);
+      }
     }
     // packed build keys: every single-candidate row's key compared up front
     // (the R record loads in flight together, beside the fetches above)
-    bool keq[R];
+    if constexpr (!ENT) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const I idx = base + r * stride;
-      keq[r] = !a.jfast && a.jkrec && cnt[r] == 1 ? join_rec_equal(a.jpk[0], idx, a.jkrec, cand[r]) : true;
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        keq[r] = !a.jfast && a.jkrec && cnt[r] == 1 ? join_rec_equal(a.jpk[0], idx, a.jkrec, cand[r]) : true;
+      }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -769,9 +827,9 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
       for (uint32_t j = 0; j < cnt[r]; ++j) {
         const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
         if (!a.jfast) {
-          const bool eq = cnt[r] == 1 && a.jkrec ? keq[r]
-                          : a.jkrec              ? join_rec_equal(a.jpk[0], idx, a.jkrec, b)
-                                                 : join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b);
+          const bool eq = cnt[r] == 1 && (ENT || a.jkrec) ? keq[r]
+                          : a.jkrec                       ? join_rec_equal(a.jpk[0], idx, a.jkrec, b)
+                                                          : join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b);
           if (!eq) continue;
         }
         const I bidx = (I)b;

@@ -74,6 +74,10 @@ JoinTuning join_tuning() {
   // PRISM_JOIN_KEY_RECORDS=0: Utf8 keys compared through the build column, not packed records
   const char* kr = std::getenv("PRISM_JOIN_KEY_RECORDS");
   if (kr && std::strcmp(kr, "0") == 0) t.key_records = false;
+  // PRISM_JOIN_KEY_ENTRIES=1: the fused join -> aggregate over a Utf8 key
+  // looks up 64-byte slot entries instead of hash slots and row records
+  const char* ke = std::getenv("PRISM_JOIN_KEY_ENTRIES");
+  if (ke && (std::strcmp(ke, "0") == 0 || std::strcmp(ke, "1") == 0)) t.key_entries = ke[0] == '1';
   const char* p = std::getenv("PRISM_JOIN_PARTITION");
   if (p && (std::strcmp(p, "0") == 0 || std::strcmp(p, "1") == 0)) {
     t.partition = p[0] - '0';
@@ -379,7 +383,12 @@ Batch join_aggregate_impl(Ctx& x, const std::vector<const Batch*>& probes, const
                           const std::vector<int>& bk, const int32_t* cols, int32_t n_cols, const prism_expr* exprs,
                           int32_t n_exprs, const prism_agg_config* agg, const AggTuning& tune) {
   for (const Batch* p : probes) check_join_keys(*p, pk, bb, bk);
-  auto t = build_join_table(x, bb, bk, join_tuning_for(bb, bk));
+  JoinTuning jt = join_tuning_for(bb, bk);
+  // a single Utf8 key looked up through slot entries by the fused kernel:
+  // they replace the row records
+  const bool entries = join_agg_fused() && jt.key_entries && bk.size() == 1 && bb.cols[bk[0]]->type == TY_UTF8;
+  if (entries) jt.key_records = false;
+  auto t = build_join_table(x, bb, bk, jt);
   // joined columns referenced by the projection (executor.rs:474-551)
   const Batch& p0 = *probes[0];
   int np = (int)p0.cols.size(), total = np + (int)bb.cols.size();
@@ -403,6 +412,17 @@ Batch join_aggregate_impl(Ctx& x, const std::vector<const Batch*>& probes, const
         need[col] = true;
       }
     }
+  }
+  if (entries) {
+    // the first referenced build column of fixed width 4 or 8 without
+    // nulls rides in the entries (read there for single-row slots)
+    int inl = -1;
+    for (int c = 0; c < (int)bb.cols.size() && inl < 0; ++c) {
+      const Column& col = *bb.cols[c];
+      const int w = width_of(col.type == TY_DICT ? col.index_type : col.type);
+      if (need[np + c] && !col.validity && col.type != TY_BOOL && (w == 4 || w == 8)) inl = c;
+    }
+    build_key_entries(x, *t, inl);
   }
   if (join_agg_fused()) {
     // one kernel per probe batch: lookup, projection and aggregation of

@@ -163,6 +163,9 @@ struct Gen {
   std::ostringstream out;     // current function body
   int id = 0;
   bool ok = true;
+  // program slot of the build column whose value the join table's slot
+  // entries carry (read from the entry for a single-row slot), or -1
+  int inl_slot = -1;
 
   Gen(const Program& p, const Batch& bb) : pg(p), b(bb) {}
 
@@ -245,13 +248,20 @@ struct Gen {
       if (nullable((int)s)) o << "    bool m" << s << ";\n";
     }
     if (!any) o << "    int unused;\n";
-    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, idx_t idx, idx_t bidx) {\n    Row w;\n";
+    o << "  };\n  static __device__ __forceinline__ Row fetch(const DCol* cols, idx_t idx, idx_t bidx, "
+         "unsigned long long inl = 0, bool use_inl = false) {\n    Row w;\n";
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       if (!fetched((int)s)) continue;
       const Column& c = *b.cols[pg.cols[s]];
       int t = c.type == TY_DICT ? c.index_type : c.type;
       std::string src = "cols[" + std::to_string(s) + "].values";
       const std::string at = rix((int)s);
+      if ((int)s == inl_slot && !c.validity && (width_of(t) == 4 || width_of(t) == 8) && t != TY_BOOL) {
+        const char* ty = width_of(t) == 4 ? "uint32_t" : "unsigned long long";
+        o << "    w.r" << s << "[0] = use_inl ? (" << ty << ")inl : static_cast<const " << ty << "*>(" << src << ")["
+          << at << "];\n";
+        continue;
+      }
       switch (t == TY_BOOL ? 0 : width_of(t)) {
         case 0:
           o << "    w.r" << s << "[0] = (static_cast<const uint8_t*>(" << src << ")[" << at << " >> 3] >> (" << at << " & 7)) & 1;\n";
@@ -663,9 +673,20 @@ static cudaLibrary_t compile_source(const std::string& source) {
     fail(PRISM_ERR_INTERNAL, "nvrtcCreateProgram failed");
   // no FMA contraction: generated Float64 arithmetic rounds after every
   // operation, like the interpreter and the reference
+  // PRISM_JIT_VERBOSE=1: ptxas's resource report (registers, spills, shared
+  // memory) of every compiled kernel on stderr
+  const char* vb = std::getenv("PRISM_JIT_VERBOSE");
+  const bool verbose = vb && vb[0] == '1';
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-int128", "--fmad=false",
-                        "--diag-suppress=550"};
-  nvrtcResult r = N.compile(prog, 5, opts);
+                        "--diag-suppress=550", "--ptxas-options=-v"};
+  nvrtcResult r = N.compile(prog, verbose ? 6 : 5, opts);
+  if (verbose && r == NVRTC_SUCCESS) {
+    size_t ls = 0;
+    N.log_size(prog, &ls);
+    std::string log(ls, '\0');
+    if (ls) N.log(prog, &log[0]);
+    std::fprintf(stderr, "[prism jit] %s\n", log.c_str());
+  }
   if (r != NVRTC_SUCCESS) {
     size_t ls = 0;
     N.log_size(prog, &ls);
@@ -914,7 +935,7 @@ std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKerne
   if (n_probe_cols >= 0)
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.block << ", " << join.min_blocks
       << ") prism_join_agg(prism::AggArgs a) {\n  prism::join_body<prism::QueryRow, " << a.n_ops << ", " << join.block
-      << ", " << join.rows << ">(a);\n}\n";
+      << ", " << join.rows << ", " << (a.jent ? "true" : "false") << ">(a);\n}\n";
   else
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.hash_block << ", 1) prism_hash_agg(prism::AggArgs a) {\n"
          "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", " << join.hash_block << ">(a);\n}\n";
@@ -966,7 +987,10 @@ std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs
                                 const JoinKernelShape& join) {
   Gen gen(pg, b);
   if (n_probe_cols >= 0)
-    for (size_t s = 0; s < pg.cols.size(); ++s) gen.bside.push_back(pg.cols[s] >= n_probe_cols ? 1 : 0);
+    for (size_t s = 0; s < pg.cols.size(); ++s) {
+      gen.bside.push_back(pg.cols[s] >= n_probe_cols ? 1 : 0);
+      if (a.jent && a.jent_col >= 0 && pg.cols[s] == a.jent_col) gen.inl_slot = (int)s;
+    }
   RowParts rp = row_parts(gen, a);
   if (!rp.ok) return "";
   // FxHash of the key columns, as fx_value computes it (common.cuh): fixed

@@ -14,6 +14,7 @@
 // reference's order (probe row ascending, build rows ascending) — no second
 // read of the probe side and no post-sort.
 #include "join.hpp"
+#include "bulk.cuh"
 #include "join_device.cuh"
 #include "prims.hpp"
 #include "sort.hpp"
@@ -164,6 +165,42 @@ __global__ void pack_key_records_kernel(DCol c, int64_t n, ulonglong2* __restric
   }
 }
 
+// The slot entries of a single Utf8 key column (layout in join_device.cuh),
+// one thread per slot: the slot words, and for a slot of one build row its
+// key (length, null flag, bytes) and the raw value of the inlined column
+// (inl_width 4 or 8 bytes, 0: none).
+__global__ void pack_key_entries_kernel(const ulonglong2* __restrict__ slots, uint64_t n_slots, DCol c,
+                                        const void* __restrict__ inl, int inl_width, ulonglong2* __restrict__ ent) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_slots;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    const ulonglong2 sl = slots[s];
+    uint64_t w[6] = {0, 0, 0, 0, 0, 0};
+    if (sl.x != JOIN_EMPTY && (sl.y >> 32) == 1) {
+      const uint32_t row = (uint32_t)sl.y;
+      const uint8_t* p;
+      int32_t len;
+      dcol_str(c, row, p, len);
+      w[0] = (uint64_t)(uint32_t)len | (dcol_valid(c, row) ? 0ULL : JOIN_KREC_NULL);
+      if (len > JOIN_ENT_BYTES) {
+        w[0] |= JOIN_ENT_LONG;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int32_t o = 8 * k;
+          w[k + 1] = o < len ? str_word(p + o, len - o < 8 ? len - o : 8) : 0ULL;
+        }
+      }
+      if (inl_width == 8) w[5] = static_cast<const unsigned long long*>(inl)[row];
+      else if (inl_width == 4) w[5] = static_cast<const uint32_t*>(inl)[row];
+    }
+    ulonglong2* e = ent + s * 4;
+    e[0] = sl;
+    e[1] = make_ulonglong2(w[0], w[1]);
+    e[2] = make_ulonglong2(w[2], w[3]);
+    e[3] = make_ulonglong2(w[4], w[5]);
+  }
+}
+
 // sorted_slot[i] starts a segment -> slots[slot].row = i (cnt unchanged)
 __global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulonglong2* slots) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -205,6 +242,7 @@ struct ProbeArgs {
   unsigned long long* total;
   uint32_t* err;
   int any_order;  // tiles reserve their output by one atomicAdd on *total, no look-back
+  int64_t prefetch_ahead;  // one-pass probe: tiles between a CTA and the tile it prefetches into L2 (0: none)
   int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
   const ulonglong2* krec;  // packed build keys (single Utf8 key), or null
 };
@@ -649,7 +687,9 @@ constexpr int AT = AB * AV * 2;    // rows per tile (2048)
 // row in prow): a tile's keys share their top hash bits, so its slot loads
 // stay inside one slice of the table (the partitioned probe of a table
 // larger than L2).
-template <bool DENSE, bool VEC, bool PART>
+// WR: each warp reserves its own output run with one atomicAdd (no
+// barrier, no shared memory) instead of one reservation per CTA.
+template <bool DENSE, bool VEC, bool PART, bool WR = false>
 __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
                                                                 const uint32_t* __restrict__ prow, int64_t n,
                                                                 ProbeArgs a) {
@@ -657,6 +697,17 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   __shared__ unsigned long long s_off;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * AT;
+  if (VEC && a.prefetch_ahead > 0 && threadIdx.x == 0) {
+    // the keys (and rows) of the tile one resident wave ahead, into L2
+    const int64_t pb = base + a.prefetch_ahead * AT;
+    if (pb < n) {
+      const int64_t r = (n - pb < AT ? n - pb : AT) & ~(int64_t)3;
+      if (r) {
+        bulk_prefetch_l2(keys + pb, (uint32_t)(r * 8));
+        if (PART) bulk_prefetch_l2(prow + pb, (uint32_t)(r * 4));
+      }
+    }
+  }
   // positions of this thread: base + 2 * (it * AB + threadIdx.x) + {0, 1}
   uint64_t key[AV][2];
   int64_t row[AV][2];  // probe row of each position
@@ -740,6 +791,40 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   // run (whole sectors) instead of every other position
   uint32_t lpos[AV][2];
   const uint32_t lt = (1u << lane) - 1u;
+  if constexpr (WR) {
+    uint32_t wtot = 0;
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const uint32_t m = __ballot_sync(0xffffffffu, brow[it][j] != NO_MATCH);
+        lpos[it][j] = wtot + __popc(m & lt);
+        wtot += __popc(m);
+      }
+    unsigned long long woff = 0;
+    if (lane == 0 && wtot) woff = atomicAdd(a.total, (unsigned long long)wtot);
+    woff = __shfl_sync(0xffffffffu, woff, 0);
+#pragma unroll
+    for (int it = 0; it < AV; ++it)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (brow[it][j] == NO_MATCH) continue;
+        const uint64_t pos = woff + lpos[it][j];
+        const int64_t r = row[it][j];
+        if (pos >= a.out_capacity) {
+          atomicOr(a.err, DERR_CAPACITY);
+          continue;
+        }
+        if (one8) {
+          if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(a.row_base + r));
+          if (a.out_build) __stcs(a.out_build + pos, brow[it][j]);
+          __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it][j]);
+        } else {
+          emit_one(a, pos, r, brow[it][j]);
+        }
+      }
+    return;
+  }
 #pragma unroll
   for (int it = 0; it < AV; ++it)
 #pragma unroll
@@ -780,6 +865,19 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
         emit_one(a, pos, r, brow[it][j]);
       }
     }
+}
+
+// PRISM_PROBE_WARP_RESERVE=1: one output reservation per warp
+bool any_warp_reserve() {
+  const char* e = std::getenv("PRISM_PROBE_WARP_RESERVE");
+  return e && std::strcmp(e, "1") == 0;
+}
+
+// PRISM_PROBE_PREFETCH=0 turns the one-pass probe's L2 prefetch off
+int64_t any_prefetch_ahead(const Ctx& ctx) {
+  const char* e = std::getenv("PRISM_PROBE_PREFETCH");
+  if (e && std::strcmp(e, "0") == 0) return 0;
+  return (int64_t)ctx.sm_count * 4;  // the resident CTAs: one wave ahead
 }
 
 template <class K, bool EMIT>
@@ -980,6 +1078,30 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   return t;
 }
 
+bool build_key_entries(Ctx& ctx, JoinTable& t, int inline_col) {
+  if (t.int64_fast || t.dense || !t.slots || t.key_cols.size() != 1 || t.build.cols[t.key_cols[0]]->type != TY_UTF8)
+    return false;
+  int w = 0;
+  const void* inl = nullptr;
+  if (inline_col >= 0) {
+    if (inline_col >= (int)t.build.cols.size()) fail(PRISM_ERR_INTERNAL, "inlined build column out of range");
+    const Column& c = *t.build.cols[inline_col];
+    w = width_of(c.type == TY_DICT ? c.index_type : c.type);
+    if (c.validity || c.type == TY_BOOL || (w != 4 && w != 8)) fail(PRISM_ERR_INTERNAL, "column cannot be inlined");
+    inl = c.values;
+  }
+  const uint64_t n_slots = t.capacity + 1;
+  MemP ent = ctx.alloc((size_t)n_slots * 64);
+  KernelTimer kt(ctx, "pack_key_entries_kernel");
+  pack_key_entries_kernel<<<grid_for(ctx, (int64_t)n_slots, 256, 16), 256, 0, ctx.stream>>>(
+      static_cast<const ulonglong2*>(t.slots->ptr), n_slots, t.key_views[0], inl, w,
+      static_cast<ulonglong2*>(ent->ptr));
+  ctx.check_launch("pack_key_entries_kernel");
+  t.key_entries = ent;
+  t.entry_col = inline_col;
+  return true;
+}
+
 int64_t match_upper_bound(const JoinTable& t, int64_t probe_rows) {
   return t.has_dups ? -1 : probe_rows;
 }
@@ -1071,6 +1193,7 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     const int64_t* pk = static_cast<const int64_t*>(probe.cols[keys[0]]->values);
     const bool vec = (reinterpret_cast<uintptr_t>(pk) & 15) == 0;
     const unsigned grid = (unsigned)ceil_div(n, AT);
+    a.prefetch_ahead = any_prefetch_ahead(ctx);
     if (!t.dense && use_partitioned(ctx, t, tune)) {
       // radix-partitioned probe: the keys reordered by the top bits of their
       // slot hash, so each tile probes one slice of the table
@@ -1085,7 +1208,9 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
                                                                              rpart, n, a);
     } else {
       KernelTimer kt(ctx, "probe_emit_any_kernel");
-      if (t.dense)
+      if (t.dense && vec && any_warp_reserve())
+        probe_emit_any_kernel<true, true, false, true><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
+      else if (t.dense)
         vec ? probe_emit_any_kernel<true, true, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a)
             : probe_emit_any_kernel<true, false, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
       else

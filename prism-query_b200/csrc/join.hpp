@@ -29,6 +29,11 @@ struct JoinTable {
   // packed build keys (single Utf8 key of at most JOIN_KREC_MAX bytes per
   // row): 64-byte records per build row, see join_device.cuh
   MemP key_records;
+  // slot entries (single Utf8 key, see join_device.cuh): 64 bytes per slot
+  // with the slot words, the key and the raw value of build column
+  // entry_col (-1: none) for the fused join -> aggregate
+  MemP key_entries;
+  int entry_col = -1;
 };
 
 struct JoinTuning {
@@ -40,6 +45,10 @@ struct JoinTuning {
   int partition = -1;
   int partition_bits = 8;
   bool key_records = true;  // packed build keys for a single Utf8 key column
+  // slot entries instead of row records for the fused join -> aggregate
+  // (single Utf8 key); measured: the same kernel time as the records and a
+  // dearer build (one random key read per slot), so off unless asked for
+  bool key_entries = false;
   // fields the environment set (the tuning table leaves them alone)
   enum : uint32_t { FIX_DENSE = 1, FIX_PARTITION = 2, FIX_LOAD = 4 };
   uint32_t fixed = 0;
@@ -47,6 +56,11 @@ struct JoinTuning {
 
 std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const std::vector<int>& keys,
                                             const JoinTuning& tune);
+
+// Packs the slot entries of a hash table over a single Utf8 key, with the
+// raw values of build column inline_col (fixed width 4 or 8, no nulls; -1:
+// none). Returns false (and builds nothing) for any other table.
+bool build_key_entries(Ctx& ctx, JoinTable& t, int inline_col);
 
 // Output spec of a probe: which index arrays to emit and which fixed-width
 // null-free columns to gather inside the probe kernel.

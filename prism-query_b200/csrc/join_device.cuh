@@ -127,4 +127,72 @@ __device__ __forceinline__ bool join_rec_equal(const DCol& pc, int64_t pr, const
   return true;
 }
 
+// Slot entries of a single Utf8 key (the fused join -> aggregate's table):
+// one 64-byte entry per hash slot, in slot order, so a probe row's lookup
+// is one aligned 64-byte read whose address follows from the row hash alone:
+//   e[0] = {row hash (JOIN_EMPTY: free slot), the slot word cnt << 32 | row}
+//   e[1] = {key length | bit 63 null | bit 62 longer than JOIN_ENT_BYTES, key bytes 0..7}
+//   e[2] = {key bytes 8..15, 16..23}
+//   e[3] = {key bytes 24..31, the raw value of one fixed-width build column at row}
+// Bytes past the key's length are zero. A slot with several build rows
+// (cnt > 1) keeps only the slot words; its rows are compared against the
+// column.
+constexpr uint64_t JOIN_ENT_LONG = 1ULL << 62;
+constexpr int JOIN_ENT_BYTES = 32;
+
+// A probe key of a Utf8 column as the entries hold it: the length word
+// (bit 63: null) and the first JOIN_ENT_BYTES bytes as little-endian words,
+// zero above the length. The bytes come from independent aligned 8-byte
+// loads of only the words that hold a byte of the key.
+struct JoinKeyWords {
+  uint64_t len;  // length | JOIN_KREC_NULL
+  uint64_t w[4];
+};
+
+// false (k unset) for a key longer than JOIN_ENT_BYTES
+__device__ __forceinline__ bool join_key_words(const DCol& c, int64_t i, JoinKeyWords& k) {
+  const int32_t a = c.offsets[i], n = c.offsets[i + 1] - a;
+  if (n < 0 || n > JOIN_ENT_BYTES) return false;
+  const uint8_t* p = c.data + a;
+  const uint32_t al = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 7);
+  const uint64_t* q = reinterpret_cast<const uint64_t*>(p - al);
+  const int32_t nw = (int32_t)(al + n + 7) >> 3;  // at most 5
+  uint64_t x[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) x[j] = j < nw ? q[j] : 0ULL;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint64_t v = al ? (x[j] >> (8 * al)) | (x[j + 1] << (64 - 8 * al)) : x[j];
+    const int32_t rem = n - 8 * j;
+    k.w[j] = rem >= 8 ? v : rem > 0 ? v & ((1ULL << (8 * rem)) - 1) : 0ULL;
+  }
+  k.len = (uint64_t)(uint32_t)n | (dcol_valid(c, i) ? 0ULL : JOIN_KREC_NULL);
+  return true;
+}
+
+// join_key_hash of a single Utf8 key from its words (fx_str over the
+// zero-padded words is fx_str over the bytes)
+__device__ __forceinline__ uint64_t join_words_hash(const JoinKeyWords& k) {
+  const int32_t n = (int32_t)(uint32_t)k.len;
+  uint64_t w;
+  if (k.len & JOIN_KREC_NULL) {
+    w = 0x6a09e667f3bcc909ULL;
+  } else {
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (8 * j < n) s = fx_word(s, k.w[j]);
+    w = fx_word(s, 0xff);
+  }
+  const uint64_t h = mix64(0x2545F4914F6CDD1DULL ^ w) + JOIN_FIB;
+  return h == JOIN_EMPTY ? JOIN_EMPTY + 1 : h;
+}
+
+// keys_equal of a probe key's words against an entry with cnt == 1 and no
+// JOIN_ENT_LONG flag (both sides zero-padded)
+__device__ __forceinline__ bool join_words_equal(const JoinKeyWords& k, const ulonglong2& e1, const ulonglong2& e2,
+                                                 const ulonglong2& e3) {
+  return k.len == e1.x && k.w[0] == e1.y && k.w[1] == e2.x && k.w[2] == e2.y && k.w[3] == e3.x;
+}
+
 }  // namespace prism

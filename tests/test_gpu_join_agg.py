@@ -210,3 +210,28 @@ def test_fused_equals_materialized(prof, tmp_path):
     for name, (cols, exprs, agg) in AGGS.items():
         got = prism_gpu.join_aggregate(probes, build, [0], [0], cols, exprs, agg, ctx=prof)
         assert_batches_equal(got, materialized[name], float_cols=float_cols(got))
+
+
+@pytest.mark.parametrize("long_keys", [False, True])
+@pytest.mark.parametrize("dups", [False, True])
+def test_utf8_slot_entries(prof, monkeypatch, long_keys, dups):
+    """The opt-in 64-byte slot entries (PRISM_JOIN_KEY_ENTRIES=1): keys of
+    up to 32 bytes compared inside the entry, longer ones (up to 48 here)
+    against the column, slots of several build rows through the row list,
+    null keys on both sides, and the group_id column (no nulls) read from the
+    entries."""
+    monkeypatch.setenv("PRISM_JOIN_KEY_ENTRIES", "1")
+    rng = np.random.default_rng(77)
+    nb = 20_000
+    ids = rng.integers(0, nb // 3, nb) if dups else np.arange(nb)
+    pad = 40 if long_keys else 13
+    keys = pa.array([f"k{i:07d}{'q' * (i % pad)}" for i in ids], mask=rng.random(nb) < 0.02)
+    build = pa.RecordBatch.from_arrays(
+        [keys, pa.array(rng.integers(0, 25, nb).astype(np.int32)), pa.array(rng.lognormal(0, 1, nb)),
+         pa.array(np.array(["x", "y", "zz", ""])[rng.integers(0, 4, nb)])],
+        names=["key", "group_id", "weight", "tag"])
+    probes = [probe_side(30_000, nb, 40 + k, build) for k in range(2)]
+    for spec in (AGG_BUILD_KEY, AGG_TWO_SIDES):
+        got, ref, ran = run(prof, probes, build, spec)
+        assert ran == len(probes)
+        assert_batches_equal(got, ref, float_cols=float_cols(ref))
