@@ -736,8 +736,8 @@ class C4:
 
     def roofline(self, kstats):
         names = ("probe_kernel", "probe_rows_kernel", "emit_rows_kernel", "insert_kernel", "pack_key_records_kernel",
-                 "pack_key_entries_kernel", "build_partition_hist_kernel", "build_partition_scatter_kernel",
-                 "agg_kernel", "agg_tiny_jit", "agg_hash_jit", "join_agg_jit")
+                 "pack_key_entries_kernel", "match_rows_kernel", "build_partition_hist_kernel", "build_partition_scatter_kernel",
+                 "match_rows_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit", "join_agg_jit")
         ms = sum(kstats.get(k, (0, 0.0))[1] for k in names)
         steps = max(1, kstats.get("insert_kernel", (1, 0.0))[0])
         kb = int(self.bo32[-1].item()) + sum(int(k[0][-1].item()) for k in self.keep)
@@ -1047,7 +1047,7 @@ def run_workload(args, rank, world, local, torch, dist):
     ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = ctx.kernel_launches - launches0
     names = ("probe_rows_kernel", "emit_rows_kernel", "probe_kernel", "insert_kernel", "pack_key_records_kernel",
-             "pack_key_entries_kernel", "build_partition_hist_kernel", "build_partition_scatter_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
+             "pack_key_entries_kernel", "match_rows_kernel", "build_partition_hist_kernel", "build_partition_scatter_kernel", "agg_kernel", "agg_tiny_jit", "agg_hash_jit",
              "join_agg_jit", "predicate_kernel", "expr_kernel", "radix_scatter_kernel", "select_hist_kernel",
              "pq_snappy_kernel", "pq_page_kernel", "pq_copy_kernel", "pq_dict_kernel", "pq_positions_kernel")
     kstats = {k: ctx.kernel_stats(k) for k in names}

@@ -34,6 +34,13 @@ namespace prism {
 
 namespace {
 
+// PRISM_JOIN_SPLIT=0: the fused join -> aggregate over a Utf8 key looks its
+// keys up itself instead of reading match_rows_kernel's per-row match words
+bool join_split() {
+  const char* e = std::getenv("PRISM_JOIN_SPLIT");
+  return !(e && std::strcmp(e, "0") == 0);
+}
+
 struct RowVals {
   double f[MAX_SRC];
   __int128 i[MAX_SRC];
@@ -1130,6 +1137,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
     uint64_t row_base = 0;
     std::vector<Program> progs;
     progs.reserve(batches.size());
+    std::vector<MemP> split_mem;  // per-batch match words of the split join, alive until the kernels ran
     for (auto* bp : batches) {
       const Batch& b = *bp;
       if (b.rows == 0) continue;
@@ -1191,6 +1199,30 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
                          b.cols[join->probe_keys[0]]->type == TY_UTF8;
         a.jent = ent ? static_cast<const ulonglong2*>(t.key_entries->ptr) : nullptr;
         a.jent_col = ent && t.entry_col >= 0 ? n_probe_cols + t.entry_col : -1;
+        a.jmatch = nullptr;
+        a.jinl = nullptr;
+        a.jinl_w = 0;
+        if (join_split() && join->probe_keys.size() == 1) {
+          // split: the lookups by match_rows_kernel (many rows in flight),
+          // then the fused kernel aggregates from its per-row match words
+          MemP mm = ctx.alloc((size_t)b.rows * 4);
+          int iw = 0;
+          if (join->inline_col >= 0) {
+            const Column& ic = *t.build.cols[join->inline_col];
+            iw = width_of(ic.type == TY_DICT ? ic.index_type : ic.type);
+          }
+          MemP mi = iw ? ctx.alloc((size_t)b.rows * iw) : MemP();
+          if (match_rows_utf8(ctx, t, *b.cols[join->probe_keys[0]], b.rows, join->inline_col,
+                              static_cast<uint32_t*>(mm->ptr), mi ? mi->ptr : nullptr)) {
+            a.jent = nullptr;  // the lookup is done; the kernel reads the match words
+            a.jmatch = static_cast<const uint32_t*>(mm->ptr);
+            a.jinl = mi ? mi->ptr : nullptr;
+            a.jinl_w = iw;
+            a.jent_col = join->inline_col >= 0 ? n_probe_cols + join->inline_col : -1;
+            split_mem.push_back(mm);
+            if (mi) split_mem.push_back(mi);
+          }
+        }
         a.jnkeys = (int)join->probe_keys.size();
         a.n_cols = (int)pg.cols.size();
         if (A.wide) fused_fail("a Float64 sum beyond the 192-bit window over a join");

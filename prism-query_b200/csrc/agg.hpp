@@ -35,6 +35,9 @@ struct JoinTable;
 struct JoinAggSpec {
   const JoinTable* table = nullptr;
   std::vector<int> probe_keys;
+  // build column whose values the lookup hands to the kernel per probe row
+  // (fixed width 4 or 8, no nulls, referenced by the projection), or -1
+  int inline_col = -1;
 };
 
 // Aggregates `batches` (all with one schema). When `pred`/`exprs` are given

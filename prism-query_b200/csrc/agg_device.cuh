@@ -95,7 +95,13 @@ struct AggArgs {
   const DCol* jbk;           // build key column views
   const ulonglong2* jkrec;   // packed build keys (single Utf8 key), or null
   const ulonglong2* jent;    // slot entries (single Utf8 key), or null
-  int32_t jent_col;          // joined column whose value the entries carry, or -1
+  int32_t jent_col;          // joined column whose value the entries (or jinl) carry, or -1
+  // split join -> aggregate: per probe row the match word written by
+  // match_rows_kernel (verified build row, JOIN_NO_MATCH, or
+  // JOIN_MATCH_SLOT | slot of several build rows) and the inlined value
+  const uint32_t* jmatch;
+  const void* jinl;
+  int32_t jinl_w;            // 4 or 8 bytes per row, 0: none
   int32_t jnkeys;
   uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
   unsigned long long* gnew_count;  // length of gnew
@@ -688,7 +694,7 @@ __device__ __forceinline__ void hash_body(const AggArgs& a) {
 // into the block's table. The order key of a joined row is
 // (global probe row << 32 | build row), which sorts like the joined rows'
 // positions (probe rows ascending, build rows ascending inside one).
-template <class E, int NOPS, int BLOCK, int R, bool ENT>
+template <class E, int NOPS, int BLOCK, int R, bool ENT, bool MATCH = false>
 __device__ __forceinline__ void join_body(const AggArgs& a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ DCol scols[TINY_MAX_COLS];
@@ -714,7 +720,7 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
     JoinKeyWords kw[ENT ? R : 1];
     bool kw_ok[ENT ? R : 1];
     bool keq[R];
-    unsigned long long inl[ENT ? R : 1];
+    unsigned long long inl[ENT || MATCH ? R : 1];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
@@ -726,12 +732,33 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
         kw_ok[r] = idx < n && join_key_words(a.jpk[0], idx, kw[r]);
         if (kw_ok[r]) key[r] = join_words_hash(kw[r]);
         else if (idx < n) key[r] = join_key_hash(a.jpk, a.jnkeys, idx);
-      } else if (idx < n) {
+      } else if (!MATCH && idx < n) {
         key[r] = a.jfast ? (uint64_t)static_cast<const int64_t*>(a.jpk[0].values)[idx]
                          : join_key_hash(a.jpk, a.jnkeys, idx);
       }
     }
-    if constexpr (ENT) {
+    if constexpr (MATCH) {
+      // the lookup is done: one coalesced word per row (and its inlined
+      // value); a slot of several build rows is expanded below
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        inl[r] = 0;
+        if (idx >= n) continue;
+        const uint32_t m = __ldcs(a.jmatch + idx);
+        if (m == JOIN_NO_MATCH) continue;
+        if (m & JOIN_MATCH_SLOT) {
+          const ulonglong2 sl = __ldg(a.jslots + (m & ~JOIN_MATCH_SLOT));
+          cand[r] = (uint32_t)sl.y;
+          cnt[r] = (uint32_t)(sl.y >> 32);
+        } else {
+          cand[r] = m;
+          cnt[r] = 1;
+          if (a.jinl_w == 8) inl[r] = __ldcs(static_cast<const unsigned long long*>(a.jinl) + idx);
+          else if (a.jinl_w == 4) inl[r] = __ldcs(static_cast<const uint32_t*>(a.jinl) + idx);
+        }
+      }
+    } else if constexpr (ENT) {
       ulonglong2 e1[R], e2[R], e3[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -808,13 +835,13 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
       if (cnt[r] == 1) {
-        if constexpr (ENT) rows[r] = E::fetch(cols, idx, (I)cand[r], inl[r], true);
+        if constexpr (ENT || MATCH) rows[r] = E::fetch(cols, idx, (I)cand[r], inl[r], true);
         else rows[r] = E::fetch(cols, idx, (I)cand[r]);
       }
     }
     // packed build keys: every single-candidate row's key compared up front
     // (the R record loads in flight together, beside the fetches above)
-    if constexpr (!ENT) {
+    if constexpr (!ENT && !MATCH) {  // (match_rows_kernel verified its single-row matches)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const I idx = base + r * stride;
@@ -827,7 +854,7 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
       for (uint32_t j = 0; j < cnt[r]; ++j) {
         const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
         if (!a.jfast) {
-          const bool eq = cnt[r] == 1 && (ENT || a.jkrec) ? keq[r]
+          const bool eq = cnt[r] == 1 && (ENT || MATCH || a.jkrec) ? keq[r]
                           : a.jkrec                       ? join_rec_equal(a.jpk[0], idx, a.jkrec, b)
                                                           : join_rows_equal(a.jpk, a.jbk, a.jnkeys, idx, b);
           if (!eq) continue;

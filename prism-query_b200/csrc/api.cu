@@ -413,23 +413,23 @@ Batch join_aggregate_impl(Ctx& x, const std::vector<const Batch*>& probes, const
       }
     }
   }
-  if (entries) {
-    // the first referenced build column of fixed width 4 or 8 without
-    // nulls rides in the entries (read there for single-row slots)
-    int inl = -1;
-    for (int c = 0; c < (int)bb.cols.size() && inl < 0; ++c) {
-      const Column& col = *bb.cols[c];
-      const int w = width_of(col.type == TY_DICT ? col.index_type : col.type);
-      if (need[np + c] && !col.validity && col.type != TY_BOOL && (w == 4 || w == 8)) inl = c;
-    }
-    build_key_entries(x, *t, inl);
+  // the first referenced build column of fixed width 4 or 8 without nulls
+  // rides with the lookup (in the slot entries, or per probe row from the
+  // split lookup) and is read from there for single-row slots
+  int inl = -1;
+  for (int c = 0; c < (int)bb.cols.size() && inl < 0; ++c) {
+    const Column& col = *bb.cols[c];
+    const int w = width_of(col.type == TY_DICT ? col.index_type : col.type);
+    if (need[np + c] && !col.validity && col.type != TY_BOOL && (w == 4 || w == 8)) inl = c;
   }
+  if (entries) build_key_entries(x, *t, inl);
   if (join_agg_fused()) {
     // one kernel per probe batch: lookup, projection and aggregation of
     // the joined rows without materializing them
     JoinAggSpec js;
     js.table = t.get();
     js.probe_keys = pk;
+    js.inline_col = inl;
     try {
       return aggregate(x, probes, *agg, nullptr, cols, n_cols, exprs, n_exprs, PRISM_ARITH_F64, true, tune, &js);
     } catch (const Failure& f) {

@@ -935,7 +935,8 @@ std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKerne
   if (n_probe_cols >= 0)
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.block << ", " << join.min_blocks
       << ") prism_join_agg(prism::AggArgs a) {\n  prism::join_body<prism::QueryRow, " << a.n_ops << ", " << join.block
-      << ", " << join.rows << ", " << (a.jent ? "true" : "false") << ">(a);\n}\n";
+      << ", " << join.rows << ", " << (a.jent ? "true" : "false") << ", " << (a.jmatch ? "true" : "false")
+      << ">(a);\n}\n";
   else
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.hash_block << ", 1) prism_hash_agg(prism::AggArgs a) {\n"
          "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", " << join.hash_block << ">(a);\n}\n";
@@ -989,7 +990,7 @@ std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs
   if (n_probe_cols >= 0)
     for (size_t s = 0; s < pg.cols.size(); ++s) {
       gen.bside.push_back(pg.cols[s] >= n_probe_cols ? 1 : 0);
-      if (a.jent && a.jent_col >= 0 && pg.cols[s] == a.jent_col) gen.inl_slot = (int)s;
+      if ((a.jent || a.jmatch) && a.jent_col >= 0 && pg.cols[s] == a.jent_col) gen.inl_slot = (int)s;
     }
   RowParts rp = row_parts(gen, a);
   if (!rp.ok) return "";

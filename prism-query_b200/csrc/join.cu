@@ -201,6 +201,159 @@ __global__ void pack_key_entries_kernel(const ulonglong2* __restrict__ slots, ui
   }
 }
 
+// ------------------------------------- per-row match of a Utf8 probe key --
+// The first half of the split join -> aggregate over a single Utf8 key: one
+// pass over a probe batch writes, per probe row, the build row whose key
+// equals its key (verified), or JOIN_NO_MATCH, or JOIN_MATCH_SLOT | slot for
+// a slot of several build rows (the aggregation compares those rows
+// itself); and the raw value of one fixed-width build column at the matched
+// row (IW bytes, 0 for none). Each thread keeps MR rows in flight through
+// the whole lookup with only their hash and slot words live (the key words
+// are read again for the verification, from L1 / L2), so an SM has 4,096
+// lookups outstanding where the fused kernel's per-row state allows
+// 1,024-2,048.
+constexpr int MB = 256;  // threads per CTA
+constexpr int MR = 4;    // rows per thread
+
+// over the hash slots and the row records (packed key records)
+template <int IW>
+__global__ void __launch_bounds__(MB, 4) match_rows_kernel(DCol pk, int64_t n, const ulonglong2* __restrict__ slots,
+                                                           int shift, uint64_t mask, const ulonglong2* __restrict__ rec,
+                                                           const void* __restrict__ inl, uint32_t* __restrict__ out_match,
+                                                           void* __restrict__ out_inl) {
+  const int64_t base = (int64_t)blockIdx.x * (MB * MR) + threadIdx.x;
+  uint64_t h[MR], s[MR];
+  ulonglong2 e[MR];
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    JoinKeyWords kw;
+    h[k] = 0;
+    if (idx < n) h[k] = join_key_words(pk, idx, kw) ? join_words_hash(kw) : join_key_hash(&pk, 1, idx);
+  }
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    s[k] = join_slot_of(h[k], shift);
+    e[k] = idx < n ? __ldg(slots + s[k]) : make_ulonglong2(JOIN_EMPTY, 0);
+  }
+  uint32_t m[MR];
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    m[k] = JOIN_NO_MATCH;
+    if (idx >= n) continue;
+    for (uint64_t steps = 0; e[k].x != h[k] && e[k].x != JOIN_EMPTY && steps <= mask; ++steps) {
+      s[k] = (s[k] + 1) & mask;
+      e[k] = __ldg(slots + s[k]);
+    }
+    if (e[k].x != h[k]) continue;
+    const uint32_t row = (uint32_t)e[k].y, cnt = (uint32_t)(e[k].y >> 32);
+    if (cnt != 1) {
+      m[k] = JOIN_MATCH_SLOT | (uint32_t)s[k];
+      continue;
+    }
+    JoinKeyWords kw;
+    bool eq;
+    if (join_key_words(pk, idx, kw)) {
+      // record words 0..4: length, key bytes 0..31 (zero past the length)
+      const ulonglong2* r = rec + (size_t)row * 4;
+      const ulonglong2 r0 = __ldg(r), r1 = __ldg(r + 1);
+      eq = r0.x == kw.len && r0.y == kw.w[0] && r1.x == kw.w[1] && r1.y == kw.w[2];
+      if (eq && (uint32_t)kw.len > 24) eq = __ldg(r + 2).x == kw.w[3];
+    } else {
+      eq = join_rec_equal(pk, idx, rec, row);
+    }
+    if (eq) m[k] = row;
+  }
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    if (idx >= n) continue;
+    __stcs(out_match + idx, m[k]);
+    if (IW == 4)
+      __stcs(static_cast<uint32_t*>(out_inl) + idx,
+             m[k] < JOIN_MATCH_SLOT ? __ldg(static_cast<const uint32_t*>(inl) + m[k]) : 0u);
+    if (IW == 8)
+      __stcs(static_cast<unsigned long long*>(out_inl) + idx,
+             m[k] < JOIN_MATCH_SLOT ? __ldg(static_cast<const unsigned long long*>(inl) + m[k]) : 0ULL);
+  }
+}
+
+// over the 64-byte slot entries: one entry's first sector (row hash, slot
+// word, length word, first key word) per row, the rest only for a row whose
+// hash and length match; the inlined build value from the entry's last
+// word. One random DRAM fetch per probe row instead of three (slot,
+// record, column).
+template <int IW>
+__global__ void __launch_bounds__(MB, 4) match_entries_kernel(DCol pk, DCol bk, int64_t n,
+                                                              const ulonglong2* __restrict__ ent, int shift,
+                                                              uint64_t mask, uint32_t* __restrict__ out_match,
+                                                              void* __restrict__ out_inl) {
+  const int64_t base = (int64_t)blockIdx.x * (MB * MR) + threadIdx.x;
+  uint64_t h[MR], s[MR];
+  ulonglong2 e0[MR], e1[MR];
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    JoinKeyWords kw;
+    h[k] = 0;
+    if (idx < n) h[k] = join_key_words(pk, idx, kw) ? join_words_hash(kw) : join_key_hash(&pk, 1, idx);
+  }
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    s[k] = join_slot_of(h[k], shift);
+    e0[k] = make_ulonglong2(JOIN_EMPTY, 0);
+    e1[k] = make_ulonglong2(0, 0);
+    if (idx < n) {
+      e0[k] = __ldg(ent + 4 * s[k]);
+      e1[k] = __ldg(ent + 4 * s[k] + 1);
+    }
+  }
+  uint32_t m[MR];
+  unsigned long long v[MR];
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    m[k] = JOIN_NO_MATCH;
+    v[k] = 0;
+    if (idx >= n) continue;
+    for (uint64_t steps = 0; e0[k].x != h[k] && e0[k].x != JOIN_EMPTY && steps <= mask; ++steps) {
+      s[k] = (s[k] + 1) & mask;
+      e0[k] = __ldg(ent + 4 * s[k]);
+      e1[k] = __ldg(ent + 4 * s[k] + 1);
+    }
+    if (e0[k].x != h[k]) continue;
+    const uint32_t row = (uint32_t)e0[k].y, cnt = (uint32_t)(e0[k].y >> 32);
+    if (cnt != 1) {
+      m[k] = JOIN_MATCH_SLOT | (uint32_t)s[k];
+      continue;
+    }
+    JoinKeyWords kw;
+    bool eq;
+    if (e1[k].x & JOIN_ENT_LONG) {
+      eq = join_rows_equal(&pk, &bk, 1, idx, row);  // a build key longer than the entry holds
+      v[k] = __ldg(ent + 4 * s[k] + 3).y;
+    } else if (join_key_words(pk, idx, kw) && kw.len == e1[k].x && kw.w[0] == e1[k].y) {
+      const ulonglong2 e2 = __ldg(ent + 4 * s[k] + 2), e3 = __ldg(ent + 4 * s[k] + 3);
+      eq = join_words_equal(kw, e1[k], e2, e3);
+      v[k] = e3.y;
+    } else {
+      eq = false;  // a probe key longer than any entry's, or another length / first word
+    }
+    if (eq) m[k] = row;
+  }
+#pragma unroll
+  for (int k = 0; k < MR; ++k) {
+    const int64_t idx = base + k * MB;
+    if (idx >= n) continue;
+    __stcs(out_match + idx, m[k]);
+    if (IW == 4) __stcs(static_cast<uint32_t*>(out_inl) + idx, m[k] < JOIN_MATCH_SLOT ? (uint32_t)v[k] : 0u);
+    if (IW == 8) __stcs(static_cast<unsigned long long*>(out_inl) + idx, m[k] < JOIN_MATCH_SLOT ? v[k] : 0ULL);
+  }
+}
+
 // sorted_slot[i] starts a segment -> slots[slot].row = i (cnt unchanged)
 __global__ void segment_heads_kernel(const uint32_t* sorted_slot, int64_t n, ulonglong2* slots) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -687,9 +840,7 @@ constexpr int AT = AB * AV * 2;    // rows per tile (2048)
 // row in prow): a tile's keys share their top hash bits, so its slot loads
 // stay inside one slice of the table (the partitioned probe of a table
 // larger than L2).
-// WR: each warp reserves its own output run with one atomicAdd (no
-// barrier, no shared memory) instead of one reservation per CTA.
-template <bool DENSE, bool VEC, bool PART, bool WR = false>
+template <bool DENSE, bool VEC, bool PART>
 __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
                                                                 const uint32_t* __restrict__ prow, int64_t n,
                                                                 ProbeArgs a) {
@@ -791,40 +942,6 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   // run (whole sectors) instead of every other position
   uint32_t lpos[AV][2];
   const uint32_t lt = (1u << lane) - 1u;
-  if constexpr (WR) {
-    uint32_t wtot = 0;
-#pragma unroll
-    for (int it = 0; it < AV; ++it)
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const uint32_t m = __ballot_sync(0xffffffffu, brow[it][j] != NO_MATCH);
-        lpos[it][j] = wtot + __popc(m & lt);
-        wtot += __popc(m);
-      }
-    unsigned long long woff = 0;
-    if (lane == 0 && wtot) woff = atomicAdd(a.total, (unsigned long long)wtot);
-    woff = __shfl_sync(0xffffffffu, woff, 0);
-#pragma unroll
-    for (int it = 0; it < AV; ++it)
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        if (brow[it][j] == NO_MATCH) continue;
-        const uint64_t pos = woff + lpos[it][j];
-        const int64_t r = row[it][j];
-        if (pos >= a.out_capacity) {
-          atomicOr(a.err, DERR_CAPACITY);
-          continue;
-        }
-        if (one8) {
-          if (a.out_probe) __stcs(a.out_probe + pos, (uint32_t)(a.row_base + r));
-          if (a.out_build) __stcs(a.out_build + pos, brow[it][j]);
-          __stcs(static_cast<unsigned long long*>(a.g_dst[0]) + pos, pre[it][j]);
-        } else {
-          emit_one(a, pos, r, brow[it][j]);
-        }
-      }
-    return;
-  }
 #pragma unroll
   for (int it = 0; it < AV; ++it)
 #pragma unroll
@@ -865,12 +982,6 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
         emit_one(a, pos, r, brow[it][j]);
       }
     }
-}
-
-// PRISM_PROBE_WARP_RESERVE=1: one output reservation per warp
-bool any_warp_reserve() {
-  const char* e = std::getenv("PRISM_PROBE_WARP_RESERVE");
-  return e && std::strcmp(e, "1") == 0;
 }
 
 // PRISM_PROBE_PREFETCH=0 turns the one-pass probe's L2 prefetch off
@@ -1102,6 +1213,51 @@ bool build_key_entries(Ctx& ctx, JoinTable& t, int inline_col) {
   return true;
 }
 
+bool match_rows_utf8(Ctx& ctx, const JoinTable& t, const Column& pkey, int64_t n, int inline_col, uint32_t* out_match,
+                     void* out_inl) {
+  const bool ent = t.key_entries && t.entry_col == inline_col;
+  if (t.int64_fast || t.dense || !t.slots || !(t.key_records || ent) || t.key_cols.size() != 1 ||
+      t.build.cols[t.key_cols[0]]->type != TY_UTF8 || pkey.type != TY_UTF8 || t.capacity >= JOIN_MATCH_SLOT ||
+      (uint64_t)t.build.rows >= JOIN_MATCH_SLOT)
+    return false;
+  int w = 0;
+  const void* inl = nullptr;
+  if (inline_col >= 0) {
+    const Column& c = *t.build.cols.at(inline_col);
+    w = width_of(c.type == TY_DICT ? c.index_type : c.type);
+    if (c.validity || c.type == TY_BOOL || (w != 4 && w != 8)) fail(PRISM_ERR_INTERNAL, "column cannot be inlined");
+    inl = c.values;
+  }
+  if (n <= 0) return true;
+  const unsigned grid = (unsigned)ceil_div(n, (int64_t)MB * MR);
+  const int shift = 64 - t.log2cap;
+  const uint64_t mask = t.capacity - 1;
+  const DCol pk = pkey.view();
+  KernelTimer kt(ctx, "match_rows_kernel");
+  if (ent) {
+    const ulonglong2* e = static_cast<const ulonglong2*>(t.key_entries->ptr);
+    const DCol bk = t.key_views[0];
+    if (w == 8)
+      match_entries_kernel<8><<<grid, MB, 0, ctx.stream>>>(pk, bk, n, e, shift, mask, out_match, out_inl);
+    else if (w == 4)
+      match_entries_kernel<4><<<grid, MB, 0, ctx.stream>>>(pk, bk, n, e, shift, mask, out_match, out_inl);
+    else
+      match_entries_kernel<0><<<grid, MB, 0, ctx.stream>>>(pk, bk, n, e, shift, mask, out_match, out_inl);
+    ctx.check_launch("match_entries_kernel");
+    return true;
+  }
+  const ulonglong2* slots = static_cast<const ulonglong2*>(t.slots->ptr);
+  const ulonglong2* rec = static_cast<const ulonglong2*>(t.key_records->ptr);
+  if (w == 8)
+    match_rows_kernel<8><<<grid, MB, 0, ctx.stream>>>(pk, n, slots, shift, mask, rec, inl, out_match, out_inl);
+  else if (w == 4)
+    match_rows_kernel<4><<<grid, MB, 0, ctx.stream>>>(pk, n, slots, shift, mask, rec, inl, out_match, out_inl);
+  else
+    match_rows_kernel<0><<<grid, MB, 0, ctx.stream>>>(pk, n, slots, shift, mask, rec, inl, out_match, out_inl);
+  ctx.check_launch("match_rows_kernel");
+  return true;
+}
+
 int64_t match_upper_bound(const JoinTable& t, int64_t probe_rows) {
   return t.has_dups ? -1 : probe_rows;
 }
@@ -1208,9 +1364,7 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
                                                                              rpart, n, a);
     } else {
       KernelTimer kt(ctx, "probe_emit_any_kernel");
-      if (t.dense && vec && any_warp_reserve())
-        probe_emit_any_kernel<true, true, false, true><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
-      else if (t.dense)
+      if (t.dense)
         vec ? probe_emit_any_kernel<true, true, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a)
             : probe_emit_any_kernel<true, false, false><<<grid, AB, 0, ctx.stream>>>(pk, nullptr, n, a);
       else

@@ -62,6 +62,16 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
 // none). Returns false (and builds nothing) for any other table.
 bool build_key_entries(Ctx& ctx, JoinTable& t, int inline_col);
 
+// The first half of the split join -> aggregate (hash table over a single
+// Utf8 key with packed key records or slot entries, Utf8 probe key): per
+// probe row of `pkey` (n rows) the verified build row, JOIN_NO_MATCH, or
+// JOIN_MATCH_SLOT | slot for a slot of several build rows, into out_match;
+// and the raw value of build column inline_col (fixed width 4 or 8, no
+// nulls; -1: none) at the matched row into out_inl. Returns false (nothing
+// launched) for any other table.
+bool match_rows_utf8(Ctx& ctx, const JoinTable& t, const Column& pkey, int64_t n, int inline_col, uint32_t* out_match,
+                     void* out_inl);
+
 // Output spec of a probe: which index arrays to emit and which fixed-width
 // null-free columns to gather inside the probe kernel.
 struct ProbeGather {

@@ -15,6 +15,9 @@
 namespace prism {
 
 constexpr uint64_t JOIN_EMPTY = 0x8000000000000000ULL;  // empty slot (an Int64 key equal to it takes the side slot)
+// per-row match word of the split join -> aggregate: a verified build row,
+// JOIN_NO_MATCH, or this bit | the slot of several build rows
+constexpr uint32_t JOIN_MATCH_SLOT = 0x80000000u;
 constexpr uint64_t JOIN_FIB = 0x9E3779B97F4A7C15ULL;
 constexpr uint32_t JOIN_NO_MATCH = 0xFFFFFFFFu;
 

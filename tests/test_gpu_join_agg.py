@@ -235,3 +235,38 @@ def test_utf8_slot_entries(prof, monkeypatch, long_keys, dups):
         got, ref, ran = run(prof, probes, build, spec)
         assert ran == len(probes)
         assert_batches_equal(got, ref, float_cols=float_cols(ref))
+
+
+@pytest.mark.parametrize("dups", [False, True])
+def test_utf8_unsplit_lookup(prof, monkeypatch, dups):
+    """PRISM_JOIN_SPLIT=0: the fused kernel looks Utf8 keys up itself (the
+    default splits the lookup into match_rows_kernel's per-row match words)."""
+    monkeypatch.setenv("PRISM_JOIN_SPLIT", "0")
+    build = build_side(20_000, 5, "utf8", dups, nulls=True)
+    probes = [probe_side(30_000, 20_000, 60 + k, build, nulls=True) for k in range(2)]
+    for spec in (AGG_BUILD_KEY, AGG_TWO_SIDES, AGG_GLOBAL):
+        before = prof.kernel_stats("match_rows_kernel")[0]
+        got, ref, ran = run(prof, probes, build, spec)
+        assert ran == len(probes)
+        assert prof.kernel_stats("match_rows_kernel")[0] == before
+        assert_batches_equal(got, ref, float_cols=float_cols(ref))
+
+
+@pytest.mark.parametrize("entries", ["0", "1"])
+def test_utf8_split_lookup_runs(prof, monkeypatch, entries):
+    """The default Utf8 path: one match_rows_kernel launch per probe batch
+    (over the row records, or over the slot entries), group_id handed over
+    per row (no nulls, so inlined); keys of 10-39 bytes, so some are longer
+    than an entry holds."""
+    monkeypatch.setenv("PRISM_JOIN_KEY_ENTRIES", entries)
+    rng = np.random.default_rng(91)
+    nb = 10_000
+    build = pa.RecordBatch.from_arrays(
+        [pa.array([f"key-{i:06d}{'z' * (i % 30)}" for i in range(nb)]),
+         pa.array(rng.integers(0, 25, nb).astype(np.int32)), pa.array(rng.lognormal(0, 1, nb)),
+         pa.array(np.array(["x", "y"])[rng.integers(0, 2, nb)])], names=["key", "group_id", "weight", "tag"])
+    probes = [probe_side(25_000, nb, 70 + k, build) for k in range(3)]
+    before = prof.kernel_stats("match_rows_kernel")[0]
+    got, ref, ran = run(prof, probes, build, AGG_BUILD_KEY)
+    assert prof.kernel_stats("match_rows_kernel")[0] - before == len(probes)
+    assert_batches_equal(got, ref, float_cols=float_cols(ref))
