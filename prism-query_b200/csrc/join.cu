@@ -201,6 +201,54 @@ __global__ void pack_key_entries_kernel(const ulonglong2* __restrict__ slots, ui
   }
 }
 
+// Row hashes of M probe rows of a Utf8 column (idx[k] >= n: none), with the
+// loads of all M rows in flight together: first every row's two offsets,
+// then every row's key words (keys of at most JOIN_ENT_BYTES bytes), then
+// the hashes. join_key_words per row would wait for each row's offsets
+// before loading its words, one row after another.
+template <int M>
+__device__ __forceinline__ void hash_utf8_rows(const DCol& pk, const int64_t (&idx)[M], int64_t n, uint64_t (&h)[M]) {
+  int32_t ka[M], kn[M];
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    ka[k] = 0;
+    kn[k] = 0;
+    if (idx[k] < n) {
+      ka[k] = pk.offsets[idx[k]];
+      kn[k] = pk.offsets[idx[k] + 1] - ka[k];
+    }
+  }
+  uint64_t x[M][5];
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const uint8_t* p = pk.data + ka[k];
+    const uint32_t al = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 7);
+    const uint64_t* q = reinterpret_cast<const uint64_t*>(p - al);
+    const int32_t nw = idx[k] < n && kn[k] >= 0 && kn[k] <= JOIN_ENT_BYTES ? (int32_t)(al + kn[k] + 7) >> 3 : 0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) x[k][j] = j < nw ? q[j] : 0ULL;
+  }
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    h[k] = 0;
+    if (idx[k] >= n) continue;
+    if (kn[k] < 0 || kn[k] > JOIN_ENT_BYTES) {
+      h[k] = join_key_hash(&pk, 1, idx[k]);  // a long key: the general hash
+      continue;
+    }
+    const uint32_t al = (uint32_t)(reinterpret_cast<uintptr_t>(pk.data + ka[k]) & 7);
+    JoinKeyWords kw;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint64_t v = al ? (x[k][j] >> (8 * al)) | (x[k][j + 1] << (64 - 8 * al)) : x[k][j];
+      const int32_t rem = kn[k] - 8 * j;
+      kw.w[j] = rem >= 8 ? v : rem > 0 ? v & ((1ULL << (8 * rem)) - 1) : 0ULL;
+    }
+    kw.len = (uint64_t)(uint32_t)kn[k] | (dcol_valid(pk, idx[k]) ? 0ULL : JOIN_KREC_NULL);
+    h[k] = join_words_hash(kw);
+  }
+}
+
 // ------------------------------------- per-row match of a Utf8 probe key --
 // The first half of the split join -> aggregate over a single Utf8 key: one
 // pass over a probe batch writes, per probe row, the build row whose key
@@ -224,13 +272,10 @@ __global__ void __launch_bounds__(MB, 4) match_rows_kernel(DCol pk, int64_t n, c
   const int64_t base = (int64_t)blockIdx.x * (MB * MR) + threadIdx.x;
   uint64_t h[MR], s[MR];
   ulonglong2 e[MR];
+  int64_t rows[MR];
 #pragma unroll
-  for (int k = 0; k < MR; ++k) {
-    const int64_t idx = base + k * MB;
-    JoinKeyWords kw;
-    h[k] = 0;
-    if (idx < n) h[k] = join_key_words(pk, idx, kw) ? join_words_hash(kw) : join_key_hash(&pk, 1, idx);
-  }
+  for (int k = 0; k < MR; ++k) rows[k] = base + k * MB;
+  hash_utf8_rows<MR>(pk, rows, n, h);
 #pragma unroll
   for (int k = 0; k < MR; ++k) {
     const int64_t idx = base + k * MB;
@@ -293,13 +338,10 @@ __global__ void __launch_bounds__(MB, 4) match_entries_kernel(DCol pk, DCol bk, 
   const int64_t base = (int64_t)blockIdx.x * (MB * MR) + threadIdx.x;
   uint64_t h[MR], s[MR];
   ulonglong2 e0[MR], e1[MR];
+  int64_t rows[MR];
 #pragma unroll
-  for (int k = 0; k < MR; ++k) {
-    const int64_t idx = base + k * MB;
-    JoinKeyWords kw;
-    h[k] = 0;
-    if (idx < n) h[k] = join_key_words(pk, idx, kw) ? join_words_hash(kw) : join_key_hash(&pk, 1, idx);
-  }
+  for (int k = 0; k < MR; ++k) rows[k] = base + k * MB;
+  hash_utf8_rows<MR>(pk, rows, n, h);
 #pragma unroll
   for (int k = 0; k < MR; ++k) {
     const int64_t idx = base + k * MB;

@@ -123,13 +123,15 @@ def c4_inputs():
     return build, probes, agg, ref
 
 
-@pytest.mark.parametrize("build_path", ["default", "partitioned", "entries"])
+@pytest.mark.parametrize("build_path", ["default", "partitioned", "entries", "split"])
 def test_c4_utf8_join_aggregate_matches_oracle(ctx, c4_inputs, monkeypatch, build_path):
     build, probes, agg, ref = c4_inputs
     if build_path == "partitioned":  # the radix-partitioned build of the Utf8 table
         monkeypatch.setenv("PRISM_JOIN_PARTITION", "1")
     if build_path == "entries":  # 64-byte slot entries carrying group_id
         monkeypatch.setenv("PRISM_JOIN_KEY_ENTRIES", "1")
+    if build_path == "split":  # match_rows_kernel's per-row match words, then the aggregation
+        monkeypatch.setenv("PRISM_JOIN_SPLIT", "1")
     assert ref.num_rows == 25
     got = prism_gpu.join_aggregate(probes, build, [0], [0], [3, 1], [], agg)
     # group keys and COUNT bit-exact (first-seen order), SUM within 1e-12

@@ -239,8 +239,8 @@ def test_utf8_slot_entries(prof, monkeypatch, long_keys, dups):
 
 @pytest.mark.parametrize("dups", [False, True])
 def test_utf8_unsplit_lookup(prof, monkeypatch, dups):
-    """PRISM_JOIN_SPLIT=0: the fused kernel looks Utf8 keys up itself (the
-    default splits the lookup into match_rows_kernel's per-row match words)."""
+    """PRISM_JOIN_SPLIT=0 (the default): the fused kernel looks Utf8 keys up
+    itself, no match_rows_kernel launch."""
     monkeypatch.setenv("PRISM_JOIN_SPLIT", "0")
     build = build_side(20_000, 5, "utf8", dups, nulls=True)
     probes = [probe_side(30_000, 20_000, 60 + k, build, nulls=True) for k in range(2)]
@@ -254,10 +254,11 @@ def test_utf8_unsplit_lookup(prof, monkeypatch, dups):
 
 @pytest.mark.parametrize("entries", ["0", "1"])
 def test_utf8_split_lookup_runs(prof, monkeypatch, entries):
-    """The default Utf8 path: one match_rows_kernel launch per probe batch
+    """PRISM_JOIN_SPLIT=1: one match_rows_kernel launch per probe batch
     (over the row records, or over the slot entries), group_id handed over
     per row (no nulls, so inlined); keys of 10-39 bytes, so some are longer
     than an entry holds."""
+    monkeypatch.setenv("PRISM_JOIN_SPLIT", "1")
     monkeypatch.setenv("PRISM_JOIN_KEY_ENTRIES", entries)
     rng = np.random.default_rng(91)
     nb = 10_000
