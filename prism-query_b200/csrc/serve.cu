@@ -636,6 +636,24 @@ int prism_server_create(int32_t device, uint64_t budget_bytes, int32_t workers, 
     }
     s->ctxs.push_back(c);
   }
+  // each worker's memory pool grown once up front (one block allocated and
+  // returned; the pool keeps it), so that the first jobs do not map new
+  // device memory while other workers' kernels run.
+  // PRISM_SERVER_POOL_MB sets the size per worker (default 2048, 0: none).
+  uint64_t pre = (uint64_t)2048 << 20;
+  if (const char* e = std::getenv("PRISM_SERVER_POOL_MB")) pre = (uint64_t)std::max(0LL, std::atoll(e)) << 20;
+  pre = std::min<uint64_t>(pre, s->budget / (uint64_t)workers);
+  if (pre) {
+    try {
+      for (auto* c : s->ctxs) {
+        MemP m = c->impl.alloc(pre);
+        m.reset();
+        c->impl.sync();
+      }
+    } catch (const Failure&) {
+      // not enough free memory for the whole block: the pools grow on demand
+    }
+  }
   s->dispatcher = std::thread(dispatch, s);
   for (auto* c : s->ctxs) s->threads.emplace_back(work, s, c);
   *out = s;

@@ -92,10 +92,19 @@ class Server:
         self._submitted = 0
         self._closed = False
         # finished tickets are turned into results (export, tensor views) and
-        # the futures' callbacks run on a pool as wide as the server
-        self._done_pool = cf.ThreadPoolExecutor(max_workers=workers)
+        # the futures' callbacks run on a pool as wide as the server. Every
+        # thread of the pool starts now and makes its export context: a pool
+        # thread started while requests run would create its context (a device
+        # and a page-locked allocation, which synchronise with the device)
+        # under load, stalling every worker's stream.
+        self._done_pool = cf.ThreadPoolExecutor(max_workers=workers, initializer=self._init_thread)
+        gate = threading.Barrier(workers)
+        list(self._done_pool.map(lambda _: gate.wait(timeout=60), range(workers)))
         self._poller = threading.Thread(target=self._poll, daemon=True)
         self._poller.start()
+
+    def _init_thread(self):
+        self._local.ctx = self._Context(self.device)
 
     def _raise(self, rc: int):
         from . import PrismError
