@@ -71,9 +71,6 @@ JoinTuning join_tuning() {
     t.dense = d[0] == '1';
     t.fixed |= JoinTuning::FIX_DENSE;
   }
-  // PRISM_JOIN_DENSE_COPIES=0: no key-order copies of the build columns in dense mode
-  const char* dc = std::getenv("PRISM_JOIN_DENSE_COPIES");
-  if (dc && std::strcmp(dc, "0") == 0) t.dense_copies = false;
   // PRISM_JOIN_KEY_RECORDS=0: Utf8 keys compared through the build column, not packed records
   const char* kr = std::getenv("PRISM_JOIN_KEY_RECORDS");
   if (kr && std::strcmp(kr, "0") == 0) t.key_records = false;

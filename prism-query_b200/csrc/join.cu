@@ -440,9 +440,6 @@ struct ProbeArgs {
   int64_t prefetch_ahead;  // one-pass probe: tiles between a CTA and the tile it prefetches into L2 (0: none)
   int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
   const ulonglong2* krec;  // packed build keys (single Utf8 key), or null
-  // one-pass dense probe: the single 8-byte gathered build column in key
-  // order (JoinTable::dense_copies), or null
-  const unsigned long long* g_dense;
 };
 
 constexpr unsigned long long FLAG_A = 1ULL << 62;
@@ -794,17 +791,8 @@ __global__ void fill_dense_kernel(uint32_t* dense, uint64_t cap, const long long
 
 // dense insert: dense[key - min] = row; a second row for a key sets flag 1,
 // a range of cap or more sets flag 2 (no insert)
-// up to two fixed-width build columns copied into key order by the dense
-// insert (JoinTable::dense_copies)
-struct DenseCopyArgs {
-  int n;
-  int width[2];
-  const void* src[2];
-  void* dst[2];
-};
-
 __global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n, const long long* mm, uint64_t cap,
-                                    uint32_t* dense, uint32_t* flag, DenseCopyArgs cp) {
+                                    uint32_t* dense, uint32_t* flag) {
   const uint64_t r = dense_range(mm, cap);
   if (r == ~0ULL) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(flag, 2u);
@@ -814,12 +802,6 @@ __global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n,
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint64_t d = (uint64_t)__ldg(keys + i) - dmin;
     if (atomicCAS(dense + d, NO_MATCH, (uint32_t)i) != NO_MATCH) atomicOr(flag, 1u);
-    for (int c = 0; c < cp.n; ++c) {
-      if (cp.width[c] == 8)
-        static_cast<unsigned long long*>(cp.dst[c])[d] = __ldcs(static_cast<const unsigned long long*>(cp.src[c]) + i);
-      else
-        static_cast<uint32_t*>(cp.dst[c])[d] = __ldcs(static_cast<const uint32_t*>(cp.src[c]) + i);
-    }
   }
 }
 
@@ -951,18 +933,13 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   uint32_t brow[AV][2];
   unsigned long long pre[AV][2];
   if (DENSE) {
-    // with the gathered column in key order its values load beside the
-    // rows, not after them
-    const unsigned long long* gd = a.g_dense;
 #pragma unroll
     for (int it = 0; it < AV; ++it)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
         const uint64_t d = key[it][j] - (uint64_t)a.dmin;
-        const bool in = q < n && d < a.drange;
-        brow[it][j] = in ? __ldg(a.dense + d) : NO_MATCH;
-        if (gd) pre[it][j] = in ? __ldg(gd + d) : 0ULL;
+        brow[it][j] = (q < n && d < a.drange) ? __ldg(a.dense + d) : NO_MATCH;
       }
   } else {
     uint64_t s[AV][2];
@@ -993,7 +970,7 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
   // one 8-byte gathered column (probe row + payload): its values loaded now,
   // all in flight before the ranking
   const bool one8 = a.ngather == 1 && a.g_width[0] == 8;
-  if (one8 && !(DENSE && a.g_dense)) {
+  if (one8) {
     const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[0]);
     const bool bside = a.g_side[0] != 0;
 #pragma unroll
@@ -1125,31 +1102,9 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
     uint32_t* dr = static_cast<uint32_t*>(dense->ptr);
     fill_dense_kernel<<<grid_for(ctx, (int64_t)dcap, 256, 8), 256, 0, ctx.stream>>>(dr, dcap, mm);
     ctx.check_launch("fill_dense_kernel");
-    // the fixed-width null-free non-key columns (at most two) also in key
-    // order, written by the same pass
-    DenseCopyArgs cp{};
-    std::vector<JoinTable::DenseCopy> copies;
-    if (tune.dense_copies) {
-      for (int c = 0; c < (int)build.cols.size(); ++c) {
-        const Column& col = *build.cols[c];
-        const int w = width_of(col.type);
-        if (c == keys[0] || col.validity || col.type == TY_BOOL || (w != 4 && w != 8)) continue;
-        if (copies.size() == 2) {
-          copies.clear();  // more columns than copies: none
-          break;
-        }
-        copies.push_back({col.values, w, ctx.alloc(dcap * (uint64_t)w)});
-      }
-      cp.n = (int)copies.size();
-      for (int c = 0; c < cp.n; ++c) {
-        cp.width[c] = copies[c].width;
-        cp.src[c] = copies[c].src;
-        cp.dst[c] = copies[c].mem->ptr;
-      }
-    }
     {
       KernelTimer kt(ctx, "insert_kernel");
-      dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, mm, dcap, dr, df, cp);
+      dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, mm, dcap, dr, df);
     }
     ctx.check_launch("dense_insert_kernel");
     long long h[2];
@@ -1162,7 +1117,6 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
       t->dmin = h[0];
       t->drange = (uint64_t)h[1] - (uint64_t)h[0] + 1;
       t->dense_rows = dense;
-      t->dense_copies = std::move(copies);
       return t;
     }
     // a repeated key (flag 1) or a range too wide (flag 2): hash slots
@@ -1438,9 +1392,6 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     const bool vec = (reinterpret_cast<uintptr_t>(pk) & 15) == 0;
     const unsigned grid = (unsigned)ceil_div(n, AT);
     a.prefetch_ahead = any_prefetch_ahead(ctx);
-    if (t.dense && gathers.size() == 1 && gathers[0].side == 1 && gathers[0].width == 8)
-      for (const auto& c : t.dense_copies)
-        if (c.src == gathers[0].src && c.width == 8) a.g_dense = static_cast<const unsigned long long*>(c.mem->ptr);
     if (!t.dense && use_partitioned(ctx, t, tune)) {
       // radix-partitioned probe: the keys reordered by the top bits of their
       // slot hash, so each tile probes one slice of the table

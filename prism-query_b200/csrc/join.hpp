@@ -21,16 +21,6 @@ struct JoinTable {
   int64_t dmin = 0;
   uint64_t drange = 0;
   MemP dense_rows;
-  // dense mode: the build's fixed-width null-free non-key columns (when there
-  // are at most two) also in key order, mem[key - dmin] = the column's value
-  // at that key's row (unspecified for absent keys); a probe loads a match's
-  // value together with its dense row instead of after it
-  struct DenseCopy {
-    const void* src;  // the build column's values
-    int width;        // 4 or 8
-    MemP mem;
-  };
-  std::vector<DenseCopy> dense_copies;
   bool has_dups = false;     // some slot holds more than one build row
   MemP dup_rows;             // build rows grouped by slot, ascending inside a slot
   int64_t n_dup_rows = 0;
@@ -50,7 +40,6 @@ struct JoinTuning {
   double load_factor = 0.5;
   int probe_blocks_per_sm = 2;
   bool dense = true;  // allow dense mode for single Int64 keys
-  bool dense_copies = true;  // dense mode: key-order copies of the build's fixed-width columns
   // radix-partitioned build / probe of hash slots (single Int64 key): -1 once
   // the slots outgrow L2, 0 never, 1 always; 2^partition_bits partitions
   int partition = -1;
