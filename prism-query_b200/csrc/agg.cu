@@ -42,6 +42,11 @@ bool join_split() {
   return e && std::strcmp(e, "1") == 0;
 }
 
+bool join_key_words_on() {
+  const char* e = std::getenv("PRISM_JOIN_KEY_WORDS");
+  return !(e && std::strcmp(e, "0") == 0);
+}
+
 struct RowVals {
   double f[MAX_SRC];
   __int128 i[MAX_SRC];
@@ -1203,6 +1208,11 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.jmatch = nullptr;
         a.jinl = nullptr;
         a.jinl_w = 0;
+        // PRISM_JOIN_KEY_WORDS=0: the probe key's bytes compared by the byte loops
+        a.jkw = !ent && t.key_records && join_key_words_on() && join->probe_keys.size() == 1 &&
+                        b.cols[join->probe_keys[0]]->type == TY_UTF8
+                    ? 1
+                    : 0;
         if (join_split() && join->probe_keys.size() == 1) {
           // split: the lookups by match_rows_kernel (many rows in flight),
           // then the fused kernel aggregates from its per-row match words
@@ -1216,6 +1226,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
           if (match_rows_utf8(ctx, t, *b.cols[join->probe_keys[0]], b.rows, join->inline_col,
                               static_cast<uint32_t*>(mm->ptr), mi ? mi->ptr : nullptr)) {
             a.jent = nullptr;  // the lookup is done; the kernel reads the match words
+            a.jkw = 0;
             a.jmatch = static_cast<const uint32_t*>(mm->ptr);
             a.jinl = mi ? mi->ptr : nullptr;
             a.jinl_w = iw;

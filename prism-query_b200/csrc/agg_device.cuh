@@ -102,6 +102,7 @@ struct AggArgs {
   const uint32_t* jmatch;
   const void* jinl;
   int32_t jinl_w;            // 4 or 8 bytes per row, 0: none
+  int32_t jkw;               // single Utf8 probe key against key records: compared as words
   int32_t jnkeys;
   uint32_t* gnew;                  // slots in creation order (ginsert appends), or null
   unsigned long long* gnew_count;  // length of gnew
@@ -694,7 +695,9 @@ __device__ __forceinline__ void hash_body(const AggArgs& a) {
 // into the block's table. The order key of a joined row is
 // (global probe row << 32 | build row), which sorts like the joined rows'
 // positions (probe rows ascending, build rows ascending inside one).
-template <class E, int NOPS, int BLOCK, int R, bool ENT, bool MATCH = false>
+// KW: a single Utf8 probe key against packed key records: the key's words
+// read once, hashed and compared as words (no byte loops, no second read)
+template <class E, int NOPS, int BLOCK, int R, bool ENT, bool MATCH = false, bool KW = false>
 __device__ __forceinline__ void join_body(const AggArgs& a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ DCol scols[TINY_MAX_COLS];
@@ -717,8 +720,8 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
     // slot entries (a single Utf8 probe key): the key's words read once,
     // hashed, then compared against the 64-byte entry; keq / inl hold each
     // single-row slot's comparison and inlined build value
-    JoinKeyWords kw[ENT ? R : 1];
-    bool kw_ok[ENT ? R : 1];
+    JoinKeyWords kw[ENT || KW ? R : 1];
+    bool kw_ok[ENT || KW ? R : 1];
     bool keq[R];
     unsigned long long inl[ENT || MATCH ? R : 1];
 #pragma unroll
@@ -728,7 +731,7 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
       cand[r] = JOIN_NO_MATCH;
       key[r] = 0;
       keq[r] = true;
-      if constexpr (ENT) {
+      if constexpr (ENT || KW) {
         kw_ok[r] = idx < n && join_key_words(a.jpk[0], idx, kw[r]);
         if (kw_ok[r]) key[r] = join_words_hash(kw[r]);
         else if (idx < n) key[r] = join_key_hash(a.jpk, a.jnkeys, idx);
@@ -841,7 +844,15 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
     }
     // packed build keys: every single-candidate row's key compared up front
     // (the R record loads in flight together, beside the fetches above)
-    if constexpr (!ENT && !MATCH) {  // (match_rows_kernel verified its single-row matches)
+    if constexpr (KW) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const I idx = base + r * stride;
+        keq[r] = cnt[r] == 1 ? (kw_ok[r] ? join_words_rec_equal(kw[r], a.jkrec, cand[r])
+                                         : join_rec_equal(a.jpk[0], idx, a.jkrec, cand[r]))
+                             : true;
+      }
+    } else if constexpr (!ENT && !MATCH) {  // (match_rows_kernel verified its single-row matches)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const I idx = base + r * stride;

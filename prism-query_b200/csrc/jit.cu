@@ -935,8 +935,8 @@ std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKerne
   if (n_probe_cols >= 0)
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.block << ", " << join.min_blocks
       << ") prism_join_agg(prism::AggArgs a) {\n  prism::join_body<prism::QueryRow, " << a.n_ops << ", " << join.block
-      << ", " << join.rows << ", " << (a.jent ? "true" : "false") << ", " << (a.jmatch ? "true" : "false")
-      << ">(a);\n}\n";
+      << ", " << join.rows << ", " << (a.jent ? "true" : "false") << ", " << (a.jmatch ? "true" : "false") << ", "
+      << (a.jkw ? "true" : "false") << ">(a);\n}\n";
   else
     k << "extern \"C\" __global__ void __launch_bounds__(" << join.hash_block << ", 1) prism_hash_agg(prism::AggArgs a) {\n"
          "  prism::hash_body<prism::QueryRow, " << a.n_ops << ", " << join.hash_block << ">(a);\n}\n";

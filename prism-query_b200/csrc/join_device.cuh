@@ -191,6 +191,16 @@ __device__ __forceinline__ uint64_t join_words_hash(const JoinKeyWords& k) {
   return h == JOIN_EMPTY ? JOIN_EMPTY + 1 : h;
 }
 
+// keys_equal of a probe key's words against build row `row`'s packed key
+// record (words 0..4: length, key bytes 0..31, zero past the length)
+__device__ __forceinline__ bool join_words_rec_equal(const JoinKeyWords& k, const ulonglong2* __restrict__ rec,
+                                                     uint32_t row) {
+  const ulonglong2* r = rec + (size_t)row * 4;
+  const ulonglong2 r0 = __ldg(r), r1 = __ldg(r + 1);
+  if (r0.x != k.len || r0.y != k.w[0] || r1.x != k.w[1] || r1.y != k.w[2]) return false;
+  return (uint32_t)k.len <= 24 || __ldg(r + 2).x == k.w[3];
+}
+
 // keys_equal of a probe key's words against an entry with cnt == 1 and no
 // JOIN_ENT_LONG flag (both sides zero-padded)
 __device__ __forceinline__ bool join_words_equal(const JoinKeyWords& k, const ulonglong2& e1, const ulonglong2& e2,
