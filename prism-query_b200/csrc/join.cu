@@ -877,13 +877,17 @@ __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restric
 constexpr int AB = 256;            // threads per CTA
 constexpr int AV = 4;              // 16-byte key loads per thread (2 rows each)
 constexpr int AT = AB * AV * 2;    // rows per tile (2048)
+// resident CTAs per SM the register budget is cut for: 5 for the dense
+// lookup (48 registers, no spills), 4 for the slot walk (64 registers;
+// at 48 it spills)
+constexpr int any_ctas(bool dense) { return dense ? 5 : 4; }
 
 // PART: the keys come in radix-partition order (kpart, with each key's probe
 // row in prow): a tile's keys share their top hash bits, so its slot loads
 // stay inside one slice of the table (the partitioned probe of a table
 // larger than L2).
 template <bool DENSE, bool VEC, bool PART>
-__global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __restrict__ keys,
+__global__ void __launch_bounds__(AB, any_ctas(DENSE)) probe_emit_any_kernel(const int64_t* __restrict__ keys,
                                                                 const uint32_t* __restrict__ prow, int64_t n,
                                                                 ProbeArgs a) {
   __shared__ uint32_t seg[2 * AV * (AB / 32)];
@@ -1027,10 +1031,10 @@ __global__ void __launch_bounds__(AB, 4) probe_emit_any_kernel(const int64_t* __
 }
 
 // PRISM_PROBE_PREFETCH=0 turns the one-pass probe's L2 prefetch off
-int64_t any_prefetch_ahead(const Ctx& ctx) {
+int64_t any_prefetch_ahead(const Ctx& ctx, bool dense) {
   const char* e = std::getenv("PRISM_PROBE_PREFETCH");
   if (e && std::strcmp(e, "0") == 0) return 0;
-  return (int64_t)ctx.sm_count * 4;  // the resident CTAs: one wave ahead
+  return (int64_t)ctx.sm_count * any_ctas(dense);  // the resident CTAs: one wave ahead
 }
 
 template <class K, bool EMIT>
@@ -1391,7 +1395,7 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     const int64_t* pk = static_cast<const int64_t*>(probe.cols[keys[0]]->values);
     const bool vec = (reinterpret_cast<uintptr_t>(pk) & 15) == 0;
     const unsigned grid = (unsigned)ceil_div(n, AT);
-    a.prefetch_ahead = any_prefetch_ahead(ctx);
+    a.prefetch_ahead = any_prefetch_ahead(ctx, t.dense);
     if (!t.dense && use_partitioned(ctx, t, tune)) {
       // radix-partitioned probe: the keys reordered by the top bits of their
       // slot hash, so each tile probes one slice of the table
