@@ -752,10 +752,27 @@ __global__ void __launch_bounds__(QB, 4) probe_rows_dense_kernel(const int64_t* 
 }
 
 // min / max of the build keys (dense-mode test)
+// min / max of the build keys into mm[0], mm[1]: 16-byte loads when the
+// keys are 16-byte aligned, a warp then block reduction, one atomic pair
+// per block (blockDim.x a multiple of 32, at most 1024)
 __global__ void minmax_i64_kernel(const int64_t* __restrict__ keys, int64_t n, long long* mm) {
+  __shared__ long long s_lo[32], s_hi[32];
   long long lo = 0x7fffffffffffffffLL, hi = (long long)0x8000000000000000ULL;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    long long k = __ldg(keys + i);
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+  int64_t head = n;  // rows read as pairs: [0, head)
+  if ((reinterpret_cast<uintptr_t>(keys) & 15) == 0) {
+    head = n & ~(int64_t)1;
+    const longlong2* k2 = reinterpret_cast<const longlong2*>(keys);
+    for (int64_t i = tid; i < head / 2; i += nt) {
+      const longlong2 k = __ldg(k2 + i);  // kept in L2 for the insert that follows
+      lo = min(lo, min(k.x, k.y));
+      hi = max(hi, max(k.x, k.y));
+    }
+  } else {
+    head = 0;
+  }
+  for (int64_t i = head + tid; i < n; i += nt) {
+    const long long k = __ldg(keys + i);
     lo = min(lo, k);
     hi = max(hi, k);
   }
@@ -764,9 +781,24 @@ __global__ void minmax_i64_kernel(const int64_t* __restrict__ keys, int64_t n, l
     lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
     hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
   }
+  const int warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
   if ((threadIdx.x & 31) == 0) {
-    atomicMin(mm, lo);
-    atomicMax(mm + 1, hi);
+    s_lo[warp] = lo;
+    s_hi[warp] = hi;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    lo = threadIdx.x < nw ? s_lo[threadIdx.x] : 0x7fffffffffffffffLL;
+    hi = threadIdx.x < nw ? s_hi[threadIdx.x] : (long long)0x8000000000000000ULL;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    if (threadIdx.x == 0) {
+      atomicMin(mm, lo);
+      atomicMax(mm + 1, hi);
+    }
   }
 }
 
