@@ -71,6 +71,9 @@ JoinTuning join_tuning() {
     t.dense = d[0] == '1';
     t.fixed |= JoinTuning::FIX_DENSE;
   }
+  // PRISM_JOIN_DENSE_PAIRS=0|1: dense tables without / with {row, value} pairs
+  const char* dp = std::getenv("PRISM_JOIN_DENSE_PAIRS");
+  if (dp && (std::strcmp(dp, "0") == 0 || std::strcmp(dp, "1") == 0)) t.dense_pairs = dp[0] == '1';
   // PRISM_JOIN_KEY_RECORDS=0: Utf8 keys compared through the build column, not packed records
   const char* kr = std::getenv("PRISM_JOIN_KEY_RECORDS");
   if (kr && std::strcmp(kr, "0") == 0) t.key_records = false;

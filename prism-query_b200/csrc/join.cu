@@ -440,6 +440,7 @@ struct ProbeArgs {
   int64_t prefetch_ahead;  // one-pass probe: tiles between a CTA and the tile it prefetches into L2 (0: none)
   int64_t row_base;  // added to every emitted probe row index (a chunk of a larger probe)
   const ulonglong2* krec;  // packed build keys (single Utf8 key), or null
+  const ulonglong2* dpairs;  // dense mode: {row, value} of the one gathered column, or null
 };
 
 constexpr unsigned long long FLAG_A = 1ULL << 62;
@@ -837,6 +838,26 @@ __global__ void dense_insert_kernel(const int64_t* __restrict__ keys, int64_t n,
   }
 }
 
+// dense pairs: pairs[d] = {dense[d], the paired column's value at that row}
+// in key order (sequential, coalesced writes; the column read where a row
+// exists), four entries a grid stride apart per thread and step so their
+// column reads are in flight together
+__global__ void dense_pairs_kernel(const uint32_t* __restrict__ dense, uint64_t r,
+                                   const unsigned long long* __restrict__ col, ulonglong2* __restrict__ pairs) {
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t d0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d0 < r; d0 += 4 * nt) {
+    uint32_t rw[4];
+    unsigned long long v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rw[k] = d0 + k * nt < r ? __ldcs(dense + d0 + k * nt) : NO_MATCH;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = rw[k] != NO_MATCH ? __ldg(col + rw[k]) : 0ULL;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (d0 + k * nt < r) __stcs(pairs + d0 + k * nt, make_ulonglong2(rw[k], v[k]));
+  }
+}
+
 __global__ void __launch_bounds__(QB) emit_rows_kernel(const uint32_t* __restrict__ rowv, int64_t n,
                                                        const uint64_t* __restrict__ tile_off, ProbeArgs a) {
   __shared__ uint32_t seg[QI][QB / 32];
@@ -969,13 +990,22 @@ __global__ void __launch_bounds__(AB, any_ctas(DENSE)) probe_emit_any_kernel(con
   uint32_t brow[AV][2];
   unsigned long long pre[AV][2];
   if (DENSE) {
+    // with {row, value} pairs the gathered value comes in the same read
+    const ulonglong2* dp = a.dpairs;
 #pragma unroll
     for (int it = 0; it < AV; ++it)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int64_t q = base + 2 * (it * AB + threadIdx.x) + j;
         const uint64_t d = key[it][j] - (uint64_t)a.dmin;
-        brow[it][j] = (q < n && d < a.drange) ? __ldg(a.dense + d) : NO_MATCH;
+        const bool in = q < n && d < a.drange;
+        if (dp) {
+          const ulonglong2 e = in ? __ldg(dp + d) : make_ulonglong2(NO_MATCH, 0);
+          brow[it][j] = (uint32_t)e.x;
+          pre[it][j] = e.y;
+        } else {
+          brow[it][j] = in ? __ldg(a.dense + d) : NO_MATCH;
+        }
       }
   } else {
     uint64_t s[AV][2];
@@ -1006,7 +1036,7 @@ __global__ void __launch_bounds__(AB, any_ctas(DENSE)) probe_emit_any_kernel(con
   // one 8-byte gathered column (probe row + payload): its values loaded now,
   // all in flight before the ranking
   const bool one8 = a.ngather == 1 && a.g_width[0] == 8;
-  if (one8) {
+  if (one8 && !(DENSE && a.dpairs)) {
     const unsigned long long* src = static_cast<const unsigned long long*>(a.g_src[0]);
     const bool bside = a.g_side[0] != 0;
 #pragma unroll
@@ -1153,6 +1183,21 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
       t->dmin = h[0];
       t->drange = (uint64_t)h[1] - (uint64_t)h[0] + 1;
       t->dense_rows = dense;
+      if (tune.dense_pairs) {
+        // the first fixed 8-byte null-free non-key column, paired with the
+        // rows in key order: a probe gathering it reads one 16-byte entry
+        for (int c = 0; c < (int)build.cols.size(); ++c) {
+          const Column& col = *build.cols[c];
+          if (c == keys[0] || col.validity || width_of(col.type) != 8) continue;
+          MemP pm = ctx.alloc(t->drange * 16);
+          dense_pairs_kernel<<<grid_for(ctx, (int64_t)t->drange, 256, 8), 256, 0, ctx.stream>>>(
+              dr, t->drange, static_cast<const unsigned long long*>(col.values), static_cast<ulonglong2*>(pm->ptr));
+          ctx.check_launch("dense_pairs_kernel");
+          t->dense_pairs = pm;
+          t->dense_pair_src = col.values;
+          break;
+        }
+      }
       return t;
     }
     // a repeated key (flag 1) or a range too wide (flag 2): hash slots
@@ -1428,6 +1473,9 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
     const bool vec = (reinterpret_cast<uintptr_t>(pk) & 15) == 0;
     const unsigned grid = (unsigned)ceil_div(n, AT);
     a.prefetch_ahead = any_prefetch_ahead(ctx, t.dense);
+    if (t.dense && t.dense_pairs && gathers.size() == 1 && gathers[0].side == 1 && gathers[0].width == 8 &&
+        gathers[0].src == t.dense_pair_src)
+      a.dpairs = static_cast<const ulonglong2*>(t.dense_pairs->ptr);
     if (!t.dense && use_partitioned(ctx, t, tune)) {
       // radix-partitioned probe: the keys reordered by the top bits of their
       // slot hash, so each tile probes one slice of the table

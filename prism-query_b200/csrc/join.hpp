@@ -21,6 +21,10 @@ struct JoinTable {
   int64_t dmin = 0;
   uint64_t drange = 0;
   MemP dense_rows;
+  // dense mode: {row, value} pairs in key order for one fixed 8-byte build
+  // column (dense_pair_src), so a probe gathering it reads one 16-byte entry
+  MemP dense_pairs;
+  const void* dense_pair_src = nullptr;
   bool has_dups = false;     // some slot holds more than one build row
   MemP dup_rows;             // build rows grouped by slot, ascending inside a slot
   int64_t n_dup_rows = 0;
@@ -40,6 +44,7 @@ struct JoinTuning {
   double load_factor = 0.5;
   int probe_blocks_per_sm = 2;
   bool dense = true;  // allow dense mode for single Int64 keys
+  bool dense_pairs = false;  // dense mode: {row, value} pairs for one 8-byte build column
   // radix-partitioned build / probe of hash slots (single Int64 key): -1 once
   // the slots outgrow L2, 0 never, 1 always; 2^partition_bits partitions
   int partition = -1;

@@ -53,10 +53,12 @@ def c2_inputs():
     return build, probe, ref
 
 
-@pytest.mark.parametrize("table", ["dense", "hash", "hash-partitioned"])
+@pytest.mark.parametrize("table", ["dense", "dense-pairs", "hash", "hash-partitioned"])
 def test_c2_zipf_join_matches_oracle(ctx, c2_inputs, monkeypatch, table):
     build, probe, ref = c2_inputs
-    if table != "dense":
+    if table == "dense-pairs":  # {row, payload} pairs in key order, one 16-byte read per probe row
+        monkeypatch.setenv("PRISM_JOIN_DENSE_PAIRS", "1")
+    if not table.startswith("dense"):
         monkeypatch.setenv("PRISM_JOIN_DENSE", "0")
         # the radix-partitioned build and probe forced on / off
         monkeypatch.setenv("PRISM_JOIN_PARTITION", "1" if table == "hash-partitioned" else "0")
