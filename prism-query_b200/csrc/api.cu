@@ -518,6 +518,11 @@ void prism_ctx_destroy(prism_ctx* c) {
   cudaStreamSynchronize(x.stream);
   x.clear_timings();
   for (auto e : x.event_pool) cudaEventDestroy(e);
+  for (auto& [fn, g] : x.probe_graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  x.probe_graphs.clear();
   if (x.d_err) cudaFree(x.d_err);
   if (x.h_err) cudaFreeHost(x.h_err);
   if (x.pool) cudaMemPoolDestroy(x.pool);

@@ -86,8 +86,17 @@ struct Ctx {
   std::string last_error;
   int sm_count = 148;
   int64_t l2_bytes = 126LL << 20;  // the device's L2 size
-  uint32_t* d_err = nullptr;  // device error flags (one word)
+  uint32_t* d_err = nullptr;  // device error flags (one word; bytes 8-15: a call's match counter)
   uint32_t* h_err = nullptr;  // pinned mirror
+  // the one-pass probe's steady shape, instantiated once per kernel variant
+  // and replayed with new arguments: memset of the match counter -> kernel
+  // -> one copy of the error word and the counter to the host
+  struct ProbeGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t kernel = nullptr;
+  };
+  std::map<const void*, ProbeGraph> probe_graphs;
   // per-kernel CUDA-event timing (off unless enabled)
   bool profiling = false;
   std::map<std::string, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>> timings;

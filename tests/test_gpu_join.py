@@ -244,6 +244,33 @@ def test_join_project_any_order_is_the_same_multiset(ctx, mode, case, monkeypatc
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("graph", ["1", "0"])
+def test_one_pass_probe_replayed_graph(ctx, monkeypatch, graph):
+    """The one-pass probe's instantiated graph (PRISM_PROBE_GRAPH=1)
+    replayed with new arguments: probes of different sizes, key alignments
+    and tables on one context, back to back, each the same multiset as the
+    probe-order output; and the call-by-call launch (the default) alike."""
+    monkeypatch.setenv("PRISM_PROBE_GRAPH", graph)
+    oc = [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 3]
+    tables = []
+    for dense in ("1", "0"):  # the dense and the hash kernel variants, each with its own graph
+        monkeypatch.setenv("PRISM_JOIN_DENSE", dense)
+        monkeypatch.setenv("PRISM_JOIN_PARTITION", "0")
+        probe0, build = _int_join_batches(80 + int(dense), 20000, 10, 26000)
+        tables.append((HashTable.build(build, [0], ctx), build))
+    for rnd, rows in enumerate([1, 2047, 2048, 100_000, 5, 37_001]):
+        for t, build in tables:
+            probe, _ = _int_join_batches(90 + rnd, 20000, rows + 1, 26000)
+            probe = probe.slice(rnd % 2, rows)  # aligned and unaligned key columns
+            anyo = t.join_project(probe, [0], oc, any_order=True, ctx=ctx)
+            ordered = t.join_project(probe, [0], oc, ctx=ctx)
+            assert anyo.num_rows == ordered.num_rows
+            for a, b in zip(_sorted_pairs(anyo, 2), _sorted_pairs(ordered, 2)):
+                assert np.array_equal(a, b)
+    for t, _ in tables:
+        t.free()
+
+
 @pytest.mark.parametrize("any_order", [False, True])
 def test_join_project_arrow_streamed_equals_device_path(ctx, any_order):
     """prism_join_project_arrow (host batch in, host batch out) streams the
