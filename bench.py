@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5", "sort", "topn", "parquet"], default="c2")
     ap.add_argument("--requests", type=int, default=10_000, help="c5: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="c5: Poisson arrival rate (requests/s)")
+    ap.add_argument("--mix", choices=["both", "probe", "agg"], default="both",
+                    help="c5: the request kinds (default: half GROUP BYs, half probes)")
+    ap.add_argument("--max-rows", type=int, default=16_777_216, help="c5: the largest request (rows, log-uniform from 8K)")
     ap.add_argument("--queue-ctas", type=int, default=0, help="c5: persistent kernel CTAs per SM (0: the library's default)")
     ap.add_argument("--device-queue", action="store_true",
                     help="c5: probes drained by the persistent kernel's device work queue instead of the workers")
@@ -1178,13 +1181,14 @@ def run_c5(args, rank, world, local, torch, dist):
     cfg = HashAggConfig([0], [AggExpr(0, AggFunc.Count, "count"), AggExpr(1, AggFunc.Sum, "sum_i"),
                               AggExpr(1, AggFunc.Min, "min_i"), AggExpr(1, AggFunc.Max, "max_i"),
                               AggExpr(2, AggFunc.Sum, "sum_f"), AggExpr(2, AggFunc.Avg, "avg_f")])
-    lo, hi = min(8192, pool), pool
+    lo, hi = min(8192, pool), max(min(8192, pool), min(pool, args.max_rows))
     reqs, t = [], 0.0
     for i in range(args.requests):
         t += rng.exponential(1.0 / args.rate)
         rows = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
         off = int(rng.integers(0, pool - rows + 1))
-        if rng.random() < 0.5:
+        coin = rng.random()
+        if args.mix == "agg" or (args.mix == "both" and coin < 0.5):
             r = S.AggRequest([("k", "l", akey[off:off + rows]), ("vi", "l", avi[off:off + rows]),
                               ("vf", "g", avf[off:off + rows])], cfg, arrival=t)
         else:
@@ -1218,22 +1222,27 @@ def run_c5(args, rank, world, local, torch, dist):
     # of a server that has been running (the first pass over a fresh server
     # measured 7-14 G rows/s where later passes over the same server gave
     # 15-16 G rows/s)
-    def drain(rs):
-        left, errs, ev, lk = [len(rs)], [], threading.Event(), threading.Lock()
+    def drain(rs, chunk=512):  # in chunks, so the device queue's ring never overflows
+        errs = []
+        for lo in range(0, len(rs), chunk):
+            part = rs[lo:lo + chunk]
+            left, ev, lk = [len(part)], threading.Event(), threading.Lock()
 
-        def one(f):
-            try:
-                f.result()
-            except BaseException as e:  # reported after the pass
-                errs.append(e)
-            with lk:
-                left[0] -= 1
-                if left[0] == 0:
-                    ev.set()
+            def one(f):
+                try:
+                    r = f.result()
+                    if isinstance(r, S.ProbeResult):
+                        r.free()
+                except BaseException as e:  # reported after the pass
+                    errs.append(e)
+                with lk:
+                    left[0] -= 1
+                    if left[0] == 0:
+                        ev.set()
 
-        for r in rs:
-            srv.submit(r).add_done_callback(one)
-        ev.wait()
+            for r in part:
+                srv.submit(r).add_done_callback(one)
+            ev.wait()
         if errs:
             raise errs[0]
 
@@ -1258,6 +1267,8 @@ def run_c5(args, rank, world, local, torch, dist):
             try:
                 r = f.result()
                 served[i] = digest(i, r) if isinstance(r, S.ProbeResult) else r
+                if isinstance(r, S.ProbeResult):
+                    r.free()  # the matches leave the device now, not when garbage collected
             except BaseException as e:  # reported after the run
                 errors.append(e)
             done[i] = time.perf_counter() - t0
@@ -1296,8 +1307,10 @@ def run_c5(args, rank, world, local, torch, dist):
             "unit": "rows/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": ss["makespan_s"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64",
             "data": "synthetic (seeded: request sizes log-uniform, Poisson arrivals, device-resident pools)",
-            "config": {"workload": f"served mixed stream: {len(reqs)} requests, Poisson {args.rate:g}/s, 50/50 C1-style agg / "
-                                   "C2-style probe of 8 resident tables (1M-10M keys), rows log-uniform 8K-16M",
+            "config": {"workload": f"served stream: {len(reqs)} requests, Poisson {args.rate:g}/s, "
+                                   + {"both": "50/50 C1-style agg / C2-style probe", "probe": "C2-style probes",
+                                      "agg": "C1-style GROUP BYs"}[args.mix]
+                                   + f" of 8 resident tables (1M-10M keys), rows log-uniform 8K-{hi}",
                        "total_rows": total_rows, "budget_bytes": 120 << 30, "workers": 4,
                        "device_queue": ("probes drained by one persistent kernel from a device work queue"
                                         if args.device_queue else "off (probes on the worker threads)"),

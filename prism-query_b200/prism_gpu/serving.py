@@ -45,12 +45,48 @@ class AggRequest:
     arrival: float = 0.0
 
 
-@dataclass
 class ProbeResult:
-    matches: int
-    probe_rows: object = None  # torch.Tensor (int32, device), rows of the request's keys, ascending
-    payload: object = None     # torch.Tensor (int64, device)
-    _owner: object = None      # the device batch holding the buffers
+    """A probe's matches, held on the device: `matches` rows of (probe row
+    of the request's keys, build payload). The tensor views are made on first
+    access (making them for every result would cost each completion more
+    than many small probes take on the GPU); free() releases the device
+    memory now instead of when the result is garbage collected."""
+
+    def __init__(self, matches: int, owner=None, device: int = 0, probe_rows=None, payload=None):
+        self.matches = matches
+        self._owner = owner   # the device batch holding the buffers
+        self._device = device
+        self._probe_rows = probe_rows
+        self._payload = payload
+
+    def _view(self, col: int, dtype):
+        import torch
+
+        return _device_tensor(torch, self._owner, col, dtype, self.matches, self._device)
+
+    @property
+    def probe_rows(self):
+        """torch.Tensor (int32, device): the rows of the request's keys that matched."""
+        if self._probe_rows is None:
+            import torch
+
+            self._probe_rows = self._view(0, torch.int32)
+        return self._probe_rows
+
+    @property
+    def payload(self):
+        """torch.Tensor (int64, device): the matched build rows' payload."""
+        if self._payload is None:
+            import torch
+
+            self._payload = self._view(1, torch.int64)
+        return self._payload
+
+    def free(self):
+        self._probe_rows = self._payload = None
+        if self._owner is not None:
+            self._owner.free()
+            self._owner = None
 
 
 @dataclass
@@ -210,8 +246,7 @@ class Server:
         try:
             if isinstance(req, ProbeRequest):
                 m = db.num_rows
-                fut.set_result(ProbeResult(m, _device_tensor(self.torch, db, 0, self.torch.int32, m, self.device),
-                                           _device_tensor(self.torch, db, 1, self.torch.int64, m, self.device), db))
+                fut.set_result(ProbeResult(m, db, self.device))
             else:
                 fut.set_result(db.to_arrow())
                 db.free()
@@ -264,11 +299,8 @@ def run_plain(requests, tables: Dict[str, _Table], ctx, device: int = 0, t0: Opt
             if digest is None:
                 out.append(res.num_rows)
             else:
-                import torch
-
                 m = res.num_rows
-                pr = ProbeResult(m, _device_tensor(torch, res, 0, torch.int32, m, device),
-                                 _device_tensor(torch, res, 1, torch.int64, m, device))
+                pr = ProbeResult(m, res, device)
                 out.append(digest(len(out), pr))
                 del pr
             res.free()
