@@ -41,7 +41,9 @@ struct JoinTable {
 };
 
 struct JoinTuning {
-  double load_factor = 0.5;
+  // target slot load; 0: automatic (0.5, or up to 0.7 when that halves a
+  // table larger than L2: fewer of its slot lines miss L2)
+  double load_factor = 0;
   int probe_blocks_per_sm = 2;
   bool dense = true;  // allow dense mode for single Int64 keys
   bool dense_pairs = false;  // dense mode: {row, value} pairs for one 8-byte build column

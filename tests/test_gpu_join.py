@@ -94,6 +94,75 @@ def test_sentinel_and_extreme_keys(ctx):
     assert_batches_equal(prism_gpu.hash_join(probe, build, cfg), oracle.hash_join(probe, build, cfg))
 
 
+@pytest.mark.parametrize("partition", ["0", "1"])
+def test_one_pass_hash_probe_extreme_keys(ctx, monkeypatch, partition):
+    """Int64 hash slots probed by the one-pass kernel (matches as a
+    multiset), streamed and radix-partitioned: the (probe_row, payload)
+    pairs, the empty-slot sentinel key and the extremes included, with and
+    without the build rows asked for."""
+    monkeypatch.setenv("PRISM_JOIN_DENSE", "0")
+    monkeypatch.setenv("PRISM_JOIN_PARTITION", partition)
+    rng = np.random.default_rng(77)
+    ext = np.array([np.iinfo(np.int64).min, np.iinfo(np.int64).max, -1, 0], dtype=np.int64)
+    keys = np.unique(rng.integers(1, 10**12, 70_000))[:60_000]  # unique, none of the extremes
+    bk = np.concatenate([ext, keys]).astype(np.int64)
+    rng.shuffle(bk)
+    bv = rng.integers(-(2**63), 2**63 - 1, len(bk), dtype=np.int64)
+    pk = np.concatenate([rng.choice(bk, 300_000), rng.integers(1, 10**12, 100_000), ext, [ext[0]] * 3]).astype(np.int64)
+    rng.shuffle(pk)
+    build = pa.RecordBatch.from_arrays([pa.array(bk), pa.array(bv)], names=["k", "v"])
+    probe = pa.RecordBatch.from_arrays([pa.array(pk)], names=["k"])
+    pos = {int(k): i for i, k in enumerate(bk)}
+    exp = sorted((r, int(bv[pos[int(k)]])) for r, k in enumerate(pk) if int(k) in pos)
+    t = HashTable.build(build, [0], ctx)
+    assert t.layout == "hash"
+    out = t.join_project(probe, [0], [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 2], any_order=True)
+    got = sorted(zip(out.column(0).to_numpy().astype(np.int64).tolist(), out.column(1).to_numpy().tolist()))
+    assert got == exp
+    out = t.join_project(probe, [0], [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, prism_gpu.PRISM_COL_BUILD_ROW_INDEX, 2],
+                         any_order=True)
+    rows = out.column(1).to_numpy().astype(np.int64)
+    assert np.array_equal(bv[rows], out.column(2).to_numpy())
+    got = sorted(zip(out.column(0).to_numpy().astype(np.int64).tolist(), out.column(2).to_numpy().tolist()))
+    assert got == exp
+    t.free()
+
+
+def test_hash_table_larger_than_l2(ctx, monkeypatch):
+    """5M unique Int64 keys: at the automatic load the slots (2^23, load
+    0.6, 134 MB) stay larger than L2 and are probed streamed; 20M probe keys,
+    80% members, as a multiset and in probe order."""
+    monkeypatch.setenv("PRISM_JOIN_DENSE", "0")
+    monkeypatch.setenv("PRISM_JOIN_PARTITION", "0")
+    rng = np.random.default_rng(91)
+    n_build, n_probe = 5_000_000, 20_000_000
+    bk = rng.permutation(np.unique(rng.integers(0, 1 << 40, n_build + n_build // 8)))[:n_build].astype(np.int64)
+    assert len(bk) == n_build
+    bv = rng.integers(-(2**63), 2**63 - 1, n_build, dtype=np.int64)
+    miss = rng.integers(1 << 40, 1 << 41, n_probe)
+    pk = np.where(rng.random(n_probe) < 0.8, bk[rng.integers(0, n_build, n_probe)], miss).astype(np.int64)
+    order = np.argsort(bk)
+    sk = bk[order]
+    at = np.minimum(np.searchsorted(sk, pk), n_build - 1)
+    hit = sk[at] == pk
+    exp_rows = np.flatnonzero(hit)
+    exp_pay = bv[order[at[hit]]]
+    build = pa.RecordBatch.from_arrays([pa.array(bk), pa.array(bv)], names=["k", "v"])
+    probe = pa.RecordBatch.from_arrays([pa.array(pk)], names=["k"])
+    t = HashTable.build(build, [0], ctx)
+    assert t.layout == "hash"
+    for any_order in (True, False):
+        out = t.join_project(probe, [0], [prism_gpu.PRISM_COL_PROBE_ROW_INDEX, 2], any_order=any_order)
+        rows = out.column(0).to_numpy().astype(np.int64)
+        pay = out.column(1).to_numpy()
+        if any_order:
+            o = np.argsort(rows, kind="stable")
+            rows, pay = rows[o], pay[o]
+        assert np.array_equal(rows, exp_rows)
+        assert np.array_equal(pay, exp_pay)
+    t.free()
+
+
 def test_sliced_inputs(ctx):
     probe, build = _int_join_batches(9, 1000, 5000, 1200, nulls=True)
     p2, b2 = probe.slice(3, 4000), build.slice(7, 900)
