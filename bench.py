@@ -340,8 +340,9 @@ def main():
     peak, peak_kind = peaks()
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("probe_phase_c2")
+    if os.path.exists(tp) and any_order and PROBE_DIST == "zipf" and not kstats["probe_partition_scatter_kernel"][0]:
+        # captured for the one-pass probe on the dense table / the streamed hash probe
+        traffic = json.load(open(tp)).get("probe_phase_c2" if layout[0] == "dense" else "probe_phase_c2_hash")
 
     # e2e: host Arrow batches in pinned memory through the C ABI
     e2e = None
