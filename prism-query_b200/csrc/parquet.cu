@@ -99,9 +99,12 @@ struct SnappyJob {
 //      64 bytes, which gets a batch of its own);
 //   3. literals and copies whose source lies before the batch run in
 //      parallel, one lane per element; copies that read the batch's own
-//      output then run in order, the warp's lanes over their bytes.
-// The last SNAP_RING output bytes are mirrored in shared memory for copies
-// with offsets up to SNAP_RING_REACH; longer ones read the output in HBM.
+//      output then run in order, the warp's lanes over their bytes;
+//   4. the batch's output goes from shared memory to HBM, consecutive lanes
+//      on consecutive bytes.
+// The last SNAP_RING output bytes are kept in shared memory (the batch is
+// assembled there) for copies with offsets up to SNAP_RING_REACH; longer
+// ones read the output in HBM.
 constexpr int SNAP_WARPS = 8;
 constexpr int SNAP_RING = 8192;  // power of two
 constexpr int SNAP_SPAN = 1024;
@@ -209,20 +212,21 @@ __global__ void __launch_bounds__(32 * SNAP_WARPS) pq_snappy_kernel(const Snappy
     const bool first_long = cnt == 1 && __shfl_sync(FULL, (int)(t == 0 && len > 64), 0);
     // 3a. independent elements, one lane each
     const bool indep_copy = mine && t != 0 && my_o - (int64_t)off + (len < (int64_t)off ? len : (int64_t)off) <= op;
+    // (the batch's output goes to the ring only; it is written to HBM by
+    // the whole warp at the end of the batch)
     if (mine && t == 0 && len <= 64) {
       const uint8_t* src = in + base + lane + (elen_in - len);
-      for (int i = 0; i < (int)len; ++i) {
-        const uint8_t v = src[i];
-        dst[my_o + i] = v;
-        ring[(my_o + i) & (SNAP_RING - 1)] = v;
-      }
+      for (int i = 0; i < (int)len; ++i) ring[(my_o + i) & (SNAP_RING - 1)] = src[i];
     } else if (indep_copy) {
+      // byte i of a copy repeats the source's first min(len, off) bytes:
+      // source index i % off, kept incrementally
       const bool near = off <= (uint32_t)SNAP_RING_REACH;
+      const int64_t s0 = my_o - off;
+      uint32_t j = 0;
       for (int i = 0; i < (int)len; ++i) {
-        const int64_t p = my_o - off + (i % off);
-        const uint8_t v = near ? ring[p & (SNAP_RING - 1)] : dst[p];
-        dst[my_o + i] = v;
-        ring[(my_o + i) & (SNAP_RING - 1)] = v;
+        const int64_t p = s0 + j;
+        ring[(my_o + i) & (SNAP_RING - 1)] = near ? ring[p & (SNAP_RING - 1)] : dst[p];
+        if (++j == off) j = 0;
       }
     }
     __syncwarp();
@@ -244,14 +248,22 @@ __global__ void __launch_bounds__(32 * SNAP_WARPS) pq_snappy_kernel(const Snappy
       const int64_t eo = __shfl_sync(FULL, my_o, sl);
       const uint32_t eoff = __shfl_sync(FULL, off, sl);
       const int el = (int)__shfl_sync(FULL, len, sl);
+      // el <= 64: lane i takes bytes i and i + 32 (source index (i mod eoff))
+      uint32_t j = (uint32_t)lane % eoff;
+      const uint32_t step = 32u % eoff;
       for (int i = lane; i < el; i += 32) {
-        const int64_t p = eo - eoff + (i % eoff);
-        const uint8_t v = ring[p & (SNAP_RING - 1)];
-        dst[eo + i] = v;
-        ring[(eo + i) & (SNAP_RING - 1)] = v;
+        const int64_t p = eo - eoff + j;
+        ring[(eo + i) & (SNAP_RING - 1)] = ring[p & (SNAP_RING - 1)];
+        j += step;
+        if (j >= eoff) j -= eoff;
       }
       __syncwarp();
     }
+    // the batch's output, ring -> HBM, consecutive lanes on consecutive bytes
+    // (a long literal batch wrote HBM directly)
+    if (!first_long)
+      for (int64_t q = op + lane; q < batch_end; q += 32) dst[q] = ring[q & (SNAP_RING - 1)];
+    __syncwarp();
     op = batch_end;
     ip = base + pos;
   }
