@@ -499,7 +499,7 @@ int prism_ctx_create(int device, uint64_t budget, prism_ctx** out) {
     if (l2 > 0) x.l2_bytes = l2;
     PRISM_CUDA(cudaMalloc(&x.d_err, 64));
     PRISM_CUDA(cudaMemset(x.d_err, 0, 64));
-    PRISM_CUDA(cudaMallocHost(&x.h_err, 64));
+    PRISM_CUDA(cudaMallocHost(&x.h_err, 128));
   } catch (const Failure& f) {
     t_err = f.msg;
     if (x.pool) cudaMemPoolDestroy(x.pool);

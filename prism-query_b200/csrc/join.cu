@@ -808,6 +808,13 @@ __global__ void fill_u32_kernel(uint32_t* p, uint64_t n, uint32_t v) {
     p[i] = v;
 }
 
+// min / max accumulators and the dense insert's flag word, before the keys
+__global__ void dense_scalars_init_kernel(long long* mm) {
+  mm[0] = 0x7fffffffffffffffLL;
+  mm[1] = (long long)0x8000000000000000ULL;
+  mm[2] = 0;
+}
+
 // The key range the min / max kernel found, or ~0 when it is cap or wider.
 __device__ __forceinline__ uint64_t dense_range(const long long* mm, uint64_t cap) {
   const uint64_t diff = (uint64_t)mm[1] - (uint64_t)mm[0];  // max >= min: the build has rows
@@ -1205,12 +1212,12 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
     // dense mode takes; the fill and the inserts read the range the min / max
     // kernel left on the device, and give up (flag 2) when it is wider
     const uint64_t dcap = (uint64_t)std::min<int64_t>(2 * n + 4096, (int64_t)1 << 28);
-    MemP mmm, mdf;
-    long long* mm = ctx.alloc_t<long long>(2, mmm);
-    uint32_t* df = ctx.alloc_t<uint32_t>(1, mdf);
-    const long long init[2] = {0x7fffffffffffffffLL, (long long)0x8000000000000000ULL};
-    PRISM_CUDA(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, ctx.stream));
-    PRISM_CUDA(cudaMemsetAsync(df, 0, 4, ctx.stream));
+    // {min, max, flag word}: set by one tiny kernel, read back by one copy
+    MemP mmm;
+    long long* mm = ctx.alloc_t<long long>(3, mmm);
+    uint32_t* df = reinterpret_cast<uint32_t*>(mm + 2);
+    dense_scalars_init_kernel<<<1, 1, 0, ctx.stream>>>(mm);
+    ctx.check_launch("dense_scalars_init_kernel");
     minmax_i64_kernel<<<grid_for(ctx, n, 256, 8), 256, 0, ctx.stream>>>(bk, n, mm);
     ctx.check_launch("minmax_i64_kernel");
     MemP dense = ctx.alloc(dcap * 4);
@@ -1222,11 +1229,11 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
       dense_insert_kernel<<<grid_for(ctx, n, 256, 16), 256, 0, ctx.stream>>>(bk, n, mm, dcap, dr, df);
     }
     ctx.check_launch("dense_insert_kernel");
-    long long h[2];
-    uint32_t hdf = 0;
-    PRISM_CUDA(cudaMemcpyAsync(h, mm, 16, cudaMemcpyDeviceToHost, ctx.stream));
-    PRISM_CUDA(cudaMemcpyAsync(&hdf, df, 4, cudaMemcpyDeviceToHost, ctx.stream));
+    long long* hs = reinterpret_cast<long long*>(reinterpret_cast<char*>(ctx.h_err) + 64);  // pinned
+    PRISM_CUDA(cudaMemcpyAsync(hs, mm, 24, cudaMemcpyDeviceToHost, ctx.stream));
     PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+    const long long h[2] = {hs[0], hs[1]};
+    const uint32_t hdf = (uint32_t)hs[2];
     if (!hdf) {
       t->dense = true;
       t->dmin = h[0];

@@ -87,7 +87,7 @@ struct Ctx {
   int sm_count = 148;
   int64_t l2_bytes = 126LL << 20;  // the device's L2 size
   uint32_t* d_err = nullptr;  // device error flags (one word; bytes 8-15: a call's match counter)
-  uint32_t* h_err = nullptr;  // pinned mirror
+  uint32_t* h_err = nullptr;  // pinned mirror (128 bytes; bytes 64-127: small readbacks of a call)
   // the one-pass probe's steady shape, instantiated once per kernel variant
   // and replayed with new arguments: memset of the match counter -> kernel
   // -> one copy of the error word and the counter to the host
