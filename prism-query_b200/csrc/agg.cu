@@ -1172,11 +1172,6 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         }
         a.src[s] = sr;
       }
-      upload_program(ctx, pg, b);
-      a.pn = pg.d_pnodes;
-      a.en = pg.d_enodes;
-      a.cl = pg.d_clauses;
-      a.cols = pg.d_cols;
       int grid = (int)std::min<int64_t>(ceil_div(b.rows, block), (int64_t)ctx.sm_count * std::max(1, tune.blocks_per_sm));
       const void* jk = nullptr;
       if (tiny) {
@@ -1252,6 +1247,14 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         std::string src = jit_hash_agg_source(pg, b, a, -1, shape);
         if (!src.empty()) hk = jit_get(src, "prism_hash_agg");
       }
+      // the program's device copy: its upload waits for the stream (the
+      // previous batch's kernel), so the kernel source above was generated
+      // while that kernel ran
+      upload_program(ctx, pg, b);
+      a.pn = pg.d_pnodes;
+      a.en = pg.d_enodes;
+      a.cl = pg.d_clauses;
+      a.cols = pg.d_cols;
       if (hk) {
         a.ss_log2 = hss_log2;
         PRISM_CUDA(cudaFuncSetAttribute(hk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
