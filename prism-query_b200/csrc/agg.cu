@@ -1307,9 +1307,12 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
                                                               s_ordered, s_firsts, s_rows, s_out);
       ctx.check_launch("small_order_kernel");
     }
-    unsigned long long small_n = ~0ULL;
-    if (small_try) PRISM_CUDA(cudaMemcpyAsync(&small_n, s_out, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    // the group count into the context's page-locked words, read after the
+    // error word's synchronisation (one round trip for both)
+    unsigned long long* h_small = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ctx.h_err) + 64);
+    if (small_try) PRISM_CUDA(cudaMemcpyAsync(h_small, s_out, 8, cudaMemcpyDeviceToHost, ctx.stream));
     uint32_t derr = ctx.take_device_errors();
+    const unsigned long long small_n = small_try ? *h_small : ~0ULL;
     if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "aggregation wait timed out");
     if (derr & DERR_TABLE_FULL) {
       if (P.n_distinct) dist_log2 += 1;
