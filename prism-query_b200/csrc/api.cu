@@ -500,6 +500,17 @@ int prism_ctx_create(int device, uint64_t budget, prism_ctx** out) {
     PRISM_CUDA(cudaMalloc(&x.d_err, 64));
     PRISM_CUDA(cudaMemset(x.d_err, 0, 64));
     PRISM_CUDA(cudaMallocHost(&x.h_err, 128));
+    // the staging ring is optional: without it staged copies wait for the stream
+    constexpr size_t STAGE = (size_t)1 << 20;
+    if (cudaMallocHost(&x.h_stage, STAGE) == cudaSuccess &&
+        cudaEventCreateWithFlags(&x.stage_ev, cudaEventDisableTiming) == cudaSuccess) {
+      x.stage_cap = STAGE;
+    } else {
+      cudaGetLastError();
+      if (x.h_stage) cudaFreeHost(x.h_stage);
+      x.h_stage = nullptr;
+      x.stage_ev = nullptr;
+    }
   } catch (const Failure& f) {
     t_err = f.msg;
     if (x.pool) cudaMemPoolDestroy(x.pool);
@@ -525,6 +536,8 @@ void prism_ctx_destroy(prism_ctx* c) {
   x.probe_graphs.clear();
   if (x.d_err) cudaFree(x.d_err);
   if (x.h_err) cudaFreeHost(x.h_err);
+  if (x.h_stage) cudaFreeHost(x.h_stage);
+  if (x.stage_ev) cudaEventDestroy(x.stage_ev);
   if (x.pool) cudaMemPoolDestroy(x.pool);
   if (x.own_stream) cudaStreamDestroy(x.own_stream);
   delete c;

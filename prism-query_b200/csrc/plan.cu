@@ -522,9 +522,7 @@ void upload_program(Ctx& ctx, Program& p, const Batch& b) {
     DCol v = b.cols[p.cols[i]]->view();
     std::memcpy(host.data() + off_d + i * sizeof(DCol), &v, sizeof(DCol));
   }
-  PRISM_CUDA(cudaMemcpyAsync(base, host.data(), total, cudaMemcpyHostToDevice, ctx.stream));
-  // the host staging vector must outlive the async copy
-  PRISM_CUDA(cudaStreamSynchronize(ctx.stream));
+  ctx.h2d_staged(base, host.data(), total);  // (copied out of `host` before this returns)
   p.d_pnodes = reinterpret_cast<const PNode*>(base + off_p);
   p.d_enodes = reinterpret_cast<const ENode*>(base + off_e);
   p.d_clauses = reinterpret_cast<const PRange*>(base + off_c);

@@ -1,4 +1,5 @@
 // runtime.cu — context, allocator and column helpers.
+#include <cstring>
 #include "runtime.hpp"
 
 namespace prism {
@@ -47,6 +48,25 @@ uint32_t Ctx::take_device_errors() {
 }
 
 void Ctx::sync() { PRISM_CUDA(cudaStreamSynchronize(stream)); }
+
+void Ctx::h2d_staged(void* dst, const void* src, size_t bytes) {
+  if (!h_stage || !stage_ev || bytes > stage_cap / 2) {
+    PRISM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    PRISM_CUDA(cudaStreamSynchronize(stream));  // the source must outlive the copy
+    return;
+  }
+  const size_t n = (bytes + 255) & ~(size_t)255;
+  if (stage_head + n > stage_cap) {
+    if (stage_pending) PRISM_CUDA(cudaEventSynchronize(stage_ev));  // the ring's earlier copies are done
+    stage_head = 0;
+  }
+  uint8_t* p = h_stage + stage_head;
+  std::memcpy(p, src, bytes);
+  PRISM_CUDA(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, stream));
+  PRISM_CUDA(cudaEventRecord(stage_ev, stream));
+  stage_pending = true;
+  stage_head += n;
+}
 
 cudaEvent_t Ctx::take_event() {
   if (!event_pool.empty()) {

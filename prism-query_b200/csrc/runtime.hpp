@@ -88,6 +88,16 @@ struct Ctx {
   int64_t l2_bytes = 126LL << 20;  // the device's L2 size
   uint32_t* d_err = nullptr;  // device error flags (one word; bytes 8-15: a call's match counter)
   uint32_t* h_err = nullptr;  // pinned mirror (128 bytes; bytes 64-127: small readbacks of a call)
+  // page-locked ring for small host -> device copies whose host source may
+  // go away at once (program uploads): the bytes are copied into the ring and
+  // the device copy is queued without waiting for the stream; a wrap of the
+  // ring waits for the last copy queued (all of them are on this stream: a
+  // stream change synchronises the old one)
+  uint8_t* h_stage = nullptr;
+  size_t stage_cap = 0, stage_head = 0;
+  cudaEvent_t stage_ev = nullptr;
+  bool stage_pending = false;
+  void h2d_staged(void* dst, const void* src, size_t bytes);
   // the one-pass probe's steady shape, instantiated once per kernel variant
   // and replayed with new arguments: memset of the match counter -> kernel
   // -> one copy of the error word and the counter to the host
