@@ -1102,7 +1102,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
       std::vector<DCol> v;
       for (int k : join->probe_keys) v.push_back(pb->cols.at(k)->view());
       MemP m = ctx.alloc(v.size() * sizeof(DCol));
-      PRISM_CUDA(cudaMemcpyAsync(m->ptr, v.data(), v.size() * sizeof(DCol), cudaMemcpyHostToDevice, ctx.stream));
+      ctx.h2d_staged(m->ptr, v.data(), v.size() * sizeof(DCol));
       jpk_dev.push_back(static_cast<const DCol*>(m->ptr));
       jpk_mem.push_back(m);
     }

@@ -230,8 +230,7 @@ void pack_batch(Ctx& ctx, const Batch& b, void* dst, uint64_t capacity) {
   if (capacity < L.total) fail(PRISM_ERR_INVALID_ARGUMENT, "pack destination smaller than the packed size");
   const std::vector<uint8_t> h = header_bytes(b, L);
   uint8_t* d = static_cast<uint8_t*>(dst);
-  // pageable source: the copy has consumed `h` when the call returns
-  PRISM_CUDA(cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, ctx.stream));
+  ctx.h2d_staged(d, h.data(), h.size());  // (copied out of `h` before this returns)
   for (const auto& p : L.pieces)
     PRISM_CUDA(cudaMemcpyAsync(d + p.first, p.second.src, p.second.bytes, cudaMemcpyDeviceToDevice, ctx.stream));
 }

@@ -1200,8 +1200,7 @@ std::unique_ptr<JoinTable> build_join_table(Ctx& ctx, const Batch& build, const 
   t->int64_fast = keys.size() == 1 && build.cols[keys[0]]->type == TY_I64;
   for (int k : keys) t->key_views.push_back(build.cols[k]->view());
   t->key_views_dev = ctx.alloc(t->key_views.size() * sizeof(DCol));
-  PRISM_CUDA(cudaMemcpyAsync(t->key_views_dev->ptr, t->key_views.data(), t->key_views.size() * sizeof(DCol),
-                             cudaMemcpyHostToDevice, ctx.stream));
+  ctx.h2d_staged(t->key_views_dev->ptr, t->key_views.data(), t->key_views.size() * sizeof(DCol));
   if (t->int64_fast && n > 0 && tune.dense) {
     // dense mode when the keys span a range of at most twice the rows (plus
     // 4096) and are unique: a direct row index per key value replaces the
@@ -1468,8 +1467,7 @@ static void fill_common(Ctx& ctx, const JoinTable& t, const Batch& probe, const 
   if (!upload_views) return;  // (the kernels of single Int64 keys read the key column directly)
   for (int k : keys) pviews.push_back(probe.cols[k]->view());
   pviews_dev = ctx.alloc(pviews.size() * sizeof(DCol));
-  PRISM_CUDA(cudaMemcpyAsync(pviews_dev->ptr, pviews.data(), pviews.size() * sizeof(DCol), cudaMemcpyHostToDevice,
-                             ctx.stream));
+  ctx.h2d_staged(pviews_dev->ptr, pviews.data(), pviews.size() * sizeof(DCol));
   a.pcols = static_cast<const DCol*>(pviews_dev->ptr);
 }
 

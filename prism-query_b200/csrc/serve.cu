@@ -273,7 +273,7 @@ prism_batch* new_batch(prism_ctx* w, Batch b) {
 
 MemP upload_starts(Ctx& x, const std::vector<uint64_t>& starts) {
   MemP m = x.alloc(starts.size() * 8);
-  PRISM_CUDA(cudaMemcpyAsync(m->ptr, starts.data(), starts.size() * 8, cudaMemcpyHostToDevice, x.stream));
+  x.h2d_staged(m->ptr, starts.data(), starts.size() * 8);
   return m;
 }
 
