@@ -1175,8 +1175,8 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
       int grid = (int)std::min<int64_t>(ceil_div(b.rows, block), (int64_t)ctx.sm_count * std::max(1, tune.blocks_per_sm));
       const void* jk = nullptr;
       if (tiny) {
-        std::string src = jit_tiny_agg_source(pg, b, a, (int)G, any_f64);
-        if (!src.empty()) jk = jit_get(src, "prism_tiny_agg");
+        jk = jit_plan_kernel(pg, b, a, {(int64_t)G, any_f64 ? 1 : 0}, "prism_tiny_agg",
+                             [&] { return jit_tiny_agg_source(pg, b, a, (int)G, any_f64); });
       }
       const void* hk = nullptr;
       if (join) {
@@ -1237,15 +1237,15 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         shape.block = tune.join_block;
         shape.min_blocks = tune.join_min_blocks;
         shape.rows = tune.join_rows;
-        std::string src = jit_hash_agg_source(pg, b, a, n_probe_cols, shape);
-        if (src.empty()) fused_fail("this projection over a join");
-        hk = jit_get(src, "prism_join_agg");
+        hk = jit_plan_kernel(pg, b, a, {n_probe_cols, shape.block, shape.min_blocks, shape.rows, shape.hash_block},
+                             "prism_join_agg", [&] { return jit_hash_agg_source(pg, b, a, n_probe_cols, shape); });
+        if (!hk) fused_fail("this projection over a join");
       } else if (!jk && hss_log2 && !A.wide) {
         a.n_cols = (int)pg.cols.size();
         JoinKernelShape shape;
         shape.hash_block = tune.hash_block;
-        std::string src = jit_hash_agg_source(pg, b, a, -1, shape);
-        if (!src.empty()) hk = jit_get(src, "prism_hash_agg");
+        hk = jit_plan_kernel(pg, b, a, {-1, shape.block, shape.min_blocks, shape.rows, shape.hash_block},
+                             "prism_hash_agg", [&] { return jit_hash_agg_source(pg, b, a, -1, shape); });
       }
       // the program's device copy: its upload waits for the stream (the
       // previous batch's kernel), so the kernel source above was generated

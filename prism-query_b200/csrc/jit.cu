@@ -945,6 +945,134 @@ std::string query_row_kernel(const AggArgs& a, int n_probe_cols, const JoinKerne
 
 }  // namespace
 
+namespace {
+
+template <class T>
+void key_put(std::string& k, const T& v) {
+  k.append(reinterpret_cast<const char*>(&v), sizeof v);
+}
+void key_str(std::string& k, const std::string& v) {
+  key_put(k, (uint64_t)v.size());
+  k.append(v);
+}
+template <class P>
+void key_nonnull(P*& p) {
+  p = p ? reinterpret_cast<P*>(uintptr_t(1)) : nullptr;
+}
+
+bool plan_cache_on() {
+  const char* e = std::getenv("PRISM_JIT_PLAN_CACHE");
+  return !(e && std::strcmp(e, "0") == 0);
+}
+
+std::mutex g_plan_mu;
+std::unordered_map<std::string, const void*> g_plan;
+
+}  // namespace
+
+const void* jit_plan_kernel(const Program& pg, const Batch& b, const AggArgs& a0, const std::vector<int64_t>& extra,
+                            const char* name, const std::function<std::string()>& make) {
+  if (!plan_cache_on()) {
+    const std::string src = make();
+    return src.empty() ? nullptr : jit_get(src, name);
+  }
+  std::string k;
+  k.reserve(8192);
+  key_str(k, name);
+  for (int64_t x : extra) key_put(k, x);
+  // the kernel arguments, pointers as null / non-null
+  AggArgs a;
+  std::memcpy(&a, &a0, sizeof a);
+  key_nonnull(a.pn);
+  key_nonnull(a.en);
+  key_nonnull(a.cl);
+  key_nonnull(a.cols);
+  key_nonnull(a.gkeys);
+  key_nonnull(a.gfirst);
+  key_nonnull(a.gacc);
+  key_nonnull(a.jslots);
+  key_nonnull(a.jdup);
+  key_nonnull(a.jdense);
+  key_nonnull(a.jpk);
+  key_nonnull(a.jbk);
+  key_nonnull(a.jkrec);
+  key_nonnull(a.jent);
+  key_nonnull(a.jmatch);
+  key_nonnull(a.jinl);
+  key_nonnull(a.gnew);
+  key_nonnull(a.gnew_count);
+  for (auto& d : a.dt) key_nonnull(d.slots);
+  key_nonnull(a.err);
+  key_nonnull(a.maxexp);
+  key_nonnull(a.gwide);
+  key_put(k, a);
+  // the program's host arrays
+  key_put(k, (uint64_t)pg.cols.size());
+  for (int c : pg.cols) key_put(k, c);
+  key_put(k, (uint64_t)pg.pnodes.size());
+  for (PNode n : pg.pnodes) {
+    key_nonnull(n.s);
+    key_put(k, n);
+  }
+  key_put(k, (uint64_t)pg.clauses.size());
+  for (const PRange& r : pg.clauses) key_put(k, r);
+  key_put(k, (uint64_t)pg.enodes.size());
+  for (const ENode& e : pg.enodes) key_put(k, e);
+  key_put(k, (uint64_t)pg.strings.size());
+  for (const std::string& x : pg.strings) key_str(k, x);
+  for (int i : pg.string_node) key_put(k, i);
+  key_put(k, (int32_t)pg.has_filter);
+  key_put(k, pg.filter);
+  key_put(k, (uint64_t)pg.exprs.size());
+  for (const CompiledExpr& e : pg.exprs) {
+    key_put(k, e.kind);
+    key_put(k, e.begin);
+    key_put(k, e.end);
+    key_put(k, e.scale);
+    key_put(k, e.out_type);
+    key_put(k, e.column);
+    prism_scalar lit = e.literal;
+    key_nonnull(lit.str);
+    key_put(k, lit);
+    key_str(k, e.literal_str);
+    for (int32_t c : e.branch_cols) key_put(k, c);
+    for (const std::string& x : e.branch_lits) key_str(k, x);
+    key_put(k, e.sel_clause_begin);
+    key_put(k, e.sel_n_clauses);
+    key_put(k, (int32_t)e.sel_has_else);
+  }
+  // the row count and every column's type and attributes (not its data)
+  key_put(k, b.rows);
+  key_put(k, (uint64_t)b.cols.size());
+  for (const ColP& c : b.cols) {
+    key_put(k, c->type);
+    key_put(k, c->index_type);
+    key_put(k, (int32_t)c->nullable);
+    key_put(k, c->precision);
+    key_put(k, c->scale);
+    key_put(k, c->length);
+    key_put(k, c->data_base);
+    key_put(k, (int32_t)((c->validity ? 1 : 0) | (c->values ? 2 : 0) | (c->offsets ? 4 : 0) | (c->data ? 8 : 0)));
+    if (c->dict) {
+      key_put(k, c->dict->type);
+      key_put(k, c->dict->length);
+      key_put(k, c->dict_fingerprint);
+    } else {
+      key_put(k, (int32_t)-1);
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plan.find(k);
+    if (it != g_plan.end()) return it->second;
+  }
+  const std::string src = make();
+  const void* kern = src.empty() ? nullptr : jit_get(src, name);
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plan.emplace(std::move(k), kern);
+  return kern;
+}
+
 std::string jit_tiny_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int g, bool f64) {
   Gen gen(pg, b);
   RowParts rp = row_parts(gen, a);

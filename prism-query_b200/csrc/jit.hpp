@@ -12,6 +12,7 @@
 // same order of operations, as the interpreter.
 #pragma once
 
+#include <functional>
 #include <string>
 
 #include "runtime.hpp"
@@ -55,5 +56,15 @@ struct JoinKernelShape {
 };
 std::string jit_hash_agg_source(const Program& pg, const Batch& b, const AggArgs& a, int n_probe_cols = -1,
                                 const JoinKernelShape& join = JoinKernelShape{});
+
+// The kernel `name` generated for this plan: the kernel made by `make` (a
+// source generator over the same inputs) the first time a plan with this key
+// is seen, the same kernel without generating its source again afterwards.
+// The key holds everything the generators read: the program's host arrays,
+// every column's type and attributes, the kernel arguments with each pointer
+// reduced to null / non-null, and `extra` (the generator's own parameters).
+// PRISM_JIT_PLAN_CACHE=0 generates the source every call.
+const void* jit_plan_kernel(const Program& pg, const Batch& b, const AggArgs& a, const std::vector<int64_t>& extra,
+                            const char* name, const std::function<std::string()>& make);
 
 }  // namespace prism

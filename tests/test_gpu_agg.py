@@ -196,3 +196,30 @@ def test_float_sum_mixed_tiny_and_unit_values(ctx):
     assert_batches_equal(got, oracle.hash_aggregate(b, cfg), float_cols=(1,))
     exact = np.array([oracle.exact_sum_f64(v[g == k]) for k in got.column(0).to_numpy()])
     assert np.array_equal(got.column(1).to_numpy(), exact)
+
+
+def test_generated_kernels_reused_per_plan(ctx):
+    """The generated aggregation kernels are looked up by plan, not by their
+    regenerated source: plans that differ only in a key column's type, its
+    nulls, the row count or the aggregate list, interleaved and each run
+    twice in one process, all equal the oracle."""
+    rng = np.random.default_rng(404)
+
+    def batch(n, key_type, nulls):
+        k = rng.integers(0, 3000, n)
+        mask = (rng.random(n) < 0.05) if nulls else None
+        return pa.RecordBatch.from_arrays(
+            [pa.array(k.astype(key_type), mask=mask), pa.array(rng.integers(-1000, 1000, n)), pa.array(rng.random(n))],
+            names=["k", "v", "f"])
+
+    cfgs = [HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "s"), AggExpr(2, AggFunc.Max, "m")]),
+            HashAggConfig([0], [AggExpr(2, AggFunc.Sum, "sf"), AggExpr(1, AggFunc.Count, "n"), AggExpr(1, AggFunc.Min, "mn")])]
+    batches = [batch(50_000, np.int64, False), batch(50_000, np.int32, False), batch(50_000, np.int64, True),
+               batch(70_001, np.int64, False)]
+    for _ in range(2):
+        for b in batches:
+            for cfg in cfgs:
+                got = prism_gpu.hash_aggregate(b, cfg)
+                ref = oracle.hash_aggregate(b, cfg)
+                assert_batches_equal(got, ref, float_cols=tuple(i for i in range(ref.num_columns)
+                                                                 if pa.types.is_floating(ref.schema.field(i).type)))
