@@ -1188,6 +1188,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
         a.jmask = t.capacity - 1;
         a.jcap = t.capacity;
         a.jdup = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+        a.jn_dup = t.n_dup_rows;
         a.jdense = t.dense ? static_cast<const uint32_t*>(t.dense_rows->ptr) : nullptr;
         a.jdmin = t.dmin;
         a.jdrange = t.drange;
@@ -1314,6 +1315,7 @@ Batch aggregate(Ctx& ctx, const std::vector<const Batch*>& batches_in, const pri
     uint32_t derr = ctx.take_device_errors();
     const unsigned long long small_n = small_try ? *h_small : ~0ULL;
     if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "aggregation wait timed out");
+    if (derr & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "join table inconsistent (build rows changed while it was built?)");
     if (derr & DERR_TABLE_FULL) {
       if (P.n_distinct) dist_log2 += 1;
       if (!dense) gcap *= 2;

@@ -88,6 +88,7 @@ struct AggArgs {
   uint64_t jmask;
   uint64_t jcap;
   const uint32_t* jdup;      // build rows of multi-row slots
+  int64_t jn_dup;            // their count (a segment past it: DERR_CORRUPT)
   const uint32_t* jdense;    // dense mode: build row per key - jdmin
   int64_t jdmin;
   uint64_t jdrange;
@@ -862,6 +863,10 @@ __device__ __forceinline__ void join_body(const AggArgs& a) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const I idx = base + r * stride;
+      if (cnt[r] > 1 && (int64_t)cand[r] + cnt[r] > a.jn_dup) {  // an inconsistent table
+        atomicOr(a.err, DERR_CORRUPT);
+        continue;
+      }
       for (uint32_t j = 0; j < cnt[r]; ++j) {
         const uint32_t b = cnt[r] == 1 ? cand[r] : a.jdup[cand[r] + j];
         if (!a.jfast) {

@@ -244,7 +244,7 @@ enum DevErr : uint32_t {
   DERR_OVERFLOW = 4,
   DERR_RANGE = 8,
   DERR_CAPACITY = 16,
-  DERR_CORRUPT = 32,  // malformed encoded input (Parquet pages, Snappy streams)
+  DERR_CORRUPT = 32,  // malformed encoded input (Parquet pages, Snappy streams), an inconsistent join table
 };
 
 #ifndef __CUDACC_RTC__

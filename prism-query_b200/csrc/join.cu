@@ -420,6 +420,7 @@ struct ProbeArgs {
   uint64_t mask;
   uint64_t cap;
   const uint32_t* dup_rows;
+  int64_t n_dup_rows;  // a slot's segment past it: the table is inconsistent (DERR_CORRUPT)
   const DCol* pcols;  // verify (general path)
   const DCol* bcols;
   int nkeys;
@@ -583,6 +584,10 @@ __global__ void __launch_bounds__(PW * 32, 2) probe_kernel(K keys, ProbeArgs a) 
         }
         uint32_t cnt = (uint32_t)(e[it].y >> 32);
         if (e[it].x != key[it] || cnt == 0) continue;
+        if (cnt > 1 && (int64_t)(uint32_t)e[it].y + cnt > a.n_dup_rows) {
+          atomicOr(a.err, DERR_CORRUPT);
+          continue;
+        }
         v[it] = (uint32_t)e[it].y;
         cand[it] = cnt;
         if (!VERIFY) {
@@ -1459,6 +1464,7 @@ static void fill_common(Ctx& ctx, const JoinTable& t, const Batch& probe, const 
   a.mask = t.capacity - 1;
   a.cap = t.capacity;
   a.dup_rows = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+  a.n_dup_rows = t.n_dup_rows;
   a.krec = t.key_records ? static_cast<const ulonglong2*>(t.key_records->ptr) : nullptr;
   a.nkeys = (int)keys.size();
   a.err = ctx.d_err;
@@ -1493,6 +1499,7 @@ int64_t probe_count(Ctx& ctx, const JoinTable& t, const Batch& probe, const std:
   PRISM_CUDA(cudaMemcpyAsync(&total, a.total, 8, cudaMemcpyDeviceToHost, ctx.stream));
   uint32_t derr = ctx.take_device_errors();
   if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+  if (derr & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "join table inconsistent (build rows changed while it was built?)");
   return (int64_t)total;
 }
 
@@ -1633,6 +1640,7 @@ ProbeResult probe_join_table(Ctx& ctx, const JoinTable& t, const Batch& probe, c
   PRISM_CUDA(cudaMemcpyAsync(&total, a.total, 8, cudaMemcpyDeviceToHost, ctx.stream));
   uint32_t derr = ctx.take_device_errors();
   if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+  if (derr & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "join table inconsistent (build rows changed while it was built?)");
   if (derr & DERR_CAPACITY) fail(PRISM_ERR_INTERNAL, "probe output capacity exceeded");
   res.matches = (int64_t)total;
   return res;
@@ -1719,6 +1727,7 @@ extern "C" int prism_hash_table_probe_noalloc(prism_ctx* c, const prism_hash_tab
     a.mask = t.capacity - 1;
     a.cap = t.capacity;
     a.dup_rows = t.dup_rows ? static_cast<const uint32_t*>(t.dup_rows->ptr) : nullptr;
+    a.n_dup_rows = t.n_dup_rows;
     a.nkeys = 1;
     a.out_probe = out_probe_idx;
     a.out_build = out_build_idx;
@@ -1739,6 +1748,7 @@ extern "C" int prism_hash_table_probe_noalloc(prism_ctx* c, const prism_hash_tab
     PRISM_CUDA(cudaMemcpyAsync(&tot, total, 8, cudaMemcpyDeviceToHost, ctx.stream));
     uint32_t derr = ctx.take_device_errors();
     if (derr & DERR_TIMEOUT) fail(PRISM_ERR_TIMEOUT, "probe look-back timed out");
+    if (derr & DERR_CORRUPT) fail(PRISM_ERR_INTERNAL, "join table inconsistent (build rows changed while it was built?)");
     *out_matches = (int64_t)tot;
     if (derr & DERR_CAPACITY)
       fail(PRISM_ERR_INVALID_ARGUMENT, "output capacity " + std::to_string(out_capacity) + " is smaller than the " +

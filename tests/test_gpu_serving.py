@@ -20,6 +20,8 @@ def _setup(torch, prism_gpu, ctx):
     for name, n in (("t0", 200_000), ("t1", 1_300_000)):
         keys = torch.randperm(n, generator=g, device=dev)
         pay = torch.randint(-(2**62), 2**62, (n,), generator=g, device=dev)
+        # torch wrote them on its stream; the library reads them on the context's
+        torch.cuda.synchronize()
         db = prism_gpu.DeviceBatch.from_device_buffers([("k", "l", keys.data_ptr()), ("v", "l", pay.data_ptr())], n, ctx)
         tables[name] = (HashTable.build(db, [0], ctx), n, keys, pay)
     kpool = torch.randint(0, 1_600_000, (3_000_000,), generator=g, device=dev)
@@ -27,6 +29,7 @@ def _setup(torch, prism_gpu, ctx):
     akey = gkeys[torch.randint(0, 64, (3_000_000,), generator=g, device=dev)]
     avi = torch.randint(-1000, 1000, (3_000_000,), generator=g, device=dev)
     avf = torch.rand(3_000_000, generator=g, device=dev, dtype=torch.float64)
+    torch.cuda.synchronize()
     cfg = HashAggConfig([0], [AggExpr(1, AggFunc.Sum, "s"), AggExpr(2, AggFunc.Avg, "a"), AggExpr(1, AggFunc.Count, "n"),
                               AggExpr(2, AggFunc.Min, "mn")])
     return tables, kpool, (akey, avi, avf), cfg
@@ -127,6 +130,7 @@ def test_device_queue_results_equal_alone(ctx):
     n = 700_000
     sparse = torch.randperm(n, generator=g, device=dev) * 7919 + 3  # no dense table: hash slots
     pay = torch.randint(-(2**62), 2**62, (n,), generator=g, device=dev)
+    torch.cuda.synchronize()  # (written on torch's stream, read on the context's)
     db = prism_gpu.DeviceBatch.from_device_buffers([("k", "l", sparse.data_ptr()), ("v", "l", pay.data_ptr())], n, ctx)
     th = prism_gpu.HashTable.build(db, [0], ctx)
     assert th.layout == "hash" and tables["t0"][0].layout == "dense"
